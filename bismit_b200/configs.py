@@ -1,0 +1,170 @@
+"""Area schemes for the benchmark workloads and the parity cases, plus seeded
+synthetic input frames.
+
+The benchmark area (one cortical area fed by a subcortical "external" area):
+
+    aff_in   spatial input, depth 1, from the external area's THAL_SP output
+    iv       spiny stellate (PSAL), depth 1, one basal proximal tuft
+             1 x S synapses from aff_in, reach 6, threshold 0 (the default)
+    iv_inhib InhibitoryBasketSurround on iv, radius 4
+    iii      pyramidal (PTAL), depth D, output layer:
+               basal proximal tuft from iv, basal distal tuft 16 x 32 from iii,
+               reach 6, max_active_dens_l2 = 3
+    iii_col  IntraColumnInhib on iii
+
+Workload sizes:
+  area_64   64 x 64 columns, S = 32, D = 1, proximal 1 x 1 reach 0
+            (2,232,320 synapses)
+  area_256  256 x 256 columns, S = 64, D = 4, proximal 16 x 32 reach 6
+            (272,629,760 synapses)
+Settings: regrowth disabled, learning on, strengths start at 0.
+"""
+import numpy as np
+
+from .map import (AreaScheme, AreaSchemeList, AxonDomain, AxonTopology, CellScheme, ControlCellKind,
+                  CorticalAreaSettings, InputTrack, LayerMapKind, LayerMapScheme, LayerMapSchemeList,
+                  LayerScheme, LayerTags, THAL_NSP, THAL_SP, TuftScheme, TuftSourceLayer)
+
+
+def _external(lmaps, areas, name, side, u_side=None, nonspatial=False):
+    lm = LayerMapScheme(name + "_lm", LayerMapKind.Subcortical)
+    lm.layer(LayerScheme.define("ganglion").depth(1).axonal(AxonTopology.Spatial)
+             .axon_domain(AxonDomain.output([THAL_SP])))
+    if nonspatial:
+        lm.layer(LayerScheme.define("ganglion_ns").depth(1).axonal(AxonTopology.Nonspatial)
+                 .axon_domain(AxonDomain.output([THAL_NSP])))
+    lmaps.add(lm)
+    areas.area(AreaScheme(name, lm.name, side, u_side))
+
+
+def benchmark_area(side, ssc_syns, pyr_depth, prox_dens, prox_syns, prox_reach, name="v1"):
+    """The benchmark layer map on a `side` x `side` area."""
+    lmaps = LayerMapSchemeList()
+    areas = AreaSchemeList()
+    _external(lmaps, areas, "v0", side)
+    lm = LayerMapScheme("visual", LayerMapKind.Cortical)
+    lm.layer(LayerScheme.define("aff_in").axonal(AxonTopology.Spatial)
+             .axon_domain(AxonDomain.input([(InputTrack.Afferent, [THAL_SP])])))
+    lm.layer(LayerScheme.define("iv").depth(1).tags(LayerTags.PSAL).axon_domain(AxonDomain.Local)
+             .cellular(CellScheme.spiny_stellate()
+                       .tft(TuftScheme.basal().proximal().syns_per_den(ssc_syns)
+                            .src_lyr(TuftSourceLayer.define("aff_in").syn_reach(6).prevalence(1)))))
+    lm.layer(LayerScheme.define("iv_inhib")
+             .cellular(CellScheme.control(ControlCellKind.InhibitoryBasketSurround("iv", 4), 0)))
+    lm.layer(LayerScheme.define("iii").depth(pyr_depth).tags(LayerTags.PTAL)
+             .axon_domain(AxonDomain.output([THAL_SP]))
+             .cellular(CellScheme.pyramidal()
+                       .tft(TuftScheme.basal().proximal().dens_per_tft(prox_dens).syns_per_den(prox_syns)
+                            .src_lyr(TuftSourceLayer.define("iv").syn_reach(prox_reach).prevalence(1)))
+                       .tft(TuftScheme.basal().distal().dens_per_tft(16).syns_per_den(32)
+                            .max_active_dens_l2(3)
+                            .src_lyr(TuftSourceLayer.define("iii").syn_reach(6).prevalence(1)))))
+    lm.layer(LayerScheme.define("iii_col")
+             .cellular(CellScheme.control(ControlCellKind.IntraColumnInhib("iii"), 0)))
+    lmaps.add(lm)
+    areas.area(AreaScheme(name, "visual", side).eff_areas(["v0"]))
+    return lmaps, areas
+
+
+def bench_settings():
+    return CorticalAreaSettings().disable_regrowth().strengths_start_at_zero()
+
+
+WORKLOADS = {
+    # name: (side, ssc_syns, pyr_depth, prox_dens, prox_syns, prox_reach, input active fraction)
+    "area_64": (64, 32, 1, 1, 1, 0, 0.02),
+    "area_256": (256, 64, 4, 16, 32, 6, 0.03),
+    "area_128": (128, 32, 2, 1, 1, 0, 0.02),
+    "area_32": (32, 32, 1, 1, 1, 0, 0.02),
+    "area_48_deep": (48, 32, 2, 4, 16, 3, 0.03),
+}
+
+
+def workload(name):
+    side, s, d, pd, ps, pr, act = WORKLOADS[name]
+    lmaps, areas = benchmark_area(side, s, d, pd, ps, pr)
+    return lmaps, areas, act
+
+
+def testbed_area(side=24):
+    """The reference's test bed layer map (src/tests/testbed.rs:18-208) without
+    its retina filter chain: spatial input, a spiny stellate layer with a
+    threshold of 400, basket inhibition and a 3-deep pyramidal layer with a
+    basal distal and an apical distal tuft (both learn, in tuft order)."""
+    lmaps = LayerMapSchemeList()
+    areas = AreaSchemeList()
+    _external(lmaps, areas, "v0", side)
+    lm = LayerMapScheme("visual", LayerMapKind.Cortical)
+    lm.layer(LayerScheme.define("motor_in").depth(1).axonal(AxonTopology.Nonspatial)
+             .axon_domain(AxonDomain.input([(InputTrack.Afferent, ["thal_motor"])])))
+    lm.layer(LayerScheme.define("eff_in").axonal(AxonTopology.Spatial)
+             .axon_domain(AxonDomain.input([(InputTrack.Efferent, [THAL_SP])])))
+    lm.layer(LayerScheme.define("aff_in").axonal(AxonTopology.Spatial)
+             .axon_domain(AxonDomain.input([(InputTrack.Afferent, [THAL_SP])])))
+    lm.layer(LayerScheme.define("out").depth(1).axonal(AxonTopology.Spatial)
+             .axon_domain(AxonDomain.output([THAL_SP])))
+    lm.layer(LayerScheme.define("unused").depth(1).tags(LayerTags.UNUSED).axonal(AxonTopology.Spatial)
+             .axon_domain(AxonDomain.Local))
+    lm.layer(LayerScheme.define("iv").depth(1).tags(LayerTags.PSAL).axon_domain(AxonDomain.Local)
+             .cellular(CellScheme.spiny_stellate()
+                       .tft(TuftScheme.basal().proximal().syns_per_den(32).thresh_init(400)
+                            .src_lyr(TuftSourceLayer.define("aff_in").syn_reach(8).prevalence(1)))))
+    lm.layer(LayerScheme.define("iv_inhib")
+             .cellular(CellScheme.control(ControlCellKind.InhibitoryBasketSurround("iv", 4), 0)))
+    lm.layer(LayerScheme.define("iii").depth(3).tags(LayerTags.PTAL).axon_domain(AxonDomain.Local)
+             .cellular(CellScheme.pyramidal()
+                       .tft(TuftScheme.basal().distal().dens_per_tft(4).syns_per_den(8).max_active_dens_l2(0)
+                            .thresh_init(1200).src_lyr(TuftSourceLayer.define("iii").syn_reach(16).prevalence(1)))
+                       .tft(TuftScheme.apical().distal().dens_per_tft(2).syns_per_den(32).max_active_dens_l2(0)
+                            .thresh_init(500).src_lyr(TuftSourceLayer.define("iii").syn_reach(3).prevalence(1)))))
+    lmaps.add(lm)
+    areas.area(AreaScheme("v1", "visual", side).eff_areas(["v0"]))
+    return lmaps, areas
+
+
+def mixed_area(side=32, src_side=48):
+    """A parity case that exercises the remaining index and control paths:
+    a scaled input slice (source area larger than the area), a nonspatial input
+    slice, prevalence repeats, a proximal+distal+apical pyramidal layer whose
+    two distal tufts learn in order, PyrOutputter followed by IntraColumnInhib
+    on the same host, and non-zero dendrite thresholds."""
+    lmaps = LayerMapSchemeList()
+    areas = AreaSchemeList()
+    _external(lmaps, areas, "v0", src_side, nonspatial=True)
+    lm = LayerMapScheme("visual", LayerMapKind.Cortical)
+    lm.layer(LayerScheme.define("aff_in").axonal(AxonTopology.Spatial)
+             .axon_domain(AxonDomain.input([(InputTrack.Afferent, [THAL_SP])])))
+    lm.layer(LayerScheme.define("ns_in").axonal(AxonTopology.Nonspatial)
+             .axon_domain(AxonDomain.input([(InputTrack.Afferent, [THAL_NSP])])))
+    lm.layer(LayerScheme.define("iv").depth(2).tags(LayerTags.PSAL)
+             .cellular(CellScheme.spiny_stellate()
+                       .tft(TuftScheme.basal().proximal().syns_per_den(24).thresh_init(40)
+                            .src_lyr(TuftSourceLayer.define("aff_in").syn_reach(4).prevalence(2)))))
+    lm.layer(LayerScheme.define("iv_inhib")
+             .cellular(CellScheme.control(ControlCellKind.InhibitoryBasketSurround("iv", 3), 0)))
+    lm.layer(LayerScheme.define("iii").depth(3).tags(LayerTags.PTAL).axon_domain(AxonDomain.output([THAL_SP]))
+             .cellular(CellScheme.pyramidal()
+                       .tft(TuftScheme.basal().proximal().dens_per_tft(2).syns_per_den(16).thresh_init(8)
+                            .src_lyr(TuftSourceLayer.define("iv").syn_reach(3).prevalence(1)))
+                       .tft(TuftScheme.basal().distal().dens_per_tft(8).syns_per_den(16).max_active_dens_l2(2)
+                            .thresh_init(4).src_lyr(TuftSourceLayer.define("iii").syn_reach(4).prevalence(1)))
+                       .tft(TuftScheme.apical().distal().dens_per_tft(4).syns_per_den(12).max_active_dens_l2(1)
+                            .src_lyr(TuftSourceLayer.define("ns_in").syn_reach(0).prevalence(1)))))
+    lm.layer(LayerScheme.define("iii_out")
+             .cellular(CellScheme.control(ControlCellKind.PyrOutputter("iii"), 0)))
+    lm.layer(LayerScheme.define("iii_col")
+             .cellular(CellScheme.control(ControlCellKind.IntraColumnInhib("iii"), 1)))
+    lmaps.add(lm)
+    areas.area(AreaScheme("v1", "visual", side).eff_areas(["v0"]))
+    return lmaps, areas
+
+
+def frames(n, length, active, seed, start=0):
+    """n seeded u8 frames: each axon active with probability `active`, active
+    values uniform in 1..255 (frame k depends only on (seed, start + k))."""
+    out = np.zeros((n, length), dtype=np.uint8)
+    for k in range(n):
+        rng = np.random.default_rng([int(seed) & 0xFFFFFFFF, 0x6672616D, start + k])
+        m = rng.random(length) < active
+        out[k, m] = rng.integers(1, 256, size=int(m.sum()), dtype=np.uint16).astype(np.uint8)
+    return out

@@ -1,0 +1,238 @@
+"""Cortex and CorticalArea: the host objects of the cortical cycle.
+
+Mirrors the reference's drop-in surface for this path
+(src/cortex/cortex.rs:37-201, src/cortex/cortical_area.rs:343-1321):
+``Cortex.builder(layer_map_schemes, area_schemes).ca_settings(..).build()``,
+``cortex.cycle()``, per-area ``cycle``, input intake and output, and the raw
+buffer read/write/fill helpers of the reference's test traits. Every call goes
+through the C ABI of the native library; errors raise BismitError.
+"""
+import ctypes as C
+
+import numpy as np
+
+from . import _ffi as F
+from .map import (AreaSchemeList, CorticalAreaSettings, LayerMapKind, LayerMapSchemeList, area_desc)
+
+
+class _Ctx:
+    def __init__(self, device=0):
+        self.lib = F.lib()
+        self.h = C.c_void_p()
+        F.check(self.lib.bm_ctx_create(int(device), 0, C.byref(self.h)))
+        self.device = device
+
+    def set_stream(self, stream_ptr):
+        F.check(self.lib.bm_ctx_set_stream(self.h, C.c_void_p(stream_ptr or 0)))
+
+    def synchronize(self):
+        F.check(self.lib.bm_ctx_synchronize(self.h))
+
+    def close(self):
+        if self.h:
+            self.lib.bm_ctx_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class CorticalArea:
+    """One cortical area on the device (CorticalArea, src/cortex/cortical_area.rs:343)."""
+
+    def __init__(self, ctx, desc, seed, name=""):
+        self.lib = F.lib()
+        self.ctx = ctx
+        self.name = name
+        self.desc = desc
+        self.h = C.c_void_p()
+        F.check(self.lib.bm_area_create(ctx.h, C.byref(desc), C.c_uint64(seed), C.byref(self.h)))
+        self.plan = F.bm_area_plan()
+        F.check(self.lib.bm_area_get_plan(self.h, C.byref(self.plan)))
+        self.layer_names = [desc.layers[i].name.decode() for i in range(desc.n_layers)]
+
+    # ---- structure ----
+    def data_layer(self, name_or_idx):
+        """Plan index of a data (cellular) layer, by scheme name or plan index."""
+        if isinstance(name_or_idx, int):
+            return name_or_idx
+        lid = self.layer_names.index(name_or_idx)
+        for i in range(self.plan.n_layers):
+            if self.plan.layers[i].layer_id == lid:
+                return i
+        raise KeyError("%r is not a cellular layer" % name_or_idx)
+
+    @property
+    def n_syns(self):
+        return int(self.plan.n_syns_total)
+
+    @property
+    def slab_bytes(self):
+        return int(self.plan.slab_bytes)
+
+    def input_len(self, idx=0):
+        return int(self.plan.inputs[idx].len)
+
+    def output_len(self, idx=0):
+        return int(self.plan.outputs[idx].len)
+
+    # ---- cycle ----
+    def write_input(self, frame, idx=0):
+        """AxonSpace::intake: one u8 frame into input layer `idx` (src/cortex/axon_space.rs:509)."""
+        a = np.ascontiguousarray(frame, dtype=np.uint8)
+        F.check(self.lib.bm_area_write_input(self.h, idx, a.ctypes.data_as(C.c_void_p), a.nbytes))
+
+    def cycle(self, n=1):
+        """CorticalArea::cycle n times (src/cortex/cortical_area.rs:716)."""
+        F.check(self.lib.bm_area_cycle(self.h, int(n)))
+
+    def cycle_frames_device(self, dev_ptr, frame_len, n):
+        F.check(self.lib.bm_area_cycle_frames_device(self.h, C.c_void_p(dev_ptr), frame_len, int(n)))
+
+    def read_output(self, idx=0):
+        """AxonSpace::output: the output layer's axons (src/cortex/axon_space.rs:594)."""
+        out = np.empty(self.output_len(idx), dtype=np.uint8)
+        F.check(self.lib.bm_area_read_output(self.h, idx, out.ctypes.data_as(C.c_void_p), out.nbytes))
+        return out
+
+    # ---- raw buffers (sampler / test-trait surface) ----
+    def read(self, buf, layer=0, offset=0, length=None):
+        kind = F.BM_BUF_AXON_STATES if buf == "axon_states" else F.BUF[buf]
+        li = 0 if kind == F.BM_BUF_AXON_STATES else self.data_layer(layer)
+        if length is None:
+            length = (self.plan.n_axons if kind == F.BM_BUF_AXON_STATES
+                      else self.plan.layers[li].buf_len[kind]) - offset
+        dt = np.int8 if buf in F.SIGNED_BUFS else np.uint8
+        out = np.empty(int(length), dtype=dt)
+        F.check(self.lib.bm_area_read(self.h, kind, li, int(offset), out.ctypes.data_as(C.c_void_p), out.nbytes))
+        return out
+
+    def write(self, buf, data, layer=0, offset=0):
+        kind = F.BM_BUF_AXON_STATES if buf == "axon_states" else F.BUF[buf]
+        li = 0 if kind == F.BM_BUF_AXON_STATES else self.data_layer(layer)
+        a = np.ascontiguousarray(data)
+        a = a.view(np.uint8) if a.dtype.itemsize == 1 else a.astype(np.uint8)
+        F.check(self.lib.bm_area_write(self.h, kind, li, int(offset), a.ctypes.data_as(C.c_void_p), a.nbytes))
+
+    def fill(self, buf, value, layer=0):
+        n = int(self.plan.n_axons) if buf == "axon_states" else int(self.plan.layers[self.data_layer(layer)].buf_len[F.BUF[buf]])
+        self.write(buf, np.full(n, value, dtype=np.int8 if buf in F.SIGNED_BUFS else np.uint8), layer)
+
+    def read_slab(self):
+        out = np.empty(self.slab_bytes, dtype=np.uint8)
+        F.check(self.lib.bm_area_read_slab(self.h, out.ctypes.data_as(C.c_void_p), out.nbytes))
+        return out
+
+    def write_slab(self, data):
+        a = np.ascontiguousarray(data, dtype=np.uint8)
+        F.check(self.lib.bm_area_write_slab(self.h, a.ctypes.data_as(C.c_void_p), a.nbytes))
+
+    def cycle_count(self):
+        v = C.c_uint64()
+        F.check(self.lib.bm_area_get_cycle(self.h, C.byref(v)))
+        return v.value
+
+    def set_cycle(self, c):
+        F.check(self.lib.bm_area_set_cycle(self.h, C.c_uint64(c)))
+
+    def slab_ptr(self):
+        p = C.c_void_p()
+        F.check(self.lib.bm_area_slab_ptr(self.h, C.byref(p)))
+        return p.value
+
+    # ---- timing ----
+    def set_profiling(self, on):
+        F.check(self.lib.bm_area_set_profiling(self.h, 1 if on else 0))
+
+    def profile(self):
+        n = 32
+        names = (C.c_char_p * n)()
+        launches = (C.c_uint64 * n)()
+        ms = (C.c_double * n)()
+        got = C.c_uint32()
+        F.check(self.lib.bm_area_get_profile(self.h, n, names, launches, ms, C.byref(got)))
+        return {names[i].decode(): (int(launches[i]), float(ms[i])) for i in range(got.value)}
+
+    def reset_profile(self):
+        F.check(self.lib.bm_area_reset_profile(self.h))
+
+    def launches_per_cycle(self):
+        v = C.c_uint32()
+        F.check(self.lib.bm_area_launches_per_cycle(self.h, C.byref(v)))
+        return v.value
+
+    def close(self):
+        if self.h:
+            self.lib.bm_area_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Cortex:
+    """A set of cortical areas cycled in order (Cortex, src/cortex/cortex.rs:37-120)."""
+
+    def __init__(self, lmaps, areas, settings=None, seed=0, device=0):
+        self.ctx = _Ctx(device)
+        self.areas = {}
+        self._order = []
+        for a in areas.areas:
+            if lmaps[a.layer_map_name].kind != LayerMapKind.Cortical:
+                continue
+            d = area_desc(a.name, lmaps, areas, settings)
+            self.areas[a.name] = CorticalArea(self.ctx, d, seed, a.name)
+            self._order.append(a.name)
+
+    @staticmethod
+    def builder(lmaps, areas):
+        return CortexBuilder(lmaps, areas)
+
+    def cycle(self):
+        """Cortex::cycle: every area once, in area order (src/cortex/cortex.rs:100-120)."""
+        for n in self._order:
+            self.areas[n].cycle(1)
+
+    def area(self, name):
+        return self.areas[name]
+
+    def synchronize(self):
+        self.ctx.synchronize()
+
+    def close(self):
+        for a in self.areas.values():
+            a.close()
+        self.ctx.close()
+
+
+class CortexBuilder:
+    """Cortex::builder(..).ca_settings(..).build() (src/cortex/cortex.rs:158-201)."""
+
+    def __init__(self, lmaps, areas):
+        if not isinstance(lmaps, LayerMapSchemeList) or not isinstance(areas, AreaSchemeList):
+            raise TypeError("Cortex.builder takes a LayerMapSchemeList and an AreaSchemeList")
+        self.lmaps, self.areas_ = lmaps, areas
+        self._settings = None
+        self._seed = 0
+        self._device = 0
+
+    def ca_settings(self, s):
+        self._settings = s
+        return self
+
+    def seed(self, seed):
+        self._seed = int(seed)
+        return self
+
+    def device(self, d):
+        self._device = int(d)
+        return self
+
+    def build(self):
+        return Cortex(self.lmaps, self.areas_, self._settings, self._seed, self._device)

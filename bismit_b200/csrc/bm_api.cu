@@ -1,0 +1,628 @@
+// bm_api.cu -- the C ABI (include/bismit_b200.h): contexts, areas, the cycle
+// scheduler and buffer I/O. The stage order is CorticalArea::cycle
+// (src/cortex/cortical_area.rs:716-789) with the layer cycles of
+// SpinyStellateLayer::cycle (src/cortex/spiny_stellates.rs:220-252) and
+// PyramidalLayer::cycle (src/cortex/pyramidals.rs:297-335).
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "bm_fused.h"
+#include "bm_kernels.h"
+#include "bm_layout.h"
+
+using namespace bm;
+
+namespace {
+
+thread_local std::string g_err;
+
+int set_err(int code, const char* fmt, ...) __attribute__((format(printf, 2, 3)));
+int set_err(int code, const char* fmt, ...) {
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g_err = buf;
+    return code;
+}
+
+int cuda_err(cudaError_t e, const char* what) {
+    return set_err(e == cudaErrorMemoryAllocation ? BM_ERR_OOM : BM_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+
+#define CU(call)                                                   \
+    do {                                                           \
+        cudaError_t e_ = (call);                                   \
+        if (e_ != cudaSuccess) return cuda_err(e_, #call);         \
+    } while (0)
+
+// Kernel kinds for per-launch timing.
+enum Kind {
+    K_SYN_FLAGS, K_SYN_CYCLE, K_DEN_CYCLE, K_TFT_CYCLE, K_SSC_CYCLE, K_INHIB_SIMPLE, K_INHIB_PASS,
+    K_SSC_MTP, K_PYR_CYCLE, K_PYR_OUTPUT, K_INTRA_COL, K_TFT_DST_MTP, K_CYCLE_END, K_INTAKE,
+    K_FUSED_TUFT, K_FUSED_SSC_SOMA, K_FUSED_PYR_SOMA, K_FUSED_SSC_MTP, K_COUNT
+};
+const char* const kKindNames[K_COUNT] = {
+    "tft_set_syn_flags", "syn_cycle", "den_cycle_tft", "tft_cycle", "ssc_cycle", "inhib_simple",
+    "inhib_passthrough", "ssc_mtp_simple", "pyr_cycle", "pyr_output", "inhib_intra_column", "tft_dst_mtp",
+    "cycle_end", "intake", "fused_tuft_cycle", "fused_ssc_soma_inhib", "fused_pyr_soma_learn",
+    "fused_ssc_mtp"};
+
+struct DevGuard {
+    int prev = -1;
+    explicit DevGuard(int dev) {
+        cudaGetDevice(&prev);
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DevGuard() {
+        int cur;
+        cudaGetDevice(&cur);
+        if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+}  // namespace
+
+struct bm_ctx_s {
+    int device = 0;
+    cudaStream_t own = nullptr;
+    cudaStream_t user = nullptr;
+    cudaStream_t stream() const { return user ? user : own; }
+};
+
+struct bm_area_s {
+    bm_ctx ctx = nullptr;
+    bm_area_plan plan;
+    uint8_t* slab = nullptr;
+    AreaCtl* ctl = nullptr;
+    SliceRec* slices = nullptr;
+    DevLayer dl[BM_MAX_LAYERS];
+    uint64_t inhib_key[BM_MAX_LAYERS][BM_MAX_CTRL];
+    uint64_t host_cycle = 0;
+    uint32_t exec_path = BM_PATH_FUSED;
+    FusedArea fused;
+    bool profiling = false;
+    struct Rec { int kind; cudaEvent_t a, b; };
+    std::vector<Rec> pending;
+    std::vector<cudaEvent_t> pool;
+    uint64_t prof_launches[K_COUNT] = {};
+    double prof_ms[K_COUNT] = {};
+    uint32_t launches = 0;   // kernel launches of the last enqueued cycle
+
+    cudaStream_t stream() const { return ctx->stream(); }
+    uint8_t* axns() const { return slab + plan.axon_off; }
+
+    cudaEvent_t ev() {
+        if (!pool.empty()) { cudaEvent_t e = pool.back(); pool.pop_back(); return e; }
+        cudaEvent_t e = nullptr;
+        cudaEventCreate(&e);
+        return e;
+    }
+    template <class F> void run(int kind, F&& f) {
+        if (kind != K_INTAKE) launches++;
+        if (!profiling) { f(); return; }
+        Rec r{kind, ev(), ev()};
+        cudaEventRecord(r.a, stream());
+        f();
+        cudaEventRecord(r.b, stream());
+        pending.push_back(r);
+    }
+    void drain_profile() {
+        for (auto& r : pending) {
+            float ms = 0.f;
+            cudaEventSynchronize(r.b);
+            cudaEventElapsedTime(&ms, r.a, r.b);
+            prof_launches[r.kind]++;
+            prof_ms[r.kind] += ms;
+            pool.push_back(r.a);
+            pool.push_back(r.b);
+        }
+        pending.clear();
+    }
+};
+
+namespace {
+
+// Control layers hosted on data layer i, in (host, exe_order) order.
+void enqueue_controls(bm_area_s* A, uint32_t i) {
+    const bm_layer_plan& L = A->plan.layers[i];
+    const DevLayer& D = A->dl[i];
+    cudaStream_t s = A->stream();
+    for (uint32_t k = 0; k < L.n_ctrl; k++) {
+        const bm_ctrl_plan& C = L.ctrl[k];
+        if (C.kind == BM_LYR_CTRL_INHIB_BASKET) {
+            if (A->plan.settings & BM_SET_BYPASS_INHIB)
+                A->run(K_INHIB_PASS, [&] { launch_inhib_passthrough(A->axns(), A->slices, D, s); });
+            else
+                A->run(K_INHIB_SIMPLE, [&] {
+                    launch_inhib_simple(A->axns(), A->slices, D, (int)C.field_radius, A->inhib_key[i][k], A->ctl, s);
+                });
+        } else if (C.kind == BM_LYR_CTRL_PYR_OUTPUT) {
+            A->run(K_PYR_OUTPUT, [&] { launch_pyr_output(A->axns(), A->slices, D, s); });
+        } else if (C.kind == BM_LYR_CTRL_INTRA_COLUMN) {
+            A->run(K_INTRA_COL, [&] { launch_inhib_intra_column_plain(A->axns(), A->slices, D, s); });
+        }
+    }
+}
+
+void enqueue_dens_plain(bm_area_s* A, uint32_t i) {
+    const bm_layer_plan& L = A->plan.layers[i];
+    const DevLayer& D = A->dl[i];
+    cudaStream_t s = A->stream();
+    A->run(K_SYN_FLAGS, [&] { launch_set_syn_flags(D, s); });
+    for (uint32_t t = 0; t < L.n_tufts; t++)
+        A->run(K_SYN_CYCLE, [&] { launch_syn_cycle_plain(A->axns(), A->slices, D, t, s); });
+    for (uint32_t t = 0; t < L.n_tufts; t++)
+        A->run(K_DEN_CYCLE, [&] { launch_den_cycle_plain(D, t, A->ctl, s); });
+}
+
+void enqueue_pyr_learn(bm_area_s* A, uint32_t i) {
+    const bm_layer_plan& L = A->plan.layers[i];
+    if (A->plan.settings & (BM_SET_DISABLE_LEARNING | BM_SET_DISABLE_PYRS)) return;
+    for (uint32_t t = 0; t < L.n_tufts; t++)
+        if (L.tufts[t].den_kind == BM_DEN_DISTAL)
+            A->run(K_TFT_DST_MTP, [&] { launch_tft_dst_mtp_plain(A->axns(), A->dl[i], t, A->ctl, A->stream()); });
+}
+
+void enqueue_layer_cycle(bm_area_s* A, uint32_t i) {
+    const bm_layer_plan& L = A->plan.layers[i];
+    const DevLayer& D = A->dl[i];
+    cudaStream_t s = A->stream();
+    bool fused = A->exec_path == BM_PATH_FUSED && A->fused.layer_ok[i];
+    if (L.kind == BM_LYR_SPINY_STELLATE) {
+        if (fused) {
+            for (uint32_t t = 0; t < L.n_tufts; t++)
+                A->run(K_FUSED_TUFT, [&] { launch_fused_tuft(A->fused, A->axns(), A->slices, D, i, t, A->ctl, s); });
+        } else {
+            enqueue_dens_plain(A, i);
+        }
+        A->run(K_SSC_CYCLE, [&] { launch_ssc_cycle(D, s); });
+        enqueue_controls(A, i);
+    } else {
+        if (fused) {
+            for (uint32_t t = 0; t < L.n_tufts; t++)
+                A->run(K_FUSED_TUFT, [&] { launch_fused_tuft(A->fused, A->axns(), A->slices, D, i, t, A->ctl, s); });
+        } else {
+            enqueue_dens_plain(A, i);
+            for (uint32_t t = 0; t < L.n_tufts; t++)
+                A->run(K_TFT_CYCLE, [&] { launch_tft_cycle_plain(D, t, s); });
+        }
+        A->run(K_PYR_CYCLE, [&] { launch_pyr_cycle_plain(D, s); });
+        enqueue_controls(A, i);
+        enqueue_pyr_learn(A, i);
+    }
+}
+
+void enqueue_layer_learn(bm_area_s* A, uint32_t i) {
+    const bm_layer_plan& L = A->plan.layers[i];
+    if (L.kind == BM_LYR_SPINY_STELLATE) {
+        if (A->plan.settings & (BM_SET_DISABLE_LEARNING | BM_SET_DISABLE_SSCS)) return;
+        A->run(K_SSC_MTP, [&] { launch_ssc_mtp_plain(A->axns(), A->dl[i], A->ctl, A->stream()); });
+    } else {
+        enqueue_pyr_learn(A, i);
+    }
+}
+
+// CorticalArea::cycle, src/cortex/cortical_area.rs:716-789 (intake happens
+// before this call; regrowth is rejected at build; output is read on demand).
+void enqueue_cycle(bm_area_s* A) {
+    const bm_area_plan& P = A->plan;
+    A->launches = 0;
+    if (!(P.settings & BM_SET_DISABLE_SSCS)) {
+        for (uint32_t k = 0; k < P.n_cycle_order; k++)
+            if (P.layers[P.cycle_order[k]].tags & BM_TAG_SPATIAL) enqueue_layer_cycle(A, P.cycle_order[k]);
+        for (uint32_t k = 0; k < P.n_cycle_order; k++)
+            if (P.layers[P.cycle_order[k]].tags & BM_TAG_SPATIAL) enqueue_layer_learn(A, P.cycle_order[k]);
+    }
+    if (!(P.settings & BM_SET_DISABLE_PYRS)) {
+        for (uint32_t k = 0; k < P.n_cycle_order; k++)
+            if (!(P.layers[P.cycle_order[k]].tags & BM_TAG_SPATIAL)) enqueue_layer_cycle(A, P.cycle_order[k]);
+    }
+    A->run(K_CYCLE_END, [&] { launch_cycle_end(A->ctl, A->stream()); });
+    A->host_cycle++;
+}
+
+bool buf_range(bm_area_s* A, uint32_t kind, uint32_t layer, uint64_t offset, uint64_t len, uint64_t* off_out) {
+    const bm_area_plan& P = A->plan;
+    if (kind == BM_BUF_AXON_STATES) {
+        if (offset > P.n_axons || len > P.n_axons - offset) return false;
+        *off_out = P.axon_off + offset;
+        return true;
+    }
+    if (kind >= BM_BUF_COUNT || layer >= P.n_layers) return false;
+    const bm_layer_plan& L = P.layers[layer];
+    if (L.buf_off[kind] == UINT64_MAX) return false;
+    if (offset > L.buf_len[kind] || len > L.buf_len[kind] - offset) return false;
+    *off_out = L.buf_off[kind] + offset;
+    return true;
+}
+
+void build_dev_layers(bm_area_s* A) {
+    const bm_area_plan& P = A->plan;
+    for (uint32_t i = 0; i < P.n_layers; i++) {
+        const bm_layer_plan& L = P.layers[i];
+        DevLayer& D = A->dl[i];
+        std::memset(&D, 0, sizeof D);
+        D.kind = L.kind;
+        D.depth = L.depth;
+        D.v_size = L.v_size;
+        D.u_size = L.u_size;
+        D.cells = L.cells;
+        D.base_slc = L.base_axn_slc;
+        D.axn_idz = L.axn_idz;
+        D.n_tufts = L.n_tufts;
+        D.enabled_flags = L.enabled_tft_flags;
+        D.prx_id = L.bsl_prx_tft_id;
+        D.dst_id = L.bsl_dst_tft_id;
+        D.apc_id = L.apc_dst_tft_id;
+        D.n_syns = L.n_syns;
+        for (int k = 0; k < BM_BUF_COUNT; k++)
+            D.buf[k] = L.buf_off[k] == UINT64_MAX ? nullptr : A->slab + L.buf_off[k];
+        for (uint32_t t = 0; t < L.n_tufts; t++) {
+            const bm_tuft_plan& T = L.tufts[t];
+            DevTuft& DT = D.tft[t];
+            DT.dpt = T.dens_per_tft;
+            DT.spd = T.syns_per_den;
+            DT.spt = T.syns_per_tft;
+            DT.mad_l2 = T.max_active_dens_l2;
+            DT.thresh = T.den_threshold;
+            DT.den_kind = T.den_kind;
+            DT.syn_idz = T.syn_idz;
+            DT.den_idz = T.den_idz;
+            DT.cel_idz = T.cel_idz;
+            DT.rnd_key_den = rnd_key(P.rnd_seed, P.area_id, L.layer_id, BM_RND_DEN_CYCLE, t);
+            DT.rnd_key_mtp = rnd_key(P.rnd_seed, P.area_id, L.layer_id, BM_RND_TFT_DST_MTP, t);
+        }
+        D.rnd_key_ssc_mtp = rnd_key(P.rnd_seed, P.area_id, L.layer_id, BM_RND_SSC_MTP, 0);
+        for (uint32_t k = 0; k < L.n_ctrl; k++)
+            A->inhib_key[i][k] = rnd_key(P.rnd_seed, P.area_id, L.ctrl[k].layer_id, BM_RND_INHIB, 0);
+    }
+}
+
+void free_area(bm_area_s* A) {
+    if (!A) return;
+    if (A->ctx) {
+        DevGuard g(A->ctx->device);
+        if (A->slab) cudaFree(A->slab);
+        if (A->ctl) cudaFree(A->ctl);
+        if (A->slices) cudaFree(A->slices);
+        free_fused(A->fused);
+        for (auto& r : A->pending) { cudaEventDestroy(r.a); cudaEventDestroy(r.b); }
+        for (auto e : A->pool) cudaEventDestroy(e);
+    }
+    delete A;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* bm_last_error(void) { return g_err.c_str(); }
+
+const char* bm_version(void) { return "bismit_b200 0.1 (sm_100a)"; }
+
+int32_t bm_rnd(uint64_t seed, uint32_t area_id, uint32_t layer_id, uint32_t role, uint32_t tft_id, uint64_t cycle) {
+    return rnd_at(rnd_key(seed, area_id, layer_id, role, tft_id), cycle);
+}
+
+int bm_ctx_create(int device, uint32_t flags, bm_ctx* out) {
+    (void)flags;
+    if (!out) return set_err(BM_ERR_INVALID, "bm_ctx_create: null out");
+    *out = nullptr;
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess || n == 0) return set_err(BM_ERR_NO_DEVICE, "no CUDA device (%s)", cudaGetErrorString(e));
+    if (device < 0 || device >= n) return set_err(BM_ERR_NO_DEVICE, "device %d out of range (%d devices)", device, n);
+    DevGuard g(device);
+    bm_ctx c = new (std::nothrow) bm_ctx_s;
+    if (!c) return set_err(BM_ERR_OOM, "host allocation failed");
+    c->device = device;
+    e = cudaStreamCreateWithFlags(&c->own, cudaStreamNonBlocking);
+    if (e != cudaSuccess) { delete c; return cuda_err(e, "cudaStreamCreate"); }
+    *out = c;
+    return BM_OK;
+}
+
+int bm_ctx_destroy(bm_ctx ctx) {
+    if (!ctx) return BM_OK;
+    DevGuard g(ctx->device);
+    if (ctx->own) { cudaStreamSynchronize(ctx->own); cudaStreamDestroy(ctx->own); }
+    delete ctx;
+    return BM_OK;
+}
+
+int bm_ctx_set_stream(bm_ctx ctx, void* stream) {
+    if (!ctx) return set_err(BM_ERR_INVALID, "null ctx");
+    ctx->user = (cudaStream_t)stream;
+    return BM_OK;
+}
+
+int bm_ctx_synchronize(bm_ctx ctx) {
+    if (!ctx) return set_err(BM_ERR_INVALID, "null ctx");
+    DevGuard g(ctx->device);
+    CU(cudaStreamSynchronize(ctx->stream()));
+    return BM_OK;
+}
+
+int bm_area_create(bm_ctx ctx, const bm_area_desc* desc, uint64_t seed, bm_area* out) {
+    if (!ctx || !desc || !out) return set_err(BM_ERR_INVALID, "bm_area_create: null argument");
+    *out = nullptr;
+    DevGuard g(ctx->device);
+    bm_area_s* A = new (std::nothrow) bm_area_s;
+    if (!A) return set_err(BM_ERR_OOM, "host allocation failed");
+    A->ctx = ctx;
+    std::vector<TuftGrowSpec> grow;
+    std::string err;
+    int rc = resolve_area(desc, seed, &A->plan, &grow, &err);
+    if (rc != BM_OK) { delete A; return set_err(rc, "%s", err.c_str()); }
+    A->exec_path = desc->exec_path;
+    if (A->exec_path != BM_PATH_FUSED && A->exec_path != BM_PATH_PLAIN) {
+        delete A;
+        return set_err(BM_ERR_INVALID, "unknown exec_path %u", desc->exec_path);
+    }
+    cudaStream_t s = ctx->stream();
+    cudaError_t e = cudaMalloc(&A->slab, A->plan.slab_bytes);
+    if (e != cudaSuccess) {
+        free_area(A);
+        return set_err(BM_ERR_OOM, "cudaMalloc of %llu state bytes failed: %s",
+                       (unsigned long long)A->plan.slab_bytes, cudaGetErrorString(e));
+    }
+    e = cudaMalloc(&A->ctl, sizeof(AreaCtl));
+    if (e == cudaSuccess) e = cudaMalloc(&A->slices, sizeof(SliceRec) * BM_MAX_SLICES);
+    if (e != cudaSuccess) { free_area(A); return cuda_err(e, "cudaMalloc"); }
+    std::vector<SliceRec> tab(BM_MAX_SLICES);
+    for (uint32_t k = 0; k < BM_MAX_SLICES; k++) {
+        const bm_area_plan& P = A->plan;
+        SliceRec r{0, 0, 0, 0};
+        if (k < P.n_slices) {
+            r.x = P.slc_axn_idz[k];
+            r.y = P.slc_v_size[k] | (P.slc_u_size[k] << 16);
+            r.z = P.slc_v_scale[k] | (P.slc_u_scale[k] << 8) | (P.slc_v_mid[k] << 16) | (P.slc_u_mid[k] << 24);
+        }
+        tab[k] = r;
+    }
+    AreaCtl ctl0{};
+    e = cudaMemsetAsync(A->slab, 0, A->plan.slab_bytes, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(A->slices, tab.data(), sizeof(SliceRec) * BM_MAX_SLICES, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(A->ctl, &ctl0, sizeof ctl0, cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) { free_area(A); return cuda_err(e, "area init copy"); }
+    build_dev_layers(A);
+
+    // Growth (Synapses::grow(true)): offset pools to the device, one launch per tuft.
+    std::vector<int8_t> ov, ou;
+    for (auto& G : grow)
+        for (auto& S : G.srcs) { ov.insert(ov.end(), S.offs_v.begin(), S.offs_v.end()); ou.insert(ou.end(), S.offs_u.begin(), S.offs_u.end()); }
+    int8_t* d_off = nullptr;
+    size_t n_off = ov.size();
+    if (n_off) {
+        e = cudaMalloc(&d_off, 2 * n_off);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(d_off, ov.data(), n_off, cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(d_off + n_off, ou.data(), n_off, cudaMemcpyHostToDevice, s);
+        if (e != cudaSuccess) { if (d_off) cudaFree(d_off); free_area(A); return cuda_err(e, "growth pools"); }
+    }
+    uint32_t base = 0;
+    for (auto& G : grow) {
+        GrowTuft GT;
+        std::memset(&GT, 0, sizeof GT);
+        GT.tft = G.tft;
+        GT.key = G.key;
+        GT.n_pool = G.n_pool;
+        std::memcpy(GT.pool, G.pool, sizeof GT.pool);
+        std::memcpy(GT.pool_src, G.pool_src, sizeof GT.pool_src);
+        for (size_t k = 0; k < G.srcs.size(); k++) {
+            GT.nonspatial[k] = G.srcs[k].nonspatial;
+            GT.rv[k] = G.srcs[k].rv;
+            GT.ru[k] = G.srcs[k].ru;
+            GT.n_offs[k] = (uint32_t)G.srcs[k].offs_v.size();
+            GT.offs_base[k] = base;
+            base += GT.n_offs[k];
+        }
+        GT.offs_v = d_off;
+        GT.offs_u = d_off ? d_off + n_off : nullptr;
+        GT.unique = !(desc->init_flags & BM_INIT_NO_UNIQUE) && !G.saturated;
+        GT.zero_strength = (desc->init_flags & BM_INIT_STRENGTH_ZERO) != 0;
+        launch_grow(A->dl[G.data_layer], GT, s);
+    }
+    e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (d_off) cudaFree(d_off);
+    if (e != cudaSuccess) { free_area(A); return cuda_err(e, "synapse growth"); }
+    rc = prepare_fused(A->fused, A->plan, A->dl, A->slab, s, &err);
+    if (rc != BM_OK) { free_area(A); return set_err(rc, "%s", err.c_str()); }
+    *out = A;
+    return BM_OK;
+}
+
+int bm_area_destroy(bm_area area) {
+    if (!area) return BM_OK;
+    {
+        DevGuard g(area->ctx->device);
+        cudaStreamSynchronize(area->stream());
+    }
+    free_area(area);
+    return BM_OK;
+}
+
+int bm_area_get_plan(bm_area area, bm_area_plan* out) {
+    if (!area || !out) return set_err(BM_ERR_INVALID, "null argument");
+    *out = area->plan;
+    return BM_OK;
+}
+
+int bm_plan_resolve(const bm_area_desc* desc, uint64_t seed, bm_area_plan* out) {
+    if (!desc || !out) return set_err(BM_ERR_INVALID, "null argument");
+    std::string err;
+    int rc = resolve_area(desc, seed, out, nullptr, &err);
+    if (rc != BM_OK) return set_err(rc, "%s", err.c_str());
+    return BM_OK;
+}
+
+int bm_area_write_input(bm_area area, uint32_t input_idx, const uint8_t* frame, size_t len) {
+    if (!area || !frame) return set_err(BM_ERR_INVALID, "null argument");
+    const bm_area_plan& P = area->plan;
+    if (input_idx >= P.n_inputs) return set_err(BM_ERR_INVALID, "input %u out of range (%u inputs)", input_idx, P.n_inputs);
+    if (len != P.inputs[input_idx].len)
+        return set_err(BM_ERR_INVALID, "frame length %zu != input layer axon count %u", len, P.inputs[input_idx].len);
+    DevGuard g(area->ctx->device);
+    CU(cudaMemcpyAsync(area->axns() + P.inputs[input_idx].axn_idz, frame, len, cudaMemcpyHostToDevice, area->stream()));
+    return BM_OK;
+}
+
+int bm_area_write_input_device(bm_area area, uint32_t input_idx, const void* dev_frame, size_t len) {
+    if (!area || !dev_frame) return set_err(BM_ERR_INVALID, "null argument");
+    const bm_area_plan& P = area->plan;
+    if (input_idx >= P.n_inputs) return set_err(BM_ERR_INVALID, "input %u out of range", input_idx);
+    if (len != P.inputs[input_idx].len) return set_err(BM_ERR_INVALID, "frame length %zu != %u", len, P.inputs[input_idx].len);
+    DevGuard g(area->ctx->device);
+    CU(cudaMemcpyAsync(area->axns() + P.inputs[input_idx].axn_idz, dev_frame, len, cudaMemcpyDeviceToDevice, area->stream()));
+    return BM_OK;
+}
+
+int bm_area_cycle(bm_area area, uint32_t n_cycles) {
+    if (!area) return set_err(BM_ERR_INVALID, "null area");
+    DevGuard g(area->ctx->device);
+    for (uint32_t k = 0; k < n_cycles; k++) enqueue_cycle(area);
+    CU(cudaGetLastError());
+    return BM_OK;
+}
+
+int bm_area_cycle_frames_device(bm_area area, const void* dev_frames, size_t frame_len, uint32_t n_cycles) {
+    if (!area || !dev_frames) return set_err(BM_ERR_INVALID, "null argument");
+    const bm_area_plan& P = area->plan;
+    if (P.n_inputs == 0) return set_err(BM_ERR_INVALID, "area has no input layer");
+    if (frame_len != P.inputs[0].len) return set_err(BM_ERR_INVALID, "frame length %zu != %u", frame_len, P.inputs[0].len);
+    DevGuard g(area->ctx->device);
+    for (uint32_t k = 0; k < n_cycles; k++) {
+        area->run(K_INTAKE, [&] {
+            cudaMemcpyAsync(area->axns() + P.inputs[0].axn_idz, (const uint8_t*)dev_frames + (uint64_t)k * frame_len,
+                            frame_len, cudaMemcpyDeviceToDevice, area->stream());
+        });
+        enqueue_cycle(area);
+    }
+    CU(cudaGetLastError());
+    return BM_OK;
+}
+
+int bm_area_read_output(bm_area area, uint32_t output_idx, uint8_t* dst, size_t len) {
+    if (!area || !dst) return set_err(BM_ERR_INVALID, "null argument");
+    const bm_area_plan& P = area->plan;
+    if (output_idx >= P.n_outputs) return set_err(BM_ERR_INVALID, "output %u out of range", output_idx);
+    if (len != P.outputs[output_idx].len) return set_err(BM_ERR_INVALID, "length %zu != %u", len, P.outputs[output_idx].len);
+    DevGuard g(area->ctx->device);
+    CU(cudaMemcpyAsync(dst, area->axns() + P.outputs[output_idx].axn_idz, len, cudaMemcpyDeviceToHost, area->stream()));
+    CU(cudaStreamSynchronize(area->stream()));
+    return BM_OK;
+}
+
+int bm_area_read(bm_area area, uint32_t buf_kind, uint32_t layer, uint64_t offset, void* dst, uint64_t len) {
+    if (!area || (!dst && len)) return set_err(BM_ERR_INVALID, "null argument");
+    uint64_t off;
+    if (!buf_range(area, buf_kind, layer, offset, len, &off))
+        return set_err(BM_ERR_INVALID, "buffer %u of layer %u: range [%llu, +%llu) out of bounds", buf_kind, layer,
+                       (unsigned long long)offset, (unsigned long long)len);
+    DevGuard g(area->ctx->device);
+    if (len) CU(cudaMemcpyAsync(dst, area->slab + off, len, cudaMemcpyDeviceToHost, area->stream()));
+    CU(cudaStreamSynchronize(area->stream()));
+    return BM_OK;
+}
+
+int bm_area_write(bm_area area, uint32_t buf_kind, uint32_t layer, uint64_t offset, const void* src, uint64_t len) {
+    if (!area || (!src && len)) return set_err(BM_ERR_INVALID, "null argument");
+    uint64_t off;
+    if (!buf_range(area, buf_kind, layer, offset, len, &off))
+        return set_err(BM_ERR_INVALID, "buffer %u of layer %u: range out of bounds", buf_kind, layer);
+    DevGuard g(area->ctx->device);
+    if (len) CU(cudaMemcpyAsync(area->slab + off, src, len, cudaMemcpyHostToDevice, area->stream()));
+    CU(cudaStreamSynchronize(area->stream()));
+    if (buf_kind == BM_BUF_SYN_SRC_SLC_IDS || buf_kind == BM_BUF_SYN_SRC_COL_V_OFFS ||
+        buf_kind == BM_BUF_SYN_SRC_COL_U_OFFS)
+        mark_sources_dirty(area->fused, layer);
+    return BM_OK;
+}
+
+int bm_area_read_slab(bm_area area, void* dst, uint64_t len) {
+    if (!area || !dst) return set_err(BM_ERR_INVALID, "null argument");
+    if (len != area->plan.slab_bytes) return set_err(BM_ERR_INVALID, "slab length %llu != %llu", (unsigned long long)len,
+                                                     (unsigned long long)area->plan.slab_bytes);
+    DevGuard g(area->ctx->device);
+    CU(cudaMemcpyAsync(dst, area->slab, len, cudaMemcpyDeviceToHost, area->stream()));
+    CU(cudaStreamSynchronize(area->stream()));
+    return BM_OK;
+}
+
+int bm_area_write_slab(bm_area area, const void* src, uint64_t len) {
+    if (!area || !src) return set_err(BM_ERR_INVALID, "null argument");
+    if (len != area->plan.slab_bytes) return set_err(BM_ERR_INVALID, "slab length mismatch");
+    DevGuard g(area->ctx->device);
+    CU(cudaMemcpyAsync(area->slab, src, len, cudaMemcpyHostToDevice, area->stream()));
+    CU(cudaStreamSynchronize(area->stream()));
+    for (uint32_t l = 0; l < area->plan.n_layers; l++) mark_sources_dirty(area->fused, l);
+    return BM_OK;
+}
+
+int bm_area_get_cycle(bm_area area, uint64_t* out) {
+    if (!area || !out) return set_err(BM_ERR_INVALID, "null argument");
+    *out = area->host_cycle;
+    return BM_OK;
+}
+
+int bm_area_set_cycle(bm_area area, uint64_t cycle) {
+    if (!area) return set_err(BM_ERR_INVALID, "null area");
+    DevGuard g(area->ctx->device);
+    AreaCtl c{};
+    c.cycle = cycle;
+    CU(cudaMemcpyAsync(area->ctl, &c, sizeof c, cudaMemcpyHostToDevice, area->stream()));
+    CU(cudaStreamSynchronize(area->stream()));
+    area->host_cycle = cycle;
+    return BM_OK;
+}
+
+int bm_area_slab_ptr(bm_area area, void** out) {
+    if (!area || !out) return set_err(BM_ERR_INVALID, "null argument");
+    *out = area->slab;
+    return BM_OK;
+}
+
+int bm_area_set_profiling(bm_area area, int on) {
+    if (!area) return set_err(BM_ERR_INVALID, "null area");
+    area->profiling = on != 0;
+    return BM_OK;
+}
+
+int bm_area_get_profile(bm_area area, uint32_t n_max, const char** names, uint64_t* launches, double* ms,
+                        uint32_t* n_out) {
+    if (!area || !n_out) return set_err(BM_ERR_INVALID, "null argument");
+    DevGuard g(area->ctx->device);
+    area->drain_profile();
+    uint32_t n = 0;
+    for (int k = 0; k < K_COUNT && n < n_max; k++) {
+        if (!area->prof_launches[k]) continue;
+        if (names) names[n] = kKindNames[k];
+        if (launches) launches[n] = area->prof_launches[k];
+        if (ms) ms[n] = area->prof_ms[k];
+        n++;
+    }
+    *n_out = n;
+    return BM_OK;
+}
+
+int bm_area_reset_profile(bm_area area) {
+    if (!area) return set_err(BM_ERR_INVALID, "null area");
+    DevGuard g(area->ctx->device);
+    area->drain_profile();
+    for (int k = 0; k < K_COUNT; k++) { area->prof_launches[k] = 0; area->prof_ms[k] = 0; }
+    return BM_OK;
+}
+
+int bm_area_launches_per_cycle(bm_area area, uint32_t* out) {
+    if (!area || !out) return set_err(BM_ERR_INVALID, "null argument");
+    *out = area->launches;
+    return BM_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,43 @@
+// bm_kernels.h -- host-callable launchers of the cycle kernels.
+#pragma once
+#include "bm_dev.cuh"
+
+namespace bm {
+
+// Growth parameters of one tuft (see bm_grow.cu).
+struct GrowTuft {
+    uint32_t tft;
+    uint64_t key;
+    uint32_t n_pool;                          // pool with prevalence repeats
+    uint8_t pool[BM_MAX_SRC_SLICES];          // slice id per pool entry
+    uint8_t pool_src[BM_MAX_SRC_SLICES];      // index of the pool entry's distinct source
+    uint8_t nonspatial[BM_MAX_SRC_SLICES];
+    int32_t rv[BM_MAX_SRC_SLICES], ru[BM_MAX_SRC_SLICES];   // scaled reaches / nonspatial half sizes
+    uint32_t n_offs[BM_MAX_SRC_SLICES];
+    uint32_t offs_base[BM_MAX_SRC_SLICES];
+    const int8_t* offs_v;
+    const int8_t* offs_u;
+    uint32_t unique, zero_strength;
+};
+
+void launch_grow(const DevLayer& L, const GrowTuft& G, cudaStream_t s);
+void launch_cycle_end(AreaCtl* ctl, cudaStream_t s);
+
+// Plain form: one kernel per reference stage (bm_plain.cu).
+void launch_set_syn_flags(const DevLayer& L, cudaStream_t s);
+void launch_syn_cycle_plain(const uint8_t* axns, const SliceRec* slices, const DevLayer& L, uint32_t t,
+                            cudaStream_t s);
+void launch_den_cycle_plain(const DevLayer& L, uint32_t t, const AreaCtl* ctl, cudaStream_t s);
+void launch_tft_cycle_plain(const DevLayer& L, uint32_t t, cudaStream_t s);
+void launch_ssc_cycle(const DevLayer& L, cudaStream_t s);
+void launch_inhib_simple(uint8_t* axns, const SliceRec* slices, const DevLayer& L, int radius, uint64_t key,
+                         const AreaCtl* ctl, cudaStream_t s);
+void launch_inhib_passthrough(uint8_t* axns, const SliceRec* slices, const DevLayer& L, cudaStream_t s);
+void launch_ssc_mtp_plain(const uint8_t* axns, const DevLayer& L, const AreaCtl* ctl, cudaStream_t s);
+void launch_pyr_cycle_plain(const DevLayer& L, cudaStream_t s);
+void launch_pyr_output(uint8_t* axns, const SliceRec* slices, const DevLayer& L, cudaStream_t s);
+void launch_inhib_intra_column_plain(uint8_t* axns, const SliceRec* slices, const DevLayer& L, cudaStream_t s);
+void launch_tft_dst_mtp_plain(const uint8_t* axns, const DevLayer& L, uint32_t t, const AreaCtl* ctl,
+                              cudaStream_t s);
+
+}  // namespace bm

@@ -1,0 +1,379 @@
+/*
+ * bismit_b200.h -- C ABI of the B200-native bismit cortical cycle.
+ *
+ * This is the drop-in boundary for bismit's per-area cortical cycle plus
+ * learning. Every entry point returns an int status (BM_OK == 0). Nothing
+ * panics or aborts across this boundary; the last error message of the
+ * calling thread is available from bm_last_error().
+ *
+ * Ownership: the library owns all device memory. Callers pass host buffers
+ * (plain pointers and byte counts) which are only read or written for the
+ * duration of the call.
+ *
+ * Threading: each handle is affine to one thread at a time. Separate areas may
+ * be driven from separate threads; each area issues work on its own CUDA
+ * stream (or the stream set with bm_ctx_set_stream).
+ *
+ * Reference interfaces replaced (paths relative to the bismit repository):
+ *   bm_ctx_create        -> Cortex::new / OpenCL context    src/cortex/cortex.rs:51-61
+ *   bm_area_create       -> CorticalArea::new               src/cortex/cortical_area.rs:376-615
+ *                           (AreaMap::new src/map/area_map.rs:25, SliceMap::new
+ *                           src/map/slice_map.rs:26, Synapses::grow
+ *                           src/cortex/synapses.rs:454-501)
+ *   bm_area_cycle        -> CorticalArea::cycle             src/cortex/cortical_area.rs:716-789
+ *   bm_area_write_input  -> AxonSpace::intake               src/cortex/axon_space.rs:509-588
+ *   bm_area_read_output  -> AxonSpace::output               src/cortex/axon_space.rs:594-629
+ *   bm_area_read/write   -> CorticalArea::sampler + the *Test traits' buffer
+ *                           read/write/fill helpers         src/cortex/cortical_area.rs:1017,1375-1516
+ *                                                           src/cortex/synapses.rs:536-709
+ *   bm_area_get_plan     -> AreaMap::gen_build_options (the resolved slice
+ *                           tables and buffer index spaces) src/map/area_map.rs:51-77
+ *   bm_last_error        -> CmnError / CmnResult            src/cmn/error.rs
+ */
+#ifndef BISMIT_B200_H
+#define BISMIT_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- status -- */
+#define BM_OK               0
+#define BM_ERR_INVALID      1   /* bad argument or scheme                      */
+#define BM_ERR_OOM          2   /* device allocation failed                    */
+#define BM_ERR_CUDA         3   /* a CUDA runtime call failed                  */
+#define BM_ERR_TIMEOUT      4   /* a bounded device-side wait gave up          */
+#define BM_ERR_UNSUPPORTED  5   /* scheme feature outside this path            */
+#define BM_ERR_NO_DEVICE    6   /* no CUDA device / device index out of range  */
+
+/* ------------------------------------------------------------- limits ---- */
+#define BM_MAX_SLICES       256 /* u8 slice ids (src/map/slice_map.rs:212)     */
+#define BM_MAX_LAYERS       16
+#define BM_MAX_TUFTS        4
+#define BM_MAX_SRC_LAYERS   8
+#define BM_MAX_SRC_SLICES   32  /* source-slice pool per tuft (with prevalence) */
+#define BM_MAX_CTRL         4
+#define BM_MAX_IO           8
+#define BM_NAME_LEN         32
+
+/* ------------------------------------------------------- layer schemes --- */
+/* Layer kinds (src/map/scheme/layer.rs, src/map/mod.rs CellClass). */
+#define BM_LYR_AXONAL              0
+#define BM_LYR_SPINY_STELLATE      1
+#define BM_LYR_PYRAMIDAL           2
+#define BM_LYR_CTRL_INHIB_BASKET   3   /* InhibitoryBasketSurround -> inhib_simple  */
+#define BM_LYR_CTRL_PYR_OUTPUT     4   /* PyrOutputter -> pyr_output                */
+#define BM_LYR_CTRL_INTRA_COLUMN   5   /* IntraColumnInhib -> inhib_intra_column    */
+#define BM_LYR_CTRL_SMOOTHER       6   /* ActivitySmoother: not on this path        */
+
+/* Axon domains (src/map/axon_domain.rs). */
+#define BM_DOM_LOCAL   0
+#define BM_DOM_INPUT   1
+#define BM_DOM_OUTPUT  2
+
+/* Axon topologies (src/map/mod.rs AxonTopology). */
+#define BM_TOPO_SPATIAL     0
+#define BM_TOPO_NONSPATIAL  1
+#define BM_TOPO_NONE        2
+
+/* Dendrite classes/kinds (src/map/mod.rs DendriteClass/DendriteKind). */
+#define BM_DEN_BASAL     0
+#define BM_DEN_APICAL    1
+#define BM_DEN_PROXIMAL  0
+#define BM_DEN_DISTAL    1
+
+/* Layer tag bits, the high word of bismit's LayerTags (src/map/layer_tags.rs:121-150). */
+#define BM_TAG_PRIMARY   (1ull << 32)
+#define BM_TAG_SPATIAL   (1ull << 36)
+#define BM_TAG_TEMPORAL  (1ull << 37)
+#define BM_TAG_FOCUS     (1ull << 38)
+#define BM_TAG_MOTOR     (1ull << 39)
+#define BM_TAG_INPUT     (1ull << 48)
+#define BM_TAG_OUTPUT    (1ull << 49)
+#define BM_TAG_UNUSED    (1ull << 47)
+#define BM_TAG_PSAL      (BM_TAG_PRIMARY | BM_TAG_SPATIAL)
+#define BM_TAG_PTAL      (BM_TAG_PRIMARY | BM_TAG_TEMPORAL)
+
+/* CorticalAreaSettings switches (src/cortex/cortical_area.rs:253-338). */
+#define BM_SET_BYPASS_INHIB      (1u << 0)
+#define BM_SET_BYPASS_FILTERS    (1u << 1)
+#define BM_SET_DISABLE_PYRS      (1u << 2)
+#define BM_SET_DISABLE_SSCS      (1u << 3)
+#define BM_SET_DISABLE_MCOLS     (1u << 4)
+#define BM_SET_DISABLE_REGROWTH  (1u << 5)
+#define BM_SET_DISABLE_LEARNING  (1u << 6)
+
+/* Growth options (bm_area_desc.init_flags). */
+#define BM_INIT_STRENGTH_ZERO     (1u << 0)  /* strengths start at 0 (else the
+                                                 SynSrcSlices::gen_src intensity x
+                                                 U[-3,3] rule, src/map/syn_src.rs:448-490) */
+#define BM_INIT_NO_UNIQUE         (1u << 1)  /* skip per-dendrite source uniqueness
+                                                 (SynSrcIdxCache, src/map/syn_src.rs:159-211) */
+
+/* Execution path (bm_area_desc.exec_path). */
+#define BM_PATH_FUSED   0   /* fused stage kernels where the scheme allows (default) */
+#define BM_PATH_PLAIN   1   /* one kernel per reference stage                         */
+
+typedef struct bm_src_layer_desc {
+    int32_t  layer_idx;    /* index into bm_area_desc.layers               */
+    int32_t  syn_reach;    /* TuftSourceLayer::syn_reach (i8 range)          */
+    uint32_t prevalence;   /* TuftSourceLayer::prevalence (>= 1)             */
+} bm_src_layer_desc;
+
+typedef struct bm_tuft_desc {
+    uint32_t den_class;          /* BM_DEN_BASAL / BM_DEN_APICAL            */
+    uint32_t den_kind;           /* BM_DEN_PROXIMAL / BM_DEN_DISTAL         */
+    uint32_t dens_per_tft;
+    uint32_t syns_per_den;
+    uint32_t max_active_dens_l2;
+    int64_t  thresh_init;        /* < 0: DENDRITE_DEFAULT_INITIAL_THRESHOLD (0) */
+    uint32_t n_src;
+    bm_src_layer_desc src[BM_MAX_SRC_LAYERS];
+} bm_tuft_desc;
+
+/* One source feeding an axonal input layer: the dims of the source layer the
+ * thalamic tract delivers (LayerInfo::new, src/map/layer_info.rs:142-215). */
+typedef struct bm_input_src_desc {
+    uint32_t v_size, u_size, depth;
+    uint32_t axon_topology;
+} bm_input_src_desc;
+
+typedef struct bm_layer_desc {
+    char     name[BM_NAME_LEN];
+    uint64_t tags;               /* BM_TAG_* bits                              */
+    uint32_t kind;               /* BM_LYR_*                                   */
+    int32_t  depth;              /* < 0: unset (0 for local/output layers)     */
+    uint32_t axon_topology;      /* BM_TOPO_*                                  */
+    uint32_t axon_domain;        /* BM_DOM_*                                   */
+    /* Axonal input layers: the sources (one slice range per source). */
+    uint32_t n_input_srcs;
+    bm_input_src_desc input_srcs[BM_MAX_IO];
+    /* Control layers. */
+    int32_t  host_layer_idx;
+    uint32_t field_radius;
+    uint32_t exe_order;
+    /* Cellular layers. */
+    uint32_t n_tufts;
+    bm_tuft_desc tufts[BM_MAX_TUFTS];
+} bm_layer_desc;
+
+typedef struct bm_area_desc {
+    uint32_t area_id;
+    uint32_t v_size, u_size;     /* area column grid                          */
+    uint32_t n_layers;
+    bm_layer_desc layers[BM_MAX_LAYERS];
+    uint32_t settings;           /* BM_SET_*                                   */
+    uint32_t init_flags;         /* BM_INIT_*                                  */
+    uint32_t exec_path;          /* BM_PATH_*                                  */
+} bm_area_desc;
+
+/* ------------------------------------------------------- resolved plan --- */
+/* The resolved index spaces of an area: slice tables, per-layer buffer
+ * offsets within the area's state slab, tuft index ranges. Used by callers
+ * that address raw buffers (tests, samplers, snapshots) and by the oracle.    */
+
+/* Buffer kinds within a layer (mirrors SamplerKind, src/cortex/cortical_area.rs:61-90). */
+#define BM_BUF_SYN_STATES               0
+#define BM_BUF_SYN_STRENGTHS            1
+#define BM_BUF_SYN_SRC_SLC_IDS          2
+#define BM_BUF_SYN_SRC_COL_V_OFFS       3
+#define BM_BUF_SYN_SRC_COL_U_OFFS       4
+#define BM_BUF_SYN_FLAG_SETS            5
+#define BM_BUF_DEN_STATES_RAW           6
+#define BM_BUF_DEN_STATES               7
+#define BM_BUF_DEN_ENERGIES             8
+#define BM_BUF_DEN_ACTIVITIES           9
+#define BM_BUF_DEN_THRESHOLDS           10
+#define BM_BUF_TFT_PREV_BEST_DEN_IDS    11
+#define BM_BUF_TFT_PREV_BEST_DEN_STATES_RAW 12
+#define BM_BUF_TFT_PREV_BEST_DEN_STATES 13
+#define BM_BUF_TFT_PREV_STATES          14
+#define BM_BUF_TFT_BEST_DEN_IDS         15
+#define BM_BUF_TFT_BEST_DEN_STATES_RAW  16
+#define BM_BUF_TFT_BEST_DEN_STATES      17
+#define BM_BUF_TFT_STATES               18
+#define BM_BUF_CEL_ENERGIES             19
+#define BM_BUF_CEL_ACTIVITIES           20
+#define BM_BUF_CEL_STATES               21   /* pyramidal soma                     */
+#define BM_BUF_CEL_FLAG_SETS            22   /* pyramidal cell flags               */
+#define BM_BUF_COUNT                    23
+#define BM_BUF_AXON_STATES              64   /* area axon space (layer ignored)    */
+
+typedef struct bm_tuft_plan {
+    uint32_t tft_id, den_class, den_kind;
+    uint32_t dens_per_tft, syns_per_den, syns_per_tft;
+    uint32_t max_active_dens_l2;
+    uint32_t den_threshold;
+    uint64_t syn_idz;      /* first synapse of the tuft (layer-relative)      */
+    uint64_t den_idz;      /* first dendrite of the tuft (layer-relative)     */
+    uint64_t cel_idz;      /* tft_id * cells (cell-tuft index base)           */
+    uint32_t n_src;        /* pool with prevalence repeats                    */
+    uint8_t  src_slc_ids[BM_MAX_SRC_SLICES];
+    int8_t   src_reaches[BM_MAX_SRC_SLICES];
+    uint32_t n_src_uniq;   /* distinct (slice, reach) pairs                  */
+    uint8_t  src_uniq_slc_ids[BM_MAX_SRC_SLICES];
+    int8_t   src_uniq_reaches[BM_MAX_SRC_SLICES];
+} bm_tuft_plan;
+
+typedef struct bm_ctrl_plan {
+    uint32_t kind;          /* BM_LYR_CTRL_*                                  */
+    uint32_t exe_order;
+    uint32_t field_radius;
+    uint32_t layer_id;
+} bm_ctrl_plan;
+
+typedef struct bm_layer_plan {
+    uint32_t layer_id;      /* index in the area's layer list                */
+    uint32_t kind;          /* BM_LYR_SPINY_STELLATE / BM_LYR_PYRAMIDAL        */
+    uint64_t tags;
+    uint32_t depth;
+    uint32_t base_axn_slc;
+    uint32_t axn_idz;
+    uint32_t v_size, u_size;
+    uint32_t cells;
+    uint32_t n_tufts;
+    bm_tuft_plan tufts[BM_MAX_TUFTS];
+    uint64_t n_syns, n_dens, n_celtfts;
+    uint32_t enabled_tft_flags;  /* pyramidal: DEN_*_FLAG bits               */
+    uint32_t bsl_prx_tft_id, bsl_dst_tft_id, apc_dst_tft_id;
+    uint32_t n_ctrl;
+    bm_ctrl_plan ctrl[BM_MAX_CTRL];   /* post-cycle controls, (host, exe_order) order */
+    uint64_t buf_off[BM_BUF_COUNT];   /* byte offset in the state slab, or UINT64_MAX */
+    uint64_t buf_len[BM_BUF_COUNT];   /* bytes                                         */
+} bm_layer_plan;
+
+typedef struct bm_io_plan {
+    uint32_t layer_idx;     /* scheme layer index                             */
+    uint32_t axn_idz;       /* first axon                                     */
+    uint32_t len;           /* axons                                          */
+} bm_io_plan;
+
+typedef struct bm_area_plan {
+    uint32_t area_id;
+    uint32_t v_size, u_size;
+    uint32_t settings;
+    uint32_t n_slices;
+    uint32_t slc_axn_idz[BM_MAX_SLICES];
+    uint32_t slc_v_size[BM_MAX_SLICES];
+    uint32_t slc_u_size[BM_MAX_SLICES];
+    uint32_t slc_v_scale[BM_MAX_SLICES];
+    uint32_t slc_u_scale[BM_MAX_SLICES];
+    uint32_t slc_v_mid[BM_MAX_SLICES];
+    uint32_t slc_u_mid[BM_MAX_SLICES];
+    uint32_t slc_layer[BM_MAX_SLICES];   /* owning scheme layer               */
+    uint32_t n_axons;
+    uint64_t axon_off;                   /* axon space offset in the slab     */
+    uint32_t n_inputs;
+    bm_io_plan inputs[BM_MAX_IO];
+    uint32_t n_outputs;
+    bm_io_plan outputs[BM_MAX_IO];
+    uint32_t n_layers;                   /* data (cellular) layers            */
+    bm_layer_plan layers[BM_MAX_LAYERS];
+    uint32_t n_cycle_order;              /* data layers in role order         */
+    uint32_t cycle_order[BM_MAX_LAYERS]; /* indices into layers[]            */
+    uint64_t slab_bytes;
+    uint64_t n_syns_total;
+    uint64_t rnd_seed;                   /* per-launch random stream key      */
+} bm_area_plan;
+
+/* ------------------------------------------------------------ handles ---- */
+typedef struct bm_ctx_s*  bm_ctx;
+typedef struct bm_area_s* bm_area;
+
+/* Thread-local message for the last failing call ("" if none). */
+const char* bm_last_error(void);
+
+/* Version string of this library. */
+const char* bm_version(void);
+
+/* Creates a context on CUDA device `device` (Cortex::new, src/cortex/cortex.rs:51-61). */
+int bm_ctx_create(int device, uint32_t flags, bm_ctx* out);
+int bm_ctx_destroy(bm_ctx ctx);
+/* Issues all subsequent work of areas created from ctx on `stream`
+ * (a cudaStream_t passed as void*; NULL = the library's own stream). */
+int bm_ctx_set_stream(bm_ctx ctx, void* stream);
+/* Blocks until all work issued through ctx has finished. */
+int bm_ctx_synchronize(bm_ctx ctx);
+
+/* Builds an area from a scheme, allocates its state and grows its synapses from
+ * the seeded stream `seed` (CorticalArea::new, src/cortex/cortical_area.rs:376). */
+int bm_area_create(bm_ctx ctx, const bm_area_desc* desc, uint64_t seed, bm_area* out);
+int bm_area_destroy(bm_area area);
+
+/* Copies the resolved plan (slice tables, buffer offsets) to *out. */
+int bm_area_get_plan(bm_area area, bm_area_plan* out);
+
+/* Resolves a scheme into its plan without creating an area or touching a
+ * device (the AreaMap::new half of CorticalArea::new). */
+int bm_plan_resolve(const bm_area_desc* desc, uint64_t seed, bm_area_plan* out);
+
+/* Writes one thalamic frame into the axon range of input layer `input_idx`
+ * (index into plan.inputs); len must equal that range (AxonSpace::intake,
+ * src/cortex/axon_space.rs:509-588). The copy is ordered before the next cycle. */
+int bm_area_write_input(bm_area area, uint32_t input_idx, const uint8_t* frame, size_t len);
+
+/* Same, from device memory (a frame already resident in HBM). */
+int bm_area_write_input_device(bm_area area, uint32_t input_idx, const void* dev_frame, size_t len);
+
+/* Runs n_cycles full cycles: intake is whatever was written before, then the
+ * spatial layers, their learning, the temporal layers with control layers and
+ * learning (CorticalArea::cycle, src/cortex/cortical_area.rs:716-789). Work is
+ * enqueued asynchronously on the area's stream. */
+int bm_area_cycle(bm_area area, uint32_t n_cycles);
+
+/* Like bm_area_cycle with one fresh input frame per cycle taken from a device
+ * array of n_cycles frames of `frame_len` bytes each (input 0). */
+int bm_area_cycle_frames_device(bm_area area, const void* dev_frames, size_t frame_len,
+                                uint32_t n_cycles);
+
+/* Reads the axons of output layer `output_idx` (AxonSpace::output,
+ * src/cortex/axon_space.rs:594-629). Synchronous. */
+int bm_area_read_output(bm_area area, uint32_t output_idx, uint8_t* dst, size_t len);
+
+/* Reads/writes `len` bytes at byte `offset` of buffer `buf_kind` of data layer
+ * `layer` (plan index; ignored for BM_BUF_AXON_STATES). Synchronous. */
+int bm_area_read(bm_area area, uint32_t buf_kind, uint32_t layer, uint64_t offset,
+                 void* dst, uint64_t len);
+int bm_area_write(bm_area area, uint32_t buf_kind, uint32_t layer, uint64_t offset,
+                  const void* src, uint64_t len);
+
+/* Whole-state snapshot and restore (the slab, plan.slab_bytes) plus the cycle counter. */
+int bm_area_read_slab(bm_area area, void* dst, uint64_t len);
+int bm_area_write_slab(bm_area area, const void* src, uint64_t len);
+int bm_area_get_cycle(bm_area area, uint64_t* out);
+int bm_area_set_cycle(bm_area area, uint64_t cycle);
+
+/* Device pointer of the state slab (for callers that move data with their own
+ * copies on the same device). */
+int bm_area_slab_ptr(bm_area area, void** out);
+
+/* Per-kernel CUDA-event timing of subsequent cycles (0 = off). */
+int bm_area_set_profiling(bm_area area, int on);
+/* Per kernel kind: launch count and summed device milliseconds since the last
+ * reset; names are static strings. n_max entries at most; *n_out = written. */
+int bm_area_get_profile(bm_area area, uint32_t n_max, const char** names,
+                        uint64_t* launches, double* ms, uint32_t* n_out);
+int bm_area_reset_profile(bm_area area);
+
+/* Number of kernel launches bm_area_cycle issues per cycle for this area. */
+int bm_area_launches_per_cycle(bm_area area, uint32_t* out);
+
+/* The per-launch random value the host would draw for (layer, role, tuft) at
+ * `cycle` (replaces the SmallRng draws of src/cortex/dendrites.rs:198,
+ * src/cortex/tufts.rs:312, src/cortex/spiny_stellates.rs:259,
+ * src/cortex/iinn.rs:113). */
+#define BM_RND_DEN_CYCLE   1
+#define BM_RND_INHIB       2
+#define BM_RND_SSC_MTP     3
+#define BM_RND_TFT_DST_MTP 4
+int32_t bm_rnd(uint64_t seed, uint32_t area_id, uint32_t layer_id, uint32_t role,
+               uint32_t tft_id, uint64_t cycle);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* BISMIT_B200_H */

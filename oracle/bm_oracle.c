@@ -1,0 +1,711 @@
+/*
+ * bm_oracle.c -- CPU oracle for the bismit cortical cycle (TEST INFRASTRUCTURE).
+ *
+ * Used only as the checker by tests/, __graft_entry__.smoke() and bench.py's
+ * CPU-baseline leg; nothing in the product library links or calls it.
+ *
+ * Every function restates one piece of bismit and cites the reference lines it
+ * follows (paths relative to the bismit repository). Integer semantics follow
+ * OpenCL C on a GPU: 32-bit two's-complement wrap-around, arithmetic right
+ * shift of negative ints, plain (non-saturating) narrowing to u8/i8.
+ */
+#include "bm_oracle.h"
+
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+/* Reference constants: cl/bismit.cl:11-22, cl/control.cl:6-13, src/cmn/mod.rs:321-336. */
+#define SYNAPSE_AXON_BIAS_LOG2          1
+#define DENDRITE_ACTIVITY_DECAY_FACTOR  1536
+#define CELL_ACTIVITY_DECAY_FACTOR      768
+#define INHIB_INFL_CENTER_OFFSET        1
+#define INHIB_INFL_HORIZ_OFFSET         3
+#define SLC_SCL_COEFF_L2                4
+#define CEL_PREV_ACTIVE_FLAG            0x08
+#define SYN_PREV_ACTIVE_FLAG            0x10
+#define DEN_BASAL_PROXIMAL_FLAG         0x01
+#define DEN_BASAL_DISTAL_FLAG           0x02
+#define DEN_APICAL_DISTAL_FLAG          0x04
+
+/* ------------------------------------------------------------ helpers ---- */
+static inline int32_t shl32(int32_t x, int n) { return (int32_t)((uint32_t)x << n); }
+/* gcc defines >> on negative signed ints as an arithmetic shift. */
+static inline int32_t asr32(int32_t x, int n) { return x >> n; }
+static inline int iabs(int x) { return x < 0 ? -x : x; }
+static inline int imax(int a, int b) { return a > b ? a : b; }
+static inline int imin(int a, int b) { return a < b ? a : b; }
+
+static inline uint64_t splitmix64(uint64_t x) {
+    x += 0x9E3779B97F4A7C15ull;
+    x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+    x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+    return x ^ (x >> 31);
+}
+
+/* The per-launch random value. It replaces bismit's host draws
+ * `rng.gen::<i32>()` (src/cortex/dendrites.rs:198, src/cortex/tufts.rs:312,
+ * src/cortex/spiny_stellates.rs:259, src/cortex/iinn.rs:113) with a seeded,
+ * counter-based stream keyed by (area, layer, role, tuft, cycle). */
+int32_t bmo_rnd(uint64_t seed, uint32_t area_id, uint32_t layer_id, uint32_t role,
+                uint32_t tft_id, uint64_t cycle) {
+    uint64_t key = ((uint64_t)area_id << 40) ^ ((uint64_t)layer_id << 32) ^
+                   ((uint64_t)role << 24) ^ ((uint64_t)tft_id << 16);
+    uint64_t x = splitmix64(splitmix64(seed) + key);
+    x = splitmix64(x + cycle);
+    return (int32_t)(uint32_t)(x >> 32);
+}
+
+/* rnd_mix, cl/bismit.cl:426-431. */
+static inline int32_t rnd_mix(int32_t rnd_a, int32_t seed) {
+    seed ^= shl32(seed ^ rnd_a, 13);
+    seed ^= asr32(seed, 17);
+    seed ^= shl32(seed, 5);
+    return seed;
+}
+
+/* rnd_inc / rnd_dec, cl/bismit.cl:447-469 (abs of a char is its magnitude). */
+static inline int rnd_inc(int32_t rnd_a, int32_t seed, int8_t val, int32_t lr_mask) {
+    return (rnd_mix(rnd_a, seed) & lr_mask) > (iabs(val) + (lr_mask - 0x7f));
+}
+static inline int rnd_dec(int32_t rnd_a, int32_t seed, int8_t val, int32_t lr_mask) {
+    int val_is_max = val == 127;
+    return (rnd_mix(rnd_a, seed) & lr_mask) > ((iabs(val) - val_is_max) + (lr_mask - 0x7f));
+}
+
+/* lshft_mask, cl/bismit.cl:473-475: (0x7F << l2i) with the low l2i bits set. */
+static inline int32_t lr_mask_of(int l2i) {
+    int32_t m = 0x7F << l2i;
+    for (int i = 0; i < l2i; i++) m |= (1 << i);
+    return m;
+}
+
+/* rnd_inc_u, cl/bismit.cl:482-484; rnd_0xFFFF :525-527. */
+static inline int rnd_inc_u(int32_t rnd_a, int32_t seed, uint8_t val) {
+    return (rnd_mix(rnd_a, seed) & 0xFF) > val;
+}
+static inline int rnd_0xFFFF(int32_t rnd, int32_t seed, uint16_t cutoff) {
+    return (rnd_mix(rnd, seed) & 0xFFFF) < cutoff;
+}
+
+/* update_activity_rating, cl/bismit.cl:531-540. */
+static inline uint8_t update_activity_rating(uint8_t act, int is_active, int32_t rnd,
+                                             int32_t seed, uint16_t decay) {
+    act = (uint8_t)(act + (rnd_inc_u(rnd, seed, act) & is_active));
+    act = (uint8_t)(act - (rnd_0xFFFF(rnd, shl32(seed, 1), decay) & (act > 0)));
+    return act;
+}
+
+/* syn_fire, cl/syns.cl:2-4. */
+static inline uint8_t syn_fire(uint8_t a) {
+    return (uint8_t)(((a != 0) << 7) + (a >> SYNAPSE_AXON_BIAS_LOG2));
+}
+
+/* Axon index and bounds of axn_idx_3d_unsafe (cl/bismit.cl:323-363). The
+ * scalar form adds the slice mid to the i8 offset in an i8 (wrapping); the
+ * vec4 form (:366-391) adds it in int. bismit launches the vec4 synapse kernel
+ * when syns_per_tft % 4 == 0 (src/cortex/synapses.rs:261-286). */
+static inline uint32_t axn_idx(const bm_area_plan* P, uint8_t slc, uint32_t v_id,
+                               int8_t v_ofs_c, uint32_t u_id, int8_t u_ofs_c, int vec4,
+                               int* safe) {
+    int v_size = (int)P->slc_v_size[slc], u_size = (int)P->slc_u_size[slc];
+    int v_ofs, u_ofs;
+    if (vec4) {
+        v_ofs = (int)v_ofs_c + (int)P->slc_v_mid[slc];
+        u_ofs = (int)u_ofs_c + (int)P->slc_u_mid[slc];
+    } else {
+        v_ofs = (int8_t)(uint8_t)((int)v_ofs_c + (int)P->slc_v_mid[slc]);
+        u_ofs = (int8_t)(uint8_t)((int)u_ofs_c + (int)P->slc_u_mid[slc]);
+    }
+    int v_sc = (int)((v_id * P->slc_v_scale[slc]) >> SLC_SCL_COEFF_L2);
+    int u_sc = (int)((u_id * P->slc_u_scale[slc]) >> SLC_SCL_COEFF_L2);
+    int vt = v_sc + v_ofs, ut = u_sc + u_ofs;
+    *safe = (vt >= 0) & (vt < v_size) & (ut >= 0) & (ut < u_size);
+    return P->slc_axn_idz[slc] + (uint32_t)(vt * u_size + ut);
+}
+
+/* axn_state_3d_safe[_vec4], cl/bismit.cl:397-418. */
+static inline uint8_t axn_state_safe(const bm_area_plan* P, const uint8_t* axns, uint8_t slc,
+                                     uint32_t v, int8_t vo, uint32_t u, int8_t uo, int vec4) {
+    int safe;
+    uint32_t idx = axn_idx(P, slc, v, vo, u, uo, vec4, &safe);
+    return safe ? axns[idx] : 0;
+}
+
+uint32_t bmo_axn_idx_scl(const bm_area_plan* P, uint8_t slc, uint32_t v, int8_t v_ofs,
+                         uint32_t u, int8_t u_ofs, int* safe) {
+    return axn_idx(P, slc, v, v_ofs, u, u_ofs, 0, safe);
+}
+uint32_t bmo_axn_idx_vec4(const bm_area_plan* P, uint8_t slc, int32_t v, int8_t v_ofs,
+                          int32_t u, int8_t u_ofs, int* safe) {
+    return axn_idx(P, slc, (uint32_t)v, v_ofs, (uint32_t)u, u_ofs, 1, safe);
+}
+
+/* ----------------------------------------------------------- layer view -- */
+typedef struct {
+    const bm_layer_plan* L;
+    uint8_t* b[BM_BUF_COUNT];
+} lview;
+
+static void view(const bm_layer_plan* L, uint8_t* slab, lview* v) {
+    v->L = L;
+    for (int k = 0; k < BM_BUF_COUNT; k++)
+        v->b[k] = (L->buf_off[k] == UINT64_MAX) ? NULL : slab + L->buf_off[k];
+}
+
+/* ------------------------------------------------------------- kernels --- */
+
+/* tft_set_syn_flags, cl/syns.cl:23-33, over every synapse of the layer. */
+static void k_set_syn_flags(lview* V) {
+    uint8_t* st = V->b[BM_BUF_SYN_STATES];
+    uint8_t* fl = V->b[BM_BUF_SYN_FLAG_SETS];
+    int64_t n = (int64_t)V->L->n_syns;
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < n; i++) {
+        uint8_t f = (uint8_t)(fl[i] & ~SYN_PREV_ACTIVE_FLAG);
+        fl[i] = (uint8_t)(f | ((st[i] != 0) ? SYN_PREV_ACTIVE_FLAG : 0));
+    }
+}
+
+/* layer_cycle_syns_wow[_vec4], cl/syns.cl:179-388: every synapse of one tuft,
+ * syn_idx = cel_idx * syns_per_tft + tft_syn_idz + k. */
+static void k_syn_cycle(const bm_area_plan* P, const uint8_t* axns, lview* V, const bm_tuft_plan* T) {
+    const bm_layer_plan* L = V->L;
+    const uint8_t* slc = V->b[BM_BUF_SYN_SRC_SLC_IDS];
+    const int8_t* vo = (const int8_t*)V->b[BM_BUF_SYN_SRC_COL_V_OFFS];
+    const int8_t* uo = (const int8_t*)V->b[BM_BUF_SYN_SRC_COL_U_OFFS];
+    uint8_t* st = V->b[BM_BUF_SYN_STATES];
+    uint32_t spt = T->syns_per_tft;
+    int vec4 = (spt % 4) == 0;
+    int64_t cells = (int64_t)L->cells;
+#pragma omp parallel for schedule(static)
+    for (int64_t c = 0; c < cells; c++) {
+        uint32_t cols = L->v_size * L->u_size;
+        uint32_t rem = (uint32_t)(c % cols);
+        uint32_t v = rem / L->u_size, u = rem % L->u_size;
+        uint64_t base = (uint64_t)c * spt + T->syn_idz;
+        for (uint32_t k = 0; k < spt; k++) {
+            uint64_t i = base + k;
+            st[i] = syn_fire(axn_state_safe(P, axns, slc[i], v, vo[i], u, uo[i], vec4));
+        }
+    }
+}
+
+/* den_cycle_tft, cl/bismit.cl:695-747. */
+static void k_den_cycle(lview* V, const bm_tuft_plan* T, int32_t rnd) {
+    const uint8_t* st = V->b[BM_BUF_SYN_STATES];
+    const int8_t* str = (const int8_t*)V->b[BM_BUF_SYN_STRENGTHS];
+    uint8_t* act = V->b[BM_BUF_DEN_ACTIVITIES];
+    uint8_t* sraw = V->b[BM_BUF_DEN_STATES_RAW];
+    uint8_t* sden = V->b[BM_BUF_DEN_STATES];
+    uint32_t spd = T->syns_per_den, thr = T->den_threshold;
+    int64_t n_dens = (int64_t)V->L->cells * T->dens_per_tft;
+#pragma omp parallel for schedule(static)
+    for (int64_t d = 0; d < n_dens; d++) {
+        uint64_t s0 = (uint64_t)d * spd + T->syn_idz;
+        int32_t sum = 0, raw = 0;
+        for (uint32_t k = 0; k < spd; k++) {
+            int8_t s = str[s0 + k];
+            uint8_t a = st[s0 + k];
+            sum += (s >= 0) * (int32_t)a;
+            raw += a;
+        }
+        int active = (uint32_t)sum > thr;
+        sum = active * sum;
+        uint64_t di = (uint64_t)d + T->den_idz;
+        uint32_t seed = ((uint32_t)raw + thr) | (uint32_t)di;
+        act[di] = update_activity_rating(act[di], active, rnd, (int32_t)seed,
+                                         DENDRITE_ACTIVITY_DECAY_FACTOR);
+        int r4 = raw >> 4, s4 = sum >> 4;
+        sraw[di] = (uint8_t)(r4 > 255 ? 255 : r4);
+        sden[di] = (uint8_t)(s4 > 255 ? 255 : s4);
+    }
+}
+
+/* tft_cycle, cl/bismit.cl:755-842 (launched per tuft over all cells of the
+ * layer, src/cortex/tufts.rs:107-127). */
+static void k_tft_cycle(lview* V, const bm_tuft_plan* T) {
+    const uint8_t* sraw = V->b[BM_BUF_DEN_STATES_RAW];
+    const uint8_t* sden = V->b[BM_BUF_DEN_STATES];
+    uint8_t* pid = V->b[BM_BUF_TFT_PREV_BEST_DEN_IDS];
+    uint8_t* praw = V->b[BM_BUF_TFT_PREV_BEST_DEN_STATES_RAW];
+    uint8_t* pst = V->b[BM_BUF_TFT_PREV_BEST_DEN_STATES];
+    uint8_t* ptft = V->b[BM_BUF_TFT_PREV_STATES];
+    uint8_t* bid = V->b[BM_BUF_TFT_BEST_DEN_IDS];
+    uint8_t* braw = V->b[BM_BUF_TFT_BEST_DEN_STATES_RAW];
+    uint8_t* bst = V->b[BM_BUF_TFT_BEST_DEN_STATES];
+    uint8_t* tst = V->b[BM_BUF_TFT_STATES];
+    uint32_t dpt = T->dens_per_tft, mad = T->max_active_dens_l2;
+    int64_t cells = (int64_t)V->L->cells;
+#pragma omp parallel for schedule(static)
+    for (int64_t c = 0; c < cells; c++) {
+        uint64_t d0 = T->den_idz + (uint64_t)c * dpt;
+        uint32_t best_id = 0, best_raw = 0, best_st = 0, sum = 0;
+        for (uint32_t d = 0; d < dpt; d++) {
+            uint32_t r = sraw[d0 + d], s = sden[d0 + d];
+            if (r > best_raw) { best_id = d; best_raw = r; }
+            if (s > best_st) best_st = s;
+            sum += s;
+        }
+        int is_max = sum >= (1u << (mad + 8));
+        uint8_t state = (uint8_t)((uint8_t)(is_max * 255u) + (uint8_t)(!is_max * (sum >> mad)));
+        uint64_t ci = T->cel_idz + (uint64_t)c;
+        pid[ci] = bid[ci]; praw[ci] = braw[ci]; pst[ci] = bst[ci]; ptft[ci] = tst[ci];
+        bid[ci] = (uint8_t)best_id; braw[ci] = (uint8_t)best_raw; bst[ci] = (uint8_t)best_st;
+        tst[ci] = state;
+    }
+}
+
+/* ssc_cycle, cl/bismit.cl:849-884; cel_states is the dendrite state buffer
+ * (SpinyStellateLayer::soma, src/cortex/spiny_stellates.rs:78-84). */
+static void k_ssc_cycle(lview* V) {
+    uint8_t* en = V->b[BM_BUF_CEL_ENERGIES];
+    uint8_t* cs = V->b[BM_BUF_DEN_STATES];
+    int64_t cells = (int64_t)V->L->cells;
+    for (int64_t c = 0; c < cells; c++) {
+        uint32_t energy = en[c], state = cs[c];
+        int active = state != 0;
+        int restless = (energy > 191) & active;
+        int dark = energy == 255;
+        en[c] = (uint8_t)((dark | restless) ? energy - 64 : energy);
+        uint32_t s = state + (uint32_t)restless * 255u + (uint32_t)dark * 255u;
+        cs[c] = (uint8_t)(s > 255 ? 255 : s);
+    }
+}
+
+/* Soma buffer and activities of a host layer (DataCellLayer::soma /
+ * activities): SSC soma = dendrite states, pyramidal soma = cell states. */
+static uint8_t* soma_of(lview* V) {
+    return V->L->kind == BM_LYR_SPINY_STELLATE ? V->b[BM_BUF_DEN_STATES] : V->b[BM_BUF_CEL_STATES];
+}
+
+/* inhib_simple, cl/control.cl:28-191. */
+static void k_inhib_simple(const bm_area_plan* P, uint8_t* axns, lview* V, int radius, int32_t rnd) {
+    const bm_layer_plan* L = V->L;
+    const uint8_t* cs = soma_of(V);
+    uint8_t* act = V->b[BM_BUF_CEL_ACTIVITIES];
+    int vsz = (int)L->v_size, usz = (int)L->u_size;
+    int64_t cells = (int64_t)L->cells;
+#pragma omp parallel for schedule(static)
+    for (int64_t c = 0; c < cells; c++) {
+        int s = (int)(c / (vsz * usz)), rem = (int)(c % (vsz * usz));
+        int v = rem / usz, u = rem % usz;
+        int safe;
+        uint32_t axi = axn_idx(P, (uint8_t)(s + L->base_axn_slc), (uint32_t)v, 0, (uint32_t)u, 0, 0, &safe);
+        uint8_t cel_state = (uint8_t)(safe * cs[c]);
+        int uninhibited = 1;
+        int horizon = radius + INHIB_INFL_HORIZ_OFFSET;
+        int infl_max = horizon * horizon;
+        for (int vo = -radius; vo <= radius; vo++) {
+            int vneg = -vo;
+            int uz = imax(-radius, vneg - radius), um = imin(radius, vneg + radius);
+            for (int uo = uz; uo <= um; uo++) {
+                /* cel_state_3d_safe, cl/bismit.cl:285-297 (offsets passed as char). */
+                int vo8 = (int8_t)vo, uo8 = (int8_t)uo;
+                int vt = v + vo8, ut = u + uo8;
+                int nsafe = (vt >= 0) & (vt < vsz) & (ut >= 0) & (ut < usz);
+                uint8_t nei = nsafe ? cs[(int64_t)s * vsz * usz + (int64_t)vt * usz + ut] : 0;
+                int dist = (iabs(vo) + iabs(uo) + iabs(-vo - uo)) >> 1;
+                int dd = dist - INHIB_INFL_CENTER_OFFSET;
+                int cel_inf = (int)cel_state * infl_max;
+                int nei_inf = (int)nei * (infl_max - dd * dd);
+                uninhibited &= cel_inf >= nei_inf;
+            }
+        }
+        axns[axi] = (uint8_t)(uninhibited * cel_state);
+        int axon_active = uninhibited & (cel_state != 0);
+        act[c] = update_activity_rating(act[c], axon_active, rnd, (int32_t)((uint32_t)cel_state | (uint32_t)c),
+                                        CELL_ACTIVITY_DECAY_FACTOR);
+    }
+}
+
+/* inhib_passthrough, cl/control.cl:194-217. */
+static void k_inhib_passthrough(const bm_area_plan* P, uint8_t* axns, lview* V, int32_t rnd) {
+    const bm_layer_plan* L = V->L;
+    const uint8_t* cs = soma_of(V);
+    uint8_t* act = V->b[BM_BUF_CEL_ACTIVITIES];
+    for (int64_t c = 0; c < (int64_t)L->cells; c++) {
+        uint32_t cols = L->v_size * L->u_size;
+        int s = (int)(c / cols), rem = (int)(c % cols);
+        int v = rem / (int)L->u_size, u = rem % (int)L->u_size;
+        int safe;
+        uint32_t axi = axn_idx(P, (uint8_t)(s + L->base_axn_slc), (uint32_t)v, 0, (uint32_t)u, 0, 0, &safe);
+        uint8_t st = cs[c];
+        axns[axi] = st;
+        act[c] = update_activity_rating(act[c], st != 0, rnd, (int32_t)((uint32_t)st | (uint32_t)c),
+                                        CELL_ACTIVITY_DECAY_FACTOR);
+    }
+}
+
+/* ssc_mtp_simple + prx_syns__active__mtp_ltd, cl/bismit.cl:888-915, :604-639.
+ * The seed is syn_idz + i with i already starting at syn_idz (doubled). */
+static void k_ssc_mtp_simple(const bm_area_plan* P, const uint8_t* axns, lview* V, int32_t rnd) {
+    const bm_layer_plan* L = V->L;
+    const uint8_t* st = V->b[BM_BUF_SYN_STATES];
+    int8_t* str = (int8_t*)V->b[BM_BUF_SYN_STRENGTHS];
+    uint32_t spt = L->tufts[0].syns_per_tft;
+    const int32_t pr_mask = lr_mask_of(0), dr_mask = lr_mask_of(2);
+    int64_t cells = (int64_t)L->cells;
+    (void)P;
+#pragma omp parallel for schedule(dynamic, 256)
+    for (int64_t c = 0; c < cells; c++) {
+        if (!axns[L->axn_idz + (uint32_t)c]) continue;
+        uint32_t syn_idz = (uint32_t)c * spt;
+        for (uint32_t i = syn_idz; i < syn_idz + spt; i++) {
+            int8_t s = str[i];
+            int32_t seed = (int32_t)(syn_idz + i);
+            int inc = rnd_inc(rnd, seed, s, pr_mask);
+            int dec = rnd_dec(rnd, seed, s, dr_mask);
+            int active = st[i] != 0;
+            s = (int8_t)(s + active * inc);
+            s = (int8_t)(s - (!active) * dec);
+            str[i] = s;
+        }
+    }
+}
+
+/* pyr_cycle, cl/bismit.cl:961-1022, bound as at src/cortex/pyramidals.rs:149-164:
+ * the first parameter receives best_den_states_raw, and the apical term is
+ * discarded by the comma operator at :1021. */
+static void k_pyr_cycle(lview* V) {
+    const bm_layer_plan* L = V->L;
+    const uint8_t* braw = V->b[BM_BUF_TFT_BEST_DEN_STATES_RAW];
+    const uint8_t* tst = V->b[BM_BUF_TFT_STATES];
+    uint8_t* ps = V->b[BM_BUF_CEL_STATES];
+    uint32_t cells = L->cells, fl = L->enabled_tft_flags;
+    for (uint32_t c = 0; c < cells; c++) {
+        int prx_en = (fl & DEN_BASAL_PROXIMAL_FLAG) != 0;
+        int dst_en = (fl & DEN_BASAL_DISTAL_FLAG) != 0;
+        uint8_t prx = (uint8_t)(prx_en * tst[(uint64_t)L->bsl_prx_tft_id * cells + c]);
+        uint8_t dst = (uint8_t)(dst_en * braw[(uint64_t)L->bsl_dst_tft_id * cells + c]);
+        int active = prx != 0;
+        int is_min = (prx <= 3) && active;
+        uint8_t prx_c = (uint8_t)((prx >> 2) + is_min);
+        uint8_t dst_c = (uint8_t)(active * (dst >> 1));
+        ps[c] = (uint8_t)(prx_c + dst_c);
+    }
+}
+
+/* pyr_output, cl/control.cl:298-314. */
+static void k_pyr_output(const bm_area_plan* P, uint8_t* axns, lview* V) {
+    const bm_layer_plan* L = V->L;
+    const uint8_t* cs = soma_of(V);
+    uint32_t cols = L->v_size * L->u_size;
+    for (uint32_t c = 0; c < L->cells; c++) {
+        uint32_t s = c / cols, rem = c % cols, v = rem / L->u_size, u = rem % L->u_size;
+        int safe;
+        uint32_t axi = axn_idx(P, (uint8_t)(s + L->base_axn_slc), v, 0, u, 0, 0, &safe);
+        axns[axi] = cs[c];
+    }
+}
+
+/* inhib_intra_column, cl/control.cl:319-352 (best = (state >= best) * state). */
+static void k_inhib_intra_column(const bm_area_plan* P, uint8_t* axns, lview* V) {
+    const bm_layer_plan* L = V->L;
+    const uint8_t* cs = soma_of(V);
+    uint32_t cols = L->v_size * L->u_size;
+    for (uint32_t col = 0; col < cols; col++) {
+        uint32_t v = col / L->u_size, u = col % L->u_size;
+        uint8_t best = 0;
+        for (uint32_t s = 0; s < L->depth; s++) {
+            uint8_t st = cs[s * cols + col];
+            best = (uint8_t)((st >= best) * st);
+        }
+        for (uint32_t s = 0; s < L->depth; s++) {
+            int safe;
+            uint32_t axi = axn_idx(P, (uint8_t)(s + L->base_axn_slc), v, 0, u, 0, 0, &safe);
+            uint8_t st = cs[s * cols + col];
+            axns[axi] = (uint8_t)((st >= best) * st);
+        }
+    }
+}
+
+/* tft_dst_mtp + dst_syns__active__mtpot_mtdep, cl/bismit.cl:1195-1268, :554-600,
+ * launched per distal tuft with pr_l2i = 0, dr_l2i = 5 (src/cortex/tufts.rs:151-208). */
+static void k_tft_dst_mtp(const uint8_t* axns, lview* V, const bm_tuft_plan* T, int32_t rnd) {
+    const bm_layer_plan* L = V->L;
+    const uint8_t* pid = V->b[BM_BUF_TFT_PREV_BEST_DEN_IDS];
+    const uint8_t* praw = V->b[BM_BUF_TFT_PREV_BEST_DEN_STATES_RAW];
+    const uint8_t* sfl = V->b[BM_BUF_SYN_FLAG_SETS];
+    uint8_t* cfl = V->b[BM_BUF_CEL_FLAG_SETS];
+    int8_t* str = (int8_t*)V->b[BM_BUF_SYN_STRENGTHS];
+    const int32_t pr_mask = lr_mask_of(0), dr_mask = lr_mask_of(5);
+    uint32_t spd = T->syns_per_den, spt = T->syns_per_tft;
+    int64_t cells = (int64_t)L->cells;
+#pragma omp parallel for schedule(dynamic, 256)
+    for (int64_t ci = 0; ci < cells; ci++) {
+        uint32_t c = (uint32_t)ci;
+        uint32_t tci = c + (uint32_t)T->cel_idz;
+        uint32_t syn_idz_celtft = c * spt + (uint32_t)T->syn_idz;
+        uint8_t f = cfl[c];
+        int active = axns[L->axn_idz + c] != 0;
+        int prev_active = (f & CEL_PREV_ACTIVE_FLAG) == CEL_PREV_ACTIVE_FLAG;
+        int newly = (!prev_active) & active;
+        int tft_prev_active = praw[tci] != 0;
+        if (newly & tft_prev_active) {
+            uint32_t syn_idz = (uint32_t)pid[tci] * spd + syn_idz_celtft;
+            for (uint32_t i = syn_idz; i < syn_idz + spd; i++) {
+                int8_t s = str[i];
+                int32_t seed = (int32_t)(syn_idz + i);
+                if ((sfl[i] & SYN_PREV_ACTIVE_FLAG) == SYN_PREV_ACTIVE_FLAG)
+                    s = (int8_t)(s + rnd_inc(rnd, seed, s, pr_mask));
+                else
+                    s = (int8_t)(s - rnd_dec(rnd, seed, s, dr_mask));
+                str[i] = s;
+            }
+        }
+        f = (uint8_t)(f & ~CEL_PREV_ACTIVE_FLAG);
+        f = (uint8_t)(f | (active * CEL_PREV_ACTIVE_FLAG));
+        cfl[c] = f;
+    }
+}
+
+/* --------------------------------------------------------- layer steps --- */
+
+/* Control layers hosted on V in (host, exe_order) order
+ * (src/cortex/control_cell_layer.rs:21, src/cortex/iinn.rs:105-127,
+ * src/cortex/intra_column_inhib.rs:80-92, src/cortex/pyr_outputter.rs:70-80). */
+static void controls_post(const bm_area_plan* P, uint8_t* axns, lview* V, uint64_t cyc) {
+    const bm_layer_plan* L = V->L;
+    for (uint32_t k = 0; k < L->n_ctrl; k++) {
+        const bm_ctrl_plan* C = &L->ctrl[k];
+        switch (C->kind) {
+        case BM_LYR_CTRL_INHIB_BASKET:
+            if (P->settings & BM_SET_BYPASS_INHIB)
+                k_inhib_passthrough(P, axns, V, 0);
+            else
+                k_inhib_simple(P, axns, V, (int)C->field_radius,
+                               bmo_rnd(P->rnd_seed, P->area_id, C->layer_id, BM_RND_INHIB, 0, cyc));
+            break;
+        case BM_LYR_CTRL_PYR_OUTPUT: k_pyr_output(P, axns, V); break;
+        case BM_LYR_CTRL_INTRA_COLUMN: k_inhib_intra_column(P, axns, V); break;
+        default: break;
+        }
+    }
+}
+
+/* Dendrites::cycle (src/cortex/dendrites.rs:191-209) with Synapses::cycle
+ * (src/cortex/synapses.rs:363-387) in front. */
+static void dens_cycle(const bm_area_plan* P, uint8_t* axns, lview* V, uint64_t cyc) {
+    const bm_layer_plan* L = V->L;
+    k_set_syn_flags(V);
+    for (uint32_t t = 0; t < L->n_tufts; t++) k_syn_cycle(P, axns, V, &L->tufts[t]);
+    for (uint32_t t = 0; t < L->n_tufts; t++)
+        k_den_cycle(V, &L->tufts[t], bmo_rnd(P->rnd_seed, P->area_id, L->layer_id, BM_RND_DEN_CYCLE, t, cyc));
+}
+
+/* SpinyStellateLayer::cycle, src/cortex/spiny_stellates.rs:220-252. */
+static void ssc_layer_cycle(const bm_area_plan* P, uint8_t* axns, lview* V, uint64_t cyc) {
+    dens_cycle(P, axns, V, cyc);
+    k_ssc_cycle(V);
+    controls_post(P, axns, V, cyc);
+}
+
+/* PyramidalLayer::cycle, src/cortex/pyramidals.rs:297-335 (learning included). */
+static void pyr_layer_cycle(const bm_area_plan* P, uint8_t* axns, lview* V, uint64_t cyc) {
+    const bm_layer_plan* L = V->L;
+    dens_cycle(P, axns, V, cyc);
+    for (uint32_t t = 0; t < L->n_tufts; t++) k_tft_cycle(V, &L->tufts[t]);
+    k_pyr_cycle(V);
+    controls_post(P, axns, V, cyc);
+    if (!(P->settings & (BM_SET_DISABLE_LEARNING | BM_SET_DISABLE_PYRS))) {
+        for (uint32_t t = 0; t < L->n_tufts; t++)
+            if (L->tufts[t].den_kind == BM_DEN_DISTAL)
+                k_tft_dst_mtp(axns, V, &L->tufts[t],
+                              bmo_rnd(P->rnd_seed, P->area_id, L->layer_id, BM_RND_TFT_DST_MTP, t, cyc));
+    }
+}
+
+static void layer_learn(const bm_area_plan* P, uint8_t* axns, lview* V, uint64_t cyc) {
+    const bm_layer_plan* L = V->L;
+    if (L->kind == BM_LYR_SPINY_STELLATE) {
+        if (!(P->settings & (BM_SET_DISABLE_LEARNING | BM_SET_DISABLE_SSCS)))
+            k_ssc_mtp_simple(P, axns, V,
+                             bmo_rnd(P->rnd_seed, P->area_id, L->layer_id, BM_RND_SSC_MTP, 0, cyc));
+    } else {
+        if (!(P->settings & (BM_SET_DISABLE_LEARNING | BM_SET_DISABLE_PYRS))) {
+            for (uint32_t t = 0; t < L->n_tufts; t++)
+                if (L->tufts[t].den_kind == BM_DEN_DISTAL)
+                    k_tft_dst_mtp(axns, V, &L->tufts[t],
+                                  bmo_rnd(P->rnd_seed, P->area_id, L->layer_id, BM_RND_TFT_DST_MTP, t, cyc));
+        }
+    }
+}
+
+static void layer_cycle(const bm_area_plan* P, uint8_t* axns, lview* V, uint64_t cyc) {
+    if (V->L->kind == BM_LYR_SPINY_STELLATE) ssc_layer_cycle(P, axns, V, cyc);
+    else pyr_layer_cycle(P, axns, V, cyc);
+}
+
+/* CorticalArea::cycle, src/cortex/cortical_area.rs:716-789 (regrowth and the
+ * samplers excluded). */
+static void area_cycle(const bm_area_plan* P, uint8_t* slab, uint64_t cyc) {
+    uint8_t* axns = slab + P->axon_off;
+    lview V[BM_MAX_LAYERS];
+    for (uint32_t l = 0; l < P->n_layers; l++) view(&P->layers[l], slab, &V[l]);
+    if (!(P->settings & BM_SET_DISABLE_SSCS)) {
+        for (uint32_t k = 0; k < P->n_cycle_order; k++) {
+            lview* v = &V[P->cycle_order[k]];
+            if (v->L->tags & BM_TAG_SPATIAL) layer_cycle(P, axns, v, cyc);
+        }
+        for (uint32_t k = 0; k < P->n_cycle_order; k++) {
+            lview* v = &V[P->cycle_order[k]];
+            if (v->L->tags & BM_TAG_SPATIAL) layer_learn(P, axns, v, cyc);
+        }
+    }
+    if (!(P->settings & BM_SET_DISABLE_PYRS)) {
+        for (uint32_t k = 0; k < P->n_cycle_order; k++) {
+            lview* v = &V[P->cycle_order[k]];
+            if (!(v->L->tags & BM_TAG_SPATIAL)) layer_cycle(P, axns, v, cyc);
+        }
+    }
+}
+
+int bmo_run(const bm_area_plan* P, uint8_t* slab, const uint8_t* frames, uint64_t frame_len,
+            uint32_t n_cycles, uint64_t start_cycle, int n_threads) {
+#ifdef _OPENMP
+    if (n_threads > 0) omp_set_num_threads(n_threads);
+#else
+    (void)n_threads;
+#endif
+    if (frames && P->n_inputs == 0) return -1;
+    if (frames && frame_len != P->inputs[0].len) return -2;
+    for (uint32_t k = 0; k < n_cycles; k++) {
+        if (frames) memcpy(slab + P->axon_off + P->inputs[0].axn_idz, frames + (uint64_t)k * frame_len, frame_len);
+        area_cycle(P, slab, start_cycle + k);
+    }
+    return 0;
+}
+
+/* ----------------------------------------------------------- growth ---- */
+
+/* gen_syn_offs, src/map/syn_src.rs:47-149 (scale: src/cmn/slice_dims.rs:192-194). */
+int bmo_gen_syn_offs(int radius, uint32_t v_scale, uint32_t u_scale, int8_t* v_out,
+                     int8_t* u_out, int cap) {
+    if (radius < 0) return -1;
+    int v_rad = (radius * (int)v_scale) >> SLC_SCL_COEFF_L2;
+    int u_rad = (radius * (int)u_scale) >> SLC_SCL_COEFF_L2;
+    int rmax = v_rad > u_rad ? v_rad : u_rad;
+    if (rmax > 127) return -1;
+    if (v_scale == 0) return -1;
+    int n = 0;
+    for (int vo = -v_rad; vo <= v_rad; vo++) {
+        int vinv = -vo;
+        int a = imax(-v_rad, vinv - v_rad), b = imin(v_rad, vinv + v_rad);
+        /* scl_inv_scl: (val * (scl << 3)) / (scl_inv << 3), truncating. */
+        int uz = (a * ((int)u_scale << 3)) / ((int)v_scale << 3);
+        int un = (b * ((int)u_scale << 3)) / ((int)v_scale << 3) + 1;
+        for (int uo = uz; uo < un; uo++) {
+            if (vo > 127 || vo < -127 || uo > 127 || uo < -127) return -1;
+            if (n >= cap) return -1;
+            v_out[n] = (int8_t)vo;
+            u_out[n] = (int8_t)uo;
+            n++;
+        }
+    }
+    return n;
+}
+
+/* The per-dendrite growth stream: word k of dendrite d of (layer, tuft). */
+static inline uint64_t grow_word(uint64_t key, uint64_t den, uint64_t k) {
+    return splitmix64(splitmix64(key + den) + k);
+}
+static inline uint32_t uniform_idx(uint32_t r, uint32_t n) {
+    return (uint32_t)(((uint64_t)r * n) >> 32);
+}
+
+#define GROW_MAX_ATTEMPTS 1024
+
+int bmo_grow(const bm_area_plan* P, uint8_t* slab, uint64_t seed, uint32_t init_flags) {
+    for (uint32_t l = 0; l < P->n_layers; l++) {
+        const bm_layer_plan* L = &P->layers[l];
+        lview V;
+        view(L, slab, &V);
+        uint8_t* slc = V.b[BM_BUF_SYN_SRC_SLC_IDS];
+        int8_t* vo = (int8_t*)V.b[BM_BUF_SYN_SRC_COL_V_OFFS];
+        int8_t* uo = (int8_t*)V.b[BM_BUF_SYN_SRC_COL_U_OFFS];
+        int8_t* str = (int8_t*)V.b[BM_BUF_SYN_STRENGTHS];
+        for (uint32_t t = 0; t < L->n_tufts; t++) {
+            const bm_tuft_plan* T = &L->tufts[t];
+            /* Offset pools per distinct source slice (SynSrcSliceInfo::new,
+             * src/map/syn_src.rs:241-310). */
+            enum { OFS_CAP = 3 * 127 * 128 + 1 };
+            int8_t* ov[BM_MAX_SRC_SLICES];
+            int8_t* ou[BM_MAX_SRC_SLICES];
+            int on[BM_MAX_SRC_SLICES];
+            int nonspatial[BM_MAX_SRC_SLICES];
+            int rv[BM_MAX_SRC_SLICES], ru[BM_MAX_SRC_SLICES];
+            uint64_t poss = 0;
+            for (uint32_t k = 0; k < T->n_src_uniq; k++) {
+                uint8_t s = T->src_uniq_slc_ids[k];
+                int reach = T->src_uniq_reaches[k];
+                nonspatial[k] = P->slc_v_scale[s] == 0;
+                ov[k] = ou[k] = NULL;
+                if (nonspatial[k]) {
+                    rv[k] = (int)(P->slc_v_size[s] / 2);
+                    ru[k] = (int)(P->slc_u_size[s] / 2);
+                    on[k] = 0;
+                    poss = (uint64_t)P->slc_v_size[s] * P->slc_u_size[s] * T->n_src;
+                } else {
+                    ov[k] = (int8_t*)malloc(OFS_CAP);
+                    ou[k] = (int8_t*)malloc(OFS_CAP);
+                    on[k] = bmo_gen_syn_offs(reach, P->slc_v_scale[s], P->slc_u_scale[s], ov[k], ou[k], OFS_CAP);
+                    if (on[k] <= 0) return -1;
+                    rv[k] = (reach * (int)P->slc_v_scale[s]) >> SLC_SCL_COEFF_L2;
+                    ru[k] = (reach * (int)P->slc_u_scale[s]) >> SLC_SCL_COEFF_L2;
+                    poss = (uint64_t)on[k] * T->n_src;
+                }
+            }
+            int saturated = poss == T->syns_per_den;
+            int unique = !(init_flags & BM_INIT_NO_UNIQUE) && !saturated;
+            uint64_t key = splitmix64(seed ^ 0x67726F77ull) + (((uint64_t)P->area_id << 48) |
+                           ((uint64_t)L->layer_id << 40) | ((uint64_t)t << 32));
+            key = splitmix64(key);
+            uint64_t n_dens = (uint64_t)L->cells * T->dens_per_tft;
+            int64_t cols = (int64_t)L->v_size * L->u_size;
+            for (uint64_t d = 0; d < n_dens; d++) {
+                uint64_t s0 = T->syn_idz + d * T->syns_per_den;
+                uint64_t wk = 0;
+                for (uint32_t j = 0; j < T->syns_per_den; j++) {
+                    uint8_t ns = 0; int nv = 0, nu = 0; int nstr = 0;
+                    for (int att = 0; att < GROW_MAX_ATTEMPTS; att++) {
+                        uint64_t w = grow_word(key, d, wk++);
+                        uint64_t w2 = grow_word(key, d, wk++);
+                        uint32_t pi = uniform_idx((uint32_t)w, T->n_src);
+                        ns = T->src_slc_ids[pi];
+                        uint32_t k = 0;
+                        while (k < T->n_src_uniq && T->src_uniq_slc_ids[k] != ns) k++;
+                        if (nonspatial[k]) {
+                            nv = (int)uniform_idx((uint32_t)(w >> 32), (uint32_t)(2 * rv[k] + 1)) - rv[k];
+                            nu = (int)uniform_idx((uint32_t)w2, (uint32_t)(2 * ru[k] + 1)) - ru[k];
+                            nstr = 0;
+                        } else {
+                            uint32_t oi = uniform_idx((uint32_t)(w >> 32), (uint32_t)on[k]);
+                            nv = ov[k][oi]; nu = ou[k][oi];
+                            int inten = ((rv[k] - iabs(nv)) + (ru[k] - iabs(nu))) >> 3;
+                            int r = (int)uniform_idx((uint32_t)w2, 7u) - 3;
+                            nstr = (int8_t)(uint8_t)(inten * r);
+                        }
+                        if (!unique) break;
+                        int64_t nk = (int64_t)ns * cols + (int64_t)nv * L->u_size + nu;
+                        if (nk == 0) break;
+                        int dup = 0;
+                        for (uint32_t jj = 0; jj < j; jj++) {
+                            int64_t ok = (int64_t)slc[s0 + jj] * cols + (int64_t)vo[s0 + jj] * L->u_size + uo[s0 + jj];
+                            if (ok == nk) { dup = 1; break; }
+                        }
+                        if (!dup) break;
+                    }
+                    slc[s0 + j] = ns;
+                    vo[s0 + j] = (int8_t)nv;
+                    uo[s0 + j] = (int8_t)nu;
+                    str[s0 + j] = (init_flags & BM_INIT_STRENGTH_ZERO) ? 0 : (int8_t)nstr;
+                }
+            }
+            for (uint32_t k = 0; k < T->n_src_uniq; k++) { free(ov[k]); free(ou[k]); }
+        }
+    }
+    return 0;
+}
