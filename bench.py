@@ -1,0 +1,358 @@
+"""Benchmark: synapse-cycles/s of bismit's cortical cycle with learning on B200.
+
+One step = one full cycle (intake, spiny stellate layer with inhibition and
+learning, pyramidal layer with column inhibition and learning) of one area over
+one input frame. Default workload: area_256 (256 x 256 columns, 272,629,760
+synapses), the reference's single-area bandwidth configuration.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--workload area_256] [--path fused|plain]
+
+With N > 1 (launched by torch.distributed.run) every rank runs an independent
+replica of the area (no collective on the data path: the areas are
+independent), timing is the max over ranks and `value` counts all ranks'
+synapses ("scaling": "weak").
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "synapse-cycles/s incl. learning (bit-exact)"
+UNIT = "synapse-cycles/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="area_256")
+    ap.add_argument("--path", default="fused", choices=["fused", "plain"])
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-sample-seconds", type=float, default=12.0)
+    return ap.parse_args()
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def workload_config(name):
+    from bismit_b200 import configs
+    side, s, d, pd, ps, pr, act = configs.WORKLOADS[name]
+    return {
+        "workload": name,
+        "columns": "%dx%d" % (side, side),
+        "spiny_stellate": "1 tuft x 1 dendrite x %d synapses, reach 6" % s,
+        "pyramidal": "depth %d; proximal %dx%d reach %d; distal 16x32 reach 6" % (d, pd, ps, pr),
+        "input_active": act,
+        "learning": True,
+        "regrowth": False,
+    }
+
+
+def algorithmic_bytes(plan, kernel):
+    """Algorithmic bytes of one launch of `kernel` (per-unit figures in DESIGN.md)."""
+    syn = sum(int(plan.layers[i].n_syns) for i in range(plan.n_layers))
+    per_tuft = []
+    for i in range(plan.n_layers):
+        L = plan.layers[i]
+        for t in range(L.n_tufts):
+            T = L.tufts[t]
+            n_syn = int(L.cells) * int(T.syns_per_tft)
+            n_den = int(L.cells) * int(T.dens_per_tft)
+            n_ct = int(L.cells) if L.kind == 2 else 0
+            per_tuft.append((n_syn, n_den, n_ct))
+    if kernel == "fused_tuft_cycle":
+        tot = sum(7 * a + 4 * b + 12 * c for a, b, c in per_tuft)
+        return tot / len(per_tuft)
+    if kernel == "syn_cycle":
+        return sum(4 * a for a, _, _ in per_tuft) / len(per_tuft)
+    if kernel == "den_cycle_tft":
+        return sum(2 * a + 4 * b for a, b, _ in per_tuft) / len(per_tuft)
+    if kernel == "tft_set_syn_flags":
+        return 3 * syn / plan.n_layers
+    return None
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons during a region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.idx = gpu_index
+        self.p = None
+        self.path = os.environ.get("BM_CLOCKS_LOG") or os.path.join("/tmp", "bm_clocks_%d_%d.csv" % (os.getpid(), gpu_index))
+
+    def start(self):
+        try:
+            self.f = open(self.path, "w")
+            self.p = subprocess.Popen(["nvidia-smi", "--query-gpu=" + self.Q, "--format=csv,noheader,nounits",
+                                       "-i", str(self.idx), "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except Exception:
+            self.p.kill()
+        self.f.close()
+        mhz, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                mhz.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not mhz:
+            return None
+        return {"sm_mhz": float(np.median(mhz)), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(mhz)}
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def traffic_for(kernel, workload):
+    """Per-launch DRAM bytes from the committed ncu summary, if any."""
+    p = os.path.join(ROOT, "profiles", "traffic.txt")
+    if not os.path.exists(p):
+        return None
+    for line in open(p):
+        parts = line.split()
+        if len(parts) >= 3 and parts[0] == kernel and parts[1] == workload:
+            return float(parts[2])
+    return None
+
+
+def cpu_baseline(plan, slab, frames, budget_s, prefer_ref=True):
+    """Times the reference kernels compiled for the CPU (oracle/_ref, all host
+    threads) or, without them, the C restatement, on cycles of the same area."""
+    import oracle
+    kind = "reference" if (prefer_ref and oracle.load_ref() is not None) else "port"
+    impl = "ref" if kind == "reference" else "port"
+    threads = os.cpu_count() or 1
+    work = slab.copy()
+    t0 = time.perf_counter()
+    n = 0
+    while True:
+        oracle.run(plan, work, frames[n % len(frames)][None, :], 1, start_cycle=n, threads=threads, impl=impl)
+        n += 1
+        if time.perf_counter() - t0 >= budget_s or n >= 1000:
+            break
+    dt = time.perf_counter() - t0
+    return {"value": int(plan.n_syns_total) * n / dt, "unit": UNIT, "cores": threads, "kind": kind,
+            "sample": "%d cycle(s) of %s on the host cores (%.1f s)" % (n, "the same area", dt)}
+
+
+def run_ours(args):
+    import torch
+    from bismit_b200 import configs, cortex, map as M
+
+    ws, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    if ws > 1:
+        import datetime
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    lmaps, areas, act = configs.workload(args.workload)
+    st = configs.bench_settings()
+    if args.path == "plain":
+        st.plain_kernels()
+    desc = M.area_desc("v1", lmaps, areas, st)
+    ctx = cortex._Ctx(local)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    ctx.set_stream(stream.cuda_stream)
+    area = cortex.CorticalArea(ctx, desc, seed=args.seed + 1000 * rank)
+    plan = area.plan
+    flen = area.input_len()
+    K, W = args.steps, args.warmup
+    nfr = K + W
+    host_frames = configs.frames(nfr, flen, act, args.seed + rank)
+    dev_frames = torch.from_numpy(host_frames).to("cuda")
+
+    def barrier():
+        if ws > 1:
+            torch.distributed.barrier()
+
+    init_slab = area.read_slab() if (rank == 0 and ws == 1 and not args.no_cpu_baseline) else None
+
+    # warm-up
+    area.cycle_frames_device(dev_frames.data_ptr(), flen, W)
+    torch.cuda.synchronize()
+    barrier()
+    clocks = Clocks(local)
+    clocks.start()
+    torch.cuda.synchronize()
+    barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    area.cycle_frames_device(dev_frames.data_ptr() + W * flen, flen, K)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    launches = area.launches_per_cycle() * K
+    if ws > 1:
+        t = torch.tensor([ms], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t.item())
+    n_syn = int(plan.n_syns_total)
+    value = n_syn * K * ws / (ms / 1e3)
+
+    # Per-kernel times (library CUDA events on this stream) for the roofline.
+    area.reset_profile()
+    area.set_profiling(True)
+    area.cycle_frames_device(dev_frames.data_ptr() + W * flen, flen, K)
+    torch.cuda.synchronize()
+    prof = area.profile()
+    area.set_profiling(False)
+    dom = max(prof.items(), key=lambda kv: kv[1][1])
+    dom_name, (dom_launches, dom_ms) = dom
+    avg_ms = dom_ms / dom_launches
+    alg = algorithmic_bytes(plan, dom_name)
+    peak, peak_kind = peaks()
+    roofline = None
+    if alg is not None:
+        ach = alg / (avg_ms / 1e3) / 1e9
+        tr = traffic_for(dom_name, args.workload)
+        roofline = {"bound": "hbm", "kernel": dom_name, "achieved": round(ach, 1), "peak": peak, "unit": "GB/s",
+                    "frac": round(ach / peak, 4), "peak_source": peak_kind, "traffic": tr,
+                    "algorithmic_bytes_per_launch": int(alg), "avg_launch_ms": round(avg_ms, 4),
+                    "share": round(dom_ms / sum(v[1] for v in prof.values()), 3)}
+
+    # End to end through the public API with host buffers.
+    import ctypes
+    pin_in = torch.from_numpy(host_frames).pin_memory()
+    out_len = area.output_len()
+    pin_out = torch.empty(out_len, dtype=torch.uint8).pin_memory()
+    lib = area.lib
+    torch.cuda.synchronize()
+    barrier()
+    t0 = time.perf_counter()
+    e0.record(stream)
+    for k in range(K):
+        lib.bm_area_write_input(area.h, 0, ctypes.c_void_p(pin_in[W + k].data_ptr()), flen)
+        lib.bm_area_cycle(area.h, 1)
+        lib.bm_area_read_output(area.h, 0, ctypes.c_void_p(pin_out.data_ptr()), out_len)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1)
+    e2e_wall = time.perf_counter() - t0
+    barrier()
+    if ws > 1:
+        t = torch.tensor([e2e_ms], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e_val = n_syn * K * ws / (e2e_ms / 1e3)
+
+    cpu = None
+    if init_slab is not None:
+        cpu = cpu_baseline(plan, init_slab, host_frames, args.cpu_sample_seconds)
+
+    if rank == 0:
+        cfg = workload_config(args.workload)
+        cfg.update({"path": args.path, "synapses_per_area": n_syn, "areas": ws, "parallelism": "replicas x%d" % ws,
+                    "l2": "state slab %.2f GB per area > 126 MB L2, no flush needed" % (plan.slab_bytes / 1e9)})
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": K, "warmup": W,
+            "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "u8/i8", "data": "synthetic (seeded frames, seeded synapse growth)", "config": cfg,
+            "clocks": clk,
+            "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": flen, "d2h_bytes_per_step": out_len,
+                    "wall_s": round(e2e_wall, 4)},
+            "gpu_launches": launches,
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "kernels": {k: {"launches": v[0], "ms": round(v[1], 4)} for k, v in prof.items()},
+        }
+        print(json.dumps(line), flush=True)
+    area.close()
+    ctx.close()
+    if ws > 1:
+        torch.distributed.destroy_process_group()
+
+
+def run_reference(args):
+    """The reference's own kernels (cl/*.cl compiled for the CPU, all host
+    threads) on the same workload; rank 0 only."""
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return
+    import oracle
+    from bismit_b200 import configs, map as M, plan_of
+    if oracle.load_ref() is None:
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref (bismit's cl/*.cl compiled for the CPU) "
+                                                             "was not built: no bismit checkout at build time"}))
+        return
+    lmaps, areas, act = configs.workload(args.workload)
+    desc = M.area_desc("v1", lmaps, areas, configs.bench_settings())
+    plan = plan_of(desc, args.seed + 1)
+    slab = np.zeros(int(plan.slab_bytes), np.uint8)
+    oracle.grow(plan, slab, args.seed + 1, desc.init_flags)
+    flen = int(plan.inputs[0].len)
+    fr = configs.frames(args.steps + args.warmup, flen, act, args.seed)
+    threads = os.cpu_count() or 1
+    for k in range(args.warmup):
+        oracle.run(plan, slab, fr[k][None, :], 1, start_cycle=k, threads=threads, impl="ref")
+    t0 = time.perf_counter()
+    for k in range(args.steps):
+        oracle.run(plan, slab, fr[args.warmup + k][None, :], 1, start_cycle=args.warmup + k, threads=threads, impl="ref")
+    dt = time.perf_counter() - t0
+    value = int(plan.n_syns_total) * args.steps / dt
+    cfg = workload_config(args.workload)
+    cfg.update({"synapses_per_area": int(plan.n_syns_total), "areas": 1})
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": dt * 1e3 / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u8/i8", "data": "synthetic", "config": cfg,
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
+                         "sample": "%d full cycles of the area" % args.steps},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -175,6 +175,7 @@ def lib():
         "bm_ctx_create": (C.c_int, [C.c_int, u32, P(vp)]),
         "bm_ctx_destroy": (C.c_int, [vp]),
         "bm_ctx_set_stream": (C.c_int, [vp, vp]),
+        "bm_ctx_use_own_stream": (C.c_int, [vp]),
         "bm_ctx_synchronize": (C.c_int, [vp]),
         "bm_area_create": (C.c_int, [vp, P(bm_area_desc), u64, P(vp)]),
         "bm_area_destroy": (C.c_int, [vp]),

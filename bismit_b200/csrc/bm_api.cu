@@ -72,7 +72,8 @@ struct bm_ctx_s {
     int device = 0;
     cudaStream_t own = nullptr;
     cudaStream_t user = nullptr;
-    cudaStream_t stream() const { return user ? user : own; }
+    bool user_set = false;
+    cudaStream_t stream() const { return user_set ? user : own; }
 };
 
 struct bm_area_s {
@@ -169,29 +170,44 @@ void enqueue_pyr_learn(bm_area_s* A, uint32_t i) {
             A->run(K_TFT_DST_MTP, [&] { launch_tft_dst_mtp_plain(A->axns(), A->dl[i], t, A->ctl, A->stream()); });
 }
 
+// Synapse flags, synapse cycle, dendrite cycle and (pyramidal) tuft cycle of
+// every tuft. The plain form launches them as bismit does: flags over the
+// whole layer, then each stage per tuft. The fused form takes each tuft on its
+// own: one fused launch where the tuft qualifies, else that tuft's four stages.
+// The stages of different tufts touch disjoint buffers, so both orders give
+// the same bytes.
+void enqueue_tufts(bm_area_s* A, uint32_t i) {
+    const bm_layer_plan& L = A->plan.layers[i];
+    const DevLayer& D = A->dl[i];
+    cudaStream_t s = A->stream();
+    const bool pyr = L.kind == BM_LYR_PYRAMIDAL;
+    if (A->exec_path == BM_PATH_PLAIN) {
+        enqueue_dens_plain(A, i);
+        if (pyr)
+            for (uint32_t t = 0; t < L.n_tufts; t++) A->run(K_TFT_CYCLE, [&] { launch_tft_cycle_plain(D, t, s); });
+        return;
+    }
+    for (uint32_t t = 0; t < L.n_tufts; t++) {
+        if (A->fused.tuft_ok[i][t]) {
+            A->run(K_FUSED_TUFT, [&] { launch_fused_tuft(A->fused, A->axns(), A->slices, D, i, t, A->ctl, s); });
+        } else {
+            A->run(K_SYN_FLAGS, [&] { launch_set_syn_flags_tuft(D, t, s); });
+            A->run(K_SYN_CYCLE, [&] { launch_syn_cycle_plain(A->axns(), A->slices, D, t, s); });
+            A->run(K_DEN_CYCLE, [&] { launch_den_cycle_plain(D, t, A->ctl, s); });
+            if (pyr) A->run(K_TFT_CYCLE, [&] { launch_tft_cycle_plain(D, t, s); });
+        }
+    }
+}
+
 void enqueue_layer_cycle(bm_area_s* A, uint32_t i) {
     const bm_layer_plan& L = A->plan.layers[i];
     const DevLayer& D = A->dl[i];
     cudaStream_t s = A->stream();
-    bool fused = A->exec_path == BM_PATH_FUSED && A->fused.layer_ok[i];
+    enqueue_tufts(A, i);
     if (L.kind == BM_LYR_SPINY_STELLATE) {
-        if (fused) {
-            for (uint32_t t = 0; t < L.n_tufts; t++)
-                A->run(K_FUSED_TUFT, [&] { launch_fused_tuft(A->fused, A->axns(), A->slices, D, i, t, A->ctl, s); });
-        } else {
-            enqueue_dens_plain(A, i);
-        }
         A->run(K_SSC_CYCLE, [&] { launch_ssc_cycle(D, s); });
         enqueue_controls(A, i);
     } else {
-        if (fused) {
-            for (uint32_t t = 0; t < L.n_tufts; t++)
-                A->run(K_FUSED_TUFT, [&] { launch_fused_tuft(A->fused, A->axns(), A->slices, D, i, t, A->ctl, s); });
-        } else {
-            enqueue_dens_plain(A, i);
-            for (uint32_t t = 0; t < L.n_tufts; t++)
-                A->run(K_TFT_CYCLE, [&] { launch_tft_cycle_plain(D, t, s); });
-        }
         A->run(K_PYR_CYCLE, [&] { launch_pyr_cycle_plain(D, s); });
         enqueue_controls(A, i);
         enqueue_pyr_learn(A, i);
@@ -339,6 +355,14 @@ int bm_ctx_destroy(bm_ctx ctx) {
 int bm_ctx_set_stream(bm_ctx ctx, void* stream) {
     if (!ctx) return set_err(BM_ERR_INVALID, "null ctx");
     ctx->user = (cudaStream_t)stream;
+    ctx->user_set = true;
+    return BM_OK;
+}
+
+int bm_ctx_use_own_stream(bm_ctx ctx) {
+    if (!ctx) return set_err(BM_ERR_INVALID, "null ctx");
+    ctx->user = nullptr;
+    ctx->user_set = false;
     return BM_OK;
 }
 
@@ -432,7 +456,7 @@ int bm_area_create(bm_ctx ctx, const bm_area_desc* desc, uint64_t seed, bm_area*
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (d_off) cudaFree(d_off);
     if (e != cudaSuccess) { free_area(A); return cuda_err(e, "synapse growth"); }
-    rc = prepare_fused(A->fused, A->plan, A->dl, A->slab, s, &err);
+    rc = prepare_fused(A->fused, A->plan, &err);
     if (rc != BM_OK) { free_area(A); return set_err(rc, "%s", err.c_str()); }
     *out = A;
     return BM_OK;
@@ -539,9 +563,6 @@ int bm_area_write(bm_area area, uint32_t buf_kind, uint32_t layer, uint64_t offs
     DevGuard g(area->ctx->device);
     if (len) CU(cudaMemcpyAsync(area->slab + off, src, len, cudaMemcpyHostToDevice, area->stream()));
     CU(cudaStreamSynchronize(area->stream()));
-    if (buf_kind == BM_BUF_SYN_SRC_SLC_IDS || buf_kind == BM_BUF_SYN_SRC_COL_V_OFFS ||
-        buf_kind == BM_BUF_SYN_SRC_COL_U_OFFS)
-        mark_sources_dirty(area->fused, layer);
     return BM_OK;
 }
 
@@ -561,7 +582,6 @@ int bm_area_write_slab(bm_area area, const void* src, uint64_t len) {
     DevGuard g(area->ctx->device);
     CU(cudaMemcpyAsync(area->slab, src, len, cudaMemcpyHostToDevice, area->stream()));
     CU(cudaStreamSynchronize(area->stream()));
-    for (uint32_t l = 0; l < area->plan.n_layers; l++) mark_sources_dirty(area->fused, l);
     return BM_OK;
 }
 

@@ -7,16 +7,17 @@
 namespace bm {
 
 struct FusedArea {
-    bool layer_ok[BM_MAX_LAYERS] = {};
+    int sms = 148;
+    bool tuft_ok[BM_MAX_LAYERS][BM_MAX_TUFTS] = {};
+    uint32_t slc0[BM_MAX_LAYERS][BM_MAX_TUFTS] = {};
+    uint32_t nrec[BM_MAX_LAYERS][BM_MAX_TUFTS] = {};
 };
 
-// Decides, per data layer, whether the fused kernels apply to its scheme and
-// buffer alignment. Returns BM_OK (layers that do not qualify use the plain form).
-int prepare_fused(FusedArea& F, const bm_area_plan& P, const DevLayer* dl, uint8_t* slab, cudaStream_t s,
-                  std::string* err);
+// Decides, per tuft, whether the fused kernel applies (syns_per_den a power of
+// two in 16..512, dens_per_tft a power of two, 16-byte aligned ranges). Tufts
+// that do not qualify run the plain per-stage kernels.
+int prepare_fused(FusedArea& F, const bm_area_plan& P, std::string* err);
 void free_fused(FusedArea& F);
-// Synapse sources of a layer were overwritten by the caller.
-void mark_sources_dirty(FusedArea& F, uint32_t layer);
 // Synapse flags + synapse cycle + dendrite cycle (+ tuft cycle for pyramidal
 // layers) of one tuft in one launch.
 void launch_fused_tuft(const FusedArea& F, const uint8_t* axns, const SliceRec* slices, const DevLayer& L,

@@ -25,6 +25,7 @@ void launch_cycle_end(AreaCtl* ctl, cudaStream_t s);
 
 // Plain form: one kernel per reference stage (bm_plain.cu).
 void launch_set_syn_flags(const DevLayer& L, cudaStream_t s);
+void launch_set_syn_flags_tuft(const DevLayer& L, uint32_t t, cudaStream_t s);
 void launch_syn_cycle_plain(const uint8_t* axns, const SliceRec* slices, const DevLayer& L, uint32_t t,
                             cudaStream_t s);
 void launch_den_cycle_plain(const DevLayer& L, uint32_t t, const AreaCtl* ctl, cudaStream_t s);

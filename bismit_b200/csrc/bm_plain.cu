@@ -256,7 +256,10 @@ __global__ void k_tft_dst_mtp(const uint8_t* __restrict__ axns, DevLayer L, uint
         const uint8_t* sfl = L.buf[BM_BUF_SYN_FLAG_SETS];
         int8_t* str = (int8_t*)L.buf[BM_BUF_SYN_STRENGTHS];
         uint32_t syn_idz = (uint32_t)L.buf[BM_BUF_TFT_PREV_BEST_DEN_IDS][tci] * T.spd + c * T.spt + (uint32_t)T.syn_idz;
-        for (uint32_t i = syn_idz; i < syn_idz + T.spd; i++) {
+        // A best-dendrite id written by the caller past the tuft can address
+        // beyond the layer's synapses; such a range is skipped.
+        uint32_t n = ((uint64_t)syn_idz + T.spd <= L.n_syns) ? T.spd : 0;
+        for (uint32_t i = syn_idz; i < syn_idz + n; i++) {
             int8_t s = str[i];
             int32_t seed = (int32_t)(syn_idz + i);
             if (sfl[i] & kSynPrevActiveFlag) s = (int8_t)(s + rnd_inc(rnd, seed, s, 0x7F));
@@ -276,6 +279,13 @@ void launch_set_syn_flags(const DevLayer& L, cudaStream_t s) {
     uint64_t n = L.n_syns;
     if (!n) return;
     k_set_syn_flags<<<nblk((n + 15) / 16, 256), 256, 0, s>>>(L.buf[BM_BUF_SYN_STATES], L.buf[BM_BUF_SYN_FLAG_SETS], n);
+}
+void launch_set_syn_flags_tuft(const DevLayer& L, uint32_t t, cudaStream_t s) {
+    const DevTuft& T = L.tft[t];
+    uint64_t n = (uint64_t)L.cells * T.spt;
+    if (!n) return;
+    k_set_syn_flags<<<nblk((n + 15) / 16, 256), 256, 0, s>>>(L.buf[BM_BUF_SYN_STATES] + T.syn_idz,
+                                                              L.buf[BM_BUF_SYN_FLAG_SETS] + T.syn_idz, n);
 }
 void launch_syn_cycle_plain(const uint8_t* axns, const SliceRec* slices, const DevLayer& L, uint32_t t,
                             cudaStream_t s) {

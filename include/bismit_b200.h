@@ -292,9 +292,11 @@ const char* bm_version(void);
 /* Creates a context on CUDA device `device` (Cortex::new, src/cortex/cortex.rs:51-61). */
 int bm_ctx_create(int device, uint32_t flags, bm_ctx* out);
 int bm_ctx_destroy(bm_ctx ctx);
-/* Issues all subsequent work of areas created from ctx on `stream`
- * (a cudaStream_t passed as void*; NULL = the library's own stream). */
+/* Issues all subsequent work of areas created from ctx on `stream` (a
+ * cudaStream_t passed as void*; NULL is the CUDA legacy default stream).
+ * bm_ctx_use_own_stream returns to the library's own non-blocking stream. */
 int bm_ctx_set_stream(bm_ctx ctx, void* stream);
+int bm_ctx_use_own_stream(bm_ctx ctx);
 /* Blocks until all work issued through ctx has finished. */
 int bm_ctx_synchronize(bm_ctx ctx);
 

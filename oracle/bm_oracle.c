@@ -446,7 +446,9 @@ static void k_tft_dst_mtp(const uint8_t* axns, lview* V, const bm_tuft_plan* T, 
         int tft_prev_active = praw[tci] != 0;
         if (newly & tft_prev_active) {
             uint32_t syn_idz = (uint32_t)pid[tci] * spd + syn_idz_celtft;
-            for (uint32_t i = syn_idz; i < syn_idz + spd; i++) {
+            /* Out-of-layer ranges (only reachable through caller-written ids) are skipped. */
+            uint32_t n = ((uint64_t)syn_idz + spd <= L->n_syns) ? spd : 0;
+            for (uint32_t i = syn_idz; i < syn_idz + n; i++) {
                 int8_t s = str[i];
                 int32_t seed = (int32_t)(syn_idz + i);
                 if ((sfl[i] & SYN_PREV_ACTIVE_FLAG) == SYN_PREV_ACTIVE_FLAG)
@@ -663,9 +665,10 @@ int bmo_grow(const bm_area_plan* P, uint8_t* slab, uint64_t seed, uint32_t init_
             uint64_t key = splitmix64(seed ^ 0x67726F77ull) + (((uint64_t)P->area_id << 48) |
                            ((uint64_t)L->layer_id << 40) | ((uint64_t)t << 32));
             key = splitmix64(key);
-            uint64_t n_dens = (uint64_t)L->cells * T->dens_per_tft;
+            int64_t n_dens = (int64_t)L->cells * T->dens_per_tft;
             int64_t cols = (int64_t)L->v_size * L->u_size;
-            for (uint64_t d = 0; d < n_dens; d++) {
+#pragma omp parallel for schedule(static)
+            for (int64_t d = 0; d < n_dens; d++) {
                 uint64_t s0 = T->syn_idz + d * T->syns_per_den;
                 uint64_t wk = 0;
                 for (uint32_t j = 0; j < T->syns_per_den; j++) {

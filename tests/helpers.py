@@ -1,0 +1,125 @@
+"""Shared test helpers: schemes, seeded initial states, buffer diffs, digests."""
+import hashlib
+
+import numpy as np
+
+from bismit_b200 import _ffi as F, configs, map as M, plan_of
+
+NO_BUF = 2 ** 64 - 1
+
+SCHEMES = {
+    "testbed": lambda: configs.testbed_area(),
+    "mixed": lambda: configs.mixed_area(),
+    "area_64": lambda: configs.workload("area_64")[:2],
+    "area_48_deep": lambda: configs.workload("area_48_deep")[:2],
+}
+
+
+def settings_for(kind="default", plain=False):
+    s = M.CorticalAreaSettings().disable_regrowth()
+    if kind == "bypass_inhib":
+        s.bypass_inhib()
+    elif kind == "no_learning":
+        s.disable_learning()
+    elif kind == "no_pyrs":
+        s.disable_pyrs()
+    elif kind == "no_sscs":
+        s.disable_sscs()
+    elif kind == "zero_strength":
+        s.strengths_start_at_zero()
+    if plain:
+        s.plain_kernels()
+    return s
+
+
+def desc_of(scheme, settings=None):
+    lmaps, areas = SCHEMES[scheme]()
+    return M.area_desc("v1", lmaps, areas, settings or settings_for())
+
+
+def plan_for(scheme, settings=None, seed=7):
+    d = desc_of(scheme, settings)
+    return d, plan_of(d, seed)
+
+
+def buffers(plan):
+    """(label, offset, length) of every buffer in the slab."""
+    out = [("axon_states", int(plan.axon_off), int(plan.n_axons))]
+    for l in range(plan.n_layers):
+        L = plan.layers[l]
+        for k, n in enumerate(F.BUF_NAMES):
+            if L.buf_off[k] != NO_BUF:
+                out.append(("L%d.%s" % (l, n), int(L.buf_off[k]), int(L.buf_len[k])))
+    return out
+
+
+def diff_report(plan, a, b, limit=12):
+    lines = []
+    for name, off, n in buffers(plan):
+        x, y = a[off:off + n], b[off:off + n]
+        if not np.array_equal(x, y):
+            idx = np.nonzero(x != y)[0]
+            lines.append("%s: %d of %d differ (first %d: %s vs %s)" % (
+                name, idx.size, n, idx[0], x[idx[:4]].tolist(), y[idx[:4]].tolist()))
+    return "\n".join(lines[:limit])
+
+
+def digests(plan, slab):
+    return {name: hashlib.sha256(slab[off:off + n].tobytes()).hexdigest()[:32] for name, off, n in buffers(plan)}
+
+
+def scramble(plan, slab, seed):
+    """Overwrites the cycle state (not the synapse sources) with seeded values so
+    every branch of the kernels is reached: energies at and above the restless
+    and dark cutoffs, flags with unrelated bits set, strengths over the whole i8
+    range (including -128 and 127), prior synapse and tuft states."""
+    rng = np.random.default_rng([seed, 0x5C7A])
+    for l in range(plan.n_layers):
+        L = plan.layers[l]
+
+        def put(k, vals):
+            off = int(L.buf_off[k])
+            slab[off:off + len(vals)] = vals
+
+        n_syn, n_den, n_cel = int(L.n_syns), int(L.n_dens), int(L.cells)
+        st = rng.integers(0, 256, n_syn, dtype=np.uint8)
+        st[rng.random(n_syn) < 0.7] = 0
+        put(F.BUF["syn_states"], st)
+        put(F.BUF["syn_strengths"], rng.integers(-128, 128, n_syn).astype(np.int8).view(np.uint8))
+        put(F.BUF["syn_flag_sets"], rng.integers(0, 256, n_syn, dtype=np.uint8))
+        for k in ("den_activities", "den_energies", "den_states", "den_states_raw"):
+            put(F.BUF[k], rng.integers(0, 256, n_den, dtype=np.uint8))
+        en = rng.integers(0, 256, n_cel, dtype=np.uint8)
+        en[rng.random(n_cel) < 0.05] = 255
+        put(F.BUF["cel_energies"], en)
+        put(F.BUF["cel_activities"], rng.integers(0, 256, n_cel, dtype=np.uint8))
+        if L.kind == F.BM_LYR_PYRAMIDAL:
+            n_ct = int(L.n_celtfts)
+            for k in ("tft_prev_best_den_ids", "tft_best_den_ids"):
+                put(F.BUF[k], np.concatenate([rng.integers(0, int(L.tufts[t].dens_per_tft), n_cel, dtype=np.uint8)
+                                              for t in range(L.n_tufts)]))
+            for k in ("tft_prev_best_den_states_raw", "tft_prev_best_den_states", "tft_prev_states",
+                      "tft_best_den_states_raw", "tft_best_den_states", "tft_states"):
+                v = rng.integers(0, 256, n_ct, dtype=np.uint8)
+                v[rng.random(n_ct) < 0.3] = 0
+                put(F.BUF[k], v)
+            put(F.BUF["cel_flag_sets"], rng.integers(0, 256, n_cel, dtype=np.uint8))
+            put(F.BUF["cel_states"], rng.integers(0, 256, n_cel, dtype=np.uint8))
+    ax = rng.integers(0, 256, int(plan.n_axons), dtype=np.uint8)
+    ax[rng.random(int(plan.n_axons)) < 0.8] = 0
+    slab[int(plan.axon_off):int(plan.axon_off) + int(plan.n_axons)] = ax
+
+
+def initial_slab(plan, grow_seed, scramble_seed=None, init_flags=0):
+    import oracle
+    slab = np.zeros(int(plan.slab_bytes), np.uint8)
+    oracle.grow(plan, slab, grow_seed, init_flags)
+    if scramble_seed is not None:
+        scramble(plan, slab, scramble_seed)
+    return slab
+
+
+def frames_for(plan, n, seed, active=0.05):
+    if plan.n_inputs == 0:
+        return None
+    return configs.frames(n, int(plan.inputs[0].len), active, seed)

@@ -1,0 +1,110 @@
+"""GPU parity: the CUDA path against the CPU oracle, byte for byte.
+
+Every test drives the device through the C ABI (bismit_b200.cortex wraps
+include/bismit_b200.h) and compares the whole state slab (every axon,
+synapse, dendrite, tuft and cell buffer) with the oracle after every cycle,
+so a divergence is reported at the cycle and buffer where it first appears.
+"""
+import numpy as np
+import pytest
+
+import oracle
+from bismit_b200 import _ffi as F, cortex
+from helpers import desc_of, diff_report, frames_for, initial_slab, settings_for
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    c = cortex._Ctx(0)
+    yield c
+    c.close()
+
+
+def _area(ctx, scheme, settings, seed=7):
+    return cortex.CorticalArea(ctx, desc_of(scheme, settings), seed)
+
+
+@pytest.mark.parametrize("scheme", ["testbed", "mixed", "area_64", "area_48_deep"])
+@pytest.mark.parametrize("flags", [0, F.BM_INIT_STRENGTH_ZERO])
+def test_growth_matches_oracle(ctx, scheme, flags):
+    s = settings_for()
+    s.init_flags = flags
+    area = _area(ctx, scheme, s, seed=123)
+    dev = area.read_slab()
+    ref = np.zeros(area.slab_bytes, np.uint8)
+    oracle.grow(area.plan, ref, 123, flags)
+    assert np.array_equal(dev, ref), diff_report(area.plan, dev, ref)
+    area.close()
+
+
+def _run_parity(ctx, scheme, kind, plain, cycles, scramble=True, active=0.05):
+    s = settings_for(kind, plain=plain)
+    area = _area(ctx, scheme, s)
+    plan = area.plan
+    slab = initial_slab(plan, 7, scramble_seed=11 if scramble else None)
+    area.write_slab(slab)
+    area.set_cycle(0)
+    fr = frames_for(plan, cycles, 5, active)
+    ora = slab.copy()
+    for k in range(cycles):
+        if fr is not None:
+            area.write_input(fr[k])
+        area.cycle(1)
+        oracle.run(plan, ora, None if fr is None else fr[k:k + 1], 1, start_cycle=k)
+        dev = area.read_slab()
+        assert np.array_equal(dev, ora), "cycle %d:\n%s" % (k, diff_report(plan, dev, ora))
+    area.close()
+
+
+@pytest.mark.parametrize("plain", [True, False], ids=["plain", "fused"])
+@pytest.mark.parametrize("scheme", ["testbed", "mixed", "area_64", "area_48_deep"])
+def test_cycles_match_oracle(ctx, scheme, plain):
+    _run_parity(ctx, scheme, "default", plain, cycles=6)
+
+
+@pytest.mark.parametrize("plain", [True, False], ids=["plain", "fused"])
+@pytest.mark.parametrize("kind", ["bypass_inhib", "no_learning", "no_pyrs", "no_sscs"])
+def test_settings_match_oracle(ctx, kind, plain):
+    _run_parity(ctx, "mixed", kind, plain, cycles=3)
+
+
+@pytest.mark.parametrize("plain", [True, False], ids=["plain", "fused"])
+def test_unscrambled_long_run(ctx, plain):
+    """From the grown state (no scrambling) for 40 cycles: learning moves the
+    strengths and the pyramidal layer fires."""
+    _run_parity(ctx, "area_64", "zero_strength", plain, cycles=40, scramble=False, active=0.02)
+
+
+def test_cortex_builder_end_to_end():
+    """The builder surface: Cortex.builder(..).ca_settings(..).build(), input,
+    cycle, output, against the oracle on the same grown state."""
+    from bismit_b200 import Cortex, configs
+    lmaps, areas, act = configs.workload("area_64")
+    cx = Cortex.builder(lmaps, areas).ca_settings(configs.bench_settings()).seed(3).build()
+    a = cx.area("v1")
+    slab = a.read_slab()
+    fr = configs.frames(5, a.input_len(), act, 9)
+    for k in range(5):
+        a.write_input(fr[k])
+        cx.cycle()
+    out = a.read_output()
+    oracle.run(a.plan, slab, fr, 5, 0)
+    o = a.plan.outputs[0]
+    assert np.array_equal(out, slab[a.plan.axon_off + o.axn_idz: a.plan.axon_off + o.axn_idz + o.len])
+    assert np.array_equal(a.read_slab(), slab)
+    assert a.cycle_count() == 5
+    cx.close()
+
+
+def test_buffer_io_bounds(ctx):
+    area = _area(ctx, "area_64", settings_for())
+    with pytest.raises(F.BismitError):
+        area.read("syn_states", layer=0, offset=int(area.plan.layers[0].n_syns), length=1)
+    with pytest.raises(F.BismitError):
+        area.write_input(np.zeros(area.input_len() + 1, np.uint8))
+    x = np.arange(64, dtype=np.int8)
+    area.write("syn_strengths", x, layer=1, offset=100)
+    assert np.array_equal(area.read("syn_strengths", layer=1, offset=100, length=64), x)
+    area.close()

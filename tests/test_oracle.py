@@ -1,0 +1,83 @@
+"""CPU: the C restatement oracle pinned against bismit's own OpenCL kernels
+(cl/bismit.cl, cl/syns.cl, cl/control.cl compiled for the CPU by oracle/ref),
+plus the reference's own known-answer tests for this path."""
+import ctypes
+
+import numpy as np
+import pytest
+
+import oracle
+from bismit_b200 import _ffi as F
+from helpers import diff_report, frames_for, initial_slab, plan_for, settings_for
+
+
+@pytest.mark.parametrize("scheme", ["testbed", "mixed", "area_64", "area_48_deep"])
+@pytest.mark.parametrize("kind", ["default", "bypass_inhib", "no_learning", "zero_strength"])
+def test_port_matches_reference_kernels(ref_oracle, scheme, kind):
+    _, plan = plan_for(scheme, settings_for(kind))
+    slab = initial_slab(plan, 7, scramble_seed=11)
+    fr = frames_for(plan, 8, 5)
+    a, b = slab.copy(), slab.copy()
+    for k in range(8):
+        f = None if fr is None else fr[k:k + 1]
+        oracle.run(plan, a, f, 1, start_cycle=k, impl="port")
+        oracle.run(plan, b, f, 1, start_cycle=k, impl="ref")
+        assert np.array_equal(a, b), "cycle %d:\n%s" % (k, diff_report(plan, a, b))
+
+
+def test_port_matches_reference_kernels_long(ref_oracle):
+    """80 cycles from the grown state: learning accumulates in both."""
+    _, plan = plan_for("area_64", settings_for("zero_strength"))
+    slab = initial_slab(plan, 3, init_flags=F.BM_INIT_STRENGTH_ZERO)
+    fr = frames_for(plan, 80, 2, active=0.02)
+    a, b = slab.copy(), slab.copy()
+    oracle.run(plan, a, fr, 80, impl="port")
+    oracle.run(plan, b, fr, 80, impl="ref")
+    assert np.array_equal(a, b), diff_report(plan, a, b)
+    L0 = plan.layers[0]
+    s = a[L0.buf_off[F.BUF["syn_strengths"]]:][:L0.n_syns].view(np.int8)
+    assert (s != 0).mean() > 0.01, "spiny stellate learning changed no strength"
+
+
+def test_axon_index_scalar_equals_vec4(ref_oracle):
+    """src/tests/kernels.rs:21-91: test_axn_idxs_scl and test_axn_idxs_vec4 give
+    identical axon indices for shuffled offsets in +-SYNAPSE_REACH (8)."""
+    _, plan = plan_for("testbed")
+    rng = np.random.default_rng(0)
+    depth, v, u = int(plan.n_slices), 24, 24
+    n = depth * v * u
+    vo = rng.permutation(np.resize(np.arange(-8, 9, dtype=np.int8), n))
+    uo = rng.permutation(np.resize(np.arange(-8, 9, dtype=np.int8), n))
+    scl, vec = oracle.ref_axn_idxs(plan, depth, v, u, vo, uo)
+    assert np.array_equal(scl, vec)
+    # The restatement gives the same indices.
+    port = oracle.load_port()
+    safe = ctypes.c_int()
+    got = np.zeros(n, np.uint32)
+    for i in range(n):
+        s, vv, uu = i // (v * u), (i // u) % v, i % u
+        got[i] = port.bmo_axn_idx_scl(ctypes.byref(plan), s, vv, int(vo[i]), uu, int(uo[i]), ctypes.byref(safe))
+    assert np.array_equal(got, scl)
+
+
+@pytest.mark.parametrize("r", [0, 1, 2, 3, 4, 6, 8, 16])
+def test_hex_offsets_count_and_symmetry(r):
+    """gen_syn_offs (src/map/syn_src.rs:47-149) at scale 16 is the hex disk of
+    radius r: 3r(r+1)+1 tiles, symmetric, max(|v|,|u|,|v+u|) <= r."""
+    v, u = oracle.gen_syn_offs(r, 16, 16)
+    assert len(v) == 3 * r * (r + 1) + 1
+    pts = set(zip(v.tolist(), u.tolist()))
+    assert len(pts) == len(v)
+    assert all(max(abs(a), abs(b), abs(a + b)) <= r for a, b in pts)
+    assert all((-a, -b) in pts for a, b in pts)
+
+
+def test_rnd_stream_is_deterministic_and_keyed():
+    a = [oracle.rnd(5, 1, 2, F.BM_RND_DEN_CYCLE, 0, c) for c in range(100)]
+    b = [oracle.rnd(5, 1, 2, F.BM_RND_DEN_CYCLE, 0, c) for c in range(100)]
+    assert a == b
+    assert len(set(a)) == 100
+    assert oracle.rnd(5, 1, 2, F.BM_RND_DEN_CYCLE, 1, 0) != a[0]
+    assert oracle.rnd(6, 1, 2, F.BM_RND_DEN_CYCLE, 0, 0) != a[0]
+    lib = F.lib()
+    assert [lib.bm_rnd(5, 1, 2, F.BM_RND_DEN_CYCLE, 0, c) for c in range(100)] == a
