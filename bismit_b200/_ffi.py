@@ -193,6 +193,8 @@ def lib():
         "bm_area_get_cycle": (C.c_int, [vp, P(u64)]),
         "bm_area_set_cycle": (C.c_int, [vp, u64]),
         "bm_area_slab_ptr": (C.c_int, [vp, P(vp)]),
+        "bm_area_sources_changed": (C.c_int, [vp, u32]),
+        "bm_area_device_errors": (C.c_int, [vp, P(u32)]),
         "bm_area_set_profiling": (C.c_int, [vp, C.c_int]),
         "bm_area_get_profile": (C.c_int, [vp, u32, P(C.c_char_p), P(u64), P(C.c_double), P(u32)]),
         "bm_area_reset_profile": (C.c_int, [vp]),

@@ -85,6 +85,7 @@ struct bm_area_s {
     DevLayer dl[BM_MAX_LAYERS];
     uint64_t inhib_key[BM_MAX_LAYERS][BM_MAX_CTRL];
     uint64_t host_cycle = 0;
+    bool verify_pending[BM_MAX_LAYERS] = {};   // sources or flags written since the last check
     uint32_t exec_path = BM_PATH_FUSED;
     FusedArea fused;
     bool profiling = false;
@@ -188,7 +189,7 @@ void enqueue_tufts(bm_area_s* A, uint32_t i) {
         return;
     }
     for (uint32_t t = 0; t < L.n_tufts; t++) {
-        if (A->fused.tuft_ok[i][t]) {
+        if (A->fused.t[i][t].ok) {
             A->run(K_FUSED_TUFT, [&] { launch_fused_tuft(A->fused, A->axns(), A->slices, D, i, t, A->ctl, s); });
         } else {
             A->run(K_SYN_FLAGS, [&] { launch_set_syn_flags_tuft(D, t, s); });
@@ -229,6 +230,11 @@ void enqueue_layer_learn(bm_area_s* A, uint32_t i) {
 void enqueue_cycle(bm_area_s* A) {
     const bm_area_plan& P = A->plan;
     A->launches = 0;
+    for (uint32_t i = 0; i < P.n_layers; i++)
+        if (A->verify_pending[i]) {
+            launch_verify_tufts(A->fused, A->dl[i], i, A->ctl, A->stream());
+            A->verify_pending[i] = false;
+        }
     if (!(P.settings & BM_SET_DISABLE_SSCS)) {
         for (uint32_t k = 0; k < P.n_cycle_order; k++)
             if (P.layers[P.cycle_order[k]].tags & BM_TAG_SPATIAL) enqueue_layer_cycle(A, P.cycle_order[k]);
@@ -457,6 +463,7 @@ int bm_area_create(bm_ctx ctx, const bm_area_desc* desc, uint64_t seed, bm_area*
     if (d_off) cudaFree(d_off);
     if (e != cudaSuccess) { free_area(A); return cuda_err(e, "synapse growth"); }
     rc = prepare_fused(A->fused, A->plan, &err);
+    for (uint32_t i = 0; i < A->plan.n_layers; i++) A->verify_pending[i] = true;
     if (rc != BM_OK) { free_area(A); return set_err(rc, "%s", err.c_str()); }
     *out = A;
     return BM_OK;
@@ -563,6 +570,9 @@ int bm_area_write(bm_area area, uint32_t buf_kind, uint32_t layer, uint64_t offs
     DevGuard g(area->ctx->device);
     if (len) CU(cudaMemcpyAsync(area->slab + off, src, len, cudaMemcpyHostToDevice, area->stream()));
     CU(cudaStreamSynchronize(area->stream()));
+    if (buf_kind == BM_BUF_SYN_SRC_SLC_IDS || buf_kind == BM_BUF_SYN_SRC_COL_V_OFFS ||
+        buf_kind == BM_BUF_SYN_SRC_COL_U_OFFS || buf_kind == BM_BUF_SYN_FLAG_SETS)
+        area->verify_pending[layer] = true;
     return BM_OK;
 }
 
@@ -582,6 +592,24 @@ int bm_area_write_slab(bm_area area, const void* src, uint64_t len) {
     DevGuard g(area->ctx->device);
     CU(cudaMemcpyAsync(area->slab, src, len, cudaMemcpyHostToDevice, area->stream()));
     CU(cudaStreamSynchronize(area->stream()));
+    for (uint32_t i = 0; i < area->plan.n_layers; i++) area->verify_pending[i] = true;
+    return BM_OK;
+}
+
+int bm_area_sources_changed(bm_area area, uint32_t layer) {
+    if (!area || layer >= area->plan.n_layers) return set_err(BM_ERR_INVALID, "bad area or layer");
+    area->verify_pending[layer] = true;
+    return BM_OK;
+}
+
+int bm_area_device_errors(bm_area area, uint32_t* bits) {
+    if (!area || !bits) return set_err(BM_ERR_INVALID, "null argument");
+    DevGuard g(area->ctx->device);
+    unsigned int e = 0;
+    CU(cudaMemcpyAsync(&e, &area->ctl->error, sizeof e, cudaMemcpyDeviceToHost, area->stream()));
+    CU(cudaStreamSynchronize(area->stream()));
+    *bits = e;
+    if (e) return set_err(BM_ERR_TIMEOUT, "device-side wait timed out (error bits 0x%x)", e);
     return BM_OK;
 }
 

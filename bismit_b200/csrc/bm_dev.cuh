@@ -44,10 +44,18 @@ struct DevLayer {
 };
 
 // Per-area control block in device memory.
+// Device-side error bits (AreaCtl::error).
+constexpr unsigned int kErrWaitTimeout = 1u;   // a bounded mbarrier wait gave up
+
+// Tuft status bits (AreaCtl::tuft_status), written by the source verifier.
+constexpr unsigned int kTuftSrcOutsideTile = 1u;   // some source is not served by the staged tile
+constexpr unsigned int kTuftFlagsForeign = 2u;     // some flag byte has bits other than SYN_PREV_ACTIVE
+
 struct AreaCtl {
     unsigned long long cycle;       // cycle number of the cycle in flight
-    unsigned int error;             // sticky device-side error bits
+    unsigned int error;             // sticky device-side error bits (kErr*)
     unsigned int pad;
+    unsigned int tuft_status[BM_MAX_LAYERS * BM_MAX_TUFTS];
 };
 
 __host__ __device__ inline uint64_t splitmix64(uint64_t x) {

@@ -10,19 +10,33 @@
 // kernel; the flags of a tuft depend only on that tuft's states, which only its
 // own synapse kernel writes, so doing both per tuft is equivalent.
 //
-// Work layout: a warp takes one 512-byte chunk of the tuft's synapse range per
-// step (32 lanes x 16 bytes). Each SoA array (source slice, v/u offsets,
-// strength, state, flags) is read with one coalesced 16-byte load per lane;
-// new states and flags are written the same way. A lane's 16 synapses belong
-// to one dendrite (syns_per_den is a power of two >= 16), so dendrite sums
-// reduce across syns_per_den/16 lanes with shuffles, and the tuft argmax across
-// the cell's lanes (or across chunks when a cell spans several chunks).
+// Main form (k_fused_tuft_tma), for tufts whose source slices share one
+// geometry: persistent CTAs of 8 consumer warps and 1 producer warp walk tiles
+// of cells (part of a row, or whole rows, of one layer slice).
+//  * Per tile the consumers stage the axon footprint the tile's synapses can
+//    reach -- the tile's scaled extent plus the pool's largest offsets, for
+//    every source slice -- in shared memory as already-fired synapse states
+//    (syn_fire(axon), 0 outside the slice).
+//  * The producer warp streams the tile's synapse arrays into a ring of
+//    shared-memory stages with TMA bulk copies (cp.async.bulk) that complete
+//    on mbarriers, running up to NST stages ahead of the consumers.
+//  * A consumer warp takes 512 synapses of a stage (32 lanes x 16), computes
+//    new states and flags, writes them with 16-byte stores, reduces dendrite
+//    sums across syns_per_den/16 lanes with shuffles and the tuft argmax across
+//    the cell's lanes (redux.sync over the warp when a cell fills it).
 //
-// The axon gather uses per-lane slice records (scaled cell coordinates and the
-// row-major base index) precomputed once per chunk for the tuft's contiguous
-// source slices; any other slice id (e.g. written by the caller) takes the
-// general per-synapse path, so every i8 offset and u8 slice id is handled
-// exactly as in axn_state_3d_safe (cl/bismit.cl:397-418).
+// Gather index: each synapse's (source slice, v offset, u offset) is compiled
+// once into a 16-bit offset into the staged footprint, (slc - slc0) * TSZ +
+// v_ofs * TW + u_ofs, kept beside the synapse arrays (the canonical source
+// arrays are unchanged and remain what readback returns). The compile pass
+// runs at build and again whenever the caller writes sources or flags. A
+// source it cannot express (slice outside the pool, offset beyond the pool's
+// reach -- only possible through caller writes) marks the tuft, and the
+// kernel then streams the original arrays and indexes every synapse as
+// axn_state_3d_safe (cl/bismit.cl:397-418) does.
+//
+// Every mbarrier wait is bounded; on a timeout the kernel records
+// kErrWaitTimeout, lets its own copies in flight land and returns.
 #include "bm_fused.h"
 
 #include <algorithm>
@@ -32,19 +46,22 @@ namespace bm {
 
 namespace {
 
-constexpr int kWarps = 8;            // warps per CTA
-constexpr int kMaxRecs = 8;          // contiguous source slices served from records
+constexpr int kWarps = 8;                    // consumer warps per CTA (tiled form)
+constexpr int kThreads = (kWarps + 1) * 32;  // plus one producer warp
+constexpr int kMaxRecs = 8;                  // contiguous source slices served by the fast gathers
+constexpr uint32_t kWaitLimit = 1u << 22;
 
 struct FusedTuftArgs {
     const uint8_t* axns;
     const SliceRec* slices;
-    const AreaCtl* ctl;
+    AreaCtl* ctl;
     const uint8_t* slc;     // tuft-relative synapse arrays
     const int8_t* vofs;
     const int8_t* uofs;
     const int8_t* str;
     uint8_t* st;
     uint8_t* fl;
+    const int16_t* gidx;    // compiled gather offsets (tiled form)
     uint8_t* den_act;       // tuft-relative dendrite arrays
     uint8_t* den_raw;
     uint8_t* den_st;
@@ -57,59 +74,216 @@ struct FusedTuftArgs {
     uint8_t* t_bst;
     uint8_t* t_st;
     uint64_t n_syn;         // synapses in the tuft
-    uint64_t n_units;       // chunks (S <= 512) or cells (S > 512)
     uint32_t den_idz;       // first dendrite (layer index) for the activity seed
     uint32_t thresh;
-    uint32_t cols, u_size;
-    uint32_t S_l2, spd_l2, lpd_l2, lpc_l2;   // log2 of syns/cell-tuft, syns/den, lanes/den, lanes/cell (<= 5)
+    uint32_t cols, u_size, v_size;
+    uint32_t S_l2, spd_l2, lpd_l2, lpc_l2;   // log2: syns/cell-tuft, syns/den, lanes/den, lanes/cell (<= 5)
     uint32_t chunks_per_unit;
     uint32_t mad_l2;
-    uint32_t slc0, nrec;    // records cover slice ids slc0 .. slc0 + nrec - 1
+    uint32_t slc0, nrec;    // fast gathers serve slice ids slc0 .. slc0 + nrec - 1
     uint32_t vec4;          // bismit's vec4 synapse kernel semantics (spt % 4 == 0)
     uint64_t rnd_key;
+    uint32_t status_idx;    // index into AreaCtl::tuft_status
+    // Global-record form: units are chunks (S <= 512) or cells (S > 512).
+    uint64_t n_units;
+    // Tiled form.
+    uint32_t tile_w, tile_h, tiles_u, tiles_v, n_tiles;
+    uint32_t usz_magic;                 // ceil(2^32 / u_size) for multi-row tiles
+    int32_t rv, ru;                     // largest |v|, |u| offset served from the footprint
+    uint32_t fw, frows, fsz;            // footprint width, rows and bytes per source slice
+    uint32_t src_vs, src_us, src_vsz, src_usz;   // geometry shared by the recorded slices
+    uint32_t src_idz[kMaxRecs];
+    uint32_t nst;                       // pipeline stages
+    uint32_t stage_bytes;               // bytes per 1-byte array per stage
+    uint32_t halo_off;                  // byte offset of the footprint in dynamic smem
+    uint32_t unit_l2;                   // log2 of the bytes of one unit (chunks_per_unit * 512)
 };
 
 struct Rec {
-    int32_t base;     // idz + vsc * u_size + usc (row-major index of the cell's scaled position)
+    int32_t base;     // idz + vsc * u_size + usc
     int32_t vsc, usc; // scaled position plus mid
     uint32_t dims;    // v_size | u_size << 16
 };
 
+// ---------------------------------------------------------------- PTX ----
+__device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void fence_mbar_init() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t tx) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(tx) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_addr(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Bounded wait; false after kWaitLimit polls.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+    for (uint32_t i = 0; i < kWaitLimit; i++)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+// 1-D bulk copy global -> shared completing on `bar` (16-byte aligned, size % 16 == 0).
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(smem_addr(dst)),
+        "l"(src), "r"(bytes), "r"(smem_addr(bar))
+        : "memory");
+}
+// Barrier among the consumer warps only (the producer warp runs free).
+__device__ __forceinline__ void consumers_sync() { asm volatile("bar.sync 1, %0;" ::"n"(kWarps * 32) : "memory"); }
+
+// ------------------------------------------------------------ helpers ----
 __device__ __forceinline__ uint32_t nz_bits(uint32_t x) {
     // 0x80 in every byte of x that is non-zero.
     return (((x & 0x7F7F7F7Fu) + 0x7F7F7F7Fu) | x) & 0x80808080u;
 }
 
-__device__ __forceinline__ uint8_t gather_general(const FusedTuftArgs& A, uint8_t slc, uint32_t v, uint32_t u,
+__device__ __forceinline__ uint8_t gather_general(const FusedTuftArgs& A, uint32_t slc, uint32_t v, uint32_t u,
                                                   int vo, int uo) {
     bool safe;
     uint32_t ai = axn_idx(A.slices[slc], v, vo, u, uo, A.vec4 != 0, safe);
-    return safe ? __ldg(A.axns + ai) : (uint8_t)0;
+    return syn_fire(safe ? __ldg(A.axns + ai) : (uint8_t)0);
 }
 
+// Loads issued at the start of a chunk so their latency overlaps the gathers:
+// the activity of the lane's dendrite (dendrite-lead lanes) and, at the first
+// chunk of a cell, the cell-tuft's current best/state bytes that the tuft
+// cycle copies to the prev arrays (cell-lead lanes).
+__device__ __forceinline__ uint32_t prefetch_act(const FusedTuftArgs& A, uint64_t off, bool on, int lane) {
+    const uint32_t lpd = 1u << A.lpd_l2;
+    return (on && (lane & (lpd - 1)) == 0) ? (uint32_t)A.den_act[off >> A.spd_l2] : 0u;
+}
+template <bool TUFT>
+__device__ __forceinline__ uint32_t prefetch_tuft(const FusedTuftArgs& A, uint64_t off, bool on, int lane) {
+    if (!TUFT) return 0u;
+    const uint32_t lpc = 1u << A.lpc_l2;
+    if (!on || (lane & (lpc - 1)) != 0) return 0u;
+    const uint32_t c = (uint32_t)(off >> A.S_l2);
+    return (uint32_t)A.t_bid[c] | ((uint32_t)A.t_braw[c] << 8) | ((uint32_t)A.t_bst[c] << 16) |
+           ((uint32_t)A.t_st[c] << 24);
+}
+
+// Everything after the new states of 16 synapses are known, for one 512-byte
+// chunk: flags, stores, dendrite reductions and the chunk's share of the tuft
+// reduction. `last` marks the final chunk of a cell.
+template <bool TUFT>
+__device__ __forceinline__ void finish_chunk(const FusedTuftArgs& A, const uint4& str4, const uint4& st4,
+                                             const uint4& fl4, const uint4& nst4, bool flags_clean, uint64_t off,
+                                             bool on, int lane, int32_t rnd, bool last, uint32_t act0,
+                                             uint32_t tuft_cur, uint32_t& t_key, uint32_t& t_best, uint32_t& t_sum) {
+    const uint32_t lpd = 1u << A.lpd_l2;
+    const uint32_t lpc = 1u << A.lpc_l2;
+    uint32_t sum = 0, raw = 0;
+    if (on) {
+        const uint32_t* strw = (const uint32_t*)&str4;
+        const uint32_t* stw = (const uint32_t*)&st4;
+        const uint32_t* flw = (const uint32_t*)&fl4;
+        const uint32_t* nstw = (const uint32_t*)&nst4;
+        uint4 nfl4;
+        uint32_t* nflw = (uint32_t*)&nfl4;
+#pragma unroll
+        for (int w = 0; w < 4; w++) {
+            const uint32_t keep = flags_clean ? 0u : (flw[w] & 0xEFEFEFEFu);
+            nflw[w] = keep | (nz_bits(stw[w]) >> 3);
+            const uint32_t neg = (strw[w] >> 7) & 0x01010101u;
+            raw = __dp4a(nstw[w], 0x01010101u, raw);
+            sum = __dp4a(nstw[w] & ~(neg * 0xFFu), 0x01010101u, sum);
+        }
+        *(uint4*)(A.st + off) = nst4;
+        *(uint4*)(A.fl + off) = nfl4;
+    }
+    for (uint32_t m = 1; m < lpd; m <<= 1) {
+        sum += __shfl_xor_sync(0xFFFFFFFFu, sum, m);
+        raw += __shfl_xor_sync(0xFFFFFFFFu, raw, m);
+    }
+    uint32_t d_raw = 0, d_st = 0;
+    const bool lead = on && (lane & (lpd - 1)) == 0;
+    const uint64_t den = off >> A.spd_l2;   // dendrite id within the tuft
+    if (lead) {
+        const int active = sum > A.thresh;
+        const uint32_t s2 = active ? sum : 0u;
+        const uint32_t di = (uint32_t)den + A.den_idz;
+        const uint32_t seed = (raw + A.thresh) | di;
+        A.den_act[den] = update_activity((uint8_t)act0, active, rnd, (int32_t)seed, kDendriteActivityDecay);
+        d_raw = min(raw >> 4, 255u);
+        d_st = min(s2 >> 4, 255u);
+        A.den_raw[den] = (uint8_t)d_raw;
+        A.den_st[den] = (uint8_t)d_st;
+    }
+    if (TUFT) {
+        // Argmax of the raw state with the first (lowest) dendrite winning
+        // ties: maximise (raw << 16 | (0xFFFF - id)).
+        const uint32_t den_in_cell = (uint32_t)(den & ((1u << (A.S_l2 - A.spd_l2)) - 1));
+        uint32_t key = lead ? ((d_raw << 16) | (0xFFFFu - den_in_cell)) : 0u;
+        uint32_t best = d_st, tot = d_st;
+        if (lpc == 32) {
+            key = __reduce_max_sync(0xFFFFFFFFu, key);
+            best = __reduce_max_sync(0xFFFFFFFFu, best);
+            tot = __reduce_add_sync(0xFFFFFFFFu, tot);
+        } else {
+            for (uint32_t m = lpd; m < lpc; m <<= 1) {
+                key = max(key, __shfl_xor_sync(0xFFFFFFFFu, key, m));
+                best = max(best, __shfl_xor_sync(0xFFFFFFFFu, best, m));
+                tot += __shfl_xor_sync(0xFFFFFFFFu, tot, m);
+            }
+        }
+        t_key = max(t_key, key);
+        t_best = max(t_best, best);
+        t_sum += tot;
+        if (last && on && (lane & (lpc - 1)) == 0) {
+            const uint32_t c = (uint32_t)(off >> A.S_l2);
+            const uint32_t best_raw = t_key >> 16;
+            const uint32_t best_id = best_raw ? (0xFFFFu - (t_key & 0xFFFFu)) : 0u;
+            const bool is_max = t_sum >= (1u << (A.mad_l2 + 8));
+            const uint8_t tst = is_max ? (uint8_t)255 : (uint8_t)(t_sum >> A.mad_l2);
+            A.t_pid[c] = (uint8_t)tuft_cur;
+            A.t_praw[c] = (uint8_t)(tuft_cur >> 8);
+            A.t_pst[c] = (uint8_t)(tuft_cur >> 16);
+            A.t_ptft[c] = (uint8_t)(tuft_cur >> 24);
+            A.t_bid[c] = (uint8_t)best_id;
+            A.t_braw[c] = (uint8_t)best_raw;
+            A.t_bst[c] = (uint8_t)t_best;
+            A.t_st[c] = tst;
+        }
+    }
+}
+
+// ------------------------------------------------ global-record form ----
+// For tufts whose source slices do not share one geometry: warps stride over
+// units of the whole tuft and gather through per-lane slice records.
 template <bool TUFT>
 __global__ void __launch_bounds__(kWarps * 32) k_fused_tuft(FusedTuftArgs A) {
-    __shared__ Rec recs[kWarps][kMaxRecs][32];
+    __shared__ Rec recs[kWarps][kMaxRecs * 32];
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
     const uint64_t gwarp = (uint64_t)blockIdx.x * kWarps + wib;
     const uint64_t nwarps = (uint64_t)gridDim.x * kWarps;
     const int32_t rnd = rnd_at(A.rnd_key, A.ctl->cycle);
-    const uint32_t lpd = 1u << A.lpd_l2;
-    const uint32_t lpc = 1u << A.lpc_l2;
-
+    const bool flags_clean = (A.ctl->tuft_status[A.status_idx] & kTuftFlagsForeign) == 0;
     for (uint64_t unit = gwarp; unit < A.n_units; unit += nwarps) {
-        // Tuft accumulators across the chunks of one cell (S > 512).
-        uint32_t t_key = 0, t_best = 0, t_sum = 0;
+        uint32_t t_key = 0, t_best = 0, t_sum = 0, tuft_cur = 0;
         for (uint32_t ch = 0; ch < A.chunks_per_unit; ch++) {
-            const uint64_t chunk = unit * A.chunks_per_unit + ch;
-            const uint64_t off = chunk * 512 + (uint64_t)lane * 16;
+            const uint64_t off = (unit * A.chunks_per_unit + ch) * 512 + (uint64_t)lane * 16;
             const bool on = off < A.n_syn;
             const uint32_t cell = (uint32_t)(off >> A.S_l2);
             const uint32_t rem = cell % A.cols;
             const uint32_t v = rem / A.u_size, u = rem % A.u_size;
-
-            // Per-lane slice records for this cell.
+            __syncwarp();
             for (uint32_t k = 0; k < A.nrec; k++) {
                 SliceRec s = A.slices[A.slc0 + k];
                 Rec r;
@@ -117,30 +291,25 @@ __global__ void __launch_bounds__(kWarps * 32) k_fused_tuft(FusedTuftArgs A) {
                 r.usc = (int32_t)((u * ((s.z >> 8) & 0xFF)) >> kSlcSclCoeffL2);
                 r.dims = s.y;
                 r.base = (int32_t)s.x + r.vsc * (int32_t)(s.y >> 16) + r.usc;
-                recs[wib][k][lane] = r;
+                recs[wib][k * 32 + lane] = r;
             }
             __syncwarp();
-
-            uint32_t sum = 0, raw = 0;
+            const uint32_t act0 = prefetch_act(A, off, on, lane);
+            if (ch == 0) tuft_cur = prefetch_tuft<TUFT>(A, off, on, lane);
+            uint4 str4{}, st4{}, fl4{}, nst4{};
             if (on) {
                 const uint4 slc4 = __ldg((const uint4*)(A.slc + off));
                 const uint4 vo4 = __ldg((const uint4*)(A.vofs + off));
                 const uint4 uo4 = __ldg((const uint4*)(A.uofs + off));
-                const uint4 str4 = __ldg((const uint4*)(A.str + off));
-                const uint4 st4 = *(const uint4*)(A.st + off);
-                const uint4 fl4 = *(const uint4*)(A.fl + off);
+                str4 = __ldg((const uint4*)(A.str + off));
+                st4 = *(const uint4*)(A.st + off);
+                fl4 = *(const uint4*)(A.fl + off);
                 const uint32_t* sw = (const uint32_t*)&slc4;
                 const uint32_t* vw = (const uint32_t*)&vo4;
                 const uint32_t* uw = (const uint32_t*)&uo4;
-                const uint32_t* strw = (const uint32_t*)&str4;
-                const uint32_t* stw = (const uint32_t*)&st4;
-                const uint32_t* flw = (const uint32_t*)&fl4;
-                uint4 nst4, nfl4;
-                uint32_t* nstw = (uint32_t*)&nst4;
-                uint32_t* nflw = (uint32_t*)&nfl4;
+                uint32_t* ow = (uint32_t*)&nst4;
 #pragma unroll
                 for (int w = 0; w < 4; w++) {
-                    nflw[w] = (flw[w] & 0xEFEFEFEFu) | (nz_bits(stw[w]) >> 3);
                     uint32_t out = 0;
 #pragma unroll
                     for (int b = 0; b < 4; b++) {
@@ -148,78 +317,341 @@ __global__ void __launch_bounds__(kWarps * 32) k_fused_tuft(FusedTuftArgs A) {
                         const int vo = (int)(int8_t)(vw[w] >> (8 * b));
                         const int uo = (int)(int8_t)(uw[w] >> (8 * b));
                         const uint32_t k = slc - A.slc0;
-                        uint8_t a;
+                        uint32_t a;
                         if (k < A.nrec) {
-                            const Rec r = recs[wib][k][lane];
+                            const Rec r = recs[wib][k * 32 + lane];
                             const int vt = r.vsc + vo, ut = r.usc + uo;
                             const bool safe = ((uint32_t)vt < (r.dims & 0xFFFF)) & ((uint32_t)ut < (r.dims >> 16));
-                            a = safe ? __ldg(A.axns + (uint32_t)(r.base + vo * (int32_t)(r.dims >> 16) + uo)) : (uint8_t)0;
+                            a = syn_fire(safe ? __ldg(A.axns + (uint32_t)(r.base + vo * (int32_t)(r.dims >> 16) + uo))
+                                              : (uint8_t)0);
                         } else {
-                            a = gather_general(A, (uint8_t)slc, v, u, vo, uo);
+                            a = gather_general(A, slc, v, u, vo, uo);
                         }
-                        out |= (uint32_t)syn_fire(a) << (8 * b);
+                        out |= a << (8 * b);
                     }
-                    nstw[w] = out;
-                    const uint32_t neg = (strw[w] >> 7) & 0x01010101u;
-                    raw = __dp4a(out, 0x01010101u, raw);
-                    sum = __dp4a(out & ~(neg * 0xFFu), 0x01010101u, sum);
+                    ow[w] = out;
                 }
-                *(uint4*)(A.st + off) = nst4;
-                *(uint4*)(A.fl + off) = nfl4;
             }
-            __syncwarp();
+            finish_chunk<TUFT>(A, str4, st4, fl4, nst4, flags_clean, off, on, lane, rnd,
+                               ch + 1 == A.chunks_per_unit, act0, tuft_cur, t_key, t_best, t_sum);
+        }
+    }
+}
 
-            // Dendrite sums across the dendrite's lanes.
-            for (uint32_t m = 1; m < lpd; m <<= 1) {
-                sum += __shfl_xor_sync(0xFFFFFFFFu, sum, m);
-                raw += __shfl_xor_sync(0xFFFFFFFFu, raw, m);
+// ------------------------------------------------------ tiled TMA form ----
+struct TileGeo {
+    uint32_t v0, u0, h, w;
+    int32_t vlo, ulo;
+    uint64_t cell0, syn0, syn_end;
+};
+
+__device__ __forceinline__ TileGeo tile_geo(const FusedTuftArgs& A, uint32_t t) {
+    TileGeo g;
+    const uint32_t per_slice = A.tiles_v * A.tiles_u;
+    const uint32_t s_lyr = t / per_slice;
+    const uint32_t tr = t - s_lyr * per_slice;
+    g.v0 = (tr / A.tiles_u) * A.tile_h;
+    g.u0 = (tr % A.tiles_u) * A.tile_w;
+    g.h = min(A.tile_h, A.v_size - g.v0);
+    g.w = min(A.tile_w, A.u_size - g.u0);
+    g.vlo = (int32_t)((g.v0 * A.src_vs) >> kSlcSclCoeffL2) - A.rv;
+    g.ulo = (int32_t)((g.u0 * A.src_us) >> kSlcSclCoeffL2) - A.ru;
+    g.cell0 = (uint64_t)s_lyr * A.cols + (uint64_t)g.v0 * A.u_size + g.u0;
+    g.syn0 = g.cell0 << A.S_l2;
+    g.syn_end = (g.cell0 + (uint64_t)g.h * g.w) << A.S_l2;
+    return g;
+}
+
+// The position of the 16 synapses at tuft offset `off` in the footprint of
+// tile G: (cell's scaled row - vlo) * fw + (cell's scaled column - ulo).
+__device__ __forceinline__ int32_t footprint_base(const FusedTuftArgs& A, const TileGeo& G, uint64_t off,
+                                                  uint32_t& v, uint32_t& u) {
+    const uint32_t local = (uint32_t)((off >> A.S_l2) - G.cell0);
+    if (A.tile_h == 1) {
+        v = G.v0;
+        u = G.u0 + local;
+    } else {
+        const uint32_t q = __umulhi(local, A.usz_magic);
+        v = G.v0 + q;
+        u = local - q * A.u_size;
+    }
+    return ((int32_t)((v * A.src_vs) >> kSlcSclCoeffL2) - G.vlo) * (int32_t)A.fw +
+           ((int32_t)((u * A.src_us) >> kSlcSclCoeffL2) - G.ulo);
+}
+
+// Stages the tile's footprint: element e (row-major over slice, row, column)
+// holds syn_fire(axon) at (vlo + row, ulo + column) of the slice, or 0 outside
+// it. Each consumer thread takes elements tid, tid + 256, ...; the loads of a
+// batch of 16 are all issued before any store so their latencies overlap.
+__device__ __forceinline__ void build_footprint(const FusedTuftArgs& A, const TileGeo& G, uint8_t* halo, uint32_t tid) {
+    const uint32_t total = A.nrec * A.fsz;
+    constexpr uint32_t kStep = kWarps * 32;
+    // Decompose the thread's first element once; later elements advance by kStep.
+    uint32_t k = tid / A.fsz, rem = tid - k * A.fsz;
+    uint32_t r = rem / A.fw, c = rem - r * A.fw;
+    for (uint32_t e0 = tid; e0 < total; e0 += 16 * kStep) {
+        uint8_t vals[16];
+#pragma unroll
+        for (int i = 0; i < 16; i++) {
+            const uint32_t e = e0 + (uint32_t)i * kStep;
+            uint8_t a = 0;
+            if (e < total) {
+                const int32_t vr = G.vlo + (int32_t)r, uc = G.ulo + (int32_t)c;
+                if (((uint32_t)vr < A.src_vsz) & ((uint32_t)uc < A.src_usz))
+                    a = __ldg(A.axns + A.src_idz[k] + (uint32_t)vr * A.src_usz + (uint32_t)uc);
             }
-            uint32_t d_raw = 0, d_st = 0;
-            const bool lead = on && (lane & (lpd - 1)) == 0;
-            const uint64_t den = off >> A.spd_l2;   // dendrite id within the tuft
-            if (lead) {
-                const int active = sum > A.thresh;
-                const uint32_t s2 = active ? sum : 0u;
-                const uint32_t di = (uint32_t)den + A.den_idz;
-                const uint32_t seed = (raw + A.thresh) | di;
-                A.den_act[den] = update_activity(A.den_act[den], active, rnd, (int32_t)seed, kDendriteActivityDecay);
-                d_raw = min(raw >> 4, 255u);
-                d_st = min(s2 >> 4, 255u);
-                A.den_raw[den] = (uint8_t)d_raw;
-                A.den_st[den] = (uint8_t)d_st;
+            vals[i] = a;
+            c += kStep;
+            while (c >= A.fw) {
+                c -= A.fw;
+                if (++r == A.frows) { r = 0; k++; }
             }
-            if (TUFT) {
-                // Argmax of the raw state with the first (lowest) dendrite winning
-                // ties: maximise (raw << 16 | (0xFFFF - id)).
-                const uint32_t den_in_cell = (uint32_t)(den & ((1u << (A.S_l2 - A.spd_l2)) - 1));
-                uint32_t key = lead ? ((d_raw << 16) | (0xFFFFu - den_in_cell)) : 0u;
-                uint32_t best = d_st, tot = d_st;
-                for (uint32_t m = lpd; m < lpc; m <<= 1) {
-                    key = max(key, __shfl_xor_sync(0xFFFFFFFFu, key, m));
-                    best = max(best, __shfl_xor_sync(0xFFFFFFFFu, best, m));
-                    tot += __shfl_xor_sync(0xFFFFFFFFu, tot, m);
+        }
+#pragma unroll
+        for (int i = 0; i < 16; i++) {
+            const uint32_t e = e0 + (uint32_t)i * kStep;
+            if (e < total) halo[e] = syn_fire(vals[i]);
+        }
+    }
+}
+
+// Stage layout, per buffer: MODE 0 streams gidx (2 x SB bytes) then strength,
+// state, flags (SB each); MODE 1 streams slc, v_ofs, u_ofs, strength, state,
+// flags (SB each).
+template <int MODE>
+__device__ __forceinline__ uint32_t arr_off(int which, uint32_t SB) {
+    // which: 0 strength, 1 state, 2 flags
+    return MODE == 0 ? (2 + which) * SB : (3 + which) * SB;
+}
+
+// Consumer work of one stage: this warp's unit (a chunk, or a cell of
+// chunks_per_unit chunks).
+template <bool TUFT, int MODE, bool FCLEAN>
+__device__ __forceinline__ void tma_stage(const FusedTuftArgs& A, const TileGeo& G, const uint8_t* halo,
+                                          const uint8_t* sb, uint64_t pos, uint32_t n_units_tile, int lane, int wib,
+                                          int32_t rnd) {
+    const uint32_t SB = A.stage_bytes;
+    const uint32_t cpu = A.chunks_per_unit;
+    const uint32_t unit = (uint32_t)((pos - G.syn0) >> A.unit_l2) + (uint32_t)wib;
+    if (unit >= n_units_tile) return;
+    const uint32_t lim = A.nrec * A.fsz - 1;
+    uint32_t t_key = 0, t_best = 0, t_sum = 0, tuft_cur = 0;
+    for (uint32_t ch = 0; ch < cpu; ch++) {
+        const uint32_t so = ((uint32_t)wib * cpu + ch) * 512 + (uint32_t)lane * 16;   // offset within the stage
+        const uint64_t off = pos + so;
+        const bool on = off < G.syn_end;
+        uint32_t v, u;
+        const int32_t base = footprint_base(A, G, off, v, u);
+        const uint32_t act0 = prefetch_act(A, off, on, lane);
+        if (ch == 0) tuft_cur = prefetch_tuft<TUFT>(A, off, on, lane);
+        uint4 str4{}, st4{}, fl4{}, nst4{};
+        if (on) {
+            str4 = *(const uint4*)(sb + arr_off<MODE>(0, SB) + so);
+            st4 = *(const uint4*)(sb + arr_off<MODE>(1, SB) + so);
+            if (!FCLEAN) fl4 = *(const uint4*)(sb + arr_off<MODE>(2, SB) + so);
+            uint32_t* ow = (uint32_t*)&nst4;
+            if (MODE == 0) {
+                const uint4 g0 = *(const uint4*)(sb + 2 * so);
+                const uint4 g1 = *(const uint4*)(sb + 2 * so + 16);
+                const uint32_t gw[8] = {g0.x, g0.y, g0.z, g0.w, g1.x, g1.y, g1.z, g1.w};
+#pragma unroll
+                for (int w = 0; w < 4; w++) {
+                    const uint32_t lo = gw[2 * w], hi = gw[2 * w + 1];
+                    const uint32_t i0 = min((uint32_t)(base + (int32_t)(int16_t)(lo & 0xFFFF)), lim);
+                    const uint32_t i1 = min((uint32_t)(base + ((int32_t)lo >> 16)), lim);
+                    const uint32_t i2 = min((uint32_t)(base + (int32_t)(int16_t)(hi & 0xFFFF)), lim);
+                    const uint32_t i3 = min((uint32_t)(base + ((int32_t)hi >> 16)), lim);
+                    ow[w] = (uint32_t)halo[i0] | ((uint32_t)halo[i1] << 8) | ((uint32_t)halo[i2] << 16) |
+                            ((uint32_t)halo[i3] << 24);
                 }
-                t_key = max(t_key, key);
-                t_best = max(t_best, best);
-                t_sum += tot;
-                if (ch + 1 == A.chunks_per_unit && on && (lane & (lpc - 1)) == 0) {
-                    const uint32_t c = cell;
-                    const uint32_t best_raw = t_key >> 16;
-                    const uint32_t best_id = best_raw ? (0xFFFFu - (t_key & 0xFFFFu)) : 0u;
-                    const bool is_max = t_sum >= (1u << (A.mad_l2 + 8));
-                    const uint8_t tst = is_max ? (uint8_t)255 : (uint8_t)(t_sum >> A.mad_l2);
-                    A.t_pid[c] = A.t_bid[c];
-                    A.t_praw[c] = A.t_braw[c];
-                    A.t_pst[c] = A.t_bst[c];
-                    A.t_ptft[c] = A.t_st[c];
-                    A.t_bid[c] = (uint8_t)best_id;
-                    A.t_braw[c] = (uint8_t)best_raw;
-                    A.t_bst[c] = (uint8_t)t_best;
-                    A.t_st[c] = tst;
+            } else {
+                const uint4 slc4 = *(const uint4*)(sb + so);
+                const uint4 vo4 = *(const uint4*)(sb + SB + so);
+                const uint4 uo4 = *(const uint4*)(sb + 2 * SB + so);
+                const uint32_t* sw = (const uint32_t*)&slc4;
+                const uint32_t* vw = (const uint32_t*)&vo4;
+                const uint32_t* uw = (const uint32_t*)&uo4;
+#pragma unroll
+                for (int w = 0; w < 4; w++) {
+                    uint32_t out = 0;
+#pragma unroll
+                    for (int b = 0; b < 4; b++) {
+                        const uint32_t slc = (sw[w] >> (8 * b)) & 0xFF;
+                        const int vo = (int)(int8_t)(vw[w] >> (8 * b));
+                        const int uo = (int)(int8_t)(uw[w] >> (8 * b));
+                        const uint32_t k = slc - A.slc0;
+                        const bool in = (k < A.nrec) & ((uint32_t)(vo + A.rv) <= (uint32_t)(2 * A.rv)) &
+                                        ((uint32_t)(uo + A.ru) <= (uint32_t)(2 * A.ru));
+                        uint32_t a;
+                        if (in) a = halo[k * A.fsz + (uint32_t)(base + vo * (int32_t)A.fw + uo)];
+                        else a = gather_general(A, slc, v, u, vo, uo);
+                        out |= a << (8 * b);
+                    }
+                    ow[w] = out;
                 }
             }
         }
+        finish_chunk<TUFT>(A, str4, st4, fl4, nst4, FCLEAN, off, on, lane, rnd, ch + 1 == cpu, act0, tuft_cur, t_key,
+                           t_best, t_sum);
     }
+}
+
+template <bool TUFT, int MODE, bool FCLEAN>
+__device__ __forceinline__ void tma_body(const FusedTuftArgs& A, uint8_t* smem, volatile int& s_abort) {
+    uint64_t* full = (uint64_t*)smem;              // [nst]
+    uint64_t* empty = full + A.nst;                // [nst]
+    uint8_t* stages = smem + 128;
+    uint8_t* halo = smem + A.halo_off;
+    const int tid = threadIdx.x;
+    const int lane = tid & 31;
+    const int wib = tid >> 5;
+    const uint32_t SB = A.stage_bytes;
+    const uint32_t buf_bytes = (MODE == 0 ? 5u : 6u) * SB;
+    const uint32_t nst = A.nst;
+
+    if (wib == kWarps) {
+        // ---- producer warp: lane 0 streams every stage of this CTA's tiles ----
+        if (lane != 0) return;
+        uint32_t pb = 0, pround = 0;
+        uint64_t issued = 0;
+        for (uint32_t t = blockIdx.x; t < A.n_tiles && !s_abort; t += gridDim.x) {
+            const TileGeo G = tile_geo(A, t);
+            for (uint64_t pos = G.syn0; pos < G.syn_end; pos += SB) {
+                if (s_abort) break;
+                // Buffer pb's previous use (round pround - 1) must be released.
+                if (pround > 0 && !mbar_wait(&empty[pb], (pround - 1) & 1)) {
+                    s_abort = 1;
+                    break;
+                }
+                const uint64_t left = G.syn_end - pos;
+                const uint32_t nb = left < SB ? (uint32_t)left : SB;
+                uint8_t* dst = stages + (size_t)pb * buf_bytes;
+                const uint32_t n_arr_bytes = (MODE == 0 ? 2 * nb : 3 * nb) + nb + nb + (FCLEAN ? 0 : nb);
+                mbar_arrive_expect_tx(&full[pb], n_arr_bytes);
+                if (MODE == 0) {
+                    bulk_g2s(dst, A.gidx + pos, 2 * nb, &full[pb]);
+                } else {
+                    bulk_g2s(dst, A.slc + pos, nb, &full[pb]);
+                    bulk_g2s(dst + SB, A.vofs + pos, nb, &full[pb]);
+                    bulk_g2s(dst + 2 * SB, A.uofs + pos, nb, &full[pb]);
+                }
+                bulk_g2s(dst + arr_off<MODE>(0, SB), A.str + pos, nb, &full[pb]);
+                bulk_g2s(dst + arr_off<MODE>(1, SB), A.st + pos, nb, &full[pb]);
+                if (!FCLEAN) bulk_g2s(dst + arr_off<MODE>(2, SB), A.fl + pos, nb, &full[pb]);
+                issued++;
+                if (++pb == nst) { pb = 0; pround++; }
+            }
+        }
+        if (s_abort) {
+            // Let this CTA's copies land before its shared memory is released:
+            // the latest use of every buffer must complete.
+            atomicOr(&A.ctl->error, kErrWaitTimeout);
+            for (uint32_t b = 0; b < nst; b++) {
+                const uint64_t uses = issued / nst + (b < issued % nst ? 1 : 0);
+                if (uses) mbar_wait(&full[b], (uint32_t)((uses - 1) & 1));
+            }
+        }
+        return;
+    }
+
+    // ---- consumer warps ----
+    const uint32_t cpu = A.chunks_per_unit;
+    const int32_t rnd = rnd_at(A.rnd_key, A.ctl->cycle);
+    uint32_t cb = 0, cphase = 0;
+    for (uint32_t t = blockIdx.x; t < A.n_tiles; t += gridDim.x) {
+        const TileGeo G = tile_geo(A, t);
+        consumers_sync();   // every consumer is done with the previous footprint
+        if (s_abort) break;
+        build_footprint(A, G, halo, wib * 32 + lane);
+        consumers_sync();
+        const uint32_t n_units_tile = cpu > 1 ? G.h * G.w : (uint32_t)((G.syn_end - G.syn0 + 511) >> 9);
+        for (uint64_t pos = G.syn0; pos < G.syn_end; pos += SB) {
+            bool got = !s_abort && mbar_wait(&full[cb], cphase);
+            got = __all_sync(0xFFFFFFFFu, got);
+            if (!got) {
+                if (lane == 0) s_abort = 1;
+                break;
+            }
+            tma_stage<TUFT, MODE, FCLEAN>(A, G, halo, stages + (size_t)cb * buf_bytes, pos, n_units_tile, lane, wib,
+                                          rnd);
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&empty[cb]);
+            if (++cb == nst) { cb = 0; cphase ^= 1; }
+        }
+    }
+}
+
+template <bool TUFT>
+__global__ void __launch_bounds__(kThreads, 2) k_fused_tuft_tma(FusedTuftArgs A) {
+    extern __shared__ __align__(128) uint8_t smem[];
+    __shared__ volatile int s_abort;   // a bounded wait gave up
+    uint64_t* full = (uint64_t*)smem;
+    uint64_t* empty = full + A.nst;
+    if (threadIdx.x == 0) {
+        for (uint32_t i = 0; i < A.nst; i++) {
+            mbar_init(&full[i], 1);
+            mbar_init(&empty[i], kWarps);
+        }
+        fence_mbar_init();
+        s_abort = 0;
+    }
+    __syncthreads();
+    // One specialised body per gather mode and flags state (uniform per launch).
+    const uint32_t status = A.ctl->tuft_status[A.status_idx];
+    const bool fclean = (status & kTuftFlagsForeign) == 0;
+    if (status & kTuftSrcOutsideTile) {
+        if (fclean) tma_body<TUFT, 1, true>(A, smem, s_abort);
+        else tma_body<TUFT, 1, false>(A, smem, s_abort);
+    } else {
+        if (fclean) tma_body<TUFT, 0, true>(A, smem, s_abort);
+        else tma_body<TUFT, 0, false>(A, smem, s_abort);
+    }
+}
+
+// ------------------------------------------------------ source compile ----
+// Writes each synapse's gather offset into the footprint,
+// (slc - slc0) * fsz + v_ofs * fw + u_ofs, and sets kTuftSrcOutsideTile if a
+// source cannot be served from the footprint, kTuftFlagsForeign if a flag
+// byte has bits other than SYN_PREV_ACTIVE. 16 synapses per thread. With
+// gidx == nullptr (untiled tufts) only the flags are checked.
+__global__ void k_compile_tuft(const uint8_t* __restrict__ slc, const int8_t* __restrict__ vo,
+                               const int8_t* __restrict__ uo, const uint8_t* __restrict__ fl, int16_t* gidx,
+                               uint64_t n, uint32_t slc0, uint32_t nrec, int32_t rv, int32_t ru, uint32_t fw,
+                               uint32_t fsz, unsigned int* status) {
+    uint32_t bits = 0;
+    for (uint64_t i = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) * 16; i < n;
+         i += (uint64_t)gridDim.x * blockDim.x * 16) {
+        const uint4 f4 = *(const uint4*)(fl + i);
+        const uint32_t* fw4 = (const uint32_t*)&f4;
+#pragma unroll
+        for (int w = 0; w < 4; w++)
+            if (fw4[w] & 0xEFEFEFEFu) bits |= kTuftFlagsForeign;
+        if (!gidx) continue;
+        const uint4 s4 = *(const uint4*)(slc + i), v4 = *(const uint4*)(vo + i), u4 = *(const uint4*)(uo + i);
+        const uint32_t* sw = (const uint32_t*)&s4;
+        const uint32_t* vw = (const uint32_t*)&v4;
+        const uint32_t* uw = (const uint32_t*)&u4;
+        uint32_t out[8];
+#pragma unroll
+        for (int w = 0; w < 4; w++) {
+            int32_t g[4];
+#pragma unroll
+            for (int b = 0; b < 4; b++) {
+                const uint32_t k = ((sw[w] >> (8 * b)) & 0xFF) - slc0;
+                const int v = (int)(int8_t)(vw[w] >> (8 * b)), u = (int)(int8_t)(uw[w] >> (8 * b));
+                const bool ok = k < nrec && v >= -rv && v <= rv && u >= -ru && u <= ru;
+                if (!ok) bits |= kTuftSrcOutsideTile;
+                g[b] = ok ? (int32_t)(k * fsz) + v * (int32_t)fw + u : 0;
+            }
+            out[2 * w] = (uint32_t)(uint16_t)g[0] | ((uint32_t)(uint16_t)g[1] << 16);
+            out[2 * w + 1] = (uint32_t)(uint16_t)g[2] | ((uint32_t)(uint16_t)g[3] << 16);
+        }
+        uint4* dst = (uint4*)(gidx + i);
+        dst[0] = make_uint4(out[0], out[1], out[2], out[3]);
+        dst[1] = make_uint4(out[4], out[5], out[6], out[7]);
+    }
+    bits = __reduce_or_sync(0xFFFFFFFFu, bits);
+    if ((threadIdx.x & 31) == 0 && bits) atomicOr(status, bits);
 }
 
 inline int ilog2(uint64_t x) {
@@ -232,7 +664,6 @@ inline bool pow2(uint64_t x) { return x && !(x & (x - 1)); }
 }  // namespace
 
 int prepare_fused(FusedArea& F, const bm_area_plan& P, std::string* err) {
-    (void)err;
     int dev = 0;
     cudaGetDevice(&dev);
     int sms = 148;
@@ -245,9 +676,11 @@ int prepare_fused(FusedArea& F, const bm_area_plan& P, std::string* err) {
             if (L.buf_off[k] != UINT64_MAX && (L.buf_off[k] % 16)) aligned = false;
         for (uint32_t t = 0; t < L.n_tufts; t++) {
             const bm_tuft_plan& T = L.tufts[t];
+            FusedTuft& FT = F.t[i][t];
+            FT = FusedTuft{};
             uint32_t spd = T.syns_per_den, dpt = T.dens_per_tft;
-            F.tuft_ok[i][t] = aligned && pow2(spd) && spd >= 16 && spd <= 512 && pow2(dpt) && (T.syn_idz % 16) == 0;
-            // Slice records serve the pool's distinct slices when their ids are
+            FT.ok = aligned && pow2(spd) && spd >= 16 && spd <= 512 && pow2(dpt) && (T.syn_idz % 16) == 0;
+            // Fast gathers serve the pool's distinct slices when their ids are
             // contiguous and spatial (mid 0, where bismit's scalar and vec4 index
             // forms agree); anything else takes the general per-synapse path.
             uint32_t lo = 255, hi = 0;
@@ -257,19 +690,124 @@ int prepare_fused(FusedArea& F, const bm_area_plan& P, std::string* err) {
             }
             uint32_t nrec = (T.n_src_uniq && hi - lo + 1 <= (uint32_t)kMaxRecs) ? hi - lo + 1 : 0;
             for (uint32_t k = 0; k < nrec; k++)
-                if (P.slc_v_mid[lo + k] || P.slc_u_mid[lo + k]) nrec = 0;
-            F.slc0[i][t] = nrec ? lo : 0;
-            F.nrec[i][t] = nrec;
+                if (P.slc_v_mid[lo + k] || P.slc_u_mid[lo + k] || !P.slc_v_scale[lo + k]) nrec = 0;
+            FT.slc0 = nrec ? lo : 0;
+            FT.nrec = nrec;
+            if (!FT.ok) continue;
+            // Tiled gathers: the recorded slices share one geometry; the
+            // footprint margin is the pool's largest offset.
+            bool same = nrec > 0;
+            for (uint32_t k = 1; k < nrec && same; k++) {
+                uint32_t a = lo, b = lo + k;
+                same = P.slc_v_size[a] == P.slc_v_size[b] && P.slc_u_size[a] == P.slc_u_size[b] &&
+                       P.slc_v_scale[a] == P.slc_v_scale[b] && P.slc_u_scale[a] == P.slc_u_scale[b];
+            }
+            int rv = 0, ru = 0;
+            for (uint32_t k = 0; k < T.n_src_uniq && same; k++) {
+                int a, b;
+                uint8_t sid = T.src_uniq_slc_ids[k];
+                if (!offset_extent(T.src_uniq_reaches[k], P.slc_v_scale[sid], P.slc_u_scale[sid], &a, &b)) same = false;
+                rv = std::max(rv, a);
+                ru = std::max(ru, b);
+            }
+            if (!same) continue;
+            const uint32_t S = T.syns_per_tft;
+            const uint32_t cpu = S > 512 ? S / 512 : 1;
+            const uint32_t SB = kWarps * cpu * 512;
+            const uint64_t n_syn = (uint64_t)L.cells * S;
+            uint64_t target = std::min<uint64_t>(32768, std::max<uint64_t>(4096, n_syn / ((uint64_t)sms * 16)));
+            uint64_t cells = std::max<uint64_t>(1, target / S);
+            uint32_t W, H;
+            if (cells >= L.u_size) {
+                W = L.u_size;
+                H = (uint32_t)std::min<uint64_t>(L.v_size, cells / L.u_size);
+            } else {
+                W = (uint32_t)cells;
+                H = 1;
+            }
+            const uint32_t vs = P.slc_v_scale[lo], us = P.slc_u_scale[lo];
+            const uint64_t frows = ((uint64_t)(H - 1) * vs + 15) / 16 + 1 + 2 * (uint64_t)rv;
+            const uint64_t fw = ((uint64_t)(W - 1) * us + 15) / 16 + 1 + 2 * (uint64_t)ru;
+            const uint64_t fsz = frows * fw;
+            const uint64_t halo = (uint64_t)nrec * fsz;
+            if (halo >= 32768) continue;   // gather offsets are 16-bit
+            const uint32_t buf_bytes = 6 * SB;
+            uint32_t nst = (uint32_t)std::max<uint64_t>(2, std::min<uint64_t>(4, (80 * 1024) / buf_bytes));
+            const uint64_t halo_off = 128 + (uint64_t)nst * buf_bytes;
+            const uint64_t smem = halo_off + ((halo + 15) / 16) * 16;
+            if (smem > 110 * 1024) continue;
+            FT.tiled = true;
+            FT.tile_w = W;
+            FT.tile_h = H;
+            FT.rv = rv;
+            FT.ru = ru;
+            FT.fw = (uint32_t)fw;
+            FT.frows = (uint32_t)frows;
+            FT.fsz = (uint32_t)fsz;
+            FT.nst = nst;
+            FT.stage_bytes = SB;
+            FT.halo_off = (uint32_t)halo_off;
+            FT.smem = (uint32_t)smem;
+            FT.src_vs = vs;
+            FT.src_us = us;
+            FT.src_vsz = P.slc_v_size[lo];
+            FT.src_usz = P.slc_u_size[lo];
+            for (uint32_t k = 0; k < nrec; k++) FT.src_idz[k] = P.slc_axn_idz[lo + k];
+            // Persistent grid: as many CTAs as fit on the device at once.
+            const bool pyr = L.kind == BM_LYR_PYRAMIDAL;
+            auto kern = pyr ? k_fused_tuft_tma<true> : k_fused_tuft_tma<false>;
+            cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)FT.smem);
+            int per_sm = 0;
+            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads, FT.smem) != cudaSuccess)
+                per_sm = 1;
+            const uint64_t n_tiles = (uint64_t)L.depth * ((L.u_size + W - 1) / W) * ((L.v_size + H - 1) / H);
+            FT.grid = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(n_tiles, (uint64_t)sms * std::max(per_sm, 1)));
+            // Compiled gather offsets: 2 bytes per synapse of the tuft.
+            if (cudaMalloc(&FT.gidx, n_syn * sizeof(int16_t)) != cudaSuccess) {
+                cudaGetLastError();
+                FT.gidx = nullptr;
+                FT.tiled = false;
+                if (err) *err = "cudaMalloc of the gather offsets failed";
+                free_fused(F);
+                return BM_ERR_OOM;
+            }
         }
     }
+    cudaGetLastError();
     return BM_OK;
 }
 
-void free_fused(FusedArea& F) { (void)F; }
+void free_fused(FusedArea& F) {
+    for (auto& row : F.t)
+        for (auto& FT : row)
+            if (FT.gidx) {
+                cudaFree(FT.gidx);
+                FT.gidx = nullptr;
+            }
+}
+
+void launch_verify_tufts(const FusedArea& F, const DevLayer& L, uint32_t layer, AreaCtl* ctl, cudaStream_t s) {
+    for (uint32_t t = 0; t < L.n_tufts; t++) {
+        const FusedTuft& FT = F.t[layer][t];
+        if (!FT.ok) continue;
+        const DevTuft& T = L.tft[t];
+        unsigned int* status = &ctl->tuft_status[layer * BM_MAX_TUFTS + t];
+        cudaMemsetAsync(status, 0, sizeof(unsigned int), s);
+        const uint64_t n = (uint64_t)L.cells * T.spt;
+        const uint64_t threads = (n + 15) / 16;
+        const unsigned grid = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((threads + 255) / 256, (uint64_t)F.sms * 8));
+        k_compile_tuft<<<grid, 256, 0, s>>>(L.buf[BM_BUF_SYN_SRC_SLC_IDS] + T.syn_idz,
+                                            (const int8_t*)L.buf[BM_BUF_SYN_SRC_COL_V_OFFS] + T.syn_idz,
+                                            (const int8_t*)L.buf[BM_BUF_SYN_SRC_COL_U_OFFS] + T.syn_idz,
+                                            L.buf[BM_BUF_SYN_FLAG_SETS] + T.syn_idz, FT.tiled ? FT.gidx : nullptr, n,
+                                            FT.slc0, FT.nrec, FT.rv, FT.ru, FT.fw, FT.fsz, status);
+    }
+}
 
 void launch_fused_tuft(const FusedArea& F, const uint8_t* axns, const SliceRec* slices, const DevLayer& L,
-                       uint32_t layer, uint32_t t, const AreaCtl* ctl, cudaStream_t s) {
+                       uint32_t layer, uint32_t t, AreaCtl* ctl, cudaStream_t s) {
     const DevTuft& T = L.tft[t];
+    const FusedTuft& FT = F.t[layer][t];
     FusedTuftArgs A;
     std::memset(&A, 0, sizeof A);
     A.axns = axns;
@@ -281,6 +819,7 @@ void launch_fused_tuft(const FusedArea& F, const uint8_t* axns, const SliceRec* 
     A.str = (const int8_t*)L.buf[BM_BUF_SYN_STRENGTHS] + T.syn_idz;
     A.st = L.buf[BM_BUF_SYN_STATES] + T.syn_idz;
     A.fl = L.buf[BM_BUF_SYN_FLAG_SETS] + T.syn_idz;
+    A.gidx = FT.gidx;
     A.den_act = L.buf[BM_BUF_DEN_ACTIVITIES] + T.den_idz;
     A.den_raw = L.buf[BM_BUF_DEN_STATES_RAW] + T.den_idz;
     A.den_st = L.buf[BM_BUF_DEN_STATES] + T.den_idz;
@@ -301,25 +840,52 @@ void launch_fused_tuft(const FusedArea& F, const uint8_t* axns, const SliceRec* 
     A.thresh = T.thresh;
     A.cols = L.v_size * L.u_size;
     A.u_size = L.u_size;
+    A.v_size = L.v_size;
     A.S_l2 = ilog2(S);
     A.spd_l2 = ilog2(T.spd);
     A.lpd_l2 = A.spd_l2 - 4;
     A.lpc_l2 = std::min<uint32_t>(A.S_l2 - 4, 5);
     A.chunks_per_unit = S > 512 ? (uint32_t)(S / 512) : 1u;
-    const uint64_t n_chunks = (A.n_syn + 511) / 512;
-    A.n_units = S > 512 ? (uint64_t)L.cells : n_chunks;
     A.mad_l2 = T.mad_l2;
-    A.slc0 = F.slc0[layer][t];
-    A.nrec = F.nrec[layer][t];
+    A.slc0 = FT.slc0;
+    A.nrec = FT.nrec;
     A.vec4 = (T.spt & 3) == 0;
     A.rnd_key = T.rnd_key_den;
-    uint64_t want = (A.n_units + kWarps - 1) / kWarps;
-    uint64_t cap = (uint64_t)F.sms * 8;
-    unsigned grid = (unsigned)std::max<uint64_t>(1, std::min(want, cap));
-    if (tuft)
-        k_fused_tuft<true><<<grid, kWarps * 32, 0, s>>>(A);
-    else
-        k_fused_tuft<false><<<grid, kWarps * 32, 0, s>>>(A);
+    A.status_idx = layer * BM_MAX_TUFTS + t;
+    if (FT.tiled) {
+        A.tile_w = FT.tile_w;
+        A.tile_h = FT.tile_h;
+        A.tiles_u = (L.u_size + FT.tile_w - 1) / FT.tile_w;
+        A.tiles_v = (L.v_size + FT.tile_h - 1) / FT.tile_h;
+        A.n_tiles = L.depth * A.tiles_u * A.tiles_v;
+        A.usz_magic = (uint32_t)(((1ull << 32) + L.u_size - 1) / L.u_size);
+        A.rv = FT.rv;
+        A.ru = FT.ru;
+        A.fw = FT.fw;
+        A.frows = FT.frows;
+        A.fsz = FT.fsz;
+        A.src_vs = FT.src_vs;
+        A.src_us = FT.src_us;
+        A.src_vsz = FT.src_vsz;
+        A.src_usz = FT.src_usz;
+        for (uint32_t k = 0; k < FT.nrec; k++) A.src_idz[k] = FT.src_idz[k];
+        A.nst = FT.nst;
+        A.stage_bytes = FT.stage_bytes;
+        A.halo_off = FT.halo_off;
+        A.unit_l2 = 9 + ilog2(A.chunks_per_unit);
+        auto kern = tuft ? k_fused_tuft_tma<true> : k_fused_tuft_tma<false>;
+        kern<<<FT.grid, kThreads, FT.smem, s>>>(A);
+    } else {
+        const uint64_t n_chunks = (A.n_syn + 511) / 512;
+        A.n_units = S > 512 ? (uint64_t)L.cells : n_chunks;
+        uint64_t want = (A.n_units + kWarps - 1) / kWarps;
+        uint64_t cap = (uint64_t)F.sms * 8;
+        unsigned grid = (unsigned)std::max<uint64_t>(1, std::min(want, cap));
+        if (tuft)
+            k_fused_tuft<true><<<grid, kWarps * 32, 0, s>>>(A);
+        else
+            k_fused_tuft<false><<<grid, kWarps * 32, 0, s>>>(A);
+    }
 }
 
 }  // namespace bm

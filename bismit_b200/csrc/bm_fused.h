@@ -3,24 +3,45 @@
 #include <string>
 
 #include "bm_dev.cuh"
+#include "bm_layout.h"
 
 namespace bm {
 
+// Launch parameters of the fused kernel for one tuft.
+struct FusedTuft {
+    bool ok = false;         // the fused kernel applies to this tuft
+    uint32_t slc0 = 0;       // fast gathers serve slices slc0 .. slc0 + nrec - 1
+    uint32_t nrec = 0;
+    bool tiled = false;      // gathers from a shared-memory footprint
+    uint32_t tile_w = 0, tile_h = 0;
+    int32_t rv = 0, ru = 0;  // footprint margin: the pool's largest |v|, |u| offsets
+    uint32_t fw = 0, frows = 0, fsz = 0;   // footprint width, rows, bytes per slice
+    int16_t* gidx = nullptr; // compiled gather offsets, one per synapse of the tuft
+    uint32_t smem = 0;       // dynamic shared memory per CTA
+    uint32_t grid = 1;       // persistent grid size
+    uint32_t nst = 2;        // TMA pipeline stages
+    uint32_t stage_bytes = 0;
+    uint32_t halo_off = 0;   // halo offset in dynamic shared memory
+    uint32_t src_vs = 0, src_us = 0, src_vsz = 0, src_usz = 0;
+    uint32_t src_idz[8] = {};
+};
+
 struct FusedArea {
     int sms = 148;
-    bool tuft_ok[BM_MAX_LAYERS][BM_MAX_TUFTS] = {};
-    uint32_t slc0[BM_MAX_LAYERS][BM_MAX_TUFTS] = {};
-    uint32_t nrec[BM_MAX_LAYERS][BM_MAX_TUFTS] = {};
+    FusedTuft t[BM_MAX_LAYERS][BM_MAX_TUFTS];
 };
 
 // Decides, per tuft, whether the fused kernel applies (syns_per_den a power of
-// two in 16..512, dens_per_tft a power of two, 16-byte aligned ranges). Tufts
-// that do not qualify run the plain per-stage kernels.
+// two in 16..512, dens_per_tft a power of two, 16-byte aligned ranges) and
+// its gather form. Tufts that do not qualify run the plain per-stage kernels.
 int prepare_fused(FusedArea& F, const bm_area_plan& P, std::string* err);
 void free_fused(FusedArea& F);
 // Synapse flags + synapse cycle + dendrite cycle (+ tuft cycle for pyramidal
 // layers) of one tuft in one launch.
 void launch_fused_tuft(const FusedArea& F, const uint8_t* axns, const SliceRec* slices, const DevLayer& L,
-                       uint32_t layer, uint32_t t, const AreaCtl* ctl, cudaStream_t s);
+                       uint32_t layer, uint32_t t, AreaCtl* ctl, cudaStream_t s);
+// Recomputes AreaCtl::tuft_status for the fused tufts of a layer (after its
+// synapse sources or flags were written by the caller).
+void launch_verify_tufts(const FusedArea& F, const DevLayer& L, uint32_t layer, AreaCtl* ctl, cudaStream_t s);
 
 }  // namespace bm

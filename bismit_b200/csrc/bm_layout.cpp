@@ -15,6 +15,7 @@
 
 #include <algorithm>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <vector>
@@ -102,6 +103,21 @@ std::vector<std::pair<int8_t, int8_t>> gen_syn_offs(int radius, uint32_t vs, uin
 uint64_t align_up(uint64_t x, uint64_t a) { return (x + a - 1) / a * a; }
 
 }  // namespace
+
+bool offset_extent(int reach, uint32_t vs, uint32_t us, int* rv, int* ru) {
+    try {
+        int mv = 0, mu = 0;
+        for (auto& o : gen_syn_offs(reach, vs, us)) {
+            mv = std::max(mv, std::abs((int)o.first));
+            mu = std::max(mu, std::abs((int)o.second));
+        }
+        *rv = mv;
+        *ru = mu;
+        return true;
+    } catch (const Fail&) {
+        return false;
+    }
+}
 
 uint64_t rnd_key(uint64_t seed, uint32_t area, uint32_t layer, uint32_t role, uint32_t tft) {
     uint64_t bits = ((uint64_t)area << 40) ^ ((uint64_t)layer << 32) ^ ((uint64_t)role << 24) ^ ((uint64_t)tft << 16);

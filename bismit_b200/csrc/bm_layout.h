@@ -33,6 +33,10 @@ struct TuftGrowSpec {
 int resolve_area(const bm_area_desc* D, uint64_t seed, bm_area_plan* P, std::vector<TuftGrowSpec>* grow,
                  std::string* err);
 
+// Largest |v| and |u| offset in gen_syn_offs(reach, [vs, us]); false if the
+// pool cannot be generated.
+bool offset_extent(int reach, uint32_t vs, uint32_t us, int* rv, int* ru);
+
 // Key of the per-launch random stream for (area, layer, role, tuft).
 uint64_t rnd_key(uint64_t seed, uint32_t area, uint32_t layer, uint32_t role, uint32_t tft);
 // Key of the growth stream of (area, layer, tuft).

@@ -349,8 +349,15 @@ int bm_area_get_cycle(bm_area area, uint64_t* out);
 int bm_area_set_cycle(bm_area area, uint64_t cycle);
 
 /* Device pointer of the state slab (for callers that move data with their own
- * copies on the same device). */
+ * copies on the same device). A caller that writes synapse sources or flags
+ * through it must call bm_area_sources_changed for that layer before the next
+ * cycle. */
 int bm_area_slab_ptr(bm_area area, void** out);
+int bm_area_sources_changed(bm_area area, uint32_t layer);
+
+/* Sticky device-side error bits of the area (bit 0: a bounded wait inside a
+ * kernel gave up). Synchronous; returns BM_ERR_TIMEOUT when any bit is set. */
+int bm_area_device_errors(bm_area area, uint32_t* bits);
 
 /* Per-kernel CUDA-event timing of subsequent cycles (0 = off). */
 int bm_area_set_profiling(bm_area area, int on);
