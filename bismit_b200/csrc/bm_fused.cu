@@ -97,6 +97,9 @@ struct FusedTuftArgs {
     uint32_t stage_bytes;               // bytes per 1-byte array per stage
     uint32_t halo_off;                  // byte offset of the footprint in dynamic smem
     uint32_t unit_l2;                   // log2 of the bytes of one unit (chunks_per_unit * 512)
+    uint32_t stage_stride;              // bytes per ring buffer (synapse arrays + windows)
+    uint32_t win;                       // dendrite / cell-tuft windows ride in the stages
+    uint32_t win_bytes;                 // bytes per window
 };
 
 struct Rec {
@@ -131,10 +134,34 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
         : "memory");
     return ok != 0;
 }
-// Bounded wait; false after kWaitLimit polls.
+// try_wait that may suspend the thread until the phase completes, for at most
+// `hint_ns` nanoseconds per call (a suspended warp issues nothing).
+__device__ __forceinline__ bool mbar_try_wait_sleep(uint64_t* bar, uint32_t parity, uint32_t hint_ns) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_addr(bar)), "r"(parity), "r"(hint_ns)
+        : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ uint64_t global_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+// Bounded wait: false once kWaitNs of wall time have passed without the
+// phase completing.
+constexpr uint64_t kWaitNs = 2000000000ull;
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
-    for (uint32_t i = 0; i < kWaitLimit; i++)
-        if (mbar_try_wait(bar, parity)) return true;
+    if (mbar_try_wait(bar, parity)) return true;
+    const uint64_t t0 = global_ns();
+    for (uint32_t i = 0; i < kWaitLimit; i++) {
+        if (mbar_try_wait_sleep(bar, parity, 200000u)) return true;
+        if (global_ns() - t0 > kWaitNs) return false;
+    }
     return false;
 }
 // 1-D bulk copy global -> shared completing on `bar` (16-byte aligned, size % 16 == 0).
@@ -183,7 +210,7 @@ __device__ __forceinline__ uint32_t prefetch_tuft(const FusedTuftArgs& A, uint64
 // reduction. `last` marks the final chunk of a cell.
 template <bool TUFT>
 __device__ __forceinline__ void finish_chunk(const FusedTuftArgs& A, const uint4& str4, const uint4& st4,
-                                             const uint4& fl4, const uint4& nst4, bool flags_clean, uint64_t off,
+                                             const uint4& fl4, const uint4& nst4, bool flags_clean, uint32_t off,
                                              bool on, int lane, int32_t rnd, bool last, uint32_t act0,
                                              uint32_t tuft_cur, uint32_t& t_key, uint32_t& t_best, uint32_t& t_sum) {
     const uint32_t lpd = 1u << A.lpd_l2;
@@ -213,11 +240,11 @@ __device__ __forceinline__ void finish_chunk(const FusedTuftArgs& A, const uint4
     }
     uint32_t d_raw = 0, d_st = 0;
     const bool lead = on && (lane & (lpd - 1)) == 0;
-    const uint64_t den = off >> A.spd_l2;   // dendrite id within the tuft
+    const uint32_t den = off >> A.spd_l2;   // dendrite id within the tuft
     if (lead) {
         const int active = sum > A.thresh;
         const uint32_t s2 = active ? sum : 0u;
-        const uint32_t di = (uint32_t)den + A.den_idz;
+        const uint32_t di = den + A.den_idz;
         const uint32_t seed = (raw + A.thresh) | di;
         A.den_act[den] = update_activity((uint8_t)act0, active, rnd, (int32_t)seed, kDendriteActivityDecay);
         d_raw = min(raw >> 4, 255u);
@@ -228,7 +255,7 @@ __device__ __forceinline__ void finish_chunk(const FusedTuftArgs& A, const uint4
     if (TUFT) {
         // Argmax of the raw state with the first (lowest) dendrite winning
         // ties: maximise (raw << 16 | (0xFFFF - id)).
-        const uint32_t den_in_cell = (uint32_t)(den & ((1u << (A.S_l2 - A.spd_l2)) - 1));
+        const uint32_t den_in_cell = den & ((1u << (A.S_l2 - A.spd_l2)) - 1);
         uint32_t key = lead ? ((d_raw << 16) | (0xFFFFu - den_in_cell)) : 0u;
         uint32_t best = d_st, tot = d_st;
         if (lpc == 32) {
@@ -246,7 +273,7 @@ __device__ __forceinline__ void finish_chunk(const FusedTuftArgs& A, const uint4
         t_best = max(t_best, best);
         t_sum += tot;
         if (last && on && (lane & (lpc - 1)) == 0) {
-            const uint32_t c = (uint32_t)(off >> A.S_l2);
+            const uint32_t c = off >> A.S_l2;
             const uint32_t best_raw = t_key >> 16;
             const uint32_t best_id = best_raw ? (0xFFFFu - (t_key & 0xFFFFu)) : 0u;
             const bool is_max = t_sum >= (1u << (A.mad_l2 + 8));
@@ -332,7 +359,7 @@ __global__ void __launch_bounds__(kWarps * 32) k_fused_tuft(FusedTuftArgs A) {
                     ow[w] = out;
                 }
             }
-            finish_chunk<TUFT>(A, str4, st4, fl4, nst4, flags_clean, off, on, lane, rnd,
+            finish_chunk<TUFT>(A, str4, st4, fl4, nst4, flags_clean, (uint32_t)off, on, lane, rnd,
                                ch + 1 == A.chunks_per_unit, act0, tuft_cur, t_key, t_best, t_sum);
         }
     }
@@ -342,7 +369,7 @@ __global__ void __launch_bounds__(kWarps * 32) k_fused_tuft(FusedTuftArgs A) {
 struct TileGeo {
     uint32_t v0, u0, h, w;
     int32_t vlo, ulo;
-    uint64_t cell0, syn0, syn_end;
+    uint32_t cell0, syn0, syn_end;   // tuft-relative (a tuft has fewer than 2^32 synapses)
 };
 
 __device__ __forceinline__ TileGeo tile_geo(const FusedTuftArgs& A, uint32_t t) {
@@ -356,17 +383,17 @@ __device__ __forceinline__ TileGeo tile_geo(const FusedTuftArgs& A, uint32_t t) 
     g.w = min(A.tile_w, A.u_size - g.u0);
     g.vlo = (int32_t)((g.v0 * A.src_vs) >> kSlcSclCoeffL2) - A.rv;
     g.ulo = (int32_t)((g.u0 * A.src_us) >> kSlcSclCoeffL2) - A.ru;
-    g.cell0 = (uint64_t)s_lyr * A.cols + (uint64_t)g.v0 * A.u_size + g.u0;
+    g.cell0 = s_lyr * A.cols + g.v0 * A.u_size + g.u0;
     g.syn0 = g.cell0 << A.S_l2;
-    g.syn_end = (g.cell0 + (uint64_t)g.h * g.w) << A.S_l2;
+    g.syn_end = (g.cell0 + g.h * g.w) << A.S_l2;
     return g;
 }
 
 // The position of the 16 synapses at tuft offset `off` in the footprint of
 // tile G: (cell's scaled row - vlo) * fw + (cell's scaled column - ulo).
-__device__ __forceinline__ int32_t footprint_base(const FusedTuftArgs& A, const TileGeo& G, uint64_t off,
+__device__ __forceinline__ int32_t footprint_base(const FusedTuftArgs& A, const TileGeo& G, uint32_t off,
                                                   uint32_t& v, uint32_t& u) {
-    const uint32_t local = (uint32_t)((off >> A.S_l2) - G.cell0);
+    const uint32_t local = (off >> A.S_l2) - G.cell0;
     if (A.tile_h == 1) {
         v = G.v0;
         u = G.u0 + local;
@@ -428,22 +455,40 @@ __device__ __forceinline__ uint32_t arr_off(int which, uint32_t SB) {
 // chunks_per_unit chunks).
 template <bool TUFT, int MODE, bool FCLEAN>
 __device__ __forceinline__ void tma_stage(const FusedTuftArgs& A, const TileGeo& G, const uint8_t* halo,
-                                          const uint8_t* sb, uint64_t pos, uint32_t n_units_tile, int lane, int wib,
+                                          const uint8_t* sb, uint32_t pos, uint32_t n_units_tile, int lane, int wib,
                                           int32_t rnd) {
     const uint32_t SB = A.stage_bytes;
     const uint32_t cpu = A.chunks_per_unit;
-    const uint32_t unit = (uint32_t)((pos - G.syn0) >> A.unit_l2) + (uint32_t)wib;
+    const uint32_t unit = ((pos - G.syn0) >> A.unit_l2) + (uint32_t)wib;
     if (unit >= n_units_tile) return;
     const uint32_t lim = A.nrec * A.fsz - 1;
     uint32_t t_key = 0, t_best = 0, t_sum = 0, tuft_cur = 0;
     for (uint32_t ch = 0; ch < cpu; ch++) {
         const uint32_t so = ((uint32_t)wib * cpu + ch) * 512 + (uint32_t)lane * 16;   // offset within the stage
-        const uint64_t off = pos + so;
+        const uint32_t off = pos + so;
         const bool on = off < G.syn_end;
         uint32_t v, u;
         const int32_t base = footprint_base(A, G, off, v, u);
-        const uint32_t act0 = prefetch_act(A, off, on, lane);
-        if (ch == 0) tuft_cur = prefetch_tuft<TUFT>(A, off, on, lane);
+        uint32_t act0;
+        if (A.win) {
+            // The stage carries the dendrite and cell-tuft bytes (windows start
+            // at the stage's first dendrite / cell rounded down to 16).
+            const uint8_t* wd = sb + 6 * SB;
+            const uint32_t lpd = 1u << A.lpd_l2;
+            act0 = (on && (lane & (lpd - 1)) == 0) ? (uint32_t)wd[(off >> A.spd_l2) - ((pos >> A.spd_l2) & ~15u)] : 0u;
+            if (TUFT && ch == 0) {
+                const uint32_t lpc = 1u << A.lpc_l2;
+                tuft_cur = 0;
+                if (on && (lane & (lpc - 1)) == 0) {
+                    const uint32_t ci = (off >> A.S_l2) - ((pos >> A.S_l2) & ~15u);
+                    tuft_cur = (uint32_t)wd[A.win_bytes + ci] | ((uint32_t)wd[2 * A.win_bytes + ci] << 8) |
+                               ((uint32_t)wd[3 * A.win_bytes + ci] << 16) | ((uint32_t)wd[4 * A.win_bytes + ci] << 24);
+                }
+            }
+        } else {
+            act0 = prefetch_act(A, off, on, lane);
+            if (ch == 0) tuft_cur = prefetch_tuft<TUFT>(A, off, on, lane);
+        }
         uint4 str4{}, st4{}, fl4{}, nst4{};
         if (on) {
             str4 = *(const uint4*)(sb + arr_off<MODE>(0, SB) + so);
@@ -506,7 +551,7 @@ __device__ __forceinline__ void tma_body(const FusedTuftArgs& A, uint8_t* smem, 
     const int lane = tid & 31;
     const int wib = tid >> 5;
     const uint32_t SB = A.stage_bytes;
-    const uint32_t buf_bytes = (MODE == 0 ? 5u : 6u) * SB;
+    const uint32_t buf_bytes = A.stage_stride;
     const uint32_t nst = A.nst;
 
     if (wib == kWarps) {
@@ -516,18 +561,33 @@ __device__ __forceinline__ void tma_body(const FusedTuftArgs& A, uint8_t* smem, 
         uint64_t issued = 0;
         for (uint32_t t = blockIdx.x; t < A.n_tiles && !s_abort; t += gridDim.x) {
             const TileGeo G = tile_geo(A, t);
-            for (uint64_t pos = G.syn0; pos < G.syn_end; pos += SB) {
+            for (uint32_t pos = G.syn0; pos < G.syn_end; pos += SB) {
                 if (s_abort) break;
                 // Buffer pb's previous use (round pround - 1) must be released.
                 if (pround > 0 && !mbar_wait(&empty[pb], (pround - 1) & 1)) {
                     s_abort = 1;
                     break;
                 }
-                const uint64_t left = G.syn_end - pos;
-                const uint32_t nb = left < SB ? (uint32_t)left : SB;
+                const uint32_t left = G.syn_end - pos;
+                const uint32_t nb = left < SB ? left : SB;
                 uint8_t* dst = stages + (size_t)pb * buf_bytes;
-                const uint32_t n_arr_bytes = (MODE == 0 ? 2 * nb : 3 * nb) + nb + nb + (FCLEAN ? 0 : nb);
+                uint32_t n_arr_bytes = (MODE == 0 ? 2 * nb : 3 * nb) + nb + nb + (FCLEAN ? 0 : nb);
+                // Windows of the stage's dendrites and cells, widened to 16-byte bounds.
+                const uint32_t d0 = (pos >> A.spd_l2) & ~15u, d1 = (((pos + nb) >> A.spd_l2) + 15) & ~15u;
+                const uint32_t c0 = (pos >> A.S_l2) & ~15u, c1 = (((pos + nb) >> A.S_l2) + 15) & ~15u;
+                if (A.win) n_arr_bytes += (uint32_t)(d1 - d0) + (TUFT ? 4 * (uint32_t)(c1 - c0) : 0u);
                 mbar_arrive_expect_tx(&full[pb], n_arr_bytes);
+                if (A.win) {
+                    uint8_t* wd = dst + 6 * SB;
+                    bulk_g2s(wd, A.den_act + d0, (uint32_t)(d1 - d0), &full[pb]);
+                    if (TUFT) {
+                        const uint32_t cb = (uint32_t)(c1 - c0);
+                        bulk_g2s(wd + A.win_bytes, A.t_bid + c0, cb, &full[pb]);
+                        bulk_g2s(wd + 2 * A.win_bytes, A.t_braw + c0, cb, &full[pb]);
+                        bulk_g2s(wd + 3 * A.win_bytes, A.t_bst + c0, cb, &full[pb]);
+                        bulk_g2s(wd + 4 * A.win_bytes, A.t_st + c0, cb, &full[pb]);
+                    }
+                }
                 if (MODE == 0) {
                     bulk_g2s(dst, A.gidx + pos, 2 * nb, &full[pb]);
                 } else {
@@ -564,8 +624,8 @@ __device__ __forceinline__ void tma_body(const FusedTuftArgs& A, uint8_t* smem, 
         if (s_abort) break;
         build_footprint(A, G, halo, wib * 32 + lane);
         consumers_sync();
-        const uint32_t n_units_tile = cpu > 1 ? G.h * G.w : (uint32_t)((G.syn_end - G.syn0 + 511) >> 9);
-        for (uint64_t pos = G.syn0; pos < G.syn_end; pos += SB) {
+        const uint32_t n_units_tile = cpu > 1 ? G.h * G.w : (G.syn_end - G.syn0 + 511) >> 9;
+        for (uint32_t pos = G.syn0; pos < G.syn_end; pos += SB) {
             bool got = !s_abort && mbar_wait(&full[cb], cphase);
             got = __all_sync(0xFFFFFFFFu, got);
             if (!got) {
@@ -731,7 +791,10 @@ int prepare_fused(FusedArea& F, const bm_area_plan& P, std::string* err) {
             const uint64_t fsz = frows * fw;
             const uint64_t halo = (uint64_t)nrec * fsz;
             if (halo >= 32768) continue;   // gather offsets are 16-bit
-            const uint32_t buf_bytes = 6 * SB;
+            // Windows: up to SB / 16 dendrites (or cells) per stage, widened by 16
+            // at both ends.
+            const uint32_t win_bytes = SB / 16 + 32;
+            const uint32_t buf_bytes = 6 * SB + 5 * win_bytes;
             uint32_t nst = (uint32_t)std::max<uint64_t>(2, std::min<uint64_t>(4, (80 * 1024) / buf_bytes));
             const uint64_t halo_off = 128 + (uint64_t)nst * buf_bytes;
             const uint64_t smem = halo_off + ((halo + 15) / 16) * 16;
@@ -746,6 +809,9 @@ int prepare_fused(FusedArea& F, const bm_area_plan& P, std::string* err) {
             FT.fsz = (uint32_t)fsz;
             FT.nst = nst;
             FT.stage_bytes = SB;
+            FT.stage_stride = buf_bytes;
+            FT.win_bytes = win_bytes;
+            FT.win = (T.den_idz % 16) == 0 && (T.cel_idz % 16) == 0;
             FT.halo_off = (uint32_t)halo_off;
             FT.smem = (uint32_t)smem;
             FT.src_vs = vs;
@@ -873,6 +939,9 @@ void launch_fused_tuft(const FusedArea& F, const uint8_t* axns, const SliceRec* 
         A.stage_bytes = FT.stage_bytes;
         A.halo_off = FT.halo_off;
         A.unit_l2 = 9 + ilog2(A.chunks_per_unit);
+        A.stage_stride = FT.stage_stride;
+        A.win = FT.win;
+        A.win_bytes = FT.win_bytes;
         auto kern = tuft ? k_fused_tuft_tma<true> : k_fused_tuft_tma<false>;
         kern<<<FT.grid, kThreads, FT.smem, s>>>(A);
     } else {

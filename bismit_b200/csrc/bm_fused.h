@@ -22,6 +22,9 @@ struct FusedTuft {
     uint32_t nst = 2;        // TMA pipeline stages
     uint32_t stage_bytes = 0;
     uint32_t halo_off = 0;   // halo offset in dynamic shared memory
+    uint32_t stage_stride = 0;   // bytes per ring buffer
+    uint32_t win_bytes = 0;      // bytes per dendrite / cell-tuft window
+    bool win = false;            // windows ride in the stages (16-byte aligned ranges)
     uint32_t src_vs = 0, src_us = 0, src_vsz = 0, src_usz = 0;
     uint32_t src_idz[8] = {};
 };
