@@ -18,18 +18,19 @@ using namespace bm;
 
 namespace {
 
-thread_local std::string g_err;
+thread_local char g_err[1024];
 
-int set_err(int code, const char* fmt, ...) __attribute__((format(printf, 2, 3)));
-int set_err(int code, const char* fmt, ...) {
-    char buf[1024];
+}  // namespace
+
+int bm::set_err(int code, const char* fmt, ...) {
     va_list ap;
     va_start(ap, fmt);
-    vsnprintf(buf, sizeof buf, fmt, ap);
+    vsnprintf(g_err, sizeof g_err, fmt, ap);
     va_end(ap);
-    g_err = buf;
     return code;
 }
+
+namespace {
 
 int cuda_err(cudaError_t e, const char* what) {
     return set_err(e == cudaErrorMemoryAllocation ? BM_ERR_OOM : BM_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
@@ -264,43 +265,63 @@ bool buf_range(bm_area_s* A, uint32_t kind, uint32_t layer, uint64_t offset, uin
     return true;
 }
 
+}  // namespace
+
+void bm::fill_dev_layer(DevLayer& D, const bm_area_plan& P, uint32_t i, uint8_t* slab) {
+    const bm_layer_plan& L = P.layers[i];
+    std::memset(&D, 0, sizeof D);
+    D.kind = L.kind;
+    D.depth = L.depth;
+    D.v_size = L.v_size;
+    D.u_size = L.u_size;
+    D.cells = L.cells;
+    D.base_slc = L.base_axn_slc;
+    D.axn_idz = L.axn_idz;
+    D.n_tufts = L.n_tufts;
+    D.enabled_flags = L.enabled_tft_flags;
+    D.prx_id = L.bsl_prx_tft_id;
+    D.dst_id = L.bsl_dst_tft_id;
+    D.apc_id = L.apc_dst_tft_id;
+    D.n_syns = L.n_syns;
+    for (int k = 0; k < BM_BUF_COUNT; k++)
+        D.buf[k] = L.buf_off[k] == UINT64_MAX ? nullptr : slab + L.buf_off[k];
+    for (uint32_t t = 0; t < L.n_tufts; t++) {
+        const bm_tuft_plan& T = L.tufts[t];
+        DevTuft& DT = D.tft[t];
+        DT.dpt = T.dens_per_tft;
+        DT.spd = T.syns_per_den;
+        DT.spt = T.syns_per_tft;
+        DT.mad_l2 = T.max_active_dens_l2;
+        DT.thresh = T.den_threshold;
+        DT.den_kind = T.den_kind;
+        DT.syn_idz = T.syn_idz;
+        DT.den_idz = T.den_idz;
+        DT.cel_idz = T.cel_idz;
+        DT.rnd_key_den = rnd_key(P.rnd_seed, P.area_id, L.layer_id, BM_RND_DEN_CYCLE, t);
+        DT.rnd_key_mtp = rnd_key(P.rnd_seed, P.area_id, L.layer_id, BM_RND_TFT_DST_MTP, t);
+    }
+    D.rnd_key_ssc_mtp = rnd_key(P.rnd_seed, P.area_id, L.layer_id, BM_RND_SSC_MTP, 0);
+}
+
+void bm::fill_slice_table(const bm_area_plan& P, SliceRec* out) {
+    for (uint32_t k = 0; k < BM_MAX_SLICES; k++) {
+        SliceRec r{0, 0, 0, 0};
+        if (k < P.n_slices) {
+            r.x = P.slc_axn_idz[k];
+            r.y = P.slc_v_size[k] | (P.slc_u_size[k] << 16);
+            r.z = P.slc_v_scale[k] | (P.slc_u_scale[k] << 8) | (P.slc_v_mid[k] << 16) | (P.slc_u_mid[k] << 24);
+        }
+        out[k] = r;
+    }
+}
+
+namespace {
+
 void build_dev_layers(bm_area_s* A) {
     const bm_area_plan& P = A->plan;
     for (uint32_t i = 0; i < P.n_layers; i++) {
         const bm_layer_plan& L = P.layers[i];
-        DevLayer& D = A->dl[i];
-        std::memset(&D, 0, sizeof D);
-        D.kind = L.kind;
-        D.depth = L.depth;
-        D.v_size = L.v_size;
-        D.u_size = L.u_size;
-        D.cells = L.cells;
-        D.base_slc = L.base_axn_slc;
-        D.axn_idz = L.axn_idz;
-        D.n_tufts = L.n_tufts;
-        D.enabled_flags = L.enabled_tft_flags;
-        D.prx_id = L.bsl_prx_tft_id;
-        D.dst_id = L.bsl_dst_tft_id;
-        D.apc_id = L.apc_dst_tft_id;
-        D.n_syns = L.n_syns;
-        for (int k = 0; k < BM_BUF_COUNT; k++)
-            D.buf[k] = L.buf_off[k] == UINT64_MAX ? nullptr : A->slab + L.buf_off[k];
-        for (uint32_t t = 0; t < L.n_tufts; t++) {
-            const bm_tuft_plan& T = L.tufts[t];
-            DevTuft& DT = D.tft[t];
-            DT.dpt = T.dens_per_tft;
-            DT.spd = T.syns_per_den;
-            DT.spt = T.syns_per_tft;
-            DT.mad_l2 = T.max_active_dens_l2;
-            DT.thresh = T.den_threshold;
-            DT.den_kind = T.den_kind;
-            DT.syn_idz = T.syn_idz;
-            DT.den_idz = T.den_idz;
-            DT.cel_idz = T.cel_idz;
-            DT.rnd_key_den = rnd_key(P.rnd_seed, P.area_id, L.layer_id, BM_RND_DEN_CYCLE, t);
-            DT.rnd_key_mtp = rnd_key(P.rnd_seed, P.area_id, L.layer_id, BM_RND_TFT_DST_MTP, t);
-        }
-        D.rnd_key_ssc_mtp = rnd_key(P.rnd_seed, P.area_id, L.layer_id, BM_RND_SSC_MTP, 0);
+        fill_dev_layer(A->dl[i], P, i, A->slab);
         for (uint32_t k = 0; k < L.n_ctrl; k++)
             A->inhib_key[i][k] = rnd_key(P.rnd_seed, P.area_id, L.ctrl[k].layer_id, BM_RND_INHIB, 0);
     }
@@ -324,7 +345,7 @@ void free_area(bm_area_s* A) {
 
 extern "C" {
 
-const char* bm_last_error(void) { return g_err.c_str(); }
+const char* bm_last_error(void) { return g_err; }
 
 const char* bm_version(void) { return "bismit_b200 0.1 (sm_100a)"; }
 
@@ -406,16 +427,7 @@ int bm_area_create(bm_ctx ctx, const bm_area_desc* desc, uint64_t seed, bm_area*
     if (e == cudaSuccess) e = cudaMalloc(&A->slices, sizeof(SliceRec) * BM_MAX_SLICES);
     if (e != cudaSuccess) { free_area(A); return cuda_err(e, "cudaMalloc"); }
     std::vector<SliceRec> tab(BM_MAX_SLICES);
-    for (uint32_t k = 0; k < BM_MAX_SLICES; k++) {
-        const bm_area_plan& P = A->plan;
-        SliceRec r{0, 0, 0, 0};
-        if (k < P.n_slices) {
-            r.x = P.slc_axn_idz[k];
-            r.y = P.slc_v_size[k] | (P.slc_u_size[k] << 16);
-            r.z = P.slc_v_scale[k] | (P.slc_u_scale[k] << 8) | (P.slc_v_mid[k] << 16) | (P.slc_u_mid[k] << 24);
-        }
-        tab[k] = r;
-    }
+    fill_slice_table(A->plan, tab.data());
     AreaCtl ctl0{};
     e = cudaMemsetAsync(A->slab, 0, A->plan.slab_bytes, s);
     if (e == cudaSuccess) e = cudaMemcpyAsync(A->slices, tab.data(), sizeof(SliceRec) * BM_MAX_SLICES, cudaMemcpyHostToDevice, s);

@@ -49,6 +49,7 @@ namespace {
 constexpr int kWarps = 8;                    // consumer warps per CTA (tiled form)
 constexpr int kThreads = (kWarps + 1) * 32;  // plus one producer warp
 constexpr int kMaxRecs = 8;                  // contiguous source slices served by the fast gathers
+constexpr uint32_t kMaxSmem = 110 * 1024;    // dynamic shared memory per CTA (two CTAs per SM)
 constexpr uint32_t kWaitLimit = 1u << 22;
 
 struct FusedTuftArgs {
@@ -723,123 +724,151 @@ inline bool pow2(uint64_t x) { return x && !(x & (x - 1)); }
 
 }  // namespace
 
-int prepare_fused(FusedArea& F, const bm_area_plan& P, std::string* err) {
-    int dev = 0;
+namespace {
+
+int device_sms() {
+    int dev = 0, sms = 148;
     cudaGetDevice(&dev);
-    int sms = 148;
     if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) sms = 148;
-    F.sms = sms;
-    for (uint32_t i = 0; i < P.n_layers; i++) {
-        const bm_layer_plan& L = P.layers[i];
-        bool aligned = true;
-        for (int k = 0; k < BM_BUF_COUNT; k++)
-            if (L.buf_off[k] != UINT64_MAX && (L.buf_off[k] % 16)) aligned = false;
-        for (uint32_t t = 0; t < L.n_tufts; t++) {
-            const bm_tuft_plan& T = L.tufts[t];
+    return sms;
+}
+
+// Launch parameters of tuft t of data layer i (gidx left null).
+void plan_tuft(FusedTuft& FT, const bm_area_plan& P, uint32_t i, uint32_t t, int sms) {
+    const bm_layer_plan& L = P.layers[i];
+    bool aligned = true;
+    for (int k = 0; k < BM_BUF_COUNT; k++)
+        if (L.buf_off[k] != UINT64_MAX && (L.buf_off[k] % 16)) aligned = false;
+    const bm_tuft_plan& T = L.tufts[t];
+    FT = FusedTuft{};
+    uint32_t spd = T.syns_per_den, dpt = T.dens_per_tft;
+    FT.ok = aligned && pow2(spd) && spd >= 16 && spd <= 512 && pow2(dpt) && (T.syn_idz % 16) == 0;
+    // Fast gathers serve the pool's distinct slices when their ids are
+    // contiguous and spatial (mid 0, where bismit's scalar and vec4 index
+    // forms agree); anything else takes the general per-synapse path.
+    uint32_t lo = 255, hi = 0;
+    for (uint32_t k = 0; k < T.n_src_uniq; k++) {
+        lo = std::min<uint32_t>(lo, T.src_uniq_slc_ids[k]);
+        hi = std::max<uint32_t>(hi, T.src_uniq_slc_ids[k]);
+    }
+    uint32_t nrec = (T.n_src_uniq && hi - lo + 1 <= (uint32_t)kMaxRecs) ? hi - lo + 1 : 0;
+    for (uint32_t k = 0; k < nrec; k++)
+        if (P.slc_v_mid[lo + k] || P.slc_u_mid[lo + k] || !P.slc_v_scale[lo + k]) nrec = 0;
+    FT.slc0 = nrec ? lo : 0;
+    FT.nrec = nrec;
+    if (!FT.ok) return;
+    // Tiled gathers: the recorded slices share one geometry; the
+    // footprint margin is the pool's largest offset.
+    bool same = nrec > 0;
+    for (uint32_t k = 1; k < nrec && same; k++) {
+        uint32_t a = lo, b = lo + k;
+        same = P.slc_v_size[a] == P.slc_v_size[b] && P.slc_u_size[a] == P.slc_u_size[b] &&
+               P.slc_v_scale[a] == P.slc_v_scale[b] && P.slc_u_scale[a] == P.slc_u_scale[b];
+    }
+    int rv = 0, ru = 0;
+    for (uint32_t k = 0; k < T.n_src_uniq && same; k++) {
+        int a, b;
+        uint8_t sid = T.src_uniq_slc_ids[k];
+        if (!offset_extent(T.src_uniq_reaches[k], P.slc_v_scale[sid], P.slc_u_scale[sid], &a, &b)) same = false;
+        rv = std::max(rv, a);
+        ru = std::max(ru, b);
+    }
+    if (!same) return;
+    const uint32_t S = T.syns_per_tft;
+    const uint32_t cpu = S > 512 ? S / 512 : 1;
+    const uint32_t SB = kWarps * cpu * 512;
+    const uint64_t n_syn = (uint64_t)L.cells * S;
+    uint64_t target = std::min<uint64_t>(32768, std::max<uint64_t>(4096, n_syn / ((uint64_t)sms * 16)));
+    uint64_t cells = std::max<uint64_t>(1, target / S);
+    uint32_t W, H;
+    if (cells >= L.u_size) {
+        W = L.u_size;
+        H = (uint32_t)std::min<uint64_t>(L.v_size, cells / L.u_size);
+    } else {
+        W = (uint32_t)cells;
+        H = 1;
+    }
+    const uint32_t vs = P.slc_v_scale[lo], us = P.slc_u_scale[lo];
+    const uint64_t frows = ((uint64_t)(H - 1) * vs + 15) / 16 + 1 + 2 * (uint64_t)rv;
+    const uint64_t fw = ((uint64_t)(W - 1) * us + 15) / 16 + 1 + 2 * (uint64_t)ru;
+    const uint64_t fsz = frows * fw;
+    const uint64_t halo = (uint64_t)nrec * fsz;
+    if (halo >= 32768) return;   // gather offsets are 16-bit
+    // Windows: up to SB / 16 dendrites (or cells) per stage, widened by 16
+    // at both ends.
+    const uint32_t win_bytes = SB / 16 + 32;
+    const uint32_t buf_bytes = 6 * SB + 5 * win_bytes;
+    uint32_t nst = (uint32_t)std::max<uint64_t>(2, std::min<uint64_t>(4, (80 * 1024) / buf_bytes));
+    const uint64_t halo_off = 128 + (uint64_t)nst * buf_bytes;
+    const uint64_t smem = halo_off + ((halo + 15) / 16) * 16;
+    if (smem > kMaxSmem) return;
+    FT.tiled = true;
+    FT.tile_w = W;
+    FT.tile_h = H;
+    FT.rv = rv;
+    FT.ru = ru;
+    FT.fw = (uint32_t)fw;
+    FT.frows = (uint32_t)frows;
+    FT.fsz = (uint32_t)fsz;
+    FT.nst = nst;
+    FT.stage_bytes = SB;
+    FT.stage_stride = buf_bytes;
+    FT.win_bytes = win_bytes;
+    FT.win = (T.den_idz % 16) == 0 && (T.cel_idz % 16) == 0;
+    FT.halo_off = (uint32_t)halo_off;
+    FT.smem = (uint32_t)smem;
+    FT.src_vs = vs;
+    FT.src_us = us;
+    FT.src_vsz = P.slc_v_size[lo];
+    FT.src_usz = P.slc_u_size[lo];
+    for (uint32_t k = 0; k < nrec; k++) FT.src_idz[k] = P.slc_axn_idz[lo + k];
+    // Persistent grid: as many CTAs as fit on the device at once.
+    const bool pyr = L.kind == BM_LYR_PYRAMIDAL;
+    auto kern = pyr ? k_fused_tuft_tma<true> : k_fused_tuft_tma<false>;
+    // The cap is a property of the kernel, shared by every area on the device:
+    // set it to the largest footprint any tuft may plan, never lower.
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMaxSmem);
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads, FT.smem) != cudaSuccess)
+        per_sm = 1;
+    const uint64_t n_tiles = (uint64_t)L.depth * ((L.u_size + W - 1) / W) * ((L.v_size + H - 1) / H);
+    FT.grid = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(n_tiles, (uint64_t)sms * std::max(per_sm, 1)));
+}
+
+}  // namespace
+
+int plan_fused(FusedArea& F, const bm_area_plan& P) {
+    F.sms = device_sms();
+    for (uint32_t i = 0; i < P.n_layers; i++)
+        for (uint32_t t = 0; t < P.layers[i].n_tufts; t++) plan_tuft(F.t[i][t], P, i, t, F.sms);
+    cudaGetLastError();
+    return BM_OK;
+}
+
+int plan_fused_tuft(FusedArea& F, const bm_area_plan& P, uint32_t layer, uint32_t t) {
+    F.sms = device_sms();
+    plan_tuft(F.t[layer][t], P, layer, t, F.sms);
+    cudaGetLastError();
+    return BM_OK;
+}
+
+int prepare_fused(FusedArea& F, const bm_area_plan& P, std::string* err) {
+    int rc = plan_fused(F, P);
+    if (rc != BM_OK) return rc;
+    // Compiled gather offsets: 2 bytes per synapse of every tiled tuft.
+    for (uint32_t i = 0; i < P.n_layers; i++)
+        for (uint32_t t = 0; t < P.layers[i].n_tufts; t++) {
             FusedTuft& FT = F.t[i][t];
-            FT = FusedTuft{};
-            uint32_t spd = T.syns_per_den, dpt = T.dens_per_tft;
-            FT.ok = aligned && pow2(spd) && spd >= 16 && spd <= 512 && pow2(dpt) && (T.syn_idz % 16) == 0;
-            // Fast gathers serve the pool's distinct slices when their ids are
-            // contiguous and spatial (mid 0, where bismit's scalar and vec4 index
-            // forms agree); anything else takes the general per-synapse path.
-            uint32_t lo = 255, hi = 0;
-            for (uint32_t k = 0; k < T.n_src_uniq; k++) {
-                lo = std::min<uint32_t>(lo, T.src_uniq_slc_ids[k]);
-                hi = std::max<uint32_t>(hi, T.src_uniq_slc_ids[k]);
-            }
-            uint32_t nrec = (T.n_src_uniq && hi - lo + 1 <= (uint32_t)kMaxRecs) ? hi - lo + 1 : 0;
-            for (uint32_t k = 0; k < nrec; k++)
-                if (P.slc_v_mid[lo + k] || P.slc_u_mid[lo + k] || !P.slc_v_scale[lo + k]) nrec = 0;
-            FT.slc0 = nrec ? lo : 0;
-            FT.nrec = nrec;
-            if (!FT.ok) continue;
-            // Tiled gathers: the recorded slices share one geometry; the
-            // footprint margin is the pool's largest offset.
-            bool same = nrec > 0;
-            for (uint32_t k = 1; k < nrec && same; k++) {
-                uint32_t a = lo, b = lo + k;
-                same = P.slc_v_size[a] == P.slc_v_size[b] && P.slc_u_size[a] == P.slc_u_size[b] &&
-                       P.slc_v_scale[a] == P.slc_v_scale[b] && P.slc_u_scale[a] == P.slc_u_scale[b];
-            }
-            int rv = 0, ru = 0;
-            for (uint32_t k = 0; k < T.n_src_uniq && same; k++) {
-                int a, b;
-                uint8_t sid = T.src_uniq_slc_ids[k];
-                if (!offset_extent(T.src_uniq_reaches[k], P.slc_v_scale[sid], P.slc_u_scale[sid], &a, &b)) same = false;
-                rv = std::max(rv, a);
-                ru = std::max(ru, b);
-            }
-            if (!same) continue;
-            const uint32_t S = T.syns_per_tft;
-            const uint32_t cpu = S > 512 ? S / 512 : 1;
-            const uint32_t SB = kWarps * cpu * 512;
-            const uint64_t n_syn = (uint64_t)L.cells * S;
-            uint64_t target = std::min<uint64_t>(32768, std::max<uint64_t>(4096, n_syn / ((uint64_t)sms * 16)));
-            uint64_t cells = std::max<uint64_t>(1, target / S);
-            uint32_t W, H;
-            if (cells >= L.u_size) {
-                W = L.u_size;
-                H = (uint32_t)std::min<uint64_t>(L.v_size, cells / L.u_size);
-            } else {
-                W = (uint32_t)cells;
-                H = 1;
-            }
-            const uint32_t vs = P.slc_v_scale[lo], us = P.slc_u_scale[lo];
-            const uint64_t frows = ((uint64_t)(H - 1) * vs + 15) / 16 + 1 + 2 * (uint64_t)rv;
-            const uint64_t fw = ((uint64_t)(W - 1) * us + 15) / 16 + 1 + 2 * (uint64_t)ru;
-            const uint64_t fsz = frows * fw;
-            const uint64_t halo = (uint64_t)nrec * fsz;
-            if (halo >= 32768) continue;   // gather offsets are 16-bit
-            // Windows: up to SB / 16 dendrites (or cells) per stage, widened by 16
-            // at both ends.
-            const uint32_t win_bytes = SB / 16 + 32;
-            const uint32_t buf_bytes = 6 * SB + 5 * win_bytes;
-            uint32_t nst = (uint32_t)std::max<uint64_t>(2, std::min<uint64_t>(4, (80 * 1024) / buf_bytes));
-            const uint64_t halo_off = 128 + (uint64_t)nst * buf_bytes;
-            const uint64_t smem = halo_off + ((halo + 15) / 16) * 16;
-            if (smem > 110 * 1024) continue;
-            FT.tiled = true;
-            FT.tile_w = W;
-            FT.tile_h = H;
-            FT.rv = rv;
-            FT.ru = ru;
-            FT.fw = (uint32_t)fw;
-            FT.frows = (uint32_t)frows;
-            FT.fsz = (uint32_t)fsz;
-            FT.nst = nst;
-            FT.stage_bytes = SB;
-            FT.stage_stride = buf_bytes;
-            FT.win_bytes = win_bytes;
-            FT.win = (T.den_idz % 16) == 0 && (T.cel_idz % 16) == 0;
-            FT.halo_off = (uint32_t)halo_off;
-            FT.smem = (uint32_t)smem;
-            FT.src_vs = vs;
-            FT.src_us = us;
-            FT.src_vsz = P.slc_v_size[lo];
-            FT.src_usz = P.slc_u_size[lo];
-            for (uint32_t k = 0; k < nrec; k++) FT.src_idz[k] = P.slc_axn_idz[lo + k];
-            // Persistent grid: as many CTAs as fit on the device at once.
-            const bool pyr = L.kind == BM_LYR_PYRAMIDAL;
-            auto kern = pyr ? k_fused_tuft_tma<true> : k_fused_tuft_tma<false>;
-            cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)FT.smem);
-            int per_sm = 0;
-            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads, FT.smem) != cudaSuccess)
-                per_sm = 1;
-            const uint64_t n_tiles = (uint64_t)L.depth * ((L.u_size + W - 1) / W) * ((L.v_size + H - 1) / H);
-            FT.grid = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(n_tiles, (uint64_t)sms * std::max(per_sm, 1)));
-            // Compiled gather offsets: 2 bytes per synapse of the tuft.
+            if (!FT.tiled) continue;
+            const uint64_t n_syn = (uint64_t)P.layers[i].cells * P.layers[i].tufts[t].syns_per_tft;
             if (cudaMalloc(&FT.gidx, n_syn * sizeof(int16_t)) != cudaSuccess) {
                 cudaGetLastError();
                 FT.gidx = nullptr;
-                FT.tiled = false;
                 if (err) *err = "cudaMalloc of the gather offsets failed";
                 free_fused(F);
                 return BM_ERR_OOM;
             }
         }
-    }
-    cudaGetLastError();
     return BM_OK;
 }
 
@@ -852,22 +881,25 @@ void free_fused(FusedArea& F) {
             }
 }
 
+void launch_compile_tuft(const FusedArea& F, const DevLayer& L, uint32_t layer, uint32_t t, AreaCtl* ctl,
+                         cudaStream_t s) {
+    const FusedTuft& FT = F.t[layer][t];
+    if (!FT.ok) return;
+    const DevTuft& T = L.tft[t];
+    unsigned int* status = &ctl->tuft_status[layer * BM_MAX_TUFTS + t];
+    cudaMemsetAsync(status, 0, sizeof(unsigned int), s);
+    const uint64_t n = (uint64_t)L.cells * T.spt;
+    const uint64_t threads = (n + 15) / 16;
+    const unsigned grid = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((threads + 255) / 256, (uint64_t)F.sms * 8));
+    k_compile_tuft<<<grid, 256, 0, s>>>(L.buf[BM_BUF_SYN_SRC_SLC_IDS] + T.syn_idz,
+                                        (const int8_t*)L.buf[BM_BUF_SYN_SRC_COL_V_OFFS] + T.syn_idz,
+                                        (const int8_t*)L.buf[BM_BUF_SYN_SRC_COL_U_OFFS] + T.syn_idz,
+                                        L.buf[BM_BUF_SYN_FLAG_SETS] + T.syn_idz, FT.tiled ? FT.gidx : nullptr, n,
+                                        FT.slc0, FT.nrec, FT.rv, FT.ru, FT.fw, FT.fsz, status);
+}
+
 void launch_verify_tufts(const FusedArea& F, const DevLayer& L, uint32_t layer, AreaCtl* ctl, cudaStream_t s) {
-    for (uint32_t t = 0; t < L.n_tufts; t++) {
-        const FusedTuft& FT = F.t[layer][t];
-        if (!FT.ok) continue;
-        const DevTuft& T = L.tft[t];
-        unsigned int* status = &ctl->tuft_status[layer * BM_MAX_TUFTS + t];
-        cudaMemsetAsync(status, 0, sizeof(unsigned int), s);
-        const uint64_t n = (uint64_t)L.cells * T.spt;
-        const uint64_t threads = (n + 15) / 16;
-        const unsigned grid = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((threads + 255) / 256, (uint64_t)F.sms * 8));
-        k_compile_tuft<<<grid, 256, 0, s>>>(L.buf[BM_BUF_SYN_SRC_SLC_IDS] + T.syn_idz,
-                                            (const int8_t*)L.buf[BM_BUF_SYN_SRC_COL_V_OFFS] + T.syn_idz,
-                                            (const int8_t*)L.buf[BM_BUF_SYN_SRC_COL_U_OFFS] + T.syn_idz,
-                                            L.buf[BM_BUF_SYN_FLAG_SETS] + T.syn_idz, FT.tiled ? FT.gidx : nullptr, n,
-                                            FT.slc0, FT.nrec, FT.rv, FT.ru, FT.fw, FT.fsz, status);
-    }
+    for (uint32_t t = 0; t < L.n_tufts; t++) launch_compile_tuft(F, L, layer, t, ctl, s);
 }
 
 void launch_fused_tuft(const FusedArea& F, const uint8_t* axns, const SliceRec* slices, const DevLayer& L,

@@ -38,6 +38,10 @@ struct FusedArea {
 // two in 16..512, dens_per_tft a power of two, 16-byte aligned ranges) and
 // its gather form. Tufts that do not qualify run the plain per-stage kernels.
 int prepare_fused(FusedArea& F, const bm_area_plan& P, std::string* err);
+// The same decisions without allocating (gidx pointers left null), for every
+// tuft of the area or for one.
+int plan_fused(FusedArea& F, const bm_area_plan& P);
+int plan_fused_tuft(FusedArea& F, const bm_area_plan& P, uint32_t layer, uint32_t t);
 void free_fused(FusedArea& F);
 // Synapse flags + synapse cycle + dendrite cycle (+ tuft cycle for pyramidal
 // layers) of one tuft in one launch.
@@ -46,5 +50,7 @@ void launch_fused_tuft(const FusedArea& F, const uint8_t* axns, const SliceRec* 
 // Recomputes AreaCtl::tuft_status for the fused tufts of a layer (after its
 // synapse sources or flags were written by the caller).
 void launch_verify_tufts(const FusedArea& F, const DevLayer& L, uint32_t layer, AreaCtl* ctl, cudaStream_t s);
+void launch_compile_tuft(const FusedArea& F, const DevLayer& L, uint32_t layer, uint32_t t, AreaCtl* ctl,
+                         cudaStream_t s);
 
 }  // namespace bm

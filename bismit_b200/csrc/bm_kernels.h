@@ -20,6 +20,13 @@ struct GrowTuft {
     uint32_t unique, zero_strength;
 };
 
+// Stores the calling thread's error message (bm_last_error) and returns `code`.
+int set_err(int code, const char* fmt, ...) __attribute__((format(printf, 2, 3)));
+// Device view of data layer i of a state slab laid out by plan P.
+void fill_dev_layer(DevLayer& D, const bm_area_plan& P, uint32_t i, uint8_t* slab);
+// Device slice records of plan P, BM_MAX_SLICES entries (zero past n_slices).
+void fill_slice_table(const bm_area_plan& P, SliceRec* out);
+
 void launch_grow(const DevLayer& L, const GrowTuft& G, cudaStream_t s);
 void launch_cycle_end(AreaCtl* ctl, cudaStream_t s);
 
