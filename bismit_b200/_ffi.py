@@ -199,6 +199,7 @@ def lib():
         "bm_area_get_profile": (C.c_int, [vp, u32, P(C.c_char_p), P(u64), P(C.c_double), P(u32)]),
         "bm_area_reset_profile": (C.c_int, [vp]),
         "bm_area_launches_per_cycle": (C.c_int, [vp, P(u32)]),
+        "bm_tuft_cycle_static": (C.c_int, [P(bm_area_plan), u32, u32, vp, u64, vp, vp]),
         "bm_rnd": (i32, [u64, u32, u32, u32, u32, u64]),
     }
     for name, (res, args) in sigs.items():

@@ -370,6 +370,41 @@ int bm_area_reset_profile(bm_area area);
 /* Number of kernel launches bm_area_cycle issues per cycle for this area. */
 int bm_area_launches_per_cycle(bm_area area, uint32_t* out);
 
+/* One tuft's stage of a cycle -- synapse flags, synapse cycle, dendrite cycle,
+ * and for pyramidal layers the tuft cycle -- on a state slab the CALLER owns,
+ * without allocating any device memory. No counterpart in the reference: bismit
+ * allocates every buffer when the area is built and has no such mode.
+ *
+ * For callers that must not allocate: a host whose device memory all comes
+ * from its own pooling allocator (a foreign cudaMalloc would fail against its
+ * reserve or escape its accounting), a real-time loop that cannot take
+ * cudaMalloc's latency or cudaFree's implicit device synchronisation, or a
+ * plugin handed pre-allocated buffers only. Such a caller resolves the plan
+ * with bm_plan_resolve (host only), allocates plan->slab_bytes itself and
+ * passes the slab here with the current device set.
+ *
+ * `slab` is the device state laid out by `plan` (inputs and outputs both
+ * live there: axons, synapse sources, strengths and flags are read; synapse
+ * states and flags, dendrite states and activities and the tuft's cell-tuft
+ * buffers are written). `cycle` is the cycle number the per-launch random
+ * value is drawn for (bm_rnd). `dev_error_out`, if not NULL, is a device word
+ * the call sets to its device error bits (bit 0: a bounded wait gave up).
+ * Work is queued on `stream` (NULL: the default stream); the call does not
+ * wait for it.
+ *
+ * Scratch: one library-held device array of about 8 MiB, reserved on every
+ * device that loads the library until the process exits. It limits a call to
+ * tufts of at most 4,194,304 synapses (cells * syns_per_tft); larger tufts
+ * get BM_ERR_INVALID, and tufts outside the fused kernel's shapes
+ * BM_ERR_UNSUPPORTED. The first call on a device looks up the array's device
+ * address (cudaGetSymbolAddress, which may load the module); make that first
+ * call before any stream capture. Every call shares the array and leaves its
+ * contents behind; the call re-initialises what it reads, but calls whose work
+ * overlaps on the GPU (different streams or threads, same device) race on
+ * it and must be serialised by the caller. Calls no cudaMalloc or cudaFree. */
+int bm_tuft_cycle_static(const bm_area_plan* plan, uint32_t layer, uint32_t tuft, void* slab,
+                         uint64_t cycle, uint32_t* dev_error_out, void* stream);
+
 /* The per-launch random value the host would draw for (layer, role, tuft) at
  * `cycle` (replaces the SmallRng draws of src/cortex/dendrites.rs:198,
  * src/cortex/tufts.rs:312, src/cortex/spiny_stellates.rs:259,
