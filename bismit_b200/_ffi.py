@@ -200,6 +200,15 @@ def lib():
         "bm_area_reset_profile": (C.c_int, [vp]),
         "bm_area_launches_per_cycle": (C.c_int, [vp, P(u32)]),
         "bm_tuft_cycle_static": (C.c_int, [P(bm_area_plan), u32, u32, vp, u64, vp, vp]),
+        "bm_batch_create": (C.c_int, [vp, P(vp), u32, P(vp)]),
+        "bm_batch_destroy": (C.c_int, [vp]),
+        "bm_batch_set_graph": (C.c_int, [vp, C.c_int]),
+        "bm_batch_cycle": (C.c_int, [vp, u32]),
+        "bm_batch_frame_bytes": (C.c_int, [vp, P(u64)]),
+        "bm_batch_cycle_frames_device": (C.c_int, [vp, vp, u32]),
+        "bm_batch_launches_per_cycle": (C.c_int, [vp, P(u32)]),
+        "bm_batch_device_errors": (C.c_int, [vp, P(u32)]),
+        "bm_batch_autotune": (C.c_int, [vp, C.c_char_p, P(u32)]),
         "bm_rnd": (i32, [u64, u32, u32, u32, u32, u64]),
     }
     for name, (res, args) in sigs.items():

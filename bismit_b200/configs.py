@@ -66,6 +66,53 @@ def benchmark_area(side, ssc_syns, pyr_depth, prox_dens, prox_syns, prox_reach, 
     return lmaps, areas
 
 
+def instance_area(side, depth, dens, syns, name="v1"):
+    """One instance of the batched workload: the benchmark layer map with the
+    64 x 64 area's shapes (spiny stellate 1 x 32, proximal 1 x 1 reach 0) on a
+    `side` x `side` grid, pyramidal depth `depth` and a distal tuft of
+    `dens` x `syns` (reach 6, max_active_dens_l2 = 3)."""
+    lmaps = LayerMapSchemeList()
+    areas = AreaSchemeList()
+    _external(lmaps, areas, "v0", side)
+    lm = LayerMapScheme("visual", LayerMapKind.Cortical)
+    lm.layer(LayerScheme.define("aff_in").axonal(AxonTopology.Spatial)
+             .axon_domain(AxonDomain.input([(InputTrack.Afferent, [THAL_SP])])))
+    lm.layer(LayerScheme.define("iv").depth(1).tags(LayerTags.PSAL).axon_domain(AxonDomain.Local)
+             .cellular(CellScheme.spiny_stellate()
+                       .tft(TuftScheme.basal().proximal().syns_per_den(32)
+                            .src_lyr(TuftSourceLayer.define("aff_in").syn_reach(6).prevalence(1)))))
+    lm.layer(LayerScheme.define("iv_inhib")
+             .cellular(CellScheme.control(ControlCellKind.InhibitoryBasketSurround("iv", 4), 0)))
+    lm.layer(LayerScheme.define("iii").depth(depth).tags(LayerTags.PTAL)
+             .axon_domain(AxonDomain.output([THAL_SP]))
+             .cellular(CellScheme.pyramidal()
+                       .tft(TuftScheme.basal().proximal().dens_per_tft(1).syns_per_den(1)
+                            .src_lyr(TuftSourceLayer.define("iv").syn_reach(0).prevalence(1)))
+                       .tft(TuftScheme.basal().distal().dens_per_tft(dens).syns_per_den(syns)
+                            .max_active_dens_l2(3)
+                            .src_lyr(TuftSourceLayer.define("iii").syn_reach(6).prevalence(1)))))
+    lm.layer(LayerScheme.define("iii_col")
+             .cellular(CellScheme.control(ControlCellKind.IntraColumnInhib("iii"), 0)))
+    lmaps.add(lm)
+    areas.area(AreaScheme(name, "visual", side).eff_areas(["v0"]))
+    return lmaps, areas
+
+
+def batch_instances(n=64, seed=0, sides=range(32, 193, 16)):
+    """The batched workload: n independent instances, each drawn from a
+    stream seeded by (seed, index): side uniform over `sides`, pyramidal depth
+    1..4, distal dendrites per tuft from {8, 16}, synapses per dendrite from
+    {16, 32, 64}, input activity uniform in [0.01, 0.04].
+    Returns [(side, depth, dens, syns, active)]."""
+    sides = list(sides)
+    out = []
+    for i in range(n):
+        rng = np.random.default_rng([int(seed) & 0xFFFFFFFF, 0x62617463, i])
+        out.append((int(sides[rng.integers(len(sides))]), int(rng.integers(1, 5)), int((8, 16)[rng.integers(2)]),
+                    int((16, 32, 64)[rng.integers(3)]), float(rng.uniform(0.01, 0.04))))
+    return out
+
+
 def bench_settings():
     return CorticalAreaSettings().disable_regrowth().strengths_start_at_zero()
 

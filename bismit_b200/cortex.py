@@ -176,6 +176,72 @@ class CorticalArea:
             pass
 
 
+class Batch:
+    """Areas of one layer map (uneven sizes allowed) cycled together: one
+    launch per stage step for all of them, the cycle replayed from a CUDA
+    graph (bm_batch_*, include/bismit_b200.h). Each area's bytes after a
+    batched cycle equal its bytes after cycling it alone."""
+
+    def __init__(self, ctx, areas, graph=True):
+        self.lib = F.lib()
+        self.ctx = ctx
+        self.areas = list(areas)
+        hs = (C.c_void_p * len(self.areas))(*[a.h.value for a in self.areas])
+        self.h = C.c_void_p()
+        F.check(self.lib.bm_batch_create(ctx.h, hs, len(self.areas), C.byref(self.h)))
+        if not graph:
+            self.set_graph(False)
+
+    def set_graph(self, on):
+        F.check(self.lib.bm_batch_set_graph(self.h, 1 if on else 0))
+
+    def cycle(self, n=1):
+        F.check(self.lib.bm_batch_cycle(self.h, int(n)))
+
+    def frame_bytes(self):
+        v = C.c_uint64()
+        F.check(self.lib.bm_batch_frame_bytes(self.h, C.byref(v)))
+        return v.value
+
+    def cycle_frames_device(self, dev_ptr, n):
+        """n cycles; cycle k first takes its frame block (input 0 of every area,
+        packed in batch order) from dev_ptr + k * frame_bytes()."""
+        F.check(self.lib.bm_batch_cycle_frames_device(self.h, C.c_void_p(dev_ptr), int(n)))
+
+    def pack_frames(self, per_area_frames):
+        """Host-side packing: per_area_frames[a] is an (n, len_a) array; returns
+        the (n, frame_bytes) array cycle_frames_device expects."""
+        return np.ascontiguousarray(np.concatenate([np.asarray(f, np.uint8) for f in per_area_frames], axis=1))
+
+    def launches_per_cycle(self):
+        v = C.c_uint32()
+        F.check(self.lib.bm_batch_launches_per_cycle(self.h, C.byref(v)))
+        return v.value
+
+    def device_errors(self):
+        v = C.c_uint32()
+        rc = self.lib.bm_batch_device_errors(self.h, C.byref(v))
+        if rc not in (F.BM_OK, F.BM_ERR_TIMEOUT):
+            F.check(rc)
+        return v.value
+
+    def autotune(self, cache_path=None):
+        n = C.c_uint32()
+        F.check(self.lib.bm_batch_autotune(self.h, cache_path.encode() if cache_path else None, C.byref(n)))
+        return n.value
+
+    def close(self):
+        if self.h:
+            self.lib.bm_batch_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 class Cortex:
     """A set of cortical areas cycled in order (Cortex, src/cortex/cortex.rs:37-120)."""
 

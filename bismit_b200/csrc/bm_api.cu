@@ -10,8 +10,7 @@
 #include <string>
 #include <vector>
 
-#include "bm_fused.h"
-#include "bm_kernels.h"
+#include "bm_area.h"
 #include "bm_layout.h"
 
 using namespace bm;
@@ -30,11 +29,11 @@ int bm::set_err(int code, const char* fmt, ...) {
     return code;
 }
 
-namespace {
-
-int cuda_err(cudaError_t e, const char* what) {
+int bm::cuda_err(cudaError_t e, const char* what) {
     return set_err(e == cudaErrorMemoryAllocation ? BM_ERR_OOM : BM_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
 }
+
+namespace {
 
 #define CU(call)                                                   \
     do {                                                           \
@@ -42,211 +41,150 @@ int cuda_err(cudaError_t e, const char* what) {
         if (e_ != cudaSuccess) return cuda_err(e_, #call);         \
     } while (0)
 
-// Kernel kinds for per-launch timing.
-enum Kind {
-    K_SYN_FLAGS, K_SYN_CYCLE, K_DEN_CYCLE, K_TFT_CYCLE, K_SSC_CYCLE, K_INHIB_SIMPLE, K_INHIB_PASS,
-    K_SSC_MTP, K_PYR_CYCLE, K_PYR_OUTPUT, K_INTRA_COL, K_TFT_DST_MTP, K_CYCLE_END, K_INTAKE,
-    K_FUSED_TUFT, K_FUSED_SSC_SOMA, K_FUSED_PYR_SOMA, K_FUSED_SSC_MTP, K_COUNT
-};
-const char* const kKindNames[K_COUNT] = {
-    "tft_set_syn_flags", "syn_cycle", "den_cycle_tft", "tft_cycle", "ssc_cycle", "inhib_simple",
-    "inhib_passthrough", "ssc_mtp_simple", "pyr_cycle", "pyr_output", "inhib_intra_column", "tft_dst_mtp",
-    "cycle_end", "intake", "fused_tuft_cycle", "fused_ssc_soma_inhib", "fused_pyr_soma_learn",
-    "fused_ssc_mtp"};
-
-struct DevGuard {
-    int prev = -1;
-    explicit DevGuard(int dev) {
-        cudaGetDevice(&prev);
-        if (prev != dev) cudaSetDevice(dev);
-    }
-    ~DevGuard() {
-        int cur;
-        cudaGetDevice(&cur);
-        if (prev >= 0 && cur != prev) cudaSetDevice(prev);
-    }
-};
-
 }  // namespace
 
-struct bm_ctx_s {
-    int device = 0;
-    cudaStream_t own = nullptr;
-    cudaStream_t user = nullptr;
-    bool user_set = false;
-    cudaStream_t stream() const { return user_set ? user : own; }
-};
-
-struct bm_area_s {
-    bm_ctx ctx = nullptr;
-    bm_area_plan plan;
-    uint8_t* slab = nullptr;
-    AreaCtl* ctl = nullptr;
-    SliceRec* slices = nullptr;
-    DevLayer dl[BM_MAX_LAYERS];
-    uint64_t inhib_key[BM_MAX_LAYERS][BM_MAX_CTRL];
-    uint64_t host_cycle = 0;
-    bool verify_pending[BM_MAX_LAYERS] = {};   // sources or flags written since the last check
-    uint32_t exec_path = BM_PATH_FUSED;
-    FusedArea fused;
-    bool profiling = false;
-    struct Rec { int kind; cudaEvent_t a, b; };
-    std::vector<Rec> pending;
-    std::vector<cudaEvent_t> pool;
-    uint64_t prof_launches[K_COUNT] = {};
-    double prof_ms[K_COUNT] = {};
-    uint32_t launches = 0;   // kernel launches of the last enqueued cycle
-
-    cudaStream_t stream() const { return ctx->stream(); }
-    uint8_t* axns() const { return slab + plan.axon_off; }
-
-    cudaEvent_t ev() {
-        if (!pool.empty()) { cudaEvent_t e = pool.back(); pool.pop_back(); return e; }
-        cudaEvent_t e = nullptr;
-        cudaEventCreate(&e);
-        return e;
-    }
-    template <class F> void run(int kind, F&& f) {
-        if (kind != K_INTAKE) launches++;
-        if (!profiling) { f(); return; }
-        Rec r{kind, ev(), ev()};
-        cudaEventRecord(r.a, stream());
-        f();
-        cudaEventRecord(r.b, stream());
-        pending.push_back(r);
-    }
-    void drain_profile() {
-        for (auto& r : pending) {
-            float ms = 0.f;
-            cudaEventSynchronize(r.b);
-            cudaEventElapsedTime(&ms, r.a, r.b);
-            prof_launches[r.kind]++;
-            prof_ms[r.kind] += ms;
-            pool.push_back(r.a);
-            pool.push_back(r.b);
-        }
-        pending.clear();
-    }
-};
-
+// ------------------------------------------------------- stage program ---
 namespace {
 
-// Control layers hosted on data layer i, in (host, exe_order) order.
-void enqueue_controls(bm_area_s* A, uint32_t i) {
+void push_controls(const bm_area_s* A, uint32_t i, std::vector<Step>& out) {
     const bm_layer_plan& L = A->plan.layers[i];
-    const DevLayer& D = A->dl[i];
-    cudaStream_t s = A->stream();
     for (uint32_t k = 0; k < L.n_ctrl; k++) {
-        const bm_ctrl_plan& C = L.ctrl[k];
-        if (C.kind == BM_LYR_CTRL_INHIB_BASKET) {
-            if (A->plan.settings & BM_SET_BYPASS_INHIB)
-                A->run(K_INHIB_PASS, [&] { launch_inhib_passthrough(A->axns(), A->slices, D, s); });
-            else
-                A->run(K_INHIB_SIMPLE, [&] {
-                    launch_inhib_simple(A->axns(), A->slices, D, (int)C.field_radius, A->inhib_key[i][k], A->ctl, s);
-                });
-        } else if (C.kind == BM_LYR_CTRL_PYR_OUTPUT) {
-            A->run(K_PYR_OUTPUT, [&] { launch_pyr_output(A->axns(), A->slices, D, s); });
-        } else if (C.kind == BM_LYR_CTRL_INTRA_COLUMN) {
-            A->run(K_INTRA_COL, [&] { launch_inhib_intra_column_plain(A->axns(), A->slices, D, s); });
-        }
+        const uint32_t kind = L.ctrl[k].kind;
+        uint8_t st;
+        if (kind == BM_LYR_CTRL_INHIB_BASKET)
+            st = (A->plan.settings & BM_SET_BYPASS_INHIB) ? ST_INHIB_PASS : ST_INHIB_SIMPLE;
+        else if (kind == BM_LYR_CTRL_PYR_OUTPUT)
+            st = ST_PYR_OUTPUT;
+        else if (kind == BM_LYR_CTRL_INTRA_COLUMN)
+            st = ST_INTRA_COL;
+        else
+            continue;
+        out.push_back({st, (uint8_t)i, (uint8_t)k});
     }
 }
 
-void enqueue_dens_plain(bm_area_s* A, uint32_t i) {
-    const bm_layer_plan& L = A->plan.layers[i];
-    const DevLayer& D = A->dl[i];
-    cudaStream_t s = A->stream();
-    A->run(K_SYN_FLAGS, [&] { launch_set_syn_flags(D, s); });
-    for (uint32_t t = 0; t < L.n_tufts; t++)
-        A->run(K_SYN_CYCLE, [&] { launch_syn_cycle_plain(A->axns(), A->slices, D, t, s); });
-    for (uint32_t t = 0; t < L.n_tufts; t++)
-        A->run(K_DEN_CYCLE, [&] { launch_den_cycle_plain(D, t, A->ctl, s); });
-}
-
-void enqueue_pyr_learn(bm_area_s* A, uint32_t i) {
+void push_pyr_learn(const bm_area_s* A, uint32_t i, std::vector<Step>& out) {
     const bm_layer_plan& L = A->plan.layers[i];
     if (A->plan.settings & (BM_SET_DISABLE_LEARNING | BM_SET_DISABLE_PYRS)) return;
     for (uint32_t t = 0; t < L.n_tufts; t++)
-        if (L.tufts[t].den_kind == BM_DEN_DISTAL)
-            A->run(K_TFT_DST_MTP, [&] { launch_tft_dst_mtp_plain(A->axns(), A->dl[i], t, A->ctl, A->stream()); });
+        if (L.tufts[t].den_kind == BM_DEN_DISTAL) out.push_back({ST_DST_MTP, (uint8_t)i, (uint8_t)t});
 }
 
-// Synapse flags, synapse cycle, dendrite cycle and (pyramidal) tuft cycle of
-// every tuft. The plain form launches them as bismit does: flags over the
-// whole layer, then each stage per tuft. The fused form takes each tuft on its
-// own: one fused launch where the tuft qualifies, else that tuft's four stages.
-// The stages of different tufts touch disjoint buffers, so both orders give
-// the same bytes.
-void enqueue_tufts(bm_area_s* A, uint32_t i) {
+// SpinyStellateLayer::cycle (src/cortex/spiny_stellates.rs:220-252) and
+// PyramidalLayer::cycle (src/cortex/pyramidals.rs:297-335, learning included).
+void push_layer_cycle(const bm_area_s* A, uint32_t i, std::vector<Step>& out) {
     const bm_layer_plan& L = A->plan.layers[i];
-    const DevLayer& D = A->dl[i];
-    cudaStream_t s = A->stream();
-    const bool pyr = L.kind == BM_LYR_PYRAMIDAL;
-    if (A->exec_path == BM_PATH_PLAIN) {
-        enqueue_dens_plain(A, i);
-        if (pyr)
-            for (uint32_t t = 0; t < L.n_tufts; t++) A->run(K_TFT_CYCLE, [&] { launch_tft_cycle_plain(D, t, s); });
-        return;
-    }
-    for (uint32_t t = 0; t < L.n_tufts; t++) {
-        if (A->fused.t[i][t].ok) {
-            A->run(K_FUSED_TUFT, [&] { launch_fused_tuft(A->fused, A->axns(), A->slices, D, i, t, A->ctl, s); });
-        } else {
-            A->run(K_SYN_FLAGS, [&] { launch_set_syn_flags_tuft(D, t, s); });
-            A->run(K_SYN_CYCLE, [&] { launch_syn_cycle_plain(A->axns(), A->slices, D, t, s); });
-            A->run(K_DEN_CYCLE, [&] { launch_den_cycle_plain(D, t, A->ctl, s); });
-            if (pyr) A->run(K_TFT_CYCLE, [&] { launch_tft_cycle_plain(D, t, s); });
-        }
-    }
-}
-
-void enqueue_layer_cycle(bm_area_s* A, uint32_t i) {
-    const bm_layer_plan& L = A->plan.layers[i];
-    const DevLayer& D = A->dl[i];
-    cudaStream_t s = A->stream();
-    enqueue_tufts(A, i);
+    if (A->exec_path == BM_PATH_PLAIN)
+        out.push_back({ST_TUFTS_PLAIN, (uint8_t)i, 0});
+    else
+        for (uint32_t t = 0; t < L.n_tufts; t++) out.push_back({ST_TUFT, (uint8_t)i, (uint8_t)t});
     if (L.kind == BM_LYR_SPINY_STELLATE) {
-        A->run(K_SSC_CYCLE, [&] { launch_ssc_cycle(D, s); });
-        enqueue_controls(A, i);
+        out.push_back({ST_SSC_CYCLE, (uint8_t)i, 0});
+        push_controls(A, i, out);
     } else {
-        A->run(K_PYR_CYCLE, [&] { launch_pyr_cycle_plain(D, s); });
-        enqueue_controls(A, i);
-        enqueue_pyr_learn(A, i);
+        out.push_back({ST_PYR_CYCLE, (uint8_t)i, 0});
+        push_controls(A, i, out);
+        push_pyr_learn(A, i, out);
     }
 }
 
-void enqueue_layer_learn(bm_area_s* A, uint32_t i) {
+void push_layer_learn(const bm_area_s* A, uint32_t i, std::vector<Step>& out) {
     const bm_layer_plan& L = A->plan.layers[i];
     if (L.kind == BM_LYR_SPINY_STELLATE) {
-        if (A->plan.settings & (BM_SET_DISABLE_LEARNING | BM_SET_DISABLE_SSCS)) return;
-        A->run(K_SSC_MTP, [&] { launch_ssc_mtp_plain(A->axns(), A->dl[i], A->ctl, A->stream()); });
+        if (!(A->plan.settings & (BM_SET_DISABLE_LEARNING | BM_SET_DISABLE_SSCS)))
+            out.push_back({ST_SSC_MTP, (uint8_t)i, 0});
     } else {
-        enqueue_pyr_learn(A, i);
+        push_pyr_learn(A, i, out);
     }
 }
+
+}  // namespace
 
 // CorticalArea::cycle, src/cortex/cortical_area.rs:716-789 (intake happens
-// before this call; regrowth is rejected at build; output is read on demand).
-void enqueue_cycle(bm_area_s* A) {
+// before the cycle; regrowth is rejected at build; output is read on demand).
+void bm::area_steps(const bm_area_s* A, std::vector<Step>& out) {
     const bm_area_plan& P = A->plan;
-    A->launches = 0;
-    for (uint32_t i = 0; i < P.n_layers; i++)
-        if (A->verify_pending[i]) {
-            launch_verify_tufts(A->fused, A->dl[i], i, A->ctl, A->stream());
-            A->verify_pending[i] = false;
-        }
+    out.clear();
     if (!(P.settings & BM_SET_DISABLE_SSCS)) {
         for (uint32_t k = 0; k < P.n_cycle_order; k++)
-            if (P.layers[P.cycle_order[k]].tags & BM_TAG_SPATIAL) enqueue_layer_cycle(A, P.cycle_order[k]);
+            if (P.layers[P.cycle_order[k]].tags & BM_TAG_SPATIAL) push_layer_cycle(A, P.cycle_order[k], out);
         for (uint32_t k = 0; k < P.n_cycle_order; k++)
-            if (P.layers[P.cycle_order[k]].tags & BM_TAG_SPATIAL) enqueue_layer_learn(A, P.cycle_order[k]);
+            if (P.layers[P.cycle_order[k]].tags & BM_TAG_SPATIAL) push_layer_learn(A, P.cycle_order[k], out);
     }
     if (!(P.settings & BM_SET_DISABLE_PYRS)) {
         for (uint32_t k = 0; k < P.n_cycle_order; k++)
-            if (!(P.layers[P.cycle_order[k]].tags & BM_TAG_SPATIAL)) enqueue_layer_cycle(A, P.cycle_order[k]);
+            if (!(P.layers[P.cycle_order[k]].tags & BM_TAG_SPATIAL)) push_layer_cycle(A, P.cycle_order[k], out);
     }
-    A->run(K_CYCLE_END, [&] { launch_cycle_end(A->ctl, A->stream()); });
+    out.push_back({ST_CYCLE_END, 0, 0});
+}
+
+// Synapse flags, synapse cycle, dendrite cycle and (pyramidal) tuft cycle: the
+// plain form launches them as bismit does (flags over the whole layer, then
+// each stage per tuft); the fused form takes each tuft on its own, one fused
+// launch where the tuft qualifies, else that tuft's four stages. The stages of
+// different tufts touch disjoint buffers, so both orders give the same bytes.
+void bm::exec_step(bm_area_s* A, const Step& st, cudaStream_t s) {
+    const uint32_t i = st.layer, x = st.idx;
+    const bm_layer_plan& L = A->plan.layers[i];
+    const DevLayer& D = A->dl[i];
+    const bool pyr = L.kind == BM_LYR_PYRAMIDAL;
+    // Launches on the area's own stream are counted (and timed when profiling);
+    // a batch passes its own stream and does its own counting.
+    const bool own = s == A->stream();
+    auto run = [&](int kind, auto&& f) {
+        if (own) A->run(kind, f);
+        else f();
+    };
+    switch (st.kind) {
+    case ST_TUFT:
+        if (A->fused.t[i][x].ok) {
+            run(K_FUSED_TUFT, [&] { launch_fused_tuft(A->fused, A->axns(), A->slices, D, i, x, A->ctl, s); });
+        } else {
+            run(K_SYN_FLAGS, [&] { launch_set_syn_flags_tuft(D, x, s); });
+            run(K_SYN_CYCLE, [&] { launch_syn_cycle_plain(A->axns(), A->slices, D, x, s); });
+            run(K_DEN_CYCLE, [&] { launch_den_cycle_plain(D, x, A->ctl, s); });
+            if (pyr) run(K_TFT_CYCLE, [&] { launch_tft_cycle_plain(D, x, s); });
+        }
+        break;
+    case ST_TUFTS_PLAIN:
+        run(K_SYN_FLAGS, [&] { launch_set_syn_flags(D, s); });
+        for (uint32_t t = 0; t < L.n_tufts; t++)
+            run(K_SYN_CYCLE, [&] { launch_syn_cycle_plain(A->axns(), A->slices, D, t, s); });
+        for (uint32_t t = 0; t < L.n_tufts; t++) run(K_DEN_CYCLE, [&] { launch_den_cycle_plain(D, t, A->ctl, s); });
+        if (pyr)
+            for (uint32_t t = 0; t < L.n_tufts; t++) run(K_TFT_CYCLE, [&] { launch_tft_cycle_plain(D, t, s); });
+        break;
+    case ST_SSC_CYCLE: run(K_SSC_CYCLE, [&] { launch_ssc_cycle(D, s); }); break;
+    case ST_INHIB_SIMPLE:
+        run(K_INHIB_SIMPLE, [&] {
+            launch_inhib_simple(A->axns(), A->slices, D, (int)L.ctrl[x].field_radius, A->inhib_key[i][x], A->ctl, s);
+        });
+        break;
+    case ST_INHIB_PASS: run(K_INHIB_PASS, [&] { launch_inhib_passthrough(A->axns(), A->slices, D, s); }); break;
+    case ST_PYR_OUTPUT: run(K_PYR_OUTPUT, [&] { launch_pyr_output(A->axns(), A->slices, D, s); }); break;
+    case ST_INTRA_COL: run(K_INTRA_COL, [&] { launch_inhib_intra_column_plain(A->axns(), A->slices, D, s); }); break;
+    case ST_PYR_CYCLE: run(K_PYR_CYCLE, [&] { launch_pyr_cycle_plain(D, s); }); break;
+    case ST_DST_MTP: run(K_TFT_DST_MTP, [&] { launch_tft_dst_mtp_plain(A->axns(), D, x, A->ctl, s); }); break;
+    case ST_SSC_MTP: run(K_SSC_MTP, [&] { launch_ssc_mtp_plain(A->axns(), D, A->ctl, s); }); break;
+    case ST_CYCLE_END: run(K_CYCLE_END, [&] { launch_cycle_end(A->ctl, s); }); break;
+    default: break;
+    }
+}
+
+void bm::run_pending_verifies(bm_area_s* A, cudaStream_t s) {
+    for (uint32_t i = 0; i < A->plan.n_layers; i++)
+        if (A->verify_pending[i]) {
+            launch_verify_tufts(A->fused, A->dl[i], i, A->ctl, s);
+            A->verify_pending[i] = false;
+        }
+}
+
+namespace {
+
+void enqueue_cycle(bm_area_s* A) {
+    A->launches = 0;
+    run_pending_verifies(A, A->stream());
+    for (const Step& st : A->steps) exec_step(A, st, A->stream());
     A->host_cycle++;
 }
 
@@ -476,6 +414,7 @@ int bm_area_create(bm_ctx ctx, const bm_area_desc* desc, uint64_t seed, bm_area*
     if (e != cudaSuccess) { free_area(A); return cuda_err(e, "synapse growth"); }
     rc = prepare_fused(A->fused, A->plan, &err);
     for (uint32_t i = 0; i < A->plan.n_layers; i++) A->verify_pending[i] = true;
+    area_steps(A, A->steps);
     if (rc != BM_OK) { free_area(A); return set_err(rc, "%s", err.c_str()); }
     *out = A;
     return BM_OK;
@@ -634,9 +573,9 @@ int bm_area_get_cycle(bm_area area, uint64_t* out) {
 int bm_area_set_cycle(bm_area area, uint64_t cycle) {
     if (!area) return set_err(BM_ERR_INVALID, "null area");
     DevGuard g(area->ctx->device);
-    AreaCtl c{};
-    c.cycle = cycle;
-    CU(cudaMemcpyAsync(area->ctl, &c, sizeof c, cudaMemcpyHostToDevice, area->stream()));
+    // Only the counter: the error bits and the tufts' verification status stay.
+    unsigned long long c = cycle;
+    CU(cudaMemcpyAsync(&area->ctl->cycle, &c, sizeof c, cudaMemcpyHostToDevice, area->stream()));
     CU(cudaStreamSynchronize(area->stream()));
     area->host_cycle = cycle;
     return BM_OK;

@@ -1,0 +1,132 @@
+// bm_area.h -- the library's internal view of contexts and areas, and the
+// per-area stage program (the ordered steps of one cycle) that the one-area
+// path and the batched path (bm_batch.cu) both execute.
+#pragma once
+#include <vector>
+
+#include "bm_fused.h"
+#include "bm_kernels.h"
+
+namespace bm {
+
+// Kernel kinds for per-launch timing.
+enum Kind {
+    K_SYN_FLAGS, K_SYN_CYCLE, K_DEN_CYCLE, K_TFT_CYCLE, K_SSC_CYCLE, K_INHIB_SIMPLE, K_INHIB_PASS,
+    K_SSC_MTP, K_PYR_CYCLE, K_PYR_OUTPUT, K_INTRA_COL, K_TFT_DST_MTP, K_CYCLE_END, K_INTAKE,
+    K_FUSED_TUFT, K_FUSED_SSC_SOMA, K_FUSED_PYR_SOMA, K_FUSED_SSC_MTP, K_COUNT
+};
+const char* const kKindNames[K_COUNT] = {
+    "tft_set_syn_flags", "syn_cycle", "den_cycle_tft", "tft_cycle", "ssc_cycle", "inhib_simple",
+    "inhib_passthrough", "ssc_mtp_simple", "pyr_cycle", "pyr_output", "inhib_intra_column", "tft_dst_mtp",
+    "cycle_end", "intake", "fused_tuft_cycle", "fused_ssc_soma_inhib", "fused_pyr_soma_learn",
+    "fused_ssc_mtp"};
+
+struct DevGuard {
+    int prev = -1;
+    explicit DevGuard(int dev) {
+        cudaGetDevice(&prev);
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DevGuard() {
+        int cur;
+        cudaGetDevice(&cur);
+        if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+// One step of an area's cycle. Areas with equal step lists can be cycled
+// together, one batched launch per step (bm_batch.cu).
+enum StepKind : uint8_t {
+    ST_TUFT,          // tuft `idx` of layer `layer`: fused launch, or its four plain stages
+    ST_TUFTS_PLAIN,   // plain form: flags of the layer, then each stage per tuft
+    ST_SSC_CYCLE,
+    ST_INHIB_SIMPLE,  // control `idx` hosted on `layer`
+    ST_INHIB_PASS,
+    ST_PYR_OUTPUT,
+    ST_INTRA_COL,
+    ST_PYR_CYCLE,
+    ST_DST_MTP,       // distal learning of tuft `idx`
+    ST_SSC_MTP,
+    ST_CYCLE_END,
+};
+struct Step {
+    uint8_t kind, layer, idx;
+    bool operator==(const Step& o) const { return kind == o.kind && layer == o.layer && idx == o.idx; }
+};
+
+}  // namespace bm
+
+struct bm_ctx_s {
+    int device = 0;
+    cudaStream_t own = nullptr;
+    cudaStream_t user = nullptr;
+    bool user_set = false;
+    cudaStream_t stream() const { return user_set ? user : own; }
+};
+
+struct bm_area_s {
+    using Step = bm::Step;
+    bm_ctx ctx = nullptr;
+    bm_area_plan plan;
+    uint8_t* slab = nullptr;
+    bm::AreaCtl* ctl = nullptr;
+    bm::SliceRec* slices = nullptr;
+    bm::DevLayer dl[BM_MAX_LAYERS];
+    uint64_t inhib_key[BM_MAX_LAYERS][BM_MAX_CTRL];
+    uint64_t host_cycle = 0;
+    bool verify_pending[BM_MAX_LAYERS] = {};   // sources or flags written since the last check
+    uint32_t exec_path = BM_PATH_FUSED;
+    bm::FusedArea fused;
+    bool profiling = false;
+    struct Rec { int kind; cudaEvent_t a, b; };
+    std::vector<Rec> pending;
+    std::vector<cudaEvent_t> pool;
+    uint64_t prof_launches[bm::K_COUNT] = {};
+    double prof_ms[bm::K_COUNT] = {};
+    uint32_t launches = 0;   // kernel launches of the last enqueued cycle
+    std::vector<Step> steps; // the cycle's stage program
+
+    cudaStream_t stream() const { return ctx->stream(); }
+    uint8_t* axns() const { return slab + plan.axon_off; }
+
+    cudaEvent_t ev() {
+        if (!pool.empty()) { cudaEvent_t e = pool.back(); pool.pop_back(); return e; }
+        cudaEvent_t e = nullptr;
+        cudaEventCreate(&e);
+        return e;
+    }
+    template <class F> void run(int kind, F&& f) {
+        if (kind != bm::K_INTAKE) launches++;
+        if (!profiling) { f(); return; }
+        Rec r{kind, ev(), ev()};
+        cudaEventRecord(r.a, stream());
+        f();
+        cudaEventRecord(r.b, stream());
+        pending.push_back(r);
+    }
+    void drain_profile() {
+        for (auto& r : pending) {
+            float ms = 0.f;
+            cudaEventSynchronize(r.b);
+            cudaEventElapsedTime(&ms, r.a, r.b);
+            prof_launches[r.kind]++;
+            prof_ms[r.kind] += ms;
+            pool.push_back(r.a);
+            pool.push_back(r.b);
+        }
+        pending.clear();
+    }
+};
+
+
+namespace bm {
+
+// The steps of one cycle of A (CorticalArea::cycle order).
+void area_steps(const bm_area_s* A, std::vector<Step>& out);
+// Enqueues one step of A on stream s.
+void exec_step(bm_area_s* A, const Step& st, cudaStream_t s);
+// Recompiles the gather offsets of layers whose sources or flags were written.
+void run_pending_verifies(bm_area_s* A, cudaStream_t s);
+int cuda_err(cudaError_t e, const char* what);
+
+}  // namespace bm

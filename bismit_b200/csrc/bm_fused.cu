@@ -42,6 +42,8 @@
 #include <algorithm>
 #include <cstring>
 
+#include "bm_kernels.h"
+
 namespace bm {
 
 namespace {
@@ -542,6 +544,95 @@ __device__ __forceinline__ void tma_stage(const FusedTuftArgs& A, const TileGeo&
     }
 }
 
+// Producer lane: issues every stage of tile G into the ring (buffer pb of
+// round pround). False when a bounded wait gave up.
+template <bool TUFT, int MODE, bool FCLEAN>
+__device__ __forceinline__ bool produce_tile(const FusedTuftArgs& A, const TileGeo& G, uint8_t* stages,
+                                             uint64_t* full, uint64_t* empty, uint32_t& pb, uint32_t& pround,
+                                             uint64_t& issued, volatile int& s_abort) {
+    const uint32_t SB = A.stage_bytes;
+    const uint32_t buf_bytes = A.stage_stride;
+    const uint32_t nst = A.nst;
+    for (uint32_t pos = G.syn0; pos < G.syn_end; pos += SB) {
+        if (s_abort) return false;
+        // Buffer pb's previous use (round pround - 1) must be released.
+        if (pround > 0 && !mbar_wait(&empty[pb], (pround - 1) & 1)) {
+            s_abort = 1;
+            return false;
+        }
+        const uint32_t left = G.syn_end - pos;
+        const uint32_t nb = left < SB ? left : SB;
+        uint8_t* dst = stages + (size_t)pb * buf_bytes;
+        uint32_t n_arr_bytes = (MODE == 0 ? 2 * nb : 3 * nb) + nb + nb + (FCLEAN ? 0 : nb);
+        // Windows of the stage's dendrites and cells, widened to 16-byte bounds.
+        const uint32_t d0 = (pos >> A.spd_l2) & ~15u, d1 = (((pos + nb) >> A.spd_l2) + 15) & ~15u;
+        const uint32_t c0 = (pos >> A.S_l2) & ~15u, c1 = (((pos + nb) >> A.S_l2) + 15) & ~15u;
+        if (A.win) n_arr_bytes += (uint32_t)(d1 - d0) + (TUFT ? 4 * (uint32_t)(c1 - c0) : 0u);
+        mbar_arrive_expect_tx(&full[pb], n_arr_bytes);
+        if (A.win) {
+            uint8_t* wd = dst + 6 * SB;
+            bulk_g2s(wd, A.den_act + d0, (uint32_t)(d1 - d0), &full[pb]);
+            if (TUFT) {
+                const uint32_t cb = (uint32_t)(c1 - c0);
+                bulk_g2s(wd + A.win_bytes, A.t_bid + c0, cb, &full[pb]);
+                bulk_g2s(wd + 2 * A.win_bytes, A.t_braw + c0, cb, &full[pb]);
+                bulk_g2s(wd + 3 * A.win_bytes, A.t_bst + c0, cb, &full[pb]);
+                bulk_g2s(wd + 4 * A.win_bytes, A.t_st + c0, cb, &full[pb]);
+            }
+        }
+        if (MODE == 0) {
+            bulk_g2s(dst, A.gidx + pos, 2 * nb, &full[pb]);
+        } else {
+            bulk_g2s(dst, A.slc + pos, nb, &full[pb]);
+            bulk_g2s(dst + SB, A.vofs + pos, nb, &full[pb]);
+            bulk_g2s(dst + 2 * SB, A.uofs + pos, nb, &full[pb]);
+        }
+        bulk_g2s(dst + arr_off<MODE>(0, SB), A.str + pos, nb, &full[pb]);
+        bulk_g2s(dst + arr_off<MODE>(1, SB), A.st + pos, nb, &full[pb]);
+        if (!FCLEAN) bulk_g2s(dst + arr_off<MODE>(2, SB), A.fl + pos, nb, &full[pb]);
+        issued++;
+        if (++pb == nst) { pb = 0; pround++; }
+    }
+    return true;
+}
+
+// After a give-up: record it and let this CTA's copies land before its
+// shared memory is released (the latest use of every buffer must complete).
+__device__ __forceinline__ void producer_drain(AreaCtl* ctl, uint64_t* full, uint32_t nst, uint64_t issued) {
+    if (ctl) atomicOr(&ctl->error, kErrWaitTimeout);
+    for (uint32_t b = 0; b < nst; b++) {
+        const uint64_t uses = issued / nst + (b < issued % nst ? 1 : 0);
+        if (uses) mbar_wait(&full[b], (uint32_t)((uses - 1) & 1));
+    }
+}
+
+// Consumer warps: stage tile G's footprint, then process its stages from the
+// ring (buffer cb, phase cphase). A give-up sets s_abort; every consumer then
+// leaves at the next tile's barrier.
+template <bool TUFT, int MODE, bool FCLEAN>
+__device__ __forceinline__ void consume_tile(const FusedTuftArgs& A, const TileGeo& G, uint8_t* halo, uint8_t* stages,
+                                             uint64_t* full, uint64_t* empty, uint32_t& cb, uint32_t& cphase,
+                                             int lane, int wib, int32_t rnd, volatile int& s_abort) {
+    build_footprint(A, G, halo, wib * 32 + lane);
+    consumers_sync();
+    const uint32_t SB = A.stage_bytes;
+    const uint32_t cpu = A.chunks_per_unit;
+    const uint32_t n_units_tile = cpu > 1 ? G.h * G.w : (G.syn_end - G.syn0 + 511) >> 9;
+    for (uint32_t pos = G.syn0; pos < G.syn_end; pos += SB) {
+        bool got = !s_abort && mbar_wait(&full[cb], cphase);
+        got = __all_sync(0xFFFFFFFFu, got);
+        if (!got) {
+            if (lane == 0) s_abort = 1;
+            return;
+        }
+        tma_stage<TUFT, MODE, FCLEAN>(A, G, halo, stages + (size_t)cb * A.stage_stride, pos, n_units_tile, lane, wib,
+                                      rnd);
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&empty[cb]);
+        if (++cb == A.nst) { cb = 0; cphase ^= 1; }
+    }
+}
+
 template <bool TUFT, int MODE, bool FCLEAN>
 __device__ __forceinline__ void tma_body(const FusedTuftArgs& A, uint8_t* smem, volatile int& s_abort) {
     uint64_t* full = (uint64_t*)smem;              // [nst]
@@ -551,105 +642,33 @@ __device__ __forceinline__ void tma_body(const FusedTuftArgs& A, uint8_t* smem, 
     const int tid = threadIdx.x;
     const int lane = tid & 31;
     const int wib = tid >> 5;
-    const uint32_t SB = A.stage_bytes;
-    const uint32_t buf_bytes = A.stage_stride;
-    const uint32_t nst = A.nst;
-
     if (wib == kWarps) {
         // ---- producer warp: lane 0 streams every stage of this CTA's tiles ----
         if (lane != 0) return;
         uint32_t pb = 0, pround = 0;
         uint64_t issued = 0;
-        for (uint32_t t = blockIdx.x; t < A.n_tiles && !s_abort; t += gridDim.x) {
-            const TileGeo G = tile_geo(A, t);
-            for (uint32_t pos = G.syn0; pos < G.syn_end; pos += SB) {
-                if (s_abort) break;
-                // Buffer pb's previous use (round pround - 1) must be released.
-                if (pround > 0 && !mbar_wait(&empty[pb], (pround - 1) & 1)) {
-                    s_abort = 1;
-                    break;
-                }
-                const uint32_t left = G.syn_end - pos;
-                const uint32_t nb = left < SB ? left : SB;
-                uint8_t* dst = stages + (size_t)pb * buf_bytes;
-                uint32_t n_arr_bytes = (MODE == 0 ? 2 * nb : 3 * nb) + nb + nb + (FCLEAN ? 0 : nb);
-                // Windows of the stage's dendrites and cells, widened to 16-byte bounds.
-                const uint32_t d0 = (pos >> A.spd_l2) & ~15u, d1 = (((pos + nb) >> A.spd_l2) + 15) & ~15u;
-                const uint32_t c0 = (pos >> A.S_l2) & ~15u, c1 = (((pos + nb) >> A.S_l2) + 15) & ~15u;
-                if (A.win) n_arr_bytes += (uint32_t)(d1 - d0) + (TUFT ? 4 * (uint32_t)(c1 - c0) : 0u);
-                mbar_arrive_expect_tx(&full[pb], n_arr_bytes);
-                if (A.win) {
-                    uint8_t* wd = dst + 6 * SB;
-                    bulk_g2s(wd, A.den_act + d0, (uint32_t)(d1 - d0), &full[pb]);
-                    if (TUFT) {
-                        const uint32_t cb = (uint32_t)(c1 - c0);
-                        bulk_g2s(wd + A.win_bytes, A.t_bid + c0, cb, &full[pb]);
-                        bulk_g2s(wd + 2 * A.win_bytes, A.t_braw + c0, cb, &full[pb]);
-                        bulk_g2s(wd + 3 * A.win_bytes, A.t_bst + c0, cb, &full[pb]);
-                        bulk_g2s(wd + 4 * A.win_bytes, A.t_st + c0, cb, &full[pb]);
-                    }
-                }
-                if (MODE == 0) {
-                    bulk_g2s(dst, A.gidx + pos, 2 * nb, &full[pb]);
-                } else {
-                    bulk_g2s(dst, A.slc + pos, nb, &full[pb]);
-                    bulk_g2s(dst + SB, A.vofs + pos, nb, &full[pb]);
-                    bulk_g2s(dst + 2 * SB, A.uofs + pos, nb, &full[pb]);
-                }
-                bulk_g2s(dst + arr_off<MODE>(0, SB), A.str + pos, nb, &full[pb]);
-                bulk_g2s(dst + arr_off<MODE>(1, SB), A.st + pos, nb, &full[pb]);
-                if (!FCLEAN) bulk_g2s(dst + arr_off<MODE>(2, SB), A.fl + pos, nb, &full[pb]);
-                issued++;
-                if (++pb == nst) { pb = 0; pround++; }
-            }
-        }
-        if (s_abort) {
-            // Let this CTA's copies land before its shared memory is released:
-            // the latest use of every buffer must complete.
-            atomicOr(&A.ctl->error, kErrWaitTimeout);
-            for (uint32_t b = 0; b < nst; b++) {
-                const uint64_t uses = issued / nst + (b < issued % nst ? 1 : 0);
-                if (uses) mbar_wait(&full[b], (uint32_t)((uses - 1) & 1));
-            }
-        }
+        for (uint32_t t = blockIdx.x; t < A.n_tiles && !s_abort; t += gridDim.x)
+            if (!produce_tile<TUFT, MODE, FCLEAN>(A, tile_geo(A, t), stages, full, empty, pb, pround, issued, s_abort))
+                break;
+        if (s_abort) producer_drain(A.ctl, full, A.nst, issued);
         return;
     }
-
     // ---- consumer warps ----
-    const uint32_t cpu = A.chunks_per_unit;
     const int32_t rnd = rnd_at(A.rnd_key, A.ctl->cycle);
     uint32_t cb = 0, cphase = 0;
     for (uint32_t t = blockIdx.x; t < A.n_tiles; t += gridDim.x) {
         const TileGeo G = tile_geo(A, t);
         consumers_sync();   // every consumer is done with the previous footprint
         if (s_abort) break;
-        build_footprint(A, G, halo, wib * 32 + lane);
-        consumers_sync();
-        const uint32_t n_units_tile = cpu > 1 ? G.h * G.w : (G.syn_end - G.syn0 + 511) >> 9;
-        for (uint32_t pos = G.syn0; pos < G.syn_end; pos += SB) {
-            bool got = !s_abort && mbar_wait(&full[cb], cphase);
-            got = __all_sync(0xFFFFFFFFu, got);
-            if (!got) {
-                if (lane == 0) s_abort = 1;
-                break;
-            }
-            tma_stage<TUFT, MODE, FCLEAN>(A, G, halo, stages + (size_t)cb * buf_bytes, pos, n_units_tile, lane, wib,
-                                          rnd);
-            __syncwarp();
-            if (lane == 0) mbar_arrive(&empty[cb]);
-            if (++cb == nst) { cb = 0; cphase ^= 1; }
-        }
+        consume_tile<TUFT, MODE, FCLEAN>(A, G, halo, stages, full, empty, cb, cphase, lane, wib, rnd, s_abort);
     }
 }
 
-template <bool TUFT>
-__global__ void __launch_bounds__(kThreads, 2) k_fused_tuft_tma(FusedTuftArgs A) {
-    extern __shared__ __align__(128) uint8_t smem[];
-    __shared__ volatile int s_abort;   // a bounded wait gave up
+__device__ __forceinline__ void init_ring(uint8_t* smem, uint32_t nst, volatile int& s_abort) {
     uint64_t* full = (uint64_t*)smem;
-    uint64_t* empty = full + A.nst;
+    uint64_t* empty = full + nst;
     if (threadIdx.x == 0) {
-        for (uint32_t i = 0; i < A.nst; i++) {
+        for (uint32_t i = 0; i < nst; i++) {
             mbar_init(&full[i], 1);
             mbar_init(&empty[i], kWarps);
         }
@@ -657,15 +676,119 @@ __global__ void __launch_bounds__(kThreads, 2) k_fused_tuft_tma(FusedTuftArgs A)
         s_abort = 0;
     }
     __syncthreads();
-    // One specialised body per gather mode and flags state (uniform per launch).
+}
+
+// Gather form (bit 1: sources outside the footprint) and flags state (bit 0:
+// foreign flag bits) of a tuft, from its verification status.
+__device__ __forceinline__ uint32_t mode_of(const FusedTuftArgs& A) {
     const uint32_t status = A.ctl->tuft_status[A.status_idx];
-    const bool fclean = (status & kTuftFlagsForeign) == 0;
-    if (status & kTuftSrcOutsideTile) {
-        if (fclean) tma_body<TUFT, 1, true>(A, smem, s_abort);
-        else tma_body<TUFT, 1, false>(A, smem, s_abort);
-    } else {
-        if (fclean) tma_body<TUFT, 0, true>(A, smem, s_abort);
-        else tma_body<TUFT, 0, false>(A, smem, s_abort);
+    return ((status & kTuftSrcOutsideTile) ? 2u : 0u) | ((status & kTuftFlagsForeign) ? 1u : 0u);
+}
+
+template <bool TUFT>
+__global__ void __launch_bounds__(kThreads, 2) k_fused_tuft_tma(FusedTuftArgs A) {
+    extern __shared__ __align__(128) uint8_t smem[];
+    __shared__ volatile int s_abort;   // a bounded wait gave up
+    init_ring(smem, A.nst, s_abort);
+    // One specialised body per gather mode and flags state (uniform per launch).
+    switch (mode_of(A)) {
+    case 0: tma_body<TUFT, 0, true>(A, smem, s_abort); break;
+    case 1: tma_body<TUFT, 0, false>(A, smem, s_abort); break;
+    case 2: tma_body<TUFT, 1, true>(A, smem, s_abort); break;
+    default: tma_body<TUFT, 1, false>(A, smem, s_abort); break;
+    }
+}
+
+// ------------------------------------------------------- batched form ----
+// One launch over the tiles of several tufts (the same tuft of several areas):
+// job j owns global tiles tile0[j] .. tile0[j + 1] - 1. Persistent CTAs walk
+// the global tiles in the same stride as the one-tuft kernel; the producer
+// lane and the consumer warps each keep their current job's arguments in
+// shared memory (the producer may run a tile ahead into the next job). Every
+// job of a launch shares the ring geometry (nst, stage_stride, halo_off).
+
+// The job of global tile t: tile0[j] <= t < tile0[j + 1].
+__device__ __forceinline__ uint32_t job_of(const uint32_t* __restrict__ tile0, uint32_t n_jobs, uint32_t t) {
+    uint32_t lo = 0, hi = n_jobs;
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (__ldg(tile0 + mid) <= t) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+__device__ __forceinline__ void load_args(FusedTuftArgs& dst, const FusedTuftArgs* src, uint32_t tid, uint32_t nthr) {
+    static_assert(sizeof(FusedTuftArgs) % 8 == 0, "argument block is copied in 8-byte words");
+    const unsigned long long* s = (const unsigned long long*)src;
+    unsigned long long* d = (unsigned long long*)&dst;
+    for (uint32_t i = tid; i < sizeof(FusedTuftArgs) / 8; i += nthr) d[i] = __ldg(s + i);
+}
+
+template <bool TUFT>
+__global__ void __launch_bounds__(kThreads, 2)
+    k_fused_tuft_batch(const FusedTuftArgs* __restrict__ jobs, const uint32_t* __restrict__ tile0, uint32_t n_jobs,
+                       uint32_t nst, uint32_t halo_off) {
+    extern __shared__ __align__(128) uint8_t smem[];
+    __shared__ volatile int s_abort;
+    __shared__ __align__(16) FusedTuftArgs s_job[2];   // [0] the producer's job, [1] the consumers'
+    init_ring(smem, nst, s_abort);
+    uint64_t* full = (uint64_t*)smem;
+    uint64_t* empty = full + nst;
+    uint8_t* stages = smem + 128;
+    uint8_t* halo = smem + halo_off;
+    const uint32_t n_tiles = __ldg(tile0 + n_jobs);
+    const int tid = threadIdx.x;
+    const int lane = tid & 31;
+    const int wib = tid >> 5;
+    if (wib == kWarps) {
+        if (lane != 0) return;
+        FusedTuftArgs& A = s_job[0];
+        uint32_t cur = 0xFFFFFFFFu, mode = 0, pb = 0, pround = 0;
+        uint64_t issued = 0;
+        AreaCtl* ctl = nullptr;
+        for (uint32_t t = blockIdx.x; t < n_tiles && !s_abort; t += gridDim.x) {
+            const uint32_t j = job_of(tile0, n_jobs, t);
+            if (j != cur) {
+                load_args(A, jobs + j, 0, 1);
+                cur = j;
+                mode = mode_of(A);
+                ctl = A.ctl;
+            }
+            const TileGeo G = tile_geo(A, t - __ldg(tile0 + j));
+            bool ok;
+            switch (mode) {
+            case 0: ok = produce_tile<TUFT, 0, true>(A, G, stages, full, empty, pb, pround, issued, s_abort); break;
+            case 1: ok = produce_tile<TUFT, 0, false>(A, G, stages, full, empty, pb, pround, issued, s_abort); break;
+            case 2: ok = produce_tile<TUFT, 1, true>(A, G, stages, full, empty, pb, pround, issued, s_abort); break;
+            default: ok = produce_tile<TUFT, 1, false>(A, G, stages, full, empty, pb, pround, issued, s_abort); break;
+            }
+            if (!ok) break;
+        }
+        if (s_abort) producer_drain(ctl, full, nst, issued);
+        return;
+    }
+    FusedTuftArgs& A = s_job[1];
+    uint32_t cur = 0xFFFFFFFFu, mode = 0, cb = 0, cphase = 0;
+    int32_t rnd = 0;
+    for (uint32_t t = blockIdx.x; t < n_tiles; t += gridDim.x) {
+        const uint32_t j = job_of(tile0, n_jobs, t);
+        consumers_sync();   // every consumer is done with the previous tile (footprint and job)
+        if (s_abort) break;
+        if (j != cur) {
+            load_args(A, jobs + j, (uint32_t)tid, kWarps * 32);
+            consumers_sync();
+            cur = j;
+            mode = mode_of(A);
+            rnd = rnd_at(A.rnd_key, A.ctl->cycle);
+        }
+        const TileGeo G = tile_geo(A, t - __ldg(tile0 + j));
+        switch (mode) {
+        case 0: consume_tile<TUFT, 0, true>(A, G, halo, stages, full, empty, cb, cphase, lane, wib, rnd, s_abort); break;
+        case 1: consume_tile<TUFT, 0, false>(A, G, halo, stages, full, empty, cb, cphase, lane, wib, rnd, s_abort); break;
+        case 2: consume_tile<TUFT, 1, true>(A, G, halo, stages, full, empty, cb, cphase, lane, wib, rnd, s_abort); break;
+        default: consume_tile<TUFT, 1, false>(A, G, halo, stages, full, empty, cb, cphase, lane, wib, rnd, s_abort); break;
+        }
     }
 }
 
@@ -733,8 +856,9 @@ int device_sms() {
     return sms;
 }
 
-// Launch parameters of tuft t of data layer i (gidx left null).
-void plan_tuft(FusedTuft& FT, const bm_area_plan& P, uint32_t i, uint32_t t, int sms) {
+// Launch parameters of tuft t of data layer i (gidx left null). `target` is
+// the synapses per tile to aim for (0: chosen from the tuft's size).
+void plan_tuft(FusedTuft& FT, const bm_area_plan& P, uint32_t i, uint32_t t, int sms, uint32_t target_syns = 0) {
     const bm_layer_plan& L = P.layers[i];
     bool aligned = true;
     for (int k = 0; k < BM_BUF_COUNT; k++)
@@ -779,6 +903,7 @@ void plan_tuft(FusedTuft& FT, const bm_area_plan& P, uint32_t i, uint32_t t, int
     const uint32_t SB = kWarps * cpu * 512;
     const uint64_t n_syn = (uint64_t)L.cells * S;
     uint64_t target = std::min<uint64_t>(32768, std::max<uint64_t>(4096, n_syn / ((uint64_t)sms * 16)));
+    if (target_syns) target = target_syns;
     uint64_t cells = std::max<uint64_t>(1, target / S);
     uint32_t W, H;
     if (cells >= L.u_size) {
@@ -852,6 +977,19 @@ int plan_fused_tuft(FusedArea& F, const bm_area_plan& P, uint32_t layer, uint32_
     return BM_OK;
 }
 
+bool retile_fused_tuft(FusedArea& F, const bm_area_plan& P, uint32_t layer, uint32_t t, uint32_t target_syns) {
+    FusedTuft& FT = F.t[layer][t];
+    if (!FT.tiled || !FT.gidx) return false;
+    FusedTuft next;
+    plan_tuft(next, P, layer, t, F.sms, target_syns);
+    cudaGetLastError();
+    if (!next.tiled) return false;
+    next.gidx = FT.gidx;
+    next.tile_target = target_syns;
+    FT = next;
+    return true;
+}
+
 int prepare_fused(FusedArea& F, const bm_area_plan& P, std::string* err) {
     int rc = plan_fused(F, P);
     if (rc != BM_OK) return rc;
@@ -902,11 +1040,13 @@ void launch_verify_tufts(const FusedArea& F, const DevLayer& L, uint32_t layer, 
     for (uint32_t t = 0; t < L.n_tufts; t++) launch_compile_tuft(F, L, layer, t, ctl, s);
 }
 
-void launch_fused_tuft(const FusedArea& F, const uint8_t* axns, const SliceRec* slices, const DevLayer& L,
-                       uint32_t layer, uint32_t t, AreaCtl* ctl, cudaStream_t s) {
+namespace {
+
+// The kernel arguments of tuft t of data layer `layer`.
+void make_args(FusedTuftArgs& A, const FusedArea& F, const uint8_t* axns, const SliceRec* slices, const DevLayer& L,
+               uint32_t layer, uint32_t t, AreaCtl* ctl) {
     const DevTuft& T = L.tft[t];
     const FusedTuft& FT = F.t[layer][t];
-    FusedTuftArgs A;
     std::memset(&A, 0, sizeof A);
     A.axns = axns;
     A.slices = slices;
@@ -974,11 +1114,23 @@ void launch_fused_tuft(const FusedArea& F, const uint8_t* axns, const SliceRec* 
         A.stage_stride = FT.stage_stride;
         A.win = FT.win;
         A.win_bytes = FT.win_bytes;
+    } else {
+        A.n_units = S > 512 ? (uint64_t)L.cells : (A.n_syn + 511) / 512;
+    }
+}
+
+}  // namespace
+
+void launch_fused_tuft(const FusedArea& F, const uint8_t* axns, const SliceRec* slices, const DevLayer& L,
+                       uint32_t layer, uint32_t t, AreaCtl* ctl, cudaStream_t s) {
+    const FusedTuft& FT = F.t[layer][t];
+    FusedTuftArgs A;
+    make_args(A, F, axns, slices, L, layer, t, ctl);
+    const bool tuft = L.kind == BM_LYR_PYRAMIDAL;
+    if (FT.tiled) {
         auto kern = tuft ? k_fused_tuft_tma<true> : k_fused_tuft_tma<false>;
         kern<<<FT.grid, kThreads, FT.smem, s>>>(A);
     } else {
-        const uint64_t n_chunks = (A.n_syn + 511) / 512;
-        A.n_units = S > 512 ? (uint64_t)L.cells : n_chunks;
         uint64_t want = (A.n_units + kWarps - 1) / kWarps;
         uint64_t cap = (uint64_t)F.sms * 8;
         unsigned grid = (unsigned)std::max<uint64_t>(1, std::min(want, cap));
@@ -987,6 +1139,80 @@ void launch_fused_tuft(const FusedArea& F, const uint8_t* axns, const SliceRec* 
         else
             k_fused_tuft<false><<<grid, kWarps * 32, 0, s>>>(A);
     }
+}
+
+// ---------------------------------------------------------- batched form --
+int prepare_fused_batch(FusedBatch& B, const std::vector<FusedJob>& jobs, uint32_t layer, uint32_t t) {
+    free_fused_batch(B);
+    B = FusedBatch{};
+    if (jobs.empty()) return BM_OK;
+    const bool tuft = jobs[0].L->kind == BM_LYR_PYRAMIDAL;
+    uint32_t stride = 0, halo = 0, sms = 148;
+    for (const FusedJob& J : jobs) {
+        const FusedTuft& FT = J.F->t[layer][t];
+        if (!FT.ok || !FT.tiled || !FT.gidx || (J.L->kind == BM_LYR_PYRAMIDAL) != tuft) return BM_OK;
+        stride = std::max(stride, FT.stage_stride);
+        halo = std::max(halo, ((FT.nrec * FT.fsz + 15) / 16) * 16);
+        sms = (uint32_t)J.F->sms;
+    }
+    uint32_t nst = (uint32_t)std::max<uint64_t>(2, std::min<uint64_t>(4, (80 * 1024) / stride));
+    while (nst > 2 && 128 + (uint64_t)nst * stride + halo > kMaxSmem) nst--;
+    const uint64_t halo_off = 128 + (uint64_t)nst * stride;
+    const uint64_t smem = halo_off + halo;
+    if (smem > kMaxSmem) return BM_OK;
+    std::vector<FusedTuftArgs> args(jobs.size());
+    std::vector<uint32_t> tile0(jobs.size() + 1);
+    uint32_t total = 0;
+    for (size_t j = 0; j < jobs.size(); j++) {
+        const FusedJob& J = jobs[j];
+        make_args(args[j], *J.F, J.axns, J.slices, *J.L, layer, t, J.ctl);
+        args[j].nst = nst;
+        args[j].stage_stride = stride;
+        args[j].halo_off = (uint32_t)halo_off;
+        tile0[j] = total;
+        total += args[j].n_tiles;
+    }
+    tile0[jobs.size()] = total;
+    if (cudaMalloc(&B.d_jobs, args.size() * sizeof(FusedTuftArgs)) != cudaSuccess ||
+        cudaMalloc(&B.d_tile0, tile0.size() * sizeof(uint32_t)) != cudaSuccess) {
+        cudaGetLastError();
+        free_fused_batch(B);
+        return set_err(BM_ERR_OOM, "cudaMalloc of the batched tuft jobs failed");
+    }
+    if (cudaMemcpy(B.d_jobs, args.data(), args.size() * sizeof(FusedTuftArgs), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(B.d_tile0, tile0.data(), tile0.size() * sizeof(uint32_t), cudaMemcpyHostToDevice) != cudaSuccess) {
+        cudaGetLastError();
+        free_fused_batch(B);
+        return set_err(BM_ERR_CUDA, "copy of the batched tuft jobs failed");
+    }
+    auto kern = tuft ? k_fused_tuft_batch<true> : k_fused_tuft_batch<false>;
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMaxSmem);
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads, (size_t)smem) != cudaSuccess) per_sm = 1;
+    cudaGetLastError();
+    B.ok = true;
+    B.tuft = tuft;
+    B.n_jobs = (uint32_t)jobs.size();
+    B.n_tiles = total;
+    B.nst = nst;
+    B.halo_off = (uint32_t)halo_off;
+    B.smem = (uint32_t)smem;
+    B.grid = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(total, (uint64_t)sms * std::max(per_sm, 1)));
+    return BM_OK;
+}
+
+void launch_fused_batch(const FusedBatch& B, cudaStream_t s) {
+    if (!B.ok || !B.n_tiles) return;
+    auto kern = B.tuft ? k_fused_tuft_batch<true> : k_fused_tuft_batch<false>;
+    kern<<<B.grid, kThreads, B.smem, s>>>((const FusedTuftArgs*)B.d_jobs, B.d_tile0, B.n_jobs, B.nst, B.halo_off);
+}
+
+void free_fused_batch(FusedBatch& B) {
+    if (B.d_jobs) cudaFree(B.d_jobs);
+    if (B.d_tile0) cudaFree(B.d_tile0);
+    B.d_jobs = nullptr;
+    B.d_tile0 = nullptr;
+    B.ok = false;
 }
 
 }  // namespace bm

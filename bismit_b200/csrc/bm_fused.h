@@ -1,6 +1,7 @@
 // bm_fused.h -- the fused stage kernels: per-area preparation and launchers.
 #pragma once
 #include <string>
+#include <vector>
 
 #include "bm_dev.cuh"
 #include "bm_layout.h"
@@ -27,6 +28,7 @@ struct FusedTuft {
     bool win = false;            // windows ride in the stages (16-byte aligned ranges)
     uint32_t src_vs = 0, src_us = 0, src_vsz = 0, src_usz = 0;
     uint32_t src_idz[8] = {};
+    uint32_t tile_target = 0;    // synapses per tile asked for (0: chosen from the tuft's size)
 };
 
 struct FusedArea {
@@ -42,6 +44,10 @@ int prepare_fused(FusedArea& F, const bm_area_plan& P, std::string* err);
 // tuft of the area or for one.
 int plan_fused(FusedArea& F, const bm_area_plan& P);
 int plan_fused_tuft(FusedArea& F, const bm_area_plan& P, uint32_t layer, uint32_t t);
+// Replans a tiled tuft for about `target_syns` synapses per tile, keeping its
+// gather-offset buffer (the caller recompiles the offsets before the next
+// launch). False, and nothing changed, when the tuft would not stay tiled.
+bool retile_fused_tuft(FusedArea& F, const bm_area_plan& P, uint32_t layer, uint32_t t, uint32_t target_syns);
 void free_fused(FusedArea& F);
 // Synapse flags + synapse cycle + dendrite cycle (+ tuft cycle for pyramidal
 // layers) of one tuft in one launch.
@@ -52,5 +58,26 @@ void launch_fused_tuft(const FusedArea& F, const uint8_t* axns, const SliceRec* 
 void launch_verify_tufts(const FusedArea& F, const DevLayer& L, uint32_t layer, AreaCtl* ctl, cudaStream_t s);
 void launch_compile_tuft(const FusedArea& F, const DevLayer& L, uint32_t layer, uint32_t t, AreaCtl* ctl,
                          cudaStream_t s);
+
+// Batched form: one launch for tuft t of layer `layer` of several areas.
+struct FusedJob {
+    const FusedArea* F;
+    const DevLayer* L;
+    const uint8_t* axns;
+    const SliceRec* slices;
+    AreaCtl* ctl;
+};
+struct FusedBatch {
+    bool ok = false;        // every job is tiled and the ring fits: one launch serves them all
+    bool tuft = false;      // pyramidal layer
+    void* d_jobs = nullptr; // device argument blocks, one per job
+    uint32_t* d_tile0 = nullptr;
+    uint32_t n_jobs = 0, n_tiles = 0, nst = 2, halo_off = 0, smem = 0, grid = 1;
+};
+// Plans the launch (B.ok false when some job cannot share it; the caller then
+// launches each job's own form). Copies the argument blocks to the device.
+int prepare_fused_batch(FusedBatch& B, const std::vector<FusedJob>& jobs, uint32_t layer, uint32_t t);
+void launch_fused_batch(const FusedBatch& B, cudaStream_t s);
+void free_fused_batch(FusedBatch& B);
 
 }  // namespace bm

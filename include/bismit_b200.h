@@ -370,6 +370,51 @@ int bm_area_reset_profile(bm_area area);
 /* Number of kernel launches bm_area_cycle issues per cycle for this area. */
 int bm_area_launches_per_cycle(bm_area area, uint32_t* out);
 
+/* ------------------------------------------------------------- batches ---
+ * A batch cycles several areas together: instances of uneven column-grid
+ * sizes that share one layer map, settings and execution path (the same
+ * stage program). Each stage step runs as one launch over every area, and the
+ * whole cycle is captured once as a CUDA graph and replayed. Every area keeps
+ * its own state; an area's bytes after a batched cycle are the bytes it would
+ * have after bm_area_cycle alone. Replaces bismit's one-area-at-a-time loop
+ * over areas in Cortex::cycle (src/cortex/cortex.rs:99-119), where every area
+ * enqueues its own kernels.
+ *
+ * The areas stay owned by the caller and usable on their own (reads, writes,
+ * bm_area_cycle); destroy the batch before any of its areas. */
+typedef struct bm_batch_s* bm_batch;
+
+int bm_batch_create(bm_ctx ctx, const bm_area* areas, uint32_t n_areas, bm_batch* out);
+int bm_batch_destroy(bm_batch batch);
+
+/* Graph capture and replay of the cycle (default on); off: the same launches
+ * issued every cycle. */
+int bm_batch_set_graph(bm_batch batch, int on);
+
+/* n cycles of every area, inputs as last written to each area. */
+int bm_batch_cycle(bm_batch batch, uint32_t n_cycles);
+
+/* Bytes of one cycle's frame block: input 0 of every area, packed in batch
+ * order (0 if some area has no input layer). */
+int bm_batch_frame_bytes(bm_batch batch, uint64_t* out);
+
+/* n cycles, each first copying its frame block (cycle k at dev_frames +
+ * k * frame_bytes) into the areas' input layers. */
+int bm_batch_cycle_frames_device(bm_batch batch, const void* dev_frames, uint32_t n_cycles);
+
+/* Kernel launches per batched cycle (all areas together). */
+int bm_batch_launches_per_cycle(bm_batch batch, uint32_t* out);
+
+/* OR of the areas' sticky device error bits; BM_ERR_TIMEOUT when any is set. */
+int bm_batch_device_errors(bm_batch batch, uint32_t* bits);
+
+/* Chooses the tile size of each batched tuft step by timing candidates on the
+ * batch itself (the buffers the trials write are saved and restored, so the
+ * areas' state is unchanged). With a non-NULL cache_path, choices already in
+ * that file are applied without timing and new ones are added to it.
+ * *n_tuned (optional) = steps tuned. Synchronous. */
+int bm_batch_autotune(bm_batch batch, const char* cache_path, uint32_t* n_tuned);
+
 /* One tuft's stage of a cycle -- synapse flags, synapse cycle, dendrite cycle,
  * and for pyramidal layers the tuft cycle -- on a state slab the CALLER owns,
  * without allocating any device memory. No counterpart in the reference: bismit

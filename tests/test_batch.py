@@ -1,0 +1,177 @@
+"""Batched cycling (bm_batch_*): several areas of one layer map and uneven
+sizes advanced together must leave every area with exactly the bytes it has
+after cycling alone, and those bytes must match the oracle.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import oracle
+from bismit_b200 import _ffi as F, configs, cortex, map as M
+from helpers import diff_report, scramble
+
+# (side, depth, distal dens, distal syns): a small spread of the batched
+# workload's shapes, proximal 1 x 1 tufts included (the unfused sub-stages).
+SMALL = [(32, 1, 8, 16), (48, 2, 16, 32), (64, 1, 8, 64), (40, 3, 16, 16)]
+
+
+def _desc(side, depth, dens, syns, settings=None):
+    lmaps, areas = configs.instance_area(side, depth, dens, syns)
+    return M.area_desc("v1", lmaps, areas, settings or configs.bench_settings())
+
+
+def _deep_desc(side):
+    """The area_48_deep layer map (fused proximal 4 x 16 tufts) on other grids."""
+    lmaps, areas = configs.benchmark_area(side, 32, 2, 4, 16, 3)
+    return M.area_desc("v1", lmaps, areas, configs.bench_settings())
+
+
+def _frames(area, n, seed):
+    return configs.frames(n, int(area.plan.inputs[0].len), 0.03, seed)
+
+
+def _pairs(ctx, descs, seed=5):
+    """Twin areas per descriptor: one to batch, one to cycle alone, from the
+    same scrambled state."""
+    batched, alone = [], []
+    for k, d in enumerate(descs):
+        a = cortex.CorticalArea(ctx, d, seed + k)
+        b = cortex.CorticalArea(ctx, d, seed + k)
+        slab = a.read_slab()
+        scramble(a.plan, slab, 100 + k)
+        a.write_slab(slab)
+        b.write_slab(slab)
+        a.set_cycle(0)
+        b.set_cycle(0)
+        batched.append(a)
+        alone.append(b)
+    return batched, alone
+
+
+def _check_equal(batched, alone, when):
+    for k, (a, b) in enumerate(zip(batched, alone)):
+        x, y = a.read_slab(), b.read_slab()
+        assert np.array_equal(x, y), "%s, area %d:\n%s" % (when, k, diff_report(a.plan, x, y))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("graph", [True, False], ids=["graph", "eager"])
+@pytest.mark.parametrize("kind", ["instances", "deep"])
+def test_batch_matches_areas_alone(graph, kind):
+    ctx = cortex._Ctx(0)
+    descs = [_desc(*s) for s in SMALL] if kind == "instances" else [_deep_desc(s) for s in (32, 48, 56)]
+    batched, alone = _pairs(ctx, descs)
+    batch = cortex.Batch(ctx, batched, graph=graph)
+    fr = [_frames(a, 6, 30 + k) for k, a in enumerate(batched)]
+    for c in range(6):
+        for k in range(len(batched)):
+            batched[k].write_input(fr[k][c])
+            alone[k].write_input(fr[k][c])
+            alone[k].cycle(1)
+        batch.cycle(1)
+        _check_equal(batched, alone, "cycle %d" % c)
+    assert batch.device_errors() == 0
+    assert all(a.cycle_count() == 6 for a in batched)
+    batch.close()
+    for a in batched + alone:
+        a.close()
+    ctx.close()
+
+
+@pytest.mark.gpu
+def test_batch_frames_from_device_match_areas_alone():
+    import torch
+    ctx = cortex._Ctx(0)
+    batched, alone = _pairs(ctx, [_desc(*s) for s in SMALL])
+    batch = cortex.Batch(ctx, batched)
+    n = 5
+    fr = [_frames(a, n, 60 + k) for k, a in enumerate(batched)]
+    packed = batch.pack_frames(fr)
+    assert packed.shape == (n, batch.frame_bytes())
+    dev = torch.from_numpy(packed).to("cuda:0")
+    torch.cuda.synchronize()
+    batch.cycle_frames_device(dev.data_ptr(), n)
+    ctx.synchronize()
+    for c in range(n):
+        for k in range(len(alone)):
+            alone[k].write_input(fr[k][c])
+            alone[k].cycle(1)
+    _check_equal(batched, alone, "after %d device-fed cycles" % n)
+    batch.close()
+    for a in batched + alone:
+        a.close()
+    ctx.close()
+
+
+@pytest.mark.gpu
+def test_batch_matches_oracle():
+    ctx = cortex._Ctx(0)
+    batched, alone = _pairs(ctx, [_desc(*s) for s in SMALL[:3]])
+    batch = cortex.Batch(ctx, batched)
+    ora = [a.read_slab() for a in batched]
+    fr = [_frames(a, 4, 80 + k) for k, a in enumerate(batched)]
+    for c in range(4):
+        for k, a in enumerate(batched):
+            a.write_input(fr[k][c])
+        batch.cycle(1)
+        for k, a in enumerate(batched):
+            oracle.run(a.plan, ora[k], fr[k][c:c + 1], 1, start_cycle=c)
+            dev = a.read_slab()
+            assert np.array_equal(dev, ora[k]), "cycle %d area %d:\n%s" % (c, k, diff_report(a.plan, dev, ora[k]))
+    batch.close()
+    for a in batched + alone:
+        a.close()
+    ctx.close()
+
+
+@pytest.mark.gpu
+def test_batch_autotune_keeps_state_and_parity(tmp_path):
+    ctx = cortex._Ctx(0)
+    batched, alone = _pairs(ctx, [_desc(*s) for s in SMALL])
+    batch = cortex.Batch(ctx, batched)
+    before = [a.read_slab() for a in batched]
+    cache = str(tmp_path / "tiles.txt")
+    n = batch.autotune(cache)
+    assert n >= 1
+    for a, s in zip(batched, before):
+        assert np.array_equal(a.read_slab(), s), "autotune changed an area's state"
+    lines = open(cache).read().split("\n")
+    assert any(l.strip() for l in lines)
+    assert batch.autotune(cache) == n   # applied from the cache
+    fr = [_frames(a, 4, 90 + k) for k, a in enumerate(batched)]
+    for c in range(4):
+        for k in range(len(batched)):
+            batched[k].write_input(fr[k][c])
+            alone[k].write_input(fr[k][c])
+            alone[k].cycle(1)
+        batch.cycle(1)
+    _check_equal(batched, alone, "after autotune")
+    batch.close()
+    for a in batched + alone:
+        a.close()
+    ctx.close()
+
+
+@pytest.mark.gpu
+def test_batch_rejects_areas_with_different_programs():
+    ctx = cortex._Ctx(0)
+    a = cortex.CorticalArea(ctx, _desc(32, 1, 8, 16), 1)
+    b = cortex.CorticalArea(ctx, _desc(32, 1, 8, 16, configs.bench_settings().disable_learning()), 1)
+    with pytest.raises(F.BismitError) as e:
+        cortex.Batch(ctx, [a, b])
+    assert e.value.code == F.BM_ERR_UNSUPPORTED
+    a.close()
+    b.close()
+    ctx.close()
+
+
+def test_batch_instances_are_seeded_and_in_range():
+    x = configs.batch_instances(64, 0)
+    assert x == configs.batch_instances(64, 0)
+    assert x != configs.batch_instances(64, 1)
+    for side, depth, dens, syns, act in x:
+        assert side in range(32, 193, 16) and 1 <= depth <= 4
+        assert dens in (8, 16) and syns in (16, 32, 64) and 0.01 <= act <= 0.04
+    # The first instance does not depend on how many are drawn.
+    assert configs.batch_instances(1, 0)[0] == x[0]
