@@ -40,6 +40,8 @@ def parse():
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-sample-seconds", type=float, default=12.0)
+    ap.add_argument("--no-batched", action="store_true", help="skip the batched-instances measurement")
+    ap.add_argument("--batch-instances", type=int, default=64)
     return ap.parse_args()
 
 
@@ -177,6 +179,113 @@ def cpu_baseline(plan, slab, frames, budget_s, prefer_ref=True):
             "sample": "%d cycle(s) of %s on the host cores (%.1f s)" % (n, "the same area", dt)}
 
 
+SOAK_S = 0.6   # seconds of the same cycles on each side of a timed region, for the clock samples
+
+
+def soak(fn, stream, seconds):
+    """Keeps the GPU on the timed workload for `seconds` (nvidia-smi samples
+    every 200 ms, longer than most timed regions)."""
+    t0 = time.perf_counter()
+    while time.perf_counter() - t0 < seconds:
+        fn()
+        stream.synchronize()
+
+
+def alg_bytes_cycle(plan):
+    """Algorithmic bytes of one full cycle: 7 per synapse, 4 per dendrite, 12
+    per cell-tuft, 4 per cell, plus the input frame."""
+    b = 0
+    for i in range(plan.n_layers):
+        L = plan.layers[i]
+        b += 7 * int(L.n_syns) + 4 * int(L.n_dens) + 4 * int(L.cells)
+        if L.kind == 2:
+            b += 12 * int(L.cells) * int(L.n_tufts)
+    if plan.n_inputs:
+        b += int(plan.inputs[0].len)
+    return b
+
+
+def run_batched(args, ctx, stream, K, W, ws):
+    """The batched-instances workload: `--batch-instances` independent areas of
+    uneven size (configs.batch_instances), cycled (a) as one batch with graph
+    replay and (b) in the plain form, one area after another with one kernel
+    per reference stage, on the same seeded frames. Returns the JSON object."""
+    import torch
+    from bismit_b200 import configs, cortex, map as M
+    n = args.batch_instances
+    ins = configs.batch_instances(n, args.seed)
+    areas_b, areas_p, frames_h = [], [], []
+    for i, (side, depth, dens, syns, act) in enumerate(ins):
+        lmaps, areas = configs.instance_area(side, depth, dens, syns)
+        st = configs.bench_settings()
+        areas_b.append(cortex.CorticalArea(ctx, M.area_desc("v1", lmaps, areas, st), args.seed * 1000 + i))
+        areas_p.append(cortex.CorticalArea(ctx, M.area_desc("v1", lmaps, areas, st.plain_kernels()),
+                                           args.seed * 1000 + i))
+        frames_h.append(configs.frames(K + W, areas_b[-1].input_len(), act, args.seed * 1000 + i))
+    n_syn = sum(int(a.plan.n_syns_total) for a in areas_b)
+    alg = sum(alg_bytes_cycle(a.plan) for a in areas_b)
+    batch = cortex.Batch(ctx, areas_b)
+    t_tune = time.perf_counter()
+    tuned = batch.autotune(None)
+    t_tune = time.perf_counter() - t_tune
+    fb = batch.frame_bytes()
+    packed = torch.from_numpy(batch.pack_frames(frames_h)).to("cuda")
+    per_area = [torch.from_numpy(f).to("cuda") for f in frames_h]
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+
+    def max_ms(ms):
+        if ws > 1:
+            t = torch.tensor([ms], device="cuda")
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            return float(t.item())
+        return ms
+
+    # (a) batched, graph replay
+    batch.cycle_frames_device(packed.data_ptr(), W)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    batch.cycle_frames_device(packed.data_ptr() + W * fb, K)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms_b = max_ms(e0.elapsed_time(e1))
+    # (b) plain, one area per launch sequence
+    def plain_cycles(c0, nc):
+        for c in range(c0, c0 + nc):
+            for a, f in zip(areas_p, per_area):
+                a.cycle_frames_device(f.data_ptr() + c * f.shape[1], f.shape[1], 1)
+    plain_cycles(0, W)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    plain_cycles(W, K)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms_p = max_ms(e0.elapsed_time(e1))
+    same = all(np.array_equal(a.read_output(), b.read_output()) for a, b in zip(areas_b, areas_p))
+    peak, peak_kind = peaks()
+    val_b = n_syn * K * ws / (ms_b / 1e3)
+    val_p = n_syn * K * ws / (ms_p / 1e3)
+    out = {
+        "workload": "batch_%d" % n, "instances": n, "synapses": n_syn,
+        "sizes": "side 32..192 step 16, depth 1..4, distal dens {8,16} x syns {16,32,64}, proximal 1x1, "
+                 "spiny stellate 1x32; active 1-4%",
+        "batched": {"value": val_b, "unit": UNIT, "ms_per_step": ms_b / K, "launches_per_cycle": batch.launches_per_cycle(),
+                    "graph": True, "hbm_frac": round(alg / (ms_b / K / 1e3) / 1e9 / peak, 4),
+                    "algorithmic_bytes_per_cycle": alg, "autotuned_steps": tuned, "autotune_s": round(t_tune, 2)},
+        "plain": {"value": val_p, "unit": UNIT, "ms_per_step": ms_p / K,
+                  "launches_per_cycle": sum(a.launches_per_cycle() for a in areas_p),
+                  "hbm_frac": round(alg / (ms_p / K / 1e3) / 1e9 / peak, 4)},
+        "batched_over_plain": round(ms_p / ms_b, 3),
+        "outputs_identical": bool(same),
+        "peak_source": peak_kind,
+    }
+    batch.close()
+    for a in areas_b + areas_p:
+        a.close()
+    return out
+
+
 def run_ours(args):
     import torch
     from bismit_b200 import configs, cortex, map as M
@@ -208,6 +317,7 @@ def run_ours(args):
             torch.distributed.barrier()
 
     init_slab = area.read_slab() if (rank == 0 and ws == 1 and not args.no_cpu_baseline) else None
+    out_len = area.output_len()
 
     # warm-up
     area.cycle_frames_device(dev_frames.data_ptr(), flen, W)
@@ -215,6 +325,7 @@ def run_ours(args):
     barrier()
     clocks = Clocks(local)
     clocks.start()
+    soak(lambda: area.cycle_frames_device(dev_frames.data_ptr(), flen, W), stream, SOAK_S)
     torch.cuda.synchronize()
     barrier()
     e0 = torch.cuda.Event(enable_timing=True)
@@ -224,6 +335,7 @@ def run_ours(args):
     e1.record(stream)
     torch.cuda.synchronize()
     barrier()
+    soak(lambda: area.cycle_frames_device(dev_frames.data_ptr(), flen, W), stream, SOAK_S)
     clk = clocks.stop()
     ms = e0.elapsed_time(e1)
     launches = area.launches_per_cycle() * K
@@ -258,7 +370,6 @@ def run_ours(args):
     # End to end through the public API with host buffers.
     import ctypes
     pin_in = torch.from_numpy(host_frames).pin_memory()
-    out_len = area.output_len()
     pin_out = torch.empty(out_len, dtype=torch.uint8).pin_memory()
     lib = area.lib
     torch.cuda.synchronize()
@@ -280,6 +391,9 @@ def run_ours(args):
         e2e_ms = float(t.item())
     e2e_val = n_syn * K * ws / (e2e_ms / 1e3)
 
+    area.close()
+    batched = None if args.no_batched else run_batched(args, ctx, stream, K, W, ws)
+
     cpu = None
     if init_slab is not None:
         cpu = cpu_baseline(plan, init_slab, host_frames, args.cpu_sample_seconds)
@@ -287,7 +401,9 @@ def run_ours(args):
     if rank == 0:
         cfg = workload_config(args.workload)
         cfg.update({"path": args.path, "synapses_per_area": n_syn, "areas": ws, "parallelism": "replicas x%d" % ws,
-                    "l2": "state slab %.2f GB per area > 126 MB L2, no flush needed" % (plan.slab_bytes / 1e9)})
+                    "l2": "state slab %.2f GB per area > 126 MB L2, no flush needed" % (plan.slab_bytes / 1e9),
+                    "clocks_window": "nvidia-smi every 200 ms over the timed region plus %.1f s of the same "
+                                     "cycles on each side" % SOAK_S})
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": K, "warmup": W,
             "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -299,9 +415,9 @@ def run_ours(args):
             "roofline": roofline,
             "cpu_baseline": cpu,
             "kernels": {k: {"launches": v[0], "ms": round(v[1], 4)} for k, v in prof.items()},
+            "batched_instances": batched,
         }
         print(json.dumps(line), flush=True)
-    area.close()
     ctx.close()
     if ws > 1:
         torch.distributed.destroy_process_group()
