@@ -205,6 +205,7 @@ def lib():
         "bm_batch_set_graph": (C.c_int, [vp, C.c_int]),
         "bm_batch_cycle": (C.c_int, [vp, u32]),
         "bm_batch_frame_bytes": (C.c_int, [vp, P(u64)]),
+        "bm_batch_connect": (C.c_int, [vp, u32, u32, u32, u32, u64]),
         "bm_batch_cycle_frames_device": (C.c_int, [vp, vp, u32]),
         "bm_batch_launches_per_cycle": (C.c_int, [vp, P(u32)]),
         "bm_batch_device_errors": (C.c_int, [vp, P(u32)]),

@@ -113,6 +113,60 @@ def batch_instances(n=64, seed=0, sides=range(32, 193, 16)):
     return out
 
 
+def _hierarchy_map(name, depth, feedback):
+    lm = LayerMapScheme(name, LayerMapKind.Cortical)
+    lm.layer(LayerScheme.define("aff_in").axonal(AxonTopology.Spatial)
+             .axon_domain(AxonDomain.input([(InputTrack.Afferent, [THAL_SP])])))
+    if feedback:
+        lm.layer(LayerScheme.define("eff_in").axonal(AxonTopology.Spatial)
+                 .axon_domain(AxonDomain.input([(InputTrack.Efferent, [THAL_SP])])))
+    lm.layer(LayerScheme.define("iv").depth(1).tags(LayerTags.PSAL).axon_domain(AxonDomain.Local)
+             .cellular(CellScheme.spiny_stellate()
+                       .tft(TuftScheme.basal().proximal().syns_per_den(32)
+                            .src_lyr(TuftSourceLayer.define("aff_in").syn_reach(6).prevalence(1)))))
+    lm.layer(LayerScheme.define("iv_inhib")
+             .cellular(CellScheme.control(ControlCellKind.InhibitoryBasketSurround("iv", 4), 0)))
+    pyr = (CellScheme.pyramidal()
+           .tft(TuftScheme.basal().proximal().dens_per_tft(1).syns_per_den(1)
+                .src_lyr(TuftSourceLayer.define("iv").syn_reach(0).prevalence(1)))
+           .tft(TuftScheme.basal().distal().dens_per_tft(16).syns_per_den(32).max_active_dens_l2(3)
+                .src_lyr(TuftSourceLayer.define("iii").syn_reach(6).prevalence(1))))
+    if feedback:
+        pyr.tft(TuftScheme.apical().distal().dens_per_tft(16).syns_per_den(32).max_active_dens_l2(3)
+                .src_lyr(TuftSourceLayer.define("eff_in").syn_reach(6).prevalence(1)))
+    lm.layer(LayerScheme.define("iii").depth(depth).tags(LayerTags.PTAL)
+             .axon_domain(AxonDomain.output([THAL_SP])).cellular(pyr))
+    lm.layer(LayerScheme.define("iii_col")
+             .cellular(CellScheme.control(ControlCellKind.IntraColumnInhib("iii"), 0)))
+    return lm
+
+
+def hierarchy(sides=(128, 192, 96), depth=2):
+    """The three-area hierarchy: cortical areas v1 -> v2 -> v3 of the given
+    sides, fed by an external area v0 the size of v1. Each area has the 64 x 64
+    area's layer shapes at pyramidal depth `depth`; its feed-forward input
+    `aff_in` comes from the previous area's output layer iii. Every area but
+    the top one also has an efferent input `eff_in`, fed back from the next
+    area's iii, which an apical distal tuft (16 x 32, reach 6) samples: bismit
+    requires the source slices of one tuft to offer equal offset pools
+    (SynSrcSlices::new), which slices of another area's scale do not, so the
+    feedback gets a tuft of its own. Returns (lmaps, areas, cortical area
+    names in order)."""
+    lmaps = LayerMapSchemeList()
+    areas = AreaSchemeList()
+    _external(lmaps, areas, "v0", sides[0])
+    lmaps.add(_hierarchy_map("visual", depth, True))
+    lmaps.add(_hierarchy_map("visual_top", depth, False))
+    names = ["v%d" % (k + 1) for k in range(len(sides))]
+    for k, (n, side) in enumerate(zip(names, sides)):
+        top = k + 1 == len(names)
+        a = AreaScheme(n, "visual_top" if top else "visual", side).eff_areas(["v0" if k == 0 else names[k - 1]])
+        if not top:
+            a.aff_areas([names[k + 1]])
+        areas.area(a)
+    return lmaps, areas, names
+
+
 def bench_settings():
     return CorticalAreaSettings().disable_regrowth().strengths_start_at_zero()
 

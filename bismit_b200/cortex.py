@@ -12,7 +12,7 @@ import ctypes as C
 import numpy as np
 
 from . import _ffi as F
-from .map import (AreaSchemeList, CorticalAreaSettings, LayerMapKind, LayerMapSchemeList, area_desc)
+from .map import (AreaSchemeList, CorticalAreaSettings, LayerMapKind, LayerMapSchemeList, area_desc, area_tracts)
 
 
 class _Ctx:
@@ -243,7 +243,12 @@ class Batch:
 
 
 class Cortex:
-    """A set of cortical areas cycled in order (Cortex, src/cortex/cortex.rs:37-120)."""
+    """A set of cortical areas (Cortex, src/cortex/cortex.rs:37-120). The areas
+    are cycled together as one batch; outputs of one area that feed inputs of
+    another (the thalamic routing of the area schemes) travel as tracts,
+    copied at the head of every cycle from the previous cycle's outputs.
+    Inputs fed from outside (subcortical areas) are written per area with
+    `area(name).write_input(..)`; `external_inputs()` lists them."""
 
     def __init__(self, lmaps, areas, settings=None, seed=0, device=0):
         self.ctx = _Ctx(device)
@@ -255,23 +260,38 @@ class Cortex:
             d = area_desc(a.name, lmaps, areas, settings)
             self.areas[a.name] = CorticalArea(self.ctx, d, seed, a.name)
             self._order.append(a.name)
+        plans = [self.areas[n].plan for n in self._order]
+        self.tracts, self.external = area_tracts(lmaps, areas, self._order, plans)
+        self.batch = Batch(self.ctx, [self.areas[n] for n in self._order]) if self._order else None
+        for (sk, so, dk, di, off, _n) in self.tracts:
+            F.check(self.batch.lib.bm_batch_connect(self.batch.h, sk, so, dk, di, C.c_uint64(off)))
 
     @staticmethod
     def builder(lmaps, areas):
         return CortexBuilder(lmaps, areas)
 
-    def cycle(self):
-        """Cortex::cycle: every area once, in area order (src/cortex/cortex.rs:100-120)."""
-        for n in self._order:
-            self.areas[n].cycle(1)
+    def cycle(self, n=1):
+        """Cortex::cycle: every area once (src/cortex/cortex.rs:99-119)."""
+        if self.batch is not None:
+            self.batch.cycle(n)
 
     def area(self, name):
         return self.areas[name]
+
+    def area_names(self):
+        return list(self._order)
+
+    def external_inputs(self):
+        """[(area name, input index, axon offset, axons, source area, source layer)]
+        of the inputs no area of this cortex feeds."""
+        return [(self._order[k], i, off, n, src, sl) for (k, i, off, n, src, sl) in self.external]
 
     def synchronize(self):
         self.ctx.synchronize()
 
     def close(self):
+        if self.batch is not None:
+            self.batch.close()
         for a in self.areas.values():
             a.close()
         self.ctx.close()

@@ -12,9 +12,11 @@
 //     blocks are split among the areas by a block prefix table, running the
 //     same per-item bodies as the one-area kernels (bm_items.cuh);
 //   * cycle end: one launch advancing every area's device cycle counter.
-// Inputs come either from each area's own bm_area_write_input, or for
-// bm_batch_cycle_frames_device from a device array of per-cycle frame blocks,
-// copied in by one intake launch at the head of each cycle.
+// Inputs come from tracts (another area's output axons, bm_batch_connect),
+// from each area's own bm_area_write_input, or for
+// bm_batch_cycle_frames_device from a device array of per-cycle frame blocks.
+// One copy launch at the head of each cycle does the tracts and the frame
+// intake, so every tract carries its source's output of the previous cycle.
 //
 // A project-written autotuner (bm_batch_autotune) picks the tile size of each
 // batched tuft step by timing candidates on the live batch (with the touched
@@ -46,10 +48,12 @@ struct CellJob {
     uint32_t block0;    // first block of this job
 };
 
-// One area's share of the batched intake.
+// One copy at the head of a cycle: a tract (src is a device pointer) or an
+// input taken from the cycle's frame block (src_off within the block).
 struct IntakeJob {
-    uint8_t* dst;       // the input layer's first axon
-    uint64_t src_off;   // offset within one cycle's frame block
+    uint8_t* dst;
+    const uint8_t* src;  // tract source, or null: from the frame block
+    uint64_t src_off;
     uint32_t len;
     uint32_t block0;
 };
@@ -114,10 +118,12 @@ __global__ void __launch_bounds__(kCellBlock) k_batch_cells(const CellJob* __res
 
 __global__ void __launch_bounds__(kIntakeBlock)
     k_batch_intake(const IntakeJob* __restrict__ jobs, uint32_t n_jobs, const BatchCtl* __restrict__ bc) {
-    const uint8_t* frames = bc->frames;
-    if (!frames) return;
     const IntakeJob& J = jobs[block_job(jobs, n_jobs)];
-    const uint8_t* src = frames + bc->cursor * bc->frame_bytes + J.src_off;
+    const uint8_t* src = J.src;
+    if (!src) {
+        if (!bc->frames) return;   // inputs as last written per area
+        src = bc->frames + bc->cursor * bc->frame_bytes + J.src_off;
+    }
     const uint32_t i0 = ((blockIdx.x - J.block0) * kIntakeBlock + threadIdx.x) * kIntakePerThread;
 #pragma unroll
     for (uint32_t k = 0; k < kIntakePerThread; k++)
@@ -179,19 +185,29 @@ struct bm_batch_s {
         std::vector<CellLaunch> cells;   // F_CELLS: launches in order
         FusedBatch fb;
     };
+    // Areas with one stage program, batched step by step.
+    struct Group {
+        std::vector<bm_area> areas;
+        std::vector<StepPlan> plan;
+        uint32_t launches = 0;
+    };
     bm_ctx ctx = nullptr;
-    std::vector<bm_area> areas;
-    std::vector<StepPlan> plan;
+    std::vector<bm_area> areas;          // every area, in batch order
+    std::vector<Group> groups;
+    struct Tract {
+        uint32_t src_area, src_output, dst_area, dst_input;
+        uint64_t dst_off;
+    };
+    std::vector<Tract> tracts;
     IntakeJob* d_intake = nullptr;
-    uint32_t intake_blocks = 0;
-    uint64_t frame_bytes = 0;
+    uint32_t n_intake = 0, intake_blocks = 0;
+    uint64_t frame_bytes = 0;            // external inputs of one cycle
     BatchCtl* d_bctl = nullptr;
     AreaCtl** d_ctls = nullptr;
     bool use_graph = true;
     cudaStream_t cap = nullptr;          // private stream for graph capture
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
-    uint32_t launches = 0;               // kernel launches of one cycle
 
     cudaStream_t stream() const { return ctx->stream(); }
     void drop_graph() {
@@ -204,19 +220,19 @@ struct bm_batch_s {
 
 namespace {
 
-void free_plan(bm_batch_s* B) {
-    for (auto& p : B->plan) {
+void free_plan(bm_batch_s::Group& G) {
+    for (auto& p : G.plan) {
         for (auto& c : p.cells) cudaFree(c.d_jobs);
         free_fused_batch(p.fb);
     }
-    B->plan.clear();
+    G.plan.clear();
 }
 
 void free_batch(bm_batch_s* B) {
     if (!B) return;
     DevGuard g(B->ctx->device);
     B->drop_graph();
-    free_plan(B);
+    for (auto& G : B->groups) free_plan(G);
     if (B->d_intake) cudaFree(B->d_intake);
     if (B->d_bctl) cudaFree(B->d_bctl);
     if (B->d_ctls) cudaFree(B->d_ctls);
@@ -237,11 +253,11 @@ uint64_t items_of(const bm_area_s* A, int k, const Step& st) {
 }
 
 // One batched per-cell launch of kind k for step st over every area.
-int add_cells(bm_batch_s* B, bm_batch_s::StepPlan& p, int k) {
+int add_cells(bm_batch_s::Group& G, bm_batch_s::StepPlan& p, int k) {
     const Step& st = p.st;
     std::vector<CellJob> jobs;
     uint64_t blocks = 0;
-    for (bm_area A : B->areas) {
+    for (bm_area A : G.areas) {
         CellJob J;
         std::memset(&J, 0, sizeof J);
         J.L = A->dl[st.layer];
@@ -273,9 +289,9 @@ int add_cells(bm_batch_s* B, bm_batch_s::StepPlan& p, int k) {
     return BM_OK;
 }
 
-int build_fused(bm_batch_s* B, bm_batch_s::StepPlan& p) {
+int build_fused(bm_batch_s::Group& G, bm_batch_s::StepPlan& p) {
     std::vector<FusedJob> jobs;
-    for (bm_area A : B->areas) {
+    for (bm_area A : G.areas) {
         if (!A->fused.t[p.st.layer][p.st.idx].ok) return BM_OK;
         jobs.push_back({&A->fused, &A->dl[p.st.layer], A->axns(), A->slices, A->ctl});
     }
@@ -285,77 +301,131 @@ int build_fused(bm_batch_s* B, bm_batch_s::StepPlan& p) {
     return BM_OK;
 }
 
-int build_step(bm_batch_s* B, bm_batch_s::StepPlan& p) {
+int build_step(bm_batch_s::Group& G, bm_batch_s::StepPlan& p) {
     const Step& st = p.st;
     if (st.kind == ST_CYCLE_END) {
         p.form = bm_batch_s::F_END;
         return BM_OK;
     }
-    if (is_cell_step(st.kind)) return add_cells(B, p, st.kind);
+    if (is_cell_step(st.kind)) return add_cells(G, p, st.kind);
     if (st.kind != ST_TUFT) return BM_OK;   // the plain form's whole-layer tuft stages: each area's own
     bool none_ok = true, all_ok = true;
-    for (bm_area A : B->areas) {
+    for (bm_area A : G.areas) {
         const bool ok = A->fused.t[st.layer][st.idx].ok;
         none_ok = none_ok && !ok;
         all_ok = all_ok && ok;
     }
-    if (all_ok) return build_fused(B, p);
+    if (all_ok) return build_fused(G, p);
     if (!none_ok) return BM_OK;
     // No area can take the fused kernel here (e.g. one-synapse dendrites):
     // the tuft's four stages, each batched.
-    int rc = add_cells(B, p, BK_FLAGS);
-    if (rc == BM_OK) rc = add_cells(B, p, BK_SYN);
-    if (rc == BM_OK) rc = add_cells(B, p, BK_DEN);
-    if (rc == BM_OK && B->areas[0]->plan.layers[st.layer].kind == BM_LYR_PYRAMIDAL) rc = add_cells(B, p, BK_TFT);
+    int rc = add_cells(G, p, BK_FLAGS);
+    if (rc == BM_OK) rc = add_cells(G, p, BK_SYN);
+    if (rc == BM_OK) rc = add_cells(G, p, BK_DEN);
+    if (rc == BM_OK && G.areas[0]->plan.layers[st.layer].kind == BM_LYR_PYRAMIDAL) rc = add_cells(G, p, BK_TFT);
     return rc;
 }
 
-int build_plan(bm_batch_s* B) {
-    free_plan(B);
-    const std::vector<Step>& steps = B->areas[0]->steps;
-    B->launches = 1;   // intake
-    for (const Step& st : steps) {
-        bm_batch_s::StepPlan p;
-        p.st = st;
-        int rc = build_step(B, p);
-        B->plan.push_back(p);
-        if (rc != BM_OK) return rc;
+void count_launches(bm_batch_s::Group& G) {
+    G.launches = 0;
+    for (const auto& p : G.plan) {
+        const Step& st = p.st;
         if (p.form == bm_batch_s::F_EACH) {
             // Each area's own launches for this step.
-            bm_area A = B->areas[0];
-            const bm_layer_plan& L = A->plan.layers[st.layer];
-            uint32_t per = 1;
-            if (st.kind == ST_TUFT && !A->fused.t[st.layer][st.idx].ok) per = L.kind == BM_LYR_PYRAMIDAL ? 4 : 3;
-            if (st.kind == ST_TUFTS_PLAIN) per = 1 + 2 * L.n_tufts + (L.kind == BM_LYR_PYRAMIDAL ? L.n_tufts : 0);
-            B->launches += per * (uint32_t)B->areas.size();
+            for (bm_area A : G.areas) {
+                const bm_layer_plan& L = A->plan.layers[st.layer];
+                uint32_t per = 1;
+                if (st.kind == ST_TUFT && !A->fused.t[st.layer][st.idx].ok) per = L.kind == BM_LYR_PYRAMIDAL ? 4 : 3;
+                if (st.kind == ST_TUFTS_PLAIN) per = 1 + 2 * L.n_tufts + (L.kind == BM_LYR_PYRAMIDAL ? L.n_tufts : 0);
+                G.launches += per;
+            }
         } else if (p.form == bm_batch_s::F_CELLS) {
-            B->launches += (uint32_t)p.cells.size();
-        } else {
-            B->launches += 1;
+            G.launches += (uint32_t)p.cells.size();
+        } else if (p.form == bm_batch_s::F_FUSED) {
+            G.launches += 1;
         }
     }
+}
+
+// The group's steps; the cycle-end step is done once for the whole batch.
+int build_plan(bm_batch_s::Group& G) {
+    free_plan(G);
+    for (const Step& st : G.areas[0]->steps) {
+        bm_batch_s::StepPlan p;
+        p.st = st;
+        int rc = build_step(G, p);
+        G.plan.push_back(p);
+        if (rc != BM_OK) return rc;
+    }
+    count_launches(G);
+    return BM_OK;
+}
+
+// The head-of-cycle copies: every tract, then every input of every area that
+// no tract feeds, taken from the frame block in (area, input) order.
+int build_intake(bm_batch_s* B) {
+    if (B->d_intake) cudaFree(B->d_intake);
+    B->d_intake = nullptr;
+    B->n_intake = B->intake_blocks = 0;
+    B->frame_bytes = 0;
+    std::vector<IntakeJob> jobs;
+    uint64_t blocks = 0;
+    const uint32_t per_block = kIntakeBlock * kIntakePerThread;
+    auto add = [&](IntakeJob J) {
+        J.block0 = (uint32_t)blocks;
+        blocks += (J.len + per_block - 1) / per_block;
+        jobs.push_back(J);
+    };
+    for (const auto& T : B->tracts) {
+        bm_area S = B->areas[T.src_area], D = B->areas[T.dst_area];
+        IntakeJob J{};
+        J.dst = D->axns() + D->plan.inputs[T.dst_input].axn_idz + T.dst_off;
+        J.src = S->axns() + S->plan.outputs[T.src_output].axn_idz;
+        J.len = S->plan.outputs[T.src_output].len;
+        add(J);
+    }
+    for (uint32_t a = 0; a < B->areas.size(); a++) {
+        bm_area A = B->areas[a];
+        for (uint32_t i = 0; i < A->plan.n_inputs; i++) {
+            bool fed = false;
+            for (const auto& T : B->tracts) fed = fed || (T.dst_area == a && T.dst_input == i);
+            if (fed) continue;
+            IntakeJob J{};
+            J.dst = A->axns() + A->plan.inputs[i].axn_idz;
+            J.src_off = B->frame_bytes;
+            J.len = A->plan.inputs[i].len;
+            B->frame_bytes += J.len;
+            add(J);
+        }
+    }
+    if (jobs.empty()) return BM_OK;
+    if (blocks > 0x7FFFFFFFull) return set_err(BM_ERR_UNSUPPORTED, "batched intake too large");
+    cudaError_t e = cudaMalloc(&B->d_intake, jobs.size() * sizeof(IntakeJob));
+    if (e == cudaSuccess) e = cudaMemcpy(B->d_intake, jobs.data(), jobs.size() * sizeof(IntakeJob), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return cuda_err(e, "batched intake jobs");
+    B->n_intake = (uint32_t)jobs.size();
+    B->intake_blocks = (uint32_t)blocks;
     return BM_OK;
 }
 
 void enqueue_batch_cycle(bm_batch_s* B, cudaStream_t s) {
     if (B->intake_blocks)
-        k_batch_intake<<<B->intake_blocks, kIntakeBlock, 0, s>>>(B->d_intake, (uint32_t)B->areas.size(), B->d_bctl);
-    for (auto& p : B->plan) {
-        switch (p.form) {
-        case bm_batch_s::F_CELLS:
-            for (auto& c : p.cells) launch_cells(c.kind, c.d_jobs, c.n_jobs, c.n_blocks, s);
-            break;
-        case bm_batch_s::F_FUSED: launch_fused_batch(p.fb, s); break;
-        case bm_batch_s::F_END: {
-            const uint32_t n = (uint32_t)B->areas.size();
-            k_batch_cycle_end<<<(n + 127) / 128, 128, 0, s>>>(B->d_ctls, n, B->d_bctl);
-            break;
+        k_batch_intake<<<B->intake_blocks, kIntakeBlock, 0, s>>>(B->d_intake, B->n_intake, B->d_bctl);
+    for (auto& G : B->groups)
+        for (auto& p : G.plan) {
+            switch (p.form) {
+            case bm_batch_s::F_CELLS:
+                for (auto& c : p.cells) launch_cells(c.kind, c.d_jobs, c.n_jobs, c.n_blocks, s);
+                break;
+            case bm_batch_s::F_FUSED: launch_fused_batch(p.fb, s); break;
+            case bm_batch_s::F_END: break;
+            default:
+                for (bm_area A : G.areas) exec_step(A, p.st, s);
+                break;
+            }
         }
-        default:
-            for (bm_area A : B->areas) exec_step(A, p.st, s);
-            break;
-        }
-    }
+    const uint32_t n = (uint32_t)B->areas.size();
+    k_batch_cycle_end<<<(n + 127) / 128, 128, 0, s>>>(B->d_ctls, n, B->d_bctl);
 }
 
 int ensure_graph(bm_batch_s* B) {
@@ -418,9 +488,9 @@ void step_ranges(bm_area_s* A, uint32_t i, uint32_t t, std::vector<Range>& out) 
         for (int k = BM_BUF_TFT_PREV_BEST_DEN_IDS; k <= BM_BUF_TFT_STATES; k++) add(k, T.cel_idz, L.cells);
 }
 
-std::string step_key(bm_batch_s* B, const Step& st) {
+std::string step_key(bm_batch_s::Group& G, const Step& st) {
     std::string k = "L" + std::to_string(st.layer) + "T" + std::to_string(st.idx);
-    for (bm_area A : B->areas) {
+    for (bm_area A : G.areas) {
         const bm_layer_plan& L = A->plan.layers[st.layer];
         const bm_tuft_plan& T = L.tufts[st.idx];
         char buf[96];
@@ -453,14 +523,14 @@ void write_cache(const char* path, const std::map<std::string, uint32_t>& m) {
 
 // Retiles tuft (i, t) of every area for `target` synapses per tile and
 // rebuilds the step's batched launch. False when some area cannot take it.
-bool apply_target(bm_batch_s* B, bm_batch_s::StepPlan& p, uint32_t target) {
-    for (bm_area A : B->areas)
+bool apply_target(bm_batch_s* B, bm_batch_s::Group& G, bm_batch_s::StepPlan& p, uint32_t target) {
+    for (bm_area A : G.areas)
         if (!retile_fused_tuft(A->fused, A->plan, p.st.layer, p.st.idx, target)) return false;
-    for (bm_area A : B->areas) {
+    for (bm_area A : G.areas) {
         A->verify_pending[p.st.layer] = true;
         run_pending_verifies(A, B->stream());
     }
-    return build_fused(B, p) == BM_OK && p.form == bm_batch_s::F_FUSED;
+    return build_fused(G, p) == BM_OK && p.form == bm_batch_s::F_FUSED;
 }
 
 }  // namespace
@@ -475,12 +545,6 @@ int bm_batch_create(bm_ctx ctx, const bm_area* areas, uint32_t n_areas, bm_batch
         if (areas[a]->ctx != ctx) return set_err(BM_ERR_INVALID, "bm_batch_create: area %u belongs to another context", a);
         for (uint32_t b = 0; b < a; b++)
             if (areas[b] == areas[a]) return set_err(BM_ERR_INVALID, "bm_batch_create: area %u appears twice", a);
-        if (!(areas[a]->steps == areas[0]->steps))
-            return set_err(BM_ERR_UNSUPPORTED,
-                           "bm_batch_create: area %u has a different stage program than area 0 (the areas of a "
-                           "batch share one layer map, settings and execution path)", a);
-        if (areas[a]->plan.n_inputs != areas[0]->plan.n_inputs)
-            return set_err(BM_ERR_UNSUPPORTED, "bm_batch_create: area %u has a different number of inputs", a);
     }
     DevGuard g(ctx->device);
     bm_batch_s* B = new (std::nothrow) bm_batch_s;
@@ -490,36 +554,27 @@ int bm_batch_create(bm_ctx ctx, const bm_area* areas, uint32_t n_areas, bm_batch
     cudaError_t e = cudaStreamCreateWithFlags(&B->cap, cudaStreamNonBlocking);
     if (e != cudaSuccess) { free_batch(B); return cuda_err(e, "cudaStreamCreate"); }
 
-    // Intake jobs: input 0 of every area, packed in batch order.
-    std::vector<IntakeJob> intake;
-    uint32_t blocks = 0;
-    const uint32_t per_block = kIntakeBlock * kIntakePerThread;
-    for (bm_area A : B->areas) {
-        if (A->plan.n_inputs == 0) continue;
-        IntakeJob J;
-        J.dst = A->axns() + A->plan.inputs[0].axn_idz;
-        J.src_off = B->frame_bytes;
-        J.len = A->plan.inputs[0].len;
-        J.block0 = blocks;
-        blocks += (J.len + per_block - 1) / per_block;
-        B->frame_bytes += J.len;
-        intake.push_back(J);
-    }
     std::vector<AreaCtl*> ctls;
     for (bm_area A : B->areas) ctls.push_back(A->ctl);
     e = cudaMalloc(&B->d_bctl, sizeof(BatchCtl));
     if (e == cudaSuccess) e = cudaMemset(B->d_bctl, 0, sizeof(BatchCtl));
     if (e == cudaSuccess) e = cudaMalloc(&B->d_ctls, ctls.size() * sizeof(AreaCtl*));
     if (e == cudaSuccess) e = cudaMemcpy(B->d_ctls, ctls.data(), ctls.size() * sizeof(AreaCtl*), cudaMemcpyHostToDevice);
-    if (e == cudaSuccess && !intake.empty()) {
-        e = cudaMalloc(&B->d_intake, intake.size() * sizeof(IntakeJob));
-        if (e == cudaSuccess)
-            e = cudaMemcpy(B->d_intake, intake.data(), intake.size() * sizeof(IntakeJob), cudaMemcpyHostToDevice);
-        B->intake_blocks = blocks;
-    }
     if (e != cudaSuccess) { free_batch(B); return cuda_err(e, "batch set-up"); }
-    if (intake.size() != B->areas.size()) B->intake_blocks = 0;   // no packed frames without an input on every area
-    int rc = build_plan(B);
+    // Areas with equal stage programs form one group (first appearance order).
+    for (bm_area A : B->areas) {
+        bm_batch_s::Group* G = nullptr;
+        for (auto& g2 : B->groups)
+            if (g2.areas[0]->steps == A->steps) G = &g2;
+        if (!G) {
+            B->groups.emplace_back();
+            G = &B->groups.back();
+        }
+        G->areas.push_back(A);
+    }
+    int rc = build_intake(B);
+    for (auto& G : B->groups)
+        if (rc == BM_OK) rc = build_plan(G);
     if (rc != BM_OK) { free_batch(B); return rc; }
     *out = B;
     return BM_OK;
@@ -549,20 +604,54 @@ int bm_batch_cycle(bm_batch batch, uint32_t n_cycles) {
 
 int bm_batch_frame_bytes(bm_batch batch, uint64_t* out) {
     if (!batch || !out) return set_err(BM_ERR_INVALID, "null argument");
-    *out = batch->intake_blocks ? batch->frame_bytes : 0;
+    *out = batch->frame_bytes;
+    return BM_OK;
+}
+
+int bm_batch_connect(bm_batch batch, uint32_t src_area, uint32_t src_output, uint32_t dst_area, uint32_t dst_input,
+                     uint64_t dst_offset) {
+    if (!batch) return set_err(BM_ERR_INVALID, "null batch");
+    bm_batch_s* B = batch;
+    const uint32_t n = (uint32_t)B->areas.size();
+    if (src_area >= n || dst_area >= n) return set_err(BM_ERR_INVALID, "bm_batch_connect: area index out of range");
+    const bm_area_plan& S = B->areas[src_area]->plan;
+    const bm_area_plan& D = B->areas[dst_area]->plan;
+    if (src_output >= S.n_outputs) return set_err(BM_ERR_INVALID, "bm_batch_connect: output %u out of range", src_output);
+    if (dst_input >= D.n_inputs) return set_err(BM_ERR_INVALID, "bm_batch_connect: input %u out of range", dst_input);
+    const uint64_t len = S.outputs[src_output].len;
+    if (dst_offset > D.inputs[dst_input].len || len > D.inputs[dst_input].len - dst_offset)
+        return set_err(BM_ERR_INVALID,
+                       "bm_batch_connect: %llu output axons at offset %llu overrun input %u of area %u (%u axons)",
+                       (unsigned long long)len, (unsigned long long)dst_offset, dst_input, dst_area,
+                       D.inputs[dst_input].len);
+    for (const auto& T : B->tracts)
+        if (T.dst_area == dst_area && T.dst_input == dst_input && dst_offset < T.dst_off + B->areas[T.src_area]->plan.outputs[T.src_output].len &&
+            T.dst_off < dst_offset + len)
+            return set_err(BM_ERR_INVALID, "bm_batch_connect: overlaps an existing tract into that input");
+    DevGuard g(B->ctx->device);
+    B->tracts.push_back({src_area, src_output, dst_area, dst_input, dst_offset});
+    B->drop_graph();
+    int rc = build_intake(B);
+    if (rc != BM_OK) {
+        B->tracts.pop_back();
+        build_intake(B);
+        return rc;
+    }
     return BM_OK;
 }
 
 int bm_batch_cycle_frames_device(bm_batch batch, const void* dev_frames, uint32_t n_cycles) {
     if (!batch || !dev_frames) return set_err(BM_ERR_INVALID, "null argument");
-    if (!batch->intake_blocks) return set_err(BM_ERR_INVALID, "the batch's areas have no input layer");
+    if (!batch->frame_bytes) return set_err(BM_ERR_INVALID, "the batch has no input that a tract does not feed");
     DevGuard g(batch->ctx->device);
     return run_cycles(batch, dev_frames, n_cycles);
 }
 
 int bm_batch_launches_per_cycle(bm_batch batch, uint32_t* out) {
     if (!batch || !out) return set_err(BM_ERR_INVALID, "null argument");
-    *out = batch->launches;
+    uint32_t n = (batch->intake_blocks ? 1u : 0u) + 1u;   // copies, cycle end
+    for (const auto& G : batch->groups) n += G.launches;
+    *out = n;
     return BM_OK;
 }
 
@@ -591,18 +680,19 @@ int bm_batch_autotune(bm_batch batch, const char* cache_path, uint32_t* n_tuned)
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
-    for (auto& p : B->plan) {
+    for (auto& G : B->groups)
+    for (auto& p : G.plan) {
         if (p.form != bm_batch_s::F_FUSED) continue;
-        const std::string key = step_key(B, p.st);
+        const std::string key = step_key(G, p.st);
         auto hit = cache.find(key);
         if (hit != cache.end()) {
-            if (!apply_target(B, p, hit->second)) build_fused(B, p);
+            if (!apply_target(B, G, p, hit->second)) build_fused(G, p);
             tuned++;
             continue;
         }
         // Save what the trials overwrite.
         std::vector<Range> ranges;
-        for (bm_area A : B->areas) step_ranges(A, p.st.layer, p.st.idx, ranges);
+        for (bm_area A : G.areas) step_ranges(A, p.st.layer, p.st.idx, ranges);
         uint64_t total = 0;
         for (auto& r : ranges) total += r.n;
         uint8_t* save = nullptr;
@@ -615,7 +705,7 @@ int bm_batch_autotune(bm_batch batch, const char* cache_path, uint32_t* n_tuned)
         uint32_t best_t = 0;
         float best_ms = 1e30f;
         for (uint32_t target : kTargets) {
-            if (!apply_target(B, p, target)) continue;
+            if (!apply_target(B, G, p, target)) continue;
             launch_fused_batch(p.fb, s);   // warm-up
             cudaEventRecord(e0, s);
             for (int r = 0; r < 5; r++) launch_fused_batch(p.fb, s);
@@ -625,7 +715,7 @@ int bm_batch_autotune(bm_batch batch, const char* cache_path, uint32_t* n_tuned)
             cudaEventElapsedTime(&ms, e0, e1);
             if (ms < best_ms) { best_ms = ms; best_t = target; }
         }
-        if (best_t == 0 || !apply_target(B, p, best_t)) build_fused(B, p);
+        if (best_t == 0 || !apply_target(B, G, p, best_t)) build_fused(G, p);
         o = 0;
         for (auto& r : ranges) { cudaMemcpyAsync(r.p, save + o, r.n, cudaMemcpyDeviceToDevice, s); o += r.n; }
         cudaStreamSynchronize(s);
@@ -634,6 +724,7 @@ int bm_batch_autotune(bm_batch batch, const char* cache_path, uint32_t* n_tuned)
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
+    for (auto& G : B->groups) count_launches(G);
     B->drop_graph();
     write_cache(cache_path, cache);
     if (n_tuned) *n_tuned = tuned;

@@ -390,8 +390,10 @@ class CorticalAreaSettings:
 
 # -------------------------------------------------------------- resolution --
 
-def _source_layers(area_sch, area_list, lmaps, sigs):
-    """matching_source_layers, src/map/layer_info.rs:14-100: (dims, topology) per source."""
+def source_list(area_sch, area_list, lmaps, sigs):
+    """matching_source_layers, src/map/layer_info.rs:14-100: the source layers
+    feeding an input layer with signatures `sigs`, in slice order, as
+    (source area name, source layer name, v_size, u_size, depth, topology)."""
     out = []
     for track, tags in sigs:
         if track == InputTrack.Afferent:
@@ -406,8 +408,12 @@ def _source_layers(area_sch, area_list, lmaps, sigs):
             for ls in src_map.output_layers_with_axon_tags(tags):
                 depth = ls._depth if ls._depth is not None else 1   # DEFAULT_OUTPUT_LAYER_DEPTH
                 topo = ls.axon_topology if ls.kind == F.BM_LYR_AXONAL else AxonTopology.Spatial
-                out.append((src_area.v_size, src_area.u_size, depth, topo))
+                out.append((an, ls.name, src_area.v_size, src_area.u_size, depth, topo))
     return out
+
+
+def _source_layers(area_sch, area_list, lmaps, sigs):
+    return [x[2:] for x in source_list(area_sch, area_list, lmaps, sigs)]
 
 
 def area_desc(area_name, lmaps, areas, settings=None, area_id=None):
@@ -469,6 +475,41 @@ def area_desc(area_name, lmaps, areas, settings=None, area_id=None):
                         raise ValueError("tuft source layer %r not in the layer map" % sl.name)
                     T.src[k] = F.bm_src_layer_desc(idx[sl.name], sl._reach, sl._prevalence)
     return d
+
+
+def area_tracts(lmaps, areas, names, plans):
+    """Thalamic routing among the cortical areas `names` (plans[k] resolves
+    names[k]): every input layer's source slices in order (LayerInfo::new,
+    src/map/layer_info.rs:142-215), each either a tract from another area of
+    `names` or an external feed. Returns (tracts, external) with
+    tracts = [(src_k, src_output, dst_k, dst_input, dst_offset, length)] and
+    external = [(dst_k, dst_input, dst_offset, length, source area, source layer)]."""
+    tracts, external = [], []
+    pos = {n: k for k, n in enumerate(names)}
+    for k, n in enumerate(names):
+        a = areas.by_name(n)
+        lm = lmaps[a.layer_map_name]
+        P = plans[k]
+        for i in range(P.n_inputs):
+            ls = lm.layers[P.inputs[i].layer_idx]
+            off = 0
+            for (src, src_layer, v, u, dep, _topo) in source_list(a, areas, lmaps, ls._axon_domain.sigs):
+                length = v * u * dep
+                if src in pos:
+                    S = plans[pos[src]]
+                    src_lm = lmaps[areas.by_name(src).layer_map_name]
+                    li = [x.name for x in src_lm.layers].index(src_layer)
+                    o = [S.outputs[j].layer_idx for j in range(S.n_outputs)].index(li)
+                    if int(S.outputs[o].len) != length:
+                        raise ValueError("tract %s.%s -> %s: %d axons, expected %d" % (src, src_layer, n,
+                                                                                     S.outputs[o].len, length))
+                    tracts.append((pos[src], o, k, i, off, length))
+                else:
+                    external.append((k, i, off, length, src, src_layer))
+                off += length
+            if off != int(P.inputs[i].len):
+                raise ValueError("input %d of %s: sources give %d axons, plan has %d" % (i, n, off, P.inputs[i].len))
+    return tracts, external
 
 
 def desc_layer_index(desc, name):

@@ -371,12 +371,13 @@ int bm_area_reset_profile(bm_area area);
 int bm_area_launches_per_cycle(bm_area area, uint32_t* out);
 
 /* ------------------------------------------------------------- batches ---
- * A batch cycles several areas together: instances of uneven column-grid
- * sizes that share one layer map, settings and execution path (the same
- * stage program). Each stage step runs as one launch over every area, and the
- * whole cycle is captured once as a CUDA graph and replayed. Every area keeps
- * its own state; an area's bytes after a batched cycle are the bytes it would
- * have after bm_area_cycle alone. Replaces bismit's one-area-at-a-time loop
+ * A batch cycles several areas together, of uneven column-grid sizes. Areas
+ * that share a stage program (layer map structure, settings and execution
+ * path) form a group, and each stage step of a group runs as one launch over
+ * all of its areas; the whole cycle is captured once as a CUDA graph and
+ * replayed. Every area keeps its own state; an area's bytes after a batched
+ * cycle are the bytes it would have after bm_area_cycle alone (given the same
+ * inputs). Replaces bismit's one-area-at-a-time loop
  * over areas in Cortex::cycle (src/cortex/cortex.rs:99-119), where every area
  * enqueues its own kernels.
  *
@@ -394,12 +395,24 @@ int bm_batch_set_graph(bm_batch batch, int on);
 /* n cycles of every area, inputs as last written to each area. */
 int bm_batch_cycle(bm_batch batch, uint32_t n_cycles);
 
-/* Bytes of one cycle's frame block: input 0 of every area, packed in batch
- * order (0 if some area has no input layer). */
+/* A tract: output `src_output` of area `src_area` (batch indices) feeds input
+ * `dst_input` of area `dst_area` at axon offset `dst_offset` within that input
+ * layer (an input layer fed by several source areas holds their slices one
+ * after another). At the head of every batched cycle each tract copies its
+ * source's output axons as they were at the end of the previous cycle, so all
+ * areas of a cycle see the previous cycle's outputs. Replaces the thalamic
+ * routing of bismit's Thalamus (src/subcortex/thalamus/thalamus.rs:97-112,
+ * 193-238) between the areas of one cortex, whose tracts are read by
+ * AxonSpace::intake (src/cortex/axon_space.rs:509-588). */
+int bm_batch_connect(bm_batch batch, uint32_t src_area, uint32_t src_output, uint32_t dst_area,
+                     uint32_t dst_input, uint64_t dst_offset);
+
+/* Bytes of one cycle's frame block: every input of every area that no tract
+ * feeds, packed in (area, input) order. */
 int bm_batch_frame_bytes(bm_batch batch, uint64_t* out);
 
 /* n cycles, each first copying its frame block (cycle k at dev_frames +
- * k * frame_bytes) into the areas' input layers. */
+ * k * frame_bytes) into those inputs. */
 int bm_batch_cycle_frames_device(bm_batch batch, const void* dev_frames, uint32_t n_cycles);
 
 /* Kernel launches per batched cycle (all areas together). */

@@ -154,15 +154,25 @@ def test_batch_autotune_keeps_state_and_parity(tmp_path):
 
 
 @pytest.mark.gpu
-def test_batch_rejects_areas_with_different_programs():
+def test_batch_groups_areas_with_different_programs():
+    """Areas whose stage programs differ (here: learning off in one) are
+    grouped; each still ends with its bytes from cycling alone."""
     ctx = cortex._Ctx(0)
-    a = cortex.CorticalArea(ctx, _desc(32, 1, 8, 16), 1)
-    b = cortex.CorticalArea(ctx, _desc(32, 1, 8, 16, configs.bench_settings().disable_learning()), 1)
-    with pytest.raises(F.BismitError) as e:
-        cortex.Batch(ctx, [a, b])
-    assert e.value.code == F.BM_ERR_UNSUPPORTED
-    a.close()
-    b.close()
+    descs = [_desc(32, 1, 8, 16), _desc(48, 2, 8, 32, configs.bench_settings().disable_learning()),
+             _desc(40, 1, 16, 16), _deep_desc(32)]
+    batched, alone = _pairs(ctx, descs)
+    batch = cortex.Batch(ctx, batched)
+    fr = [_frames(a, 3, 70 + k) for k, a in enumerate(batched)]
+    for c in range(3):
+        for k in range(len(batched)):
+            batched[k].write_input(fr[k][c])
+            alone[k].write_input(fr[k][c])
+            alone[k].cycle(1)
+        batch.cycle(1)
+        _check_equal(batched, alone, "cycle %d" % c)
+    batch.close()
+    for a in batched + alone:
+        a.close()
     ctx.close()
 
 

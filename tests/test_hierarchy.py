@@ -1,0 +1,60 @@
+"""Multi-area cortex: the hierarchy v1 -> v2 -> v3 with feed-forward and
+feedback tracts, batched, against the oracle run area by area with the same
+tract timing (every tract carries its source's output of the previous cycle).
+"""
+import numpy as np
+import pytest
+
+import oracle
+from bismit_b200 import Cortex, configs, map as M, plan_of
+from helpers import diff_report, scramble
+
+SIDES = (32, 48, 24)
+
+
+def test_tract_routing_of_the_hierarchy():
+    lm, ar, names = configs.hierarchy(SIDES)
+    plans = [plan_of(M.area_desc(n, lm, ar, configs.bench_settings()), 1) for n in names]
+    tracts, external = M.area_tracts(lm, ar, names, plans)
+    # v2.iii -> v1.eff_in, v1.iii -> v2.aff_in, v3.iii -> v2.eff_in, v2.iii -> v3.aff_in
+    assert sorted((s, d, i) for (s, _o, d, i, _off, _n) in tracts) == [(0, 1, 0), (1, 0, 1), (1, 2, 0), (2, 1, 1)]
+    for (s, o, d, i, off, n) in tracts:
+        assert n == int(plans[s].outputs[o].len) and off + n <= int(plans[d].inputs[i].len)
+    assert external == [(0, 0, 0, SIDES[0] ** 2, "v0", "ganglion")]
+
+
+def _oracle_cycle(plans, slabs, tracts, ext_frame, cycle):
+    outs = [s[int(p.axon_off):].copy() for p, s in zip(plans, slabs)]
+    for (s, o, d, i, off, n) in tracts:
+        src = int(plans[s].outputs[o].axn_idz)
+        dst = int(plans[d].axon_off) + int(plans[d].inputs[i].axn_idz) + off
+        slabs[d][dst:dst + n] = outs[s][src:src + n]
+    P0 = plans[0]
+    a0 = int(P0.axon_off) + int(P0.inputs[0].axn_idz)
+    slabs[0][a0:a0 + ext_frame.size] = ext_frame
+    for p, s in zip(plans, slabs):
+        oracle.run(p, s, None, 1, start_cycle=cycle)
+
+
+@pytest.mark.gpu
+def test_hierarchy_matches_oracle():
+    lm, ar, names = configs.hierarchy(SIDES)
+    cx = Cortex.builder(lm, ar).ca_settings(configs.bench_settings()).seed(3).build()
+    plans = [cx.area(n).plan for n in names]
+    slabs = []
+    for k, n in enumerate(names):
+        s = cx.area(n).read_slab()
+        scramble(plans[k], s, 40 + k)
+        cx.area(n).write_slab(s)
+        cx.area(n).set_cycle(0)
+        slabs.append(s.copy())
+    fr = configs.frames(6, SIDES[0] ** 2, 0.02, 5)
+    v1 = cx.area("v1")
+    for c in range(6):
+        v1.write_input(fr[c])
+        cx.cycle()
+        _oracle_cycle(plans, slabs, cx.tracts, fr[c], c)
+        for k, n in enumerate(names):
+            dev = cx.area(n).read_slab()
+            assert np.array_equal(dev, slabs[k]), "cycle %d, %s:\n%s" % (c, n, diff_report(plans[k], dev, slabs[k]))
+    cx.close()
