@@ -159,6 +159,14 @@ class BismitError(RuntimeError):
         self.code = code
 
 
+class bm_server_stats(C.Structure):
+    _fields_ = [("ticks", C.c_uint64), ("frames", C.c_uint64), ("batch_rebuilds", C.c_uint64),
+                ("syn_cycles", C.c_double), ("busy_s", C.c_double), ("span_s", C.c_double),
+                ("p50_ms", C.c_double), ("p99_ms", C.c_double), ("mean_ms", C.c_double),
+                ("used_bytes", C.c_uint64), ("budget_bytes", C.c_uint64),
+                ("resident", C.c_uint32), ("waiting", C.c_uint32)]
+
+
 def lib():
     """Returns the loaded native library; raises if it has not been built."""
     global _lib
@@ -210,6 +218,16 @@ def lib():
         "bm_batch_launches_per_cycle": (C.c_int, [vp, P(u32)]),
         "bm_batch_device_errors": (C.c_int, [vp, P(u32)]),
         "bm_batch_autotune": (C.c_int, [vp, C.c_char_p, P(u32)]),
+        "bm_server_create": (C.c_int, [vp, u64, P(vp)]),
+        "bm_server_destroy": (C.c_int, [vp]),
+        "bm_server_open": (C.c_int, [vp, P(bm_area_desc), u64, P(u32)]),
+        "bm_server_submit": (C.c_int, [vp, u32, vp, sz, u32]),
+        "bm_server_close": (C.c_int, [vp, u32]),
+        "bm_server_tick": (C.c_int, [vp, P(u32)]),
+        "bm_server_read_output": (C.c_int, [vp, u32, vp, sz, P(u64)]),
+        "bm_server_session_area": (C.c_int, [vp, u32, P(vp)]),
+        "bm_server_get_stats": (C.c_int, [vp, P(bm_server_stats)]),
+        "bm_server_reset_stats": (C.c_int, [vp]),
         "bm_rnd": (i32, [u64, u32, u32, u32, u32, u64]),
     }
     for name, (res, args) in sigs.items():

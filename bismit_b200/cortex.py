@@ -242,6 +242,74 @@ class Batch:
             pass
 
 
+class Server:
+    """Continuous-batching serving of cortex sessions (bm_server_*,
+    include/bismit_b200.h): sessions are admitted by device-memory budget,
+    stay resident, and every tick cycles all resident sessions that have a
+    pending frame in one batch."""
+
+    def __init__(self, ctx, budget_bytes=0):
+        self.lib = F.lib()
+        self.ctx = ctx
+        self.h = C.c_void_p()
+        F.check(self.lib.bm_server_create(ctx.h, C.c_uint64(int(budget_bytes)), C.byref(self.h)))
+
+    def open(self, desc, seed):
+        sid = C.c_uint32()
+        F.check(self.lib.bm_server_open(self.h, C.byref(desc), C.c_uint64(seed), C.byref(sid)))
+        return sid.value
+
+    def submit(self, sid, frames):
+        a = np.ascontiguousarray(frames, dtype=np.uint8)
+        if a.ndim == 1:
+            a = a[None, :]
+        F.check(self.lib.bm_server_submit(self.h, sid, a.ctypes.data_as(C.c_void_p), a.shape[1], a.shape[0]))
+
+    def close_session(self, sid):
+        F.check(self.lib.bm_server_close(self.h, sid))
+
+    def tick(self):
+        n = C.c_uint32()
+        F.check(self.lib.bm_server_tick(self.h, C.byref(n)))
+        return n.value
+
+    def read_output(self, sid, length):
+        out = np.empty(int(length), np.uint8)
+        done = C.c_uint64()
+        F.check(self.lib.bm_server_read_output(self.h, sid, out.ctypes.data_as(C.c_void_p), out.nbytes,
+                                               C.byref(done)))
+        return out, done.value
+
+    def session_slab(self, sid, slab_bytes):
+        """The session's whole state (while resident)."""
+        h = C.c_void_p()
+        F.check(self.lib.bm_server_session_area(self.h, sid, C.byref(h)))
+        if not h.value:
+            return None
+        out = np.empty(int(slab_bytes), np.uint8)
+        F.check(self.lib.bm_area_read_slab(h, out.ctypes.data_as(C.c_void_p), out.nbytes))
+        return out
+
+    def stats(self):
+        st = F.bm_server_stats()
+        F.check(self.lib.bm_server_get_stats(self.h, C.byref(st)))
+        return {k: getattr(st, k) for k, _ in F.bm_server_stats._fields_}
+
+    def reset_stats(self):
+        F.check(self.lib.bm_server_reset_stats(self.h))
+
+    def close(self):
+        if self.h:
+            self.lib.bm_server_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 class Cortex:
     """A set of cortical areas (Cortex, src/cortex/cortex.rs:37-120). The areas
     are cycled together as one batch; outputs of one area that feed inputs of

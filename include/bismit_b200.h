@@ -463,6 +463,50 @@ int bm_batch_autotune(bm_batch batch, const char* cache_path, uint32_t* n_tuned)
 int bm_tuft_cycle_static(const bm_area_plan* plan, uint32_t layer, uint32_t tuft, void* slab,
                          uint64_t cycle, uint32_t* dev_error_out, void* stream);
 
+/* ------------------------------------------------------------- serving ---
+ * A continuous-batching server over cortex sessions (one area each, with
+ * exactly one input layer). bm_server_open queues a session; it is admitted
+ * when the device-memory budget has room for its whole state (computed from
+ * its resolved plan before anything is allocated), in FIFO order, and stays
+ * resident until closed and drained. Each bm_server_tick cycles every
+ * resident session that has a pending frame exactly once, all in one batch
+ * (rebuilt only when that set changes), and meanwhile builds the areas of
+ * newly admitted sessions on a second stream so their set-up overlaps the
+ * running cycles. No counterpart in the reference, which cycles a fixed set
+ * of areas (Cortex::cycle, src/cortex/cortex.rs:99-119). */
+typedef struct bm_server_s* bm_server;
+
+typedef struct bm_server_stats {
+    uint64_t ticks, frames, batch_rebuilds;
+    double   syn_cycles;          /* synapse-cycles done                         */
+    double   busy_s;              /* time inside bm_server_tick                  */
+    double   span_s;              /* first tick start to last tick end           */
+    double   p50_ms, p99_ms, mean_ms;  /* per-frame latency: completion minus the
+                                     moment the frame was ready (submitted, or its
+                                     session's previous frame done)              */
+    uint64_t used_bytes, budget_bytes;
+    uint32_t resident, waiting;
+} bm_server_stats;
+
+/* mem_budget 0: 90 % of the device memory free at creation. */
+int bm_server_create(bm_ctx ctx, uint64_t mem_budget, bm_server* out);
+int bm_server_destroy(bm_server server);
+/* Queues a session; BM_ERR_OOM if it could never fit the budget. */
+int bm_server_open(bm_server server, const bm_area_desc* desc, uint64_t seed, uint32_t* session);
+/* Appends n_frames input frames (copied). */
+int bm_server_submit(bm_server server, uint32_t session, const uint8_t* frames, size_t frame_len,
+                     uint32_t n_frames);
+/* The session leaves once its submitted frames are cycled. */
+int bm_server_close(bm_server server, uint32_t session);
+/* One tick; *n_cycled (optional) = sessions cycled. Synchronous. */
+int bm_server_tick(bm_server server, uint32_t* n_cycled);
+/* Output 0 after the session's latest cycled frame; *frames_done (optional). */
+int bm_server_read_output(bm_server server, uint32_t session, uint8_t* dst, size_t len, uint64_t* frames_done);
+/* The session's area while it is resident (NULL while waiting). */
+int bm_server_session_area(bm_server server, uint32_t session, bm_area* out);
+int bm_server_get_stats(bm_server server, bm_server_stats* out);
+int bm_server_reset_stats(bm_server server);
+
 /* The per-launch random value the host would draw for (layer, role, tuft) at
  * `cycle` (replaces the SmallRng draws of src/cortex/dendrites.rs:198,
  * src/cortex/tufts.rs:312, src/cortex/spiny_stellates.rs:259,
