@@ -43,9 +43,10 @@ def parse():
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-instances measurement")
     ap.add_argument("--batch-instances", type=int, default=64)
     ap.add_argument("--no-serving", action="store_true", help="skip the serving measurement")
+    ap.add_argument("--no-hierarchy", action="store_true", help="skip the three-area hierarchy measurement")
     ap.add_argument("--serve-sessions", type=int, default=64)
     ap.add_argument("--serve-rate", type=float, default=200.0, help="mean session arrivals per second (Poisson)")
-    ap.add_argument("--serve-budget-gb", type=float, default=4.0)
+    ap.add_argument("--serve-budget-gb", type=float, default=8.0)
     return ap.parse_args()
 
 
@@ -209,6 +210,17 @@ def alg_bytes_cycle(plan):
     return b
 
 
+def batch_profile(batch, frames, fb, W, K):
+    """Per-step device time of K eager cycles of a batch (CUDA events on its
+    stream, graph bypassed): {step: [areas, ms per cycle]}."""
+    batch.reset_profile()
+    batch.set_profiling(True)
+    batch.cycle_frames_device(frames.data_ptr() + W * fb, K)
+    prof = batch.profile()
+    batch.set_profiling(False)
+    return {"%s L%d.%d" % (n, l, i): [a, round(ms / K, 4)] for (n, l, i, a, _c, ms) in prof}
+
+
 def run_batched(args, ctx, stream, K, W, ws):
     """The batched-instances workload: `--batch-instances` independent areas of
     uneven size (configs.batch_instances), cycled (a) as one batch with graph
@@ -267,6 +279,7 @@ def run_batched(args, ctx, stream, K, W, ws):
     torch.cuda.synchronize()
     ms_p = max_ms(e0.elapsed_time(e1))
     same = all(np.array_equal(a.read_output(), b.read_output()) for a, b in zip(areas_b, areas_p))
+    steps_b = batch_profile(batch, packed, fb, W, K)
     peak, peak_kind = peaks()
     val_b = n_syn * K * ws / (ms_b / 1e3)
     val_p = n_syn * K * ws / (ms_p / 1e3)
@@ -282,11 +295,80 @@ def run_batched(args, ctx, stream, K, W, ws):
                   "hbm_frac": round(alg / (ms_p / K / 1e3) / 1e9 / peak, 4)},
         "batched_over_plain": round(ms_p / ms_b, 3),
         "outputs_identical": bool(same),
+        "steps": steps_b,
         "peak_source": peak_kind,
     }
     batch.close()
     for a in areas_b + areas_p:
         a.close()
+    return out
+
+
+def run_hierarchy(args, ctx, stream, K, W, ws):
+    """The three-area hierarchy (128 -> 192 -> 96, depth 2, feed-forward and
+    feedback tracts, input 2 % active): (a) one batch with tracts and graph
+    replay, (b) the plain form, one area after another with one kernel per
+    reference stage (the tract copies, about 0.1 MB a cycle, left out)."""
+    import torch
+    from bismit_b200 import Cortex, configs, cortex, map as M
+    lmaps, areas, names = configs.hierarchy()
+    st = configs.bench_settings()
+    cx = Cortex(lmaps, areas, st, seed=args.seed, ctx=ctx)
+    plain = [cortex.CorticalArea(ctx, M.area_desc(n, lmaps, areas, configs.bench_settings().plain_kernels()),
+                                 args.seed) for n in names]
+    fb = cx.batch.frame_bytes()
+    fr = torch.from_numpy(configs.frames(K + W, fb, 0.02, args.seed + 3)).to("cuda")
+    n_syn = sum(int(cx.area(n).plan.n_syns_total) for n in names)
+    alg = sum(alg_bytes_cycle(cx.area(n).plan) for n in names)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+
+    def max_ms(ms):
+        if ws > 1:
+            t = torch.tensor([ms], device="cuda")
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            return float(t.item())
+        return ms
+
+    cx.batch.cycle_frames_device(fr.data_ptr(), W)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    cx.batch.cycle_frames_device(fr.data_ptr() + W * fb, K)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms_b = max_ms(e0.elapsed_time(e1))
+    v1 = plain[0]
+
+    def plain_cycles(c0, nc):
+        for c in range(c0, c0 + nc):
+            v1.cycle_frames_device(fr.data_ptr() + c * fb, fb, 1)
+            for a in plain[1:]:
+                a.cycle(1)
+    plain_cycles(0, W)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    plain_cycles(W, K)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms_p = max_ms(e0.elapsed_time(e1))
+    peak, _ = peaks()
+    steps_h = batch_profile(cx.batch, fr, fb, W, K)
+    out = {
+        "steps": steps_h,
+        "workload": "hierarchy_3", "areas": "128x128 -> 192x192 -> 96x96, depth 2", "synapses": n_syn,
+        "tracts": len(cx.tracts),
+        "batched": {"value": n_syn * K * ws / (ms_b / 1e3), "unit": UNIT, "ms_per_step": ms_b / K,
+                    "launches_per_cycle": cx.batch.launches_per_cycle(),
+                    "hbm_frac": round(alg / (ms_b / K / 1e3) / 1e9 / peak, 4)},
+        "plain": {"value": n_syn * K * ws / (ms_p / 1e3), "unit": UNIT, "ms_per_step": ms_p / K,
+                  "launches_per_cycle": sum(a.launches_per_cycle() for a in plain),
+                  "hbm_frac": round(alg / (ms_p / K / 1e3) / 1e9 / peak, 4)},
+        "batched_over_plain": round(ms_p / ms_b, 3),
+    }
+    for a in plain:
+        a.close()
+    cx.close()
     return out
 
 
@@ -309,20 +391,29 @@ def run_serving(args, ctx):
         descs.append(d)
         pools.append(configs.frames(8, side * side, act, args.seed * 7919 + i))
     srv = cortex.Server(ctx, int(args.serve_budget_gb * 1e9))
-    opened, total = 0, 0
+    opened, total, queued = 0, 0, 0
+    t_tick = t_submit = 0.0
     t0 = time.perf_counter()
     while True:
         now = time.perf_counter() - t0
         while opened < n and arrivals[opened] <= now:
+            ts = time.perf_counter()
             sid = srv.open(descs[opened], args.seed * 1000 + opened)
             k = int(n_frames[opened])
-            srv.submit(sid, np.tile(pools[opened], (k // 8 + 1, 1))[:k])
+            for r in range(k // 8):
+                srv.submit(sid, pools[opened])
+            if k % 8:
+                srv.submit(sid, pools[opened][:k % 8])
+            t_submit += time.perf_counter() - ts
             srv.close_session(sid)
             total += k
             opened += 1
+        ts = time.perf_counter()
         cycled = srv.tick()
-        st = srv.stats()
-        if opened == n and st["frames"] >= total:
+        t_tick += time.perf_counter() - ts
+        queued += cycled
+        if opened == n and queued >= total:
+            srv.drain()
             break
         if cycled == 0 and opened < n:
             time.sleep(max(0.0, min(0.001, arrivals[opened] - (time.perf_counter() - t0))))
@@ -337,7 +428,8 @@ def run_serving(args, ctx):
         "value": st["syn_cycles"] / st["span_s"] if st["span_s"] else None, "unit": UNIT,
         "p50_ms": round(st["p50_ms"], 3), "p99_ms": round(st["p99_ms"], 3), "mean_ms": round(st["mean_ms"], 3),
         "ticks": int(st["ticks"]), "batch_rebuilds": int(st["batch_rebuilds"]),
-        "busy_s": round(st["busy_s"], 3), "wall_s": round(wall, 3),
+        "rebuild_s": round(st["rebuild_s"], 3), "admit_s": round(st["admit_s"], 3), "gpu_s": round(st["gpu_s"], 3),
+        "tick_call_s": round(t_tick, 3), "submit_s": round(t_submit, 3), "wall_s": round(wall, 3),
         "latency": "per frame: tick completion minus the moment the frame was ready (its session's previous "
                    "frame done, or its arrival); admission waits included",
     }
@@ -450,6 +542,7 @@ def run_ours(args):
 
     area.close()
     batched = None if args.no_batched else run_batched(args, ctx, stream, K, W, ws)
+    hierarchy = None if args.no_hierarchy else run_hierarchy(args, ctx, stream, K, W, ws)
     serving = None if (args.no_serving or ws > 1) else run_serving(args, ctx)
 
     cpu = None
@@ -474,6 +567,7 @@ def run_ours(args):
             "cpu_baseline": cpu,
             "kernels": {k: {"launches": v[0], "ms": round(v[1], 4)} for k, v in prof.items()},
             "batched_instances": batched,
+            "hierarchy": hierarchy,
             "serving": serving,
         }
         print(json.dumps(line), flush=True)

@@ -161,7 +161,8 @@ class BismitError(RuntimeError):
 
 class bm_server_stats(C.Structure):
     _fields_ = [("ticks", C.c_uint64), ("frames", C.c_uint64), ("batch_rebuilds", C.c_uint64),
-                ("syn_cycles", C.c_double), ("busy_s", C.c_double), ("span_s", C.c_double),
+                ("syn_cycles", C.c_double), ("busy_s", C.c_double), ("rebuild_s", C.c_double),
+                ("admit_s", C.c_double), ("gpu_s", C.c_double), ("span_s", C.c_double),
                 ("p50_ms", C.c_double), ("p99_ms", C.c_double), ("mean_ms", C.c_double),
                 ("used_bytes", C.c_uint64), ("budget_bytes", C.c_uint64),
                 ("resident", C.c_uint32), ("waiting", C.c_uint32)]
@@ -218,12 +219,16 @@ def lib():
         "bm_batch_launches_per_cycle": (C.c_int, [vp, P(u32)]),
         "bm_batch_device_errors": (C.c_int, [vp, P(u32)]),
         "bm_batch_autotune": (C.c_int, [vp, C.c_char_p, P(u32)]),
+        "bm_batch_set_profiling": (C.c_int, [vp, C.c_int]),
+        "bm_batch_get_profile": (C.c_int, [vp, u32, P(u32), P(u32), P(u32), P(u32), P(u64), P(C.c_double), P(u32)]),
+        "bm_batch_reset_profile": (C.c_int, [vp]),
         "bm_server_create": (C.c_int, [vp, u64, P(vp)]),
         "bm_server_destroy": (C.c_int, [vp]),
         "bm_server_open": (C.c_int, [vp, P(bm_area_desc), u64, P(u32)]),
         "bm_server_submit": (C.c_int, [vp, u32, vp, sz, u32]),
         "bm_server_close": (C.c_int, [vp, u32]),
         "bm_server_tick": (C.c_int, [vp, P(u32)]),
+        "bm_server_drain": (C.c_int, [vp]),
         "bm_server_read_output": (C.c_int, [vp, u32, vp, sz, P(u64)]),
         "bm_server_session_area": (C.c_int, [vp, u32, P(vp)]),
         "bm_server_get_stats": (C.c_int, [vp, P(bm_server_stats)]),

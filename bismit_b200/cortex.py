@@ -225,6 +225,31 @@ class Batch:
             F.check(rc)
         return v.value
 
+    STEP_NAMES = {0: "tuft", 1: "tufts_plain", 2: "ssc_cycle", 3: "inhib_simple", 4: "inhib_passthrough",
+                  5: "pyr_output", 6: "inhib_intra_column", 7: "pyr_cycle", 8: "tft_dst_mtp", 9: "ssc_mtp_simple",
+                  10: "cycle_end", 11: "inhib_mtp", 12: "pyr_tail", 1000: "fused_tuft_batch"}
+
+    def set_profiling(self, on):
+        F.check(self.lib.bm_batch_set_profiling(self.h, 1 if on else 0))
+
+    def profile(self):
+        """[(step name, layer, index, areas, launches, device ms)] of the steps that ran."""
+        n = 64
+        arrs = [(C.c_uint32 * n)() for _ in range(4)]
+        launches = (C.c_uint64 * n)()
+        ms = (C.c_double * n)()
+        got = C.c_uint32()
+        F.check(self.lib.bm_batch_get_profile(self.h, n, *arrs, launches, ms, C.byref(got)))
+        out = []
+        for i in range(got.value):
+            k = int(arrs[0][i])
+            name = self.STEP_NAMES.get(k, self.STEP_NAMES[1000] if k >= 1000 else str(k))
+            out.append((name, int(arrs[1][i]), int(arrs[2][i]), int(arrs[3][i]), int(launches[i]), float(ms[i])))
+        return out
+
+    def reset_profile(self):
+        F.check(self.lib.bm_batch_reset_profile(self.h))
+
     def autotune(self, cache_path=None):
         n = C.c_uint32()
         F.check(self.lib.bm_batch_autotune(self.h, cache_path.encode() if cache_path else None, C.byref(n)))
@@ -273,6 +298,10 @@ class Server:
         F.check(self.lib.bm_server_tick(self.h, C.byref(n)))
         return n.value
 
+    def drain(self):
+        """Completes every queued tick (ticks are pipelined two deep)."""
+        F.check(self.lib.bm_server_drain(self.h))
+
     def read_output(self, sid, length):
         out = np.empty(int(length), np.uint8)
         done = C.c_uint64()
@@ -318,8 +347,9 @@ class Cortex:
     Inputs fed from outside (subcortical areas) are written per area with
     `area(name).write_input(..)`; `external_inputs()` lists them."""
 
-    def __init__(self, lmaps, areas, settings=None, seed=0, device=0):
-        self.ctx = _Ctx(device)
+    def __init__(self, lmaps, areas, settings=None, seed=0, device=0, ctx=None):
+        self._own_ctx = ctx is None
+        self.ctx = _Ctx(device) if ctx is None else ctx
         self.areas = {}
         self._order = []
         for a in areas.areas:
@@ -362,7 +392,8 @@ class Cortex:
             self.batch.close()
         for a in self.areas.values():
             a.close()
-        self.ctx.close()
+        if self._own_ctx:
+            self.ctx.close()
 
 
 class CortexBuilder:

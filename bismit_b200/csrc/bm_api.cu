@@ -59,7 +59,7 @@ void push_controls(const bm_area_s* A, uint32_t i, std::vector<Step>& out) {
             st = ST_INTRA_COL;
         else
             continue;
-        out.push_back({st, (uint8_t)i, (uint8_t)k});
+        out.push_back({st, (uint8_t)i, (uint8_t)k, 0});
     }
 }
 
@@ -67,7 +67,7 @@ void push_pyr_learn(const bm_area_s* A, uint32_t i, std::vector<Step>& out) {
     const bm_layer_plan& L = A->plan.layers[i];
     if (A->plan.settings & (BM_SET_DISABLE_LEARNING | BM_SET_DISABLE_PYRS)) return;
     for (uint32_t t = 0; t < L.n_tufts; t++)
-        if (L.tufts[t].den_kind == BM_DEN_DISTAL) out.push_back({ST_DST_MTP, (uint8_t)i, (uint8_t)t});
+        if (L.tufts[t].den_kind == BM_DEN_DISTAL) out.push_back({ST_DST_MTP, (uint8_t)i, (uint8_t)t, 0});
 }
 
 // SpinyStellateLayer::cycle (src/cortex/spiny_stellates.rs:220-252) and
@@ -75,14 +75,14 @@ void push_pyr_learn(const bm_area_s* A, uint32_t i, std::vector<Step>& out) {
 void push_layer_cycle(const bm_area_s* A, uint32_t i, std::vector<Step>& out) {
     const bm_layer_plan& L = A->plan.layers[i];
     if (A->exec_path == BM_PATH_PLAIN)
-        out.push_back({ST_TUFTS_PLAIN, (uint8_t)i, 0});
+        out.push_back({ST_TUFTS_PLAIN, (uint8_t)i, 0, 0});
     else
-        for (uint32_t t = 0; t < L.n_tufts; t++) out.push_back({ST_TUFT, (uint8_t)i, (uint8_t)t});
+        for (uint32_t t = 0; t < L.n_tufts; t++) out.push_back({ST_TUFT, (uint8_t)i, (uint8_t)t, 0});
     if (L.kind == BM_LYR_SPINY_STELLATE) {
-        out.push_back({ST_SSC_CYCLE, (uint8_t)i, 0});
+        out.push_back({ST_SSC_CYCLE, (uint8_t)i, 0, 0});
         push_controls(A, i, out);
     } else {
-        out.push_back({ST_PYR_CYCLE, (uint8_t)i, 0});
+        out.push_back({ST_PYR_CYCLE, (uint8_t)i, 0, 0});
         push_controls(A, i, out);
         push_pyr_learn(A, i, out);
     }
@@ -92,10 +92,70 @@ void push_layer_learn(const bm_area_s* A, uint32_t i, std::vector<Step>& out) {
     const bm_layer_plan& L = A->plan.layers[i];
     if (L.kind == BM_LYR_SPINY_STELLATE) {
         if (!(A->plan.settings & (BM_SET_DISABLE_LEARNING | BM_SET_DISABLE_SSCS)))
-            out.push_back({ST_SSC_MTP, (uint8_t)i, 0});
+            out.push_back({ST_SSC_MTP, (uint8_t)i, 0, 0});
     } else {
         push_pyr_learn(A, i, out);
     }
+}
+
+// Slices of data layer i are plain: unscaled, unshifted and laid out back to
+// back from the layer's first axon, so the axon a control writes for cell c
+// is axn_idz + c.
+bool layer_plain(const bm_area_plan& P, uint32_t i) {
+    const bm_layer_plan& L = P.layers[i];
+    const uint32_t cols = L.v_size * L.u_size;
+    for (uint32_t s = 0; s < L.depth; s++) {
+        const uint32_t k = L.base_axn_slc + s;
+        if (k >= P.n_slices) return false;
+        if (P.slc_v_scale[k] != 16 || P.slc_u_scale[k] != 16 || P.slc_v_mid[k] || P.slc_u_mid[k]) return false;
+        if (P.slc_v_size[k] != L.v_size || P.slc_u_size[k] != L.u_size) return false;
+        if (P.slc_axn_idz[k] != L.axn_idz + s * cols) return false;
+    }
+    return true;
+}
+
+// Fused forms of adjacent steps whose later stages only read what the earlier
+// ones wrote for the same cell (bm_items.cuh).
+void fuse_steps(const bm_area_s* A, std::vector<Step>& v) {
+    const bm_area_plan& P = A->plan;
+    std::vector<Step> out;
+    for (size_t k = 0; k < v.size(); k++) {
+        const Step& s = v[k];
+        if (s.kind == ST_INHIB_SIMPLE && layer_plain(P, s.layer) &&
+            P.layers[s.layer].kind == BM_LYR_SPINY_STELLATE) {
+            const bool learn = k + 1 < v.size() && v[k + 1].kind == ST_SSC_MTP && v[k + 1].layer == s.layer;
+            out.push_back({ST_INHIB_MTP, s.layer, s.idx, (uint8_t)learn});
+            if (learn) k++;
+            continue;
+        }
+        if (s.kind == ST_PYR_CYCLE && layer_plain(P, s.layer)) {
+            const bm_layer_plan& L = P.layers[s.layer];
+            size_t j = k + 1;
+            uint8_t ctrl = 0xFF;
+            if (j < v.size() && v[j].layer == s.layer && (v[j].kind == ST_INTRA_COL || v[j].kind == ST_PYR_OUTPUT)) {
+                ctrl = v[j].idx;
+                j++;
+            }
+            // Every distal tuft's learning, in tuft order, or none.
+            size_t m = j;
+            bool all = true;
+            uint32_t n_dst = 0;
+            for (uint32_t t = 0; t < L.n_tufts; t++) {
+                if (L.tufts[t].den_kind != BM_DEN_DISTAL) continue;
+                n_dst++;
+                if (m < v.size() && v[m].kind == ST_DST_MTP && v[m].layer == s.layer && v[m].idx == t) m++;
+                else all = false;
+            }
+            const bool learn = n_dst > 0 && all;
+            if (learn || m == j) {
+                out.push_back({ST_PYR_TAIL, s.layer, ctrl, (uint8_t)learn});
+                k = (learn ? m : j) - 1;
+                continue;
+            }
+        }
+        out.push_back(s);
+    }
+    v.swap(out);
 }
 
 }  // namespace
@@ -115,7 +175,8 @@ void bm::area_steps(const bm_area_s* A, std::vector<Step>& out) {
         for (uint32_t k = 0; k < P.n_cycle_order; k++)
             if (!(P.layers[P.cycle_order[k]].tags & BM_TAG_SPATIAL)) push_layer_cycle(A, P.cycle_order[k], out);
     }
-    out.push_back({ST_CYCLE_END, 0, 0});
+    out.push_back({ST_CYCLE_END, 0, 0, 0});
+    if (A->exec_path == BM_PATH_FUSED) fuse_steps(A, out);
 }
 
 // Synapse flags, synapse cycle, dendrite cycle and (pyramidal) tuft cycle: the
@@ -140,12 +201,20 @@ void bm::exec_step(bm_area_s* A, const Step& st, cudaStream_t s) {
         if (A->fused.t[i][x].ok) {
             run(K_FUSED_TUFT, [&] { launch_fused_tuft(A->fused, A->axns(), A->slices, D, i, x, A->ctl, s); });
         } else {
-            run(K_SYN_FLAGS, [&] { launch_set_syn_flags_tuft(D, x, s); });
-            run(K_SYN_CYCLE, [&] { launch_syn_cycle_plain(A->axns(), A->slices, D, x, s); });
-            run(K_DEN_CYCLE, [&] { launch_den_cycle_plain(D, x, A->ctl, s); });
-            if (pyr) run(K_TFT_CYCLE, [&] { launch_tft_cycle_plain(D, x, s); });
+            run(K_TUFT_CELLS, [&] { launch_tuft_cells(A->axns(), A->slices, D, x, A->ctl, s); });
         }
         break;
+    case ST_INHIB_MTP:
+        run(K_INHIB_MTP, [&] {
+            launch_inhib_mtp(A->axns(), A->slices, D, (int)L.ctrl[x].field_radius, A->inhib_key[i][x], st.arg != 0,
+                             A->ctl, s);
+        });
+        break;
+    case ST_PYR_TAIL: {
+        const int ctrl = x == 0xFF ? 0 : (L.ctrl[x].kind == BM_LYR_CTRL_INTRA_COLUMN ? 1 : 2);
+        run(K_PYR_TAIL, [&] { launch_pyr_tail(A->axns(), A->slices, D, ctrl, st.arg != 0, A->ctl, s); });
+        break;
+    }
     case ST_TUFTS_PLAIN:
         run(K_SYN_FLAGS, [&] { launch_set_syn_flags(D, s); });
         for (uint32_t t = 0; t < L.n_tufts; t++)

@@ -13,13 +13,12 @@ namespace bm {
 enum Kind {
     K_SYN_FLAGS, K_SYN_CYCLE, K_DEN_CYCLE, K_TFT_CYCLE, K_SSC_CYCLE, K_INHIB_SIMPLE, K_INHIB_PASS,
     K_SSC_MTP, K_PYR_CYCLE, K_PYR_OUTPUT, K_INTRA_COL, K_TFT_DST_MTP, K_CYCLE_END, K_INTAKE,
-    K_FUSED_TUFT, K_FUSED_SSC_SOMA, K_FUSED_PYR_SOMA, K_FUSED_SSC_MTP, K_COUNT
+    K_FUSED_TUFT, K_TUFT_CELLS, K_INHIB_MTP, K_PYR_TAIL, K_COUNT
 };
 const char* const kKindNames[K_COUNT] = {
     "tft_set_syn_flags", "syn_cycle", "den_cycle_tft", "tft_cycle", "ssc_cycle", "inhib_simple",
     "inhib_passthrough", "ssc_mtp_simple", "pyr_cycle", "pyr_output", "inhib_intra_column", "tft_dst_mtp",
-    "cycle_end", "intake", "fused_tuft_cycle", "fused_ssc_soma_inhib", "fused_pyr_soma_learn",
-    "fused_ssc_mtp"};
+    "cycle_end", "intake", "fused_tuft_cycle", "tuft_cells", "inhib_mtp", "pyr_tail"};
 
 struct DevGuard {
     int prev = -1;
@@ -48,10 +47,16 @@ enum StepKind : uint8_t {
     ST_DST_MTP,       // distal learning of tuft `idx`
     ST_SSC_MTP,
     ST_CYCLE_END,
+    // Fused forms (the fused execution path, layers with plain slices):
+    ST_INHIB_MTP,     // ST_INHIB_SIMPLE `idx` followed by ST_SSC_MTP (arg 1) of the same layer
+    ST_PYR_TAIL,      // ST_PYR_CYCLE, control `idx` (intra-column or output; 0xFF none), and
+                      // (arg 1) ST_DST_MTP of every distal tuft, in that order
 };
 struct Step {
-    uint8_t kind, layer, idx;
-    bool operator==(const Step& o) const { return kind == o.kind && layer == o.layer && idx == o.idx; }
+    uint8_t kind, layer, idx, arg;
+    bool operator==(const Step& o) const {
+        return kind == o.kind && layer == o.layer && idx == o.idx && arg == o.arg;
+    }
 };
 
 }  // namespace bm
@@ -85,6 +90,7 @@ struct bm_area_s {
     double prof_ms[bm::K_COUNT] = {};
     uint32_t launches = 0;   // kernel launches of the last enqueued cycle
     std::vector<Step> steps; // the cycle's stage program
+    uint32_t n_batches = 0;  // batches holding this area (its tiles are retiled only when one does)
 
     cudaStream_t stream() const { return ctx->stream(); }
     uint8_t* axns() const { return slab + plan.axon_off; }

@@ -21,6 +21,7 @@
 // A project-written autotuner (bm_batch_autotune) picks the tile size of each
 // batched tuft step by timing candidates on the live batch (with the touched
 // buffers saved and restored) and can keep its choices in a cache file.
+#include <algorithm>
 #include <cstdio>
 #include <cstring>
 #include <map>
@@ -43,6 +44,8 @@ struct CellJob {
     AreaCtl* ctl;
     uint64_t key;       // inhibition rnd key (other steps take theirs from L)
     int32_t radius;     // inhibition radius
+    int32_t ctrl;       // pyramidal tail: 0 none, 1 intra-column, 2 output
+    uint32_t learn;     // fused steps: learning included
     uint32_t x;         // tuft or control index
     uint32_t n;         // work items (cells or columns)
     uint32_t block0;    // first block of this job
@@ -64,9 +67,8 @@ struct BatchCtl {
     uint64_t frame_bytes;    // bytes of one cycle's block
 };
 
-// Sub-stages of an unfused tuft, batched like the per-cell steps (item =
-// synapse, synapse, dendrite, cell).
-constexpr int BK_FLAGS = 100, BK_SYN = 101, BK_DEN = 102, BK_TFT = 103;
+// An unfused tuft's four stages, one thread per cell (tuft_cell_item).
+constexpr int BK_TUFT_CELLS = 100;
 
 constexpr uint32_t kCellBlock = 128;
 constexpr uint32_t kIntakeBlock = 256;
@@ -92,6 +94,16 @@ template <int ST>
 __global__ void __launch_bounds__(kCellBlock) k_batch_cells(const CellJob* __restrict__ jobs, uint32_t n_jobs) {
     const CellJob& J = jobs[block_job(jobs, n_jobs)];
     const uint32_t i = (blockIdx.x - J.block0) * kCellBlock + threadIdx.x;
+    // Warp-cooperative steps keep every lane (a block's warps belong to one job).
+    if (ST == ST_INHIB_MTP) {
+        inhib_mtp_warp(J.axns, J.slices, J.L, J.radius, rnd_at(J.key, J.ctl->cycle),
+                       rnd_at(J.L.rnd_key_ssc_mtp, J.ctl->cycle), J.learn != 0, i, i < J.n);
+        return;
+    }
+    if (ST == ST_PYR_TAIL) {
+        pyr_tail_warp(J.axns, J.slices, J.L, J.ctrl, J.learn != 0, J.ctl, i, i < J.n);
+        return;
+    }
     if (i >= J.n) return;
     switch (ST) {
     case ST_SSC_CYCLE: ssc_cycle_item(J.L, i); break;
@@ -102,16 +114,9 @@ __global__ void __launch_bounds__(kCellBlock) k_batch_cells(const CellJob* __res
     case ST_PYR_CYCLE: pyr_cycle_item(J.L, i); break;
     case ST_DST_MTP: tft_dst_mtp_item(J.axns, J.L, J.x, rnd_at(J.L.tft[J.x].rnd_key_mtp, J.ctl->cycle), i); break;
     case ST_SSC_MTP: ssc_mtp_item(J.axns, J.L, rnd_at(J.L.rnd_key_ssc_mtp, J.ctl->cycle), i); break;
-    case BK_FLAGS: {
-        // tft_set_syn_flags, cl/syns.cl:23-33, for the tuft's synapses.
-        const uint64_t si = J.L.tft[J.x].syn_idz + i;
-        uint8_t* fl = J.L.buf[BM_BUF_SYN_FLAG_SETS];
-        fl[si] = (uint8_t)((fl[si] & ~kSynPrevActiveFlag) | (J.L.buf[BM_BUF_SYN_STATES][si] ? kSynPrevActiveFlag : 0));
+    case BK_TUFT_CELLS:
+        tuft_cell_item(J.axns, J.slices, J.L, J.x, rnd_at(J.L.tft[J.x].rnd_key_den, J.ctl->cycle), i);
         break;
-    }
-    case BK_SYN: syn_cycle_item(J.axns, J.slices, J.L, J.x, i); break;
-    case BK_DEN: den_cycle_item(J.L, J.x, rnd_at(J.L.tft[J.x].rnd_key_den, J.ctl->cycle), i); break;
-    case BK_TFT: tft_cycle_item(J.L, J.x, i); break;
     default: break;
     }
 }
@@ -156,10 +161,9 @@ void launch_cells(int st, const CellJob* jobs, uint32_t n_jobs, uint32_t n_block
         BM_CELLS(ST_PYR_CYCLE)
         BM_CELLS(ST_DST_MTP)
         BM_CELLS(ST_SSC_MTP)
-        BM_CELLS(BK_FLAGS)
-        BM_CELLS(BK_SYN)
-        BM_CELLS(BK_DEN)
-        BM_CELLS(BK_TFT)
+        BM_CELLS(ST_INHIB_MTP)
+        BM_CELLS(ST_PYR_TAIL)
+        BM_CELLS(BK_TUFT_CELLS)
 #undef BM_CELLS
     default: break;
     }
@@ -167,7 +171,8 @@ void launch_cells(int st, const CellJob* jobs, uint32_t n_jobs, uint32_t n_block
 
 bool is_cell_step(int st) {
     return st == ST_SSC_CYCLE || st == ST_INHIB_SIMPLE || st == ST_INHIB_PASS || st == ST_PYR_OUTPUT ||
-           st == ST_INTRA_COL || st == ST_PYR_CYCLE || st == ST_DST_MTP || st == ST_SSC_MTP;
+           st == ST_INTRA_COL || st == ST_PYR_CYCLE || st == ST_DST_MTP || st == ST_SSC_MTP ||
+           st == ST_INHIB_MTP || st == ST_PYR_TAIL;
 }
 
 }  // namespace
@@ -179,21 +184,43 @@ struct bm_batch_s {
         CellJob* d_jobs;
         uint32_t n_jobs, n_blocks;
     };
+    // One step of the batch's schedule: the areas whose programs have it.
     struct StepPlan {
         Step st;
+        std::vector<bm_area> areas;
         Form form = F_EACH;
         std::vector<CellLaunch> cells;   // F_CELLS: launches in order
         FusedBatch fb;
-    };
-    // Areas with one stage program, batched step by step.
-    struct Group {
-        std::vector<bm_area> areas;
-        std::vector<StepPlan> plan;
-        uint32_t launches = 0;
+        // Profiling (eager cycles only): launches and device milliseconds.
+        uint64_t prof_n = 0;
+        double prof_ms = 0;
     };
     bm_ctx ctx = nullptr;
     std::vector<bm_area> areas;          // every area, in batch order
-    std::vector<Group> groups;
+    std::vector<StepPlan> plan;          // the schedule: a common supersequence of the areas' programs
+    uint32_t plan_launches = 0;
+    bool profiling = false;
+    struct Rec { size_t step; cudaEvent_t a, b; };
+    std::vector<Rec> pending;
+    std::vector<cudaEvent_t> pool;
+    cudaEvent_t ev() {
+        if (!pool.empty()) { cudaEvent_t e = pool.back(); pool.pop_back(); return e; }
+        cudaEvent_t e = nullptr;
+        cudaEventCreate(&e);
+        return e;
+    }
+    void drain_profile() {
+        for (auto& r : pending) {
+            float ms = 0.f;
+            cudaEventSynchronize(r.b);
+            cudaEventElapsedTime(&ms, r.a, r.b);
+            plan[r.step].prof_n++;
+            plan[r.step].prof_ms += ms;
+            pool.push_back(r.a);
+            pool.push_back(r.b);
+        }
+        pending.clear();
+    }
     struct Tract {
         uint32_t src_area, src_output, dst_area, dst_input;
         uint64_t dst_off;
@@ -220,23 +247,27 @@ struct bm_batch_s {
 
 namespace {
 
-void free_plan(bm_batch_s::Group& G) {
-    for (auto& p : G.plan) {
+void free_plan(bm_batch_s* B) {
+    for (auto& p : B->plan) {
         for (auto& c : p.cells) cudaFree(c.d_jobs);
         free_fused_batch(p.fb);
     }
-    G.plan.clear();
+    B->plan.clear();
 }
 
 void free_batch(bm_batch_s* B) {
     if (!B) return;
     DevGuard g(B->ctx->device);
+    for (bm_area A : B->areas)
+        if (A->n_batches) A->n_batches--;
     B->drop_graph();
-    for (auto& G : B->groups) free_plan(G);
+    free_plan(B);
     if (B->d_intake) cudaFree(B->d_intake);
     if (B->d_bctl) cudaFree(B->d_bctl);
     if (B->d_ctls) cudaFree(B->d_ctls);
     if (B->cap) cudaStreamDestroy(B->cap);
+    for (auto& r : B->pending) { cudaEventDestroy(r.a); cudaEventDestroy(r.b); }
+    for (auto e : B->pool) cudaEventDestroy(e);
     delete B;
 }
 
@@ -244,20 +275,18 @@ void free_batch(bm_batch_s* B) {
 uint64_t items_of(const bm_area_s* A, int k, const Step& st) {
     const bm_layer_plan& L = A->plan.layers[st.layer];
     switch (k) {
-    case ST_INTRA_COL: return (uint64_t)L.v_size * L.u_size;
-    case BK_FLAGS:
-    case BK_SYN: return (uint64_t)L.cells * L.tufts[st.idx].syns_per_tft;
-    case BK_DEN: return (uint64_t)L.cells * L.tufts[st.idx].dens_per_tft;
+    case ST_INTRA_COL:
+    case ST_PYR_TAIL: return (uint64_t)L.v_size * L.u_size;
     default: return L.cells;
     }
 }
 
 // One batched per-cell launch of kind k for step st over every area.
-int add_cells(bm_batch_s::Group& G, bm_batch_s::StepPlan& p, int k) {
+int add_cells(bm_batch_s::StepPlan& p, int k) {
     const Step& st = p.st;
     std::vector<CellJob> jobs;
     uint64_t blocks = 0;
-    for (bm_area A : G.areas) {
+    for (bm_area A : p.areas) {
         CellJob J;
         std::memset(&J, 0, sizeof J);
         J.L = A->dl[st.layer];
@@ -265,10 +294,13 @@ int add_cells(bm_batch_s::Group& G, bm_batch_s::StepPlan& p, int k) {
         J.slices = A->slices;
         J.ctl = A->ctl;
         J.x = st.idx;
-        if (k == ST_INHIB_SIMPLE) {
+        if (k == ST_INHIB_SIMPLE || k == ST_INHIB_MTP) {
             J.key = A->inhib_key[st.layer][st.idx];
             J.radius = (int32_t)A->plan.layers[st.layer].ctrl[st.idx].field_radius;
         }
+        if (k == ST_PYR_TAIL)
+            J.ctrl = st.idx == 0xFF ? 0 : (A->plan.layers[st.layer].ctrl[st.idx].kind == BM_LYR_CTRL_INTRA_COLUMN ? 1 : 2);
+        J.learn = st.arg;
         const uint64_t n = items_of(A, k, st);
         if (n > 0xFFFFFFFFull) return set_err(BM_ERR_UNSUPPORTED, "batched step of more than 2^32 items");
         J.n = (uint32_t)n;
@@ -289,9 +321,9 @@ int add_cells(bm_batch_s::Group& G, bm_batch_s::StepPlan& p, int k) {
     return BM_OK;
 }
 
-int build_fused(bm_batch_s::Group& G, bm_batch_s::StepPlan& p) {
+int build_fused(bm_batch_s::StepPlan& p) {
     std::vector<FusedJob> jobs;
-    for (bm_area A : G.areas) {
+    for (bm_area A : p.areas) {
         if (!A->fused.t[p.st.layer][p.st.idx].ok) return BM_OK;
         jobs.push_back({&A->fused, &A->dl[p.st.layer], A->axns(), A->slices, A->ctl});
     }
@@ -301,63 +333,124 @@ int build_fused(bm_batch_s::Group& G, bm_batch_s::StepPlan& p) {
     return BM_OK;
 }
 
-int build_step(bm_batch_s::Group& G, bm_batch_s::StepPlan& p) {
+int build_step(bm_batch_s::StepPlan& p) {
     const Step& st = p.st;
     if (st.kind == ST_CYCLE_END) {
         p.form = bm_batch_s::F_END;
         return BM_OK;
     }
-    if (is_cell_step(st.kind)) return add_cells(G, p, st.kind);
+    if (is_cell_step(st.kind)) return add_cells(p, st.kind);
     if (st.kind != ST_TUFT) return BM_OK;   // the plain form's whole-layer tuft stages: each area's own
     bool none_ok = true, all_ok = true;
-    for (bm_area A : G.areas) {
+    for (bm_area A : p.areas) {
         const bool ok = A->fused.t[st.layer][st.idx].ok;
         none_ok = none_ok && !ok;
         all_ok = all_ok && ok;
     }
-    if (all_ok) return build_fused(G, p);
+    if (all_ok) {
+        // Tile size from the whole step's work, not each area's own: one
+        // launch serves every area, so small areas need not cut tiny tiles
+        // to fill the device (the autotuner refines this).
+        uint64_t total = 0;
+        int sms = 148;
+        for (bm_area A : p.areas) {
+            const bm_layer_plan& L = A->plan.layers[st.layer];
+            total += (uint64_t)L.cells * L.tufts[st.idx].syns_per_tft;
+            sms = A->fused.sms;
+        }
+        const uint32_t target = (uint32_t)std::min<uint64_t>(32768, std::max<uint64_t>(4096, total / ((uint64_t)sms * 16)));
+        for (bm_area A : p.areas) {
+            FusedTuft& FT = A->fused.t[st.layer][st.idx];
+            // An autotuned choice stays; an area another batch also holds
+            // keeps its tiles (that batch's launches are planned on them).
+            if (!FT.tiled || FT.tile_tuned || FT.tile_target == target || A->n_batches > 1) continue;
+            if (retile_fused_tuft(A->fused, A->plan, st.layer, st.idx, target)) A->verify_pending[st.layer] = true;
+        }
+        return build_fused(p);
+    }
     if (!none_ok) return BM_OK;
     // No area can take the fused kernel here (e.g. one-synapse dendrites):
-    // the tuft's four stages, each batched.
-    int rc = add_cells(G, p, BK_FLAGS);
-    if (rc == BM_OK) rc = add_cells(G, p, BK_SYN);
-    if (rc == BM_OK) rc = add_cells(G, p, BK_DEN);
-    if (rc == BM_OK && G.areas[0]->plan.layers[st.layer].kind == BM_LYR_PYRAMIDAL) rc = add_cells(G, p, BK_TFT);
-    return rc;
+    // the tuft's four stages per cell, batched.
+    return add_cells(p, BK_TUFT_CELLS);
 }
 
-void count_launches(bm_batch_s::Group& G) {
-    G.launches = 0;
-    for (const auto& p : G.plan) {
+void count_launches(bm_batch_s* B) {
+    uint32_t n = 0;
+    for (const auto& p : B->plan) {
         const Step& st = p.st;
         if (p.form == bm_batch_s::F_EACH) {
             // Each area's own launches for this step.
-            for (bm_area A : G.areas) {
+            for (bm_area A : p.areas) {
                 const bm_layer_plan& L = A->plan.layers[st.layer];
                 uint32_t per = 1;
-                if (st.kind == ST_TUFT && !A->fused.t[st.layer][st.idx].ok) per = L.kind == BM_LYR_PYRAMIDAL ? 4 : 3;
                 if (st.kind == ST_TUFTS_PLAIN) per = 1 + 2 * L.n_tufts + (L.kind == BM_LYR_PYRAMIDAL ? L.n_tufts : 0);
-                G.launches += per;
+                n += per;
             }
         } else if (p.form == bm_batch_s::F_CELLS) {
-            G.launches += (uint32_t)p.cells.size();
+            n += (uint32_t)p.cells.size();
         } else if (p.form == bm_batch_s::F_FUSED) {
-            G.launches += 1;
+            n += 1;
         }
     }
+    B->plan_launches = n;
 }
 
-// The group's steps; the cycle-end step is done once for the whole batch.
-int build_plan(bm_batch_s::Group& G) {
-    free_plan(G);
-    for (const Step& st : G.areas[0]->steps) {
+// The schedule: the shortest common supersequence of the areas' stage
+// programs (merged one distinct program at a time through their longest
+// common subsequence), each step run over the areas that have it. Areas are
+// independent, so any order that keeps each area's own order is exact. The
+// cycle-end step is done once for the whole batch.
+int build_plan(bm_batch_s* B) {
+    free_plan(B);
+    std::vector<Step> U;
+    std::vector<std::vector<uint32_t>> who;   // who[k]: areas (batch indices) having U[k]
+    for (uint32_t a = 0; a < B->areas.size(); a++) {
+        const std::vector<Step>& P = B->areas[a]->steps;
+        // Same program as an earlier area: its positions in U are known.
+        bool placed = false;
+        for (uint32_t b = 0; b < a && !placed; b++) {
+            if (!(B->areas[b]->steps == P)) continue;
+            for (auto& w : who)
+                if (std::find(w.begin(), w.end(), b) != w.end()) w.push_back(a);
+            placed = true;
+        }
+        if (placed) continue;
+        const size_t n = U.size(), m = P.size();
+        std::vector<std::vector<uint16_t>> L(n + 1, std::vector<uint16_t>(m + 1, 0));
+        for (size_t i = n; i-- > 0;)
+            for (size_t j = m; j-- > 0;)
+                L[i][j] = (U[i] == P[j]) ? (uint16_t)(L[i + 1][j + 1] + 1) : std::max(L[i + 1][j], L[i][j + 1]);
+        std::vector<Step> U2;
+        std::vector<std::vector<uint32_t>> who2;
+        size_t i = 0, j = 0;
+        while (i < n || j < m) {
+            if (i < n && j < m && U[i] == P[j]) {
+                U2.push_back(U[i]);
+                who2.push_back(who[i]);
+                who2.back().push_back(a);
+                i++, j++;
+            } else if (j == m || (i < n && L[i + 1][j] >= L[i][j + 1])) {
+                U2.push_back(U[i]);
+                who2.push_back(who[i]);
+                i++;
+            } else {
+                U2.push_back(P[j]);
+                who2.push_back({a});
+                j++;
+            }
+        }
+        U.swap(U2);
+        who.swap(who2);
+    }
+    for (size_t k = 0; k < U.size(); k++) {
         bm_batch_s::StepPlan p;
-        p.st = st;
-        int rc = build_step(G, p);
-        G.plan.push_back(p);
+        p.st = U[k];
+        for (uint32_t a : who[k]) p.areas.push_back(B->areas[a]);
+        int rc = p.st.kind == ST_CYCLE_END ? (p.form = bm_batch_s::F_END, BM_OK) : build_step(p);
+        B->plan.push_back(p);
         if (rc != BM_OK) return rc;
     }
-    count_launches(G);
+    count_launches(B);
     return BM_OK;
 }
 
@@ -411,19 +504,30 @@ int build_intake(bm_batch_s* B) {
 void enqueue_batch_cycle(bm_batch_s* B, cudaStream_t s) {
     if (B->intake_blocks)
         k_batch_intake<<<B->intake_blocks, kIntakeBlock, 0, s>>>(B->d_intake, B->n_intake, B->d_bctl);
-    for (auto& G : B->groups)
-        for (auto& p : G.plan) {
-            switch (p.form) {
-            case bm_batch_s::F_CELLS:
-                for (auto& c : p.cells) launch_cells(c.kind, c.d_jobs, c.n_jobs, c.n_blocks, s);
-                break;
-            case bm_batch_s::F_FUSED: launch_fused_batch(p.fb, s); break;
-            case bm_batch_s::F_END: break;
-            default:
-                for (bm_area A : G.areas) exec_step(A, p.st, s);
-                break;
-            }
+    const bool prof = B->profiling && s != B->cap;
+    for (size_t k = 0; k < B->plan.size(); k++) {
+        auto& p = B->plan[k];
+        bm_batch_s::Rec r{k, nullptr, nullptr};
+        if (prof && p.form != bm_batch_s::F_END) {
+            r.a = B->ev();
+            r.b = B->ev();
+            cudaEventRecord(r.a, s);
         }
+        switch (p.form) {
+        case bm_batch_s::F_CELLS:
+            for (auto& c : p.cells) launch_cells(c.kind, c.d_jobs, c.n_jobs, c.n_blocks, s);
+            break;
+        case bm_batch_s::F_FUSED: launch_fused_batch(p.fb, s); break;
+        case bm_batch_s::F_END: break;
+        default:
+            for (bm_area A : p.areas) exec_step(A, p.st, s);
+            break;
+        }
+        if (r.a) {
+            cudaEventRecord(r.b, s);
+            B->pending.push_back(r);
+        }
+    }
     const uint32_t n = (uint32_t)B->areas.size();
     k_batch_cycle_end<<<(n + 127) / 128, 128, 0, s>>>(B->d_ctls, n, B->d_bctl);
 }
@@ -450,7 +554,7 @@ int run_cycles(bm_batch_s* B, const void* frames, uint32_t n_cycles) {
     cudaStream_t s = B->stream();
     for (bm_area A : B->areas) run_pending_verifies(A, s);
     k_batch_begin<<<1, 1, 0, s>>>(B->d_bctl, (const uint8_t*)frames, B->frame_bytes);
-    if (B->use_graph) {
+    if (B->use_graph && !B->profiling) {
         int rc = ensure_graph(B);
         if (rc != BM_OK) return rc;
         for (uint32_t k = 0; k < n_cycles; k++) {
@@ -488,9 +592,10 @@ void step_ranges(bm_area_s* A, uint32_t i, uint32_t t, std::vector<Range>& out) 
         for (int k = BM_BUF_TFT_PREV_BEST_DEN_IDS; k <= BM_BUF_TFT_STATES; k++) add(k, T.cel_idz, L.cells);
 }
 
-std::string step_key(bm_batch_s::Group& G, const Step& st) {
+std::string step_key(const bm_batch_s::StepPlan& p) {
+    const Step& st = p.st;
     std::string k = "L" + std::to_string(st.layer) + "T" + std::to_string(st.idx);
-    for (bm_area A : G.areas) {
+    for (bm_area A : p.areas) {
         const bm_layer_plan& L = A->plan.layers[st.layer];
         const bm_tuft_plan& T = L.tufts[st.idx];
         char buf[96];
@@ -523,14 +628,18 @@ void write_cache(const char* path, const std::map<std::string, uint32_t>& m) {
 
 // Retiles tuft (i, t) of every area for `target` synapses per tile and
 // rebuilds the step's batched launch. False when some area cannot take it.
-bool apply_target(bm_batch_s* B, bm_batch_s::Group& G, bm_batch_s::StepPlan& p, uint32_t target) {
-    for (bm_area A : G.areas)
+bool apply_target(bm_batch_s* B, bm_batch_s::StepPlan& p, uint32_t target) {
+    for (bm_area A : p.areas)
+        if (A->n_batches > 1) return false;   // another batch's launches are planned on these tiles
+    for (bm_area A : p.areas) {
         if (!retile_fused_tuft(A->fused, A->plan, p.st.layer, p.st.idx, target)) return false;
-    for (bm_area A : G.areas) {
+        A->fused.t[p.st.layer][p.st.idx].tile_tuned = true;
+    }
+    for (bm_area A : p.areas) {
         A->verify_pending[p.st.layer] = true;
         run_pending_verifies(A, B->stream());
     }
-    return build_fused(G, p) == BM_OK && p.form == bm_batch_s::F_FUSED;
+    return build_fused(p) == BM_OK && p.form == bm_batch_s::F_FUSED;
 }
 
 }  // namespace
@@ -551,6 +660,7 @@ int bm_batch_create(bm_ctx ctx, const bm_area* areas, uint32_t n_areas, bm_batch
     if (!B) return set_err(BM_ERR_OOM, "host allocation failed");
     B->ctx = ctx;
     B->areas.assign(areas, areas + n_areas);
+    for (bm_area A : B->areas) A->n_batches++;
     cudaError_t e = cudaStreamCreateWithFlags(&B->cap, cudaStreamNonBlocking);
     if (e != cudaSuccess) { free_batch(B); return cuda_err(e, "cudaStreamCreate"); }
 
@@ -561,20 +671,8 @@ int bm_batch_create(bm_ctx ctx, const bm_area* areas, uint32_t n_areas, bm_batch
     if (e == cudaSuccess) e = cudaMalloc(&B->d_ctls, ctls.size() * sizeof(AreaCtl*));
     if (e == cudaSuccess) e = cudaMemcpy(B->d_ctls, ctls.data(), ctls.size() * sizeof(AreaCtl*), cudaMemcpyHostToDevice);
     if (e != cudaSuccess) { free_batch(B); return cuda_err(e, "batch set-up"); }
-    // Areas with equal stage programs form one group (first appearance order).
-    for (bm_area A : B->areas) {
-        bm_batch_s::Group* G = nullptr;
-        for (auto& g2 : B->groups)
-            if (g2.areas[0]->steps == A->steps) G = &g2;
-        if (!G) {
-            B->groups.emplace_back();
-            G = &B->groups.back();
-        }
-        G->areas.push_back(A);
-    }
     int rc = build_intake(B);
-    for (auto& G : B->groups)
-        if (rc == BM_OK) rc = build_plan(G);
+    if (rc == BM_OK) rc = build_plan(B);
     if (rc != BM_OK) { free_batch(B); return rc; }
     *out = B;
     return BM_OK;
@@ -647,10 +745,46 @@ int bm_batch_cycle_frames_device(bm_batch batch, const void* dev_frames, uint32_
     return run_cycles(batch, dev_frames, n_cycles);
 }
 
+int bm_batch_set_profiling(bm_batch batch, int on) {
+    if (!batch) return set_err(BM_ERR_INVALID, "null batch");
+    batch->profiling = on != 0;
+    return BM_OK;
+}
+
+int bm_batch_get_profile(bm_batch batch, uint32_t n_max, uint32_t* kinds, uint32_t* layers, uint32_t* idx,
+                         uint32_t* n_areas, uint64_t* launches, double* ms, uint32_t* n_out) {
+    if (!batch || !n_out) return set_err(BM_ERR_INVALID, "null argument");
+    DevGuard g(batch->ctx->device);
+    batch->drain_profile();
+    uint32_t n = 0;
+    for (auto& p : batch->plan) {
+        if (!p.prof_n || n >= n_max) continue;
+        if (kinds) kinds[n] = p.form == bm_batch_s::F_FUSED ? 1000u + p.st.kind : p.st.kind;
+        if (layers) layers[n] = p.st.layer;
+        if (idx) idx[n] = p.st.idx;
+        if (n_areas) n_areas[n] = (uint32_t)p.areas.size();
+        if (launches) launches[n] = p.prof_n;
+        if (ms) ms[n] = p.prof_ms;
+        n++;
+    }
+    *n_out = n;
+    return BM_OK;
+}
+
+int bm_batch_reset_profile(bm_batch batch) {
+    if (!batch) return set_err(BM_ERR_INVALID, "null batch");
+    batch->drain_profile();
+    for (auto& p : batch->plan) {
+        p.prof_n = 0;
+        p.prof_ms = 0;
+    }
+    return BM_OK;
+}
+
 int bm_batch_launches_per_cycle(bm_batch batch, uint32_t* out) {
     if (!batch || !out) return set_err(BM_ERR_INVALID, "null argument");
     uint32_t n = (batch->intake_blocks ? 1u : 0u) + 1u;   // copies, cycle end
-    for (const auto& G : batch->groups) n += G.launches;
+    n += batch->plan_launches;
     *out = n;
     return BM_OK;
 }
@@ -680,19 +814,18 @@ int bm_batch_autotune(bm_batch batch, const char* cache_path, uint32_t* n_tuned)
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
-    for (auto& G : B->groups)
-    for (auto& p : G.plan) {
+    for (auto& p : B->plan) {
         if (p.form != bm_batch_s::F_FUSED) continue;
-        const std::string key = step_key(G, p.st);
+        const std::string key = step_key(p);
         auto hit = cache.find(key);
         if (hit != cache.end()) {
-            if (!apply_target(B, G, p, hit->second)) build_fused(G, p);
+            if (!apply_target(B, p, hit->second)) build_fused(p);
             tuned++;
             continue;
         }
         // Save what the trials overwrite.
         std::vector<Range> ranges;
-        for (bm_area A : G.areas) step_ranges(A, p.st.layer, p.st.idx, ranges);
+        for (bm_area A : p.areas) step_ranges(A, p.st.layer, p.st.idx, ranges);
         uint64_t total = 0;
         for (auto& r : ranges) total += r.n;
         uint8_t* save = nullptr;
@@ -705,7 +838,7 @@ int bm_batch_autotune(bm_batch batch, const char* cache_path, uint32_t* n_tuned)
         uint32_t best_t = 0;
         float best_ms = 1e30f;
         for (uint32_t target : kTargets) {
-            if (!apply_target(B, G, p, target)) continue;
+            if (!apply_target(B, p, target)) continue;
             launch_fused_batch(p.fb, s);   // warm-up
             cudaEventRecord(e0, s);
             for (int r = 0; r < 5; r++) launch_fused_batch(p.fb, s);
@@ -715,7 +848,7 @@ int bm_batch_autotune(bm_batch batch, const char* cache_path, uint32_t* n_tuned)
             cudaEventElapsedTime(&ms, e0, e1);
             if (ms < best_ms) { best_ms = ms; best_t = target; }
         }
-        if (best_t == 0 || !apply_target(B, G, p, best_t)) build_fused(G, p);
+        if (best_t == 0 || !apply_target(B, p, best_t)) build_fused(p);
         o = 0;
         for (auto& r : ranges) { cudaMemcpyAsync(r.p, save + o, r.n, cudaMemcpyDeviceToDevice, s); o += r.n; }
         cudaStreamSynchronize(s);
@@ -724,7 +857,7 @@ int bm_batch_autotune(bm_batch batch, const char* cache_path, uint32_t* n_tuned)
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    for (auto& G : B->groups) count_launches(G);
+    count_launches(B);
     B->drop_graph();
     write_cache(cache_path, cache);
     if (n_tuned) *n_tuned = tuned;

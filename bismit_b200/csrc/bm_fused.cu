@@ -41,6 +41,7 @@
 
 #include <algorithm>
 #include <cstring>
+#include <new>
 
 #include "bm_kernels.h"
 
@@ -700,62 +701,61 @@ __global__ void __launch_bounds__(kThreads, 2) k_fused_tuft_tma(FusedTuftArgs A)
 }
 
 // ------------------------------------------------------- batched form ----
-// One launch over the tiles of several tufts (the same tuft of several areas):
-// job j owns global tiles tile0[j] .. tile0[j + 1] - 1. Persistent CTAs walk
-// the global tiles in the same stride as the one-tuft kernel; the producer
-// lane and the consumer warps each keep their current job's arguments in
-// shared memory (the producer may run a tile ahead into the next job). Every
-// job of a launch shares the ring geometry (nst, stage_stride, halo_off).
+// One launch over the tiles of several tufts (the same tuft step of several
+// areas): job j owns global tiles tile0[j] .. tile0[j + 1] - 1. Persistent
+// CTAs walk the global tiles in the same stride as the one-tuft kernel. The
+// job table is the launch's own parameter block (__grid_constant__): it is
+// read-only there, so the compiler keeps argument fields in registers across
+// the stores of a stage, and nothing needs copying per job. Every job of a
+// launch shares the ring geometry (nst, stage_stride, halo_off).
+constexpr uint32_t kMaxBatchJobs = 80;   // 80 argument blocks fit the 32 KB parameter limit
+
+struct BatchParams {
+    FusedTuftArgs jobs[kMaxBatchJobs];
+    uint32_t tile0[kMaxBatchJobs + 1];
+    uint32_t n_jobs, nst, halo_off;
+};
+static_assert(sizeof(BatchParams) <= 32764, "batched tuft parameter block exceeds the kernel parameter limit");
 
 // The job of global tile t: tile0[j] <= t < tile0[j + 1].
-__device__ __forceinline__ uint32_t job_of(const uint32_t* __restrict__ tile0, uint32_t n_jobs, uint32_t t) {
-    uint32_t lo = 0, hi = n_jobs;
+__device__ __forceinline__ uint32_t job_of(const BatchParams& P, uint32_t t) {
+    uint32_t lo = 0, hi = P.n_jobs;
     while (hi - lo > 1) {
         const uint32_t mid = (lo + hi) >> 1;
-        if (__ldg(tile0 + mid) <= t) lo = mid;
+        if (P.tile0[mid] <= t) lo = mid;
         else hi = mid;
     }
     return lo;
 }
 
-__device__ __forceinline__ void load_args(FusedTuftArgs& dst, const FusedTuftArgs* src, uint32_t tid, uint32_t nthr) {
-    static_assert(sizeof(FusedTuftArgs) % 8 == 0, "argument block is copied in 8-byte words");
-    const unsigned long long* s = (const unsigned long long*)src;
-    unsigned long long* d = (unsigned long long*)&dst;
-    for (uint32_t i = tid; i < sizeof(FusedTuftArgs) / 8; i += nthr) d[i] = __ldg(s + i);
-}
-
 template <bool TUFT>
-__global__ void __launch_bounds__(kThreads, 2)
-    k_fused_tuft_batch(const FusedTuftArgs* __restrict__ jobs, const uint32_t* __restrict__ tile0, uint32_t n_jobs,
-                       uint32_t nst, uint32_t halo_off) {
+__global__ void __launch_bounds__(kThreads, 2) k_fused_tuft_batch(const __grid_constant__ BatchParams P) {
     extern __shared__ __align__(128) uint8_t smem[];
     __shared__ volatile int s_abort;
-    __shared__ __align__(16) FusedTuftArgs s_job[2];   // [0] the producer's job, [1] the consumers'
+    const uint32_t nst = P.nst;
     init_ring(smem, nst, s_abort);
     uint64_t* full = (uint64_t*)smem;
     uint64_t* empty = full + nst;
     uint8_t* stages = smem + 128;
-    uint8_t* halo = smem + halo_off;
-    const uint32_t n_tiles = __ldg(tile0 + n_jobs);
+    uint8_t* halo = smem + P.halo_off;
+    const uint32_t n_tiles = P.tile0[P.n_jobs];
     const int tid = threadIdx.x;
     const int lane = tid & 31;
     const int wib = tid >> 5;
     if (wib == kWarps) {
         if (lane != 0) return;
-        FusedTuftArgs& A = s_job[0];
         uint32_t cur = 0xFFFFFFFFu, mode = 0, pb = 0, pround = 0;
         uint64_t issued = 0;
         AreaCtl* ctl = nullptr;
         for (uint32_t t = blockIdx.x; t < n_tiles && !s_abort; t += gridDim.x) {
-            const uint32_t j = job_of(tile0, n_jobs, t);
+            const uint32_t j = job_of(P, t);
+            const FusedTuftArgs& A = P.jobs[j];
             if (j != cur) {
-                load_args(A, jobs + j, 0, 1);
                 cur = j;
                 mode = mode_of(A);
                 ctl = A.ctl;
             }
-            const TileGeo G = tile_geo(A, t - __ldg(tile0 + j));
+            const TileGeo G = tile_geo(A, t - P.tile0[j]);
             bool ok;
             switch (mode) {
             case 0: ok = produce_tile<TUFT, 0, true>(A, G, stages, full, empty, pb, pround, issued, s_abort); break;
@@ -768,21 +768,19 @@ __global__ void __launch_bounds__(kThreads, 2)
         if (s_abort) producer_drain(ctl, full, nst, issued);
         return;
     }
-    FusedTuftArgs& A = s_job[1];
     uint32_t cur = 0xFFFFFFFFu, mode = 0, cb = 0, cphase = 0;
     int32_t rnd = 0;
     for (uint32_t t = blockIdx.x; t < n_tiles; t += gridDim.x) {
-        const uint32_t j = job_of(tile0, n_jobs, t);
-        consumers_sync();   // every consumer is done with the previous tile (footprint and job)
+        const uint32_t j = job_of(P, t);
+        const FusedTuftArgs& A = P.jobs[j];
+        consumers_sync();   // every consumer is done with the previous footprint
         if (s_abort) break;
         if (j != cur) {
-            load_args(A, jobs + j, (uint32_t)tid, kWarps * 32);
-            consumers_sync();
             cur = j;
             mode = mode_of(A);
             rnd = rnd_at(A.rnd_key, A.ctl->cycle);
         }
-        const TileGeo G = tile_geo(A, t - __ldg(tile0 + j));
+        const TileGeo G = tile_geo(A, t - P.tile0[j]);
         switch (mode) {
         case 0: consume_tile<TUFT, 0, true>(A, G, halo, stages, full, empty, cb, cphase, lane, wib, rnd, s_abort); break;
         case 1: consume_tile<TUFT, 0, false>(A, G, halo, stages, full, empty, cb, cphase, lane, wib, rnd, s_abort); break;
@@ -1160,58 +1158,58 @@ int prepare_fused_batch(FusedBatch& B, const std::vector<FusedJob>& jobs, uint32
     const uint64_t halo_off = 128 + (uint64_t)nst * stride;
     const uint64_t smem = halo_off + halo;
     if (smem > kMaxSmem) return BM_OK;
-    std::vector<FusedTuftArgs> args(jobs.size());
-    std::vector<uint32_t> tile0(jobs.size() + 1);
-    uint32_t total = 0;
-    for (size_t j = 0; j < jobs.size(); j++) {
-        const FusedJob& J = jobs[j];
-        make_args(args[j], *J.F, J.axns, J.slices, *J.L, layer, t, J.ctl);
-        args[j].nst = nst;
-        args[j].stage_stride = stride;
-        args[j].halo_off = (uint32_t)halo_off;
-        tile0[j] = total;
-        total += args[j].n_tiles;
-    }
-    tile0[jobs.size()] = total;
-    if (cudaMalloc(&B.d_jobs, args.size() * sizeof(FusedTuftArgs)) != cudaSuccess ||
-        cudaMalloc(&B.d_tile0, tile0.size() * sizeof(uint32_t)) != cudaSuccess) {
-        cudaGetLastError();
-        free_fused_batch(B);
-        return set_err(BM_ERR_OOM, "cudaMalloc of the batched tuft jobs failed");
-    }
-    if (cudaMemcpy(B.d_jobs, args.data(), args.size() * sizeof(FusedTuftArgs), cudaMemcpyHostToDevice) != cudaSuccess ||
-        cudaMemcpy(B.d_tile0, tile0.data(), tile0.size() * sizeof(uint32_t), cudaMemcpyHostToDevice) != cudaSuccess) {
-        cudaGetLastError();
-        free_fused_batch(B);
-        return set_err(BM_ERR_CUDA, "copy of the batched tuft jobs failed");
-    }
     auto kern = tuft ? k_fused_tuft_batch<true> : k_fused_tuft_batch<false>;
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMaxSmem);
     int per_sm = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads, (size_t)smem) != cudaSuccess) per_sm = 1;
     cudaGetLastError();
+    // One launch per kMaxBatchJobs jobs.
+    for (size_t j0 = 0; j0 < jobs.size(); j0 += kMaxBatchJobs) {
+        auto* P = new (std::nothrow) BatchParams;
+        if (!P) {
+            free_fused_batch(B);
+            return set_err(BM_ERR_OOM, "host allocation failed");
+        }
+        std::memset(P, 0, sizeof *P);
+        const size_t n = std::min<size_t>(kMaxBatchJobs, jobs.size() - j0);
+        uint32_t total = 0;
+        for (size_t j = 0; j < n; j++) {
+            const FusedJob& J = jobs[j0 + j];
+            make_args(P->jobs[j], *J.F, J.axns, J.slices, *J.L, layer, t, J.ctl);
+            P->jobs[j].nst = nst;
+            P->jobs[j].stage_stride = stride;
+            P->jobs[j].halo_off = (uint32_t)halo_off;
+            P->tile0[j] = total;
+            total += P->jobs[j].n_tiles;
+        }
+        P->tile0[n] = total;
+        P->n_jobs = (uint32_t)n;
+        P->nst = nst;
+        P->halo_off = (uint32_t)halo_off;
+        B.params.push_back(P);
+        B.grids.push_back((uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(total, (uint64_t)sms * std::max(per_sm, 1))));
+        B.n_tiles += total;
+    }
     B.ok = true;
     B.tuft = tuft;
     B.n_jobs = (uint32_t)jobs.size();
-    B.n_tiles = total;
     B.nst = nst;
     B.halo_off = (uint32_t)halo_off;
     B.smem = (uint32_t)smem;
-    B.grid = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(total, (uint64_t)sms * std::max(per_sm, 1)));
     return BM_OK;
 }
 
 void launch_fused_batch(const FusedBatch& B, cudaStream_t s) {
     if (!B.ok || !B.n_tiles) return;
     auto kern = B.tuft ? k_fused_tuft_batch<true> : k_fused_tuft_batch<false>;
-    kern<<<B.grid, kThreads, B.smem, s>>>((const FusedTuftArgs*)B.d_jobs, B.d_tile0, B.n_jobs, B.nst, B.halo_off);
+    for (size_t k = 0; k < B.params.size(); k++)
+        kern<<<B.grids[k], kThreads, B.smem, s>>>(*(const BatchParams*)B.params[k]);
 }
 
 void free_fused_batch(FusedBatch& B) {
-    if (B.d_jobs) cudaFree(B.d_jobs);
-    if (B.d_tile0) cudaFree(B.d_tile0);
-    B.d_jobs = nullptr;
-    B.d_tile0 = nullptr;
+    for (void* p : B.params) delete (BatchParams*)p;
+    B.params.clear();
+    B.grids.clear();
     B.ok = false;
 }
 

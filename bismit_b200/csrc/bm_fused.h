@@ -29,6 +29,7 @@ struct FusedTuft {
     uint32_t src_vs = 0, src_us = 0, src_vsz = 0, src_usz = 0;
     uint32_t src_idz[8] = {};
     uint32_t tile_target = 0;    // synapses per tile asked for (0: chosen from the tuft's size)
+    bool tile_tuned = false;     // tile_target came from the autotuner
 };
 
 struct FusedArea {
@@ -68,14 +69,14 @@ struct FusedJob {
     AreaCtl* ctl;
 };
 struct FusedBatch {
-    bool ok = false;        // every job is tiled and the ring fits: one launch serves them all
-    bool tuft = false;      // pyramidal layer
-    void* d_jobs = nullptr; // device argument blocks, one per job
-    uint32_t* d_tile0 = nullptr;
-    uint32_t n_jobs = 0, n_tiles = 0, nst = 2, halo_off = 0, smem = 0, grid = 1;
+    bool ok = false;             // every job is tiled and the ring fits: batched launches serve them all
+    bool tuft = false;           // pyramidal layer
+    std::vector<void*> params;   // host parameter blocks, one launch each (up to 80 jobs per launch)
+    std::vector<uint32_t> grids;
+    uint32_t n_jobs = 0, n_tiles = 0, nst = 2, halo_off = 0, smem = 0;
 };
-// Plans the launch (B.ok false when some job cannot share it; the caller then
-// launches each job's own form). Copies the argument blocks to the device.
+// Plans the launches (B.ok false when some job cannot share them; the caller
+// then launches each job's own form).
 int prepare_fused_batch(FusedBatch& B, const std::vector<FusedJob>& jobs, uint32_t layer, uint32_t t);
 void launch_fused_batch(const FusedBatch& B, cudaStream_t s);
 void free_fused_batch(FusedBatch& B);

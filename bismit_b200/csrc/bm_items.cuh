@@ -90,9 +90,9 @@ __device__ __forceinline__ uint8_t* soma_of(const DevLayer& L) {
     return L.kind == BM_LYR_SPINY_STELLATE ? L.buf[BM_BUF_DEN_STATES] : L.buf[BM_BUF_CEL_STATES];
 }
 
-// inhib_simple, cl/control.cl:28-191; cell c.
-__device__ __forceinline__ void inhib_simple_item(uint8_t* __restrict__ axns, const SliceRec* __restrict__ slices,
-                                                  const DevLayer& L, int radius, int32_t rnd, uint32_t c) {
+// inhib_simple, cl/control.cl:28-191; cell c. Returns the axon it wrote.
+__device__ __forceinline__ uint8_t inhib_simple_item(uint8_t* __restrict__ axns, const SliceRec* __restrict__ slices,
+                                                     const DevLayer& L, int radius, int32_t rnd, uint32_t c) {
     const uint8_t* cs = soma_of(L);
     int vsz = (int)L.v_size, usz = (int)L.u_size;
     int s = (int)(c / (uint32_t)(vsz * usz)), rem = (int)(c % (uint32_t)(vsz * usz));
@@ -114,10 +114,12 @@ __device__ __forceinline__ void inhib_simple_item(uint8_t* __restrict__ axns, co
             uninhibited &= ((int)cel_state * infl_max) >= ((int)nei * (infl_max - dd * dd));
         }
     }
-    axns[axi] = (uint8_t)(uninhibited * cel_state);
+    const uint8_t out = (uint8_t)(uninhibited * cel_state);
+    axns[axi] = out;
     int axon_active = uninhibited & (cel_state != 0);
     uint8_t* act = L.buf[BM_BUF_CEL_ACTIVITIES];
     act[c] = update_activity(act[c], axon_active, rnd, (int32_t)((uint32_t)cel_state | c), kCellActivityDecay);
+    return out;
 }
 
 // inhib_passthrough, cl/control.cl:194-217 (rnd is left at 0 by bismit's host,
@@ -223,6 +225,125 @@ __device__ __forceinline__ void tft_dst_mtp_item(const uint8_t* __restrict__ axn
         }
     }
     cfl[c] = (uint8_t)((f & ~kCelPrevActiveFlag) | (active ? kCelPrevActiveFlag : 0));
+}
+
+// ---------------------------------------------------- fused cell steps ----
+// The per-cell steps below run several of bismit's stages for one cell (or
+// column) in one thread where each stage depends only on that cell's own
+// earlier results; learning, whose work is a run of synapses per active cell,
+// is shared by the warp (lanes over synapses) so its accesses coalesce. Their
+// per-synapse arithmetic is the per-item bodies' above, unchanged.
+
+// tft_set_syn_flags + layer_cycle_syns + den_cycle_tft (+ tft_cycle) for cell c
+// of a tuft the fused tuft kernel does not take (e.g. one-synapse dendrites).
+// Flags of a synapse are set from its state before the synapse cycle rewrites
+// it, as the stage order has it.
+__device__ __forceinline__ void tuft_cell_item(const uint8_t* __restrict__ axns, const SliceRec* __restrict__ slices,
+                                               const DevLayer& L, uint32_t t, int32_t rnd_den, uint32_t c) {
+    const DevTuft& T = L.tft[t];
+    uint8_t* fl = L.buf[BM_BUF_SYN_FLAG_SETS];
+    const uint8_t* st = L.buf[BM_BUF_SYN_STATES];
+    for (uint32_t k = 0; k < T.spt; k++) {
+        const uint64_t i = (uint64_t)c * T.spt + k;
+        const uint64_t si = T.syn_idz + i;
+        fl[si] = (uint8_t)((fl[si] & ~kSynPrevActiveFlag) | (st[si] ? kSynPrevActiveFlag : 0));
+        syn_cycle_item(axns, slices, L, t, i);
+    }
+    for (uint32_t d = 0; d < T.dpt; d++) den_cycle_item(L, t, rnd_den, (uint64_t)c * T.dpt + d);
+    if (L.kind == BM_LYR_PYRAMIDAL) tft_cycle_item(L, t, c);
+}
+
+// Lanes of the warp apply ssc_mtp_simple's update to cell cc's synapses
+// (prx_syns__active__mtp_ltd, cl/bismit.cl:604-639; seed syn_idz + i).
+__device__ __forceinline__ void ssc_mtp_lanes(const DevLayer& L, int32_t rnd, uint32_t cc, int lane) {
+    const uint32_t spt = L.tft[0].spt;
+    const uint8_t* st = L.buf[BM_BUF_SYN_STATES];
+    int8_t* str = (int8_t*)L.buf[BM_BUF_SYN_STRENGTHS];
+    const uint32_t syn_idz = cc * spt;
+    for (uint32_t i = syn_idz + (uint32_t)lane; i < syn_idz + spt; i += 32) {
+        int8_t s = str[i];
+        const int32_t seed = (int32_t)(syn_idz + i);
+        if (st[i] != 0) s = (int8_t)(s + rnd_inc(rnd, seed, s, 0x7F));
+        else s = (int8_t)(s - rnd_dec(rnd, seed, s, 0x1FF));
+        str[i] = s;
+    }
+}
+
+// inhib_simple for cell c, then ssc_mtp_simple for the warp's cells whose axon
+// came out non-zero. The layer's slices must be plain (the axon inhib_simple
+// writes for cell c is axns[axn_idz + c], the one ssc_mtp_simple reads). Every
+// lane of the warp calls this; `valid` false for lanes past the last cell.
+__device__ __forceinline__ void inhib_mtp_warp(uint8_t* __restrict__ axns, const SliceRec* __restrict__ slices,
+                                               const DevLayer& L, int radius, int32_t rnd_inhib, int32_t rnd_mtp,
+                                               bool learn, uint32_t c, bool valid) {
+    const uint8_t ax = valid ? inhib_simple_item(axns, slices, L, radius, rnd_inhib, c) : (uint8_t)0;
+    if (!learn) return;
+    const int lane = threadIdx.x & 31;
+    unsigned mask = __ballot_sync(0xFFFFFFFFu, ax != 0);
+    while (mask) {
+        const int b = __ffs(mask) - 1;
+        mask &= mask - 1;
+        ssc_mtp_lanes(L, rnd_mtp, __shfl_sync(0xFFFFFFFFu, c, b), lane);
+    }
+}
+
+// pyr_cycle for the cells of column col, then its control (1: inhib_intra_column,
+// 2: pyr_output, 0: none), then tft_dst_mtp for every distal tuft in tuft order
+// (each one's CEL_PREV_ACTIVE update seen by the next), the warp sharing the
+// synapse runs of the cells that learn. The layer's slices must be plain (the
+// axon written for cell c is axns[axn_idz + c], the one learning reads).
+// Every lane of the warp calls this; `valid` false past the last column.
+__device__ __forceinline__ void pyr_tail_warp(uint8_t* __restrict__ axns, const SliceRec* __restrict__ slices,
+                                              const DevLayer& L, int ctrl, bool learn, const AreaCtl* ctl,
+                                              uint32_t col, bool valid) {
+    const uint32_t cols = L.v_size * L.u_size;
+    if (valid) {
+        for (uint32_t d = 0; d < L.depth; d++) pyr_cycle_item(L, d * cols + col);
+        if (ctrl == 1) intra_column_item(axns, slices, L, col);
+        else if (ctrl == 2)
+            for (uint32_t d = 0; d < L.depth; d++) pyr_output_item(axns, slices, L, d * cols + col);
+    }
+    if (!learn) return;
+    const int lane = threadIdx.x & 31;
+    uint8_t* cfl = L.buf[BM_BUF_CEL_FLAG_SETS];
+    const uint8_t* sfl = L.buf[BM_BUF_SYN_FLAG_SETS];
+    int8_t* str = (int8_t*)L.buf[BM_BUF_SYN_STRENGTHS];
+    for (uint32_t d = 0; d < L.depth; d++) {
+        const uint32_t c = d * cols + col;
+        uint8_t f = valid ? cfl[c] : (uint8_t)0;
+        const int active = valid ? (axns[L.axn_idz + c] != 0) : 0;
+        for (uint32_t t = 0; t < L.n_tufts; t++) {
+            const DevTuft& T = L.tft[t];
+            if (T.den_kind != BM_DEN_DISTAL) continue;
+            const int32_t rnd = rnd_at(T.rnd_key_mtp, ctl->cycle);
+            const uint32_t tci = c + (uint32_t)T.cel_idz;
+            const bool cond = valid && !(f & kCelPrevActiveFlag) && active &&
+                              L.buf[BM_BUF_TFT_PREV_BEST_DEN_STATES_RAW][tci] != 0;
+            uint32_t syn_idz = 0, n = 0;
+            if (cond) {
+                syn_idz = (uint32_t)L.buf[BM_BUF_TFT_PREV_BEST_DEN_IDS][tci] * T.spd + c * T.spt + (uint32_t)T.syn_idz;
+                // A best-dendrite id written by the caller past the tuft can
+                // address beyond the layer's synapses; such a range is skipped.
+                n = ((uint64_t)syn_idz + T.spd <= L.n_syns) ? T.spd : 0;
+            }
+            unsigned mask = __ballot_sync(0xFFFFFFFFu, cond && n);
+            while (mask) {
+                const int b = __ffs(mask) - 1;
+                mask &= mask - 1;
+                const uint32_t z = __shfl_sync(0xFFFFFFFFu, syn_idz, b);
+                const uint32_t nn = __shfl_sync(0xFFFFFFFFu, n, b);
+                for (uint32_t i = z + (uint32_t)lane; i < z + nn; i += 32) {
+                    int8_t s = str[i];
+                    const int32_t seed = (int32_t)(z + i);
+                    if (sfl[i] & kSynPrevActiveFlag) s = (int8_t)(s + rnd_inc(rnd, seed, s, 0x7F));
+                    else s = (int8_t)(s - rnd_dec(rnd, seed, s, 0xFFF));
+                    str[i] = s;
+                }
+            }
+            f = (uint8_t)((f & ~kCelPrevActiveFlag) | (active ? kCelPrevActiveFlag : 0));
+        }
+        if (valid) cfl[c] = f;
+    }
 }
 
 }  // namespace bm

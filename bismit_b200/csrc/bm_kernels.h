@@ -45,6 +45,15 @@ void launch_ssc_mtp_plain(const uint8_t* axns, const DevLayer& L, const AreaCtl*
 void launch_pyr_cycle_plain(const DevLayer& L, cudaStream_t s);
 void launch_pyr_output(uint8_t* axns, const SliceRec* slices, const DevLayer& L, cudaStream_t s);
 void launch_inhib_intra_column_plain(uint8_t* axns, const SliceRec* slices, const DevLayer& L, cudaStream_t s);
+// Fused cell steps (bm_items.cuh): an unfused tuft's four stages per cell;
+// inhibition with spiny stellate learning; pyramidal soma, control and distal
+// learning per column (ctrl: 0 none, 1 intra-column, 2 output).
+void launch_tuft_cells(const uint8_t* axns, const SliceRec* slices, const DevLayer& L, uint32_t t,
+                       const AreaCtl* ctl, cudaStream_t s);
+void launch_inhib_mtp(uint8_t* axns, const SliceRec* slices, const DevLayer& L, int radius, uint64_t key,
+                      bool learn, const AreaCtl* ctl, cudaStream_t s);
+void launch_pyr_tail(uint8_t* axns, const SliceRec* slices, const DevLayer& L, int ctrl, bool learn,
+                     const AreaCtl* ctl, cudaStream_t s);
 void launch_tft_dst_mtp_plain(const uint8_t* axns, const DevLayer& L, uint32_t t, const AreaCtl* ctl,
                               cudaStream_t s);
 

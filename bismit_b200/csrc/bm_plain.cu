@@ -93,6 +93,27 @@ __global__ void k_tft_dst_mtp(const uint8_t* __restrict__ axns, DevLayer L, uint
     if (c < L.cells) tft_dst_mtp_item(axns, L, t, rnd_at(L.tft[t].rnd_key_mtp, ctl->cycle), c);
 }
 
+__global__ void k_tuft_cells(const uint8_t* __restrict__ axns, const SliceRec* __restrict__ slices, DevLayer L,
+                             uint32_t t, const AreaCtl* ctl) {
+    uint32_t c = (uint32_t)gtid();
+    if (c < L.cells) tuft_cell_item(axns, slices, L, t, rnd_at(L.tft[t].rnd_key_den, ctl->cycle), c);
+}
+
+// Warp-cooperative: no thread leaves before the warp's shared part.
+__global__ void __launch_bounds__(128) k_inhib_mtp(uint8_t* __restrict__ axns, const SliceRec* __restrict__ slices,
+                                                   DevLayer L, int radius, uint64_t key, int learn,
+                                                   const AreaCtl* ctl) {
+    uint32_t c = (uint32_t)gtid();
+    inhib_mtp_warp(axns, slices, L, radius, rnd_at(key, ctl->cycle), rnd_at(L.rnd_key_ssc_mtp, ctl->cycle),
+                   learn != 0, c, c < L.cells);
+}
+
+__global__ void __launch_bounds__(128) k_pyr_tail(uint8_t* __restrict__ axns, const SliceRec* __restrict__ slices,
+                                                  DevLayer L, int ctrl, int learn, const AreaCtl* ctl) {
+    uint32_t col = (uint32_t)gtid();
+    pyr_tail_warp(axns, slices, L, ctrl, learn != 0, ctl, col, col < L.v_size * L.u_size);
+}
+
 inline unsigned nblk(uint64_t n, unsigned b) { return (unsigned)((n + b - 1) / b); }
 
 }  // namespace
@@ -143,6 +164,18 @@ void launch_pyr_output(uint8_t* axns, const SliceRec* slices, const DevLayer& L,
 }
 void launch_inhib_intra_column_plain(uint8_t* axns, const SliceRec* slices, const DevLayer& L, cudaStream_t s) {
     k_inhib_intra_column<<<nblk((uint64_t)L.v_size * L.u_size, 256), 256, 0, s>>>(axns, slices, L);
+}
+void launch_tuft_cells(const uint8_t* axns, const SliceRec* slices, const DevLayer& L, uint32_t t,
+                       const AreaCtl* ctl, cudaStream_t s) {
+    k_tuft_cells<<<nblk(L.cells, 128), 128, 0, s>>>(axns, slices, L, t, ctl);
+}
+void launch_inhib_mtp(uint8_t* axns, const SliceRec* slices, const DevLayer& L, int radius, uint64_t key,
+                      bool learn, const AreaCtl* ctl, cudaStream_t s) {
+    k_inhib_mtp<<<nblk(L.cells, 128), 128, 0, s>>>(axns, slices, L, radius, key, learn ? 1 : 0, ctl);
+}
+void launch_pyr_tail(uint8_t* axns, const SliceRec* slices, const DevLayer& L, int ctrl, bool learn,
+                     const AreaCtl* ctl, cudaStream_t s) {
+    k_pyr_tail<<<nblk((uint64_t)L.v_size * L.u_size, 128), 128, 0, s>>>(axns, slices, L, ctrl, learn ? 1 : 0, ctl);
 }
 void launch_tft_dst_mtp_plain(const uint8_t* axns, const DevLayer& L, uint32_t t, const AreaCtl* ctl,
                               cudaStream_t s) {

@@ -11,10 +11,13 @@
 // once, all of them in one batch (bm_batch.cu: one launch per stage step per
 // layer-map group, replayed from a CUDA graph); the batch is rebuilt only when
 // the set of sessions in the tick changes. Frames of the tick are packed into
-// one pinned block and copied in with one transfer; each session's output
-// axons come back into its own pinned buffer. While a tick runs on the GPU the
-// host admits waiting sessions: their areas are built and grown on a second
-// stream, so set-up overlaps the running cycles.
+// one pinned block and copied in with one transfer; the sessions' output axons
+// are gathered on the device and come back with one transfer. Ticks are
+// pipelined two deep: a call queues tick N and then completes tick N - 1, so
+// the host's packing and bookkeeping overlap the GPU's cycles (pinned blocks
+// are double-buffered). While tick N runs the host also admits waiting
+// sessions: their areas are built and grown on a second stream, so set-up
+// overlaps the running cycles too.
 //
 // Latency of a frame = completion of the tick that cycled it minus the moment
 // it became ready (its submission, or the completion of the session's
@@ -36,10 +39,54 @@ using Clock = std::chrono::steady_clock;
 
 double now_s() { return std::chrono::duration<double>(Clock::now().time_since_epoch()).count(); }
 
-struct Frame {
+// Frames of one bm_server_submit call, consumed front to back.
+struct Chunk {
     std::vector<uint8_t> bytes;
-    double submitted;
+    uint32_t n = 0, next = 0;
+    double submitted = 0;
 };
+
+// A session's frame queue: chunks in submission order.
+struct FrameQueue {
+    std::deque<Chunk> chunks;
+    uint32_t len = 0;
+    bool empty() const { return chunks.empty(); }
+    const uint8_t* front() const { return chunks.front().bytes.data() + (size_t)chunks.front().next * len; }
+    double front_submitted() const { return chunks.front().submitted; }
+    void pop() {
+        if (++chunks.front().next == chunks.front().n) chunks.pop_front();
+    }
+};
+
+// One session's output in a tick's gathered output block.
+struct OutJob {
+    const uint8_t* src;
+    uint64_t dst_off;
+    uint32_t len;
+    uint32_t block0;
+};
+
+constexpr uint32_t kGatherBlock = 256;
+
+__global__ void __launch_bounds__(kGatherBlock) k_gather_outputs(const OutJob* __restrict__ jobs, uint32_t n_jobs,
+                                                                 uint8_t* __restrict__ dst) {
+    __shared__ uint32_t s_j;
+    if (threadIdx.x == 0) {
+        uint32_t lo = 0, hi = n_jobs;
+        while (hi - lo > 1) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (jobs[mid].block0 <= blockIdx.x) lo = mid;
+            else hi = mid;
+        }
+        s_j = lo;
+    }
+    __syncthreads();
+    const OutJob& J = jobs[s_j];
+    const uint32_t i = (blockIdx.x - J.block0) * kGatherBlock * 4 + threadIdx.x;
+#pragma unroll
+    for (uint32_t k = 0; k < 4; k++)
+        if (i + k * kGatherBlock < J.len) dst[J.dst_off + i + k * kGatherBlock] = J.src[i + k * kGatherBlock];
+}
 
 }  // namespace
 
@@ -50,13 +97,23 @@ struct bm_server_s {
         uint64_t seed = 0;
         uint64_t bytes = 0;          // device bytes while resident
         bm_area area = nullptr;
-        std::deque<Frame> frames;
+        FrameQueue frames;
         uint8_t* out = nullptr;      // pinned: output 0 after the latest cycled frame
         uint32_t out_len = 0, in_len = 0;
         uint64_t done = 0;           // frames cycled
+        uint32_t inflight = 0;       // queued ticks holding one of its frames
         double last_done = 0;        // completion time of the latest cycled frame
         double opened = 0, admitted = 0;
         bool closing = false, resident = false, retired = false;
+    };
+    // A queued tick: its sessions (with their frames' submission times), its
+    // pinned blocks and completion event.
+    struct Tick {
+        bool live = false;
+        std::vector<Session*> members;
+        std::vector<double> submitted;
+        double syn = 0, started = 0;
+        uint32_t buf = 0;
     };
     bm_ctx ctx = nullptr;            // the serving stream
     bm_ctx setup = nullptr;          // area construction, overlapping the ticks
@@ -65,14 +122,25 @@ struct bm_server_s {
     std::vector<Session*> sessions;  // every open session, in open order
     bm_batch batch = nullptr;
     std::vector<Session*> members;   // the batch's sessions, in batch order
-    uint8_t* h_frames = nullptr;     // pinned frame block
+    uint8_t* h_frames[2] = {};       // pinned frame blocks (double-buffered)
     uint8_t* d_frames = nullptr;
     uint64_t frames_cap = 0;
-    cudaEvent_t done_ev = nullptr;
+    uint8_t* h_out[2] = {};          // pinned gathered-output blocks
+    uint8_t* d_out = nullptr;
+    uint64_t out_cap = 0;
+    OutJob* d_outjobs = nullptr;     // the current batch's output gather
+    uint32_t out_blocks = 0;
+    uint64_t out_bytes = 0;
+    cudaEvent_t done_ev[2] = {};
+    cudaEvent_t start_ev[2] = {};    // timing: device time of each tick
+    Tick inflight[2];
+    uint64_t tick_no = 0;
     // Statistics.
     std::vector<float> lat_ms;
     uint64_t ticks = 0, frames_cycled = 0, rebuilds = 0;
     double syn_cycles = 0, busy_s = 0, first_tick = 0, last_tick = 0;
+    double rebuild_s = 0, admit_s = 0;   // host time in batch rebuilds and in admissions
+    double gpu_s = 0;                    // device time of the ticks (frames in to outputs out)
 
     Session* find(uint32_t id) {
         for (Session* s : sessions)
@@ -122,19 +190,90 @@ void retire(bm_server_s* V, bm_server_s::Session* S) {
     S->area = nullptr;
 }
 
-int ensure_frames(bm_server_s* V, uint64_t bytes) {
-    if (bytes <= V->frames_cap) return BM_OK;
-    if (V->h_frames) cudaFreeHost(V->h_frames);
-    if (V->d_frames) cudaFree(V->d_frames);
-    V->h_frames = nullptr;
-    V->d_frames = nullptr;
-    V->frames_cap = 0;
-    uint64_t cap = std::max<uint64_t>(bytes, 1 << 20);
-    if (cudaHostAlloc(&V->h_frames, cap, cudaHostAllocDefault) != cudaSuccess || cudaMalloc(&V->d_frames, cap) != cudaSuccess) {
+// Grows a pair of pinned blocks and their device block (the stream must be
+// idle: callers only grow right after a batch rebuild, which synchronises).
+int ensure_blocks(uint8_t* (&h)[2], uint8_t*& d, uint64_t& cap, uint64_t bytes, const char* what) {
+    if (bytes <= cap) return BM_OK;
+    for (auto& p : h)
+        if (p) cudaFreeHost(p);
+    if (d) cudaFree(d);
+    h[0] = h[1] = nullptr;
+    d = nullptr;
+    cap = 0;
+    uint64_t c = std::max<uint64_t>(bytes, 1 << 20);
+    if (cudaHostAlloc(&h[0], c, cudaHostAllocDefault) != cudaSuccess ||
+        cudaHostAlloc(&h[1], c, cudaHostAllocDefault) != cudaSuccess || cudaMalloc(&d, c) != cudaSuccess) {
         cudaGetLastError();
-        return set_err(BM_ERR_OOM, "frame staging of %llu bytes", (unsigned long long)cap);
+        return set_err(BM_ERR_OOM, "%s staging of %llu bytes", what, (unsigned long long)c);
     }
-    V->frames_cap = cap;
+    cap = c;
+    return BM_OK;
+}
+
+// Completes queued tick slot b: latencies, outputs, counters.
+int complete(bm_server_s* V, uint32_t b) {
+    bm_server_s::Tick& T = V->inflight[b];
+    if (!T.live) return BM_OK;
+    cudaError_t e = cudaEventSynchronize(V->done_ev[b]);
+    if (e != cudaSuccess) return cuda_err(e, "tick");
+    const double t1 = now_s();
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, V->start_ev[b], V->done_ev[b]) == cudaSuccess) V->gpu_s += ms * 1e-3;
+    cudaGetLastError();
+    uint64_t o = 0;
+    for (size_t k = 0; k < T.members.size(); k++) {
+        auto* S = T.members[k];
+        std::memcpy(S->out, V->h_out[T.buf] + o, S->out_len);
+        o += S->out_len;
+        const double ready = std::max(T.submitted[k], S->last_done);
+        V->lat_ms.push_back((float)((t1 - ready) * 1e3));
+        S->done++;
+        S->inflight--;
+        S->last_done = t1;
+    }
+    V->ticks++;
+    V->frames_cycled += T.members.size();
+    V->syn_cycles += T.syn;
+    V->busy_s += t1 - T.started;
+    V->last_tick = t1;
+    T.live = false;
+    T.members.clear();
+    T.submitted.clear();
+    return BM_OK;
+}
+
+int complete_all(bm_server_s* V) {
+    // Ticks complete in queue order: the older slot first (the latest queued
+    // tick, tick_no - 1, sits in slot (tick_no - 1) & 1).
+    const uint32_t older = (uint32_t)(V->tick_no & 1);
+    int rc = complete(V, older);
+    if (rc == BM_OK) rc = complete(V, older ^ 1);
+    return rc;
+}
+
+// Output gather of the current batch's members, packed in batch order.
+int build_outjobs(bm_server_s* V) {
+    if (V->d_outjobs) cudaFree(V->d_outjobs);
+    V->d_outjobs = nullptr;
+    std::vector<OutJob> jobs;
+    uint64_t blocks = 0, o = 0;
+    for (auto* S : V->members) {
+        OutJob J;
+        J.src = S->area->axns() + S->area->plan.outputs[0].axn_idz;
+        J.dst_off = o;
+        J.len = S->out_len;
+        J.block0 = (uint32_t)blocks;
+        blocks += (J.len + kGatherBlock * 4 - 1) / (kGatherBlock * 4);
+        o += J.len;
+        jobs.push_back(J);
+    }
+    V->out_blocks = (uint32_t)blocks;
+    V->out_bytes = o;
+    int rc = ensure_blocks(V->h_out, V->d_out, V->out_cap, o, "output");
+    if (rc != BM_OK) return rc;
+    cudaError_t e = cudaMalloc(&V->d_outjobs, jobs.size() * sizeof(OutJob));
+    if (e == cudaSuccess) e = cudaMemcpy(V->d_outjobs, jobs.data(), jobs.size() * sizeof(OutJob), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return cuda_err(e, "output gather jobs");
     return BM_OK;
 }
 
@@ -157,7 +296,8 @@ int bm_server_create(bm_ctx ctx, uint64_t mem_budget, bm_server* out) {
         mem_budget = (uint64_t)(fr * 0.9);
     }
     V->budget = mem_budget;
-    if (cudaEventCreateWithFlags(&V->done_ev, cudaEventDisableTiming) != cudaSuccess) {
+    if (cudaEventCreate(&V->done_ev[0]) != cudaSuccess || cudaEventCreate(&V->done_ev[1]) != cudaSuccess ||
+        cudaEventCreate(&V->start_ev[0]) != cudaSuccess || cudaEventCreate(&V->start_ev[1]) != cudaSuccess) {
         cudaGetLastError();
         bm_ctx_destroy(V->setup);
         delete V;
@@ -173,9 +313,15 @@ int bm_server_destroy(bm_server V) {
     cudaStreamSynchronize(V->ctx->stream());
     if (V->batch) bm_batch_destroy(V->batch);
     for (auto* S : V->sessions) free_session(S);
-    if (V->h_frames) cudaFreeHost(V->h_frames);
+    for (int b = 0; b < 2; b++) {
+        if (V->h_frames[b]) cudaFreeHost(V->h_frames[b]);
+        if (V->h_out[b]) cudaFreeHost(V->h_out[b]);
+        if (V->done_ev[b]) cudaEventDestroy(V->done_ev[b]);
+        if (V->start_ev[b]) cudaEventDestroy(V->start_ev[b]);
+    }
     if (V->d_frames) cudaFree(V->d_frames);
-    if (V->done_ev) cudaEventDestroy(V->done_ev);
+    if (V->d_out) cudaFree(V->d_out);
+    if (V->d_outjobs) cudaFree(V->d_outjobs);
     bm_ctx_destroy(V->setup);
     delete V;
     return BM_OK;
@@ -214,7 +360,14 @@ int bm_server_submit(bm_server V, uint32_t session, const uint8_t* frames, size_
     if (S->closing) return set_err(BM_ERR_INVALID, "bm_server_submit: session %u is closing", session);
     if (frame_len != S->in_len) return set_err(BM_ERR_INVALID, "frame length %zu != %u", frame_len, S->in_len);
     const double t = now_s();
-    for (uint32_t k = 0; k < n_frames; k++) S->frames.push_back({std::vector<uint8_t>(frames + k * frame_len, frames + (k + 1) * frame_len), t});
+    if (n_frames) {
+        Chunk c;
+        c.bytes.assign(frames, frames + (size_t)n_frames * frame_len);
+        c.n = n_frames;
+        c.submitted = t;
+        S->frames.len = (uint32_t)frame_len;
+        S->frames.chunks.push_back(std::move(c));
+    }
     return BM_OK;
 }
 
@@ -233,10 +386,10 @@ int bm_server_tick(bm_server V, uint32_t* n_cycled) {
     const double t0 = now_s();
     if (!V->first_tick) V->first_tick = t0;
 
-    // 1. Retire drained, closed sessions (their last tick has completed). A
+    // 1. Retire drained, closed sessions (no frame left, none in flight). A
     //    batch that holds one is dropped first.
     for (auto* S : V->sessions) {
-        if (!S->closing || !S->frames.empty()) continue;
+        if (!S->closing || !S->frames.empty() || S->inflight) continue;
         if (std::find(V->members.begin(), V->members.end(), S) != V->members.end()) {
             if (V->batch) bm_batch_destroy(V->batch);
             V->batch = nullptr;
@@ -250,77 +403,85 @@ int bm_server_tick(bm_server V, uint32_t* n_cycled) {
         else free_session(S);
     V->sessions.swap(live);
 
-    // 2. This tick's sessions: resident with a pending frame. Frames in, one
-    //    batched cycle, outputs out, all queued on the serving stream.
+    // 2. Queue tick N: resident sessions with a pending frame.
     std::vector<bm_server_s::Session*> m;
     for (auto* S : V->sessions)
         if (S->resident && !S->frames.empty()) m.push_back(S);
     if (n_cycled) *n_cycled = (uint32_t)m.size();
-    double syn = 0;
+    const uint32_t slot = (uint32_t)(V->tick_no & 1);
     if (!m.empty()) {
         if (m != V->members || !V->batch) {
+            // The previous tick completes first: its outputs sit in the pinned
+            // blocks that a rebuild may reallocate.
+            const double r0 = now_s();
+            int rc = complete_all(V);
+            if (rc != BM_OK) return rc;
             if (V->batch) bm_batch_destroy(V->batch);
             V->batch = nullptr;
             V->members.clear();
             std::vector<bm_area> areas;
             for (auto* S : m) areas.push_back(S->area);
-            int rc = bm_batch_create(V->ctx, areas.data(), (uint32_t)areas.size(), &V->batch);
+            rc = bm_batch_create(V->ctx, areas.data(), (uint32_t)areas.size(), &V->batch);
             if (rc != BM_OK) return rc;
             V->members = m;
             V->rebuilds++;
+            uint64_t fb = 0;
+            bm_batch_frame_bytes(V->batch, &fb);
+            rc = ensure_blocks(V->h_frames, V->d_frames, V->frames_cap, fb, "frame");
+            if (rc == BM_OK) rc = build_outjobs(V);
+            if (rc != BM_OK) return rc;
+            V->rebuild_s += now_s() - r0;
         }
-        uint64_t fb = 0;
-        bm_batch_frame_bytes(V->batch, &fb);
-        int rc = ensure_frames(V, fb);
-        if (rc != BM_OK) return rc;
+        // Slot `slot` was completed at least one call ago, so its pinned
+        // blocks are free.
+        bm_server_s::Tick& T = V->inflight[slot];
+        T.live = true;
+        T.buf = slot;
+        T.started = t0;
+        T.syn = 0;
+        T.members = m;
         uint64_t o = 0;
         for (auto* S : m) {
-            std::memcpy(V->h_frames + o, S->frames.front().bytes.data(), S->in_len);
+            std::memcpy(V->h_frames[slot] + o, S->frames.front(), S->in_len);
             o += S->in_len;
-            syn += (double)S->area->plan.n_syns_total;
+            T.submitted.push_back(S->frames.front_submitted());
+            T.syn += (double)S->area->plan.n_syns_total;
+            S->frames.pop();
+            S->inflight++;
         }
-        cudaError_t e = cudaMemcpyAsync(V->d_frames, V->h_frames, fb, cudaMemcpyHostToDevice, s);
+        cudaError_t e = cudaEventRecord(V->start_ev[slot], s);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(V->d_frames, V->h_frames[slot], o, cudaMemcpyHostToDevice, s);
         if (e != cudaSuccess) return cuda_err(e, "frame block copy");
-        rc = bm_batch_cycle_frames_device(V->batch, V->d_frames, 1);
+        int rc = bm_batch_cycle_frames_device(V->batch, V->d_frames, 1);
         if (rc != BM_OK) return rc;
-        for (auto* S : m) {
-            const bm_io_plan& out = S->area->plan.outputs[0];
-            e = cudaMemcpyAsync(S->out, S->area->axns() + out.axn_idz, out.len, cudaMemcpyDeviceToHost, s);
-            if (e != cudaSuccess) return cuda_err(e, "output copy");
-        }
-        e = cudaEventRecord(V->done_ev, s);
-        if (e != cudaSuccess) return cuda_err(e, "cudaEventRecord");
+        if (V->out_blocks) k_gather_outputs<<<V->out_blocks, kGatherBlock, 0, s>>>(V->d_outjobs, (uint32_t)m.size(), V->d_out);
+        e = cudaMemcpyAsync(V->h_out[slot], V->d_out, V->out_bytes, cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaEventRecord(V->done_ev[slot], s);
+        if (e != cudaSuccess) return cuda_err(e, "tick");
+        V->tick_no++;
     }
 
-    // 3. While that runs: admit waiting sessions in FIFO order as the budget
+    // 3. While it runs: admit waiting sessions in FIFO order as the budget
     //    allows (none overtakes an earlier one that does not fit). Their areas
-    //    are built and grown on the set-up stream; they join the next tick.
+    //    are built and grown on the set-up stream; they join a later tick.
+    const double a0 = now_s();
     for (auto* S : V->sessions) {
         if (S->resident) continue;
         if (V->used + S->bytes > V->budget) break;
         int rc = admit(V, S);
         if (rc != BM_OK) return rc;
     }
-    if (m.empty()) return BM_OK;
+    V->admit_s += now_s() - a0;
 
-    // 4. Completion.
-    cudaError_t e = cudaEventSynchronize(V->done_ev);
-    if (e != cudaSuccess) return cuda_err(e, "tick");
-    const double t1 = now_s();
-    for (auto* S : m) {
-        const Frame& f = S->frames.front();
-        const double ready = std::max(f.submitted, S->last_done);
-        V->lat_ms.push_back((float)((t1 - ready) * 1e3));
-        S->frames.pop_front();
-        S->done++;
-        S->last_done = t1;
-    }
-    V->ticks++;
-    V->frames_cycled += m.size();
-    V->syn_cycles += syn;
-    V->busy_s += t1 - t0;
-    V->last_tick = t1;
-    return BM_OK;
+    // 4. Complete the previous tick (with nothing queued now: every tick).
+    if (!m.empty()) return complete(V, slot ^ 1);
+    return complete_all(V);
+}
+
+int bm_server_drain(bm_server V) {
+    if (!V) return set_err(BM_ERR_INVALID, "null server");
+    DevGuard g(V->ctx->device);
+    return complete_all(V);
 }
 
 int bm_server_read_output(bm_server V, uint32_t session, uint8_t* dst, size_t len, uint64_t* frames_done) {
@@ -351,6 +512,9 @@ int bm_server_get_stats(bm_server V, bm_server_stats* st) {
     st->syn_cycles = V->syn_cycles;
     st->busy_s = V->busy_s;
     st->span_s = V->last_tick > V->first_tick ? V->last_tick - V->first_tick : 0;
+    st->rebuild_s = V->rebuild_s;
+    st->gpu_s = V->gpu_s;
+    st->admit_s = V->admit_s;
     st->used_bytes = V->used;
     st->budget_bytes = V->budget;
     for (auto* S : V->sessions) {
@@ -377,7 +541,7 @@ int bm_server_reset_stats(bm_server V) {
     if (!V) return set_err(BM_ERR_INVALID, "null server");
     V->lat_ms.clear();
     V->ticks = V->frames_cycled = V->rebuilds = 0;
-    V->syn_cycles = V->busy_s = V->first_tick = V->last_tick = 0;
+    V->syn_cycles = V->busy_s = V->first_tick = V->last_tick = V->rebuild_s = V->admit_s = V->gpu_s = 0;
     return BM_OK;
 }
 

@@ -371,11 +371,11 @@ int bm_area_reset_profile(bm_area area);
 int bm_area_launches_per_cycle(bm_area area, uint32_t* out);
 
 /* ------------------------------------------------------------- batches ---
- * A batch cycles several areas together, of uneven column-grid sizes. Areas
- * that share a stage program (layer map structure, settings and execution
- * path) form a group, and each stage step of a group runs as one launch over
- * all of its areas; the whole cycle is captured once as a CUDA graph and
- * replayed. Every area keeps its own state; an area's bytes after a batched
+ * A batch cycles several areas together, of uneven column-grid sizes and
+ * possibly different layer maps. It schedules one sequence of stage steps
+ * that contains every area's own step sequence in order, and runs each step
+ * as one launch over all areas that have it; the whole cycle is captured once
+ * as a CUDA graph and replayed. Every area keeps its own state; an area's bytes after a batched
  * cycle are the bytes it would have after bm_area_cycle alone (given the same
  * inputs). Replaces bismit's one-area-at-a-time loop
  * over areas in Cortex::cycle (src/cortex/cortex.rs:99-119), where every area
@@ -417,6 +417,16 @@ int bm_batch_cycle_frames_device(bm_batch batch, const void* dev_frames, uint32_
 
 /* Kernel launches per batched cycle (all areas together). */
 int bm_batch_launches_per_cycle(bm_batch batch, uint32_t* out);
+
+/* Per-step CUDA-event timing of later cycles (the graph is bypassed while
+ * on). bm_batch_get_profile reports, per scheduled step that ran: its step
+ * kind (+1000 when it ran as one batched fused-tuft launch), layer, tuft or
+ * control index, number of areas, launches and summed device milliseconds;
+ * n_max entries at most, *n_out written. Arrays may be NULL. */
+int bm_batch_set_profiling(bm_batch batch, int on);
+int bm_batch_get_profile(bm_batch batch, uint32_t n_max, uint32_t* kinds, uint32_t* layers, uint32_t* idx,
+                         uint32_t* n_areas, uint64_t* launches, double* ms, uint32_t* n_out);
+int bm_batch_reset_profile(bm_batch batch);
 
 /* OR of the areas' sticky device error bits; BM_ERR_TIMEOUT when any is set. */
 int bm_batch_device_errors(bm_batch batch, uint32_t* bits);
@@ -479,7 +489,9 @@ typedef struct bm_server_s* bm_server;
 typedef struct bm_server_stats {
     uint64_t ticks, frames, batch_rebuilds;
     double   syn_cycles;          /* synapse-cycles done                         */
-    double   busy_s;              /* time inside bm_server_tick                  */
+    double   busy_s;              /* summed tick spans (queue to completion)     */
+    double   rebuild_s, admit_s;  /* host time in batch rebuilds / admissions    */
+    double   gpu_s;               /* device time of the ticks                    */
     double   span_s;              /* first tick start to last tick end           */
     double   p50_ms, p99_ms, mean_ms;  /* per-frame latency: completion minus the
                                      moment the frame was ready (submitted, or its
@@ -498,8 +510,12 @@ int bm_server_submit(bm_server server, uint32_t session, const uint8_t* frames, 
                      uint32_t n_frames);
 /* The session leaves once its submitted frames are cycled. */
 int bm_server_close(bm_server server, uint32_t session);
-/* One tick; *n_cycled (optional) = sessions cycled. Synchronous. */
+/* Queues one tick (*n_cycled, optional: sessions in it) and completes the
+ * previous one: ticks are pipelined two deep, so a session's output and
+ * frame count reflect the tick before the latest. */
 int bm_server_tick(bm_server server, uint32_t* n_cycled);
+/* Completes every queued tick. */
+int bm_server_drain(bm_server server);
 /* Output 0 after the session's latest cycled frame; *frames_done (optional). */
 int bm_server_read_output(bm_server server, uint32_t session, uint8_t* dst, size_t len, uint64_t* frames_done);
 /* The session's area while it is resident (NULL while waiting). */

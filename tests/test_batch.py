@@ -155,8 +155,9 @@ def test_batch_autotune_keeps_state_and_parity(tmp_path):
 
 @pytest.mark.gpu
 def test_batch_groups_areas_with_different_programs():
-    """Areas whose stage programs differ (here: learning off in one) are
-    grouped; each still ends with its bytes from cycling alone."""
+    """Areas whose stage programs differ (learning off in one, another layer
+    map in another) share one schedule; each still ends with its bytes from
+    cycling alone."""
     ctx = cortex._Ctx(0)
     descs = [_desc(32, 1, 8, 16), _desc(48, 2, 8, 32, configs.bench_settings().disable_learning()),
              _desc(40, 1, 16, 16), _deep_desc(32)]
