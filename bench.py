@@ -51,10 +51,8 @@ def parse():
 
 
 def dist_env():
-    ws = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    return ws, rank, local
+    from bismit_b200.replicas import dist_env as env
+    return env()
 
 
 def workload_config(name):
@@ -251,12 +249,10 @@ def run_batched(args, ctx, stream, K, W, ws):
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
 
+    from bismit_b200.replicas import max_over_ranks
+
     def max_ms(ms):
-        if ws > 1:
-            t = torch.tensor([ms], device="cuda")
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-            return float(t.item())
-        return ms
+        return max_over_ranks(ms, "cuda")
 
     # (a) batched, graph replay
     batch.cycle_frames_device(packed.data_ptr(), W)
@@ -324,12 +320,10 @@ def run_hierarchy(args, ctx, stream, K, W, ws):
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
 
+    from bismit_b200.replicas import max_over_ranks
+
     def max_ms(ms):
-        if ws > 1:
-            t = torch.tensor([ms], device="cuda")
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-            return float(t.item())
-        return ms
+        return max_over_ranks(ms, "cuda")
 
     cx.batch.cycle_frames_device(fr.data_ptr(), W)
     torch.cuda.synchronize()
@@ -453,12 +447,13 @@ def run_ours(args):
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
     ctx.set_stream(stream.cuda_stream)
-    area = cortex.CorticalArea(ctx, desc, seed=args.seed + 1000 * rank)
+    from bismit_b200.replicas import frame_seed, max_over_ranks, replica_seed
+    area = cortex.CorticalArea(ctx, desc, seed=replica_seed(args.seed, rank))
     plan = area.plan
     flen = area.input_len()
     K, W = args.steps, args.warmup
     nfr = K + W
-    host_frames = configs.frames(nfr, flen, act, args.seed + rank)
+    host_frames = configs.frames(nfr, flen, act, frame_seed(args.seed, rank))
     dev_frames = torch.from_numpy(host_frames).to("cuda")
 
     def barrier():
@@ -486,12 +481,8 @@ def run_ours(args):
     barrier()
     soak(lambda: area.cycle_frames_device(dev_frames.data_ptr(), flen, W), stream, SOAK_S)
     clk = clocks.stop()
-    ms = e0.elapsed_time(e1)
+    ms = max_over_ranks(e0.elapsed_time(e1), "cuda")
     launches = area.launches_per_cycle() * K
-    if ws > 1:
-        t = torch.tensor([ms], device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms = float(t.item())
     n_syn = int(plan.n_syns_total)
     value = n_syn * K * ws / (ms / 1e3)
 
@@ -534,10 +525,7 @@ def run_ours(args):
     e2e_ms = e0.elapsed_time(e1)
     e2e_wall = time.perf_counter() - t0
     barrier()
-    if ws > 1:
-        t = torch.tensor([e2e_ms], device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    e2e_ms = max_over_ranks(e2e_ms, "cuda")
     e2e_val = n_syn * K * ws / (e2e_ms / 1e3)
 
     area.close()

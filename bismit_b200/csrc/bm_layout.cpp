@@ -26,6 +26,7 @@ namespace {
 
 struct Fail {
     std::string msg;
+    int code = BM_ERR_INVALID;
 };
 
 [[noreturn]] void fail(const char* fmt, ...) __attribute__((format(printf, 1, 2)));
@@ -35,8 +36,11 @@ void fail(const char* fmt, ...) {
     va_start(ap, fmt);
     vsnprintf(buf, sizeof buf, fmt, ap);
     va_end(ap);
-    throw Fail{buf};
+    throw Fail{buf, BM_ERR_INVALID};
 }
+
+// A scheme feature outside this path (a valid scheme this library does not run).
+[[noreturn]] void unsupported(const char* msg) { throw Fail{msg, BM_ERR_UNSUPPORTED}; }
 
 // calc_scale, src/cmn/slice_dims.rs:201-224.
 uint32_t calc_scale(uint32_t src_dim, uint32_t tar_dim) {
@@ -138,8 +142,8 @@ int resolve_area(const bm_area_desc* D, uint64_t seed, bm_area_plan* P, std::vec
         if (D->v_size == 0 || D->u_size == 0 || D->v_size > 4096 || D->u_size > 4096)
             fail("area dims must be 1..4096 (got %u x %u)", D->v_size, D->u_size);
         if (!(D->settings & BM_SET_DISABLE_REGROWTH))
-            fail("synapse regrowth (CorticalAreaSettings without disable_regrowth) is not on this path: "
-                 "set BM_SET_DISABLE_REGROWTH");
+            unsupported("synapse regrowth (CorticalAreaSettings without disable_regrowth) is not on this path: "
+                        "set BM_SET_DISABLE_REGROWTH");
         P->area_id = D->area_id;
         P->v_size = D->v_size;
         P->u_size = D->u_size;
@@ -430,7 +434,7 @@ int resolve_area(const bm_area_desc* D, uint64_t seed, bm_area_plan* P, std::vec
         return BM_OK;
     } catch (const Fail& f) {
         if (err) *err = f.msg;
-        return BM_ERR_INVALID;
+        return f.code;
     }
 }
 
