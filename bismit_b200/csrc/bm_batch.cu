@@ -389,7 +389,7 @@ void count_launches(bm_batch_s* B) {
         } else if (p.form == bm_batch_s::F_CELLS) {
             n += (uint32_t)p.cells.size();
         } else if (p.form == bm_batch_s::F_FUSED) {
-            n += 1;
+            n += (uint32_t)p.fb.params.size();
         }
     }
     B->plan_launches = n;

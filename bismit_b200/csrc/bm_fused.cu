@@ -53,6 +53,7 @@ constexpr int kWarps = 8;                    // consumer warps per CTA (tiled fo
 constexpr int kThreads = (kWarps + 1) * 32;  // plus one producer warp
 constexpr int kMaxRecs = 8;                  // contiguous source slices served by the fast gathers
 constexpr uint32_t kMaxSmem = 110 * 1024;    // dynamic shared memory per CTA (two CTAs per SM)
+constexpr uint32_t kSmem3 = 73 * 1024;       // ... with which three CTAs fit one SM
 constexpr uint32_t kWaitLimit = 1u << 22;
 
 struct FusedTuftArgs {
@@ -687,7 +688,7 @@ __device__ __forceinline__ uint32_t mode_of(const FusedTuftArgs& A) {
 }
 
 template <bool TUFT>
-__global__ void __launch_bounds__(kThreads, 2) k_fused_tuft_tma(FusedTuftArgs A) {
+__global__ void __launch_bounds__(kThreads, 3) k_fused_tuft_tma(FusedTuftArgs A) {
     extern __shared__ __align__(128) uint8_t smem[];
     __shared__ volatile int s_abort;   // a bounded wait gave up
     init_ring(smem, A.nst, s_abort);
@@ -729,7 +730,7 @@ __device__ __forceinline__ uint32_t job_of(const BatchParams& P, uint32_t t) {
 }
 
 template <bool TUFT>
-__global__ void __launch_bounds__(kThreads, 2) k_fused_tuft_batch(const __grid_constant__ BatchParams P) {
+__global__ void __launch_bounds__(kThreads, 3) k_fused_tuft_batch(const __grid_constant__ BatchParams P) {
     extern __shared__ __align__(128) uint8_t smem[];
     __shared__ volatile int s_abort;
     const uint32_t nst = P.nst;
@@ -847,6 +848,14 @@ inline bool pow2(uint64_t x) { return x && !(x & (x - 1)); }
 
 namespace {
 
+// Stages of the shared-memory ring: two when that lets three CTAs share an
+// SM (more warps to hide the gathers' latency, the same bytes in flight per
+// SM), else as many as fit about 80 KB with two CTAs per SM.
+uint32_t ring_stages(uint64_t stride, uint64_t halo) {
+    if (128 + 2 * stride + halo <= kSmem3) return 2;
+    return (uint32_t)std::max<uint64_t>(2, std::min<uint64_t>(4, (80 * 1024) / stride));
+}
+
 int device_sms() {
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
@@ -921,7 +930,7 @@ void plan_tuft(FusedTuft& FT, const bm_area_plan& P, uint32_t i, uint32_t t, int
     // at both ends.
     const uint32_t win_bytes = SB / 16 + 32;
     const uint32_t buf_bytes = 6 * SB + 5 * win_bytes;
-    uint32_t nst = (uint32_t)std::max<uint64_t>(2, std::min<uint64_t>(4, (80 * 1024) / buf_bytes));
+    const uint32_t nst = ring_stages(buf_bytes, ((halo + 15) / 16) * 16);
     const uint64_t halo_off = 128 + (uint64_t)nst * buf_bytes;
     const uint64_t smem = halo_off + ((halo + 15) / 16) * 16;
     if (smem > kMaxSmem) return;
@@ -1145,57 +1154,74 @@ int prepare_fused_batch(FusedBatch& B, const std::vector<FusedJob>& jobs, uint32
     B = FusedBatch{};
     if (jobs.empty()) return BM_OK;
     const bool tuft = jobs[0].L->kind == BM_LYR_PYRAMIDAL;
-    uint32_t stride = 0, halo = 0, sms = 148;
+    uint32_t sms = 148;
     for (const FusedJob& J : jobs) {
         const FusedTuft& FT = J.F->t[layer][t];
         if (!FT.ok || !FT.tiled || !FT.gidx || (J.L->kind == BM_LYR_PYRAMIDAL) != tuft) return BM_OK;
-        stride = std::max(stride, FT.stage_stride);
-        halo = std::max(halo, ((FT.nrec * FT.fsz + 15) / 16) * 16);
         sms = (uint32_t)J.F->sms;
     }
-    uint32_t nst = (uint32_t)std::max<uint64_t>(2, std::min<uint64_t>(4, (80 * 1024) / stride));
-    while (nst > 2 && 128 + (uint64_t)nst * stride + halo > kMaxSmem) nst--;
-    const uint64_t halo_off = 128 + (uint64_t)nst * stride;
-    const uint64_t smem = halo_off + halo;
-    if (smem > kMaxSmem) return BM_OK;
     auto kern = tuft ? k_fused_tuft_batch<true> : k_fused_tuft_batch<false>;
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMaxSmem);
-    int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads, (size_t)smem) != cudaSuccess) per_sm = 1;
-    cudaGetLastError();
-    // One launch per kMaxBatchJobs jobs.
-    for (size_t j0 = 0; j0 < jobs.size(); j0 += kMaxBatchJobs) {
-        auto* P = new (std::nothrow) BatchParams;
-        if (!P) {
+    // Jobs of one stage geometry share launches (a launch's ring is uniform,
+    // and jobs with smaller stages then keep three CTAs per SM).
+    std::vector<uint32_t> strides;
+    for (const FusedJob& J : jobs) {
+        const uint32_t st = J.F->t[layer][t].stage_stride;
+        if (std::find(strides.begin(), strides.end(), st) == strides.end()) strides.push_back(st);
+    }
+    std::sort(strides.begin(), strides.end());
+    for (uint32_t stride : strides) {
+        std::vector<const FusedJob*> cls;
+        uint32_t halo = 0;
+        for (const FusedJob& J : jobs) {
+            const FusedTuft& FT = J.F->t[layer][t];
+            if (FT.stage_stride != stride) continue;
+            cls.push_back(&J);
+            halo = std::max(halo, ((FT.nrec * FT.fsz + 15) / 16) * 16);
+        }
+        uint32_t nst = ring_stages(stride, halo);
+        while (nst > 2 && 128 + (uint64_t)nst * stride + halo > kMaxSmem) nst--;
+        const uint64_t halo_off = 128 + (uint64_t)nst * stride;
+        const uint64_t smem = halo_off + halo;
+        if (smem > kMaxSmem) {
             free_fused_batch(B);
-            return set_err(BM_ERR_OOM, "host allocation failed");
+            return BM_OK;
         }
-        std::memset(P, 0, sizeof *P);
-        const size_t n = std::min<size_t>(kMaxBatchJobs, jobs.size() - j0);
-        uint32_t total = 0;
-        for (size_t j = 0; j < n; j++) {
-            const FusedJob& J = jobs[j0 + j];
-            make_args(P->jobs[j], *J.F, J.axns, J.slices, *J.L, layer, t, J.ctl);
-            P->jobs[j].nst = nst;
-            P->jobs[j].stage_stride = stride;
-            P->jobs[j].halo_off = (uint32_t)halo_off;
-            P->tile0[j] = total;
-            total += P->jobs[j].n_tiles;
+        int per_sm = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads, (size_t)smem) != cudaSuccess)
+            per_sm = 1;
+        cudaGetLastError();
+        for (size_t j0 = 0; j0 < cls.size(); j0 += kMaxBatchJobs) {
+            auto* P = new (std::nothrow) BatchParams;
+            if (!P) {
+                free_fused_batch(B);
+                return set_err(BM_ERR_OOM, "host allocation failed");
+            }
+            std::memset(P, 0, sizeof *P);
+            const size_t n = std::min<size_t>(kMaxBatchJobs, cls.size() - j0);
+            uint32_t total = 0;
+            for (size_t j = 0; j < n; j++) {
+                const FusedJob& J = *cls[j0 + j];
+                make_args(P->jobs[j], *J.F, J.axns, J.slices, *J.L, layer, t, J.ctl);
+                P->jobs[j].nst = nst;
+                P->jobs[j].stage_stride = stride;
+                P->jobs[j].halo_off = (uint32_t)halo_off;
+                P->tile0[j] = total;
+                total += P->jobs[j].n_tiles;
+            }
+            P->tile0[n] = total;
+            P->n_jobs = (uint32_t)n;
+            P->nst = nst;
+            P->halo_off = (uint32_t)halo_off;
+            B.params.push_back(P);
+            B.grids.push_back((uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(total, (uint64_t)sms * std::max(per_sm, 1))));
+            B.smems.push_back((uint32_t)smem);
+            B.n_tiles += total;
         }
-        P->tile0[n] = total;
-        P->n_jobs = (uint32_t)n;
-        P->nst = nst;
-        P->halo_off = (uint32_t)halo_off;
-        B.params.push_back(P);
-        B.grids.push_back((uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(total, (uint64_t)sms * std::max(per_sm, 1))));
-        B.n_tiles += total;
     }
     B.ok = true;
     B.tuft = tuft;
     B.n_jobs = (uint32_t)jobs.size();
-    B.nst = nst;
-    B.halo_off = (uint32_t)halo_off;
-    B.smem = (uint32_t)smem;
     return BM_OK;
 }
 
@@ -1203,13 +1229,14 @@ void launch_fused_batch(const FusedBatch& B, cudaStream_t s) {
     if (!B.ok || !B.n_tiles) return;
     auto kern = B.tuft ? k_fused_tuft_batch<true> : k_fused_tuft_batch<false>;
     for (size_t k = 0; k < B.params.size(); k++)
-        kern<<<B.grids[k], kThreads, B.smem, s>>>(*(const BatchParams*)B.params[k]);
+        kern<<<B.grids[k], kThreads, B.smems[k], s>>>(*(const BatchParams*)B.params[k]);
 }
 
 void free_fused_batch(FusedBatch& B) {
     for (void* p : B.params) delete (BatchParams*)p;
     B.params.clear();
     B.grids.clear();
+    B.smems.clear();
     B.ok = false;
 }
 

@@ -71,9 +71,10 @@ struct FusedJob {
 struct FusedBatch {
     bool ok = false;             // every job is tiled and the ring fits: batched launches serve them all
     bool tuft = false;           // pyramidal layer
-    std::vector<void*> params;   // host parameter blocks, one launch each (up to 80 jobs per launch)
-    std::vector<uint32_t> grids;
-    uint32_t n_jobs = 0, n_tiles = 0, nst = 2, halo_off = 0, smem = 0;
+    std::vector<void*> params;   // host parameter blocks, one launch each (up to 80 jobs of one
+    std::vector<uint32_t> grids; // stage geometry per launch)
+    std::vector<uint32_t> smems;
+    uint32_t n_jobs = 0, n_tiles = 0;
 };
 // Plans the launches (B.ok false when some job cannot share them; the caller
 // then launches each job's own form).
