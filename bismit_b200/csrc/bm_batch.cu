@@ -275,8 +275,8 @@ void free_batch(bm_batch_s* B) {
 uint64_t items_of(const bm_area_s* A, int k, const Step& st) {
     const bm_layer_plan& L = A->plan.layers[st.layer];
     switch (k) {
-    case ST_INTRA_COL:
-    case ST_PYR_TAIL: return (uint64_t)L.v_size * L.u_size;
+    case ST_INTRA_COL: return (uint64_t)L.v_size * L.u_size;
+    case ST_PYR_TAIL: return tail_items(L.depth, L.v_size * L.u_size);
     default: return L.cells;
     }
 }

@@ -293,10 +293,111 @@ __device__ __forceinline__ void inhib_mtp_warp(uint8_t* __restrict__ axns, const
 // synapse runs of the cells that learn. The layer's slices must be plain (the
 // axon written for cell c is axns[axn_idz + c], the one learning reads).
 // Every lane of the warp calls this; `valid` false past the last column.
+// Columns up to kTailDepth cells deep keep the column in registers: every
+// input is loaded before any result is stored, so the loads overlap.
+constexpr uint32_t kTailDepth = 8;
+
+__device__ __forceinline__ void dst_mtp_lanes(const DevLayer& L, const DevTuft& T, int32_t rnd, uint32_t z,
+                                              uint32_t nn, int lane) {
+    const uint8_t* sfl = L.buf[BM_BUF_SYN_FLAG_SETS];
+    int8_t* str = (int8_t*)L.buf[BM_BUF_SYN_STRENGTHS];
+    for (uint32_t i = z + (uint32_t)lane; i < z + nn; i += 32) {
+        int8_t s = str[i];
+        const int32_t seed = (int32_t)(z + i);
+        if (sfl[i] & kSynPrevActiveFlag) s = (int8_t)(s + rnd_inc(rnd, seed, s, 0x7F));
+        else s = (int8_t)(s - rnd_dec(rnd, seed, s, 0xFFF));
+        str[i] = s;
+    }
+}
+
+// Cell c of distal tuft T learns (tft_dst_mtp's condition): its synapse run
+// [z, z + n), n = 0 when it does not.
+__device__ __forceinline__ void dst_mtp_range(const DevLayer& L, const DevTuft& T, uint32_t c, uint8_t f, bool active,
+                                              bool valid, uint32_t& z, uint32_t& n) {
+    z = 0;
+    n = 0;
+    const uint32_t tci = c + (uint32_t)T.cel_idz;
+    if (valid && !(f & kCelPrevActiveFlag) && active && L.buf[BM_BUF_TFT_PREV_BEST_DEN_STATES_RAW][tci] != 0) {
+        z = (uint32_t)L.buf[BM_BUF_TFT_PREV_BEST_DEN_IDS][tci] * T.spd + c * T.spt + (uint32_t)T.syn_idz;
+        // A best-dendrite id written by the caller past the tuft can address
+        // beyond the layer's synapses; such a range is skipped.
+        n = ((uint64_t)z + T.spd <= L.n_syns) ? T.spd : 0;
+    }
+}
+
+// Lanes per column of the cell-parallel tail: the column's cells sit in
+// adjacent lanes (a power of two >= depth); 0 when the column is too deep and
+// one thread takes the whole column.
+__device__ __forceinline__ uint32_t tail_group(uint32_t depth) {
+    return depth <= 1 ? 1u : depth <= 2 ? 2u : depth <= 4 ? 4u : depth <= kTailDepth ? 8u : 0u;
+}
+__host__ __device__ __forceinline__ uint64_t tail_items(uint32_t depth, uint32_t cols) {
+    const uint32_t g = depth <= 1 ? 1u : depth <= 2 ? 2u : depth <= 4 ? 4u : depth <= kTailDepth ? 8u : 1u;
+    return (uint64_t)cols * g;
+}
+
+// Item t of the tail: lane d of column t / G, G = tail_group(depth), or the
+// whole column t when the column is deeper than kTailDepth.
 __device__ __forceinline__ void pyr_tail_warp(uint8_t* __restrict__ axns, const SliceRec* __restrict__ slices,
                                               const DevLayer& L, int ctrl, bool learn, const AreaCtl* ctl,
-                                              uint32_t col, bool valid) {
+                                              uint32_t item, bool valid_item) {
     const uint32_t cols = L.v_size * L.u_size;
+    const int lane = threadIdx.x & 31;
+    uint8_t* cfl = L.buf[BM_BUF_CEL_FLAG_SETS];
+    const uint32_t G = tail_group(L.depth);
+    if (G) {
+        const uint32_t col = item / G, d = item & (G - 1);
+        const bool valid = valid_item && col < cols && d < L.depth;
+        const uint32_t c = d * cols + col;
+        const bool prx_on = (L.enabled_flags & kDenBasalProximalFlag) != 0;
+        const bool dst_on = (L.enabled_flags & kDenBasalDistalFlag) != 0;
+        uint8_t prx = 0, dst = 0, f = 0, ax = 0;
+        if (valid) {
+            prx = prx_on ? L.buf[BM_BUF_TFT_STATES][(uint64_t)L.prx_id * L.cells + c] : (uint8_t)0;
+            dst = dst_on ? L.buf[BM_BUF_TFT_BEST_DEN_STATES_RAW][(uint64_t)L.dst_id * L.cells + c] : (uint8_t)0;
+            if (learn) f = cfl[c];
+            if (ctrl == 0) ax = axns[L.axn_idz + c];
+        }
+        // pyr_cycle, cl/bismit.cl:961-1022 (as pyr_cycle_item).
+        const int p_active = prx != 0;
+        const int is_min = (prx <= 3) && p_active;
+        const uint8_t soma = (uint8_t)((uint8_t)((prx >> 2) + is_min) + (uint8_t)(p_active ? (dst >> 1) : 0));
+        if (valid) L.buf[BM_BUF_CEL_STATES][c] = soma;
+        if (ctrl == 1) {
+            // inhib_intra_column, cl/control.cl:319-352: the column's cells in
+            // depth order through the group's lanes.
+            const int base = lane & ~(int)(G - 1);
+            uint8_t best = 0;
+            for (uint32_t k = 0; k < G; k++) {
+                const uint8_t st = (uint8_t)__shfl_sync(0xFFFFFFFFu, (uint32_t)soma, base + (int)k);
+                if (k < L.depth) best = (st >= best) ? st : (uint8_t)0;
+            }
+            ax = (soma >= best) ? soma : (uint8_t)0;
+        } else if (ctrl == 2) {
+            ax = soma;   // pyr_output, cl/control.cl:298-314
+        }
+        if (valid && ctrl != 0) axns[L.axn_idz + c] = ax;
+        if (!learn) return;
+        for (uint32_t t = 0; t < L.n_tufts; t++) {
+            const DevTuft& T = L.tft[t];
+            if (T.den_kind != BM_DEN_DISTAL) continue;
+            const int32_t rnd = rnd_at(T.rnd_key_mtp, ctl->cycle);
+            uint32_t z, n;
+            dst_mtp_range(L, T, c, f, ax != 0, valid, z, n);
+            unsigned mask = __ballot_sync(0xFFFFFFFFu, n != 0);
+            while (mask) {
+                const int b = __ffs(mask) - 1;
+                mask &= mask - 1;
+                dst_mtp_lanes(L, T, rnd, __shfl_sync(0xFFFFFFFFu, z, b), __shfl_sync(0xFFFFFFFFu, n, b), lane);
+            }
+            f = (uint8_t)((f & ~kCelPrevActiveFlag) | (ax ? kCelPrevActiveFlag : 0));
+        }
+        if (valid) cfl[c] = f;
+        return;
+    }
+    const uint32_t col = item;
+    const bool valid = valid_item && col < cols;
+    // Deeper columns: the same steps one cell at a time.
     if (valid) {
         for (uint32_t d = 0; d < L.depth; d++) pyr_cycle_item(L, d * cols + col);
         if (ctrl == 1) intra_column_item(axns, slices, L, col);
@@ -304,41 +405,21 @@ __device__ __forceinline__ void pyr_tail_warp(uint8_t* __restrict__ axns, const 
             for (uint32_t d = 0; d < L.depth; d++) pyr_output_item(axns, slices, L, d * cols + col);
     }
     if (!learn) return;
-    const int lane = threadIdx.x & 31;
-    uint8_t* cfl = L.buf[BM_BUF_CEL_FLAG_SETS];
-    const uint8_t* sfl = L.buf[BM_BUF_SYN_FLAG_SETS];
-    int8_t* str = (int8_t*)L.buf[BM_BUF_SYN_STRENGTHS];
     for (uint32_t d = 0; d < L.depth; d++) {
         const uint32_t c = d * cols + col;
         uint8_t f = valid ? cfl[c] : (uint8_t)0;
-        const int active = valid ? (axns[L.axn_idz + c] != 0) : 0;
+        const bool active = valid && axns[L.axn_idz + c] != 0;
         for (uint32_t t = 0; t < L.n_tufts; t++) {
             const DevTuft& T = L.tft[t];
             if (T.den_kind != BM_DEN_DISTAL) continue;
             const int32_t rnd = rnd_at(T.rnd_key_mtp, ctl->cycle);
-            const uint32_t tci = c + (uint32_t)T.cel_idz;
-            const bool cond = valid && !(f & kCelPrevActiveFlag) && active &&
-                              L.buf[BM_BUF_TFT_PREV_BEST_DEN_STATES_RAW][tci] != 0;
-            uint32_t syn_idz = 0, n = 0;
-            if (cond) {
-                syn_idz = (uint32_t)L.buf[BM_BUF_TFT_PREV_BEST_DEN_IDS][tci] * T.spd + c * T.spt + (uint32_t)T.syn_idz;
-                // A best-dendrite id written by the caller past the tuft can
-                // address beyond the layer's synapses; such a range is skipped.
-                n = ((uint64_t)syn_idz + T.spd <= L.n_syns) ? T.spd : 0;
-            }
-            unsigned mask = __ballot_sync(0xFFFFFFFFu, cond && n);
+            uint32_t z, n;
+            dst_mtp_range(L, T, c, f, active, valid, z, n);
+            unsigned mask = __ballot_sync(0xFFFFFFFFu, n != 0);
             while (mask) {
                 const int b = __ffs(mask) - 1;
                 mask &= mask - 1;
-                const uint32_t z = __shfl_sync(0xFFFFFFFFu, syn_idz, b);
-                const uint32_t nn = __shfl_sync(0xFFFFFFFFu, n, b);
-                for (uint32_t i = z + (uint32_t)lane; i < z + nn; i += 32) {
-                    int8_t s = str[i];
-                    const int32_t seed = (int32_t)(z + i);
-                    if (sfl[i] & kSynPrevActiveFlag) s = (int8_t)(s + rnd_inc(rnd, seed, s, 0x7F));
-                    else s = (int8_t)(s - rnd_dec(rnd, seed, s, 0xFFF));
-                    str[i] = s;
-                }
+                dst_mtp_lanes(L, T, rnd, __shfl_sync(0xFFFFFFFFu, z, b), __shfl_sync(0xFFFFFFFFu, n, b), lane);
             }
             f = (uint8_t)((f & ~kCelPrevActiveFlag) | (active ? kCelPrevActiveFlag : 0));
         }

@@ -110,8 +110,8 @@ __global__ void __launch_bounds__(128) k_inhib_mtp(uint8_t* __restrict__ axns, c
 
 __global__ void __launch_bounds__(128) k_pyr_tail(uint8_t* __restrict__ axns, const SliceRec* __restrict__ slices,
                                                   DevLayer L, int ctrl, int learn, const AreaCtl* ctl) {
-    uint32_t col = (uint32_t)gtid();
-    pyr_tail_warp(axns, slices, L, ctrl, learn != 0, ctl, col, col < L.v_size * L.u_size);
+    const uint64_t i = gtid();
+    pyr_tail_warp(axns, slices, L, ctrl, learn != 0, ctl, (uint32_t)i, i < tail_items(L.depth, L.v_size * L.u_size));
 }
 
 inline unsigned nblk(uint64_t n, unsigned b) { return (unsigned)((n + b - 1) / b); }
@@ -175,7 +175,8 @@ void launch_inhib_mtp(uint8_t* axns, const SliceRec* slices, const DevLayer& L, 
 }
 void launch_pyr_tail(uint8_t* axns, const SliceRec* slices, const DevLayer& L, int ctrl, bool learn,
                      const AreaCtl* ctl, cudaStream_t s) {
-    k_pyr_tail<<<nblk((uint64_t)L.v_size * L.u_size, 128), 128, 0, s>>>(axns, slices, L, ctrl, learn ? 1 : 0, ctl);
+    k_pyr_tail<<<nblk(tail_items(L.depth, L.v_size * L.u_size), 128), 128, 0, s>>>(axns, slices, L, ctrl,
+                                                                                   learn ? 1 : 0, ctl);
 }
 void launch_tft_dst_mtp_plain(const uint8_t* axns, const DevLayer& L, uint32_t t, const AreaCtl* ctl,
                               cudaStream_t s) {
