@@ -188,6 +188,7 @@ struct bm_batch_s {
     struct StepPlan {
         Step st;
         std::vector<bm_area> areas;
+        std::vector<std::pair<bm_area, uint32_t>> tufts;   // tuft steps: the (area, tuft) jobs
         Form form = F_EACH;
         std::vector<CellLaunch> cells;   // F_CELLS: launches in order
         FusedBatch fb;
@@ -323,11 +324,11 @@ int add_cells(bm_batch_s::StepPlan& p, int k) {
 
 int build_fused(bm_batch_s::StepPlan& p) {
     std::vector<FusedJob> jobs;
-    for (bm_area A : p.areas) {
-        if (!A->fused.t[p.st.layer][p.st.idx].ok) return BM_OK;
-        jobs.push_back({&A->fused, &A->dl[p.st.layer], A->axns(), A->slices, A->ctl});
+    for (auto& [A, t] : p.tufts) {
+        if (!A->fused.t[p.st.layer][t].ok) return BM_OK;
+        jobs.push_back({&A->fused, &A->dl[p.st.layer], A->axns(), A->slices, A->ctl, p.st.layer, t});
     }
-    int rc = prepare_fused_batch(p.fb, jobs, p.st.layer, p.st.idx);
+    int rc = prepare_fused_batch(p.fb, jobs);
     if (rc != BM_OK) return rc;
     p.form = p.fb.ok ? bm_batch_s::F_FUSED : bm_batch_s::F_EACH;
     return BM_OK;
@@ -341,9 +342,11 @@ int build_step(bm_batch_s::StepPlan& p) {
     }
     if (is_cell_step(st.kind)) return add_cells(p, st.kind);
     if (st.kind != ST_TUFT) return BM_OK;   // the plain form's whole-layer tuft stages: each area's own
+    p.tufts.clear();
+    for (bm_area A : p.areas) p.tufts.push_back({A, st.idx});
     bool none_ok = true, all_ok = true;
-    for (bm_area A : p.areas) {
-        const bool ok = A->fused.t[st.layer][st.idx].ok;
+    for (auto& [A, t] : p.tufts) {
+        const bool ok = A->fused.t[st.layer][t].ok;
         none_ok = none_ok && !ok;
         all_ok = all_ok && ok;
     }
@@ -353,18 +356,18 @@ int build_step(bm_batch_s::StepPlan& p) {
         // to fill the device (the autotuner refines this).
         uint64_t total = 0;
         int sms = 148;
-        for (bm_area A : p.areas) {
+        for (auto& [A, t] : p.tufts) {
             const bm_layer_plan& L = A->plan.layers[st.layer];
-            total += (uint64_t)L.cells * L.tufts[st.idx].syns_per_tft;
+            total += (uint64_t)L.cells * L.tufts[t].syns_per_tft;
             sms = A->fused.sms;
         }
         const uint32_t target = (uint32_t)std::min<uint64_t>(32768, std::max<uint64_t>(4096, total / ((uint64_t)sms * 16)));
-        for (bm_area A : p.areas) {
-            FusedTuft& FT = A->fused.t[st.layer][st.idx];
+        for (auto& [A, t] : p.tufts) {
+            FusedTuft& FT = A->fused.t[st.layer][t];
             // An autotuned choice stays; an area another batch also holds
             // keeps its tiles (that batch's launches are planned on them).
             if (!FT.tiled || FT.tile_tuned || FT.tile_target == target || A->n_batches > 1) continue;
-            if (retile_fused_tuft(A->fused, A->plan, st.layer, st.idx, target)) A->verify_pending[st.layer] = true;
+            if (retile_fused_tuft(A->fused, A->plan, st.layer, t, target)) A->verify_pending[st.layer] = true;
         }
         return build_fused(p);
     }
@@ -372,6 +375,28 @@ int build_step(bm_batch_s::StepPlan& p) {
     // No area can take the fused kernel here (e.g. one-synapse dendrites):
     // the tuft's four stages per cell, batched.
     return add_cells(p, BK_TUFT_CELLS);
+}
+
+// Consecutive batched tuft steps of one layer touch disjoint buffers: one
+// launch serves all their (area, tuft) jobs.
+int merge_tuft_steps(bm_batch_s* B) {
+    std::vector<bm_batch_s::StepPlan> out;
+    for (auto& p : B->plan) {
+        if (!out.empty() && p.form == bm_batch_s::F_FUSED && out.back().form == bm_batch_s::F_FUSED &&
+            p.st.kind == ST_TUFT && out.back().st.kind == ST_TUFT && p.st.layer == out.back().st.layer) {
+            auto& q = out.back();
+            q.tufts.insert(q.tufts.end(), p.tufts.begin(), p.tufts.end());
+            for (bm_area A : p.areas)
+                if (std::find(q.areas.begin(), q.areas.end(), A) == q.areas.end()) q.areas.push_back(A);
+            free_fused_batch(p.fb);
+            int rc = build_fused(q);
+            if (rc != BM_OK) return rc;
+            continue;
+        }
+        out.push_back(p);
+    }
+    B->plan.swap(out);
+    return BM_OK;
 }
 
 void count_launches(bm_batch_s* B) {
@@ -450,6 +475,8 @@ int build_plan(bm_batch_s* B) {
         B->plan.push_back(p);
         if (rc != BM_OK) return rc;
     }
+    int rc = merge_tuft_steps(B);
+    if (rc != BM_OK) return rc;
     count_launches(B);
     return BM_OK;
 }
@@ -593,13 +620,12 @@ void step_ranges(bm_area_s* A, uint32_t i, uint32_t t, std::vector<Range>& out) 
 }
 
 std::string step_key(const bm_batch_s::StepPlan& p) {
-    const Step& st = p.st;
-    std::string k = "L" + std::to_string(st.layer) + "T" + std::to_string(st.idx);
-    for (bm_area A : p.areas) {
-        const bm_layer_plan& L = A->plan.layers[st.layer];
-        const bm_tuft_plan& T = L.tufts[st.idx];
+    std::string k = "L" + std::to_string(p.st.layer);
+    for (auto& [A, t] : p.tufts) {
+        const bm_layer_plan& L = A->plan.layers[p.st.layer];
+        const bm_tuft_plan& T = L.tufts[t];
         char buf[96];
-        snprintf(buf, sizeof buf, ":%ux%ux%u/%u/%u/%u", L.v_size, L.u_size, L.depth, T.syns_per_tft,
+        snprintf(buf, sizeof buf, ":T%u:%ux%ux%u/%u/%u/%u", t, L.v_size, L.u_size, L.depth, T.syns_per_tft,
                  T.syns_per_den, T.n_src_uniq);
         k += buf;
     }
@@ -629,11 +655,11 @@ void write_cache(const char* path, const std::map<std::string, uint32_t>& m) {
 // Retiles tuft (i, t) of every area for `target` synapses per tile and
 // rebuilds the step's batched launch. False when some area cannot take it.
 bool apply_target(bm_batch_s* B, bm_batch_s::StepPlan& p, uint32_t target) {
-    for (bm_area A : p.areas)
+    for (auto& [A, t] : p.tufts)
         if (A->n_batches > 1) return false;   // another batch's launches are planned on these tiles
-    for (bm_area A : p.areas) {
-        if (!retile_fused_tuft(A->fused, A->plan, p.st.layer, p.st.idx, target)) return false;
-        A->fused.t[p.st.layer][p.st.idx].tile_tuned = true;
+    for (auto& [A, t] : p.tufts) {
+        if (!retile_fused_tuft(A->fused, A->plan, p.st.layer, t, target)) return false;
+        A->fused.t[p.st.layer][t].tile_tuned = true;
     }
     for (bm_area A : p.areas) {
         A->verify_pending[p.st.layer] = true;
@@ -825,7 +851,7 @@ int bm_batch_autotune(bm_batch batch, const char* cache_path, uint32_t* n_tuned)
         }
         // Save what the trials overwrite.
         std::vector<Range> ranges;
-        for (bm_area A : p.areas) step_ranges(A, p.st.layer, p.st.idx, ranges);
+        for (auto& [A, t] : p.tufts) step_ranges(A, p.st.layer, t, ranges);
         uint64_t total = 0;
         for (auto& r : ranges) total += r.n;
         uint8_t* save = nullptr;

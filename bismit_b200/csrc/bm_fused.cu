@@ -1149,14 +1149,14 @@ void launch_fused_tuft(const FusedArea& F, const uint8_t* axns, const SliceRec* 
 }
 
 // ---------------------------------------------------------- batched form --
-int prepare_fused_batch(FusedBatch& B, const std::vector<FusedJob>& jobs, uint32_t layer, uint32_t t) {
+int prepare_fused_batch(FusedBatch& B, const std::vector<FusedJob>& jobs) {
     free_fused_batch(B);
     B = FusedBatch{};
     if (jobs.empty()) return BM_OK;
     const bool tuft = jobs[0].L->kind == BM_LYR_PYRAMIDAL;
     uint32_t sms = 148;
     for (const FusedJob& J : jobs) {
-        const FusedTuft& FT = J.F->t[layer][t];
+        const FusedTuft& FT = J.F->t[J.layer][J.t];
         if (!FT.ok || !FT.tiled || !FT.gidx || (J.L->kind == BM_LYR_PYRAMIDAL) != tuft) return BM_OK;
         sms = (uint32_t)J.F->sms;
     }
@@ -1166,7 +1166,7 @@ int prepare_fused_batch(FusedBatch& B, const std::vector<FusedJob>& jobs, uint32
     // and jobs with smaller stages then keep three CTAs per SM).
     std::vector<uint32_t> strides;
     for (const FusedJob& J : jobs) {
-        const uint32_t st = J.F->t[layer][t].stage_stride;
+        const uint32_t st = J.F->t[J.layer][J.t].stage_stride;
         if (std::find(strides.begin(), strides.end(), st) == strides.end()) strides.push_back(st);
     }
     std::sort(strides.begin(), strides.end());
@@ -1174,7 +1174,7 @@ int prepare_fused_batch(FusedBatch& B, const std::vector<FusedJob>& jobs, uint32
         std::vector<const FusedJob*> cls;
         uint32_t halo = 0;
         for (const FusedJob& J : jobs) {
-            const FusedTuft& FT = J.F->t[layer][t];
+            const FusedTuft& FT = J.F->t[J.layer][J.t];
             if (FT.stage_stride != stride) continue;
             cls.push_back(&J);
             halo = std::max(halo, ((FT.nrec * FT.fsz + 15) / 16) * 16);
@@ -1202,7 +1202,7 @@ int prepare_fused_batch(FusedBatch& B, const std::vector<FusedJob>& jobs, uint32
             uint32_t total = 0;
             for (size_t j = 0; j < n; j++) {
                 const FusedJob& J = *cls[j0 + j];
-                make_args(P->jobs[j], *J.F, J.axns, J.slices, *J.L, layer, t, J.ctl);
+                make_args(P->jobs[j], *J.F, J.axns, J.slices, *J.L, J.layer, J.t, J.ctl);
                 P->jobs[j].nst = nst;
                 P->jobs[j].stage_stride = stride;
                 P->jobs[j].halo_off = (uint32_t)halo_off;

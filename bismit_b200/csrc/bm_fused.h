@@ -60,13 +60,14 @@ void launch_verify_tufts(const FusedArea& F, const DevLayer& L, uint32_t layer, 
 void launch_compile_tuft(const FusedArea& F, const DevLayer& L, uint32_t layer, uint32_t t, AreaCtl* ctl,
                          cudaStream_t s);
 
-// Batched form: one launch for tuft t of layer `layer` of several areas.
+// Batched form: launches over several tufts (of one area or several).
 struct FusedJob {
     const FusedArea* F;
     const DevLayer* L;
     const uint8_t* axns;
     const SliceRec* slices;
     AreaCtl* ctl;
+    uint32_t layer, t;   // the tuft: data layer index and tuft index
 };
 struct FusedBatch {
     bool ok = false;             // every job is tiled and the ring fits: batched launches serve them all
@@ -78,7 +79,7 @@ struct FusedBatch {
 };
 // Plans the launches (B.ok false when some job cannot share them; the caller
 // then launches each job's own form).
-int prepare_fused_batch(FusedBatch& B, const std::vector<FusedJob>& jobs, uint32_t layer, uint32_t t);
+int prepare_fused_batch(FusedBatch& B, const std::vector<FusedJob>& jobs);
 void launch_fused_batch(const FusedBatch& B, cudaStream_t s);
 void free_fused_batch(FusedBatch& B);
 
