@@ -53,7 +53,7 @@ BUF_NAMES = [
     "syn_flag_sets", "den_states_raw", "den_states", "den_energies", "den_activities", "den_thresholds",
     "tft_prev_best_den_ids", "tft_prev_best_den_states_raw", "tft_prev_best_den_states", "tft_prev_states",
     "tft_best_den_ids", "tft_best_den_states_raw", "tft_best_den_states", "tft_states",
-    "cel_energies", "cel_activities", "cel_states", "cel_flag_sets",
+    "cel_energies", "cel_activities", "cel_states", "cel_flag_sets", "den_src_key0",
 ]
 BM_BUF_COUNT = len(BUF_NAMES)
 BUF = {n: i for i, n in enumerate(BUF_NAMES)}

@@ -161,7 +161,9 @@ void fuse_steps(const bm_area_s* A, std::vector<Step>& v) {
 }  // namespace
 
 // CorticalArea::cycle, src/cortex/cortical_area.rs:716-789 (intake happens
-// before the cycle; regrowth is rejected at build; output is read on demand).
+// before the cycle; output is read on demand), with CorticalArea::regrow
+// (src/cortex/cortical_area.rs:792-806) as a step of every cycle that acts on
+// the cycles its counter fires.
 void bm::area_steps(const bm_area_s* A, std::vector<Step>& out) {
     const bm_area_plan& P = A->plan;
     out.clear();
@@ -175,6 +177,7 @@ void bm::area_steps(const bm_area_s* A, std::vector<Step>& out) {
         for (uint32_t k = 0; k < P.n_cycle_order; k++)
             if (!(P.layers[P.cycle_order[k]].tags & BM_TAG_SPATIAL)) push_layer_cycle(A, P.cycle_order[k], out);
     }
+    if (A->regrow_blocks) out.push_back({ST_REGROW, 0, 0, 0});
     out.push_back({ST_CYCLE_END, 0, 0, 0});
     if (A->exec_path == BM_PATH_FUSED) fuse_steps(A, out);
 }
@@ -235,16 +238,41 @@ void bm::exec_step(bm_area_s* A, const Step& st, cudaStream_t s) {
     case ST_PYR_CYCLE: run(K_PYR_CYCLE, [&] { launch_pyr_cycle_plain(D, s); }); break;
     case ST_DST_MTP: run(K_TFT_DST_MTP, [&] { launch_tft_dst_mtp_plain(A->axns(), D, x, A->ctl, s); }); break;
     case ST_SSC_MTP: run(K_SSC_MTP, [&] { launch_ssc_mtp_plain(A->axns(), D, A->ctl, s); }); break;
+    case ST_REGROW:
+        run(K_REGROW, [&] { launch_regrow(A->d_regrow, (uint32_t)A->regrow.size(), A->regrow_blocks, s); });
+        break;
     case ST_CYCLE_END: run(K_CYCLE_END, [&] { launch_cycle_end(A->ctl, s); }); break;
     default: break;
     }
 }
 
 void bm::run_pending_verifies(bm_area_s* A, cudaStream_t s) {
+    bool any = false;
     for (uint32_t i = 0; i < A->plan.n_layers; i++)
         if (A->verify_pending[i]) {
             launch_verify_tufts(A->fused, A->dl[i], i, A->ctl, s);
             A->verify_pending[i] = false;
+            any = true;
+        }
+    // Regrowth keeps the compiled gather offsets current: it needs each
+    // tuft's footprint geometry as last planned (retiling changes it).
+    if (any && A->d_geo) {
+        refresh_geo(A);
+        cudaMemcpyAsync(A->d_geo, A->geo, sizeof A->geo, cudaMemcpyHostToDevice, s);
+    }
+}
+
+void bm::refresh_geo(bm_area_s* A) {
+    for (uint32_t i = 0; i < A->plan.n_layers; i++)
+        for (uint32_t t = 0; t < A->plan.layers[i].n_tufts; t++) {
+            const FusedTuft& FT = A->fused.t[i][t];
+            TuftGeo& G = A->geo[i][t];
+            const bool tiled = A->exec_path == BM_PATH_FUSED && FT.ok && FT.tiled && FT.gidx;
+            G.gidx = tiled ? FT.gidx : nullptr;
+            G.slc0 = FT.slc0;
+            G.fsz = FT.fsz;
+            G.fw = FT.fw;
+            G.tiled = tiled;
         }
 }
 
@@ -334,6 +362,49 @@ void build_dev_layers(bm_area_s* A) {
     }
 }
 
+// Regrowth jobs of A: every tuft of every data layer, layers in cycle order
+// (CorticalArea::regrow, src/cortex/cortical_area.rs:792-806), each tuft's
+// stream keyed by its growth key.
+int prepare_regrow(bm_area_s* A, const std::vector<TuftGrowSpec>& grow, const std::vector<GrowTuft>& gts) {
+    const bm_area_plan& P = A->plan;
+    cudaError_t e = cudaMalloc(&A->d_geo, sizeof A->geo);
+    if (e != cudaSuccess) return cuda_err(e, "regrowth geometry");
+    refresh_geo(A);
+    e = cudaMemcpy(A->d_geo, A->geo, sizeof A->geo, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return cuda_err(e, "regrowth geometry");
+    uint64_t blocks = 0;
+    for (uint32_t k = 0; k < P.n_cycle_order; k++) {
+        const uint32_t i = P.cycle_order[k];
+        for (size_t g = 0; g < grow.size(); g++) {
+            if (grow[g].data_layer != i) continue;
+            const uint32_t t = grow[g].tft;
+            const uint64_t n = (uint64_t)P.layers[i].cells * P.layers[i].tufts[t].dens_per_tft;
+            if (!n) continue;
+            if (n > 0xFFFFFFFFull) return set_err(BM_ERR_UNSUPPORTED, "regrowth of more than 2^32 dendrites in a tuft");
+            RegrowJob J;
+            std::memset(&J, 0, sizeof J);
+            J.L = A->dl[i];
+            J.G = gts[g];
+            J.ctl = A->ctl;
+            J.geo = A->d_geo + i * BM_MAX_TUFTS + t;
+            J.rkey = regrow_key(grow[g].key);
+            J.saturated = grow[g].saturated;
+            J.n = (uint32_t)n;
+            J.block0 = (uint32_t)blocks;
+            blocks += (n + kRegrowBlock - 1) / kRegrowBlock;
+            A->regrow.push_back(J);
+        }
+    }
+    if (blocks > 0x7FFFFFFFull) return set_err(BM_ERR_UNSUPPORTED, "regrowth launch of too many blocks");
+    if (A->regrow.empty()) return BM_OK;
+    e = cudaMalloc(&A->d_regrow, A->regrow.size() * sizeof(RegrowJob));
+    if (e == cudaSuccess)
+        e = cudaMemcpy(A->d_regrow, A->regrow.data(), A->regrow.size() * sizeof(RegrowJob), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return cuda_err(e, "regrowth jobs");
+    A->regrow_blocks = (uint32_t)blocks;
+    return BM_OK;
+}
+
 void free_area(bm_area_s* A) {
     if (!A) return;
     if (A->ctx) {
@@ -342,6 +413,9 @@ void free_area(bm_area_s* A) {
         if (A->ctl) cudaFree(A->ctl);
         if (A->slices) cudaFree(A->slices);
         free_fused(A->fused);
+        if (A->d_regrow) cudaFree(A->d_regrow);
+        if (A->grow_offs) cudaFree(A->grow_offs);
+        if (A->d_geo) cudaFree(A->d_geo);
         for (auto& r : A->pending) { cudaEventDestroy(r.a); cudaEventDestroy(r.b); }
         for (auto e : A->pool) cudaEventDestroy(e);
     }
@@ -455,6 +529,7 @@ int bm_area_create(bm_ctx ctx, const bm_area_desc* desc, uint64_t seed, bm_area*
         if (e != cudaSuccess) { if (d_off) cudaFree(d_off); free_area(A); return cuda_err(e, "growth pools"); }
     }
     uint32_t base = 0;
+    std::vector<GrowTuft> gts;
     for (auto& G : grow) {
         GrowTuft GT;
         std::memset(&GT, 0, sizeof GT);
@@ -476,15 +551,22 @@ int bm_area_create(bm_ctx ctx, const bm_area_desc* desc, uint64_t seed, bm_area*
         GT.unique = !(desc->init_flags & BM_INIT_NO_UNIQUE) && !G.saturated;
         GT.zero_strength = (desc->init_flags & BM_INIT_STRENGTH_ZERO) != 0;
         launch_grow(A->dl[G.data_layer], GT, s);
+        gts.push_back(GT);
     }
     e = cudaGetLastError();
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-    if (d_off) cudaFree(d_off);
+    const bool regrow = !(A->plan.settings & BM_SET_DISABLE_REGROWTH);
+    if (regrow) A->grow_offs = d_off;   // kept: regrowth draws from the same pools
+    else if (d_off) cudaFree(d_off);
     if (e != cudaSuccess) { free_area(A); return cuda_err(e, "synapse growth"); }
     rc = prepare_fused(A->fused, A->plan, &err);
+    if (rc != BM_OK) { free_area(A); return set_err(rc, "%s", err.c_str()); }
+    if (regrow) {
+        rc = prepare_regrow(A, grow, gts);
+        if (rc != BM_OK) { free_area(A); return rc; }
+    }
     for (uint32_t i = 0; i < A->plan.n_layers; i++) A->verify_pending[i] = true;
     area_steps(A, A->steps);
-    if (rc != BM_OK) { free_area(A); return set_err(rc, "%s", err.c_str()); }
     *out = A;
     return BM_OK;
 }

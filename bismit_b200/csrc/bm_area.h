@@ -13,12 +13,12 @@ namespace bm {
 enum Kind {
     K_SYN_FLAGS, K_SYN_CYCLE, K_DEN_CYCLE, K_TFT_CYCLE, K_SSC_CYCLE, K_INHIB_SIMPLE, K_INHIB_PASS,
     K_SSC_MTP, K_PYR_CYCLE, K_PYR_OUTPUT, K_INTRA_COL, K_TFT_DST_MTP, K_CYCLE_END, K_INTAKE,
-    K_FUSED_TUFT, K_TUFT_CELLS, K_INHIB_MTP, K_PYR_TAIL, K_COUNT
+    K_FUSED_TUFT, K_TUFT_CELLS, K_INHIB_MTP, K_PYR_TAIL, K_REGROW, K_COUNT
 };
 const char* const kKindNames[K_COUNT] = {
     "tft_set_syn_flags", "syn_cycle", "den_cycle_tft", "tft_cycle", "ssc_cycle", "inhib_simple",
     "inhib_passthrough", "ssc_mtp_simple", "pyr_cycle", "pyr_output", "inhib_intra_column", "tft_dst_mtp",
-    "cycle_end", "intake", "fused_tuft_cycle", "tuft_cells", "inhib_mtp", "pyr_tail"};
+    "cycle_end", "intake", "fused_tuft_cycle", "tuft_cells", "inhib_mtp", "pyr_tail", "regrow"};
 
 struct DevGuard {
     int prev = -1;
@@ -51,6 +51,7 @@ enum StepKind : uint8_t {
     ST_INHIB_MTP,     // ST_INHIB_SIMPLE `idx` followed by ST_SSC_MTP (arg 1) of the same layer
     ST_PYR_TAIL,      // ST_PYR_CYCLE, control `idx` (intra-column or output; 0xFF none), and
                       // (arg 1) ST_DST_MTP of every distal tuft, in that order
+    ST_REGROW,        // regrowth of every tuft of every data layer (acts on its cycles only)
 };
 struct Step {
     uint8_t kind, layer, idx, arg;
@@ -91,6 +92,14 @@ struct bm_area_s {
     uint32_t launches = 0;   // kernel launches of the last enqueued cycle
     std::vector<Step> steps; // the cycle's stage program
     uint32_t n_batches = 0;  // batches holding this area (its tiles are retiled only when one does)
+    // Regrowth (absent when disabled): one job per (data layer, tuft), layers
+    // in cycle order, block0 counted within the area's own launch.
+    std::vector<bm::RegrowJob> regrow;
+    bm::RegrowJob* d_regrow = nullptr;
+    uint32_t regrow_blocks = 0;
+    int8_t* grow_offs = nullptr;             // the growth offset pools (v then u)
+    bm::TuftGeo* d_geo = nullptr;            // per (layer, tuft): layer * BM_MAX_TUFTS + tuft
+    bm::TuftGeo geo[BM_MAX_LAYERS][BM_MAX_TUFTS] = {};
 
     cudaStream_t stream() const { return ctx->stream(); }
     uint8_t* axns() const { return slab + plan.axon_off; }
@@ -133,6 +142,8 @@ void area_steps(const bm_area_s* A, std::vector<Step>& out);
 void exec_step(bm_area_s* A, const Step& st, cudaStream_t s);
 // Recompiles the gather offsets of layers whose sources or flags were written.
 void run_pending_verifies(bm_area_s* A, cudaStream_t s);
+// Rebuilds A->geo (the tiled tufts' footprint geometry that regrowth uses).
+void refresh_geo(bm_area_s* A);
 int cuda_err(cudaError_t e, const char* what);
 
 }  // namespace bm

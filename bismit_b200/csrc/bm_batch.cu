@@ -178,7 +178,7 @@ bool is_cell_step(int st) {
 }  // namespace
 
 struct bm_batch_s {
-    enum Form { F_CELLS, F_FUSED, F_EACH, F_END };
+    enum Form { F_CELLS, F_FUSED, F_EACH, F_END, F_REGROW };
     struct CellLaunch {
         int kind;
         CellJob* d_jobs;
@@ -192,6 +192,8 @@ struct bm_batch_s {
         Form form = F_EACH;
         std::vector<CellLaunch> cells;   // F_CELLS: launches in order
         FusedBatch fb;
+        RegrowJob* d_regrow = nullptr;   // F_REGROW: every area's regrowth jobs, one launch
+        uint32_t n_regrow = 0, regrow_blocks = 0;
         // Profiling (eager cycles only): launches and device milliseconds.
         uint64_t prof_n = 0;
         double prof_ms = 0;
@@ -251,6 +253,7 @@ namespace {
 void free_plan(bm_batch_s* B) {
     for (auto& p : B->plan) {
         for (auto& c : p.cells) cudaFree(c.d_jobs);
+        if (p.d_regrow) cudaFree(p.d_regrow);
         free_fused_batch(p.fb);
     }
     B->plan.clear();
@@ -334,12 +337,37 @@ int build_fused(bm_batch_s::StepPlan& p) {
     return BM_OK;
 }
 
+// Every area's regrowth jobs in one table (block0 rebased), one launch.
+int build_regrow(bm_batch_s::StepPlan& p) {
+    std::vector<RegrowJob> jobs;
+    uint64_t blocks = 0;
+    for (bm_area A : p.areas)
+        for (RegrowJob J : A->regrow) {
+            J.block0 = (uint32_t)blocks;
+            blocks += (J.n + kRegrowBlock - 1) / kRegrowBlock;
+            jobs.push_back(J);
+        }
+    if (blocks > 0x7FFFFFFFull) return set_err(BM_ERR_UNSUPPORTED, "batched regrowth of too many blocks");
+    if (jobs.empty()) {
+        p.form = bm_batch_s::F_END;
+        return BM_OK;
+    }
+    cudaError_t e = cudaMalloc(&p.d_regrow, jobs.size() * sizeof(RegrowJob));
+    if (e == cudaSuccess) e = cudaMemcpy(p.d_regrow, jobs.data(), jobs.size() * sizeof(RegrowJob), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return cuda_err(e, "batched regrowth jobs");
+    p.n_regrow = (uint32_t)jobs.size();
+    p.regrow_blocks = (uint32_t)blocks;
+    p.form = bm_batch_s::F_REGROW;
+    return BM_OK;
+}
+
 int build_step(bm_batch_s::StepPlan& p) {
     const Step& st = p.st;
     if (st.kind == ST_CYCLE_END) {
         p.form = bm_batch_s::F_END;
         return BM_OK;
     }
+    if (st.kind == ST_REGROW) return build_regrow(p);
     if (is_cell_step(st.kind)) return add_cells(p, st.kind);
     if (st.kind != ST_TUFT) return BM_OK;   // the plain form's whole-layer tuft stages: each area's own
     p.tufts.clear();
@@ -415,6 +443,8 @@ void count_launches(bm_batch_s* B) {
             n += (uint32_t)p.cells.size();
         } else if (p.form == bm_batch_s::F_FUSED) {
             n += (uint32_t)p.fb.params.size();
+        } else if (p.form == bm_batch_s::F_REGROW) {
+            n += 1;
         }
     }
     B->plan_launches = n;
@@ -545,6 +575,7 @@ void enqueue_batch_cycle(bm_batch_s* B, cudaStream_t s) {
             for (auto& c : p.cells) launch_cells(c.kind, c.d_jobs, c.n_jobs, c.n_blocks, s);
             break;
         case bm_batch_s::F_FUSED: launch_fused_batch(p.fb, s); break;
+        case bm_batch_s::F_REGROW: launch_regrow(p.d_regrow, p.n_regrow, p.regrow_blocks, s); break;
         case bm_batch_s::F_END: break;
         default:
             for (bm_area A : p.areas) exec_step(A, p.st, s);

@@ -5,7 +5,8 @@
 // uniqueness rule of SynSrcIdxCache::insert (src/map/syn_src.rs:186-203). The
 // entropy-seeded SmallRng is replaced by a seeded per-dendrite counter stream,
 // so one thread grows one dendrite and the result does not depend on launch
-// order. The same rule is restated in the oracle (bmo_grow).
+// order. The same rule is restated in the oracle (bmo_grow). Regrowth
+// (k_regrow) draws from the same pools with a per-round stream.
 #include "bm_kernels.h"
 
 namespace bm {
@@ -20,6 +21,30 @@ __device__ __forceinline__ uint32_t uniform_idx(uint32_t r, uint32_t n) {
 }
 
 constexpr int kGrowMaxAttempts = 1024;
+
+// One candidate source from two words of a dendrite's stream
+// (SynSrcSlices::gen_src, src/map/syn_src.rs:448-490): a uniform pick of the
+// tuft's source slices, then of that slice's offset pool (or of its whole
+// grid for a nonspatial slice), and a strength of intensity x U[-3, 3] where
+// intensity is the scaled reach left over by the offset, >> 3.
+__device__ __forceinline__ void draw_src(const GrowTuft& G, uint64_t w, uint64_t w2, uint8_t& ns, int& nv, int& nu,
+                                         int& nstr) {
+    const uint32_t pi = uniform_idx((uint32_t)w, G.n_pool);
+    ns = G.pool[pi];
+    const uint32_t k = G.pool_src[pi];
+    if (G.nonspatial[k]) {
+        nv = (int)uniform_idx((uint32_t)(w >> 32), (uint32_t)(2 * G.rv[k] + 1)) - G.rv[k];
+        nu = (int)uniform_idx((uint32_t)w2, (uint32_t)(2 * G.ru[k] + 1)) - G.ru[k];
+        nstr = 0;
+    } else {
+        const uint32_t oi = uniform_idx((uint32_t)(w >> 32), G.n_offs[k]);
+        nv = G.offs_v[G.offs_base[k] + oi];
+        nu = G.offs_u[G.offs_base[k] + oi];
+        const int inten = ((G.rv[k] - abs(nv)) + (G.ru[k] - abs(nu))) >> 3;
+        const int r = (int)uniform_idx((uint32_t)w2, 7u) - 3;
+        nstr = (int)(int8_t)(uint8_t)(inten * r);
+    }
+}
 
 __global__ void k_grow(DevLayer L, GrowTuft G) {
     uint64_t d = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -37,23 +62,9 @@ __global__ void k_grow(DevLayer L, GrowTuft G) {
         uint8_t ns = 0;
         int nv = 0, nu = 0, nstr = 0;
         for (int att = 0; att < kGrowMaxAttempts; att++) {
-            uint64_t w = grow_word(G.key, d, wk++);
-            uint64_t w2 = grow_word(G.key, d, wk++);
-            uint32_t pi = uniform_idx((uint32_t)w, G.n_pool);
-            ns = G.pool[pi];
-            uint32_t k = G.pool_src[pi];
-            if (G.nonspatial[k]) {
-                nv = (int)uniform_idx((uint32_t)(w >> 32), (uint32_t)(2 * G.rv[k] + 1)) - G.rv[k];
-                nu = (int)uniform_idx((uint32_t)w2, (uint32_t)(2 * G.ru[k] + 1)) - G.ru[k];
-                nstr = 0;
-            } else {
-                uint32_t oi = uniform_idx((uint32_t)(w >> 32), G.n_offs[k]);
-                nv = G.offs_v[G.offs_base[k] + oi];
-                nu = G.offs_u[G.offs_base[k] + oi];
-                int inten = ((G.rv[k] - abs(nv)) + (G.ru[k] - abs(nu))) >> 3;
-                int r = (int)uniform_idx((uint32_t)w2, 7u) - 3;
-                nstr = (int)(int8_t)(uint8_t)(inten * r);
-            }
+            const uint64_t w = grow_word(G.key, d, wk++);
+            const uint64_t w2 = grow_word(G.key, d, wk++);
+            draw_src(G, w, w2, ns, nv, nu, nstr);
             if (!G.unique) break;
             int64_t nk = (int64_t)ns * cols + (int64_t)nv * L.u_size + nu;
             if (nk == 0) break;  // key 0 is never retained (old-source removal at init)
@@ -73,6 +84,86 @@ __global__ void k_grow(DevLayer L, GrowTuft G) {
 
 __global__ void k_cycle_end(AreaCtl* ctl) { ctl->cycle += 1; }
 
+// Synapses::regrow (src/cortex/synapses.rs:411-501) with SynSrcIdxCache
+// (src/map/syn_src.rs:159-211), one dendrite per thread, on the cycles c with
+// c % kRegrowPeriod == kRegrowPeriod - 1 (other cycles return at once). Each
+// synapse at or below the strength floor draws sources, in synapse order,
+// until the dendrite's source set lacks the new key (slice * columns + v_ofs
+// * u_size + u_ofs), or at once for a saturated pool. The set is every
+// non-zero key of the dendrite's sources plus key 0 when den_src_key0 says so:
+// bismit's cache inserts the new key and, if that was new, drops the old one,
+// so an accepted key 0 enters unless the old key was 0, which always leaves.
+// Draws stop after kGrowMaxAttempts, keeping the last. A tiled tuft's
+// compiled gather offset follows each moved synapse. The same rule is
+// restated in the oracle.
+__global__ void __launch_bounds__(kRegrowBlock) k_regrow(const RegrowJob* __restrict__ jobs, uint32_t n_jobs) {
+    __shared__ uint32_t s_j;
+    if (threadIdx.x == 0) {
+        uint32_t lo = 0, hi = n_jobs;
+        while (hi - lo > 1) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (jobs[mid].block0 <= blockIdx.x) lo = mid;
+            else hi = mid;
+        }
+        s_j = lo;
+    }
+    __syncthreads();
+    const RegrowJob& J = jobs[s_j];
+    const uint64_t cyc = J.ctl->cycle;
+    if (cyc % kRegrowPeriod != kRegrowPeriod - 1) return;
+    const uint32_t d = (blockIdx.x - J.block0) * kRegrowBlock + threadIdx.x;
+    if (d >= J.n) return;
+    const DevLayer& L = J.L;
+    const DevTuft& T = L.tft[J.G.tft];
+    uint8_t* slc = L.buf[BM_BUF_SYN_SRC_SLC_IDS];
+    int8_t* vo = (int8_t*)L.buf[BM_BUF_SYN_SRC_COL_V_OFFS];
+    int8_t* uo = (int8_t*)L.buf[BM_BUF_SYN_SRC_COL_U_OFFS];
+    int8_t* str = (int8_t*)L.buf[BM_BUF_SYN_STRENGTHS];
+    uint8_t* z = L.buf[BM_BUF_DEN_SRC_KEY0] + T.den_idz + d;
+    const TuftGeo geo = *J.geo;
+    const uint64_t rk = splitmix64(J.rkey + cyc / kRegrowPeriod);
+    const int64_t cols = (int64_t)L.v_size * L.u_size;
+    const uint64_t s0 = T.syn_idz + (uint64_t)d * T.spd;
+    uint64_t wk = 0;
+    for (uint32_t j = 0; j < T.spd; j++) {
+        if (str[s0 + j] > kStrengthFloor) continue;
+        const int64_t ko = (int64_t)slc[s0 + j] * cols + (int64_t)vo[s0 + j] * L.u_size + uo[s0 + j];
+        uint8_t ns = 0;
+        int nv = 0, nu = 0, nstr = 0;
+        int64_t nk = 0;
+        for (int att = 0; att < kGrowMaxAttempts; att++) {
+            const uint64_t w = grow_word(rk, d, wk++);
+            const uint64_t w2 = grow_word(rk, d, wk++);
+            draw_src(J.G, w, w2, ns, nv, nu, nstr);
+            nk = (int64_t)ns * cols + (int64_t)nv * L.u_size + nu;
+            if (J.saturated) break;
+            bool held;
+            if (nk == 0) {
+                held = *z != 0;
+            } else {
+                held = false;
+                for (uint32_t jj = 0; jj < T.spd; jj++) {
+                    const int64_t ok = (int64_t)slc[s0 + jj] * cols + (int64_t)vo[s0 + jj] * L.u_size + uo[s0 + jj];
+                    if (ok == nk) { held = true; break; }
+                }
+            }
+            if (!held) break;
+        }
+        if (!J.saturated) {
+            if (ko == 0) *z = 0;
+            else if (nk == 0) *z = 1;
+        }
+        slc[s0 + j] = ns;
+        vo[s0 + j] = (int8_t)nv;
+        uo[s0 + j] = (int8_t)nu;
+        str[s0 + j] = (int8_t)nstr;
+        // A tiled tuft's sources all come from the pools its footprint covers.
+        if (geo.tiled)
+            geo.gidx[s0 + j - T.syn_idz] =
+                (int16_t)((int32_t)(ns - geo.slc0) * (int32_t)geo.fsz + nv * (int32_t)geo.fw + nu);
+    }
+}
+
 }  // namespace
 
 void launch_grow(const DevLayer& L, const GrowTuft& G, cudaStream_t s) {
@@ -81,5 +172,11 @@ void launch_grow(const DevLayer& L, const GrowTuft& G, cudaStream_t s) {
 }
 
 void launch_cycle_end(AreaCtl* ctl, cudaStream_t s) { k_cycle_end<<<1, 1, 0, s>>>(ctl); }
+
+uint64_t regrow_key(uint64_t gkey) { return splitmix64(gkey ^ 0x7265677277ull); }
+
+void launch_regrow(const RegrowJob* jobs, uint32_t n_jobs, uint32_t n_blocks, cudaStream_t s) {
+    if (n_blocks) k_regrow<<<n_blocks, kRegrowBlock, 0, s>>>(jobs, n_jobs);
+}
 
 }  // namespace bm

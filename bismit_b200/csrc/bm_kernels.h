@@ -28,6 +28,35 @@ void fill_dev_layer(DevLayer& D, const bm_area_plan& P, uint32_t i, uint8_t* sla
 void fill_slice_table(const bm_area_plan& P, SliceRec* out);
 
 void launch_grow(const DevLayer& L, const GrowTuft& G, cudaStream_t s);
+
+// Regrowth (bm_grow.cu) acts on the cycles c with c % kRegrowPeriod ==
+// kRegrowPeriod - 1: bismit's counter (src/cortex/cortical_area.rs:792-806)
+// counts up from 0 and fires, resetting, once it has reached
+// SYNAPSE_REGROWTH_INTERVAL (200, src/cmn/mod.rs:234).
+constexpr uint32_t kRegrowPeriod = 201;
+constexpr int kStrengthFloor = -25;   // SYNAPSE_STRENGTH_FLOOR, src/cmn/mod.rs:233
+constexpr uint32_t kRegrowBlock = 128;
+
+// Gather-offset geometry of a tiled tuft (regrowth recompiles the offsets of
+// the synapses it moves); kept current in device memory across retiling.
+struct TuftGeo {
+    int16_t* gidx;           // null: the tuft is not tiled
+    uint32_t slc0, fsz, fw, tiled;
+};
+
+// Regrowth of one tuft of one area: one thread per dendrite.
+struct RegrowJob {
+    DevLayer L;
+    GrowTuft G;              // the tuft's pools (offset arrays kept by the area)
+    const AreaCtl* ctl;
+    const TuftGeo* geo;
+    uint64_t rkey;           // stream key; round r = c / kRegrowPeriod draws from splitmix64(rkey + r)
+    uint32_t saturated;      // the pool is saturated: the first draw is kept
+    uint32_t n;              // dendrites
+    uint32_t block0;         // first block of this job in its launch
+};
+uint64_t regrow_key(uint64_t grow_key);
+void launch_regrow(const RegrowJob* jobs, uint32_t n_jobs, uint32_t n_blocks, cudaStream_t s);
 void launch_cycle_end(AreaCtl* ctl, cudaStream_t s);
 
 // Plain form: one kernel per reference stage (bm_plain.cu).

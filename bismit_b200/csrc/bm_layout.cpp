@@ -39,9 +39,6 @@ void fail(const char* fmt, ...) {
     throw Fail{buf, BM_ERR_INVALID};
 }
 
-// A scheme feature outside this path (a valid scheme this library does not run).
-[[noreturn]] void unsupported(const char* msg) { throw Fail{msg, BM_ERR_UNSUPPORTED}; }
-
 // calc_scale, src/cmn/slice_dims.rs:201-224.
 uint32_t calc_scale(uint32_t src_dim, uint32_t tar_dim) {
     uint64_t src = (uint64_t)src_dim * 1024, tar = (uint64_t)tar_dim * 1024;
@@ -141,9 +138,6 @@ int resolve_area(const bm_area_desc* D, uint64_t seed, bm_area_plan* P, std::vec
         if (D->n_layers == 0 || D->n_layers > BM_MAX_LAYERS) fail("n_layers must be 1..%d", BM_MAX_LAYERS);
         if (D->v_size == 0 || D->u_size == 0 || D->v_size > 4096 || D->u_size > 4096)
             fail("area dims must be 1..4096 (got %u x %u)", D->v_size, D->u_size);
-        if (!(D->settings & BM_SET_DISABLE_REGROWTH))
-            unsupported("synapse regrowth (CorticalAreaSettings without disable_regrowth) is not on this path: "
-                        "set BM_SET_DISABLE_REGROWTH");
         P->area_id = D->area_id;
         P->v_size = D->v_size;
         P->u_size = D->u_size;
@@ -428,6 +422,7 @@ int resolve_area(const bm_area_desc* D, uint64_t seed, bm_area_plan* P, std::vec
             }
             put(BM_BUF_CEL_ENERGIES, L.cells);
             put(BM_BUF_CEL_ACTIVITIES, L.cells);
+            if (!(P->settings & BM_SET_DISABLE_REGROWTH)) put(BM_BUF_DEN_SRC_KEY0, L.n_dens);
             P->n_syns_total += L.n_syns;
         }
         P->slab_bytes = off;

@@ -199,7 +199,10 @@ typedef struct bm_area_desc {
 #define BM_BUF_CEL_ACTIVITIES           20
 #define BM_BUF_CEL_STATES               21   /* pyramidal soma                     */
 #define BM_BUF_CEL_FLAG_SETS            22   /* pyramidal cell flags               */
-#define BM_BUF_COUNT                    23
+#define BM_BUF_DEN_SRC_KEY0             23   /* per dendrite, regrowth on only: key 0
+                                                 held in the dendrite's source set
+                                                 (SynSrcIdxCache, src/map/syn_src.rs:159-211) */
+#define BM_BUF_COUNT                    24
 #define BM_BUF_AXON_STATES              64   /* area axon space (layer ignored)    */
 
 typedef struct bm_tuft_plan {

@@ -29,6 +29,8 @@
 #define DEN_BASAL_PROXIMAL_FLAG         0x01
 #define DEN_BASAL_DISTAL_FLAG           0x02
 #define DEN_APICAL_DISTAL_FLAG          0x04
+#define BMO_REGROW_PERIOD               201    /* SYNAPSE_REGROWTH_INTERVAL (200, src/cmn/mod.rs:234) + the resetting cycle */
+#define BMO_STRENGTH_FLOOR              (-25)  /* SYNAPSE_STRENGTH_FLOOR, src/cmn/mod.rs:233 */
 
 /* ------------------------------------------------------------ helpers ---- */
 static inline int32_t shl32(int32_t x, int n) { return (int32_t)((uint32_t)x << n); }
@@ -541,8 +543,10 @@ static void layer_cycle(const bm_area_plan* P, uint8_t* axns, lview* V, uint64_t
     else pyr_layer_cycle(P, axns, V, cyc);
 }
 
-/* CorticalArea::cycle, src/cortex/cortical_area.rs:716-789 (regrowth and the
- * samplers excluded). */
+static void regrow_layer(const bm_area_plan* P, lview* V, uint64_t cyc);
+
+/* CorticalArea::cycle, src/cortex/cortical_area.rs:716-789 (the samplers
+ * excluded), regrowth included. */
 static void area_cycle(const bm_area_plan* P, uint8_t* slab, uint64_t cyc) {
     uint8_t* axns = slab + P->axon_off;
     lview V[BM_MAX_LAYERS];
@@ -563,6 +567,11 @@ static void area_cycle(const bm_area_plan* P, uint8_t* slab, uint64_t cyc) {
             if (!(v->L->tags & BM_TAG_SPATIAL)) layer_cycle(P, axns, v, cyc);
         }
     }
+    /* CorticalArea::regrow (src/cortex/cortical_area.rs:792-806): every data
+     * layer in cycle order, on the cycles the regrowth counter fires (it
+     * counts up from 0 and fires, resetting, once it has reached 200). */
+    if (!(P->settings & BM_SET_DISABLE_REGROWTH) && cyc % BMO_REGROW_PERIOD == BMO_REGROW_PERIOD - 1)
+        for (uint32_t k = 0; k < P->n_cycle_order; k++) regrow_layer(P, &V[P->cycle_order[k]], cyc);
 }
 
 int bmo_run(const bm_area_plan* P, uint8_t* slab, const uint8_t* frames, uint64_t frame_len,
@@ -620,6 +629,81 @@ static inline uint32_t uniform_idx(uint32_t r, uint32_t n) {
 
 #define GROW_MAX_ATTEMPTS 1024
 
+/* The source pools of one tuft: SynSrcSlices / SynSrcSliceInfo
+ * (src/map/syn_src.rs:241-310,327-437). */
+typedef struct {
+    int8_t* ov[BM_MAX_SRC_SLICES];
+    int8_t* ou[BM_MAX_SRC_SLICES];
+    int on[BM_MAX_SRC_SLICES];
+    int nonspatial[BM_MAX_SRC_SLICES];
+    int rv[BM_MAX_SRC_SLICES], ru[BM_MAX_SRC_SLICES];
+    int saturated;   /* every possible source is needed by each dendrite */
+} tuft_pools;
+
+static void free_pools(tuft_pools* Q) {
+    for (int k = 0; k < BM_MAX_SRC_SLICES; k++) { free(Q->ov[k]); free(Q->ou[k]); }
+}
+
+static int make_pools(const bm_area_plan* P, const bm_tuft_plan* T, tuft_pools* Q) {
+    enum { OFS_CAP = 3 * 127 * 128 + 1 };
+    memset(Q, 0, sizeof *Q);
+    uint64_t poss = 0;
+    for (uint32_t k = 0; k < T->n_src_uniq; k++) {
+        uint8_t s = T->src_uniq_slc_ids[k];
+        int reach = T->src_uniq_reaches[k];
+        Q->nonspatial[k] = P->slc_v_scale[s] == 0;
+        if (Q->nonspatial[k]) {
+            Q->rv[k] = (int)(P->slc_v_size[s] / 2);
+            Q->ru[k] = (int)(P->slc_u_size[s] / 2);
+            poss = (uint64_t)P->slc_v_size[s] * P->slc_u_size[s] * T->n_src;
+        } else {
+            Q->ov[k] = (int8_t*)malloc(OFS_CAP);
+            Q->ou[k] = (int8_t*)malloc(OFS_CAP);
+            Q->on[k] = bmo_gen_syn_offs(reach, P->slc_v_scale[s], P->slc_u_scale[s], Q->ov[k], Q->ou[k], OFS_CAP);
+            if (Q->on[k] <= 0) { free_pools(Q); return -1; }
+            Q->rv[k] = (reach * (int)P->slc_v_scale[s]) >> SLC_SCL_COEFF_L2;
+            Q->ru[k] = (reach * (int)P->slc_u_scale[s]) >> SLC_SCL_COEFF_L2;
+            poss = (uint64_t)Q->on[k] * T->n_src;
+        }
+    }
+    Q->saturated = poss == T->syns_per_den;
+    return 0;
+}
+
+/* One candidate source from two words of the dendrite's stream:
+ * SynSrcSlices::gen_src (src/map/syn_src.rs:448-490) with its strength rule
+ * (intensity = scaled reach minus offset, >> INTENSITY_REDUCTION_L2, times
+ * U[-3, 3]; 0 for nonspatial slices). */
+static void draw_src(const tuft_pools* Q, const bm_tuft_plan* T, uint64_t w, uint64_t w2, uint8_t* ns, int* nv,
+                     int* nu, int* nstr) {
+    uint32_t pi = uniform_idx((uint32_t)w, T->n_src);
+    *ns = T->src_slc_ids[pi];
+    uint32_t k = 0;
+    while (k < T->n_src_uniq && T->src_uniq_slc_ids[k] != *ns) k++;
+    if (Q->nonspatial[k]) {
+        *nv = (int)uniform_idx((uint32_t)(w >> 32), (uint32_t)(2 * Q->rv[k] + 1)) - Q->rv[k];
+        *nu = (int)uniform_idx((uint32_t)w2, (uint32_t)(2 * Q->ru[k] + 1)) - Q->ru[k];
+        *nstr = 0;
+    } else {
+        uint32_t oi = uniform_idx((uint32_t)(w >> 32), (uint32_t)Q->on[k]);
+        *nv = Q->ov[k][oi];
+        *nu = Q->ou[k][oi];
+        int inten = ((Q->rv[k] - iabs(*nv)) + (Q->ru[k] - iabs(*nu))) >> 3;
+        int r = (int)uniform_idx((uint32_t)w2, 7u) - 3;
+        *nstr = (int8_t)(uint8_t)(inten * r);
+    }
+}
+
+/* Key of the growth stream of (area, layer, tuft). */
+static inline uint64_t grow_key_of(uint64_t seed, uint32_t area, uint32_t layer, uint32_t t) {
+    uint64_t key = splitmix64(seed ^ 0x67726F77ull) + (((uint64_t)area << 48) | ((uint64_t)layer << 40) | ((uint64_t)t << 32));
+    return splitmix64(key);
+}
+
+/* Synapses::grow(true) (src/cortex/synapses.rs:448-501, regrow_syn :411-446):
+ * every synapse draws sources from its tuft's pools; unless the pool is
+ * saturated (or BM_INIT_NO_UNIQUE), a draw repeating an earlier synapse's
+ * non-zero key in the same dendrite is redrawn. */
 int bmo_grow(const bm_area_plan* P, uint8_t* slab, uint64_t seed, uint32_t init_flags) {
     for (uint32_t l = 0; l < P->n_layers; l++) {
         const bm_layer_plan* L = &P->layers[l];
@@ -631,40 +715,10 @@ int bmo_grow(const bm_area_plan* P, uint8_t* slab, uint64_t seed, uint32_t init_
         int8_t* str = (int8_t*)V.b[BM_BUF_SYN_STRENGTHS];
         for (uint32_t t = 0; t < L->n_tufts; t++) {
             const bm_tuft_plan* T = &L->tufts[t];
-            /* Offset pools per distinct source slice (SynSrcSliceInfo::new,
-             * src/map/syn_src.rs:241-310). */
-            enum { OFS_CAP = 3 * 127 * 128 + 1 };
-            int8_t* ov[BM_MAX_SRC_SLICES];
-            int8_t* ou[BM_MAX_SRC_SLICES];
-            int on[BM_MAX_SRC_SLICES];
-            int nonspatial[BM_MAX_SRC_SLICES];
-            int rv[BM_MAX_SRC_SLICES], ru[BM_MAX_SRC_SLICES];
-            uint64_t poss = 0;
-            for (uint32_t k = 0; k < T->n_src_uniq; k++) {
-                uint8_t s = T->src_uniq_slc_ids[k];
-                int reach = T->src_uniq_reaches[k];
-                nonspatial[k] = P->slc_v_scale[s] == 0;
-                ov[k] = ou[k] = NULL;
-                if (nonspatial[k]) {
-                    rv[k] = (int)(P->slc_v_size[s] / 2);
-                    ru[k] = (int)(P->slc_u_size[s] / 2);
-                    on[k] = 0;
-                    poss = (uint64_t)P->slc_v_size[s] * P->slc_u_size[s] * T->n_src;
-                } else {
-                    ov[k] = (int8_t*)malloc(OFS_CAP);
-                    ou[k] = (int8_t*)malloc(OFS_CAP);
-                    on[k] = bmo_gen_syn_offs(reach, P->slc_v_scale[s], P->slc_u_scale[s], ov[k], ou[k], OFS_CAP);
-                    if (on[k] <= 0) return -1;
-                    rv[k] = (reach * (int)P->slc_v_scale[s]) >> SLC_SCL_COEFF_L2;
-                    ru[k] = (reach * (int)P->slc_u_scale[s]) >> SLC_SCL_COEFF_L2;
-                    poss = (uint64_t)on[k] * T->n_src;
-                }
-            }
-            int saturated = poss == T->syns_per_den;
-            int unique = !(init_flags & BM_INIT_NO_UNIQUE) && !saturated;
-            uint64_t key = splitmix64(seed ^ 0x67726F77ull) + (((uint64_t)P->area_id << 48) |
-                           ((uint64_t)L->layer_id << 40) | ((uint64_t)t << 32));
-            key = splitmix64(key);
+            tuft_pools Q;
+            if (make_pools(P, T, &Q)) return -1;
+            int unique = !(init_flags & BM_INIT_NO_UNIQUE) && !Q.saturated;
+            uint64_t key = grow_key_of(seed, P->area_id, L->layer_id, t);
             int64_t n_dens = (int64_t)L->cells * T->dens_per_tft;
             int64_t cols = (int64_t)L->v_size * L->u_size;
 #pragma omp parallel for schedule(static)
@@ -676,21 +730,7 @@ int bmo_grow(const bm_area_plan* P, uint8_t* slab, uint64_t seed, uint32_t init_
                     for (int att = 0; att < GROW_MAX_ATTEMPTS; att++) {
                         uint64_t w = grow_word(key, d, wk++);
                         uint64_t w2 = grow_word(key, d, wk++);
-                        uint32_t pi = uniform_idx((uint32_t)w, T->n_src);
-                        ns = T->src_slc_ids[pi];
-                        uint32_t k = 0;
-                        while (k < T->n_src_uniq && T->src_uniq_slc_ids[k] != ns) k++;
-                        if (nonspatial[k]) {
-                            nv = (int)uniform_idx((uint32_t)(w >> 32), (uint32_t)(2 * rv[k] + 1)) - rv[k];
-                            nu = (int)uniform_idx((uint32_t)w2, (uint32_t)(2 * ru[k] + 1)) - ru[k];
-                            nstr = 0;
-                        } else {
-                            uint32_t oi = uniform_idx((uint32_t)(w >> 32), (uint32_t)on[k]);
-                            nv = ov[k][oi]; nu = ou[k][oi];
-                            int inten = ((rv[k] - iabs(nv)) + (ru[k] - iabs(nu))) >> 3;
-                            int r = (int)uniform_idx((uint32_t)w2, 7u) - 3;
-                            nstr = (int8_t)(uint8_t)(inten * r);
-                        }
+                        draw_src(&Q, T, w, w2, &ns, &nv, &nu, &nstr);
                         if (!unique) break;
                         int64_t nk = (int64_t)ns * cols + (int64_t)nv * L->u_size + nu;
                         if (nk == 0) break;
@@ -707,8 +747,80 @@ int bmo_grow(const bm_area_plan* P, uint8_t* slab, uint64_t seed, uint32_t init_
                     str[s0 + j] = (init_flags & BM_INIT_STRENGTH_ZERO) ? 0 : (int8_t)nstr;
                 }
             }
-            for (uint32_t k = 0; k < T->n_src_uniq; k++) { free(ov[k]); free(ou[k]); }
+            free_pools(&Q);
         }
     }
     return 0;
+}
+
+/* Synapses::regrow (src/cortex/synapses.rs:411-501) with SynSrcIdxCache
+ * (src/map/syn_src.rs:159-211): every synapse whose strength is at or below
+ * SYNAPSE_STRENGTH_FLOOR draws sources until one is accepted, in synapse
+ * order within each dendrite. A source is accepted when the dendrite's source
+ * set lacks its key (slice * columns + v_ofs * u_size + u_ofs), or at once
+ * when the tuft's pool is saturated. The set holds every non-zero key of the
+ * dendrite's current sources, plus key 0 when the dendrite's den_src_key0
+ * flag says so. bismit's cache inserts the new key and, when that insert is
+ * new, removes the old key: so an accepted key 0 enters the set unless the
+ * synapse's old key was 0, and an old key 0 always leaves it. Growth leaves
+ * every flag at 0 (the old key of every synapse is then 0). The draws come
+ * from a per-(round, dendrite) stream; draws stop after GROW_MAX_ATTEMPTS,
+ * keeping the last one (bismit draws until one is accepted). Sources,
+ * offsets and strengths change; synapse flags do not. */
+static void regrow_layer(const bm_area_plan* P, lview* V, uint64_t cyc) {
+    const bm_layer_plan* L = V->L;
+    uint8_t* slc = V->b[BM_BUF_SYN_SRC_SLC_IDS];
+    int8_t* vo = (int8_t*)V->b[BM_BUF_SYN_SRC_COL_V_OFFS];
+    int8_t* uo = (int8_t*)V->b[BM_BUF_SYN_SRC_COL_U_OFFS];
+    int8_t* str = (int8_t*)V->b[BM_BUF_SYN_STRENGTHS];
+    uint8_t* key0 = V->b[BM_BUF_DEN_SRC_KEY0];
+    const uint64_t round = cyc / BMO_REGROW_PERIOD;
+    for (uint32_t t = 0; t < L->n_tufts; t++) {
+        const bm_tuft_plan* T = &L->tufts[t];
+        tuft_pools Q;
+        if (make_pools(P, T, &Q)) return;
+        const uint64_t rkey =
+            splitmix64(splitmix64(grow_key_of(P->rnd_seed, P->area_id, L->layer_id, t) ^ 0x7265677277ull) + round);
+        const int64_t n_dens = (int64_t)L->cells * T->dens_per_tft;
+        const int64_t cols = (int64_t)L->v_size * L->u_size;
+#pragma omp parallel for schedule(static)
+        for (int64_t d = 0; d < n_dens; d++) {
+            const uint64_t s0 = T->syn_idz + d * T->syns_per_den;
+            uint8_t* z = key0 + T->den_idz + d;
+            uint64_t wk = 0;
+            for (uint32_t j = 0; j < T->syns_per_den; j++) {
+                if (str[s0 + j] > BMO_STRENGTH_FLOOR) continue;
+                const int64_t ko = (int64_t)slc[s0 + j] * cols + (int64_t)vo[s0 + j] * L->u_size + uo[s0 + j];
+                uint8_t ns = 0; int nv = 0, nu = 0, nstr = 0;
+                int64_t nk = 0;
+                for (int att = 0; att < GROW_MAX_ATTEMPTS; att++) {
+                    uint64_t w = grow_word(rkey, d, wk++);
+                    uint64_t w2 = grow_word(rkey, d, wk++);
+                    draw_src(&Q, T, w, w2, &ns, &nv, &nu, &nstr);
+                    nk = (int64_t)ns * cols + (int64_t)nv * L->u_size + nu;
+                    if (Q.saturated) break;
+                    int held;
+                    if (nk == 0) {
+                        held = *z != 0;
+                    } else {
+                        held = 0;
+                        for (uint32_t jj = 0; jj < T->syns_per_den; jj++) {
+                            int64_t ok = (int64_t)slc[s0 + jj] * cols + (int64_t)vo[s0 + jj] * L->u_size + uo[s0 + jj];
+                            if (ok == nk) { held = 1; break; }
+                        }
+                    }
+                    if (!held) break;
+                }
+                if (!Q.saturated) {
+                    if (ko == 0) *z = 0;
+                    else if (nk == 0) *z = 1;
+                }
+                slc[s0 + j] = ns;
+                vo[s0 + j] = (int8_t)nv;
+                uo[s0 + j] = (int8_t)nu;
+                str[s0 + j] = (int8_t)nstr;
+            }
+        }
+        free_pools(&Q);
+    }
 }

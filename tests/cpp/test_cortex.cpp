@@ -184,14 +184,17 @@ int cmd_desc(const std::string& dir) {
         benchmark_area(lm, ar, 64, 32, 1, 1, 1, 0);
         area_desc("v9", lm, ar, settings());
     });
-    ok &= raises(BM_ERR_UNSUPPORTED, [] {
+    {
+        // Regrowth on (the settings' default): the plan carries one
+        // den_src_key0 byte per dendrite in every data layer.
         LayerMapSchemeList lm;
         AreaSchemeList ar;
         benchmark_area(lm, ar, 64, 32, 1, 1, 1, 0);
-        bm_area_desc d = area_desc("v1", lm, ar, CorticalAreaSettings());   // regrowth on
+        bm_area_desc d = area_desc("v1", lm, ar, CorticalAreaSettings());
         bm_area_plan p;
         check(bm_plan_resolve(&d, 0, &p));
-    });
+        for (uint32_t l = 0; l < p.n_layers; l++) ok &= p.layers[l].buf_len[BM_BUF_DEN_SRC_KEY0] == p.layers[l].n_dens;
+    }
     std::cout << (ok ? "errors ok" : "errors WRONG") << std::endl;
     return ok ? 0 : 1;
 }

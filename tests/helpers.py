@@ -16,7 +16,11 @@ SCHEMES = {
 
 
 def settings_for(kind="default", plain=False):
-    s = M.CorticalAreaSettings().disable_regrowth()
+    """Regrowth is off except for kind "regrowth" (the reference's parity runs
+    set disable_regrowth)."""
+    s = M.CorticalAreaSettings()
+    if kind != "regrowth":
+        s.disable_regrowth()
     if kind == "bypass_inhib":
         s.bypass_inhib()
     elif kind == "no_learning":
@@ -51,6 +55,11 @@ def buffers(plan):
             if L.buf_off[k] != NO_BUF:
                 out.append(("L%d.%s" % (l, n), int(L.buf_off[k]), int(L.buf_len[k])))
     return out
+
+
+def named(plan, slab):
+    """{label: bytes} of every buffer of the slab."""
+    return {name: slab[off:off + n] for name, off, n in buffers(plan)}
 
 
 def diff_report(plan, a, b, limit=12):

@@ -63,12 +63,24 @@ def test_errors_are_status_codes_with_messages():
     assert lib.bm_server_tick(None, None) == F.BM_ERR_INVALID
 
 
-def test_regrowth_is_rejected():
-    s = configs.bench_settings()
-    s.bits &= ~F.BM_SET_DISABLE_REGROWTH
-    d = M.area_desc("v1", *configs.workload("area_64")[:2], s)
-    p = F.bm_area_plan()
-    assert F.lib().bm_plan_resolve(C.byref(d), 0, C.byref(p)) == F.BM_ERR_UNSUPPORTED
+def test_regrowth_adds_the_key0_buffer():
+    """With regrowth on, every data layer carries one den_src_key0 byte per
+    dendrite (the key-0 membership of the dendrite's source set); with it
+    off, none."""
+    lib = F.lib()
+    on = configs.bench_settings()
+    on.bits &= ~F.BM_SET_DISABLE_REGROWTH
+    for s, present in ((on, True), (configs.bench_settings(), False)):
+        d = M.area_desc("v1", *configs.workload("area_64")[:2], s)
+        p = F.bm_area_plan()
+        assert lib.bm_plan_resolve(C.byref(d), 0, C.byref(p)) == F.BM_OK
+        for l in range(p.n_layers):
+            L = p.layers[l]
+            k = F.BUF["den_src_key0"]
+            if present:
+                assert L.buf_len[k] == L.n_dens
+            else:
+                assert L.buf_off[k] == 2 ** 64 - 1
 
 
 def test_rnd_stream_is_host_computable():

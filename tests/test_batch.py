@@ -9,7 +9,7 @@ import pytest
 
 import oracle
 from bismit_b200 import _ffi as F, configs, cortex, map as M
-from helpers import diff_report, scramble
+from helpers import buffers, diff_report, scramble
 
 # (side, depth, distal dens, distal syns): a small spread of the batched
 # workload's shapes, proximal 1 x 1 tufts included (the unfused sub-stages).
@@ -104,21 +104,43 @@ def test_batch_frames_from_device_match_areas_alone():
     ctx.close()
 
 
+def _regrowth_settings():
+    s = configs.bench_settings()
+    s.bits &= ~F.BM_SET_DISABLE_REGROWTH
+    return s
+
+
 @pytest.mark.gpu
-def test_batch_matches_oracle():
+@pytest.mark.parametrize("regrowth", [False, True], ids=["static", "regrowth"])
+def test_batch_matches_oracle(regrowth):
+    """The graph-replayed batch against the oracle; with regrowth on, over
+    cycles 198 to 201 (the batch's one regrowth launch for every area acts at
+    cycle 200)."""
     ctx = cortex._Ctx(0)
-    batched, alone = _pairs(ctx, [_desc(*s) for s in SMALL[:3]])
+    st = _regrowth_settings() if regrowth else None
+    start = 198 if regrowth else 0
+    batched, alone = _pairs(ctx, [_desc(*s, settings=st) for s in SMALL[:3]])
+    for a in batched:
+        a.set_cycle(start)
     batch = cortex.Batch(ctx, batched)
     ora = [a.read_slab() for a in batched]
+    first = [o.copy() for o in ora]
     fr = [_frames(a, 4, 80 + k) for k, a in enumerate(batched)]
     for c in range(4):
         for k, a in enumerate(batched):
             a.write_input(fr[k][c])
         batch.cycle(1)
         for k, a in enumerate(batched):
-            oracle.run(a.plan, ora[k], fr[k][c:c + 1], 1, start_cycle=c)
+            oracle.run(a.plan, ora[k], fr[k][c:c + 1], 1, start_cycle=start + c)
             dev = a.read_slab()
-            assert np.array_equal(dev, ora[k]), "cycle %d area %d:\n%s" % (c, k, diff_report(a.plan, dev, ora[k]))
+            assert np.array_equal(dev, ora[k]), "cycle %d area %d:\n%s" % (start + c, k, diff_report(a.plan, dev, ora[k]))
+    if regrowth:
+        for k, a in enumerate(batched):
+            moved = 0
+            for name, off, n in buffers(a.plan):
+                if name.endswith("syn_src_col_v_offs"):
+                    moved += int(np.count_nonzero(first[k][off:off + n] != ora[k][off:off + n]))
+            assert moved > 0, k
     batch.close()
     for a in batched + alone:
         a.close()

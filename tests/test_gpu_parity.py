@@ -10,7 +10,7 @@ import pytest
 
 import oracle
 from bismit_b200 import _ffi as F, cortex
-from helpers import desc_of, diff_report, frames_for, initial_slab, settings_for
+from helpers import buffers, desc_of, diff_report, frames_for, initial_slab, settings_for
 
 pytestmark = pytest.mark.gpu
 
@@ -39,23 +39,24 @@ def test_growth_matches_oracle(ctx, scheme, flags):
     area.close()
 
 
-def _run_parity(ctx, scheme, kind, plain, cycles, scramble=True, active=0.05):
+def _run_parity(ctx, scheme, kind, plain, cycles, scramble=True, active=0.05, start=0):
     s = settings_for(kind, plain=plain)
     area = _area(ctx, scheme, s)
     plan = area.plan
     slab = initial_slab(plan, 7, scramble_seed=11 if scramble else None)
     area.write_slab(slab)
-    area.set_cycle(0)
+    area.set_cycle(start)
     fr = frames_for(plan, cycles, 5, active)
     ora = slab.copy()
     for k in range(cycles):
         if fr is not None:
             area.write_input(fr[k])
         area.cycle(1)
-        oracle.run(plan, ora, None if fr is None else fr[k:k + 1], 1, start_cycle=k)
+        oracle.run(plan, ora, None if fr is None else fr[k:k + 1], 1, start_cycle=start + k)
         dev = area.read_slab()
-        assert np.array_equal(dev, ora), "cycle %d:\n%s" % (k, diff_report(plan, dev, ora))
+        assert np.array_equal(dev, ora), "cycle %d:\n%s" % (start + k, diff_report(plan, dev, ora))
     area.close()
+    return plan, slab, ora
 
 
 @pytest.mark.parametrize("plain", [True, False], ids=["plain", "fused"])
@@ -68,6 +69,21 @@ def test_cycles_match_oracle(ctx, scheme, plain):
 @pytest.mark.parametrize("kind", ["bypass_inhib", "no_learning", "no_pyrs", "no_sscs"])
 def test_settings_match_oracle(ctx, kind, plain):
     _run_parity(ctx, "mixed", kind, plain, cycles=3)
+
+
+@pytest.mark.parametrize("plain", [True, False], ids=["plain", "fused"])
+@pytest.mark.parametrize("scheme", ["testbed", "mixed", "area_64", "area_48_deep"])
+def test_regrowth_matches_oracle(ctx, scheme, plain):
+    """Cycles 198 to 201 with regrowth on: cycle 200 redraws every synapse whose
+    strength is at or below the floor (Synapses::regrow,
+    src/cortex/synapses.rs:411-501), the fused path's compiled gather offsets
+    follow, and the cycles after it read the new sources."""
+    plan, before, after = _run_parity(ctx, scheme, "regrowth", plain, cycles=4, start=198)
+    moved = 0
+    for name, off, n in buffers(plan):
+        if name.endswith("syn_src_slc_ids") or name.endswith("syn_src_col_v_offs"):
+            moved += int(np.count_nonzero(before[off:off + n] != after[off:off + n]))
+    assert moved > 0
 
 
 @pytest.mark.parametrize("plain", [True, False], ids=["plain", "fused"])
