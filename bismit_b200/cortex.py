@@ -8,6 +8,7 @@ buffer read/write/fill helpers of the reference's test traits. Every call goes
 through the C ABI of the native library; errors raise BismitError.
 """
 import ctypes as C
+import weakref
 
 import numpy as np
 
@@ -21,6 +22,11 @@ class _Ctx:
         self.h = C.c_void_p()
         F.check(self.lib.bm_ctx_create(int(device), 0, C.byref(self.h)))
         self.device = device
+        self._owned = []   # weak references to the areas, batches and servers made on this context
+
+    def _adopt(self, obj):
+        self._owned = [r for r in self._owned if r() is not None]
+        self._owned.append(weakref.ref(obj))
 
     def set_stream(self, stream_ptr):
         F.check(self.lib.bm_ctx_set_stream(self.h, C.c_void_p(stream_ptr or 0)))
@@ -29,7 +35,17 @@ class _Ctx:
         F.check(self.lib.bm_ctx_synchronize(self.h))
 
     def close(self):
+        """Destroys the context after everything made on it (batches and
+        servers first, then areas): finalizers at interpreter exit run in no
+        set order, and a handle must not outlive what it points into."""
         if self.h:
+            objs = [o for o in (r() for r in self._owned) if o is not None]
+            for o in objs:
+                if not isinstance(o, CorticalArea):
+                    o.close()
+            for o in objs:
+                o.close()
+            self._owned = []
             self.lib.bm_ctx_destroy(self.h)
             self.h = C.c_void_p()
 
@@ -50,6 +66,8 @@ class CorticalArea:
         self.desc = desc
         self.h = C.c_void_p()
         F.check(self.lib.bm_area_create(ctx.h, C.byref(desc), C.c_uint64(seed), C.byref(self.h)))
+        self._holders = []
+        ctx._adopt(self)
         self.plan = F.bm_area_plan()
         F.check(self.lib.bm_area_get_plan(self.h, C.byref(self.plan)))
         self.layer_names = [desc.layers[i].name.decode() for i in range(desc.n_layers)]
@@ -166,6 +184,12 @@ class CorticalArea:
 
     def close(self):
         if self.h:
+            # A batch that holds this area goes first (it points into the area).
+            for r in getattr(self, "_holders", []):
+                b = r()
+                if b is not None:
+                    b.close()
+            self._holders = []
             self.lib.bm_area_destroy(self.h)
             self.h = C.c_void_p()
 
@@ -189,6 +213,9 @@ class Batch:
         hs = (C.c_void_p * len(self.areas))(*[a.h.value for a in self.areas])
         self.h = C.c_void_p()
         F.check(self.lib.bm_batch_create(ctx.h, hs, len(self.areas), C.byref(self.h)))
+        ctx._adopt(self)
+        for a in self.areas:
+            a._holders.append(weakref.ref(self))
         if not graph:
             self.set_graph(False)
 
@@ -278,6 +305,7 @@ class Server:
         self.ctx = ctx
         self.h = C.c_void_p()
         F.check(self.lib.bm_server_create(ctx.h, C.c_uint64(int(budget_bytes)), C.byref(self.h)))
+        ctx._adopt(self)
 
     def open(self, desc, seed):
         sid = C.c_uint32()

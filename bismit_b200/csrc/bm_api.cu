@@ -269,9 +269,7 @@ void bm::refresh_geo(bm_area_s* A) {
             TuftGeo& G = A->geo[i][t];
             const bool tiled = A->exec_path == BM_PATH_FUSED && FT.ok && FT.tiled && FT.gidx;
             G.gidx = tiled ? FT.gidx : nullptr;
-            G.slc0 = FT.slc0;
-            G.fsz = FT.fsz;
-            G.fw = FT.fw;
+            G.g = gather_geo(A->fused, A->plan, i, t);
             G.tiled = tiled;
         }
 }

@@ -40,6 +40,7 @@
 #include "bm_fused.h"
 
 #include <algorithm>
+#include <cstddef>
 #include <cstring>
 #include <new>
 
@@ -66,7 +67,7 @@ struct FusedTuftArgs {
     const int8_t* str;
     uint8_t* st;
     uint8_t* fl;
-    const int16_t* gidx;    // compiled gather offsets (tiled form)
+    const uint16_t* gidx;   // compiled gather offsets (tiled form): bytes into the tile's footprint
     uint8_t* den_act;       // tuft-relative dendrite arrays
     uint8_t* den_raw;
     uint8_t* den_st;
@@ -100,12 +101,17 @@ struct FusedTuftArgs {
     uint32_t src_idz[kMaxRecs];
     uint32_t nst;                       // pipeline stages
     uint32_t stage_bytes;               // bytes per 1-byte array per stage
-    uint32_t halo_off;                  // byte offset of the footprint in dynamic smem
+    uint32_t ring_off;                  // byte offset of the ring (mbarriers, then stages) in dynamic smem;
+                                        // the footprint starts at 0
     uint32_t unit_l2;                   // log2 of the bytes of one unit (chunks_per_unit * 512)
     uint32_t stage_stride;              // bytes per ring buffer (synapse arrays + windows)
     uint32_t win;                       // dendrite / cell-tuft windows ride in the stages
     uint32_t win_bytes;                 // bytes per window
 };
+
+// Lanes of a cell write its eight cell-tuft fields through one pointer table.
+static_assert(offsetof(FusedTuftArgs, t_st) == offsetof(FusedTuftArgs, t_pid) + 7 * sizeof(uint8_t*),
+              "the cell-tuft arrays must be consecutive pointers");
 
 struct Rec {
     int32_t base;     // idz + vsc * u_size + usc
@@ -180,6 +186,16 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
 __device__ __forceinline__ void consumers_sync() { asm volatile("bar.sync 1, %0;" ::"n"(kWarps * 32) : "memory"); }
 
 // ------------------------------------------------------------ helpers ----
+// 0xFF in every byte of x whose sign bit is set (prmt's sign-replicate mode).
+__device__ __forceinline__ uint32_t sign_bytes(uint32_t x) {
+    uint32_t r;
+    asm("prmt.b32 %0, %1, %2, 0xBA98;" : "=r"(r) : "r"(x), "r"(0u));
+    return r;
+}
+// The low bytes of a0..a3 as one word (a0 lowest).
+__device__ __forceinline__ uint32_t pack4(uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3) {
+    return __byte_perm(__byte_perm(a0, a1, 0x0040), __byte_perm(a2, a3, 0x0040), 0x5410);
+}
 __device__ __forceinline__ uint32_t nz_bits(uint32_t x) {
     // 0x80 in every byte of x that is non-zero.
     return (((x & 0x7F7F7F7Fu) + 0x7F7F7F7Fu) | x) & 0x80808080u;
@@ -195,17 +211,20 @@ __device__ __forceinline__ uint8_t gather_general(const FusedTuftArgs& A, uint32
 // Loads issued at the start of a chunk so their latency overlaps the gathers:
 // the activity of the lane's dendrite (dendrite-lead lanes) and, at the first
 // chunk of a cell, the cell-tuft's current best/state bytes that the tuft
-// cycle copies to the prev arrays (cell-lead lanes).
+// cycle copies to the prev arrays. Cells of 8 or more lanes spread that copy
+// over lanes: lane f < 4 of the cell holds field f (best id, best raw, best
+// state, tuft state); smaller cells keep all four, packed, in their first lane.
 __device__ __forceinline__ uint32_t prefetch_act(const FusedTuftArgs& A, uint64_t off, bool on, int lane) {
     const uint32_t lpd = 1u << A.lpd_l2;
     return (on && (lane & (lpd - 1)) == 0) ? (uint32_t)A.den_act[off >> A.spd_l2] : 0u;
 }
 template <bool TUFT>
 __device__ __forceinline__ uint32_t prefetch_tuft(const FusedTuftArgs& A, uint64_t off, bool on, int lane) {
-    if (!TUFT) return 0u;
-    const uint32_t lpc = 1u << A.lpc_l2;
-    if (!on || (lane & (lpc - 1)) != 0) return 0u;
+    if (!TUFT || !on) return 0u;
+    const uint32_t f = lane & ((1u << A.lpc_l2) - 1);
     const uint32_t c = (uint32_t)(off >> A.S_l2);
+    if (A.lpc_l2 >= 3) return f < 4 ? (uint32_t)(&A.t_bid)[f][c] : 0u;
+    if (f != 0) return 0u;
     return (uint32_t)A.t_bid[c] | ((uint32_t)A.t_braw[c] << 8) | ((uint32_t)A.t_bst[c] << 16) |
            ((uint32_t)A.t_st[c] << 24);
 }
@@ -232,9 +251,8 @@ __device__ __forceinline__ void finish_chunk(const FusedTuftArgs& A, const uint4
         for (int w = 0; w < 4; w++) {
             const uint32_t keep = flags_clean ? 0u : (flw[w] & 0xEFEFEFEFu);
             nflw[w] = keep | (nz_bits(stw[w]) >> 3);
-            const uint32_t neg = (strw[w] >> 7) & 0x01010101u;
             raw = __dp4a(nstw[w], 0x01010101u, raw);
-            sum = __dp4a(nstw[w] & ~(neg * 0xFFu), 0x01010101u, sum);
+            sum = __dp4a(nstw[w] & ~sign_bytes(strw[w]), 0x01010101u, sum);
         }
         *(uint4*)(A.st + off) = nst4;
         *(uint4*)(A.fl + off) = nfl4;
@@ -273,24 +291,41 @@ __device__ __forceinline__ void finish_chunk(const FusedTuftArgs& A, const uint4
                 best = max(best, __shfl_xor_sync(0xFFFFFFFFu, best, m));
                 tot += __shfl_xor_sync(0xFFFFFFFFu, tot, m);
             }
+            // The butterfly leaves the cell's totals in its dendrite-lead
+            // lanes only; every lane of the cell writes a field.
+            if (lpd > 1 && lpc >= 8) {
+                const int src = lane & ~(int)(lpd - 1);
+                key = __shfl_sync(0xFFFFFFFFu, key, src);
+                best = __shfl_sync(0xFFFFFFFFu, best, src);
+                tot = __shfl_sync(0xFFFFFFFFu, tot, src);
+            }
         }
         t_key = max(t_key, key);
         t_best = max(t_best, best);
         t_sum += tot;
-        if (last && on && (lane & (lpc - 1)) == 0) {
+        const uint32_t f = lane & (lpc - 1);
+        if (last && on && (lpc >= 8 ? f < 8 : f == 0)) {
             const uint32_t c = off >> A.S_l2;
             const uint32_t best_raw = t_key >> 16;
             const uint32_t best_id = best_raw ? (0xFFFFu - (t_key & 0xFFFFu)) : 0u;
             const bool is_max = t_sum >= (1u << (A.mad_l2 + 8));
-            const uint8_t tst = is_max ? (uint8_t)255 : (uint8_t)(t_sum >> A.mad_l2);
-            A.t_pid[c] = (uint8_t)tuft_cur;
-            A.t_praw[c] = (uint8_t)(tuft_cur >> 8);
-            A.t_pst[c] = (uint8_t)(tuft_cur >> 16);
-            A.t_ptft[c] = (uint8_t)(tuft_cur >> 24);
-            A.t_bid[c] = (uint8_t)best_id;
-            A.t_braw[c] = (uint8_t)best_raw;
-            A.t_bst[c] = (uint8_t)t_best;
-            A.t_st[c] = tst;
+            const uint32_t tst = is_max ? 255u : ((t_sum >> A.mad_l2) & 0xFFu);
+            if (lpc >= 8) {
+                // Lane f writes field f: the prev copies of the current fields
+                // (f < 4), then best id, best raw, best state, tuft state. The
+                // eight arrays are consecutive in the arguments.
+                const uint32_t nv = f == 4 ? best_id : f == 5 ? best_raw : f == 6 ? t_best : tst;
+                (&A.t_pid)[f][c] = (uint8_t)(f < 4 ? tuft_cur : nv);
+            } else {
+                A.t_pid[c] = (uint8_t)tuft_cur;
+                A.t_praw[c] = (uint8_t)(tuft_cur >> 8);
+                A.t_pst[c] = (uint8_t)(tuft_cur >> 16);
+                A.t_ptft[c] = (uint8_t)(tuft_cur >> 24);
+                A.t_bid[c] = (uint8_t)best_id;
+                A.t_braw[c] = (uint8_t)best_raw;
+                A.t_bst[c] = (uint8_t)t_best;
+                A.t_st[c] = (uint8_t)tst;
+            }
         }
     }
 }
@@ -466,14 +501,15 @@ __device__ __forceinline__ void tma_stage(const FusedTuftArgs& A, const TileGeo&
     const uint32_t cpu = A.chunks_per_unit;
     const uint32_t unit = ((pos - G.syn0) >> A.unit_l2) + (uint32_t)wib;
     if (unit >= n_units_tile) return;
-    const uint32_t lim = A.nrec * A.fsz - 1;
     uint32_t t_key = 0, t_best = 0, t_sum = 0, tuft_cur = 0;
     for (uint32_t ch = 0; ch < cpu; ch++) {
         const uint32_t so = ((uint32_t)wib * cpu + ch) * 512 + (uint32_t)lane * 16;   // offset within the stage
         const uint32_t off = pos + so;
         const bool on = off < G.syn_end;
-        uint32_t v, u;
-        const int32_t base = footprint_base(A, G, off, v, u);
+        // The general gather form indexes from the cell's footprint position.
+        uint32_t v = 0, u = 0;
+        int32_t base = 0;
+        if (MODE != 0) base = footprint_base(A, G, off, v, u);
         uint32_t act0;
         if (A.win) {
             // The stage carries the dendrite and cell-tuft bytes (windows start
@@ -482,10 +518,12 @@ __device__ __forceinline__ void tma_stage(const FusedTuftArgs& A, const TileGeo&
             const uint32_t lpd = 1u << A.lpd_l2;
             act0 = (on && (lane & (lpd - 1)) == 0) ? (uint32_t)wd[(off >> A.spd_l2) - ((pos >> A.spd_l2) & ~15u)] : 0u;
             if (TUFT && ch == 0) {
-                const uint32_t lpc = 1u << A.lpc_l2;
+                const uint32_t f = lane & ((1u << A.lpc_l2) - 1);
+                const uint32_t ci = (off >> A.S_l2) - ((pos >> A.S_l2) & ~15u);
                 tuft_cur = 0;
-                if (on && (lane & (lpc - 1)) == 0) {
-                    const uint32_t ci = (off >> A.S_l2) - ((pos >> A.S_l2) & ~15u);
+                if (A.lpc_l2 >= 3) {
+                    if (on && f < 4) tuft_cur = wd[(1 + f) * A.win_bytes + ci];
+                } else if (on && f == 0) {
                     tuft_cur = (uint32_t)wd[A.win_bytes + ci] | ((uint32_t)wd[2 * A.win_bytes + ci] << 8) |
                                ((uint32_t)wd[3 * A.win_bytes + ci] << 16) | ((uint32_t)wd[4 * A.win_bytes + ci] << 24);
                 }
@@ -501,18 +539,17 @@ __device__ __forceinline__ void tma_stage(const FusedTuftArgs& A, const TileGeo&
             if (!FCLEAN) fl4 = *(const uint4*)(sb + arr_off<MODE>(2, SB) + so);
             uint32_t* ow = (uint32_t*)&nst4;
             if (MODE == 0) {
+                // Compiled offsets index the footprint directly (it starts at
+                // shared offset 0); the 15-bit mask keeps even a stray offset
+                // inside the CTA's shared memory.
                 const uint4 g0 = *(const uint4*)(sb + 2 * so);
                 const uint4 g1 = *(const uint4*)(sb + 2 * so + 16);
                 const uint32_t gw[8] = {g0.x, g0.y, g0.z, g0.w, g1.x, g1.y, g1.z, g1.w};
 #pragma unroll
                 for (int w = 0; w < 4; w++) {
                     const uint32_t lo = gw[2 * w], hi = gw[2 * w + 1];
-                    const uint32_t i0 = min((uint32_t)(base + (int32_t)(int16_t)(lo & 0xFFFF)), lim);
-                    const uint32_t i1 = min((uint32_t)(base + ((int32_t)lo >> 16)), lim);
-                    const uint32_t i2 = min((uint32_t)(base + (int32_t)(int16_t)(hi & 0xFFFF)), lim);
-                    const uint32_t i3 = min((uint32_t)(base + ((int32_t)hi >> 16)), lim);
-                    ow[w] = (uint32_t)halo[i0] | ((uint32_t)halo[i1] << 8) | ((uint32_t)halo[i2] << 16) |
-                            ((uint32_t)halo[i3] << 24);
+                    ow[w] = pack4(halo[lo & 0x7FFFu], halo[(lo >> 16) & 0x7FFFu], halo[hi & 0x7FFFu],
+                                  halo[(hi >> 16) & 0x7FFFu]);
                 }
             } else {
                 const uint4 slc4 = *(const uint4*)(sb + so);
@@ -637,10 +674,10 @@ __device__ __forceinline__ void consume_tile(const FusedTuftArgs& A, const TileG
 
 template <bool TUFT, int MODE, bool FCLEAN>
 __device__ __forceinline__ void tma_body(const FusedTuftArgs& A, uint8_t* smem, volatile int& s_abort) {
-    uint64_t* full = (uint64_t*)smem;              // [nst]
-    uint64_t* empty = full + A.nst;                // [nst]
-    uint8_t* stages = smem + 128;
-    uint8_t* halo = smem + A.halo_off;
+    uint64_t* full = (uint64_t*)(smem + A.ring_off);   // [nst]
+    uint64_t* empty = full + A.nst;                    // [nst]
+    uint8_t* stages = smem + A.ring_off + 128;
+    uint8_t* halo = smem;
     const int tid = threadIdx.x;
     const int lane = tid & 31;
     const int wib = tid >> 5;
@@ -666,8 +703,8 @@ __device__ __forceinline__ void tma_body(const FusedTuftArgs& A, uint8_t* smem, 
     }
 }
 
-__device__ __forceinline__ void init_ring(uint8_t* smem, uint32_t nst, volatile int& s_abort) {
-    uint64_t* full = (uint64_t*)smem;
+__device__ __forceinline__ void init_ring(uint8_t* ring, uint32_t nst, volatile int& s_abort) {
+    uint64_t* full = (uint64_t*)ring;
     uint64_t* empty = full + nst;
     if (threadIdx.x == 0) {
         for (uint32_t i = 0; i < nst; i++) {
@@ -691,7 +728,7 @@ template <bool TUFT>
 __global__ void __launch_bounds__(kThreads, 3) k_fused_tuft_tma(FusedTuftArgs A) {
     extern __shared__ __align__(128) uint8_t smem[];
     __shared__ volatile int s_abort;   // a bounded wait gave up
-    init_ring(smem, A.nst, s_abort);
+    init_ring(smem + A.ring_off, A.nst, s_abort);
     // One specialised body per gather mode and flags state (uniform per launch).
     switch (mode_of(A)) {
     case 0: tma_body<TUFT, 0, true>(A, smem, s_abort); break;
@@ -708,13 +745,13 @@ __global__ void __launch_bounds__(kThreads, 3) k_fused_tuft_tma(FusedTuftArgs A)
 // job table is the launch's own parameter block (__grid_constant__): it is
 // read-only there, so the compiler keeps argument fields in registers across
 // the stores of a stage, and nothing needs copying per job. Every job of a
-// launch shares the ring geometry (nst, stage_stride, halo_off).
+// launch shares the ring geometry (nst, stage_stride, ring_off).
 constexpr uint32_t kMaxBatchJobs = 80;   // 80 argument blocks fit the 32 KB parameter limit
 
 struct BatchParams {
     FusedTuftArgs jobs[kMaxBatchJobs];
     uint32_t tile0[kMaxBatchJobs + 1];
-    uint32_t n_jobs, nst, halo_off;
+    uint32_t n_jobs, nst, ring_off;
 };
 static_assert(sizeof(BatchParams) <= 32764, "batched tuft parameter block exceeds the kernel parameter limit");
 
@@ -734,11 +771,11 @@ __global__ void __launch_bounds__(kThreads, 3) k_fused_tuft_batch(const __grid_c
     extern __shared__ __align__(128) uint8_t smem[];
     __shared__ volatile int s_abort;
     const uint32_t nst = P.nst;
-    init_ring(smem, nst, s_abort);
-    uint64_t* full = (uint64_t*)smem;
+    init_ring(smem + P.ring_off, nst, s_abort);
+    uint64_t* full = (uint64_t*)(smem + P.ring_off);
     uint64_t* empty = full + nst;
-    uint8_t* stages = smem + 128;
-    uint8_t* halo = smem + P.halo_off;
+    uint8_t* stages = smem + P.ring_off + 128;
+    uint8_t* halo = smem;
     const uint32_t n_tiles = P.tile0[P.n_jobs];
     const int tid = threadIdx.x;
     const int lane = tid & 31;
@@ -792,15 +829,14 @@ __global__ void __launch_bounds__(kThreads, 3) k_fused_tuft_batch(const __grid_c
 }
 
 // ------------------------------------------------------ source compile ----
-// Writes each synapse's gather offset into the footprint,
-// (slc - slc0) * fsz + v_ofs * fw + u_ofs, and sets kTuftSrcOutsideTile if a
-// source cannot be served from the footprint, kTuftFlagsForeign if a flag
-// byte has bits other than SYN_PREV_ACTIVE. 16 synapses per thread. With
-// gidx == nullptr (untiled tufts) only the flags are checked.
+// Writes each synapse's gather offset into its tile's footprint
+// (gather_offset) and sets kTuftSrcOutsideTile if a source cannot be served
+// from the footprint, kTuftFlagsForeign if a flag byte has bits other than
+// SYN_PREV_ACTIVE. 16 synapses (of one cell) per thread. With gidx == nullptr
+// (untiled tufts) only the flags are checked.
 __global__ void k_compile_tuft(const uint8_t* __restrict__ slc, const int8_t* __restrict__ vo,
-                               const int8_t* __restrict__ uo, const uint8_t* __restrict__ fl, int16_t* gidx,
-                               uint64_t n, uint32_t slc0, uint32_t nrec, int32_t rv, int32_t ru, uint32_t fw,
-                               uint32_t fsz, unsigned int* status) {
+                               const int8_t* __restrict__ uo, const uint8_t* __restrict__ fl, uint16_t* gidx,
+                               uint64_t n, GatherGeo g, unsigned int* status) {
     uint32_t bits = 0;
     for (uint64_t i = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) * 16; i < n;
          i += (uint64_t)gridDim.x * blockDim.x * 16) {
@@ -817,17 +853,16 @@ __global__ void k_compile_tuft(const uint8_t* __restrict__ slc, const int8_t* __
         uint32_t out[8];
 #pragma unroll
         for (int w = 0; w < 4; w++) {
-            int32_t g[4];
+            uint32_t o[4];
 #pragma unroll
             for (int b = 0; b < 4; b++) {
-                const uint32_t k = ((sw[w] >> (8 * b)) & 0xFF) - slc0;
-                const int v = (int)(int8_t)(vw[w] >> (8 * b)), u = (int)(int8_t)(uw[w] >> (8 * b));
-                const bool ok = k < nrec && v >= -rv && v <= rv && u >= -ru && u <= ru;
+                bool ok;
+                o[b] = gather_offset(g, i, (sw[w] >> (8 * b)) & 0xFF, (int)(int8_t)(vw[w] >> (8 * b)),
+                                     (int)(int8_t)(uw[w] >> (8 * b)), ok);
                 if (!ok) bits |= kTuftSrcOutsideTile;
-                g[b] = ok ? (int32_t)(k * fsz) + v * (int32_t)fw + u : 0;
             }
-            out[2 * w] = (uint32_t)(uint16_t)g[0] | ((uint32_t)(uint16_t)g[1] << 16);
-            out[2 * w + 1] = (uint32_t)(uint16_t)g[2] | ((uint32_t)(uint16_t)g[3] << 16);
+            out[2 * w] = o[0] | (o[1] << 16);
+            out[2 * w + 1] = o[2] | (o[3] << 16);
         }
         uint4* dst = (uint4*)(gidx + i);
         dst[0] = make_uint4(out[0], out[1], out[2], out[3]);
@@ -930,9 +965,13 @@ void plan_tuft(FusedTuft& FT, const bm_area_plan& P, uint32_t i, uint32_t t, int
     // at both ends.
     const uint32_t win_bytes = SB / 16 + 32;
     const uint32_t buf_bytes = 6 * SB + 5 * win_bytes;
-    const uint32_t nst = ring_stages(buf_bytes, ((halo + 15) / 16) * 16);
-    const uint64_t halo_off = 128 + (uint64_t)nst * buf_bytes;
-    const uint64_t smem = halo_off + ((halo + 15) / 16) * 16;
+    // The footprint sits at the start of dynamic shared memory (gathers then
+    // address it with a constant base), the ring after it.
+    const uint64_t ring_off = ((halo + 127) / 128) * 128;
+    const uint32_t nst = ring_stages(buf_bytes, ring_off);
+    // Gathers mask offsets to 15 bits: at least 32 KB of shared memory keeps
+    // every masked offset inside the CTA's allocation.
+    const uint64_t smem = std::max<uint64_t>(32768, ring_off + 128 + (uint64_t)nst * buf_bytes);
     if (smem > kMaxSmem) return;
     FT.tiled = true;
     FT.tile_w = W;
@@ -947,7 +986,7 @@ void plan_tuft(FusedTuft& FT, const bm_area_plan& P, uint32_t i, uint32_t t, int
     FT.stage_stride = buf_bytes;
     FT.win_bytes = win_bytes;
     FT.win = (T.den_idz % 16) == 0 && (T.cel_idz % 16) == 0;
-    FT.halo_off = (uint32_t)halo_off;
+    FT.ring_off = (uint32_t)ring_off;
     FT.smem = (uint32_t)smem;
     FT.src_vs = vs;
     FT.src_us = us;
@@ -1026,6 +1065,34 @@ void free_fused(FusedArea& F) {
             }
 }
 
+namespace {
+
+GatherGeo geo_of(const FusedTuft& FT, const DevLayer& L, const DevTuft& T) {
+    GatherGeo g{};
+    g.S_l2 = (uint32_t)ilog2(T.spt);
+    g.cols = L.v_size * L.u_size;
+    g.u_size = L.u_size;
+    g.tile_w = FT.tiled ? FT.tile_w : 1;
+    g.tile_h = FT.tiled ? FT.tile_h : 1;
+    g.vs = FT.src_vs;
+    g.us = FT.src_us;
+    g.rv = FT.rv;
+    g.ru = FT.ru;
+    g.fw = FT.fw;
+    g.fsz = FT.fsz;
+    g.slc0 = FT.slc0;
+    g.nrec = FT.nrec;
+    return g;
+}
+
+}  // namespace
+
+GatherGeo gather_geo(const FusedArea& F, const bm_area_plan& P, uint32_t layer, uint32_t t) {
+    DevLayer D;
+    fill_dev_layer(D, P, layer, nullptr);
+    return geo_of(F.t[layer][t], D, D.tft[t]);
+}
+
 void launch_compile_tuft(const FusedArea& F, const DevLayer& L, uint32_t layer, uint32_t t, AreaCtl* ctl,
                          cudaStream_t s) {
     const FusedTuft& FT = F.t[layer][t];
@@ -1040,7 +1107,7 @@ void launch_compile_tuft(const FusedArea& F, const DevLayer& L, uint32_t layer, 
                                         (const int8_t*)L.buf[BM_BUF_SYN_SRC_COL_V_OFFS] + T.syn_idz,
                                         (const int8_t*)L.buf[BM_BUF_SYN_SRC_COL_U_OFFS] + T.syn_idz,
                                         L.buf[BM_BUF_SYN_FLAG_SETS] + T.syn_idz, FT.tiled ? FT.gidx : nullptr, n,
-                                        FT.slc0, FT.nrec, FT.rv, FT.ru, FT.fw, FT.fsz, status);
+                                        geo_of(FT, L, T), status);
 }
 
 void launch_verify_tufts(const FusedArea& F, const DevLayer& L, uint32_t layer, AreaCtl* ctl, cudaStream_t s) {
@@ -1116,7 +1183,7 @@ void make_args(FusedTuftArgs& A, const FusedArea& F, const uint8_t* axns, const 
         for (uint32_t k = 0; k < FT.nrec; k++) A.src_idz[k] = FT.src_idz[k];
         A.nst = FT.nst;
         A.stage_bytes = FT.stage_bytes;
-        A.halo_off = FT.halo_off;
+        A.ring_off = FT.ring_off;
         A.unit_l2 = 9 + ilog2(A.chunks_per_unit);
         A.stage_stride = FT.stage_stride;
         A.win = FT.win;
@@ -1177,12 +1244,12 @@ int prepare_fused_batch(FusedBatch& B, const std::vector<FusedJob>& jobs) {
             const FusedTuft& FT = J.F->t[J.layer][J.t];
             if (FT.stage_stride != stride) continue;
             cls.push_back(&J);
-            halo = std::max(halo, ((FT.nrec * FT.fsz + 15) / 16) * 16);
+            halo = std::max(halo, ((FT.nrec * FT.fsz + 127) / 128) * 128);
         }
         uint32_t nst = ring_stages(stride, halo);
         while (nst > 2 && 128 + (uint64_t)nst * stride + halo > kMaxSmem) nst--;
-        const uint64_t halo_off = 128 + (uint64_t)nst * stride;
-        const uint64_t smem = halo_off + halo;
+        const uint64_t ring_off = halo;
+        const uint64_t smem = std::max<uint64_t>(32768, ring_off + 128 + (uint64_t)nst * stride);
         if (smem > kMaxSmem) {
             free_fused_batch(B);
             return BM_OK;
@@ -1205,14 +1272,14 @@ int prepare_fused_batch(FusedBatch& B, const std::vector<FusedJob>& jobs) {
                 make_args(P->jobs[j], *J.F, J.axns, J.slices, *J.L, J.layer, J.t, J.ctl);
                 P->jobs[j].nst = nst;
                 P->jobs[j].stage_stride = stride;
-                P->jobs[j].halo_off = (uint32_t)halo_off;
+                P->jobs[j].ring_off = (uint32_t)ring_off;
                 P->tile0[j] = total;
                 total += P->jobs[j].n_tiles;
             }
             P->tile0[n] = total;
             P->n_jobs = (uint32_t)n;
             P->nst = nst;
-            P->halo_off = (uint32_t)halo_off;
+            P->ring_off = (uint32_t)ring_off;
             B.params.push_back(P);
             B.grids.push_back((uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(total, (uint64_t)sms * std::max(per_sm, 1))));
             B.smems.push_back((uint32_t)smem);

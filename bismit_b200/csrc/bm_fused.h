@@ -4,6 +4,7 @@
 #include <vector>
 
 #include "bm_dev.cuh"
+#include "bm_kernels.h"
 #include "bm_layout.h"
 
 namespace bm {
@@ -17,12 +18,12 @@ struct FusedTuft {
     uint32_t tile_w = 0, tile_h = 0;
     int32_t rv = 0, ru = 0;  // footprint margin: the pool's largest |v|, |u| offsets
     uint32_t fw = 0, frows = 0, fsz = 0;   // footprint width, rows, bytes per slice
-    int16_t* gidx = nullptr; // compiled gather offsets, one per synapse of the tuft
+    uint16_t* gidx = nullptr;   // compiled gather offsets, one per synapse of the tuft
     uint32_t smem = 0;       // dynamic shared memory per CTA
     uint32_t grid = 1;       // persistent grid size
     uint32_t nst = 2;        // TMA pipeline stages
     uint32_t stage_bytes = 0;
-    uint32_t halo_off = 0;   // halo offset in dynamic shared memory
+    uint32_t ring_off = 0;   // ring offset in dynamic shared memory (the footprint is at 0)
     uint32_t stage_stride = 0;   // bytes per ring buffer
     uint32_t win_bytes = 0;      // bytes per dendrite / cell-tuft window
     bool win = false;            // windows ride in the stages (16-byte aligned ranges)
@@ -50,6 +51,8 @@ int plan_fused_tuft(FusedArea& F, const bm_area_plan& P, uint32_t layer, uint32_
 // launch). False, and nothing changed, when the tuft would not stay tiled.
 bool retile_fused_tuft(FusedArea& F, const bm_area_plan& P, uint32_t layer, uint32_t t, uint32_t target_syns);
 void free_fused(FusedArea& F);
+// Gather geometry of tiled tuft t of data layer `layer` as planned in F.
+GatherGeo gather_geo(const FusedArea& F, const bm_area_plan& P, uint32_t layer, uint32_t t);
 // Synapse flags + synapse cycle + dendrite cycle (+ tuft cycle for pyramidal
 // layers) of one tuft in one launch.
 void launch_fused_tuft(const FusedArea& F, const uint8_t* axns, const SliceRec* slices, const DevLayer& L,

@@ -157,10 +157,12 @@ __global__ void __launch_bounds__(kRegrowBlock) k_regrow(const RegrowJob* __rest
         vo[s0 + j] = (int8_t)nv;
         uo[s0 + j] = (int8_t)nu;
         str[s0 + j] = (int8_t)nstr;
-        // A tiled tuft's sources all come from the pools its footprint covers.
-        if (geo.tiled)
-            geo.gidx[s0 + j - T.syn_idz] =
-                (int16_t)((int32_t)(ns - geo.slc0) * (int32_t)geo.fsz + nv * (int32_t)geo.fw + nu);
+        // A tiled tuft's pools lie inside its footprint (every draw is held).
+        if (geo.tiled) {
+            bool ok;
+            const uint64_t i = s0 + j - T.syn_idz;
+            geo.gidx[i] = (uint16_t)gather_offset(geo.g, i, ns, nv, nu, ok);
+        }
     }
 }
 

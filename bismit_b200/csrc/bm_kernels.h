@@ -37,11 +37,46 @@ constexpr uint32_t kRegrowPeriod = 201;
 constexpr int kStrengthFloor = -25;   // SYNAPSE_STRENGTH_FLOOR, src/cmn/mod.rs:233
 constexpr uint32_t kRegrowBlock = 128;
 
-// Gather-offset geometry of a tiled tuft (regrowth recompiles the offsets of
-// the synapses it moves); kept current in device memory across retiling.
+// Gather geometry of a tiled tuft. Its cells are cut into tiles of tile_h
+// rows x tile_w columns of one layer slice; a tile's footprint holds, for each
+// of the nrec source slices from slc0 on, the rows and columns its cells'
+// scaled positions reach with offsets up to rv, ru (fw columns, fsz bytes per
+// slice).
+struct GatherGeo {
+    uint32_t S_l2;           // log2 synapses per cell-tuft
+    uint32_t cols, u_size;   // layer columns, row width
+    uint32_t tile_w, tile_h;
+    uint32_t vs, us;         // scale of the source slices (shared by all of them)
+    int32_t rv, ru;
+    uint32_t fw, fsz;
+    uint32_t slc0, nrec;
+};
+
+// The byte that the synapse at tuft offset i with source (slc, v_ofs, u_ofs)
+// gathers, as an offset into its tile's footprint; false (and 0) when the
+// footprint does not hold it. The tile's footprint starts (rv, ru) before its
+// first cell's scaled position, so a cell at (v, u) in the tile with origin
+// (v0, u0) reads row (v*vs >> 4) - (v0*vs >> 4) + rv + v_ofs.
+__host__ __device__ __forceinline__ uint32_t gather_offset(const GatherGeo& g, uint64_t i, uint32_t slc, int vo,
+                                                           int uo, bool& ok) {
+    const uint32_t c = (uint32_t)(i >> g.S_l2);
+    const uint32_t rem = c % g.cols;
+    const uint32_t v = rem / g.u_size, u = rem - (rem / g.u_size) * g.u_size;
+    const uint32_t v0 = v - v % g.tile_h, u0 = u - u % g.tile_w;
+    const int32_t row = (int32_t)((v * g.vs) >> 4) - (int32_t)((v0 * g.vs) >> 4) + g.rv + vo;
+    const int32_t col = (int32_t)((u * g.us) >> 4) - (int32_t)((u0 * g.us) >> 4) + g.ru + uo;
+    const uint32_t k = slc - g.slc0;
+    ok = k < g.nrec && vo >= -g.rv && vo <= g.rv && uo >= -g.ru && uo <= g.ru;
+    return ok ? k * g.fsz + (uint32_t)row * g.fw + (uint32_t)col : 0u;
+}
+
+// Gather geometry of a tiled tuft as regrowth needs it (regrowth recompiles
+// the offsets of the synapses it moves); kept current in device memory across
+// retiling.
 struct TuftGeo {
-    int16_t* gidx;           // null: the tuft is not tiled
-    uint32_t slc0, fsz, fw, tiled;
+    uint16_t* gidx;          // null: the tuft is not tiled
+    GatherGeo g;
+    uint32_t tiled;
 };
 
 // Regrowth of one tuft of one area: one thread per dendrite.

@@ -122,7 +122,7 @@ extern "C" int bm_tuft_cycle_static(const bm_area_plan* plan, uint32_t layer, ui
                        "bm_tuft_cycle_static: tuft %u of layer %u is outside the fused kernel's shapes "
                        "(syns_per_den a power of two in 16..512, dens_per_tft a power of two, 16-byte aligned buffers)",
                        tuft, layer);
-    if (FT.tiled) FT.gidx = (int16_t*)(scratch + kGidxOff);
+    if (FT.tiled) FT.gidx = (uint16_t*)(scratch + kGidxOff);
     DevLayer D;
     fill_dev_layer(D, P, layer, (uint8_t*)slab);
     SliceTable tab;
