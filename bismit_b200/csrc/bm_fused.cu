@@ -107,6 +107,7 @@ struct FusedTuftArgs {
     uint32_t stage_stride;              // bytes per ring buffer (synapse arrays + windows)
     uint32_t win;                       // dendrite / cell-tuft windows ride in the stages
     uint32_t win_bytes;                 // bytes per window
+    uint32_t geom;                      // specialised consumer for this shape (0: the general one)
 };
 
 // Lanes of a cell write its eight cell-tuft fields through one pointer table.
@@ -583,6 +584,141 @@ __device__ __forceinline__ void tma_stage(const FusedTuftArgs& A, const TileGeo&
     }
 }
 
+// ----------------------------------------------------------- fast form ----
+// The common case with its shape fixed at compile time: compiled gather
+// offsets, flags carrying only SYN_PREV_ACTIVE, cells of at most 512 synapses
+// (a warp's 512-synapse unit holds whole cells) and dendrite / cell-tuft
+// windows riding in the stages. Dendrites of 2^SPD_L2 synapses span
+// LPD = 2^(SPD_L2 - 4) lanes, cells LPC = 2^LPC_L2 lanes. It computes what
+// tma_stage + finish_chunk compute for that case, with every loop bound,
+// shift and branch on the shape resolved by the compiler.
+// Shapes: 1 (spd 32, S 32), 2 (64, 64), 3 (16, 128), 4 (16, 256), 5 (32, 256),
+// 6 (32, 512), 7 (64, 512).
+constexpr int kGeoms = 8;
+__host__ __device__ constexpr int geom_spd_l2(int g) {
+    return g == 1 ? 5 : g == 2 ? 6 : g == 3 ? 4 : g == 4 ? 4 : g == 5 ? 5 : g == 6 ? 5 : 6;
+}
+__host__ __device__ constexpr int geom_lpc_l2(int g) {
+    return g == 1 ? 1 : g == 2 ? 2 : g == 3 ? 3 : g == 4 ? 4 : g == 5 ? 4 : 5;
+}
+
+template <bool TUFT, int SPD_L2, int LPC_L2>
+__device__ __forceinline__ void stage_fast(const FusedTuftArgs& A, const TileGeo& G, const uint8_t* halo,
+                                           const uint8_t* sb, uint32_t pos, int lane, int wib, int32_t rnd) {
+    constexpr uint32_t SB = kWarps * 512;
+    constexpr uint32_t WIN = SB / 16 + 32;
+    constexpr uint32_t LPD = 1u << (SPD_L2 - 4);
+    constexpr uint32_t LPC = 1u << LPC_L2;
+    constexpr uint32_t S_L2 = LPC_L2 + 4;
+    static_assert(LPC >= LPD, "a cell holds whole dendrites");
+    const uint32_t unit0 = pos + (uint32_t)wib * 512;
+    if (unit0 >= G.syn_end) return;   // the warp's unit lies past the tile (uniform per warp)
+    const uint32_t so = (uint32_t)wib * 512 + (uint32_t)lane * 16;
+    const uint32_t off = pos + so;
+    const bool on = off < G.syn_end;
+    const uint8_t* wd = sb + 6 * SB;
+    const uint32_t f = (uint32_t)lane & (LPC - 1);
+    uint32_t act0 = 0, cur = 0;
+    if (on) {
+        if ((lane & (LPD - 1)) == 0) act0 = wd[(off >> SPD_L2) - ((pos >> SPD_L2) & ~15u)];
+        if (TUFT) {
+            const uint32_t ci = (off >> S_L2) - ((pos >> S_L2) & ~15u);
+            if (LPC >= 8) {
+                if (f < 4) cur = wd[(1 + f) * WIN + ci];
+            } else if (f == 0) {
+                cur = (uint32_t)wd[WIN + ci] | ((uint32_t)wd[2 * WIN + ci] << 8) | ((uint32_t)wd[3 * WIN + ci] << 16) |
+                      ((uint32_t)wd[4 * WIN + ci] << 24);
+            }
+        }
+    }
+    uint32_t sum = 0, raw = 0;
+    if (on) {
+        const uint4 str4 = *(const uint4*)(sb + 2 * SB + so);
+        const uint4 st4 = *(const uint4*)(sb + 3 * SB + so);
+        const uint4 g0 = *(const uint4*)(sb + 2 * so);
+        const uint4 g1 = *(const uint4*)(sb + 2 * so + 16);
+        const uint32_t gw[8] = {g0.x, g0.y, g0.z, g0.w, g1.x, g1.y, g1.z, g1.w};
+        const uint32_t strw[4] = {str4.x, str4.y, str4.z, str4.w};
+        const uint32_t stw[4] = {st4.x, st4.y, st4.z, st4.w};
+        uint32_t nst[4], nfl[4];
+#pragma unroll
+        for (int w = 0; w < 4; w++) {
+            const uint32_t lo = gw[2 * w], hi = gw[2 * w + 1];
+            nst[w] = pack4(halo[lo & 0x7FFFu], halo[(lo >> 16) & 0x7FFFu], halo[hi & 0x7FFFu],
+                           halo[(hi >> 16) & 0x7FFFu]);
+        }
+#pragma unroll
+        for (int w = 0; w < 4; w++) {
+            nfl[w] = nz_bits(stw[w]) >> 3;
+            raw = __dp4a(nst[w], 0x01010101u, raw);
+            sum = __dp4a(nst[w] & ~sign_bytes(strw[w]), 0x01010101u, sum);
+        }
+        *(uint4*)(A.st + off) = make_uint4(nst[0], nst[1], nst[2], nst[3]);
+        *(uint4*)(A.fl + off) = make_uint4(nfl[0], nfl[1], nfl[2], nfl[3]);
+    }
+#pragma unroll
+    for (uint32_t m = 1; m < LPD; m <<= 1) {
+        sum += __shfl_xor_sync(0xFFFFFFFFu, sum, m);
+        raw += __shfl_xor_sync(0xFFFFFFFFu, raw, m);
+    }
+    const bool lead = on && (lane & (LPD - 1)) == 0;
+    const uint32_t den = off >> SPD_L2;
+    uint32_t d_raw = 0, d_st = 0;
+    if (lead) {
+        const int active = sum > A.thresh;
+        const uint32_t s2 = active ? sum : 0u;
+        const uint32_t seed = (raw + A.thresh) | (den + A.den_idz);
+        A.den_act[den] = update_activity((uint8_t)act0, active, rnd, (int32_t)seed, kDendriteActivityDecay);
+        d_raw = min(raw >> 4, 255u);
+        d_st = min(s2 >> 4, 255u);
+        A.den_raw[den] = (uint8_t)d_raw;
+        A.den_st[den] = (uint8_t)d_st;
+    }
+    if (TUFT) {
+        constexpr uint32_t kDenMask = (1u << (S_L2 - SPD_L2)) - 1;   // dendrite index within its cell
+        uint32_t key = lead ? ((d_raw << 16) | (0xFFFFu - (den & kDenMask))) : 0u;
+        uint32_t best = d_st, tot = d_st;
+        if (LPC == 32) {
+            key = __reduce_max_sync(0xFFFFFFFFu, key);
+            best = __reduce_max_sync(0xFFFFFFFFu, best);
+            tot = __reduce_add_sync(0xFFFFFFFFu, tot);
+        } else {
+#pragma unroll
+            for (uint32_t m = LPD; m < LPC; m <<= 1) {
+                key = max(key, __shfl_xor_sync(0xFFFFFFFFu, key, m));
+                best = max(best, __shfl_xor_sync(0xFFFFFFFFu, best, m));
+                tot += __shfl_xor_sync(0xFFFFFFFFu, tot, m);
+            }
+            if (LPD > 1 && LPC >= 8) {
+                const int src = lane & ~(int)(LPD - 1);
+                key = __shfl_sync(0xFFFFFFFFu, key, src);
+                best = __shfl_sync(0xFFFFFFFFu, best, src);
+                tot = __shfl_sync(0xFFFFFFFFu, tot, src);
+            }
+        }
+        if (on && (LPC >= 8 ? f < 8 : f == 0)) {
+            const uint32_t c = off >> S_L2;
+            const uint32_t best_raw = key >> 16;
+            const uint32_t best_id = best_raw ? (0xFFFFu - (key & 0xFFFFu)) : 0u;
+            const bool is_max = tot >= (1u << (A.mad_l2 + 8));
+            const uint32_t tst = is_max ? 255u : ((tot >> A.mad_l2) & 0xFFu);
+            if (LPC >= 8) {
+                const uint32_t nv = f == 4 ? best_id : f == 5 ? best_raw : f == 6 ? best : tst;
+                (&A.t_pid)[f][c] = (uint8_t)(f < 4 ? cur : nv);
+            } else {
+                A.t_pid[c] = (uint8_t)cur;
+                A.t_praw[c] = (uint8_t)(cur >> 8);
+                A.t_pst[c] = (uint8_t)(cur >> 16);
+                A.t_ptft[c] = (uint8_t)(cur >> 24);
+                A.t_bid[c] = (uint8_t)best_id;
+                A.t_braw[c] = (uint8_t)best_raw;
+                A.t_bst[c] = (uint8_t)best;
+                A.t_st[c] = (uint8_t)tst;
+            }
+        }
+    }
+}
+
 // Producer lane: issues every stage of tile G into the ring (buffer pb of
 // round pround). False when a bounded wait gave up.
 template <bool TUFT, int MODE, bool FCLEAN>
@@ -648,7 +784,7 @@ __device__ __forceinline__ void producer_drain(AreaCtl* ctl, uint64_t* full, uin
 // Consumer warps: stage tile G's footprint, then process its stages from the
 // ring (buffer cb, phase cphase). A give-up sets s_abort; every consumer then
 // leaves at the next tile's barrier.
-template <bool TUFT, int MODE, bool FCLEAN>
+template <bool TUFT, int MODE, bool FCLEAN, int GEOM>
 __device__ __forceinline__ void consume_tile(const FusedTuftArgs& A, const TileGeo& G, uint8_t* halo, uint8_t* stages,
                                              uint64_t* full, uint64_t* empty, uint32_t& cb, uint32_t& cphase,
                                              int lane, int wib, int32_t rnd, volatile int& s_abort) {
@@ -664,15 +800,19 @@ __device__ __forceinline__ void consume_tile(const FusedTuftArgs& A, const TileG
             if (lane == 0) s_abort = 1;
             return;
         }
-        tma_stage<TUFT, MODE, FCLEAN>(A, G, halo, stages + (size_t)cb * A.stage_stride, pos, n_units_tile, lane, wib,
-                                      rnd);
+        if constexpr (GEOM == 0)
+            tma_stage<TUFT, MODE, FCLEAN>(A, G, halo, stages + (size_t)cb * A.stage_stride, pos, n_units_tile, lane,
+                                          wib, rnd);
+        else
+            stage_fast<TUFT, geom_spd_l2(GEOM), geom_lpc_l2(GEOM)>(A, G, halo, stages + (size_t)cb * A.stage_stride,
+                                                                   pos, lane, wib, rnd);
         __syncwarp();
         if (lane == 0) mbar_arrive(&empty[cb]);
         if (++cb == A.nst) { cb = 0; cphase ^= 1; }
     }
 }
 
-template <bool TUFT, int MODE, bool FCLEAN>
+template <bool TUFT, int MODE, bool FCLEAN, int GEOM>
 __device__ __forceinline__ void tma_body(const FusedTuftArgs& A, uint8_t* smem, volatile int& s_abort) {
     uint64_t* full = (uint64_t*)(smem + A.ring_off);   // [nst]
     uint64_t* empty = full + A.nst;                    // [nst]
@@ -699,7 +839,7 @@ __device__ __forceinline__ void tma_body(const FusedTuftArgs& A, uint8_t* smem, 
         const TileGeo G = tile_geo(A, t);
         consumers_sync();   // every consumer is done with the previous footprint
         if (s_abort) break;
-        consume_tile<TUFT, MODE, FCLEAN>(A, G, halo, stages, full, empty, cb, cphase, lane, wib, rnd, s_abort);
+        consume_tile<TUFT, MODE, FCLEAN, GEOM>(A, G, halo, stages, full, empty, cb, cphase, lane, wib, rnd, s_abort);
     }
 }
 
@@ -731,10 +871,30 @@ __global__ void __launch_bounds__(kThreads, 3) k_fused_tuft_tma(FusedTuftArgs A)
     init_ring(smem + A.ring_off, A.nst, s_abort);
     // One specialised body per gather mode and flags state (uniform per launch).
     switch (mode_of(A)) {
-    case 0: tma_body<TUFT, 0, true>(A, smem, s_abort); break;
-    case 1: tma_body<TUFT, 0, false>(A, smem, s_abort); break;
-    case 2: tma_body<TUFT, 1, true>(A, smem, s_abort); break;
-    default: tma_body<TUFT, 1, false>(A, smem, s_abort); break;
+    case 0:
+        // Shapes with a specialised consumer (pyramidal tufts, or the
+        // one-dendrite cells of spiny stellates).
+        if (TUFT) {
+            switch (A.geom) {
+            case 3: tma_body<TUFT, 0, true, 3>(A, smem, s_abort); return;
+            case 4: tma_body<TUFT, 0, true, 4>(A, smem, s_abort); return;
+            case 5: tma_body<TUFT, 0, true, 5>(A, smem, s_abort); return;
+            case 6: tma_body<TUFT, 0, true, 6>(A, smem, s_abort); return;
+            case 7: tma_body<TUFT, 0, true, 7>(A, smem, s_abort); return;
+            default: break;
+            }
+        } else {
+            switch (A.geom) {
+            case 1: tma_body<TUFT, 0, true, 1>(A, smem, s_abort); return;
+            case 2: tma_body<TUFT, 0, true, 2>(A, smem, s_abort); return;
+            default: break;
+            }
+        }
+        tma_body<TUFT, 0, true, 0>(A, smem, s_abort);
+        break;
+    case 1: tma_body<TUFT, 0, false, 0>(A, smem, s_abort); break;
+    case 2: tma_body<TUFT, 1, true, 0>(A, smem, s_abort); break;
+    default: tma_body<TUFT, 1, false, 0>(A, smem, s_abort); break;
     }
 }
 
@@ -819,12 +979,32 @@ __global__ void __launch_bounds__(kThreads, 3) k_fused_tuft_batch(const __grid_c
             rnd = rnd_at(A.rnd_key, A.ctl->cycle);
         }
         const TileGeo G = tile_geo(A, t - P.tile0[j]);
+#define BM_CONSUME(M, FC, GM) \
+    consume_tile<TUFT, M, FC, GM>(A, G, halo, stages, full, empty, cb, cphase, lane, wib, rnd, s_abort)
         switch (mode) {
-        case 0: consume_tile<TUFT, 0, true>(A, G, halo, stages, full, empty, cb, cphase, lane, wib, rnd, s_abort); break;
-        case 1: consume_tile<TUFT, 0, false>(A, G, halo, stages, full, empty, cb, cphase, lane, wib, rnd, s_abort); break;
-        case 2: consume_tile<TUFT, 1, true>(A, G, halo, stages, full, empty, cb, cphase, lane, wib, rnd, s_abort); break;
-        default: consume_tile<TUFT, 1, false>(A, G, halo, stages, full, empty, cb, cphase, lane, wib, rnd, s_abort); break;
+        case 0:
+            if (TUFT) {
+                switch (A.geom) {
+                case 3: BM_CONSUME(0, true, 3); break;
+                case 4: BM_CONSUME(0, true, 4); break;
+                case 5: BM_CONSUME(0, true, 5); break;
+                case 6: BM_CONSUME(0, true, 6); break;
+                case 7: BM_CONSUME(0, true, 7); break;
+                default: BM_CONSUME(0, true, 0); break;
+                }
+            } else {
+                switch (A.geom) {
+                case 1: BM_CONSUME(0, true, 1); break;
+                case 2: BM_CONSUME(0, true, 2); break;
+                default: BM_CONSUME(0, true, 0); break;
+                }
+            }
+            break;
+        case 1: BM_CONSUME(0, false, 0); break;
+        case 2: BM_CONSUME(1, true, 0); break;
+        default: BM_CONSUME(1, false, 0); break;
         }
+#undef BM_CONSUME
     }
 }
 
@@ -1188,6 +1368,11 @@ void make_args(FusedTuftArgs& A, const FusedArea& F, const uint8_t* axns, const 
         A.stage_stride = FT.stage_stride;
         A.win = FT.win;
         A.win_bytes = FT.win_bytes;
+        // The specialised consumer of this shape, if there is one.
+        A.geom = 0;
+        if (FT.win && A.chunks_per_unit == 1 && FT.stage_bytes == (uint32_t)kWarps * 512)
+            for (int g = 1; g < kGeoms; g++)
+                if ((uint32_t)geom_spd_l2(g) == A.spd_l2 && (uint32_t)geom_lpc_l2(g) + 4 == A.S_l2) A.geom = (uint32_t)g;
     } else {
         A.n_units = S > 512 ? (uint64_t)L.cells : (A.n_syn + 511) / 512;
     }
