@@ -94,7 +94,8 @@ struct FusedTuftArgs {
     uint64_t n_units;
     // Tiled form.
     uint32_t tile_w, tile_h, tiles_u, tiles_v, n_tiles;
-    uint32_t usz_magic;                 // ceil(2^32 / u_size) for multi-row tiles
+    uint64_t usz_magic;                 // div_magic(u_size), for multi-row tiles
+    uint64_t per_slice_magic, tiles_u_magic;   // div_magic of the tiles per slice and per row
     int32_t rv, ru;                     // largest |v|, |u| offset served from the footprint
     uint32_t fw, frows, fsz;            // footprint width, rows and bytes per source slice
     uint32_t src_vs, src_us, src_vsz, src_usz;   // geometry shared by the recorded slices
@@ -407,6 +408,14 @@ __global__ void __launch_bounds__(kWarps * 32) k_fused_tuft(FusedTuftArgs A) {
 }
 
 // ------------------------------------------------------ tiled TMA form ----
+// x / d by a 64-bit multiply-high with m = div_magic(d) = ceil(2^64 / d):
+// exact for every 32-bit x and 2 <= d < 2^32 (the rounding error of m
+// stays below 2^-32 < 1/d); d == 1 is passed through.
+inline uint64_t div_magic(uint32_t d) { return d > 1 ? UINT64_MAX / d + 1 : 0; }
+__device__ __forceinline__ uint32_t fast_div(uint32_t x, uint32_t d, uint64_t m) {
+    return d == 1 ? x : (uint32_t)__umul64hi((uint64_t)x, m);
+}
+
 struct TileGeo {
     uint32_t v0, u0, h, w;
     int32_t vlo, ulo;
@@ -416,10 +425,11 @@ struct TileGeo {
 __device__ __forceinline__ TileGeo tile_geo(const FusedTuftArgs& A, uint32_t t) {
     TileGeo g;
     const uint32_t per_slice = A.tiles_v * A.tiles_u;
-    const uint32_t s_lyr = t / per_slice;
+    const uint32_t s_lyr = fast_div(t, per_slice, A.per_slice_magic);
     const uint32_t tr = t - s_lyr * per_slice;
-    g.v0 = (tr / A.tiles_u) * A.tile_h;
-    g.u0 = (tr % A.tiles_u) * A.tile_w;
+    const uint32_t tv = fast_div(tr, A.tiles_u, A.tiles_u_magic);
+    g.v0 = tv * A.tile_h;
+    g.u0 = (tr - tv * A.tiles_u) * A.tile_w;
     g.h = min(A.tile_h, A.v_size - g.v0);
     g.w = min(A.tile_w, A.u_size - g.u0);
     g.vlo = (int32_t)((g.v0 * A.src_vs) >> kSlcSclCoeffL2) - A.rv;
@@ -439,7 +449,7 @@ __device__ __forceinline__ int32_t footprint_base(const FusedTuftArgs& A, const 
         v = G.v0;
         u = G.u0 + local;
     } else {
-        const uint32_t q = __umulhi(local, A.usz_magic);
+        const uint32_t q = fast_div(local, A.u_size, A.usz_magic);
         v = G.v0 + q;
         u = local - q * A.u_size;
     }
@@ -447,38 +457,35 @@ __device__ __forceinline__ int32_t footprint_base(const FusedTuftArgs& A, const 
            ((int32_t)((u * A.src_us) >> kSlcSclCoeffL2) - G.ulo);
 }
 
-// Stages the tile's footprint: element e (row-major over slice, row, column)
-// holds syn_fire(axon) at (vlo + row, ulo + column) of the slice, or 0 outside
-// it. Each consumer thread takes elements tid, tid + 256, ...; the loads of a
-// batch of 16 are all issued before any store so their latencies overlap.
-__device__ __forceinline__ void build_footprint(const FusedTuftArgs& A, const TileGeo& G, uint8_t* halo, uint32_t tid) {
-    const uint32_t total = A.nrec * A.fsz;
-    constexpr uint32_t kStep = kWarps * 32;
-    // Decompose the thread's first element once; later elements advance by kStep.
-    uint32_t k = tid / A.fsz, rem = tid - k * A.fsz;
-    uint32_t r = rem / A.fw, c = rem - r * A.fw;
-    for (uint32_t e0 = tid; e0 < total; e0 += 16 * kStep) {
-        uint8_t vals[16];
+// Stages the tile's footprint: element (k, row, column), row-major, holds
+// syn_fire(axon) at (vlo + row, ulo + column) of recorded slice k, or 0
+// outside it. Warps take whole rows (warp w: rows w, w + 8, ... of each
+// slice); lanes take columns, so loads of a row are coalesced and the four
+// loads of a lane are issued before any store.
+__device__ __forceinline__ void build_footprint(const FusedTuftArgs& A, const TileGeo& G, uint8_t* halo, int lane,
+                                                int wib) {
+    for (uint32_t k = 0; k < A.nrec; k++) {
+        const uint8_t* slice = A.axns + A.src_idz[k];
+        uint8_t* dst_k = halo + k * A.fsz;
+        for (uint32_t r = (uint32_t)wib; r < A.frows; r += kWarps) {
+            const int32_t vr = G.vlo + (int32_t)r;
+            const bool row_in = (uint32_t)vr < A.src_vsz;
+            const uint8_t* src = slice + (row_in ? (uint32_t)vr * A.src_usz : 0u);
+            uint8_t* dst = dst_k + r * A.fw;
+            for (uint32_t c0 = 0; c0 < A.fw; c0 += 128) {
+                uint32_t v[4];
 #pragma unroll
-        for (int i = 0; i < 16; i++) {
-            const uint32_t e = e0 + (uint32_t)i * kStep;
-            uint8_t a = 0;
-            if (e < total) {
-                const int32_t vr = G.vlo + (int32_t)r, uc = G.ulo + (int32_t)c;
-                if (((uint32_t)vr < A.src_vsz) & ((uint32_t)uc < A.src_usz))
-                    a = __ldg(A.axns + A.src_idz[k] + (uint32_t)vr * A.src_usz + (uint32_t)uc);
-            }
-            vals[i] = a;
-            c += kStep;
-            while (c >= A.fw) {
-                c -= A.fw;
-                if (++r == A.frows) { r = 0; k++; }
-            }
-        }
+                for (int q = 0; q < 4; q++) {
+                    const uint32_t c = c0 + (uint32_t)lane + 32u * q;
+                    const int32_t uc = G.ulo + (int32_t)c;
+                    v[q] = (row_in && c < A.fw && (uint32_t)uc < A.src_usz) ? (uint32_t)__ldg(src + uc) : 0u;
+                }
 #pragma unroll
-        for (int i = 0; i < 16; i++) {
-            const uint32_t e = e0 + (uint32_t)i * kStep;
-            if (e < total) halo[e] = syn_fire(vals[i]);
+                for (int q = 0; q < 4; q++) {
+                    const uint32_t c = c0 + (uint32_t)lane + 32u * q;
+                    if (c < A.fw) dst[c] = syn_fire((uint8_t)v[q]);
+                }
+            }
         }
     }
 }
@@ -788,7 +795,7 @@ template <bool TUFT, int MODE, bool FCLEAN, int GEOM>
 __device__ __forceinline__ void consume_tile(const FusedTuftArgs& A, const TileGeo& G, uint8_t* halo, uint8_t* stages,
                                              uint64_t* full, uint64_t* empty, uint32_t& cb, uint32_t& cphase,
                                              int lane, int wib, int32_t rnd, volatile int& s_abort) {
-    build_footprint(A, G, halo, wib * 32 + lane);
+    build_footprint(A, G, halo, lane, wib);
     consumers_sync();
     const uint32_t SB = A.stage_bytes;
     const uint32_t cpu = A.chunks_per_unit;
@@ -906,7 +913,8 @@ __global__ void __launch_bounds__(kThreads, 3) k_fused_tuft_tma(FusedTuftArgs A)
 // read-only there, so the compiler keeps argument fields in registers across
 // the stores of a stage, and nothing needs copying per job. Every job of a
 // launch shares the ring geometry (nst, stage_stride, ring_off).
-constexpr uint32_t kMaxBatchJobs = 80;   // 80 argument blocks fit the 32 KB parameter limit
+// As many argument blocks as fit the 32 KB kernel parameter limit.
+constexpr uint32_t kMaxBatchJobs = (32764 - 16) / (sizeof(FusedTuftArgs) + 4) - 1;
 
 struct BatchParams {
     FusedTuftArgs jobs[kMaxBatchJobs];
@@ -1350,7 +1358,9 @@ void make_args(FusedTuftArgs& A, const FusedArea& F, const uint8_t* axns, const 
         A.tiles_u = (L.u_size + FT.tile_w - 1) / FT.tile_w;
         A.tiles_v = (L.v_size + FT.tile_h - 1) / FT.tile_h;
         A.n_tiles = L.depth * A.tiles_u * A.tiles_v;
-        A.usz_magic = (uint32_t)(((1ull << 32) + L.u_size - 1) / L.u_size);
+        A.usz_magic = div_magic(L.u_size);
+        A.per_slice_magic = div_magic(A.tiles_u * A.tiles_v);
+        A.tiles_u_magic = div_magic(A.tiles_u);
         A.rv = FT.rv;
         A.ru = FT.ru;
         A.fw = FT.fw;
