@@ -92,6 +92,7 @@ __device__ __forceinline__ uint32_t block_job(const J* __restrict__ jobs, uint32
 
 template <int ST>
 __global__ void __launch_bounds__(kCellBlock) k_batch_cells(const CellJob* __restrict__ jobs, uint32_t n_jobs) {
+    pdl_begin();
     const CellJob& J = jobs[block_job(jobs, n_jobs)];
     const uint32_t i = (blockIdx.x - J.block0) * kCellBlock + threadIdx.x;
     // Warp-cooperative steps keep every lane (a block's warps belong to one job).
@@ -123,6 +124,7 @@ __global__ void __launch_bounds__(kCellBlock) k_batch_cells(const CellJob* __res
 
 __global__ void __launch_bounds__(kIntakeBlock)
     k_batch_intake(const IntakeJob* __restrict__ jobs, uint32_t n_jobs, const BatchCtl* __restrict__ bc) {
+    pdl_begin();
     const IntakeJob& J = jobs[block_job(jobs, n_jobs)];
     const uint8_t* src = J.src;
     if (!src) {
@@ -136,6 +138,7 @@ __global__ void __launch_bounds__(kIntakeBlock)
 }
 
 __global__ void k_batch_cycle_end(AreaCtl* const* __restrict__ ctls, uint32_t n, BatchCtl* bc) {
+    pdl_begin();
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) ctls[i]->cycle += 1;
     if (i == 0) bc->cursor += 1;
@@ -152,7 +155,7 @@ void launch_cells(int st, const CellJob* jobs, uint32_t n_jobs, uint32_t n_block
     if (!n_blocks) return;
     switch (st) {
 #define BM_CELLS(K) \
-    case K: k_batch_cells<K><<<n_blocks, kCellBlock, 0, s>>>(jobs, n_jobs); break;
+    case K: launch_pdl(k_batch_cells<K>, n_blocks, kCellBlock, 0, s, jobs, n_jobs); break;
         BM_CELLS(ST_SSC_CYCLE)
         BM_CELLS(ST_INHIB_SIMPLE)
         BM_CELLS(ST_INHIB_PASS)
@@ -560,7 +563,7 @@ int build_intake(bm_batch_s* B) {
 
 void enqueue_batch_cycle(bm_batch_s* B, cudaStream_t s) {
     if (B->intake_blocks)
-        k_batch_intake<<<B->intake_blocks, kIntakeBlock, 0, s>>>(B->d_intake, B->n_intake, B->d_bctl);
+        launch_pdl(k_batch_intake, B->intake_blocks, kIntakeBlock, 0, s, B->d_intake, B->n_intake, B->d_bctl);
     const bool prof = B->profiling && s != B->cap;
     for (size_t k = 0; k < B->plan.size(); k++) {
         auto& p = B->plan[k];
@@ -587,7 +590,7 @@ void enqueue_batch_cycle(bm_batch_s* B, cudaStream_t s) {
         }
     }
     const uint32_t n = (uint32_t)B->areas.size();
-    k_batch_cycle_end<<<(n + 127) / 128, 128, 0, s>>>(B->d_ctls, n, B->d_bctl);
+    launch_pdl(k_batch_cycle_end, (n + 127) / 128, 128, 0, s, B->d_ctls, n, B->d_bctl);
 }
 
 int ensure_graph(bm_batch_s* B) {

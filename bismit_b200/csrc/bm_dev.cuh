@@ -7,7 +7,36 @@
 
 #include "../../include/bismit_b200.h"
 
+#include <utility>
+
 namespace bm {
+
+// Programmatic dependent launch. The cycle's kernels are launched with the
+// programmatic-serialization attribute (launch_pdl), so a kernel's blocks may
+// be scheduled while the previous kernel of the stream drains. Every such
+// kernel calls pdl_begin() before touching global memory: it waits until the
+// previous kernel has finished and its writes are visible, then lets the next
+// kernel be scheduled. Launched without the attribute, both are no-ops.
+__device__ __forceinline__ void pdl_begin() {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
+template <typename... KArgs, typename... Args>
+inline cudaError_t launch_pdl(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                              Args&&... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kern, std::forward<Args>(args)...);
+}
 
 // Reference constants: cl/bismit.cl:11-22, cl/control.cl:6-13,
 // src/cmn/mod.rs:242,321-336.

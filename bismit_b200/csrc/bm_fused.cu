@@ -337,6 +337,7 @@ __device__ __forceinline__ void finish_chunk(const FusedTuftArgs& A, const uint4
 // units of the whole tuft and gather through per-lane slice records.
 template <bool TUFT>
 __global__ void __launch_bounds__(kWarps * 32) k_fused_tuft(FusedTuftArgs A) {
+    pdl_begin();
     __shared__ Rec recs[kWarps][kMaxRecs * 32];
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
@@ -490,9 +491,15 @@ __device__ __forceinline__ void build_footprint(const FusedTuftArgs& A, const Ti
     }
 }
 
-// Stage layout, per buffer: MODE 0 streams gidx (2 x SB bytes) then strength,
-// state, flags (SB each); MODE 1 streams slc, v_ofs, u_ofs, strength, state,
-// flags (SB each).
+// Stage layout, per buffer of 4 x SB bytes of synapse arrays followed by the
+// windows: MODE 0 streams gidx (2 bytes a synapse) then strength, state and
+// (unless FCLEAN) flags; MODE 1 streams slc, v_ofs, u_ofs, strength, state,
+// flags. The common form (MODE 0, FCLEAN) takes SB synapses a stage; the wider
+// forms take SB / 2, so every form fits the same buffer.
+template <int MODE, bool FCLEAN>
+__device__ __forceinline__ uint32_t stage_syns(uint32_t SB) {
+    return (MODE == 0 && FCLEAN) ? SB : SB / 2;
+}
 template <int MODE>
 __device__ __forceinline__ uint32_t arr_off(int which, uint32_t SB) {
     // which: 0 strength, 1 state, 2 flags
@@ -505,8 +512,9 @@ template <bool TUFT, int MODE, bool FCLEAN>
 __device__ __forceinline__ void tma_stage(const FusedTuftArgs& A, const TileGeo& G, const uint8_t* halo,
                                           const uint8_t* sb, uint32_t pos, uint32_t n_units_tile, int lane, int wib,
                                           int32_t rnd) {
-    const uint32_t SB = A.stage_bytes;
+    const uint32_t SB = stage_syns<MODE, FCLEAN>(A.stage_bytes);   // synapses of this stage's arrays
     const uint32_t cpu = A.chunks_per_unit;
+    if ((uint32_t)wib * cpu * 512 >= SB) return;   // half-size stages keep half the warps busy
     const uint32_t unit = ((pos - G.syn0) >> A.unit_l2) + (uint32_t)wib;
     if (unit >= n_units_tile) return;
     uint32_t t_key = 0, t_best = 0, t_sum = 0, tuft_cur = 0;
@@ -522,7 +530,7 @@ __device__ __forceinline__ void tma_stage(const FusedTuftArgs& A, const TileGeo&
         if (A.win) {
             // The stage carries the dendrite and cell-tuft bytes (windows start
             // at the stage's first dendrite / cell rounded down to 16).
-            const uint8_t* wd = sb + 6 * SB;
+            const uint8_t* wd = sb + 4 * A.stage_bytes;
             const uint32_t lpd = 1u << A.lpd_l2;
             act0 = (on && (lane & (lpd - 1)) == 0) ? (uint32_t)wd[(off >> A.spd_l2) - ((pos >> A.spd_l2) & ~15u)] : 0u;
             if (TUFT && ch == 0) {
@@ -623,7 +631,7 @@ __device__ __forceinline__ void stage_fast(const FusedTuftArgs& A, const TileGeo
     const uint32_t so = (uint32_t)wib * 512 + (uint32_t)lane * 16;
     const uint32_t off = pos + so;
     const bool on = off < G.syn_end;
-    const uint8_t* wd = sb + 6 * SB;
+    const uint8_t* wd = sb + 4 * SB;
     const uint32_t f = (uint32_t)lane & (LPC - 1);
     uint32_t act0 = 0, cur = 0;
     if (on) {
@@ -732,7 +740,7 @@ template <bool TUFT, int MODE, bool FCLEAN>
 __device__ __forceinline__ bool produce_tile(const FusedTuftArgs& A, const TileGeo& G, uint8_t* stages,
                                              uint64_t* full, uint64_t* empty, uint32_t& pb, uint32_t& pround,
                                              uint64_t& issued, volatile int& s_abort) {
-    const uint32_t SB = A.stage_bytes;
+    const uint32_t SB = stage_syns<MODE, FCLEAN>(A.stage_bytes);
     const uint32_t buf_bytes = A.stage_stride;
     const uint32_t nst = A.nst;
     for (uint32_t pos = G.syn0; pos < G.syn_end; pos += SB) {
@@ -752,7 +760,7 @@ __device__ __forceinline__ bool produce_tile(const FusedTuftArgs& A, const TileG
         if (A.win) n_arr_bytes += (uint32_t)(d1 - d0) + (TUFT ? 4 * (uint32_t)(c1 - c0) : 0u);
         mbar_arrive_expect_tx(&full[pb], n_arr_bytes);
         if (A.win) {
-            uint8_t* wd = dst + 6 * SB;
+            uint8_t* wd = dst + 4 * A.stage_bytes;
             bulk_g2s(wd, A.den_act + d0, (uint32_t)(d1 - d0), &full[pb]);
             if (TUFT) {
                 const uint32_t cb = (uint32_t)(c1 - c0);
@@ -797,7 +805,7 @@ __device__ __forceinline__ void consume_tile(const FusedTuftArgs& A, const TileG
                                              int lane, int wib, int32_t rnd, volatile int& s_abort) {
     build_footprint(A, G, halo, lane, wib);
     consumers_sync();
-    const uint32_t SB = A.stage_bytes;
+    const uint32_t SB = stage_syns<MODE, FCLEAN>(A.stage_bytes);
     const uint32_t cpu = A.chunks_per_unit;
     const uint32_t n_units_tile = cpu > 1 ? G.h * G.w : (G.syn_end - G.syn0 + 511) >> 9;
     for (uint32_t pos = G.syn0; pos < G.syn_end; pos += SB) {
@@ -873,6 +881,7 @@ __device__ __forceinline__ uint32_t mode_of(const FusedTuftArgs& A) {
 
 template <bool TUFT>
 __global__ void __launch_bounds__(kThreads, 3) k_fused_tuft_tma(FusedTuftArgs A) {
+    pdl_begin();
     extern __shared__ __align__(128) uint8_t smem[];
     __shared__ volatile int s_abort;   // a bounded wait gave up
     init_ring(smem + A.ring_off, A.nst, s_abort);
@@ -936,6 +945,7 @@ __device__ __forceinline__ uint32_t job_of(const BatchParams& P, uint32_t t) {
 
 template <bool TUFT>
 __global__ void __launch_bounds__(kThreads, 3) k_fused_tuft_batch(const __grid_constant__ BatchParams P) {
+    pdl_begin();
     extern __shared__ __align__(128) uint8_t smem[];
     __shared__ volatile int s_abort;
     const uint32_t nst = P.nst;
@@ -1025,6 +1035,7 @@ __global__ void __launch_bounds__(kThreads, 3) k_fused_tuft_batch(const __grid_c
 __global__ void k_compile_tuft(const uint8_t* __restrict__ slc, const int8_t* __restrict__ vo,
                                const int8_t* __restrict__ uo, const uint8_t* __restrict__ fl, uint16_t* gidx,
                                uint64_t n, GatherGeo g, unsigned int* status) {
+    pdl_begin();
     uint32_t bits = 0;
     for (uint64_t i = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) * 16; i < n;
          i += (uint64_t)gridDim.x * blockDim.x * 16) {
@@ -1071,12 +1082,16 @@ inline bool pow2(uint64_t x) { return x && !(x & (x - 1)); }
 
 namespace {
 
-// Stages of the shared-memory ring: two when that lets three CTAs share an
-// SM (more warps to hide the gathers' latency, the same bytes in flight per
-// SM), else as many as fit about 80 KB with two CTAs per SM.
-uint32_t ring_stages(uint64_t stride, uint64_t halo) {
-    if (128 + 2 * stride + halo <= kSmem3) return 2;
-    return (uint32_t)std::max<uint64_t>(2, std::min<uint64_t>(4, (80 * 1024) / stride));
+// Stages of the shared-memory ring: the deepest ring of at most max_n stages
+// with which three CTAs share an SM, else with which two do. Measured on
+// B200: one tuft alone (area_256) runs fastest with two stages, batched steps
+// (many tufts of several areas per launch) with up to four.
+uint32_t ring_stages(uint64_t stride, uint64_t halo, uint32_t max_n) {
+    for (uint32_t n = max_n; n >= 2; n--)
+        if (128 + n * stride + halo <= kSmem3) return n;
+    for (uint32_t n = max_n; n >= 2; n--)
+        if (128 + n * stride + halo <= kMaxSmem) return n;
+    return 2;
 }
 
 int device_sms() {
@@ -1152,11 +1167,11 @@ void plan_tuft(FusedTuft& FT, const bm_area_plan& P, uint32_t i, uint32_t t, int
     // Windows: up to SB / 16 dendrites (or cells) per stage, widened by 16
     // at both ends.
     const uint32_t win_bytes = SB / 16 + 32;
-    const uint32_t buf_bytes = 6 * SB + 5 * win_bytes;
+    const uint32_t buf_bytes = 4 * SB + 5 * win_bytes;
     // The footprint sits at the start of dynamic shared memory (gathers then
     // address it with a constant base), the ring after it.
     const uint64_t ring_off = ((halo + 127) / 128) * 128;
-    const uint32_t nst = ring_stages(buf_bytes, ring_off);
+    const uint32_t nst = ring_stages(buf_bytes, ring_off, 2);
     // Gathers mask offsets to 15 bits: at least 32 KB of shared memory keeps
     // every masked offset inside the CTA's allocation.
     const uint64_t smem = std::max<uint64_t>(32768, ring_off + 128 + (uint64_t)nst * buf_bytes);
@@ -1291,7 +1306,7 @@ void launch_compile_tuft(const FusedArea& F, const DevLayer& L, uint32_t layer, 
     const uint64_t n = (uint64_t)L.cells * T.spt;
     const uint64_t threads = (n + 15) / 16;
     const unsigned grid = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((threads + 255) / 256, (uint64_t)F.sms * 8));
-    k_compile_tuft<<<grid, 256, 0, s>>>(L.buf[BM_BUF_SYN_SRC_SLC_IDS] + T.syn_idz,
+    launch_pdl(k_compile_tuft, grid, 256, 0, s, L.buf[BM_BUF_SYN_SRC_SLC_IDS] + T.syn_idz,
                                         (const int8_t*)L.buf[BM_BUF_SYN_SRC_COL_V_OFFS] + T.syn_idz,
                                         (const int8_t*)L.buf[BM_BUF_SYN_SRC_COL_U_OFFS] + T.syn_idz,
                                         L.buf[BM_BUF_SYN_FLAG_SETS] + T.syn_idz, FT.tiled ? FT.gidx : nullptr, n,
@@ -1398,15 +1413,15 @@ void launch_fused_tuft(const FusedArea& F, const uint8_t* axns, const SliceRec* 
     const bool tuft = L.kind == BM_LYR_PYRAMIDAL;
     if (FT.tiled) {
         auto kern = tuft ? k_fused_tuft_tma<true> : k_fused_tuft_tma<false>;
-        kern<<<FT.grid, kThreads, FT.smem, s>>>(A);
+        launch_pdl(kern, FT.grid, kThreads, FT.smem, s, A);
     } else {
         uint64_t want = (A.n_units + kWarps - 1) / kWarps;
         uint64_t cap = (uint64_t)F.sms * 8;
         unsigned grid = (unsigned)std::max<uint64_t>(1, std::min(want, cap));
         if (tuft)
-            k_fused_tuft<true><<<grid, kWarps * 32, 0, s>>>(A);
+            launch_pdl(k_fused_tuft<true>, grid, kWarps * 32, 0, s, A);
         else
-            k_fused_tuft<false><<<grid, kWarps * 32, 0, s>>>(A);
+            launch_pdl(k_fused_tuft<false>, grid, kWarps * 32, 0, s, A);
     }
 }
 
@@ -1441,7 +1456,7 @@ int prepare_fused_batch(FusedBatch& B, const std::vector<FusedJob>& jobs) {
             cls.push_back(&J);
             halo = std::max(halo, ((FT.nrec * FT.fsz + 127) / 128) * 128);
         }
-        uint32_t nst = ring_stages(stride, halo);
+        uint32_t nst = ring_stages(stride, halo, 4);
         while (nst > 2 && 128 + (uint64_t)nst * stride + halo > kMaxSmem) nst--;
         const uint64_t ring_off = halo;
         const uint64_t smem = std::max<uint64_t>(32768, ring_off + 128 + (uint64_t)nst * stride);
@@ -1491,7 +1506,7 @@ void launch_fused_batch(const FusedBatch& B, cudaStream_t s) {
     if (!B.ok || !B.n_tiles) return;
     auto kern = B.tuft ? k_fused_tuft_batch<true> : k_fused_tuft_batch<false>;
     for (size_t k = 0; k < B.params.size(); k++)
-        kern<<<B.grids[k], kThreads, B.smems[k], s>>>(*(const BatchParams*)B.params[k]);
+        launch_pdl(kern, B.grids[k], kThreads, B.smems[k], s, *(const BatchParams*)B.params[k]);
 }
 
 void free_fused_batch(FusedBatch& B) {

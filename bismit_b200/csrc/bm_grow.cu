@@ -82,7 +82,7 @@ __global__ void k_grow(DevLayer L, GrowTuft G) {
     }
 }
 
-__global__ void k_cycle_end(AreaCtl* ctl) { ctl->cycle += 1; }
+__global__ void k_cycle_end(AreaCtl* ctl) { pdl_begin(); ctl->cycle += 1; }
 
 // Synapses::regrow (src/cortex/synapses.rs:411-501) with SynSrcIdxCache
 // (src/map/syn_src.rs:159-211), one dendrite per thread, on the cycles c with
@@ -97,6 +97,7 @@ __global__ void k_cycle_end(AreaCtl* ctl) { ctl->cycle += 1; }
 // compiled gather offset follows each moved synapse. The same rule is
 // restated in the oracle.
 __global__ void __launch_bounds__(kRegrowBlock) k_regrow(const RegrowJob* __restrict__ jobs, uint32_t n_jobs) {
+    pdl_begin();
     __shared__ uint32_t s_j;
     if (threadIdx.x == 0) {
         uint32_t lo = 0, hi = n_jobs;
@@ -173,12 +174,12 @@ void launch_grow(const DevLayer& L, const GrowTuft& G, cudaStream_t s) {
     k_grow<<<(unsigned)((n + 127) / 128), 128, 0, s>>>(L, G);
 }
 
-void launch_cycle_end(AreaCtl* ctl, cudaStream_t s) { k_cycle_end<<<1, 1, 0, s>>>(ctl); }
+void launch_cycle_end(AreaCtl* ctl, cudaStream_t s) { launch_pdl(k_cycle_end, 1, 1, 0, s, ctl); }
 
 uint64_t regrow_key(uint64_t gkey) { return splitmix64(gkey ^ 0x7265677277ull); }
 
 void launch_regrow(const RegrowJob* jobs, uint32_t n_jobs, uint32_t n_blocks, cudaStream_t s) {
-    if (n_blocks) k_regrow<<<n_blocks, kRegrowBlock, 0, s>>>(jobs, n_jobs);
+    if (n_blocks) launch_pdl(k_regrow, n_blocks, kRegrowBlock, 0, s, jobs, n_jobs);
 }
 
 }  // namespace bm

@@ -13,6 +13,7 @@ __device__ __forceinline__ uint64_t gtid() { return (uint64_t)blockIdx.x * block
 
 // tft_set_syn_flags, cl/syns.cl:23-33, 16 synapses per thread.
 __global__ void k_set_syn_flags(const uint8_t* __restrict__ states, uint8_t* __restrict__ flags, uint64_t n) {
+    pdl_begin();
     uint64_t i = gtid() * 16;
     if (i + 16 <= n && ((((uintptr_t)states) | ((uintptr_t)flags)) & 15) == 0) {
         uint4 s = *(const uint4*)(states + i);
@@ -36,65 +37,77 @@ __global__ void k_set_syn_flags(const uint8_t* __restrict__ states, uint8_t* __r
 // stage, one thread per item.
 __global__ void k_syn_cycle(const uint8_t* __restrict__ axns, const SliceRec* __restrict__ slices,
                             DevLayer L, uint32_t t) {
+    pdl_begin();
     uint64_t i = gtid();
     if (i >= (uint64_t)L.cells * L.tft[t].spt) return;
     syn_cycle_item(axns, slices, L, t, i);
 }
 
 __global__ void k_den_cycle(DevLayer L, uint32_t t, const AreaCtl* ctl) {
+    pdl_begin();
     uint64_t d = gtid();
     if (d >= (uint64_t)L.cells * L.tft[t].dpt) return;
     den_cycle_item(L, t, rnd_at(L.tft[t].rnd_key_den, ctl->cycle), d);
 }
 
 __global__ void k_tft_cycle(DevLayer L, uint32_t t) {
+    pdl_begin();
     uint32_t c = (uint32_t)gtid();
     if (c < L.cells) tft_cycle_item(L, t, c);
 }
 
 __global__ void k_ssc_cycle(DevLayer L) {
+    pdl_begin();
     uint32_t c = (uint32_t)gtid();
     if (c < L.cells) ssc_cycle_item(L, c);
 }
 
 __global__ void k_inhib_simple(uint8_t* __restrict__ axns, const SliceRec* __restrict__ slices, DevLayer L,
                                int radius, uint64_t rnd_key, const AreaCtl* ctl) {
+    pdl_begin();
     uint32_t c = (uint32_t)gtid();
     if (c < L.cells) inhib_simple_item(axns, slices, L, radius, rnd_at(rnd_key, ctl->cycle), c);
 }
 
 __global__ void k_inhib_passthrough(uint8_t* __restrict__ axns, const SliceRec* __restrict__ slices, DevLayer L) {
+    pdl_begin();
     uint32_t c = (uint32_t)gtid();
     if (c < L.cells) inhib_passthrough_item(axns, slices, L, c);
 }
 
 __global__ void k_ssc_mtp_simple(const uint8_t* __restrict__ axns, DevLayer L, const AreaCtl* ctl) {
+    pdl_begin();
     uint32_t c = (uint32_t)gtid();
     if (c < L.cells) ssc_mtp_item(axns, L, rnd_at(L.rnd_key_ssc_mtp, ctl->cycle), c);
 }
 
 __global__ void k_pyr_cycle(DevLayer L) {
+    pdl_begin();
     uint32_t c = (uint32_t)gtid();
     if (c < L.cells) pyr_cycle_item(L, c);
 }
 
 __global__ void k_pyr_output(uint8_t* __restrict__ axns, const SliceRec* __restrict__ slices, DevLayer L) {
+    pdl_begin();
     uint32_t c = (uint32_t)gtid();
     if (c < L.cells) pyr_output_item(axns, slices, L, c);
 }
 
 __global__ void k_inhib_intra_column(uint8_t* __restrict__ axns, const SliceRec* __restrict__ slices, DevLayer L) {
+    pdl_begin();
     uint32_t col = (uint32_t)gtid();
     if (col < L.v_size * L.u_size) intra_column_item(axns, slices, L, col);
 }
 
 __global__ void k_tft_dst_mtp(const uint8_t* __restrict__ axns, DevLayer L, uint32_t t, const AreaCtl* ctl) {
+    pdl_begin();
     uint32_t c = (uint32_t)gtid();
     if (c < L.cells) tft_dst_mtp_item(axns, L, t, rnd_at(L.tft[t].rnd_key_mtp, ctl->cycle), c);
 }
 
 __global__ void k_tuft_cells(const uint8_t* __restrict__ axns, const SliceRec* __restrict__ slices, DevLayer L,
                              uint32_t t, const AreaCtl* ctl) {
+    pdl_begin();
     uint32_t c = (uint32_t)gtid();
     if (c < L.cells) tuft_cell_item(axns, slices, L, t, rnd_at(L.tft[t].rnd_key_den, ctl->cycle), c);
 }
@@ -103,6 +116,7 @@ __global__ void k_tuft_cells(const uint8_t* __restrict__ axns, const SliceRec* _
 __global__ void __launch_bounds__(128) k_inhib_mtp(uint8_t* __restrict__ axns, const SliceRec* __restrict__ slices,
                                                    DevLayer L, int radius, uint64_t key, int learn,
                                                    const AreaCtl* ctl) {
+    pdl_begin();
     uint32_t c = (uint32_t)gtid();
     inhib_mtp_warp(axns, slices, L, radius, rnd_at(key, ctl->cycle), rnd_at(L.rnd_key_ssc_mtp, ctl->cycle),
                    learn != 0, c, c < L.cells);
@@ -110,6 +124,7 @@ __global__ void __launch_bounds__(128) k_inhib_mtp(uint8_t* __restrict__ axns, c
 
 __global__ void __launch_bounds__(128) k_pyr_tail(uint8_t* __restrict__ axns, const SliceRec* __restrict__ slices,
                                                   DevLayer L, int ctrl, int learn, const AreaCtl* ctl) {
+    pdl_begin();
     const uint64_t i = gtid();
     pyr_tail_warp(axns, slices, L, ctrl, learn != 0, ctl, (uint32_t)i, i < tail_items(L.depth, L.v_size * L.u_size));
 }
@@ -122,65 +137,65 @@ inline unsigned nblk(uint64_t n, unsigned b) { return (unsigned)((n + b - 1) / b
 void launch_set_syn_flags(const DevLayer& L, cudaStream_t s) {
     uint64_t n = L.n_syns;
     if (!n) return;
-    k_set_syn_flags<<<nblk((n + 15) / 16, 256), 256, 0, s>>>(L.buf[BM_BUF_SYN_STATES], L.buf[BM_BUF_SYN_FLAG_SETS], n);
+    launch_pdl(k_set_syn_flags, nblk((n + 15) / 16, 256), 256, 0, s, L.buf[BM_BUF_SYN_STATES], L.buf[BM_BUF_SYN_FLAG_SETS], n);
 }
 void launch_set_syn_flags_tuft(const DevLayer& L, uint32_t t, cudaStream_t s) {
     const DevTuft& T = L.tft[t];
     uint64_t n = (uint64_t)L.cells * T.spt;
     if (!n) return;
-    k_set_syn_flags<<<nblk((n + 15) / 16, 256), 256, 0, s>>>(L.buf[BM_BUF_SYN_STATES] + T.syn_idz,
+    launch_pdl(k_set_syn_flags, nblk((n + 15) / 16, 256), 256, 0, s, L.buf[BM_BUF_SYN_STATES] + T.syn_idz,
                                                               L.buf[BM_BUF_SYN_FLAG_SETS] + T.syn_idz, n);
 }
 void launch_syn_cycle_plain(const uint8_t* axns, const SliceRec* slices, const DevLayer& L, uint32_t t,
                             cudaStream_t s) {
     uint64_t n = (uint64_t)L.cells * L.tft[t].spt;
-    k_syn_cycle<<<nblk(n, 256), 256, 0, s>>>(axns, slices, L, t);
+    launch_pdl(k_syn_cycle, nblk(n, 256), 256, 0, s, axns, slices, L, t);
 }
 void launch_den_cycle_plain(const DevLayer& L, uint32_t t, const AreaCtl* ctl, cudaStream_t s) {
     uint64_t n = (uint64_t)L.cells * L.tft[t].dpt;
-    k_den_cycle<<<nblk(n, 256), 256, 0, s>>>(L, t, ctl);
+    launch_pdl(k_den_cycle, nblk(n, 256), 256, 0, s, L, t, ctl);
 }
 void launch_tft_cycle_plain(const DevLayer& L, uint32_t t, cudaStream_t s) {
-    k_tft_cycle<<<nblk(L.cells, 256), 256, 0, s>>>(L, t);
+    launch_pdl(k_tft_cycle, nblk(L.cells, 256), 256, 0, s, L, t);
 }
 void launch_ssc_cycle(const DevLayer& L, cudaStream_t s) {
-    k_ssc_cycle<<<nblk(L.cells, 256), 256, 0, s>>>(L);
+    launch_pdl(k_ssc_cycle, nblk(L.cells, 256), 256, 0, s, L);
 }
 void launch_inhib_simple(uint8_t* axns, const SliceRec* slices, const DevLayer& L, int radius, uint64_t key,
                          const AreaCtl* ctl, cudaStream_t s) {
-    k_inhib_simple<<<nblk(L.cells, 128), 128, 0, s>>>(axns, slices, L, radius, key, ctl);
+    launch_pdl(k_inhib_simple, nblk(L.cells, 128), 128, 0, s, axns, slices, L, radius, key, ctl);
 }
 void launch_inhib_passthrough(uint8_t* axns, const SliceRec* slices, const DevLayer& L, cudaStream_t s) {
-    k_inhib_passthrough<<<nblk(L.cells, 256), 256, 0, s>>>(axns, slices, L);
+    launch_pdl(k_inhib_passthrough, nblk(L.cells, 256), 256, 0, s, axns, slices, L);
 }
 void launch_ssc_mtp_plain(const uint8_t* axns, const DevLayer& L, const AreaCtl* ctl, cudaStream_t s) {
-    k_ssc_mtp_simple<<<nblk(L.cells, 128), 128, 0, s>>>(axns, L, ctl);
+    launch_pdl(k_ssc_mtp_simple, nblk(L.cells, 128), 128, 0, s, axns, L, ctl);
 }
 void launch_pyr_cycle_plain(const DevLayer& L, cudaStream_t s) {
-    k_pyr_cycle<<<nblk(L.cells, 256), 256, 0, s>>>(L);
+    launch_pdl(k_pyr_cycle, nblk(L.cells, 256), 256, 0, s, L);
 }
 void launch_pyr_output(uint8_t* axns, const SliceRec* slices, const DevLayer& L, cudaStream_t s) {
-    k_pyr_output<<<nblk(L.cells, 256), 256, 0, s>>>(axns, slices, L);
+    launch_pdl(k_pyr_output, nblk(L.cells, 256), 256, 0, s, axns, slices, L);
 }
 void launch_inhib_intra_column_plain(uint8_t* axns, const SliceRec* slices, const DevLayer& L, cudaStream_t s) {
-    k_inhib_intra_column<<<nblk((uint64_t)L.v_size * L.u_size, 256), 256, 0, s>>>(axns, slices, L);
+    launch_pdl(k_inhib_intra_column, nblk((uint64_t)L.v_size * L.u_size, 256), 256, 0, s, axns, slices, L);
 }
 void launch_tuft_cells(const uint8_t* axns, const SliceRec* slices, const DevLayer& L, uint32_t t,
                        const AreaCtl* ctl, cudaStream_t s) {
-    k_tuft_cells<<<nblk(L.cells, 128), 128, 0, s>>>(axns, slices, L, t, ctl);
+    launch_pdl(k_tuft_cells, nblk(L.cells, 128), 128, 0, s, axns, slices, L, t, ctl);
 }
 void launch_inhib_mtp(uint8_t* axns, const SliceRec* slices, const DevLayer& L, int radius, uint64_t key,
                       bool learn, const AreaCtl* ctl, cudaStream_t s) {
-    k_inhib_mtp<<<nblk(L.cells, 128), 128, 0, s>>>(axns, slices, L, radius, key, learn ? 1 : 0, ctl);
+    launch_pdl(k_inhib_mtp, nblk(L.cells, 128), 128, 0, s, axns, slices, L, radius, key, learn ? 1 : 0, ctl);
 }
 void launch_pyr_tail(uint8_t* axns, const SliceRec* slices, const DevLayer& L, int ctrl, bool learn,
                      const AreaCtl* ctl, cudaStream_t s) {
-    k_pyr_tail<<<nblk(tail_items(L.depth, L.v_size * L.u_size), 128), 128, 0, s>>>(axns, slices, L, ctrl,
+    launch_pdl(k_pyr_tail, nblk(tail_items(L.depth, L.v_size * L.u_size), 128), 128, 0, s, axns, slices, L, ctrl,
                                                                                    learn ? 1 : 0, ctl);
 }
 void launch_tft_dst_mtp_plain(const uint8_t* axns, const DevLayer& L, uint32_t t, const AreaCtl* ctl,
                               cudaStream_t s) {
-    k_tft_dst_mtp<<<nblk(L.cells, 128), 128, 0, s>>>(axns, L, t, ctl);
+    launch_pdl(k_tft_dst_mtp, nblk(L.cells, 128), 128, 0, s, axns, L, t, ctl);
 }
 
 }  // namespace bm
