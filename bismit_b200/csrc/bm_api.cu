@@ -246,6 +246,80 @@ void bm::exec_step(bm_area_s* A, const Step& st, cudaStream_t s) {
     }
 }
 
+namespace {
+
+void layer_axons(const bm_area_plan& P, uint32_t i, std::bitset<BM_MAX_SLICES>& out) {
+    const bm_layer_plan& L = P.layers[i];
+    for (uint32_t k = 0; k < L.depth && L.base_axn_slc + k < BM_MAX_SLICES; k++) out.set(L.base_axn_slc + k);
+}
+
+void tuft_sources(const bm_area_plan& P, uint32_t i, uint32_t t, std::bitset<BM_MAX_SLICES>& out) {
+    const bm_tuft_plan& T = P.layers[i].tufts[t];
+    for (uint32_t k = 0; k < T.n_src_uniq; k++) out.set(T.src_uniq_slc_ids[k]);
+}
+
+uint64_t tuft_bit(uint32_t i, uint32_t t) { return 1ull << (i * BM_MAX_TUFTS + t); }
+uint64_t layer_tufts(const bm_area_plan& P, uint32_t i) {
+    uint64_t m = 0;
+    for (uint32_t t = 0; t < P.layers[i].n_tufts; t++) m |= tuft_bit(i, t);
+    return m;
+}
+
+}  // namespace
+
+// Reads and writes of each step kind (the item bodies in bm_items.cuh, the
+// fused kernels in bm_fused.cu); learning steps are taken to read every axon.
+bm::StepAccess bm::step_access(const bm_area_s* A, const Step& st, int t) {
+    const bm_area_plan& P = A->plan;
+    const uint32_t i = st.layer;
+    StepAccess a;
+    switch (st.kind) {
+    case ST_TUFT: {
+        const uint32_t tt = t >= 0 ? (uint32_t)t : st.idx;
+        tuft_sources(P, i, tt, a.ax_r);
+        a.tf_r = a.tf_w = tuft_bit(i, tt);
+        break;
+    }
+    case ST_TUFTS_PLAIN:
+        for (uint32_t k = 0; k < P.layers[i].n_tufts; k++) tuft_sources(P, i, k, a.ax_r);
+        a.tf_r = a.tf_w = layer_tufts(P, i);
+        break;
+    case ST_SSC_CYCLE:
+    case ST_PYR_CYCLE:
+        a.tf_r = layer_tufts(P, i);
+        a.ce_r = a.ce_w = 1u << i;
+        break;
+    case ST_INHIB_SIMPLE:
+    case ST_INHIB_PASS:
+        a.ce_r = a.ce_w = 1u << i;
+        layer_axons(P, i, a.ax_w);
+        break;
+    case ST_INHIB_MTP:
+    case ST_SSC_MTP:
+        a.ce_r = a.ce_w = 1u << i;
+        layer_axons(P, i, a.ax_w);
+        a.ax_r = a.ax_w;
+        a.tf_r = a.tf_w = layer_tufts(P, i);
+        break;
+    case ST_PYR_OUTPUT:
+    case ST_INTRA_COL:
+        a.ce_r = 1u << i;
+        layer_axons(P, i, a.ax_w);
+        break;
+    case ST_DST_MTP:
+    case ST_PYR_TAIL:
+        a.ax_r.set();
+        layer_axons(P, i, a.ax_w);
+        a.tf_r = a.tf_w = layer_tufts(P, i);
+        a.ce_r = a.ce_w = 1u << i;
+        break;
+    default:
+        a.all = true;
+        break;
+    }
+    return a;
+}
+
 void bm::run_pending_verifies(bm_area_s* A, cudaStream_t s) {
     bool any = false;
     for (uint32_t i = 0; i < A->plan.n_layers; i++)

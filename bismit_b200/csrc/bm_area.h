@@ -2,6 +2,7 @@
 // per-area stage program (the ordered steps of one cycle) that the one-area
 // path and the batched path (bm_batch.cu) both execute.
 #pragma once
+#include <bitset>
 #include <vector>
 
 #include "bm_fused.h"
@@ -59,6 +60,31 @@ struct Step {
         return kind == o.kind && layer == o.layer && idx == o.idx && arg == o.arg;
     }
 };
+
+// What a step of one area reads and writes, at the granularity its kernels
+// touch: axon slices, the synapse / dendrite / cell-tuft arrays of one tuft of
+// a layer, and the cell arrays of a layer. Two steps of an area whose accesses
+// do not conflict may run concurrently.
+struct StepAccess {
+    std::bitset<BM_MAX_SLICES> ax_r, ax_w;
+    uint64_t tf_r = 0, tf_w = 0;   // bit layer * BM_MAX_TUFTS + tuft
+    uint32_t ce_r = 0, ce_w = 0;   // bit layer
+    bool all = false;              // touches everything (regrowth, the cycle end)
+    StepAccess& operator|=(const StepAccess& o) {
+        ax_r |= o.ax_r; ax_w |= o.ax_w;
+        tf_r |= o.tf_r; tf_w |= o.tf_w;
+        ce_r |= o.ce_r; ce_w |= o.ce_w;
+        all = all || o.all;
+        return *this;
+    }
+};
+inline bool conflict(const StepAccess& a, const StepAccess& b) {
+    if (a.all || b.all) return true;
+    if ((a.ax_w & (b.ax_r | b.ax_w)).any() || (b.ax_w & a.ax_r).any()) return true;
+    if ((a.tf_w & (b.tf_r | b.tf_w)) || (b.tf_w & a.tf_r)) return true;
+    if ((a.ce_w & (b.ce_r | b.ce_w)) || (b.ce_w & a.ce_r)) return true;
+    return false;
+}
 
 }  // namespace bm
 
@@ -144,6 +170,9 @@ void exec_step(bm_area_s* A, const Step& st, cudaStream_t s);
 void run_pending_verifies(bm_area_s* A, cudaStream_t s);
 // Rebuilds A->geo (the tiled tufts' footprint geometry that regrowth uses).
 void refresh_geo(bm_area_s* A);
+// The accesses of step st of A; for a tuft step, of tuft `t` (the step's own
+// tuft unless given).
+StepAccess step_access(const bm_area_s* A, const Step& st, int t = -1);
 int cuda_err(cudaError_t e, const char* what);
 
 }  // namespace bm

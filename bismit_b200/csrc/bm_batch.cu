@@ -195,6 +195,8 @@ struct bm_batch_s {
         Form form = F_EACH;
         std::vector<CellLaunch> cells;   // F_CELLS: launches in order
         FusedBatch fb;
+        bool side = false;               // runs on the side stream (no conflict with any earlier main step)
+        std::vector<size_t> waits;       // side steps this main step must wait for
         RegrowJob* d_regrow = nullptr;   // F_REGROW: every area's regrowth jobs, one launch
         uint32_t n_regrow = 0, regrow_blocks = 0;
         // Profiling (eager cycles only): launches and device milliseconds.
@@ -239,6 +241,13 @@ struct bm_batch_s {
     AreaCtl** d_ctls = nullptr;
     bool use_graph = true;
     cudaStream_t cap = nullptr;          // private stream for graph capture
+    // Side stream: tuft steps that depend on nothing earlier in the cycle
+    // (e.g. the pyramidal distal tufts, which read only the previous cycle's
+    // axons) run beside the main stream's chain of dependent steps.
+    cudaStream_t side = nullptr;
+    cudaEvent_t ev_fork = nullptr;
+    std::vector<cudaEvent_t> side_ev;    // per plan step (side steps only)
+    size_t last_side = SIZE_MAX;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
 
@@ -273,6 +282,10 @@ void free_batch(bm_batch_s* B) {
     if (B->d_bctl) cudaFree(B->d_bctl);
     if (B->d_ctls) cudaFree(B->d_ctls);
     if (B->cap) cudaStreamDestroy(B->cap);
+    if (B->side) cudaStreamDestroy(B->side);
+    if (B->ev_fork) cudaEventDestroy(B->ev_fork);
+    for (cudaEvent_t e : B->side_ev)
+        if (e) cudaEventDestroy(e);
     for (auto& r : B->pending) { cudaEventDestroy(r.a); cudaEventDestroy(r.b); }
     for (auto e : B->pool) cudaEventDestroy(e);
     delete B;
@@ -453,6 +466,65 @@ void count_launches(bm_batch_s* B) {
     B->plan_launches = n;
 }
 
+// The accesses of plan step p for area A (a merged tuft step: every tuft of
+// A in it).
+StepAccess plan_access(const bm_batch_s::StepPlan& p, bm_area A) {
+    if (p.st.kind == ST_TUFT && !p.tufts.empty()) {
+        StepAccess a;
+        for (auto& [B, t] : p.tufts)
+            if (B == A) a |= step_access(A, p.st, (int)t);
+        return a;
+    }
+    return step_access(A, p.st);
+}
+
+// Splits the schedule over two streams: a tuft step whose accesses conflict,
+// in no area, with any earlier step left on the main stream goes to the side
+// stream (side steps keep their order there); a main step waits for every
+// earlier side step it conflicts with, and the cycle end for all of them.
+int schedule_side(bm_batch_s* B) {
+    const size_t n = B->plan.size();
+    B->last_side = SIZE_MAX;
+    std::vector<std::vector<std::pair<bm_area, StepAccess>>> acc(n);
+    for (size_t k = 0; k < n; k++)
+        for (bm_area A : B->plan[k].areas) acc[k].push_back({A, plan_access(B->plan[k], A)});
+    auto clash = [&](size_t j, size_t k) {
+        for (auto& [a, x] : acc[j])
+            for (auto& [b, y] : acc[k])
+                if (a == b && conflict(x, y)) return true;
+        return false;
+    };
+    for (size_t k = 0; k < n; k++) {
+        auto& p = B->plan[k];
+        p.side = false;
+        p.waits.clear();
+        if ((p.st.kind != ST_TUFT && p.st.kind != ST_TUFTS_PLAIN) || p.form == bm_batch_s::F_END) continue;
+        bool free = true;
+        for (size_t j = 0; j < k && free; j++)
+            if (!B->plan[j].side && clash(j, k)) free = false;
+        p.side = free;
+    }
+    for (size_t k = 0; k < n; k++) {
+        if (B->plan[k].side) {
+            B->last_side = k;
+            continue;
+        }
+        for (size_t j = 0; j < k; j++)
+            if (B->plan[j].side && clash(j, k)) B->plan[k].waits.push_back(j);
+    }
+    if (B->last_side == SIZE_MAX) return BM_OK;
+    cudaError_t e = cudaSuccess;
+    if (!B->side) e = cudaStreamCreateWithFlags(&B->side, cudaStreamNonBlocking);
+    if (e == cudaSuccess && !B->ev_fork) e = cudaEventCreateWithFlags(&B->ev_fork, cudaEventDisableTiming);
+    for (cudaEvent_t ev : B->side_ev)
+        if (ev) cudaEventDestroy(ev);
+    B->side_ev.assign(n, nullptr);
+    for (size_t k = 0; k < n && e == cudaSuccess; k++)
+        if (B->plan[k].side) e = cudaEventCreateWithFlags(&B->side_ev[k], cudaEventDisableTiming);
+    if (e != cudaSuccess) return cuda_err(e, "side stream");
+    return BM_OK;
+}
+
 // The schedule: the shortest common supersequence of the areas' stage
 // programs (merged one distinct program at a time through their longest
 // common subsequence), each step run over the areas that have it. Areas are
@@ -511,7 +583,7 @@ int build_plan(bm_batch_s* B) {
     int rc = merge_tuft_steps(B);
     if (rc != BM_OK) return rc;
     count_launches(B);
-    return BM_OK;
+    return schedule_side(B);
 }
 
 // The head-of-cycle copies: every tract, then every input of every area that
@@ -561,12 +633,22 @@ int build_intake(bm_batch_s* B) {
     return BM_OK;
 }
 
-void enqueue_batch_cycle(bm_batch_s* B, cudaStream_t s) {
+void enqueue_batch_cycle(bm_batch_s* B, cudaStream_t main) {
     if (B->intake_blocks)
-        launch_pdl(k_batch_intake, B->intake_blocks, kIntakeBlock, 0, s, B->d_intake, B->n_intake, B->d_bctl);
-    const bool prof = B->profiling && s != B->cap;
+        launch_pdl(k_batch_intake, B->intake_blocks, kIntakeBlock, 0, main, B->d_intake, B->n_intake, B->d_bctl);
+    const bool prof = B->profiling && main != B->cap;
+    // Profiling times each step on its own: everything on the main stream.
+    const bool fork = !prof && B->last_side != SIZE_MAX;
+    if (fork) {
+        cudaEventRecord(B->ev_fork, main);
+        cudaStreamWaitEvent(B->side, B->ev_fork, 0);
+    }
     for (size_t k = 0; k < B->plan.size(); k++) {
         auto& p = B->plan[k];
+        const bool on_side = fork && p.side;
+        cudaStream_t s = on_side ? B->side : main;
+        if (fork && !on_side)
+            for (size_t j : p.waits) cudaStreamWaitEvent(main, B->side_ev[j], 0);
         bm_batch_s::Rec r{k, nullptr, nullptr};
         if (prof && p.form != bm_batch_s::F_END) {
             r.a = B->ev();
@@ -588,9 +670,11 @@ void enqueue_batch_cycle(bm_batch_s* B, cudaStream_t s) {
             cudaEventRecord(r.b, s);
             B->pending.push_back(r);
         }
+        if (on_side) cudaEventRecord(B->side_ev[k], B->side);
     }
+    if (fork) cudaStreamWaitEvent(main, B->side_ev[B->last_side], 0);   // the side stream rejoins
     const uint32_t n = (uint32_t)B->areas.size();
-    launch_pdl(k_batch_cycle_end, (n + 127) / 128, 128, 0, s, B->d_ctls, n, B->d_bctl);
+    launch_pdl(k_batch_cycle_end, (n + 127) / 128, 128, 0, main, B->d_ctls, n, B->d_bctl);
 }
 
 int ensure_graph(bm_batch_s* B) {
