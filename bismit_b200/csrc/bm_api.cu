@@ -194,7 +194,7 @@ void bm::exec_step(bm_area_s* A, const Step& st, cudaStream_t s) {
     const bool pyr = L.kind == BM_LYR_PYRAMIDAL;
     // Launches on the area's own stream are counted (and timed when profiling);
     // a batch passes its own stream and does its own counting.
-    const bool own = s == A->stream();
+    const bool own = s == A->stream() || (A->side && s == A->side);
     auto run = [&](int kind, auto&& f) {
         if (own) A->run(kind, f);
         else f();
@@ -320,6 +320,44 @@ bm::StepAccess bm::step_access(const bm_area_s* A, const Step& st, int t) {
     return a;
 }
 
+// A tuft step whose accesses conflict with no earlier step left on the main
+// stream runs on the side stream (side steps keep their order there); a main
+// step waits for each earlier side step it conflicts with, and the cycle's end
+// for all of them. Concurrent steps touch disjoint bytes, so the result is
+// the sequential program's.
+int bm::schedule_area(bm_area_s* A) {
+    const size_t n = A->steps.size();
+    std::vector<StepAccess> acc(n);
+    for (size_t k = 0; k < n; k++) acc[k] = step_access(A, A->steps[k]);
+    A->step_side.assign(n, 0);
+    A->step_waits.assign(n, {});
+    A->last_side = SIZE_MAX;
+    for (size_t k = 0; k < n; k++) {
+        const uint8_t kind = A->steps[k].kind;
+        if (kind != ST_TUFT && kind != ST_TUFTS_PLAIN) continue;
+        bool free = true;
+        for (size_t j = 0; j < k && free; j++)
+            if (!A->step_side[j] && conflict(acc[j], acc[k])) free = false;
+        A->step_side[k] = free;
+    }
+    for (size_t k = 0; k < n; k++) {
+        if (A->step_side[k]) {
+            A->last_side = k;
+            continue;
+        }
+        for (size_t j = 0; j < k; j++)
+            if (A->step_side[j] && conflict(acc[j], acc[k])) A->step_waits[k].push_back(j);
+    }
+    if (A->last_side == SIZE_MAX) return BM_OK;
+    cudaError_t e = cudaStreamCreateWithFlags(&A->side, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&A->ev_fork, cudaEventDisableTiming);
+    A->side_ev.assign(n, nullptr);
+    for (size_t k = 0; k < n && e == cudaSuccess; k++)
+        if (A->step_side[k]) e = cudaEventCreateWithFlags(&A->side_ev[k], cudaEventDisableTiming);
+    if (e != cudaSuccess) return cuda_err(e, "side stream");
+    return BM_OK;
+}
+
 void bm::run_pending_verifies(bm_area_s* A, cudaStream_t s) {
     bool any = false;
     for (uint32_t i = 0; i < A->plan.n_layers; i++)
@@ -352,8 +390,22 @@ namespace {
 
 void enqueue_cycle(bm_area_s* A) {
     A->launches = 0;
-    run_pending_verifies(A, A->stream());
-    for (const Step& st : A->steps) exec_step(A, st, A->stream());
+    cudaStream_t main = A->stream();
+    run_pending_verifies(A, main);
+    // Profiling times each launch on its own: everything on the main stream.
+    const bool fork = !A->profiling && A->last_side != SIZE_MAX;
+    if (fork) {
+        cudaEventRecord(A->ev_fork, main);
+        cudaStreamWaitEvent(A->side, A->ev_fork, 0);
+    }
+    for (size_t k = 0; k < A->steps.size(); k++) {
+        const bool on_side = fork && A->step_side[k];
+        if (fork && !on_side)
+            for (size_t j : A->step_waits[k]) cudaStreamWaitEvent(main, A->side_ev[j], 0);
+        exec_step(A, A->steps[k], on_side ? A->side : main);
+        if (on_side) cudaEventRecord(A->side_ev[k], A->side);
+    }
+    if (fork) cudaStreamWaitEvent(main, A->side_ev[A->last_side], 0);
     A->host_cycle++;
 }
 
@@ -488,6 +540,10 @@ void free_area(bm_area_s* A) {
         if (A->d_regrow) cudaFree(A->d_regrow);
         if (A->grow_offs) cudaFree(A->grow_offs);
         if (A->d_geo) cudaFree(A->d_geo);
+        if (A->side) cudaStreamDestroy(A->side);
+        if (A->ev_fork) cudaEventDestroy(A->ev_fork);
+        for (cudaEvent_t e : A->side_ev)
+            if (e) cudaEventDestroy(e);
         for (auto& r : A->pending) { cudaEventDestroy(r.a); cudaEventDestroy(r.b); }
         for (auto e : A->pool) cudaEventDestroy(e);
     }
@@ -639,6 +695,8 @@ int bm_area_create(bm_ctx ctx, const bm_area_desc* desc, uint64_t seed, bm_area*
     }
     for (uint32_t i = 0; i < A->plan.n_layers; i++) A->verify_pending[i] = true;
     area_steps(A, A->steps);
+    rc = schedule_area(A);
+    if (rc != BM_OK) { free_area(A); return rc; }
     *out = A;
     return BM_OK;
 }

@@ -3,6 +3,7 @@
 // path and the batched path (bm_batch.cu) both execute.
 #pragma once
 #include <bitset>
+#include <cstdint>
 #include <vector>
 
 #include "bm_fused.h"
@@ -117,6 +118,14 @@ struct bm_area_s {
     double prof_ms[bm::K_COUNT] = {};
     uint32_t launches = 0;   // kernel launches of the last enqueued cycle
     std::vector<Step> steps; // the cycle's stage program
+    // Two-stream form of the program (schedule_area): steps on the side
+    // stream, the side steps each main step waits for, events and the stream.
+    std::vector<uint8_t> step_side;
+    std::vector<std::vector<size_t>> step_waits;
+    size_t last_side = SIZE_MAX;
+    cudaStream_t side = nullptr;
+    cudaEvent_t ev_fork = nullptr;
+    std::vector<cudaEvent_t> side_ev;
     uint32_t n_batches = 0;  // batches holding this area (its tiles are retiled only when one does)
     // Regrowth (absent when disabled): one job per (data layer, tuft), layers
     // in cycle order, block0 counted within the area's own launch.
@@ -173,6 +182,8 @@ void refresh_geo(bm_area_s* A);
 // The accesses of step st of A; for a tuft step, of tuft `t` (the step's own
 // tuft unless given).
 StepAccess step_access(const bm_area_s* A, const Step& st, int t = -1);
+// Splits A's program over its stream and a side stream (see step_access).
+int schedule_area(bm_area_s* A);
 int cuda_err(cudaError_t e, const char* what);
 
 }  // namespace bm
