@@ -58,6 +58,7 @@ BUF_NAMES = [
 BM_BUF_COUNT = len(BUF_NAMES)
 BUF = {n: i for i, n in enumerate(BUF_NAMES)}
 BM_BUF_AXON_STATES = 64
+BM_ALL_LAYERS = 0xFFFFFFFF
 SIGNED_BUFS = {"syn_strengths", "syn_src_col_v_offs", "syn_src_col_u_offs"}
 
 BM_RND_DEN_CYCLE, BM_RND_INHIB, BM_RND_SSC_MTP, BM_RND_TFT_DST_MTP = 1, 2, 3, 4
@@ -198,6 +199,14 @@ def lib():
         "bm_area_read": (C.c_int, [vp, u32, u32, u64, vp, u64]),
         "bm_area_write": (C.c_int, [vp, u32, u32, u64, vp, u64]),
         "bm_area_read_slab": (C.c_int, [vp, vp, u64]),
+        "bm_area_side_steps": (C.c_int, [vp, P(u32)]),
+        "bm_sampler_create": (C.c_int, [vp, u32, u32, C.c_int, P(vp)]),
+        "bm_sampler_destroy": (C.c_int, [vp]),
+        "bm_sampler_len": (C.c_int, [vp, P(u64)]),
+        "bm_sampler_set_backpressure": (C.c_int, [vp, C.c_int, P(C.c_int)]),
+        "bm_sampler_set_timeout": (C.c_int, [vp, u32]),
+        "bm_sampler_recv": (C.c_int, [vp, C.c_int, vp, u64, P(u64), P(C.c_int)]),
+        "bm_sampler_stats": (C.c_int, [vp, P(u64), P(u64)]),
         "bm_area_write_slab": (C.c_int, [vp, vp, u64]),
         "bm_area_get_cycle": (C.c_int, [vp, P(u64)]),
         "bm_area_set_cycle": (C.c_int, [vp, u64]),

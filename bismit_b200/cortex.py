@@ -67,6 +67,7 @@ class CorticalArea:
         self.h = C.c_void_p()
         F.check(self.lib.bm_area_create(ctx.h, C.byref(desc), C.c_uint64(seed), C.byref(self.h)))
         self._holders = []
+        self._samplers = []
         ctx._adopt(self)
         self.plan = F.bm_area_plan()
         F.check(self.lib.bm_area_get_plan(self.h, C.byref(self.plan)))
@@ -161,6 +162,17 @@ class CorticalArea:
         F.check(self.lib.bm_area_slab_ptr(self.h, C.byref(p)))
         return p.value
 
+    def side_steps(self):
+        """Steps of the cycle that run beside the chain of dependent steps."""
+        v = C.c_uint32()
+        F.check(self.lib.bm_area_side_steps(self.h, C.byref(v)))
+        return v.value
+
+    def sampler(self, kind, layer=None, backpressure=False):
+        """CorticalArea::sampler: a Sampler over `kind` (a SAMPLER_KINDS name)
+        of data layer `layer` (name or index; for "axons", None = every axon)."""
+        return Sampler(self, kind, layer, backpressure)
+
     # ---- timing ----
     def set_profiling(self, on):
         F.check(self.lib.bm_area_set_profiling(self.h, 1 if on else 0))
@@ -190,6 +202,12 @@ class CorticalArea:
                 if b is not None:
                     b.close()
             self._holders = []
+            # The library destroys the area's samplers with it.
+            for r in self._samplers:
+                smp = r()
+                if smp is not None:
+                    smp.h = C.c_void_p()
+            self._samplers = []
             self.lib.bm_area_destroy(self.h)
             self.h = C.c_void_p()
 
@@ -198,6 +216,82 @@ class CorticalArea:
             self.close()
         except Exception:
             pass
+
+
+# Sampler kinds (SamplerKind, src/cortex/cortical_area.rs:61-90) -> buffer kind.
+SAMPLER_KINDS = {
+    "axons": F.BM_BUF_AXON_STATES,
+    "soma_states": F.BUF["cel_states"], "soma_energies": F.BUF["cel_energies"],
+    "soma_activities": F.BUF["cel_activities"], "soma_flag_sets": F.BUF["cel_flag_sets"],
+    "tuft_states": F.BUF["tft_states"], "tuft_best_den_ids": F.BUF["tft_best_den_ids"],
+    "tuft_best_den_states_raw": F.BUF["tft_best_den_states_raw"],
+    "tuft_best_den_states": F.BUF["tft_best_den_states"], "tuft_prev_states": F.BUF["tft_prev_states"],
+    "tuft_prev_best_den_ids": F.BUF["tft_prev_best_den_ids"],
+    "tuft_prev_best_den_states_raw": F.BUF["tft_prev_best_den_states_raw"],
+    "tuft_prev_best_den_states": F.BUF["tft_prev_best_den_states"],
+    "den_states": F.BUF["den_states"], "den_states_raw": F.BUF["den_states_raw"],
+    "den_energies": F.BUF["den_energies"], "den_activities": F.BUF["den_activities"],
+    "den_thresholds": F.BUF["den_thresholds"],
+    "syn_states": F.BUF["syn_states"], "syn_strengths": F.BUF["syn_strengths"],
+    "syn_src_slc_ids": F.BUF["syn_src_slc_ids"], "syn_src_col_v_offs": F.BUF["syn_src_col_v_offs"],
+    "syn_src_col_u_offs": F.BUF["syn_src_col_u_offs"], "syn_flag_sets": F.BUF["syn_flag_sets"],
+}
+SIGNED_KINDS = {"syn_strengths", "syn_src_col_v_offs", "syn_src_col_u_offs"}
+
+
+class Sampler:
+    """Per-cycle readback of one buffer of an area (CorticalArea::sampler,
+    src/cortex/cortical_area.rs:1017-1284) through a one-frame channel with
+    the tract channel's send / skip / backpressure rules
+    (src/subcortex/tract_channel.rs:400-488); bm_sampler_* in
+    include/bismit_b200.h."""
+
+    def __init__(self, area, kind, layer=None, backpressure=False):
+        self.lib = F.lib()
+        self.area = area
+        self.kind = kind
+        buf = SAMPLER_KINDS[kind]
+        if layer is None:
+            if kind != "axons":
+                raise ValueError("sampler %r needs a layer" % kind)
+            li = F.BM_ALL_LAYERS
+        else:
+            li = area.data_layer(layer) if isinstance(layer, str) else int(layer)
+        self.h = C.c_void_p()
+        F.check(self.lib.bm_sampler_create(area.h, buf, li, 1 if backpressure else 0, C.byref(self.h)))
+        n = C.c_uint64()
+        F.check(self.lib.bm_sampler_len(self.h, C.byref(n)))
+        self.len = n.value
+        area._samplers.append(weakref.ref(self))
+
+    def recv(self, wait_for_frame=False):
+        """(cycle, frame) of the unread frame, or None (TractReceiver::recv)."""
+        out = np.empty(self.len, np.uint8)
+        cyc = C.c_uint64()
+        got = C.c_int()
+        F.check(self.lib.bm_sampler_recv(self.h, 1 if wait_for_frame else 0, out.ctypes.data, self.len,
+                                         C.byref(cyc), C.byref(got)))
+        if not got.value:
+            return None
+        return cyc.value, (out.view(np.int8) if self.kind in SIGNED_KINDS else out)
+
+    def set_backpressure(self, on):
+        prior = C.c_int()
+        F.check(self.lib.bm_sampler_set_backpressure(self.h, 1 if on else 0, C.byref(prior)))
+        return bool(prior.value)
+
+    def set_timeout(self, ms):
+        F.check(self.lib.bm_sampler_set_timeout(self.h, int(ms)))
+
+    def stats(self):
+        sent, skipped = C.c_uint64(), C.c_uint64()
+        F.check(self.lib.bm_sampler_stats(self.h, C.byref(sent), C.byref(skipped)))
+        return {"sent": sent.value, "skipped": skipped.value}
+
+    def close(self):
+        if self.h and self.area.h:
+            self.lib.bm_sampler_destroy(self.h)
+        self.h = C.c_void_p()
 
 
 class Batch:

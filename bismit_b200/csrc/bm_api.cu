@@ -276,12 +276,15 @@ bm::StepAccess bm::step_access(const bm_area_s* A, const Step& st, int t) {
     switch (st.kind) {
     case ST_TUFT: {
         const uint32_t tt = t >= 0 ? (uint32_t)t : st.idx;
-        tuft_sources(P, i, tt, a.ax_r);
+        if ((A->foreign_src[i] >> tt) & 1) a.ax_r.set();   // sources anywhere: any slice
+        else tuft_sources(P, i, tt, a.ax_r);
         a.tf_r = a.tf_w = tuft_bit(i, tt);
         break;
     }
     case ST_TUFTS_PLAIN:
-        for (uint32_t k = 0; k < P.layers[i].n_tufts; k++) tuft_sources(P, i, k, a.ax_r);
+        if (A->foreign_src[i]) a.ax_r.set();
+        else
+            for (uint32_t k = 0; k < P.layers[i].n_tufts; k++) tuft_sources(P, i, k, a.ax_r);
         a.tf_r = a.tf_w = layer_tufts(P, i);
         break;
     case ST_SSC_CYCLE:
@@ -325,6 +328,37 @@ bm::StepAccess bm::step_access(const bm_area_s* A, const Step& st, int t) {
 // step waits for each earlier side step it conflicts with, and the cycle's end
 // for all of them. Concurrent steps touch disjoint bytes, so the result is
 // the sequential program's.
+// Records which tufts of layer i may hold source slice ids outside their
+// pools after the caller wrote slice ids [b, e) of the layer (`data`, or
+// null when the bytes are not known here). With `exact` the write covered the
+// whole layer and replaces the record; else it can only add to it.
+void bm::note_sources(bm_area_s* A, uint32_t i, uint64_t b, uint64_t e, const uint8_t* data, bool exact) {
+    const bm_layer_plan& L = A->plan.layers[i];
+    uint8_t mark = 0;
+    for (uint32_t t = 0; t < L.n_tufts; t++) {
+        const bm_tuft_plan& T = L.tufts[t];
+        const uint64_t lo = std::max<uint64_t>(b, T.syn_idz);
+        const uint64_t hi = std::min<uint64_t>(e, T.syn_idz + (uint64_t)L.cells * T.syns_per_tft);
+        if (lo >= hi) continue;
+        if (!data) {
+            mark |= (uint8_t)(1u << t);
+            continue;
+        }
+        bool pool[256] = {};
+        for (uint32_t k = 0; k < T.n_src_uniq; k++) pool[T.src_uniq_slc_ids[k]] = true;
+        for (uint64_t x = lo; x < hi; x++)
+            if (!pool[data[x - b]]) {
+                mark |= (uint8_t)(1u << t);
+                break;
+            }
+    }
+    const uint8_t next = exact ? mark : (uint8_t)(A->foreign_src[i] | mark);
+    if (next == A->foreign_src[i]) return;
+    A->foreign_src[i] = next;
+    A->access_version++;
+    schedule_area(A);
+}
+
 int bm::schedule_area(bm_area_s* A) {
     const size_t n = A->steps.size();
     std::vector<StepAccess> acc(n);
@@ -348,9 +382,13 @@ int bm::schedule_area(bm_area_s* A) {
         for (size_t j = 0; j < k; j++)
             if (A->step_side[j] && conflict(acc[j], acc[k])) A->step_waits[k].push_back(j);
     }
+    for (cudaEvent_t ev : A->side_ev)
+        if (ev) cudaEventDestroy(ev);
+    A->side_ev.clear();
     if (A->last_side == SIZE_MAX) return BM_OK;
-    cudaError_t e = cudaStreamCreateWithFlags(&A->side, cudaStreamNonBlocking);
-    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&A->ev_fork, cudaEventDisableTiming);
+    cudaError_t e = cudaSuccess;
+    if (!A->side) e = cudaStreamCreateWithFlags(&A->side, cudaStreamNonBlocking);
+    if (e == cudaSuccess && !A->ev_fork) e = cudaEventCreateWithFlags(&A->ev_fork, cudaEventDisableTiming);
     A->side_ev.assign(n, nullptr);
     for (size_t k = 0; k < n && e == cudaSuccess; k++)
         if (A->step_side[k]) e = cudaEventCreateWithFlags(&A->side_ev[k], cudaEventDisableTiming);
@@ -388,7 +426,7 @@ void bm::refresh_geo(bm_area_s* A) {
 
 namespace {
 
-void enqueue_cycle(bm_area_s* A) {
+int enqueue_cycle(bm_area_s* A) {
     A->launches = 0;
     cudaStream_t main = A->stream();
     run_pending_verifies(A, main);
@@ -407,6 +445,7 @@ void enqueue_cycle(bm_area_s* A) {
     }
     if (fork) cudaStreamWaitEvent(main, A->side_ev[A->last_side], 0);
     A->host_cycle++;
+    return A->samplers.empty() ? BM_OK : sample_after_cycle(A, main);
 }
 
 bool buf_range(bm_area_s* A, uint32_t kind, uint32_t layer, uint64_t offset, uint64_t len, uint64_t* off_out) {
@@ -536,6 +575,7 @@ void free_area(bm_area_s* A) {
         if (A->slab) cudaFree(A->slab);
         if (A->ctl) cudaFree(A->ctl);
         if (A->slices) cudaFree(A->slices);
+        free_samplers(A);
         free_fused(A->fused);
         if (A->d_regrow) cudaFree(A->d_regrow);
         if (A->grow_offs) cudaFree(A->grow_offs);
@@ -749,7 +789,10 @@ int bm_area_write_input_device(bm_area area, uint32_t input_idx, const void* dev
 int bm_area_cycle(bm_area area, uint32_t n_cycles) {
     if (!area) return set_err(BM_ERR_INVALID, "null area");
     DevGuard g(area->ctx->device);
-    for (uint32_t k = 0; k < n_cycles; k++) enqueue_cycle(area);
+    for (uint32_t k = 0; k < n_cycles; k++) {
+        const int rc = enqueue_cycle(area);
+        if (rc != BM_OK) return rc;
+    }
     CU(cudaGetLastError());
     return BM_OK;
 }
@@ -765,7 +808,8 @@ int bm_area_cycle_frames_device(bm_area area, const void* dev_frames, size_t fra
             cudaMemcpyAsync(area->axns() + P.inputs[0].axn_idz, (const uint8_t*)dev_frames + (uint64_t)k * frame_len,
                             frame_len, cudaMemcpyDeviceToDevice, area->stream());
         });
-        enqueue_cycle(area);
+        const int rc = enqueue_cycle(area);
+        if (rc != BM_OK) return rc;
     }
     CU(cudaGetLastError());
     return BM_OK;
@@ -802,6 +846,8 @@ int bm_area_write(bm_area area, uint32_t buf_kind, uint32_t layer, uint64_t offs
     DevGuard g(area->ctx->device);
     if (len) CU(cudaMemcpyAsync(area->slab + off, src, len, cudaMemcpyHostToDevice, area->stream()));
     CU(cudaStreamSynchronize(area->stream()));
+    if (buf_kind == BM_BUF_SYN_SRC_SLC_IDS && len)
+        note_sources(area, layer, offset, offset + len, (const uint8_t*)src, false);
     if (buf_kind == BM_BUF_SYN_SRC_SLC_IDS || buf_kind == BM_BUF_SYN_SRC_COL_V_OFFS ||
         buf_kind == BM_BUF_SYN_SRC_COL_U_OFFS || buf_kind == BM_BUF_SYN_FLAG_SETS)
         area->verify_pending[layer] = true;
@@ -824,13 +870,18 @@ int bm_area_write_slab(bm_area area, const void* src, uint64_t len) {
     DevGuard g(area->ctx->device);
     CU(cudaMemcpyAsync(area->slab, src, len, cudaMemcpyHostToDevice, area->stream()));
     CU(cudaStreamSynchronize(area->stream()));
-    for (uint32_t i = 0; i < area->plan.n_layers; i++) area->verify_pending[i] = true;
+    for (uint32_t i = 0; i < area->plan.n_layers; i++) {
+        area->verify_pending[i] = true;
+        const bm_layer_plan& L = area->plan.layers[i];
+        note_sources(area, i, 0, L.n_syns, (const uint8_t*)src + L.buf_off[BM_BUF_SYN_SRC_SLC_IDS], true);
+    }
     return BM_OK;
 }
 
 int bm_area_sources_changed(bm_area area, uint32_t layer) {
     if (!area || layer >= area->plan.n_layers) return set_err(BM_ERR_INVALID, "bad area or layer");
     area->verify_pending[layer] = true;
+    note_sources(area, layer, 0, area->plan.layers[layer].n_syns, nullptr, false);   // written on the device: unknown
     return BM_OK;
 }
 
@@ -859,6 +910,14 @@ int bm_area_set_cycle(bm_area area, uint64_t cycle) {
     CU(cudaMemcpyAsync(&area->ctl->cycle, &c, sizeof c, cudaMemcpyHostToDevice, area->stream()));
     CU(cudaStreamSynchronize(area->stream()));
     area->host_cycle = cycle;
+    return BM_OK;
+}
+
+int bm_area_side_steps(bm_area area, uint32_t* n) {
+    if (!area || !n) return set_err(BM_ERR_INVALID, "null argument");
+    uint32_t c = 0;
+    for (uint8_t x : area->step_side) c += x;
+    *n = c;
     return BM_OK;
 }
 

@@ -126,6 +126,11 @@ struct bm_area_s {
     cudaStream_t side = nullptr;
     cudaEvent_t ev_fork = nullptr;
     std::vector<cudaEvent_t> side_ev;
+    std::vector<bm_sampler_s*> samplers;   // per-cycle readback channels (bm_sampler.cu)
+    // Per data layer, bit t: tuft t may hold source slice ids outside its
+    // pool (written by the caller), so its steps may read any axon slice.
+    uint8_t foreign_src[BM_MAX_LAYERS] = {};
+    uint32_t access_version = 0;   // bumped whenever foreign_src changes
     uint32_t n_batches = 0;  // batches holding this area (its tiles are retiled only when one does)
     // Regrowth (absent when disabled): one job per (data layer, tuft), layers
     // in cycle order, block0 counted within the area's own launch.
@@ -184,6 +189,12 @@ void refresh_geo(bm_area_s* A);
 StepAccess step_access(const bm_area_s* A, const Step& st, int t = -1);
 // Splits A's program over its stream and a side stream (see step_access).
 int schedule_area(bm_area_s* A);
+// Records caller-written source slice ids of layer i (see foreign_src).
+void note_sources(bm_area_s* A, uint32_t i, uint64_t b, uint64_t e, const uint8_t* data, bool exact);
+// After a cycle of A enqueued on stream s: sends each sampler's frame, or
+// skips it, or waits for the receiver (bm_sampler.cu).
+int sample_after_cycle(bm_area_s* A, cudaStream_t s);
+void free_samplers(bm_area_s* A);
 int cuda_err(cudaError_t e, const char* what);
 
 }  // namespace bm

@@ -248,6 +248,7 @@ struct bm_batch_s {
     cudaEvent_t ev_fork = nullptr;
     std::vector<cudaEvent_t> side_ev;    // per plan step (side steps only)
     size_t last_side = SIZE_MAX;
+    std::vector<uint32_t> versions;      // each area's access_version when the schedule was made
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
 
@@ -485,6 +486,8 @@ StepAccess plan_access(const bm_batch_s::StepPlan& p, bm_area A) {
 int schedule_side(bm_batch_s* B) {
     const size_t n = B->plan.size();
     B->last_side = SIZE_MAX;
+    B->versions.clear();
+    for (bm_area A : B->areas) B->versions.push_back(A->access_version);
     std::vector<std::vector<std::pair<bm_area, StepAccess>>> acc(n);
     for (size_t k = 0; k < n; k++)
         for (bm_area A : B->plan[k].areas) acc[k].push_back({A, plan_access(B->plan[k], A)});
@@ -695,9 +698,29 @@ int ensure_graph(bm_batch_s* B) {
     return BM_OK;
 }
 
+// After each batched cycle: every area's cycle count, then its samplers.
+int after_cycle(bm_batch_s* B, cudaStream_t s) {
+    for (bm_area A : B->areas) {
+        A->host_cycle++;
+        if (!A->samplers.empty()) {
+            const int rc = sample_after_cycle(A, s);
+            if (rc != BM_OK) return rc;
+        }
+    }
+    return BM_OK;
+}
+
 int run_cycles(bm_batch_s* B, const void* frames, uint32_t n_cycles) {
     cudaStream_t s = B->stream();
     for (bm_area A : B->areas) run_pending_verifies(A, s);
+    // Caller writes may have changed what an area's tuft steps read.
+    for (size_t a = 0; a < B->areas.size(); a++)
+        if (a >= B->versions.size() || B->areas[a]->access_version != B->versions[a]) {
+            B->drop_graph();
+            const int rc = schedule_side(B);
+            if (rc != BM_OK) return rc;
+            break;
+        }
     k_batch_begin<<<1, 1, 0, s>>>(B->d_bctl, (const uint8_t*)frames, B->frame_bytes);
     if (B->use_graph && !B->profiling) {
         int rc = ensure_graph(B);
@@ -705,11 +728,16 @@ int run_cycles(bm_batch_s* B, const void* frames, uint32_t n_cycles) {
         for (uint32_t k = 0; k < n_cycles; k++) {
             cudaError_t e = cudaGraphLaunch(B->exec, s);
             if (e != cudaSuccess) return cuda_err(e, "cudaGraphLaunch");
+            const int rc = after_cycle(B, s);
+            if (rc != BM_OK) return rc;
         }
     } else {
-        for (uint32_t k = 0; k < n_cycles; k++) enqueue_batch_cycle(B, s);
+        for (uint32_t k = 0; k < n_cycles; k++) {
+            enqueue_batch_cycle(B, s);
+            const int rc = after_cycle(B, s);
+            if (rc != BM_OK) return rc;
+        }
     }
-    for (bm_area A : B->areas) A->host_cycle += n_cycles;
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_err(e, "batched cycle");
     return BM_OK;

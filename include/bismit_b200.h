@@ -23,7 +23,10 @@
  *   bm_area_cycle        -> CorticalArea::cycle             src/cortex/cortical_area.rs:716-789
  *   bm_area_write_input  -> AxonSpace::intake               src/cortex/axon_space.rs:509-588
  *   bm_area_read_output  -> AxonSpace::output               src/cortex/axon_space.rs:594-629
- *   bm_area_read/write   -> CorticalArea::sampler + the *Test traits' buffer
+ *   bm_sampler_*         -> CorticalArea::sampler + TractReceiver
+ *                                                           src/cortex/cortical_area.rs:809-880,1017-1284
+ *                                                           src/subcortex/tract_channel.rs:400-548
+ *   bm_area_read/write   -> the *Test traits' buffer
  *                           read/write/fill helpers         src/cortex/cortical_area.rs:1017,1375-1516
  *                                                           src/cortex/synapses.rs:536-709
  *   bm_area_get_plan     -> AreaMap::gen_build_options (the resolved slice
@@ -45,7 +48,7 @@ extern "C" {
 #define BM_ERR_INVALID      1   /* bad argument or scheme                      */
 #define BM_ERR_OOM          2   /* device allocation failed                    */
 #define BM_ERR_CUDA         3   /* a CUDA runtime call failed                  */
-#define BM_ERR_TIMEOUT      4   /* a bounded device-side wait gave up          */
+#define BM_ERR_TIMEOUT      4   /* a bounded wait gave up                      */
 #define BM_ERR_UNSUPPORTED  5   /* scheme feature outside this path            */
 #define BM_ERR_NO_DEVICE    6   /* no CUDA device / device index out of range  */
 
@@ -351,11 +354,53 @@ int bm_area_write_slab(bm_area area, const void* src, uint64_t len);
 int bm_area_get_cycle(bm_area area, uint64_t* out);
 int bm_area_set_cycle(bm_area area, uint64_t cycle);
 
+/* ------------------------------------------------------------- samplers -- */
+/* Per-cycle readback of one buffer of an area through a one-frame channel:
+ * CorticalArea::sampler (src/cortex/cortical_area.rs:1017-1284,
+ * SamplerBufferKind::Single) with the tract channel of
+ * src/subcortex/tract_channel.rs:400-488. After every cycle of the area
+ * (bm_area_cycle, bm_area_cycle_frames_device, bm_batch_cycle,
+ * bm_batch_cycle_frames_device) the sampler sends a frame if the receiver has
+ * taken the last one; if not, the new frame is skipped, or with backpressure
+ * the cycling call waits until the receiver takes it (another thread calls
+ * bm_sampler_recv). A frame is an asynchronous copy after the cycle's
+ * kernels; bm_sampler_recv waits for it. Samplers belong to their area and
+ * are destroyed with it. */
+typedef struct bm_sampler_s* bm_sampler;
+#define BM_ALL_LAYERS 0xFFFFFFFFu   /* with BM_BUF_AXON_STATES: every axon of the area */
+
+/* kind: a BM_BUF_* buffer of data layer `layer` (the whole buffer, every
+ * tuft: SomaStates .. SynFlagSets), or BM_BUF_AXON_STATES for the axons of
+ * layer `layer` (its slices) or of the whole area (BM_ALL_LAYERS):
+ * SamplerKind::Axons, src/cortex/cortical_area.rs:61-90. */
+int bm_sampler_create(bm_area area, uint32_t kind, uint32_t layer, int backpressure, bm_sampler* out);
+int bm_sampler_destroy(bm_sampler sampler);
+int bm_sampler_len(bm_sampler sampler, uint64_t* len);
+/* TractSender/TractReceiver::set_backpressure (tract_channel.rs:496-503). */
+int bm_sampler_set_backpressure(bm_sampler sampler, int on, int* prior);
+/* Bounds the waits of bm_sampler_recv and of a backpressured cycle (ms; 0,
+ * the default, waits forever as the reference does); a wait that runs out
+ * returns BM_ERR_TIMEOUT. */
+int bm_sampler_set_timeout(bm_sampler sampler, uint32_t ms);
+/* TractReceiver::recv (tract_channel.rs:438-488): copies the unread frame
+ * (`len` = bm_sampler_len) to dst and sets *got = 1 and *cycle to the cycle
+ * whose end state it holds; with no unread frame, waits for the next one if
+ * wait_for_frame, else sets *got = 0. */
+int bm_sampler_recv(bm_sampler sampler, int wait_for_frame, void* dst, uint64_t len, uint64_t* cycle,
+                    int* got);
+/* Frames sent, and frames skipped because one was unread. */
+int bm_sampler_stats(bm_sampler sampler, uint64_t* sent, uint64_t* skipped);
+
 /* Device pointer of the state slab (for callers that move data with their own
  * copies on the same device). A caller that writes synapse sources or flags
  * through it must call bm_area_sources_changed for that layer before the next
  * cycle. */
 int bm_area_slab_ptr(bm_area area, void** out);
+/* Steps of the area's cycle that run on its side stream, beside the chain of
+ * steps they do not touch (tuft steps that depend on nothing earlier in the
+ * cycle, e.g. pyramidal distal tufts). Caller-written source slice ids
+ * outside a tuft's pool keep that tuft's steps in the chain. */
+int bm_area_side_steps(bm_area area, uint32_t* n);
 int bm_area_sources_changed(bm_area area, uint32_t layer);
 
 /* Sticky device-side error bits of the area (bit 0: a bounded wait inside a

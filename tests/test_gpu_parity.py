@@ -135,6 +135,26 @@ def test_caller_written_sources_match_oracle(ctx, plain):
     area.close()
 
 
+def test_side_stream_follows_caller_sources(ctx):
+    """The pyramidal distal tuft runs beside the spiny stellate chain while its
+    sources stay in its pool; once the caller writes slice ids outside the
+    pool it may read any slice, so it rejoins the chain; a slab restore with
+    pool sources sends it back beside. (The plain form cycles a layer's tufts
+    as one step, which reads the proximal tuft's spiny stellate axons and so
+    always stays in the chain.)"""
+    area = _area(ctx, "area_64", settings_for())
+    grown = area.read_slab()
+    n0 = area.side_steps()
+    assert n0 >= 1
+    li = next(i for i in range(area.plan.n_layers) if area.plan.layers[i].kind == F.BM_LYR_PYRAMIDAL)
+    area.write("syn_src_slc_ids", np.array([250], np.uint8), layer=li,
+               offset=int(area.plan.layers[li].n_syns) - 1)
+    assert area.side_steps() < n0
+    area.write_slab(grown)
+    assert area.side_steps() == n0
+    area.close()
+
+
 def test_device_error_bits_clear(ctx):
     import ctypes
     area = _area(ctx, "area_64", settings_for())
