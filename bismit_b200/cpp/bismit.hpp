@@ -390,6 +390,69 @@ struct ExternalInput {
 
 // ---------------------------------------------------------------- runtime --
 
+// SamplerKind (src/cortex/cortical_area.rs:61-90): the buffer a sampler reads.
+enum class SamplerKind : uint32_t {
+    Axons = BM_BUF_AXON_STATES,
+    SomaStates = BM_BUF_CEL_STATES,
+    SomaEnergies = BM_BUF_CEL_ENERGIES,
+    SomaActivities = BM_BUF_CEL_ACTIVITIES,
+    SomaFlagSets = BM_BUF_CEL_FLAG_SETS,
+    TuftStates = BM_BUF_TFT_STATES,
+    TuftBestDenIds = BM_BUF_TFT_BEST_DEN_IDS,
+    TuftBestDenStatesRaw = BM_BUF_TFT_BEST_DEN_STATES_RAW,
+    TuftBestDenStates = BM_BUF_TFT_BEST_DEN_STATES,
+    TuftPrevStates = BM_BUF_TFT_PREV_STATES,
+    TuftPrevBestDenIds = BM_BUF_TFT_PREV_BEST_DEN_IDS,
+    TuftPrevBestDenStatesRaw = BM_BUF_TFT_PREV_BEST_DEN_STATES_RAW,
+    TuftPrevBestDenStates = BM_BUF_TFT_PREV_BEST_DEN_STATES,
+    DenStates = BM_BUF_DEN_STATES,
+    DenStatesRaw = BM_BUF_DEN_STATES_RAW,
+    DenEnergies = BM_BUF_DEN_ENERGIES,
+    DenActivities = BM_BUF_DEN_ACTIVITIES,
+    DenThresholds = BM_BUF_DEN_THRESHOLDS,
+    SynStates = BM_BUF_SYN_STATES,
+    SynStrengths = BM_BUF_SYN_STRENGTHS,
+    SynSrcSlcIds = BM_BUF_SYN_SRC_SLC_IDS,
+    SynSrcColVOffs = BM_BUF_SYN_SRC_COL_V_OFFS,
+    SynSrcColUOffs = BM_BUF_SYN_SRC_COL_U_OFFS,
+    SynFlagSets = BM_BUF_SYN_FLAG_SETS,
+};
+
+// The receiving end of a sampler (TractReceiver, src/subcortex/tract_channel.rs:
+// 535-548). Owned by its area, which destroys it first.
+class Sampler {
+   public:
+    explicit Sampler(bm_sampler h) : h_(h) { check(bm_sampler_len(h_, &len_)); }
+    ~Sampler() {
+        if (h_) bm_sampler_destroy(h_);
+    }
+    Sampler(const Sampler&) = delete;
+    Sampler& operator=(const Sampler&) = delete;
+
+    uint64_t len() const { return len_; }
+    // TractReceiver::recv: true with the unread frame (and the cycle whose end
+    // state it holds), or false when there is none and wait_for_frame is off.
+    bool recv(bool wait_for_frame, std::vector<uint8_t>& frame, uint64_t* cycle = nullptr) {
+        frame.resize(len_);
+        int got = 0;
+        uint64_t c = 0;
+        check(bm_sampler_recv(h_, wait_for_frame ? 1 : 0, frame.data(), len_, &c, &got));
+        if (cycle) *cycle = c;
+        return got != 0;
+    }
+    // TractReceiver::set_backpressure: returns the prior state.
+    bool set_backpressure(bool on) {
+        int prior = 0;
+        check(bm_sampler_set_backpressure(h_, on ? 1 : 0, &prior));
+        return prior != 0;
+    }
+    void set_timeout(uint32_t ms) { check(bm_sampler_set_timeout(h_, ms)); }
+
+   private:
+    bm_sampler h_ = nullptr;
+    uint64_t len_ = 0;
+};
+
 class CorticalArea {
    public:
     CorticalArea(bm_ctx ctx, const bm_area_desc& desc, uint64_t seed, std::string name)
@@ -398,6 +461,7 @@ class CorticalArea {
         check(bm_area_get_plan(h_, &plan_));
     }
     ~CorticalArea() {
+        samplers_.clear();
         if (h_) bm_area_destroy(h_);
     }
     CorticalArea(const CorticalArea&) = delete;
@@ -440,11 +504,22 @@ class CorticalArea {
     }
     void set_cycle(uint64_t c) { check(bm_area_set_cycle(h_, c)); }
 
+    // CorticalArea::sampler (src/cortex/cortical_area.rs:1017-1284): a
+    // sampler over `kind` of data layer `layer` (for Axons, BM_ALL_LAYERS
+    // samples every axon of the area).
+    Sampler& sampler(SamplerKind kind, uint32_t layer, bool backpressure = false) {
+        bm_sampler h = nullptr;
+        check(bm_sampler_create(h_, (uint32_t)kind, layer, backpressure ? 1 : 0, &h));
+        samplers_.push_back(std::make_unique<Sampler>(h));
+        return *samplers_.back();
+    }
+
    private:
     std::string name_;
     bm_area_desc desc_;
     bm_area h_ = nullptr;
     bm_area_plan plan_;
+    std::vector<std::unique_ptr<Sampler>> samplers_;
 };
 
 class CortexBuilder;

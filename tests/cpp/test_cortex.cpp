@@ -215,10 +215,21 @@ int cmd_cycle(const std::string& dir) {
     const auto frames = read_file(dir + "/frames.bin");
     const size_t len = cx->external_inputs()[0].length;
     const size_t n = frames.size() / len;
+    // A sampler on v2's axons: after each cycle it holds exactly what a read
+    // of the same range returns.
+    auto& v2 = cx->area("v2");
+    Sampler& smp = v2.sampler(SamplerKind::Axons, BM_ALL_LAYERS);
+    bool sampled = true;
+    std::vector<uint8_t> frame;
     for (size_t c = 0; c < n; c++) {
         cx->area("v1").write_input(std::vector<uint8_t>(frames.begin() + c * len, frames.begin() + (c + 1) * len));
         cx->cycle();
+        uint64_t cyc = 0;
+        sampled = sampled && smp.recv(false, frame, &cyc) && cyc == c &&
+                  frame == v2.read(BM_BUF_AXON_STATES, 0, 0, v2.plan().n_axons);
     }
+    std::cout << (sampled ? "sampler ok" : "sampler WRONG") << std::endl;
+    if (!sampled) return 1;
     for (const auto& a : names) {
         auto s = cx->area(a).read_slab();
         write_file(dir + "/final_" + a + ".bin", s.data(), s.size());
