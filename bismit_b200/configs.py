@@ -223,6 +223,41 @@ def testbed_area(side=24):
     return lmaps, areas
 
 
+def smoother_area(side=40, radius=3, pyr_radius=2, smoothers=True):
+    """An instance-style layer map with ActivitySmoother control layers
+    (src/cortex/smoother.rs): one on the spiny stellate layer after its basket
+    inhibition, one on the pyramidal layer after its intra-column inhibition.
+    Group side `radius` / `pyr_radius`."""
+    lmaps = LayerMapSchemeList()
+    areas = AreaSchemeList()
+    _external(lmaps, areas, "v0", side)
+    lm = LayerMapScheme("visual", LayerMapKind.Cortical)
+    lm.layer(LayerScheme.define("aff_in").axonal(AxonTopology.Spatial)
+             .axon_domain(AxonDomain.input([(InputTrack.Afferent, [THAL_SP])])))
+    lm.layer(LayerScheme.define("iv").depth(1).tags(LayerTags.PSAL).axon_domain(AxonDomain.Local)
+             .cellular(CellScheme.spiny_stellate()
+                       .tft(TuftScheme.basal().proximal().syns_per_den(32)
+                            .src_lyr(TuftSourceLayer.define("aff_in").syn_reach(6).prevalence(1)))))
+    lm.layer(LayerScheme.define("iv_inhib")
+             .cellular(CellScheme.control(ControlCellKind.InhibitoryBasketSurround("iv", 4), 0)))
+    lm.layer(LayerScheme.define("iii").depth(2).tags(LayerTags.PTAL).axon_domain(AxonDomain.output([THAL_SP]))
+             .cellular(CellScheme.pyramidal()
+                       .tft(TuftScheme.basal().proximal().dens_per_tft(1).syns_per_den(1)
+                            .src_lyr(TuftSourceLayer.define("iv").syn_reach(0).prevalence(1)))
+                       .tft(TuftScheme.basal().distal().dens_per_tft(8).syns_per_den(32).max_active_dens_l2(3)
+                            .src_lyr(TuftSourceLayer.define("iii").syn_reach(6).prevalence(1)))))
+    lm.layer(LayerScheme.define("iii_col")
+             .cellular(CellScheme.control(ControlCellKind.IntraColumnInhib("iii"), 0)))
+    if smoothers:   # last, so that every other layer keeps its id (and its random streams)
+        lm.layer(LayerScheme.define("iv_smooth")
+                 .cellular(CellScheme.control(ControlCellKind.ActivitySmoother("iv", radius), 1)))
+        lm.layer(LayerScheme.define("iii_smooth")
+                 .cellular(CellScheme.control(ControlCellKind.ActivitySmoother("iii", pyr_radius), 1)))
+    lmaps.add(lm)
+    areas.area(AreaScheme("v1", "visual", side).eff_areas(["v0"]))
+    return lmaps, areas
+
+
 def mixed_area(side=32, src_side=48):
     """A parity case that exercises the remaining index and control paths:
     a scaled input slice (source area larger than the area), a nonspatial input

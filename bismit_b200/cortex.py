@@ -348,7 +348,8 @@ class Batch:
 
     STEP_NAMES = {0: "tuft", 1: "tufts_plain", 2: "ssc_cycle", 3: "inhib_simple", 4: "inhib_passthrough",
                   5: "pyr_output", 6: "inhib_intra_column", 7: "pyr_cycle", 8: "tft_dst_mtp", 9: "ssc_mtp_simple",
-                  10: "cycle_end", 11: "inhib_mtp", 12: "pyr_tail", 13: "regrow", 1000: "fused_tuft_batch"}
+                  10: "cycle_end", 11: "inhib_mtp", 12: "pyr_tail", 13: "regrow", 14: "smooth_activity",
+                  1000: "fused_tuft_batch"}
 
     def set_profiling(self, on):
         F.check(self.lib.bm_batch_set_profiling(self.h, 1 if on else 0))

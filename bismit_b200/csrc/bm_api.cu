@@ -3,6 +3,7 @@
 // (src/cortex/cortical_area.rs:716-789) with the layer cycles of
 // SpinyStellateLayer::cycle (src/cortex/spiny_stellates.rs:220-252) and
 // PyramidalLayer::cycle (src/cortex/pyramidals.rs:297-335).
+#include <algorithm>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -57,6 +58,8 @@ void push_controls(const bm_area_s* A, uint32_t i, std::vector<Step>& out) {
             st = ST_PYR_OUTPUT;
         else if (kind == BM_LYR_CTRL_INTRA_COLUMN)
             st = ST_INTRA_COL;
+        else if (kind == BM_LYR_CTRL_SMOOTHER)
+            st = ST_SMOOTH;
         else
             continue;
         out.push_back({st, (uint8_t)i, (uint8_t)k, 0});
@@ -241,6 +244,16 @@ void bm::exec_step(bm_area_s* A, const Step& st, cudaStream_t s) {
     case ST_REGROW:
         run(K_REGROW, [&] { launch_regrow(A->d_regrow, (uint32_t)A->regrow.size(), A->regrow_blocks, s); });
         break;
+    case ST_SMOOTH: {
+        // The six lattices in order (the reference runs them as one racing
+        // launch; this is one of the orders it can produce).
+        const uint32_t* off = A->center_off[i][x];
+        for (int k = 0; k < 6; k++)
+            run(K_SMOOTH, [&] {
+                launch_smooth(D, A->d_centers[i][x] + off[k], off[k + 1] - off[k], (int32_t)L.ctrl[x].field_radius, s);
+            });
+        break;
+    }
     case ST_CYCLE_END: run(K_CYCLE_END, [&] { launch_cycle_end(A->ctl, s); }); break;
     default: break;
     }
@@ -308,6 +321,9 @@ bm::StepAccess bm::step_access(const bm_area_s* A, const Step& st, int t) {
     case ST_INTRA_COL:
         a.ce_r = 1u << i;
         layer_axons(P, i, a.ax_w);
+        break;
+    case ST_SMOOTH:
+        a.ce_r = a.ce_w = 1u << i;
         break;
     case ST_DST_MTP:
     case ST_PYR_TAIL:
@@ -575,11 +591,15 @@ void free_area(bm_area_s* A) {
         if (A->slab) cudaFree(A->slab);
         if (A->ctl) cudaFree(A->ctl);
         if (A->slices) cudaFree(A->slices);
+        detach_from_batches(A);
         free_samplers(A);
         free_fused(A->fused);
         if (A->d_regrow) cudaFree(A->d_regrow);
         if (A->grow_offs) cudaFree(A->grow_offs);
         if (A->d_geo) cudaFree(A->d_geo);
+        for (auto& row : A->d_centers)
+            for (int32_t* c : row)
+                if (c) cudaFree(c);
         if (A->side) cudaStreamDestroy(A->side);
         if (A->ev_fork) cudaEventDestroy(A->ev_fork);
         for (cudaEvent_t e : A->side_ev)
@@ -732,6 +752,19 @@ int bm_area_create(bm_ctx ctx, const bm_area_desc* desc, uint64_t seed, bm_area*
     if (regrow) {
         rc = prepare_regrow(A, grow, gts);
         if (rc != BM_OK) { free_area(A); return rc; }
+    }
+    // Activity smoothers' group centers.
+    for (uint32_t i = 0; i < A->plan.n_layers; i++) {
+        const bm_layer_plan& L = A->plan.layers[i];
+        for (uint32_t k = 0; k < L.n_ctrl; k++) {
+            if (L.ctrl[k].kind != BM_LYR_CTRL_SMOOTHER) continue;
+            std::vector<int32_t> c;
+            smoother_centers((int)L.ctrl[k].field_radius, (int)L.v_size, (int)L.u_size, c, A->center_off[i][k]);
+            e = cudaMalloc(&A->d_centers[i][k], std::max<size_t>(1, c.size()) * sizeof(int32_t));
+            if (e == cudaSuccess && !c.empty())
+                e = cudaMemcpy(A->d_centers[i][k], c.data(), c.size() * sizeof(int32_t), cudaMemcpyHostToDevice);
+            if (e != cudaSuccess) { free_area(A); return cuda_err(e, "smoother centers"); }
+        }
     }
     for (uint32_t i = 0; i < A->plan.n_layers; i++) A->verify_pending[i] = true;
     area_steps(A, A->steps);

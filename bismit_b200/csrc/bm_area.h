@@ -15,12 +15,13 @@ namespace bm {
 enum Kind {
     K_SYN_FLAGS, K_SYN_CYCLE, K_DEN_CYCLE, K_TFT_CYCLE, K_SSC_CYCLE, K_INHIB_SIMPLE, K_INHIB_PASS,
     K_SSC_MTP, K_PYR_CYCLE, K_PYR_OUTPUT, K_INTRA_COL, K_TFT_DST_MTP, K_CYCLE_END, K_INTAKE,
-    K_FUSED_TUFT, K_TUFT_CELLS, K_INHIB_MTP, K_PYR_TAIL, K_REGROW, K_COUNT
+    K_FUSED_TUFT, K_TUFT_CELLS, K_INHIB_MTP, K_PYR_TAIL, K_REGROW, K_SMOOTH, K_COUNT
 };
 const char* const kKindNames[K_COUNT] = {
     "tft_set_syn_flags", "syn_cycle", "den_cycle_tft", "tft_cycle", "ssc_cycle", "inhib_simple",
     "inhib_passthrough", "ssc_mtp_simple", "pyr_cycle", "pyr_output", "inhib_intra_column", "tft_dst_mtp",
-    "cycle_end", "intake", "fused_tuft_cycle", "tuft_cells", "inhib_mtp", "pyr_tail", "regrow"};
+    "cycle_end", "intake", "fused_tuft_cycle", "tuft_cells", "inhib_mtp", "pyr_tail", "regrow",
+    "smooth_activity"};
 
 struct DevGuard {
     int prev = -1;
@@ -54,6 +55,7 @@ enum StepKind : uint8_t {
     ST_PYR_TAIL,      // ST_PYR_CYCLE, control `idx` (intra-column or output; 0xFF none), and
                       // (arg 1) ST_DST_MTP of every distal tuft, in that order
     ST_REGROW,        // regrowth of every tuft of every data layer (acts on its cycles only)
+    ST_SMOOTH,        // activity smoother `idx` hosted on `layer` (six lattice launches)
 };
 struct Step {
     uint8_t kind, layer, idx, arg;
@@ -127,11 +129,16 @@ struct bm_area_s {
     cudaEvent_t ev_fork = nullptr;
     std::vector<cudaEvent_t> side_ev;
     std::vector<bm_sampler_s*> samplers;   // per-cycle readback channels (bm_sampler.cu)
+    // Activity smoothers: group centers per (host layer, control), six
+    // lattices in center_off ranges.
+    int32_t* d_centers[BM_MAX_LAYERS][BM_MAX_CTRL] = {};
+    uint32_t center_off[BM_MAX_LAYERS][BM_MAX_CTRL][7] = {};
     // Per data layer, bit t: tuft t may hold source slice ids outside its
     // pool (written by the caller), so its steps may read any axon slice.
     uint8_t foreign_src[BM_MAX_LAYERS] = {};
     uint32_t access_version = 0;   // bumped whenever foreign_src changes
     uint32_t n_batches = 0;  // batches holding this area (its tiles are retiled only when one does)
+    std::vector<bm_batch_s*> batches;   // the batches holding it (detached when it is destroyed)
     // Regrowth (absent when disabled): one job per (data layer, tuft), layers
     // in cycle order, block0 counted within the area's own launch.
     std::vector<bm::RegrowJob> regrow;
@@ -195,6 +202,8 @@ void note_sources(bm_area_s* A, uint32_t i, uint64_t b, uint64_t e, const uint8_
 // skips it, or waits for the receiver (bm_sampler.cu).
 int sample_after_cycle(bm_area_s* A, cudaStream_t s);
 void free_samplers(bm_area_s* A);
+// Detaches A from the batches holding it before it is destroyed (bm_batch.cu).
+void detach_from_batches(bm_area_s* A);
 int cuda_err(cudaError_t e, const char* what);
 
 }  // namespace bm

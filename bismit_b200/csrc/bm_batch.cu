@@ -248,6 +248,7 @@ struct bm_batch_s {
     cudaEvent_t ev_fork = nullptr;
     std::vector<cudaEvent_t> side_ev;    // per plan step (side steps only)
     size_t last_side = SIZE_MAX;
+    bool detached = false;               // an area was destroyed first: the batch only waits to be freed
     std::vector<uint32_t> versions;      // each area's access_version when the schedule was made
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
@@ -260,6 +261,21 @@ struct bm_batch_s {
         graph = nullptr;
     }
 };
+
+// An area being destroyed leaves every batch holding it: the batch keeps
+// nothing that points into the area and will not cycle again.
+void bm::detach_from_batches(bm_area_s* A) {
+    for (bm_batch_s* B : A->batches) {
+        DevGuard g(B->ctx->device);
+        cudaStreamSynchronize(B->stream());
+        B->drop_graph();
+        for (bm_area& X : B->areas)
+            if (X == A) X = nullptr;
+        B->detached = true;
+    }
+    A->batches.clear();
+    A->n_batches = 0;
+}
 
 namespace {
 
@@ -275,8 +291,12 @@ void free_plan(bm_batch_s* B) {
 void free_batch(bm_batch_s* B) {
     if (!B) return;
     DevGuard g(B->ctx->device);
-    for (bm_area A : B->areas)
+    // Areas destroyed before the batch were detached (their entries are null).
+    for (bm_area A : B->areas) {
+        if (!A) continue;
         if (A->n_batches) A->n_batches--;
+        A->batches.erase(std::remove(A->batches.begin(), A->batches.end(), B), A->batches.end());
+    }
     B->drop_graph();
     free_plan(B);
     if (B->d_intake) cudaFree(B->d_intake);
@@ -454,6 +474,7 @@ void count_launches(bm_batch_s* B) {
                 const bm_layer_plan& L = A->plan.layers[st.layer];
                 uint32_t per = 1;
                 if (st.kind == ST_TUFTS_PLAIN) per = 1 + 2 * L.n_tufts + (L.kind == BM_LYR_PYRAMIDAL ? L.n_tufts : 0);
+                if (st.kind == ST_SMOOTH) per = 6;
                 n += per;
             }
         } else if (p.form == bm_batch_s::F_CELLS) {
@@ -711,6 +732,7 @@ int after_cycle(bm_batch_s* B, cudaStream_t s) {
 }
 
 int run_cycles(bm_batch_s* B, const void* frames, uint32_t n_cycles) {
+    if (B->detached) return set_err(BM_ERR_INVALID, "an area of this batch was destroyed");
     cudaStream_t s = B->stream();
     for (bm_area A : B->areas) run_pending_verifies(A, s);
     // Caller writes may have changed what an area's tuft steps read.
@@ -832,7 +854,10 @@ int bm_batch_create(bm_ctx ctx, const bm_area* areas, uint32_t n_areas, bm_batch
     if (!B) return set_err(BM_ERR_OOM, "host allocation failed");
     B->ctx = ctx;
     B->areas.assign(areas, areas + n_areas);
-    for (bm_area A : B->areas) A->n_batches++;
+    for (bm_area A : B->areas) {
+        A->n_batches++;
+        A->batches.push_back(B);
+    }
     cudaError_t e = cudaStreamCreateWithFlags(&B->cap, cudaStreamNonBlocking);
     if (e != cudaSuccess) { free_batch(B); return cuda_err(e, "cudaStreamCreate"); }
 
@@ -861,6 +886,7 @@ int bm_batch_destroy(bm_batch batch) {
 }
 
 int bm_batch_set_graph(bm_batch batch, int on) {
+    if (batch && batch->detached) return set_err(BM_ERR_INVALID, "an area of this batch was destroyed");
     if (!batch) return set_err(BM_ERR_INVALID, "null batch");
     batch->use_graph = on != 0;
     return BM_OK;
@@ -873,6 +899,7 @@ int bm_batch_cycle(bm_batch batch, uint32_t n_cycles) {
 }
 
 int bm_batch_frame_bytes(bm_batch batch, uint64_t* out) {
+    if (batch && batch->detached) return set_err(BM_ERR_INVALID, "an area of this batch was destroyed");
     if (!batch || !out) return set_err(BM_ERR_INVALID, "null argument");
     *out = batch->frame_bytes;
     return BM_OK;
@@ -880,6 +907,7 @@ int bm_batch_frame_bytes(bm_batch batch, uint64_t* out) {
 
 int bm_batch_connect(bm_batch batch, uint32_t src_area, uint32_t src_output, uint32_t dst_area, uint32_t dst_input,
                      uint64_t dst_offset) {
+    if (batch && batch->detached) return set_err(BM_ERR_INVALID, "an area of this batch was destroyed");
     if (!batch) return set_err(BM_ERR_INVALID, "null batch");
     bm_batch_s* B = batch;
     const uint32_t n = (uint32_t)B->areas.size();
@@ -918,6 +946,7 @@ int bm_batch_cycle_frames_device(bm_batch batch, const void* dev_frames, uint32_
 }
 
 int bm_batch_set_profiling(bm_batch batch, int on) {
+    if (batch && batch->detached) return set_err(BM_ERR_INVALID, "an area of this batch was destroyed");
     if (!batch) return set_err(BM_ERR_INVALID, "null batch");
     batch->profiling = on != 0;
     return BM_OK;
@@ -925,6 +954,7 @@ int bm_batch_set_profiling(bm_batch batch, int on) {
 
 int bm_batch_get_profile(bm_batch batch, uint32_t n_max, uint32_t* kinds, uint32_t* layers, uint32_t* idx,
                          uint32_t* n_areas, uint64_t* launches, double* ms, uint32_t* n_out) {
+    if (batch && batch->detached) return set_err(BM_ERR_INVALID, "an area of this batch was destroyed");
     if (!batch || !n_out) return set_err(BM_ERR_INVALID, "null argument");
     DevGuard g(batch->ctx->device);
     batch->drain_profile();
@@ -944,6 +974,7 @@ int bm_batch_get_profile(bm_batch batch, uint32_t n_max, uint32_t* kinds, uint32
 }
 
 int bm_batch_reset_profile(bm_batch batch) {
+    if (batch && batch->detached) return set_err(BM_ERR_INVALID, "an area of this batch was destroyed");
     if (!batch) return set_err(BM_ERR_INVALID, "null batch");
     batch->drain_profile();
     for (auto& p : batch->plan) {
@@ -954,6 +985,7 @@ int bm_batch_reset_profile(bm_batch batch) {
 }
 
 int bm_batch_launches_per_cycle(bm_batch batch, uint32_t* out) {
+    if (batch && batch->detached) return set_err(BM_ERR_INVALID, "an area of this batch was destroyed");
     if (!batch || !out) return set_err(BM_ERR_INVALID, "null argument");
     uint32_t n = (batch->intake_blocks ? 1u : 0u) + 1u;   // copies, cycle end
     n += batch->plan_launches;
@@ -962,6 +994,7 @@ int bm_batch_launches_per_cycle(bm_batch batch, uint32_t* out) {
 }
 
 int bm_batch_device_errors(bm_batch batch, uint32_t* bits) {
+    if (batch && batch->detached) return set_err(BM_ERR_INVALID, "an area of this batch was destroyed");
     if (!batch || !bits) return set_err(BM_ERR_INVALID, "null argument");
     uint32_t all = 0;
     for (bm_area A : batch->areas) {
@@ -976,6 +1009,7 @@ int bm_batch_device_errors(bm_batch batch, uint32_t* bits) {
 }
 
 int bm_batch_autotune(bm_batch batch, const char* cache_path, uint32_t* n_tuned) {
+    if (batch && batch->detached) return set_err(BM_ERR_INVALID, "an area of this batch was destroyed");
     if (!batch) return set_err(BM_ERR_INVALID, "null batch");
     bm_batch_s* B = batch;
     DevGuard g(B->ctx->device);

@@ -109,6 +109,8 @@ void launch_ssc_mtp_plain(const uint8_t* axns, const DevLayer& L, const AreaCtl*
 void launch_pyr_cycle_plain(const DevLayer& L, cudaStream_t s);
 void launch_pyr_output(uint8_t* axns, const SliceRec* slices, const DevLayer& L, cudaStream_t s);
 void launch_inhib_intra_column_plain(uint8_t* axns, const SliceRec* slices, const DevLayer& L, cudaStream_t s);
+// One lattice of the activity smoother's group centers (bm_plain.cu).
+void launch_smooth(const DevLayer& L, const int32_t* centers, uint32_t n, int32_t radius, cudaStream_t s);
 // Fused cell steps (bm_items.cuh): an unfused tuft's four stages per cell;
 // inhibition with spiny stellate learning; pyramidal soma, control and distal
 // learning per column (ctrl: 0 none, 1 intra-column, 2 output).

@@ -18,6 +18,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <map>
+#include <set>
 #include <vector>
 
 namespace bm {
@@ -128,6 +129,37 @@ uint64_t rnd_key(uint64_t seed, uint32_t area, uint32_t layer, uint32_t role, ui
 uint64_t grow_key(uint64_t seed, uint32_t area, uint32_t layer, uint32_t tft) {
     uint64_t k = splitmix64(seed ^ 0x67726F77ull) + (((uint64_t)area << 48) | ((uint64_t)layer << 40) | ((uint64_t)tft << 32));
     return splitmix64(k);
+}
+
+// gen_grp_centers (src/cortex/smoother.rs:11-33) with HexGroupCenters
+// (src/cmn/mod.rs:809-917): six lattices of hexagonal group centers of side
+// r, each grown from its start by the six moves of add_surrounds within
+// [-r, dims + r), as sets (the reference's hash-set order is not kept; the
+// groups of one lattice do not overlap, so no result depends on it).
+void smoother_centers(int r, int v_size, int u_size, std::vector<int32_t>& out, uint32_t off[7]) {
+    const int l = r + 1, s = r, ls = l + s;
+    const int moves[6][2] = {{-s, ls}, {l, s}, {ls, -l}, {s, -ls}, {-l, -s}, {-ls, l}};
+    const int ofs = (r + 1) / 2;
+    const int starts[6][2] = {{0, ofs}, {-ofs, ofs}, {-ofs, 0}, {0, -ofs}, {ofs, -ofs}, {ofs, 0}};
+    out.clear();
+    for (int k = 0; k < 6; k++) {
+        off[k] = (uint32_t)out.size();
+        std::set<std::pair<int, int>> seen;
+        std::vector<std::pair<int, int>> todo;
+        auto add = [&](int v, int u) {
+            if (v < -r || u < -r || v >= v_size + r || u >= u_size + r) return;
+            if (seen.insert({v, u}).second) todo.push_back({v, u});
+        };
+        add(starts[k][0], starts[k][1]);
+        while (!todo.empty()) {
+            const auto c = todo.back();
+            todo.pop_back();
+            for (const auto& m : moves) add(c.first + m[0], c.second + m[1]);
+        }
+        for (const auto& c : seen) out.push_back((int32_t)(((uint32_t)(uint16_t)(int16_t)c.first << 16) |
+                                                           (uint16_t)(int16_t)c.second));
+    }
+    off[6] = (uint32_t)out.size();
 }
 
 int resolve_area(const bm_area_desc* D, uint64_t seed, bm_area_plan* P, std::vector<TuftGrowSpec>* grow,
@@ -354,8 +386,6 @@ int resolve_area(const bm_area_desc* D, uint64_t seed, bm_area_plan* P, std::vec
         for (uint32_t l = 0; l < D->n_layers; l++) {
             const bm_layer_desc& Ld = D->layers[l];
             if (Ld.kind < BM_LYR_CTRL_INHIB_BASKET) continue;
-            if (Ld.kind == BM_LYR_CTRL_SMOOTHER)
-                fail("ActivitySmoother control layers are not on this path");
             if (Ld.host_layer_idx < 0 || (uint32_t)Ld.host_layer_idx >= D->n_layers || data_idx[Ld.host_layer_idx] < 0)
                 fail("control layer '%.*s': host layer must be a cellular data layer", BM_NAME_LEN, Ld.name);
             bm_layer_plan& H = P->layers[data_idx[Ld.host_layer_idx]];
@@ -364,7 +394,8 @@ int resolve_area(const bm_area_desc* D, uint64_t seed, bm_area_plan* P, std::vec
                     fail("Duplicate control cell layer address / order index found for layer: %.*s (%u)",
                          BM_NAME_LEN, Ld.name, Ld.exe_order);
             if (H.n_ctrl >= BM_MAX_CTRL) fail("too many control layers on one host");
-            if (Ld.kind == BM_LYR_CTRL_INHIB_BASKET && Ld.field_radius > 127) fail("field_radius must be <= 127");
+            if ((Ld.kind == BM_LYR_CTRL_INHIB_BASKET || Ld.kind == BM_LYR_CTRL_SMOOTHER) && Ld.field_radius > 127)
+                fail("field_radius must be <= 127");
             bm_ctrl_plan C{};
             C.kind = Ld.kind;
             C.exe_order = Ld.exe_order;

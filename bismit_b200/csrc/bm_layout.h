@@ -39,6 +39,11 @@ bool offset_extent(int reach, uint32_t vs, uint32_t us, int* rv, int* ru);
 
 // Key of the per-launch random stream for (area, layer, role, tuft).
 uint64_t rnd_key(uint64_t seed, uint32_t area, uint32_t layer, uint32_t role, uint32_t tft);
+// The activity smoother's group centers for a host layer of v_size x u_size
+// and group side r: six lattices, lattice k in out[off[k] .. off[k + 1]),
+// each center packed as (v << 16) | (u & 0xFFFF) in 16-bit two's complement.
+void smoother_centers(int r, int v_size, int u_size, std::vector<int32_t>& out, uint32_t off[7]);
+
 // Key of the growth stream of (area, layer, tuft).
 uint64_t grow_key(uint64_t seed, uint32_t area, uint32_t layer, uint32_t tft);
 

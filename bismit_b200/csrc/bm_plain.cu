@@ -177,6 +177,52 @@ void launch_pyr_cycle_plain(const DevLayer& L, cudaStream_t s) {
 void launch_pyr_output(uint8_t* axns, const SliceRec* slices, const DevLayer& L, cudaStream_t s) {
     launch_pdl(k_pyr_output, nblk(L.cells, 256), 256, 0, s, axns, slices, L);
 }
+// smooth_activity (cl/control.cl:227-295), one lattice of group centers: each
+// center scans the hexagon of side r around it over every slice of the host
+// layer (slice, then v offset, then u offset, as the reference loops), keeps
+// the least active cell (ties: the later one) and the most active (ties: the
+// later one), then raises the least active cell's energy by one and lowers
+// the most active's by one, each within 0..255 and only when they differ.
+// The groups of one lattice do not overlap, so the centers of a launch touch
+// disjoint cells.
+__global__ void k_smooth(DevLayer L, const int32_t* __restrict__ centers, uint32_t n, int32_t r) {
+    pdl_begin();
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int32_t cv = centers[i] >> 16, cu = (int32_t)(int16_t)(centers[i] & 0xFFFF);
+    const uint8_t* act = L.buf[BM_BUF_CEL_ACTIVITIES];
+    uint8_t* en = L.buf[BM_BUF_CEL_ENERGIES];
+    const int32_t vs = (int32_t)L.v_size, us = (int32_t)L.u_size;
+    uint32_t least_idx = 0, most_idx = 0;
+    uint32_t least_act = 255, most_act = 0;
+    for (uint32_t slc = 0; slc < L.depth; slc++)
+        for (int32_t vo = -r; vo <= r; vo++) {
+            const int32_t uz = max(-r, -vo - r), um = min(r, -vo + r);
+            const int32_t v = cv + vo;
+            for (int32_t uo = uz; uo <= um; uo++) {
+                const int32_t u = cu + uo;
+                if (v < 0 || v >= vs || u < 0 || u >= us) continue;
+                const uint32_t idx = slc * (uint32_t)(vs * us) + (uint32_t)(v * us + u);
+                const uint32_t a = act[idx];
+                if (a <= least_act) { least_idx = idx; least_act = a; }
+                if (a >= most_act) { most_idx = idx; most_act = a; }
+            }
+        }
+    // Equal indices change nothing; skipping the write matters, because a
+    // hexagon wholly outside the layer leaves both at cell 0, and writing
+    // cell 0's energy back would race the one hexagon of the lattice that
+    // holds cell 0.
+    if (least_idx == most_idx) return;
+    const uint32_t le = en[least_idx];
+    en[least_idx] = (uint8_t)(le + (uint32_t)((le < 255) & (most_act < 255)));
+    const uint32_t me = en[most_idx];
+    en[most_idx] = (uint8_t)(me - (uint32_t)((me > 0) & (most_act > 0)));
+}
+
+void launch_smooth(const DevLayer& L, const int32_t* centers, uint32_t n, int32_t radius, cudaStream_t s) {
+    if (n) launch_pdl(k_smooth, nblk(n, 128), 128, 0, s, L, centers, n, radius);
+}
+
 void launch_inhib_intra_column_plain(uint8_t* axns, const SliceRec* slices, const DevLayer& L, cudaStream_t s) {
     launch_pdl(k_inhib_intra_column, nblk((uint64_t)L.v_size * L.u_size, 256), 256, 0, s, axns, slices, L);
 }

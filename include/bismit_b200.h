@@ -70,7 +70,7 @@ extern "C" {
 #define BM_LYR_CTRL_INHIB_BASKET   3   /* InhibitoryBasketSurround -> inhib_simple  */
 #define BM_LYR_CTRL_PYR_OUTPUT     4   /* PyrOutputter -> pyr_output                */
 #define BM_LYR_CTRL_INTRA_COLUMN   5   /* IntraColumnInhib -> inhib_intra_column    */
-#define BM_LYR_CTRL_SMOOTHER       6   /* ActivitySmoother: not on this path        */
+#define BM_LYR_CTRL_SMOOTHER       6   /* ActivitySmoother -> smooth_activity       */
 
 /* Axon domains (src/map/axon_domain.rs). */
 #define BM_DOM_LOCAL   0

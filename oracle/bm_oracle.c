@@ -466,11 +466,107 @@ static void k_tft_dst_mtp(const uint8_t* axns, lview* V, const bm_tuft_plan* T, 
     }
 }
 
+/* ActivitySmoother group centers: gen_grp_centers (src/cortex/smoother.rs:
+ * 11-33) with HexGroupCenters (src/cmn/mod.rs:809-917). Lattice k is grown
+ * from its start by the six moves of add_surrounds, within [-r, dims + r);
+ * centers are returned row-major (the reference keeps them in a hash set;
+ * the groups of one lattice are disjoint, so their order does not matter).
+ * Writes (v, u) pairs into out (capacity 2 * cap) and the lattice ranges
+ * into off[7]; returns -1 on overflow. */
+static int smoother_centers(int r, int V, int U, int32_t* out, int cap, int off[7]) {
+    const int l = r + 1, s = r, ls = l + s;
+    const int mv[6][2] = {{-s, ls}, {l, s}, {ls, -l}, {s, -ls}, {-l, -s}, {-ls, l}};
+    const int ofs = (r + 1) / 2;
+    const int st[6][2] = {{0, ofs}, {-ofs, ofs}, {-ofs, 0}, {0, -ofs}, {ofs, -ofs}, {ofs, 0}};
+    const int W = U + 2 * r, H = V + 2 * r;
+    uint8_t* seen = (uint8_t*)calloc((size_t)W * H, 1);
+    int* stack = (int*)malloc(sizeof(int) * 2 * (size_t)W * H + 16);
+    int n = 0;
+    for (int k = 0; k < 6; k++) {
+        memset(seen, 0, (size_t)W * H);
+        off[k] = n;
+        int top = 0;
+        if (st[k][0] >= -r && st[k][1] >= -r && st[k][0] < V + r && st[k][1] < U + r) {
+            seen[(st[k][0] + r) * W + (st[k][1] + r)] = 1;
+            stack[top++] = st[k][0];
+            stack[top++] = st[k][1];
+        }
+        while (top) {
+            int cu = stack[--top], cv = stack[--top];
+            for (int m = 0; m < 6; m++) {
+                int v = cv + mv[m][0], u = cu + mv[m][1];
+                if (v < -r || u < -r || v >= V + r || u >= U + r) continue;
+                if (seen[(v + r) * W + (u + r)]) continue;
+                seen[(v + r) * W + (u + r)] = 1;
+                stack[top++] = v;
+                stack[top++] = u;
+            }
+        }
+        for (int v = -r; v < V + r; v++)
+            for (int u = -r; u < U + r; u++)
+                if (seen[(v + r) * W + (u + r)]) {
+                    if (n >= cap) { free(seen); free(stack); return -1; }
+                    out[2 * n] = v;
+                    out[2 * n + 1] = u;
+                    n++;
+                }
+    }
+    off[6] = n;
+    free(seen);
+    free(stack);
+    return 0;
+}
+
+/* smooth_activity (cl/control.cl:227-295), the six lattices in order (the
+ * reference launches every center at once and its work-items race on the
+ * energies; lattice order is one of the outcomes that race can give). For
+ * each center: scan the hexagon of side r over every slice of the host layer
+ * (slice, v offset, u offset), keep the least active in-bounds cell (ties:
+ * the later) and the most active (ties: the later); then the least active
+ * cell's energy += 1 when below 255, the most active's -= 1 when above 0,
+ * both only when the two cells differ and (for the raise) the most active
+ * activity is below 255, (for the lowering) above 0. ActivitySmoother::cycle
+ * (src/cortex/smoother.rs:154-169) runs it every cycle: its counter is never
+ * stored, so `cycle_count & 0xFF == 0` always holds. */
+static void k_smooth_activity(lview* V, int r) {
+    const bm_layer_plan* L = V->L;
+    const int Vs = (int)L->v_size, Us = (int)L->u_size;
+    const int cap = 6 * (Vs + 2 * r + 2) * (Us + 2 * r + 2);
+    int32_t* c = (int32_t*)malloc(sizeof(int32_t) * 2 * (size_t)cap);
+    int off[7];
+    if (smoother_centers(r, Vs, Us, c, cap, off)) { free(c); return; }
+    const uint8_t* act = V->b[BM_BUF_CEL_ACTIVITIES];
+    uint8_t* en = V->b[BM_BUF_CEL_ENERGIES];
+    for (int i = 0; i < off[6]; i++) {
+        const int cv = c[2 * i], cu = c[2 * i + 1];
+        uint32_t li = 0, mi = 0, la = 255, ma = 0;
+        for (uint32_t slc = 0; slc < L->depth; slc++)
+            for (int vo = -r; vo <= r; vo++) {
+                int uz = imax(-r, -vo - r), um = imin(r, -vo + r);
+                for (int uo = uz; uo <= um; uo++) {
+                    int v = cv + vo, u = cu + uo;
+                    if (v < 0 || v >= Vs || u < 0 || u >= Us) continue;
+                    uint32_t idx = slc * (uint32_t)(Vs * Us) + (uint32_t)(v * Us + u);
+                    uint32_t a = act[idx];
+                    if (a <= la) { li = idx; la = a; }
+                    if (a >= ma) { mi = idx; ma = a; }
+                }
+            }
+        int differ = li != mi;
+        uint32_t le = en[li];
+        en[li] = (uint8_t)(le + (uint32_t)((le < 255) & (ma < 255) & differ));
+        uint32_t me = en[mi];
+        en[mi] = (uint8_t)(me - (uint32_t)((me > 0) & (ma > 0) & differ));
+    }
+    free(c);
+}
+
 /* --------------------------------------------------------- layer steps --- */
 
 /* Control layers hosted on V in (host, exe_order) order
  * (src/cortex/control_cell_layer.rs:21, src/cortex/iinn.rs:105-127,
- * src/cortex/intra_column_inhib.rs:80-92, src/cortex/pyr_outputter.rs:70-80). */
+ * src/cortex/intra_column_inhib.rs:80-92, src/cortex/pyr_outputter.rs:70-80,
+ * src/cortex/smoother.rs:154-169). */
 static void controls_post(const bm_area_plan* P, uint8_t* axns, lview* V, uint64_t cyc) {
     const bm_layer_plan* L = V->L;
     for (uint32_t k = 0; k < L->n_ctrl; k++) {
@@ -485,6 +581,7 @@ static void controls_post(const bm_area_plan* P, uint8_t* axns, lview* V, uint64
             break;
         case BM_LYR_CTRL_PYR_OUTPUT: k_pyr_output(P, axns, V); break;
         case BM_LYR_CTRL_INTRA_COLUMN: k_inhib_intra_column(P, axns, V); break;
+        case BM_LYR_CTRL_SMOOTHER: k_smooth_activity(V, (int)C->field_radius); break;
         default: break;
         }
     }

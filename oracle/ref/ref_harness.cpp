@@ -12,6 +12,7 @@
 // The slice tables (the __constant arrays of cl/bismit.cl:108-114) are
 // process-global here, so runs of different plans must not overlap in time.
 #include <cstdint>
+#include <vector>
 #include <cstring>
 #include <initializer_list>
 #include <omp.h>
@@ -114,6 +115,39 @@ static void set_tables(const bm_area_plan* P) {
     }
 }
 
+// gen_grp_centers (src/cortex/smoother.rs:11-33) with HexGroupCenters
+// (src/cmn/mod.rs:809-917): six lattices, each grown from its start by the
+// six moves of add_surrounds within [-r, dims + r), row-major per lattice.
+static void smoother_centers(int r, int V, int U, std::vector<int>& cv, std::vector<int>& cu,
+                             std::vector<size_t>& off) {
+    const int l = r + 1, s = r, ls = l + s;
+    const int mv[6][2] = {{-s, ls}, {l, s}, {ls, -l}, {s, -ls}, {-l, -s}, {-ls, l}};
+    const int ofs = (r + 1) / 2;
+    const int st[6][2] = {{0, ofs}, {-ofs, ofs}, {-ofs, 0}, {0, -ofs}, {ofs, -ofs}, {ofs, 0}};
+    const int W = U + 2 * r, H = V + 2 * r;
+    off.assign(7, 0);
+    for (int k = 0; k < 6; k++) {
+        std::vector<char> seen((size_t)W * H, 0);
+        std::vector<std::pair<int, int>> todo;
+        off[k] = cv.size();
+        auto add = [&](int v, int u) {
+            if (v < -r || u < -r || v >= V + r || u >= U + r) return;
+            char& f = seen[(size_t)(v + r) * W + (u + r)];
+            if (!f) { f = 1; todo.push_back({v, u}); }
+        };
+        add(st[k][0], st[k][1]);
+        while (!todo.empty()) {
+            auto c = todo.back();
+            todo.pop_back();
+            for (auto& m : mv) add(c.first + m[0], c.second + m[1]);
+        }
+        for (int v = -r; v < V + r; v++)
+            for (int u = -r; u < U + r; u++)
+                if (seen[(size_t)(v + r) * W + (u + r)]) { cv.push_back(v); cu.push_back(u); }
+    }
+    off[6] = cv.size();
+}
+
 struct Layer {
     const bm_layer_plan* L;
     uint8_t* b[BM_BUF_COUNT];
@@ -202,6 +236,28 @@ static void controls_post(Area& A, Layer& Y, uint64_t cyc) {
             A.err |= launch(L->v_size, L->u_size, 1, 1, 1, 1, [&] {
                 clref::inhib_intra_column(Y.soma(), depth, base, A.axns);
             });
+        } else if (C.kind == BM_LYR_CTRL_SMOOTHER) {
+            // ActivitySmoother::cycle (src/cortex/smoother.rs:154-169, kernel
+            // args :99-110), every cycle (its counter is never stored). The
+            // centers of one lattice per launch, lattices in order: the
+            // groups of a lattice are disjoint, so its work-items may run in
+            // any order.
+            int radius = (int)C.field_radius;
+            uchar depth = (uchar)L->depth;
+            uint v_size = L->v_size, u_size = L->u_size;
+            std::vector<int> cv, cu;
+            std::vector<size_t> off;
+            smoother_centers(radius, (int)v_size, (int)u_size, cv, cu, off);
+            for (int k = 0; k < 6; k++) {
+                const size_t n = off[k + 1] - off[k];
+                if (!n) continue;
+                const int* pv = cv.data() + off[k];
+                const int* pu = cu.data() + off[k];
+                A.err |= launch(n, 1, 1, 1, 1, 1, [&] {
+                    clref::smooth_activity(pv, pu, v_size, u_size, radius, depth, Y.u(BM_BUF_CEL_ACTIVITIES),
+                                           Y.u(BM_BUF_CEL_ENERGIES));
+                });
+            }
         }
     }
 }

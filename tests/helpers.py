@@ -12,6 +12,7 @@ SCHEMES = {
     "mixed": lambda: configs.mixed_area(),
     "area_64": lambda: configs.workload("area_64")[:2],
     "area_48_deep": lambda: configs.workload("area_48_deep")[:2],
+    "smoother": lambda: configs.smoother_area(),
 }
 
 

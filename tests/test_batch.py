@@ -208,3 +208,46 @@ def test_batch_instances_are_seeded_and_in_range():
         assert dens in (8, 16) and syns in (16, 32, 64) and 0.01 <= act <= 0.04
     # The first instance does not depend on how many are drawn.
     assert configs.batch_instances(1, 0)[0] == x[0]
+
+
+@pytest.mark.gpu
+def test_batch_with_smoothers_matches_oracle():
+    """Areas with ActivitySmoother control layers (each area's own six lattice
+    launches inside the batched cycle) against the oracle."""
+    ctx = cortex._Ctx(0)
+    descs = [M.area_desc("v1", *configs.smoother_area(side, 3, 2), configs.bench_settings()) for side in (40, 56)]
+    batched, alone = _pairs(ctx, descs)
+    batch = cortex.Batch(ctx, batched)
+    ora = [a.read_slab() for a in batched]
+    fr = [_frames(a, 3, 90 + k) for k, a in enumerate(batched)]
+    for c in range(3):
+        for k, a in enumerate(batched):
+            a.write_input(fr[k][c])
+        batch.cycle(1)
+        for k, a in enumerate(batched):
+            oracle.run(a.plan, ora[k], fr[k][c:c + 1], 1, start_cycle=c)
+            dev = a.read_slab()
+            assert np.array_equal(dev, ora[k]), "cycle %d area %d:\n%s" % (c, k, diff_report(a.plan, dev, ora[k]))
+    batch.close()
+    for a in batched + alone:
+        a.close()
+    ctx.close()
+
+
+@pytest.mark.gpu
+def test_destroying_an_area_first_detaches_its_batch():
+    """An area destroyed before its batch leaves the batch: the batch refuses
+    to cycle, and destroying it afterwards touches nothing freed."""
+    ctx = cortex._Ctx(0)
+    a = cortex.CorticalArea(ctx, _desc(*SMALL[0]), 3)
+    b = cortex.CorticalArea(ctx, _desc(*SMALL[1]), 4)
+    batch = cortex.Batch(ctx, [a, b])
+    batch.cycle(1)
+    a.lib.bm_area_destroy(a.h)   # the library call alone, not the wrapper's cascade
+    a.h = C.c_void_p()
+    assert batch.lib.bm_batch_cycle(batch.h, 1) == F.BM_ERR_INVALID
+    assert batch.lib.bm_batch_destroy(batch.h) == F.BM_OK
+    batch.h = C.c_void_p()
+    b.cycle(1)                   # the other area is unaffected
+    b.close()
+    ctx.close()

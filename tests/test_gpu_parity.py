@@ -60,7 +60,7 @@ def _run_parity(ctx, scheme, kind, plain, cycles, scramble=True, active=0.05, st
 
 
 @pytest.mark.parametrize("plain", [True, False], ids=["plain", "fused"])
-@pytest.mark.parametrize("scheme", ["testbed", "mixed", "area_64", "area_48_deep"])
+@pytest.mark.parametrize("scheme", ["testbed", "mixed", "area_64", "area_48_deep", "smoother"])
 def test_cycles_match_oracle(ctx, scheme, plain):
     _run_parity(ctx, scheme, "default", plain, cycles=6)
 

@@ -7,11 +7,11 @@ import numpy as np
 import pytest
 
 import oracle
-from bismit_b200 import _ffi as F
-from helpers import diff_report, frames_for, initial_slab, plan_for, settings_for
+from bismit_b200 import _ffi as F, configs, map as M
+from helpers import diff_report, frames_for, initial_slab, plan_for, scramble, settings_for
 
 
-@pytest.mark.parametrize("scheme", ["testbed", "mixed", "area_64", "area_48_deep"])
+@pytest.mark.parametrize("scheme", ["testbed", "mixed", "area_64", "area_48_deep", "smoother"])
 @pytest.mark.parametrize("kind", ["default", "bypass_inhib", "no_learning", "zero_strength"])
 def test_port_matches_reference_kernels(ref_oracle, scheme, kind):
     _, plan = plan_for(scheme, settings_for(kind))
@@ -81,3 +81,32 @@ def test_rnd_stream_is_deterministic_and_keyed():
     assert oracle.rnd(6, 1, 2, F.BM_RND_DEN_CYCLE, 0, 0) != a[0]
     lib = F.lib()
     assert [lib.bm_rnd(5, 1, 2, F.BM_RND_DEN_CYCLE, 0, c) for c in range(100)] == a
+
+
+def test_smoother_only_nudges_energies():
+    """One cycle with and without the activity smoothers from the same state:
+    only the hosts' cell energies differ, each by at most one step per lattice
+    (six), and some do (src/cortex/smoother.rs, cl/control.cl:227-295)."""
+    from bismit_b200 import plan_of
+    from helpers import named
+    with_s = M.area_desc("v1", *configs.smoother_area(), configs.bench_settings())
+    without = M.area_desc("v1", *configs.smoother_area(smoothers=False), configs.bench_settings())
+    p1, p0 = plan_of(with_s, 7), plan_of(without, 7)
+    a = np.zeros(int(p1.slab_bytes), np.uint8)
+    oracle.grow(p1, a, 7, 0)
+    scramble(p1, a, 11)
+    b = a.copy()
+    assert p0.slab_bytes == p1.slab_bytes
+    fr = configs.frames(1, int(p1.inputs[0].len), 0.05, 5)
+    oracle.run(p1, a, fr, 1, start_cycle=0)
+    oracle.run(p0, b, fr, 1, start_cycle=0)
+    na, nb = named(p1, a), named(p0, b)
+    moved = 0
+    for name in nb:
+        if name.endswith("cel_energies"):
+            d = na[name].astype(int) - nb[name].astype(int)
+            assert np.abs(d).max() <= 6
+            moved += int(np.count_nonzero(d))
+        else:
+            assert np.array_equal(na[name], nb[name]), name
+    assert moved > 0
