@@ -18,6 +18,7 @@ BM_MAX_SRC_LAYERS = 8
 BM_MAX_SRC_SLICES = 32
 BM_MAX_CTRL = 4
 BM_MAX_IO = 8
+BM_MAX_FILTERS = 4
 BM_NAME_LEN = 32
 
 BM_LYR_AXONAL, BM_LYR_SPINY_STELLATE, BM_LYR_PYRAMIDAL = 0, 1, 2
@@ -47,6 +48,7 @@ BM_SET_DISABLE_LEARNING = 1 << 6
 BM_INIT_STRENGTH_ZERO = 1 << 0
 BM_INIT_NO_UNIQUE = 1 << 1
 BM_PATH_FUSED, BM_PATH_PLAIN = 0, 1
+BM_FILTER_RETINA = 1
 
 BUF_NAMES = [
     "syn_states", "syn_strengths", "syn_src_slc_ids", "syn_src_col_v_offs", "syn_src_col_u_offs",
@@ -78,7 +80,8 @@ class bm_tuft_desc(C.Structure):
 
 
 class bm_input_src_desc(C.Structure):
-    _fields_ = [("v_size", C.c_uint32), ("u_size", C.c_uint32), ("depth", C.c_uint32), ("axon_topology", C.c_uint32)]
+    _fields_ = [("v_size", C.c_uint32), ("u_size", C.c_uint32), ("depth", C.c_uint32), ("axon_topology", C.c_uint32),
+                ("n_filters", C.c_uint32), ("filters", C.c_uint32 * BM_MAX_FILTERS)]
 
 
 class bm_layer_desc(C.Structure):
@@ -131,6 +134,14 @@ class bm_io_plan(C.Structure):
     _fields_ = [("layer_idx", C.c_uint32), ("axn_idz", C.c_uint32), ("len", C.c_uint32)]
 
 
+class bm_filter_chain_plan(C.Structure):
+    _fields_ = [
+        ("input", C.c_uint32), ("frame_off", C.c_uint32), ("tar_slc", C.c_uint32), ("depth", C.c_uint32),
+        ("v_size", C.c_uint32), ("u_size", C.c_uint32), ("n_filters", C.c_uint32),
+        ("filters", C.c_uint32 * BM_MAX_FILTERS), ("buf_off", C.c_uint64 * BM_MAX_FILTERS),
+    ]
+
+
 class bm_area_plan(C.Structure):
     _fields_ = [
         ("area_id", C.c_uint32), ("v_size", C.c_uint32), ("u_size", C.c_uint32), ("settings", C.c_uint32),
@@ -145,6 +156,7 @@ class bm_area_plan(C.Structure):
         ("n_layers", C.c_uint32), ("layers", bm_layer_plan * BM_MAX_LAYERS),
         ("n_cycle_order", C.c_uint32), ("cycle_order", C.c_uint32 * BM_MAX_LAYERS),
         ("slab_bytes", C.c_uint64), ("n_syns_total", C.c_uint64), ("rnd_seed", C.c_uint64),
+        ("n_filter_chains", C.c_uint32), ("filter_chains", bm_filter_chain_plan * BM_MAX_IO),
     ]
 
 

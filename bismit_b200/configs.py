@@ -26,9 +26,9 @@ from .map import (AreaScheme, AreaSchemeList, AxonDomain, AxonTopology, CellSche
                   LayerScheme, LayerTags, THAL_NSP, THAL_SP, TuftScheme, TuftSourceLayer)
 
 
-def _external(lmaps, areas, name, side, u_side=None, nonspatial=False):
+def _external(lmaps, areas, name, side, u_side=None, nonspatial=False, depth=1):
     lm = LayerMapScheme(name + "_lm", LayerMapKind.Subcortical)
-    lm.layer(LayerScheme.define("ganglion").depth(1).axonal(AxonTopology.Spatial)
+    lm.layer(LayerScheme.define("ganglion").depth(depth).axonal(AxonTopology.Spatial)
              .axon_domain(AxonDomain.output([THAL_SP])))
     if nonspatial:
         lm.layer(LayerScheme.define("ganglion_ns").depth(1).axonal(AxonTopology.Nonspatial)
@@ -187,11 +187,12 @@ def workload(name):
     return lmaps, areas, act
 
 
-def testbed_area(side=24):
-    """The reference's test bed layer map (src/tests/testbed.rs:18-208) without
-    its retina filter chain: spatial input, a spiny stellate layer with a
-    threshold of 400, basket inhibition and a 3-deep pyramidal layer with a
-    basal distal and an apical distal tuft (both learn, in tuft order)."""
+def testbed_area(side=24, retina=False):
+    """The reference's test bed layer map (src/tests/testbed.rs:18-208):
+    spatial input, a spiny stellate layer with a threshold of 400, basket
+    inhibition and a 3-deep pyramidal layer with a basal distal and an apical
+    distal tuft (both learn, in tuft order); with `retina`, also its retina
+    filter chain on the afferent input (testbed.rs:188)."""
     lmaps = LayerMapSchemeList()
     areas = AreaSchemeList()
     _external(lmaps, areas, "v0", side)
@@ -219,7 +220,40 @@ def testbed_area(side=24):
                        .tft(TuftScheme.apical().distal().dens_per_tft(2).syns_per_den(32).max_active_dens_l2(0)
                             .thresh_init(500).src_lyr(TuftSourceLayer.define("iii").syn_reach(3).prevalence(1)))))
     lmaps.add(lm)
-    areas.area(AreaScheme("v1", "visual", side).eff_areas(["v0"]))
+    a = AreaScheme("v1", "visual", side).eff_areas(["v0"])
+    if retina:
+        a.filter_chain(InputTrack.Afferent, [THAL_SP], [("retina", None)])
+    areas.area(a)
+    return lmaps, areas
+
+
+def retina_area(side=48, n_filters=1, src_depth=1, src_side=None):
+    """An instance-style area whose afferent input passes through a chain of
+    `n_filters` retina filters (cl/filters.cl:34-100) from a source `src_depth`
+    slices deep and `src_side` wide (default: the area's side)."""
+    lmaps = LayerMapSchemeList()
+    areas = AreaSchemeList()
+    _external(lmaps, areas, "v0", src_side or side, depth=src_depth)
+    lm = LayerMapScheme("visual", LayerMapKind.Cortical)
+    lm.layer(LayerScheme.define("aff_in").axonal(AxonTopology.Spatial)
+             .axon_domain(AxonDomain.input([(InputTrack.Afferent, [THAL_SP])])))
+    lm.layer(LayerScheme.define("iv").depth(1).tags(LayerTags.PSAL).axon_domain(AxonDomain.Local)
+             .cellular(CellScheme.spiny_stellate()
+                       .tft(TuftScheme.basal().proximal().syns_per_den(32)
+                            .src_lyr(TuftSourceLayer.define("aff_in").syn_reach(6).prevalence(1)))))
+    lm.layer(LayerScheme.define("iv_inhib")
+             .cellular(CellScheme.control(ControlCellKind.InhibitoryBasketSurround("iv", 4), 0)))
+    lm.layer(LayerScheme.define("iii").depth(2).tags(LayerTags.PTAL).axon_domain(AxonDomain.output([THAL_SP]))
+             .cellular(CellScheme.pyramidal()
+                       .tft(TuftScheme.basal().proximal().dens_per_tft(1).syns_per_den(1)
+                            .src_lyr(TuftSourceLayer.define("iv").syn_reach(0).prevalence(1)))
+                       .tft(TuftScheme.basal().distal().dens_per_tft(8).syns_per_den(32).max_active_dens_l2(3)
+                            .src_lyr(TuftSourceLayer.define("iii").syn_reach(6).prevalence(1)))))
+    lm.layer(LayerScheme.define("iii_col")
+             .cellular(CellScheme.control(ControlCellKind.IntraColumnInhib("iii"), 0)))
+    lmaps.add(lm)
+    areas.area(AreaScheme("v1", "visual", side).eff_areas(["v0"])
+               .filter_chain(InputTrack.Afferent, [THAL_SP], ["retina"] * n_filters))
     return lmaps, areas
 
 

@@ -170,6 +170,10 @@ void fuse_steps(const bm_area_s* A, std::vector<Step>& v) {
 void bm::area_steps(const bm_area_s* A, std::vector<Step>& out) {
     const bm_area_plan& P = A->plan;
     out.clear();
+    // AxonSpace::intake (src/cortex/axon_space.rs:510-525): each filtered
+    // input's chain runs before the layers.
+    if (filters_run(P))
+        for (uint32_t c = 0; c < P.n_filter_chains; c++) out.push_back({ST_FILTER, 0, (uint8_t)c, 0});
     if (!(P.settings & BM_SET_DISABLE_SSCS)) {
         for (uint32_t k = 0; k < P.n_cycle_order; k++)
             if (P.layers[P.cycle_order[k]].tags & BM_TAG_SPATIAL) push_layer_cycle(A, P.cycle_order[k], out);
@@ -254,6 +258,22 @@ void bm::exec_step(bm_area_s* A, const Step& st, cudaStream_t s) {
             });
         break;
     }
+    case ST_FILTER: {
+        // SensoryFilter::cycle (src/cortex/sensory_filter.rs:157-168) of each
+        // filter in order: filter k reads its own buffer and writes the next
+        // one's (slice offsets from slice 0, cl/filters.cl:45-47), the last
+        // the target slices.
+        const bm_filter_chain_plan& c = A->plan.filter_chains[x];
+        for (uint32_t f = 0; f < c.n_filters; f++) {
+            const bool last = f + 1 == c.n_filters;
+            uint8_t* out = last ? A->axns() : A->slab + c.buf_off[f + 1];
+            run(K_RETINA, [&] {
+                launch_retina(A->slab + c.buf_off[f], out, A->slices, last ? c.tar_slc : 0, c.depth, c.v_size,
+                              c.u_size, s);
+            });
+        }
+        break;
+    }
     case ST_CYCLE_END: run(K_CYCLE_END, [&] { launch_cycle_end(A->ctl, s); }); break;
     default: break;
     }
@@ -325,6 +345,12 @@ bm::StepAccess bm::step_access(const bm_area_s* A, const Step& st, int t) {
     case ST_SMOOTH:
         a.ce_r = a.ce_w = 1u << i;
         break;
+    case ST_FILTER: {
+        // Reads the chain's own buffers, which nothing else in a cycle touches.
+        const bm_filter_chain_plan& c = P.filter_chains[st.idx];
+        for (uint32_t k = 0; k < c.depth; k++) a.ax_w.set(c.tar_slc + k);
+        break;
+    }
     case ST_DST_MTP:
     case ST_PYR_TAIL:
         a.ax_r.set();
@@ -612,6 +638,45 @@ void free_area(bm_area_s* A) {
 
 }  // namespace
 
+void bm::frame_pieces(bm_area_s* A, uint32_t input, uint32_t off, uint32_t len, std::vector<FramePiece>& out) {
+    const bm_area_plan& P = A->plan;
+    out.clear();
+    uint8_t* axons = A->axns() + P.inputs[input].axn_idz;
+    const bool filtered = filters_run(P);
+    const uint32_t end = off + len;
+    uint32_t pos = off;
+    while (pos < end) {
+        const bm_filter_chain_plan* hit = nullptr;
+        uint32_t next = end;
+        for (uint32_t k = 0; filtered && k < P.n_filter_chains; k++) {
+            const bm_filter_chain_plan& c = P.filter_chains[k];
+            if (c.input != input) continue;
+            const uint32_t c0 = c.frame_off, c1 = c0 + c.depth * c.v_size * c.u_size;
+            if (pos >= c0 && pos < c1) {
+                hit = &c;
+                next = std::min(end, c1);
+            } else if (!hit && c0 > pos && c0 < next) {
+                next = c0;
+            }
+        }
+        out.push_back({pos - off, next - pos, hit ? A->slab + hit->buf_off[0] + (pos - hit->frame_off) : axons + pos});
+        pos = next;
+    }
+}
+
+namespace {
+
+// Copies one input frame to where its pieces land (see frame_pieces).
+int write_frame(bm_area_s* A, uint32_t input, const void* src, cudaMemcpyKind kind, cudaStream_t s) {
+    std::vector<FramePiece> pieces;
+    frame_pieces(A, input, 0, A->plan.inputs[input].len, pieces);
+    for (const FramePiece& p : pieces)
+        CU(cudaMemcpyAsync(p.dst, (const uint8_t*)src + p.off, p.len, kind, s));
+    return BM_OK;
+}
+
+}  // namespace
+
 extern "C" {
 
 const char* bm_last_error(void) { return g_err; }
@@ -805,8 +870,7 @@ int bm_area_write_input(bm_area area, uint32_t input_idx, const uint8_t* frame, 
     if (len != P.inputs[input_idx].len)
         return set_err(BM_ERR_INVALID, "frame length %zu != input layer axon count %u", len, P.inputs[input_idx].len);
     DevGuard g(area->ctx->device);
-    CU(cudaMemcpyAsync(area->axns() + P.inputs[input_idx].axn_idz, frame, len, cudaMemcpyHostToDevice, area->stream()));
-    return BM_OK;
+    return write_frame(area, input_idx, frame, cudaMemcpyHostToDevice, area->stream());
 }
 
 int bm_area_write_input_device(bm_area area, uint32_t input_idx, const void* dev_frame, size_t len) {
@@ -815,8 +879,7 @@ int bm_area_write_input_device(bm_area area, uint32_t input_idx, const void* dev
     if (input_idx >= P.n_inputs) return set_err(BM_ERR_INVALID, "input %u out of range", input_idx);
     if (len != P.inputs[input_idx].len) return set_err(BM_ERR_INVALID, "frame length %zu != %u", len, P.inputs[input_idx].len);
     DevGuard g(area->ctx->device);
-    CU(cudaMemcpyAsync(area->axns() + P.inputs[input_idx].axn_idz, dev_frame, len, cudaMemcpyDeviceToDevice, area->stream()));
-    return BM_OK;
+    return write_frame(area, input_idx, dev_frame, cudaMemcpyDeviceToDevice, area->stream());
 }
 
 int bm_area_cycle(bm_area area, uint32_t n_cycles) {
@@ -837,11 +900,12 @@ int bm_area_cycle_frames_device(bm_area area, const void* dev_frames, size_t fra
     if (frame_len != P.inputs[0].len) return set_err(BM_ERR_INVALID, "frame length %zu != %u", frame_len, P.inputs[0].len);
     DevGuard g(area->ctx->device);
     for (uint32_t k = 0; k < n_cycles; k++) {
+        int rc = BM_OK;
         area->run(K_INTAKE, [&] {
-            cudaMemcpyAsync(area->axns() + P.inputs[0].axn_idz, (const uint8_t*)dev_frames + (uint64_t)k * frame_len,
-                            frame_len, cudaMemcpyDeviceToDevice, area->stream());
+            rc = write_frame(area, 0, (const uint8_t*)dev_frames + (uint64_t)k * frame_len, cudaMemcpyDeviceToDevice,
+                             area->stream());
         });
-        const int rc = enqueue_cycle(area);
+        if (rc == BM_OK) rc = enqueue_cycle(area);
         if (rc != BM_OK) return rc;
     }
     CU(cudaGetLastError());

@@ -15,13 +15,13 @@ namespace bm {
 enum Kind {
     K_SYN_FLAGS, K_SYN_CYCLE, K_DEN_CYCLE, K_TFT_CYCLE, K_SSC_CYCLE, K_INHIB_SIMPLE, K_INHIB_PASS,
     K_SSC_MTP, K_PYR_CYCLE, K_PYR_OUTPUT, K_INTRA_COL, K_TFT_DST_MTP, K_CYCLE_END, K_INTAKE,
-    K_FUSED_TUFT, K_TUFT_CELLS, K_INHIB_MTP, K_PYR_TAIL, K_REGROW, K_SMOOTH, K_COUNT
+    K_FUSED_TUFT, K_TUFT_CELLS, K_INHIB_MTP, K_PYR_TAIL, K_REGROW, K_SMOOTH, K_RETINA, K_COUNT
 };
 const char* const kKindNames[K_COUNT] = {
     "tft_set_syn_flags", "syn_cycle", "den_cycle_tft", "tft_cycle", "ssc_cycle", "inhib_simple",
     "inhib_passthrough", "ssc_mtp_simple", "pyr_cycle", "pyr_output", "inhib_intra_column", "tft_dst_mtp",
     "cycle_end", "intake", "fused_tuft_cycle", "tuft_cells", "inhib_mtp", "pyr_tail", "regrow",
-    "smooth_activity"};
+    "smooth_activity", "retina"};
 
 struct DevGuard {
     int prev = -1;
@@ -56,6 +56,7 @@ enum StepKind : uint8_t {
                       // (arg 1) ST_DST_MTP of every distal tuft, in that order
     ST_REGROW,        // regrowth of every tuft of every data layer (acts on its cycles only)
     ST_SMOOTH,        // activity smoother `idx` hosted on `layer` (six lattice launches)
+    ST_FILTER,        // input filter chain `idx`, from its first buffer to its target slices
 };
 struct Step {
     uint8_t kind, layer, idx, arg;
@@ -194,6 +195,19 @@ void refresh_geo(bm_area_s* A);
 // The accesses of step st of A; for a tuft step, of tuft `t` (the step's own
 // tuft unless given).
 StepAccess step_access(const bm_area_s* A, const Step& st, int t = -1);
+// Input filter chains run when A has some and BM_SET_BYPASS_FILTERS is off.
+inline bool filters_run(const bm_area_plan& P) {
+    return P.n_filter_chains && !(P.settings & BM_SET_BYPASS_FILTERS);
+}
+// Where bytes [off, off + len) of input `input`'s frame land: piece k takes
+// bytes off + pieces[k].off .. + pieces[k].len of the frame to pieces[k].dst,
+// the input's axons, or, for a source whose filter chain runs, that chain's
+// first buffer (the chain then writes the axons at the head of each cycle).
+struct FramePiece {
+    uint32_t off, len;
+    uint8_t* dst;
+};
+void frame_pieces(bm_area_s* A, uint32_t input, uint32_t off, uint32_t len, std::vector<FramePiece>& out);
 // Splits A's program over its stream and a side stream (see step_access).
 int schedule_area(bm_area_s* A);
 // Records caller-written source slice ids of layer i (see foreign_src).

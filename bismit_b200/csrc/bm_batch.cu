@@ -475,6 +475,7 @@ void count_launches(bm_batch_s* B) {
                 uint32_t per = 1;
                 if (st.kind == ST_TUFTS_PLAIN) per = 1 + 2 * L.n_tufts + (L.kind == BM_LYR_PYRAMIDAL ? L.n_tufts : 0);
                 if (st.kind == ST_SMOOTH) per = 6;
+                if (st.kind == ST_FILTER) per = A->plan.filter_chains[st.idx].n_filters;
                 n += per;
             }
         } else if (p.form == bm_batch_s::F_CELLS) {
@@ -625,13 +626,18 @@ int build_intake(bm_batch_s* B) {
         blocks += (J.len + per_block - 1) / per_block;
         jobs.push_back(J);
     };
+    // A filtered source's bytes land in its chain's first buffer.
+    std::vector<FramePiece> pieces;
     for (const auto& T : B->tracts) {
         bm_area S = B->areas[T.src_area], D = B->areas[T.dst_area];
-        IntakeJob J{};
-        J.dst = D->axns() + D->plan.inputs[T.dst_input].axn_idz + T.dst_off;
-        J.src = S->axns() + S->plan.outputs[T.src_output].axn_idz;
-        J.len = S->plan.outputs[T.src_output].len;
-        add(J);
+        frame_pieces(D, T.dst_input, T.dst_off, S->plan.outputs[T.src_output].len, pieces);
+        for (const FramePiece& p : pieces) {
+            IntakeJob J{};
+            J.dst = p.dst;
+            J.src = S->axns() + S->plan.outputs[T.src_output].axn_idz + p.off;
+            J.len = p.len;
+            add(J);
+        }
     }
     for (uint32_t a = 0; a < B->areas.size(); a++) {
         bm_area A = B->areas[a];
@@ -639,12 +645,15 @@ int build_intake(bm_batch_s* B) {
             bool fed = false;
             for (const auto& T : B->tracts) fed = fed || (T.dst_area == a && T.dst_input == i);
             if (fed) continue;
-            IntakeJob J{};
-            J.dst = A->axns() + A->plan.inputs[i].axn_idz;
-            J.src_off = B->frame_bytes;
-            J.len = A->plan.inputs[i].len;
-            B->frame_bytes += J.len;
-            add(J);
+            frame_pieces(A, i, 0, A->plan.inputs[i].len, pieces);
+            for (const FramePiece& p : pieces) {
+                IntakeJob J{};
+                J.dst = p.dst;
+                J.src_off = B->frame_bytes + p.off;
+                J.len = p.len;
+                add(J);
+            }
+            B->frame_bytes += A->plan.inputs[i].len;
         }
     }
     if (jobs.empty()) return BM_OK;

@@ -46,6 +46,7 @@ constexpr int kCellActivityDecay = 768;
 constexpr int kInhibCenterOffset = 1;
 constexpr int kInhibHorizOffset = 3;
 constexpr int kSlcSclCoeffL2 = 4;
+constexpr int kRetinalThreshold = 48;   // RETNAL_THRESHOLD, cl/bismit.cl:19
 constexpr uint8_t kCelPrevActiveFlag = 0x08;
 constexpr uint8_t kSynPrevActiveFlag = 0x10;
 constexpr uint32_t kDenBasalProximalFlag = 0x01;

@@ -111,6 +111,10 @@ void launch_pyr_output(uint8_t* axns, const SliceRec* slices, const DevLayer& L,
 void launch_inhib_intra_column_plain(uint8_t* axns, const SliceRec* slices, const DevLayer& L, cudaStream_t s);
 // One lattice of the activity smoother's group centers (bm_plain.cu).
 void launch_smooth(const DevLayer& L, const int32_t* centers, uint32_t n, int32_t radius, cudaStream_t s);
+// One retina filter (cl/filters.cl:34-100) from a (depth, v_size, u_size)
+// input grid to slices base_slc.. of `out`, each at its slice-table offset.
+void launch_retina(const uint8_t* in, uint8_t* out, const SliceRec* slices, uint32_t base_slc, uint32_t depth,
+                   uint32_t v_size, uint32_t u_size, cudaStream_t s);
 // Fused cell steps (bm_items.cuh): an unfused tuft's four stages per cell;
 // inhibition with spiny stellate learning; pyramidal soma, control and distal
 // learning per column (ctrl: 0 none, 1 intra-column, 2 output).

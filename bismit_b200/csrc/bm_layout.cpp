@@ -179,6 +179,12 @@ int resolve_area(const bm_area_desc* D, uint64_t seed, bm_area_plan* P, std::vec
         // ---- slices (LayerMap::new + SliceMap::new) ----
         uint32_t slc_start[BM_MAX_LAYERS], slc_count[BM_MAX_LAYERS];
         uint32_t ns = 0, axons = 0;
+        // Filtered sources, resolved to inputs[] once the io ranges exist.
+        struct PendingChain {
+            uint32_t layer;
+            bm_filter_chain_plan c;
+        };
+        std::vector<PendingChain> chains;
         auto add_slice = [&](uint32_t layer, const SliceDims& d) {
             if (ns >= 255) fail("more than 255 axon slices");
             P->slc_axn_idz[ns] = axons;
@@ -204,17 +210,36 @@ int resolve_area(const bm_area_desc* D, uint64_t seed, bm_area_plan* P, std::vec
                     fail("Error assembling LayerInfo for '%.*s'. Input layers must be 'AxonTopology::Axonal'.",
                          BM_NAME_LEN, Ld.name);
                 if (Ld.n_input_srcs > BM_MAX_IO) fail("layer %u: too many input sources", l);
+                uint32_t frame_off = 0;
                 for (uint32_t s = 0; s < Ld.n_input_srcs; s++) {
                     const bm_input_src_desc& S = Ld.input_srcs[s];
                     if (S.v_size == 0 || S.u_size == 0) fail("input source dims are zero");
+                    if (S.n_filters) {
+                        if (S.n_filters > BM_MAX_FILTERS) fail("layer %u source %u: more than %d filters", l, s, BM_MAX_FILTERS);
+                        PendingChain pc{l, {}};
+                        pc.c.frame_off = frame_off;
+                        pc.c.tar_slc = ns;
+                        pc.c.depth = S.depth;
+                        pc.c.v_size = S.v_size;
+                        pc.c.u_size = S.u_size;
+                        pc.c.n_filters = S.n_filters;
+                        for (uint32_t k = 0; k < S.n_filters; k++) {
+                            if (S.filters[k] != BM_FILTER_RETINA)
+                                fail("layer %u source %u: unknown filter %u", l, s, S.filters[k]);
+                            pc.c.filters[k] = S.filters[k];
+                        }
+                        chains.push_back(pc);
+                    }
                     if (S.axon_topology != Ld.axon_topology) {
                         if (!(S.axon_topology == BM_TOPO_SPATIAL && Ld.axon_topology == BM_TOPO_NONSPATIAL))
                             fail("SliceMap::new(): Layers may only convert from Spatial -> Nonspatial");
                         if (S.v_size > 254 || S.u_size > 254)
                             fail("Nonspatial layer sources must have dimensions less than or equal to 254v x 254u.");
                     }
+                    const uint32_t axons_before = axons;
                     for (uint32_t k = 0; k < S.depth; k++)
                         add_slice(l, slice_dims(D->v_size, D->u_size, &S, Ld.axon_topology));
+                    frame_off += axons - axons_before;
                 }
             } else {
                 uint32_t depth = Ld.depth < 0 ? 0 : (uint32_t)Ld.depth;
@@ -422,6 +447,37 @@ int resolve_area(const bm_area_desc* D, uint64_t seed, bm_area_plan* P, std::vec
             }
         }
 
+        // ---- input filter chains (AxonSpace::new, src/cortex/axon_space.rs:338-412) ----
+        for (const PendingChain& pc : chains) {
+            bm_filter_chain_plan c = pc.c;
+            c.input = UINT32_MAX;
+            for (uint32_t i = 0; i < P->n_inputs; i++)
+                if (P->inputs[i].layer_idx == pc.layer) c.input = i;
+            if (c.input == UINT32_MAX) fail("filter chain on layer %u, which is not an input layer", pc.layer);
+            if (c.depth == 0) fail("filter chain on a source of depth 0 (layer %u)", pc.layer);
+            // The filter kernels run as (depth, v, u) NDRanges of 1 x 8 x 8
+            // work-groups (SensoryFilter::new, src/cortex/sensory_filter.rs:
+            // 47-54), which OpenCL refuses unless 8 divides v and u.
+            if (c.v_size % 8 || c.u_size % 8)
+                fail("filter chain on layer %u: source dims %u x %u are not multiples of 8 (1 x 8 x 8 work-groups)",
+                     pc.layer, c.v_size, c.u_size);
+            for (uint32_t k = 0; k < c.depth; k++)
+                if (P->slc_v_size[c.tar_slc + k] != c.v_size || P->slc_u_size[c.tar_slc + k] != c.u_size)
+                    fail("filter chain on layer %u: target slice %u is %u x %u, the source %u x %u", pc.layer,
+                         c.tar_slc + k, P->slc_v_size[c.tar_slc + k], P->slc_u_size[c.tar_slc + k], c.v_size, c.u_size);
+            // A filter that feeds another writes slice k of its output at the
+            // area's axon offset of slice k (get_axn_idz with a zero base,
+            // cl/filters.cl:45-47), which must stay inside that buffer.
+            const uint64_t len = (uint64_t)c.depth * c.v_size * c.u_size;
+            if (c.n_filters > 1)
+                for (uint32_t k = 0; k < c.depth; k++)
+                    if ((uint64_t)P->slc_axn_idz[k] + (uint64_t)c.v_size * c.u_size > len)
+                        fail("filter chain on layer %u: an inner filter would write slice %u past its %llu-byte "
+                             "buffer (axon offset %u)", pc.layer, k, (unsigned long long)len, P->slc_axn_idz[k]);
+            if (P->n_filter_chains >= BM_MAX_IO) fail("more than %d filter chains", BM_MAX_IO);
+            P->filter_chains[P->n_filter_chains++] = c;
+        }
+
         // ---- cycle order by role (ROLE_ORDER, src/cortex/cortical_area.rs:31,601-613) ----
         const uint64_t roles[4] = {BM_TAG_FOCUS, BM_TAG_SPATIAL, BM_TAG_TEMPORAL, BM_TAG_MOTOR};
         bool used[BM_MAX_LAYERS] = {};
@@ -455,6 +511,13 @@ int resolve_area(const bm_area_desc* D, uint64_t seed, bm_area_plan* P, std::vec
             put(BM_BUF_CEL_ACTIVITIES, L.cells);
             if (!(P->settings & BM_SET_DISABLE_REGROWTH)) put(BM_BUF_DEN_SRC_KEY0, L.n_dens);
             P->n_syns_total += L.n_syns;
+        }
+        for (uint32_t i = 0; i < P->n_filter_chains; i++) {
+            bm_filter_chain_plan& c = P->filter_chains[i];
+            for (uint32_t k = 0; k < c.n_filters; k++) {
+                c.buf_off[k] = off;
+                off = align_up(off + (uint64_t)c.depth * c.v_size * c.u_size, 256);
+            }
         }
         P->slab_bytes = off;
         return BM_OK;

@@ -223,6 +223,57 @@ void launch_smooth(const DevLayer& L, const int32_t* centers, uint32_t n, int32_
     if (n) launch_pdl(k_smooth, nblk(n, 128), 128, 0, s, L, centers, n, radius);
 }
 
+// retina (cl/filters.cl:34-100), one input filter over a (depth, v, u) grid
+// of input bytes. Cell i (its index in the grid) is an off-center cell when
+// bit 0 of i is set and a large one when bits 1 and 0 differ; it averages the
+// hexagon of radius 5 (large) or 3 (small) around it in its own slice,
+// counting cells outside the grid as zero but still dividing by the full
+// hexagon (get_neighbors_avg, :8-31). The output is how far the average
+// exceeds the cell by more than RETNAL_THRESHOLD (48, cl/bismit.cl:19) for an
+// off-center cell, or the cell the average, else 0. It goes to slice
+// base_slc + slice of the output at that slice's first axon (the slice
+// table's x), the cell's (v, u) place within the slice.
+__global__ void k_retina(const uint8_t* __restrict__ in, uint8_t* __restrict__ out, const SliceRec* __restrict__ slices,
+                         uint32_t base_slc, uint32_t depth, uint32_t vs, uint32_t us) {
+    pdl_begin();
+    const uint32_t cols = vs * us;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= depth * cols) return;
+    const uint32_t slc = i / cols, col = i - slc * cols;
+    const int32_t v = (int32_t)(col / us), u = (int32_t)(col - (uint32_t)v * us);
+    const uint8_t* plane = in + (uint64_t)slc * cols;
+    const uint32_t off_cen = i & 1, large = ((i & 3) >> 1) ^ off_cen;
+    const int32_t r = large ? 5 : 3;
+    int32_t sum = 0;
+    for (int32_t vo = -r; vo <= r; vo++) {
+        const int32_t vv = v + vo;
+        if (vv < 0 || vv >= (int32_t)vs) continue;
+        const int32_t uz = max(-r, -vo - r), um = min(r, -vo + r);
+        const uint8_t* row = plane + (uint32_t)vv * us;
+        for (int32_t uo = uz; uo <= um; uo++) {
+            const int32_t uu = u + uo;
+            if (uu >= 0 && uu < (int32_t)us) sum += row[uu];
+        }
+    }
+    const int32_t avg = sum / (3 * r * r + 3 * r + 1);
+    const int32_t center = in[i];
+    int32_t st;
+    if (off_cen) {
+        const int32_t cst = center + kRetinalThreshold;
+        st = avg > cst ? avg - cst : 0;
+    } else {
+        const int32_t nat = avg + kRetinalThreshold;
+        st = center > nat ? center - nat : 0;
+    }
+    out[slices[(base_slc + slc) & 0xFF].x + col] = (uint8_t)st;
+}
+
+void launch_retina(const uint8_t* in, uint8_t* out, const SliceRec* slices, uint32_t base_slc, uint32_t depth,
+                   uint32_t v_size, uint32_t u_size, cudaStream_t s) {
+    const uint32_t n = depth * v_size * u_size;
+    if (n) launch_pdl(k_retina, nblk(n, 256), 256, 0, s, in, out, slices, base_slc, depth, v_size, u_size);
+}
+
 void launch_inhib_intra_column_plain(uint8_t* axns, const SliceRec* slices, const DevLayer& L, cudaStream_t s) {
     launch_pdl(k_inhib_intra_column, nblk((uint64_t)L.v_size * L.u_size, 256), 256, 0, s, axns, slices, L);
 }

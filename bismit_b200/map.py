@@ -295,6 +295,27 @@ class LayerMapSchemeList:
         return self.maps[name]
 
 
+class FilterScheme:
+    """FilterScheme::new(filter_name, cl_file_name) (src/map/scheme/filter.rs:3-40):
+    one filter of an input filter chain, named by its kernel. The built-in
+    filter is "retina" (cl/filters.cl:34-100); a kernel from a custom OpenCL
+    file has no counterpart here."""
+
+    KINDS = {"retina": F.BM_FILTER_RETINA}
+
+    def __init__(self, filter_name, cl_file_name=None):
+        if filter_name not in self.KINDS:
+            raise ValueError("unknown filter %r (built in: %s)" % (filter_name, ", ".join(sorted(self.KINDS))))
+        if cl_file_name is not None:
+            raise ValueError("filter %r: kernels from custom OpenCL files are not supported" % filter_name)
+        self.filter_name = filter_name
+        self.cl_file_name = cl_file_name
+
+    @property
+    def kind(self):
+        return self.KINDS[self.filter_name]
+
+
 class AreaScheme:
     """AreaScheme::new(name, layer_map_name, side) (src/map/scheme/area.rs:22-198)."""
 
@@ -306,6 +327,25 @@ class AreaScheme:
         self._eff_areas = []
         self._aff_areas = []
         self._other_areas = []
+        self._filter_chains = []
+
+    def filter_chain(self, input_track, axn_tags, filter_chain):
+        """AreaScheme::filter_chain (src/map/scheme/area.rs:70-85): frames of
+        the source matched by the input signature (input_track, axn_tags) pass
+        through the filters in order. Each filter is a FilterScheme, a
+        (name, cl_file_name) pair or a name."""
+        chain = []
+        for f in filter_chain:
+            if isinstance(f, FilterScheme):
+                chain.append(f)
+            elif isinstance(f, tuple):
+                chain.append(FilterScheme(*f))
+            else:
+                chain.append(FilterScheme(f))
+        if len(chain) > F.BM_MAX_FILTERS:
+            raise ValueError("more than %d filters in one chain" % F.BM_MAX_FILTERS)
+        self._filter_chains.append((input_track, frozenset(axn_tags), chain))
+        return self
 
     @staticmethod
     def irregular(name, layer_map_name, dims):
@@ -416,6 +456,36 @@ def _source_layers(area_sch, area_list, lmaps, sigs):
     return [x[2:] for x in source_list(area_sch, area_list, lmaps, sigs)]
 
 
+def _attach_filter_chains(d, a, areas, lmaps, lm):
+    """Each filter chain of area scheme `a` goes to the one source whose input
+    signature it names (AxonSpace::new, src/cortex/axon_space.rs:340-345, with
+    LayerMap::src_layer_info_by_sig, src/map/layer_map.rs:242-261)."""
+    for track, tags, chain in a._filter_chains:
+        hits = []
+        for i, ls in enumerate(lm.layers):
+            if ls._axon_domain.kind != F.BM_DOM_INPUT:
+                continue
+            k = 0
+            for sig in ls._axon_domain.sigs:
+                n = len(source_list(a, areas, lmaps, [sig]))
+                if sig == (track, tags):
+                    hits += [(i, k + j) for j in range(n)]
+                k += n
+        if not hits:
+            raise ValueError("Unable to find a layer within the area map matching the axon domain "
+                             "(track: %r, tags: %r) specified by the filter chain scheme." % (track, sorted(tags)))
+        if len(hits) > 1:
+            raise ValueError("Duplicate axon signatures (%r, %r) found within the layer map for area %r."
+                             % (track, sorted(tags), a.name))
+        i, k = hits[0]
+        S = d.layers[i].input_srcs[k]
+        if S.n_filters:
+            raise ValueError("two filter chains for the source (%r, %r)" % (track, sorted(tags)))
+        S.n_filters = len(chain)
+        for j, f in enumerate(chain):
+            S.filters[j] = f.kind
+
+
 def area_desc(area_name, lmaps, areas, settings=None, area_id=None):
     """Resolves one cortical area of `areas` into a bm_area_desc."""
     settings = settings or CorticalAreaSettings().disable_regrowth()
@@ -474,6 +544,7 @@ def area_desc(area_name, lmaps, areas, settings=None, area_id=None):
                     if sl.name not in idx:
                         raise ValueError("tuft source layer %r not in the layer map" % sl.name)
                     T.src[k] = F.bm_src_layer_desc(idx[sl.name], sl._reach, sl._prevalence)
+    _attach_filter_chains(d, a, areas, lmaps, lm)
     return d
 
 

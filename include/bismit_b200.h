@@ -60,7 +60,12 @@ extern "C" {
 #define BM_MAX_SRC_SLICES   32  /* source-slice pool per tuft (with prevalence) */
 #define BM_MAX_CTRL         4
 #define BM_MAX_IO           8
+#define BM_MAX_FILTERS      4   /* filters in one input filter chain            */
 #define BM_NAME_LEN         32
+
+/* Input filters (FilterScheme names, src/map/scheme/filter.rs; kernels of
+ * cl/filters.cl). */
+#define BM_FILTER_RETINA    1   /* "retina", cl/filters.cl:34-100 */
 
 /* ------------------------------------------------------- layer schemes --- */
 /* Layer kinds (src/map/scheme/layer.rs, src/map/mod.rs CellClass). */
@@ -138,10 +143,16 @@ typedef struct bm_tuft_desc {
 } bm_tuft_desc;
 
 /* One source feeding an axonal input layer: the dims of the source layer the
- * thalamic tract delivers (LayerInfo::new, src/map/layer_info.rs:142-215). */
+ * thalamic tract delivers (LayerInfo::new, src/map/layer_info.rs:142-215),
+ * and the filter chain its frames pass through on intake: the chain an
+ * AreaScheme::filter_chain entry (src/map/scheme/area.rs:70-85) attaches to
+ * the one source whose input signature it names
+ * (LayerMap::src_layer_info_by_sig, src/map/layer_map.rs:242-261). */
 typedef struct bm_input_src_desc {
     uint32_t v_size, u_size, depth;
     uint32_t axon_topology;
+    uint32_t n_filters;                /* 0: frames written straight to the axons */
+    uint32_t filters[BM_MAX_FILTERS];  /* BM_FILTER_*, first applied first        */
 } bm_input_src_desc;
 
 typedef struct bm_layer_desc {
@@ -257,6 +268,21 @@ typedef struct bm_io_plan {
     uint32_t len;           /* axons                                          */
 } bm_io_plan;
 
+/* One input filter chain (AxonSpace::new, src/cortex/axon_space.rs:338-412):
+ * filter k reads its input buffer (depth x v_size x u_size bytes) and writes
+ * the next filter's, the last one the target axon slices. Frames for the
+ * source land in the first buffer; the chain runs at the head of every cycle
+ * unless BM_SET_BYPASS_FILTERS is set (AxonSpace::intake, :510-525). */
+typedef struct bm_filter_chain_plan {
+    uint32_t input;          /* index into bm_area_plan.inputs                */
+    uint32_t frame_off;      /* the source's first byte within that input      */
+    uint32_t tar_slc;        /* first target axon slice (tar_slc_range.start)  */
+    uint32_t depth, v_size, u_size;
+    uint32_t n_filters;
+    uint32_t filters[BM_MAX_FILTERS];
+    uint64_t buf_off[BM_MAX_FILTERS];  /* each filter's input buffer in the slab */
+} bm_filter_chain_plan;
+
 typedef struct bm_area_plan {
     uint32_t area_id;
     uint32_t v_size, u_size;
@@ -283,6 +309,8 @@ typedef struct bm_area_plan {
     uint64_t slab_bytes;
     uint64_t n_syns_total;
     uint64_t rnd_seed;                   /* per-launch random stream key      */
+    uint32_t n_filter_chains;
+    bm_filter_chain_plan filter_chains[BM_MAX_IO];
 } bm_area_plan;
 
 /* ------------------------------------------------------------ handles ---- */

@@ -45,6 +45,8 @@ def load_port():
         vp, u32, u64 = C.c_void_p, C.c_uint32, C.c_uint64
         L.bmo_run.restype = C.c_int
         L.bmo_run.argtypes = [vp, vp, vp, u64, u32, u64, C.c_int]
+        L.bmo_intake.restype = C.c_int
+        L.bmo_intake.argtypes = [vp, vp, u32, u32, vp, u32]
         L.bmo_grow.restype = C.c_int
         L.bmo_grow.argtypes = [vp, vp, u64, u32]
         L.bmo_rnd.restype = C.c_int32
@@ -94,6 +96,16 @@ def run(plan, slab, frames=None, n_cycles=1, start_cycle=0, threads=0, impl="por
     rc = fn(C.cast(_plan_ptr(plan), C.c_void_p), _np_ptr(slab), _np_ptr(frames), flen, n_cycles, start_cycle, threads)
     if rc != 0:
         raise RuntimeError("oracle run failed (%d)" % rc)
+
+
+def intake(plan, slab, input_idx, offset, data):
+    """Writes `data` at byte `offset` of a frame of input `input_idx`, where
+    intake puts it (a filtered source's bytes into its chain's first buffer)."""
+    data = np.ascontiguousarray(data, dtype=np.uint8)
+    rc = load_port().bmo_intake(C.cast(_plan_ptr(plan), C.c_void_p), _np_ptr(slab), input_idx, offset,
+                                _np_ptr(data), data.size)
+    if rc != 0:
+        raise RuntimeError("oracle intake out of range")
 
 
 def grow(plan, slab, seed, init_flags):

@@ -561,6 +561,84 @@ static void k_smooth_activity(lview* V, int r) {
     free(c);
 }
 
+/* retina (cl/filters.cl:34-100) over a (depth, vs, us) grid of input bytes:
+ * cell i is off-center when bit 0 of i is set and large when bits 1 and 0
+ * differ; get_neighbors_avg (:8-31) sums the hexagon of radius 5 (large) or 3
+ * (small) in the cell's slice, a cell outside the grid reading as 0
+ * (cel_state_3d_safe, cl/bismit.cl:285-297) but counted all the same. The
+ * output goes to slice base_slc + slice at that slice's first axon
+ * (get_axn_idz, cl/bismit.cl:117-119) plus the cell's place in the slice. */
+static void k_retina(const bm_area_plan* P, const uint8_t* in, uint8_t* out, uint32_t base_slc,
+                     uint32_t depth, uint32_t vs, uint32_t us) {
+    const uint32_t cols = vs * us;
+    for (uint32_t i = 0; i < depth * cols; i++) {
+        const uint32_t slc = i / cols, col = i % cols;
+        const int v = (int)(col / us), u = (int)(col % us);
+        const int off_cen = (int)(i & 1), large = (int)((i & 3) >> 1) ^ off_cen;
+        const int r = large ? 5 : 3;
+        int sum = 0, count = 0;
+        for (int vo = -r; vo <= r; vo++) {
+            const int uz = imax(-r, -vo - r), um = imin(r, -vo + r);
+            for (int uo = uz; uo <= um; uo++) {
+                const int vv = v + vo, uu = u + uo;
+                if (vv >= 0 && vv < (int)vs && uu >= 0 && uu < (int)us)
+                    sum += in[slc * cols + (uint32_t)(vv * (int)us + uu)];
+                count++;
+            }
+        }
+        const int avg = sum / count, center = in[i];
+        int st = 0;
+        if (off_cen) {
+            const int cst = center + 48;   /* RETNAL_THRESHOLD, cl/bismit.cl:19 */
+            if (avg > cst) st = avg - cst;
+        } else {
+            const int nat = avg + 48;
+            if (center > nat) st = center - nat;
+        }
+        out[P->slc_axn_idz[(base_slc + slc) & 0xFF] + col] = (uint8_t)st;
+    }
+}
+
+static int filters_run(const bm_area_plan* P) {
+    return P->n_filter_chains && !(P->settings & BM_SET_BYPASS_FILTERS);
+}
+
+/* AxonSpace::intake (src/cortex/axon_space.rs:510-525): every filter of each
+ * chain in order, filter k from its buffer to the next one's (output slices
+ * from slice 0), the last to the target slices (SensoryFilter::new and
+ * ::cycle, src/cortex/sensory_filter.rs:25-110,157-168). */
+static void run_filters(const bm_area_plan* P, uint8_t* slab) {
+    if (!filters_run(P)) return;
+    for (uint32_t k = 0; k < P->n_filter_chains; k++) {
+        const bm_filter_chain_plan* c = &P->filter_chains[k];
+        for (uint32_t f = 0; f < c->n_filters; f++) {
+            const int last = f + 1 == c->n_filters;
+            k_retina(P, slab + c->buf_off[f], last ? slab + P->axon_off : slab + c->buf_off[f + 1],
+                     last ? c->tar_slc : 0, c->depth, c->v_size, c->u_size);
+        }
+    }
+}
+
+/* Bytes [off, off + len) of a frame of input `input`: a source with a running
+ * filter chain goes to the chain's first buffer (SensoryFilter::write,
+ * sensory_filter.rs:122-155), the rest straight to the input's axons
+ * (axon_space.rs:526-560). */
+int bmo_intake(const bm_area_plan* P, uint8_t* slab, uint32_t input, uint32_t off, const uint8_t* data,
+               uint32_t len) {
+    if (input >= P->n_inputs || off > P->inputs[input].len || len > P->inputs[input].len - off) return -1;
+    uint8_t* axns = slab + P->axon_off + P->inputs[input].axn_idz;
+    for (uint32_t b = off; b < off + len; b++) {
+        uint8_t* dst = axns + b;
+        for (uint32_t k = 0; filters_run(P) && k < P->n_filter_chains; k++) {
+            const bm_filter_chain_plan* c = &P->filter_chains[k];
+            const uint32_t c0 = c->frame_off, c1 = c0 + c->depth * c->v_size * c->u_size;
+            if (c->input == input && b >= c0 && b < c1) dst = slab + c->buf_off[0] + (b - c0);
+        }
+        *dst = data[b - off];
+    }
+    return 0;
+}
+
 /* --------------------------------------------------------- layer steps --- */
 
 /* Control layers hosted on V in (host, exe_order) order
@@ -648,6 +726,7 @@ static void area_cycle(const bm_area_plan* P, uint8_t* slab, uint64_t cyc) {
     uint8_t* axns = slab + P->axon_off;
     lview V[BM_MAX_LAYERS];
     for (uint32_t l = 0; l < P->n_layers; l++) view(&P->layers[l], slab, &V[l]);
+    run_filters(P, slab);
     if (!(P->settings & BM_SET_DISABLE_SSCS)) {
         for (uint32_t k = 0; k < P->n_cycle_order; k++) {
             lview* v = &V[P->cycle_order[k]];
@@ -681,7 +760,7 @@ int bmo_run(const bm_area_plan* P, uint8_t* slab, const uint8_t* frames, uint64_
     if (frames && P->n_inputs == 0) return -1;
     if (frames && frame_len != P->inputs[0].len) return -2;
     for (uint32_t k = 0; k < n_cycles; k++) {
-        if (frames) memcpy(slab + P->axon_off + P->inputs[0].axn_idz, frames + (uint64_t)k * frame_len, frame_len);
+        if (frames) bmo_intake(P, slab, 0, 0, frames + (uint64_t)k * frame_len, P->inputs[0].len);
         area_cycle(P, slab, start_cycle + k);
     }
     return 0;

@@ -25,6 +25,12 @@ extern "C" {
 int32_t bmo_rnd(uint64_t seed, uint32_t area_id, uint32_t layer_id, uint32_t role,
                 uint32_t tft_id, uint64_t cycle);
 
+/* Writes bytes [off, off + len) of a frame of input `input` where intake puts
+ * them: a source with a running filter chain into the chain's first buffer,
+ * the rest into the input's axons. */
+int bmo_intake(const bm_area_plan* plan, uint8_t* slab, uint32_t input, uint32_t off, const uint8_t* data,
+               uint32_t len);
+
 /* Runs n_cycles cycles on `slab` (plan->slab_bytes bytes). Before cycle k the
  * frame frames + k*frame_len (if frames != NULL) is written to input 0.
  * Cycle numbers start at start_cycle. n_threads <= 1 runs single-threaded. */

@@ -1,6 +1,7 @@
 """Prepares bismit's OpenCL kernel sources for compilation as C++ (TEST INFRASTRUCTURE).
 
-Reads cl/bismit.cl, cl/syns.cl, cl/control.cl and cl/tests.cl from a bismit
+Reads cl/bismit.cl, cl/syns.cl, cl/control.cl, cl/filters.cl and cl/tests.cl
+from a bismit
 checkout and writes their concatenation to an output file (under oracle/_ref/,
 never committed), changing exactly one construct: OpenCL vector literals
 ``(int4)(a, b, c, d)`` become C++ constructor calls ``int4(a, b, c, d)``. In
@@ -13,7 +14,7 @@ Usage: python prep_cl.py <bismit checkout> <output file>
 import re
 import sys
 
-FILES = ["cl/bismit.cl", "cl/syns.cl", "cl/control.cl", "cl/tests.cl"]
+FILES = ["cl/bismit.cl", "cl/syns.cl", "cl/control.cl", "cl/filters.cl", "cl/tests.cl"]
 VEC_CAST = re.compile(r"\((u?char4|u?short4|u?int4)\)\s*\(")
 
 

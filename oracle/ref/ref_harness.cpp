@@ -2,7 +2,7 @@
 // INFRASTRUCTURE: the reference-side checker and the reference CPU baseline).
 //
 // The kernel text comes verbatim from a bismit checkout (cl/bismit.cl,
-// cl/syns.cl, cl/control.cl, cl/tests.cl), prepared by prep_cl.py and compiled
+// cl/syns.cl, cl/control.cl, cl/filters.cl, cl/tests.cl), prepared by prep_cl.py and compiled
 // as C++ against cl_compat.hpp. This file supplies what bismit's Rust host
 // supplies: the -D build options (src/cmn/mod.rs:400-442,
 // src/map/area_map.rs:51-77), the NDRange of every launch and its arguments
@@ -337,6 +337,48 @@ static void layer_learn(Area& A, Layer& Y, uint64_t cyc) {
     else tufts_learn(A, Y, cyc);
 }
 
+static bool filters_run(const bm_area_plan* P) {
+    return P->n_filter_chains && !(P->settings & BM_SET_BYPASS_FILTERS);
+}
+
+// One frame of input 0: a source with a running filter chain goes to the
+// chain's first buffer (SensoryFilter::write, src/cortex/sensory_filter.rs:
+// 122-155), the rest to the input's axons (AxonSpace::intake,
+// src/cortex/axon_space.rs:510-560).
+static void intake(const bm_area_plan* P, uint8_t* slab, const uint8_t* frame) {
+    const bm_io_plan& io = P->inputs[0];
+    uint8_t* axns = slab + P->axon_off + io.axn_idz;
+    for (uint32_t b = 0; b < io.len; b++) {
+        uint8_t* dst = axns + b;
+        for (uint32_t k = 0; filters_run(P) && k < P->n_filter_chains; k++) {
+            const bm_filter_chain_plan& c = P->filter_chains[k];
+            const uint32_t c0 = c.frame_off, c1 = c0 + c.depth * c.v_size * c.u_size;
+            if (c.input == 0 && b >= c0 && b < c1) dst = slab + c.buf_off[0] + (b - c0);
+        }
+        *dst = frame[b];
+    }
+}
+
+// SensoryFilter::cycle of every filter of each chain in order: the
+// (depth, v, u) NDRange in 1 x 8 x 8 work-groups, arguments (input buffer,
+// output slice base, output buffer) as SensoryFilter::new binds them
+// (src/cortex/sensory_filter.rs:47-54; the last filter's output is the axon
+// space at the target slices, an inner one's the next filter's buffer from
+// slice 0, src/cortex/axon_space.rs:353-365).
+static void run_filters(Area& A, uint8_t* slab) {
+    if (!filters_run(A.P)) return;
+    for (uint32_t k = 0; k < A.P->n_filter_chains; k++) {
+        const bm_filter_chain_plan& c = A.P->filter_chains[k];
+        for (uint32_t f = 0; f < c.n_filters; f++) {
+            const bool last = f + 1 == c.n_filters;
+            const uchar* in = slab + c.buf_off[f];
+            uchar* out = last ? A.axns : slab + c.buf_off[f + 1];
+            const uchar base = (uchar)(last ? c.tar_slc : 0);
+            A.err |= launch(c.depth, c.v_size, c.u_size, 1, 8, 8, [&] { clref::retina(in, base, out); });
+        }
+    }
+}
+
 }  // namespace
 
 extern "C" {
@@ -357,7 +399,8 @@ int bmr_run(const bm_area_plan* P, uint8_t* slab, const uint8_t* frames, uint64_
     }
     for (uint32_t k = 0; k < n_cycles; k++) {
         uint64_t cyc = start_cycle + k;
-        if (frames) memcpy(A.axns + P->inputs[0].axn_idz, frames + (uint64_t)k * frame_len, frame_len);
+        if (frames) intake(P, slab, frames + (uint64_t)k * frame_len);
+        run_filters(A, slab);
         // CorticalArea::cycle, src/cortex/cortical_area.rs:716-789.
         if (!(P->settings & BM_SET_DISABLE_SSCS)) {
             for (uint32_t i = 0; i < P->n_cycle_order; i++) {

@@ -13,6 +13,9 @@ SCHEMES = {
     "area_64": lambda: configs.workload("area_64")[:2],
     "area_48_deep": lambda: configs.workload("area_48_deep")[:2],
     "smoother": lambda: configs.smoother_area(),
+    "testbed_retina": lambda: configs.testbed_area(retina=True),
+    "retina": lambda: configs.retina_area(48, n_filters=2, src_depth=2),
+    "retina_scaled": lambda: configs.retina_area(64, n_filters=3, src_side=32),
 }
 
 
@@ -30,6 +33,8 @@ def settings_for(kind="default", plain=False):
         s.disable_pyrs()
     elif kind == "no_sscs":
         s.disable_sscs()
+    elif kind == "bypass_filters":
+        s.bypass_filters()
     elif kind == "zero_strength":
         s.strengths_start_at_zero()
     if plain:
@@ -55,6 +60,10 @@ def buffers(plan):
         for k, n in enumerate(F.BUF_NAMES):
             if L.buf_off[k] != NO_BUF:
                 out.append(("L%d.%s" % (l, n), int(L.buf_off[k]), int(L.buf_len[k])))
+    for c in range(plan.n_filter_chains):
+        ch = plan.filter_chains[c]
+        for k in range(ch.n_filters):
+            out.append(("filter%d.in%d" % (c, k), int(ch.buf_off[k]), int(ch.depth * ch.v_size * ch.u_size)))
     return out
 
 

@@ -89,3 +89,29 @@ def test_rnd_stream_is_host_computable():
     b = lib.bm_rnd(7, 1, 2, 1, 0, 5)
     assert a == b
     assert lib.bm_rnd(7, 1, 2, 1, 0, 6) != b
+
+
+STRUCTS = ["bm_src_layer_desc", "bm_tuft_desc", "bm_input_src_desc", "bm_layer_desc", "bm_area_desc",
+           "bm_tuft_plan", "bm_ctrl_plan", "bm_layer_plan", "bm_io_plan", "bm_filter_chain_plan", "bm_area_plan"]
+
+
+def test_ctypes_structures_match_the_header(tmp_path):
+    """Every descriptor and plan structure of the ctypes mirror has the C
+    compiler's size and field offsets."""
+    import subprocess
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "bismit_b200.h"', "int main(void) {"]
+    for name in STRUCTS:
+        lines.append('printf("%s %%zu\\n", sizeof(%s));' % (name, name))
+        for f, _ in getattr(F, name)._fields_:
+            lines.append('printf("%s.%s %%zu\\n", offsetof(%s, %s));' % (name, f, name, f))
+    lines.append("return 0; }")
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-std=c11", "-I", os.path.join(ROOT, "include"), "-o", str(exe), str(src)], check=True)
+    got = dict(l.split() for l in subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split("\n") if l)
+    for name in STRUCTS:
+        S = getattr(F, name)
+        assert int(got[name]) == C.sizeof(S), name
+        for f, _ in S._fields_:
+            assert int(got[name + "." + f]) == getattr(S, f).offset, name + "." + f

@@ -60,9 +60,40 @@ def _run_parity(ctx, scheme, kind, plain, cycles, scramble=True, active=0.05, st
 
 
 @pytest.mark.parametrize("plain", [True, False], ids=["plain", "fused"])
-@pytest.mark.parametrize("scheme", ["testbed", "mixed", "area_64", "area_48_deep", "smoother"])
+@pytest.mark.parametrize("scheme", ["testbed", "mixed", "area_64", "area_48_deep", "smoother", "testbed_retina",
+                                    "retina", "retina_scaled"])
 def test_cycles_match_oracle(ctx, scheme, plain):
     _run_parity(ctx, scheme, "default", plain, cycles=6)
+
+
+@pytest.mark.parametrize("plain", [True, False], ids=["plain", "fused"])
+def test_bypassed_filters_match_oracle(ctx, plain):
+    """With bypass_filters the frames go straight to the axons and no filter
+    runs (AxonSpace::intake, src/cortex/axon_space.rs:516)."""
+    _run_parity(ctx, "retina", "bypass_filters", plain, cycles=3)
+
+
+def test_filtered_frames_from_device_match_oracle(ctx):
+    """Per-cycle frames taken from device memory land in the filter chain's
+    buffer as host-written ones do; a cycle with no new frame filters the
+    stored one again."""
+    import torch
+    area = _area(ctx, "retina", settings_for())
+    plan = area.plan
+    slab = initial_slab(plan, 7, scramble_seed=11)
+    area.write_slab(slab)
+    area.set_cycle(0)
+    fr = frames_for(plan, 4, 5, 0.05)
+    dev = torch.from_numpy(np.ascontiguousarray(fr[:3])).to("cuda:0")
+    torch.cuda.synchronize()
+    area.cycle_frames_device(dev.data_ptr(), fr.shape[1], 3)
+    area.cycle(1)
+    ora = slab.copy()
+    oracle.run(plan, ora, fr[:3], 3, start_cycle=0)
+    oracle.run(plan, ora, None, 1, start_cycle=3)
+    got = area.read_slab()
+    assert np.array_equal(got, ora), diff_report(plan, got, ora)
+    area.close()
 
 
 @pytest.mark.parametrize("plain", [True, False], ids=["plain", "fused"])

@@ -27,20 +27,30 @@ def _oracle_cycle(plans, slabs, tracts, ext_frame, cycle):
     outs = [s[int(p.axon_off):].copy() for p, s in zip(plans, slabs)]
     for (s, o, d, i, off, n) in tracts:
         src = int(plans[s].outputs[o].axn_idz)
-        dst = int(plans[d].axon_off) + int(plans[d].inputs[i].axn_idz) + off
-        slabs[d][dst:dst + n] = outs[s][src:src + n]
-    P0 = plans[0]
-    a0 = int(P0.axon_off) + int(P0.inputs[0].axn_idz)
-    slabs[0][a0:a0 + ext_frame.size] = ext_frame
+        oracle.intake(plans[d], slabs[d], i, off, outs[s][src:src + n])
+    oracle.intake(plans[0], slabs[0], 0, 0, ext_frame)
     for p, s in zip(plans, slabs):
         oracle.run(p, s, None, 1, start_cycle=cycle)
 
 
+def _with_filters(lm, ar):
+    """Retina chains on an external input (v1), on a tract-fed feed-forward
+    input two slices deep (v2, two filters) and on a feedback input (v2)."""
+    ar.by_name("v1").filter_chain(M.InputTrack.Afferent, [M.THAL_SP], ["retina"])
+    ar.by_name("v2").filter_chain(M.InputTrack.Afferent, [M.THAL_SP], ["retina", "retina"])
+    ar.by_name("v2").filter_chain(M.InputTrack.Efferent, [M.THAL_SP], ["retina"])
+    return lm, ar
+
+
 @pytest.mark.gpu
-def test_hierarchy_matches_oracle():
+@pytest.mark.parametrize("filters", [False, True], ids=["plain_inputs", "filtered_inputs"])
+def test_hierarchy_matches_oracle(filters):
     lm, ar, names = configs.hierarchy(SIDES)
+    if filters:
+        _with_filters(lm, ar)
     cx = Cortex.builder(lm, ar).ca_settings(configs.bench_settings()).seed(3).build()
     plans = [cx.area(n).plan for n in names]
+    assert sum(int(p.n_filter_chains) for p in plans) == (3 if filters else 0)
     slabs = []
     for k, n in enumerate(names):
         s = cx.area(n).read_slab()

@@ -11,7 +11,8 @@ from bismit_b200 import _ffi as F, configs, map as M
 from helpers import diff_report, frames_for, initial_slab, plan_for, scramble, settings_for
 
 
-@pytest.mark.parametrize("scheme", ["testbed", "mixed", "area_64", "area_48_deep", "smoother"])
+@pytest.mark.parametrize("scheme", ["testbed", "mixed", "area_64", "area_48_deep", "smoother", "testbed_retina",
+                                    "retina", "retina_scaled"])
 @pytest.mark.parametrize("kind", ["default", "bypass_inhib", "no_learning", "zero_strength"])
 def test_port_matches_reference_kernels(ref_oracle, scheme, kind):
     _, plan = plan_for(scheme, settings_for(kind))
@@ -110,3 +111,91 @@ def test_smoother_only_nudges_energies():
         else:
             assert np.array_equal(na[name], nb[name]), name
     assert moved > 0
+
+
+def _retina_py(grid):
+    """retina (cl/filters.cl:34-100) over a (depth, v, u) uint8 grid, written
+    out loop by loop from the kernel text: the cell index picks off-center
+    (bit 0) and large (bit 1 xor bit 0) cells, the hexagon of radius 5 or 3
+    is averaged with cells outside the grid read as 0, and the cell's output
+    is its margin over the threshold 48 (cl/bismit.cl:19)."""
+    depth, vs, us = grid.shape
+    out = np.zeros_like(grid)
+    for s in range(depth):
+        for v in range(vs):
+            for u in range(us):
+                i = (s * vs + v) * us + u
+                off_cen = i & 1
+                large = ((i & 3) >> 1) ^ off_cen
+                r = 5 if large else 3
+                tot = cnt = 0
+                for vo in range(-r, r + 1):
+                    for uo in range(max(-r, -vo - r), min(r, -vo + r) + 1):
+                        vv, uu = v + vo, u + uo
+                        if 0 <= vv < vs and 0 <= uu < us:
+                            tot += int(grid[s, vv, uu])
+                        cnt += 1
+                avg, c = tot // cnt, int(grid[s, v, u])
+                if off_cen:
+                    out[s, v, u] = avg - (c + 48) if avg > c + 48 else 0
+                else:
+                    out[s, v, u] = c - (avg + 48) if c > avg + 48 else 0
+    return out
+
+
+@pytest.mark.parametrize("n_filters,depth", [(1, 1), (1, 2), (2, 2)])
+def test_retina_filter_known_answers(n_filters, depth):
+    """The input axons after a cycle are the retina chain applied to the frame
+    (each filter of a chain of two reads the previous one's whole output, the
+    slices of a two-deep source being back to back from axon 0); bypassing the
+    filters leaves the frame itself; a cycle without a new frame filters the
+    same stored frame again, not the filtered output."""
+    from bismit_b200 import plan_of
+    side = 16
+    for bypass in (False, True):
+        st = configs.bench_settings()
+        if bypass:
+            st.bypass_filters()
+        plan = plan_of(M.area_desc("v1", *configs.retina_area(side, n_filters, depth), st), 3)
+        assert plan.n_filter_chains == 1
+        io = plan.inputs[0]
+        assert io.len == depth * side * side
+        slab = np.zeros(int(plan.slab_bytes), np.uint8)
+        oracle.grow(plan, slab, 3, 0)
+        rng = np.random.default_rng(depth * 10 + n_filters)
+        frame = rng.integers(0, 256, size=(1, io.len), dtype=np.uint8)
+        frame[0, rng.random(io.len) < 0.5] = 0     # sparse enough for both cell kinds to fire
+        want = frame[0].reshape(depth, side, side)
+        if not bypass:
+            for _ in range(n_filters):
+                want = _retina_py(want)
+            assert np.count_nonzero(want) > 0
+        a0 = int(plan.axon_off + io.axn_idz)
+        oracle.run(plan, slab, frame, 1, start_cycle=0)
+        assert np.array_equal(slab[a0:a0 + io.len], want.reshape(-1))
+        oracle.run(plan, slab, None, 1, start_cycle=1)
+        assert np.array_equal(slab[a0:a0 + io.len], want.reshape(-1))
+
+
+def test_filter_chain_plans_and_refusals():
+    """Chains resolve to the source their signature names, with one
+    depth x v x u buffer per filter; source dims that are not multiples of 8
+    (the 1 x 8 x 8 work-groups of SensoryFilter::new) and unknown or custom
+    filters are refused."""
+    from bismit_b200 import plan_of
+    plan = plan_of(M.area_desc("v1", *configs.retina_area(64, 3, 1, src_side=32), configs.bench_settings()), 1)
+    c = plan.filter_chains[0]
+    assert (c.input, c.frame_off, c.tar_slc, c.depth, c.v_size, c.u_size, c.n_filters) == (0, 0, 0, 1, 32, 32, 3)
+    assert all(c.filters[k] == F.BM_FILTER_RETINA for k in range(3))
+    offs = [int(c.buf_off[k]) for k in range(3)]
+    assert all(o % 256 == 0 for o in offs) and offs == sorted(offs) and offs[-1] + 1024 <= plan.slab_bytes
+    with pytest.raises(F.BismitError, match="multiples of 8"):
+        plan_of(M.area_desc("v1", *configs.retina_area(44), configs.bench_settings()), 1)
+    with pytest.raises(ValueError, match="unknown filter"):
+        M.FilterScheme("sharpen")
+    with pytest.raises(ValueError, match="custom OpenCL"):
+        M.FilterScheme("retina", "my_filters.cl")
+    lmaps, areas = configs.retina_area(48)
+    areas.by_name("v1").filter_chain(M.InputTrack.Efferent, [M.THAL_SP], ["retina"])
+    with pytest.raises(ValueError, match="Unable to find a layer"):
+        M.area_desc("v1", lmaps, areas, configs.bench_settings())
