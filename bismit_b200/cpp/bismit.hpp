@@ -218,10 +218,30 @@ struct LayerMapSchemeList {
 };
 
 // AreaScheme::new(name, layer_map_name, side) (src/map/scheme/area.rs:22-198).
+// FilterScheme::new(filter_name, cl_file_name) (src/map/scheme/filter.rs:3-40):
+// one filter of an input filter chain, named by its kernel. The built-in
+// filter is "retina" (cl/filters.cl:34-100); a kernel from a custom OpenCL
+// file has no counterpart here.
+struct FilterScheme {
+    std::string filter_name;
+    uint32_t kind = 0;
+    FilterScheme(const std::string& name, const char* cl_file_name = nullptr) : filter_name(name) {
+        if (name != "retina") invalid("unknown filter '" + name + "' (built in: retina)");
+        if (cl_file_name) invalid("filter '" + name + "': kernels from custom OpenCL files are not supported");
+        kind = BM_FILTER_RETINA;
+    }
+};
+
+struct FilterChain {
+    AxonSig sig;
+    std::vector<FilterScheme> filters;
+};
+
 struct AreaScheme {
     std::string name, layer_map_name;
     uint32_t v_size, u_size;
     std::vector<std::string> eff, aff, other;
+    std::vector<FilterChain> chains;
 
     AreaScheme(std::string n, std::string lm, uint32_t side)
         : name(std::move(n)), layer_map_name(std::move(lm)), v_size(side), u_size(side) {}
@@ -233,6 +253,16 @@ struct AreaScheme {
     AreaScheme eff_areas(std::vector<std::string> v) const { auto c = *this; c.eff = std::move(v); return c; }
     AreaScheme aff_areas(std::vector<std::string> v) const { auto c = *this; c.aff = std::move(v); return c; }
     AreaScheme other_areas(std::vector<std::string> v) const { auto c = *this; c.other = std::move(v); return c; }
+    // AreaScheme::filter_chain (src/map/scheme/area.rs:70-85): frames of the
+    // source matched by the input signature (track, tags) pass through the
+    // filters in order.
+    AreaScheme filter_chain(InputTrack track, const std::vector<std::string>& tags,
+                            std::vector<FilterScheme> filters) const {
+        if (filters.size() > BM_MAX_FILTERS) invalid("more than " + std::to_string(BM_MAX_FILTERS) + " filters in one chain");
+        auto c = *this;
+        c.chains.push_back({{track, std::set<std::string>(tags.begin(), tags.end())}, std::move(filters)});
+        return c;
+    }
 };
 
 struct AreaSchemeList {
@@ -370,6 +400,29 @@ inline bm_area_desc area_desc(const std::string& name, const LayerMapSchemeList&
                 }
             }
         }
+    }
+    // Each filter chain goes to the one source whose input signature it names
+    // (AxonSpace::new, src/cortex/axon_space.rs:340-345, with
+    // LayerMap::src_layer_info_by_sig, src/map/layer_map.rs:242-261).
+    for (const FilterChain& ch : a.chains) {
+        std::vector<std::pair<size_t, size_t>> hits;
+        for (size_t i = 0; i < lm.layers.size(); i++) {
+            const LayerScheme& ls = lm.layers[i];
+            if (ls.domain.kind != BM_DOM_INPUT) continue;
+            size_t k = 0;
+            for (const AxonSig& sig : ls.domain.sigs) {
+                const size_t n = source_list(a, areas, lmaps, {sig}).size();
+                if (sig.track == ch.sig.track && sig.tags == ch.sig.tags)
+                    for (size_t j = 0; j < n; j++) hits.push_back({i, k + j});
+                k += n;
+            }
+        }
+        if (hits.empty()) invalid("Unable to find a layer within the area map matching the axon domain specified by a filter chain scheme.");
+        if (hits.size() > 1) invalid("Duplicate axon signatures found within the layer map for area '" + name + "'.");
+        bm_input_src_desc& S = d.layers[hits[0].first].input_srcs[hits[0].second];
+        if (S.n_filters) invalid("two filter chains for one source");
+        S.n_filters = (uint32_t)ch.filters.size();
+        for (size_t j = 0; j < ch.filters.size(); j++) S.filters[j] = ch.filters[j].kind;
     }
     return d;
 }

@@ -173,11 +173,33 @@ int cmd_desc(const std::string& dir) {
             write_file(dir + "/hierarchy_" + n + ".bin", &d, sizeof d);
         }
     }
+    {
+        // The hierarchy with retina chains on an external, a feed-forward and
+        // a feedback input.
+        LayerMapSchemeList lm;
+        AreaSchemeList ar;
+        hierarchy(lm, ar, {32, 48, 24}, 2);
+        AreaSchemeList ar2;
+        for (const AreaScheme& a : ar.areas) {
+            AreaScheme b = a;
+            if (a.name == "v1") b = b.filter_chain(InputTrack::Afferent, {THAL_SP}, {FilterScheme("retina")});
+            if (a.name == "v2")
+                b = b.filter_chain(InputTrack::Afferent, {THAL_SP}, {FilterScheme("retina"), FilterScheme("retina")})
+                        .filter_chain(InputTrack::Efferent, {THAL_SP}, {FilterScheme("retina")});
+            ar2.area(b);
+        }
+        for (const char* n : {"v1", "v2"}) {
+            bm_area_desc d = area_desc(n, lm, ar2, settings());
+            write_file(dir + "/filtered_" + n + ".bin", &d, sizeof d);
+        }
+    }
     // Error behaviour: builder misuse and unresolvable schemes raise CmnError
     // with the C status code.
     bool ok = true;
     ok &= raises(BM_ERR_INVALID, [] { TuftSourceLayer::define("x").syn_reach(3).build(); });
     ok &= raises(BM_ERR_INVALID, [] { CellScheme::pyramidal().tft(TuftScheme::basal().syns_per_den(8)); });
+    ok &= raises(BM_ERR_INVALID, [] { FilterScheme("sharpen"); });
+    ok &= raises(BM_ERR_INVALID, [] { FilterScheme("retina", "my_filters.cl"); });
     ok &= raises(BM_ERR_INVALID, [] {
         LayerMapSchemeList lm;
         AreaSchemeList ar;

@@ -43,6 +43,10 @@ def test_cpp_builders_resolve_the_python_descriptors(exe, tmp_path):
     assert "errors ok" in r.stdout
     assert open(tmp_path / "area_64_v1.bin", "rb").read() == _py_desc(lambda: configs.workload("area_64"))
     assert open(tmp_path / "mixed_v1.bin", "rb").read() == _py_desc(lambda: configs.mixed_area(32, 48))
+    from test_hierarchy import _with_filters
+    for n in ("v1", "v2"):
+        want = _py_desc(lambda: _with_filters(*configs.hierarchy(SIDES)[:2]), n)
+        assert open(tmp_path / ("filtered_%s.bin" % n), "rb").read() == want, n
     lmaps, areas, names = configs.hierarchy(SIDES)
     for n in names:
         assert open(tmp_path / ("hierarchy_%s.bin" % n), "rb").read() == bytes(
