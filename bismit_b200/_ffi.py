@@ -219,6 +219,14 @@ def lib():
         "bm_sampler_set_timeout": (C.c_int, [vp, u32]),
         "bm_sampler_recv": (C.c_int, [vp, C.c_int, vp, u64, P(u64), P(C.c_int)]),
         "bm_sampler_stats": (C.c_int, [vp, P(u64), P(u64)]),
+        "bm_encode_images": (C.c_int, [vp, vp, u32, u32, u32, C.c_float, vp, u64, u32, u32]),
+        "bm_encode_hex_mold": (C.c_int, [vp, C.c_int32, u32, u32, vp, u32, u32]),
+        "bm_encode_scalar": (C.c_int, [vp, vp, u32, C.c_float, C.c_float, u64, vp, u64, u32, u32]),
+        "bm_sdr_writer_create": (C.c_int, [vp, C.c_float, C.c_float, C.c_float, u32, u32, u64, P(vp)]),
+        "bm_sdr_writer_destroy": (C.c_int, [vp]),
+        "bm_sdr_writer_info": (C.c_int, [vp, P(u32), P(u32), P(u32)]),
+        "bm_sdr_writer_waypoints": (C.c_int, [vp, vp, u64]),
+        "bm_sdr_writer_encode": (C.c_int, [vp, vp, u32, vp, u64]),
         "bm_area_write_slab": (C.c_int, [vp, vp, u64]),
         "bm_area_get_cycle": (C.c_int, [vp, P(u64)]),
         "bm_area_set_cycle": (C.c_int, [vp, u64]),

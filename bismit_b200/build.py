@@ -19,7 +19,7 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall",
          "--expt-relaxed-constexpr", "-Xptxas", "-warn-spills"]
-SOURCES = ["bm_api.cu", "bm_plain.cu", "bm_fused.cu", "bm_grow.cu", "bm_static.cu", "bm_batch.cu", "bm_server.cu", "bm_sampler.cu", "bm_layout.cpp"]
+SOURCES = ["bm_api.cu", "bm_plain.cu", "bm_fused.cu", "bm_grow.cu", "bm_static.cu", "bm_batch.cu", "bm_server.cu", "bm_sampler.cu", "bm_encode.cu", "bm_layout.cpp"]
 
 
 def _newer(src_paths, dst):

@@ -610,6 +610,44 @@ int bm_server_reset_stats(bm_server server);
 int32_t bm_rnd(uint64_t seed, uint32_t area_id, uint32_t layer_id, uint32_t role,
                uint32_t tft_id, uint64_t cycle);
 
+/* ------------------------------------------------------------ encoders ---
+ * Input encoders (src/encode/) as kernels writing frames in device memory on
+ * the context's stream. The f32 arithmetic follows the reference's operation
+ * by operation; its entropy-seeded random bytes and waypoint indices come
+ * from a seeded stream here. Frames are `frame_stride` bytes apart. */
+
+/* encode_2d_image (src/encode/mod.rs:66-93): n images of x_size x y_size
+ * bytes (contiguous, device) resampled onto v_size x u_size hexagonal frames
+ * (device). Cells whose pixel falls outside the image keep their bytes. */
+int bm_encode_images(bm_ctx ctx, const uint8_t* images, uint32_t n, uint32_t x_size, uint32_t y_size,
+                     float scale_factor, uint8_t* frames, uint64_t frame_stride, uint32_t v_size, uint32_t u_size);
+
+/* encode_hex_mold_scaled (src/encode/write/mod.rs:190-217): a 1 at every
+ * offset of gen_syn_offs(radius, calc_scale(frame, source)) around the
+ * frame's middle; other bytes are left alone. A mold that would leave the
+ * frame is refused. */
+int bm_encode_hex_mold(bm_ctx ctx, int32_t radius, uint32_t src_v_size, uint32_t src_u_size, uint8_t* frame,
+                       uint32_t v_size, uint32_t u_size);
+
+/* encode_scalar (src/encode/write/mod.rs:28-172): each of n values (host,
+ * n <= 4096, within [lo, hi], hi > 0) clears its frame and draws a hexagon
+ * of radius (v + u) / 32 of bytes in 64..127 along the frame's border. */
+int bm_encode_scalar(bm_ctx ctx, const float* vals, uint32_t n, float lo, float hi, uint64_t seed, uint8_t* frames,
+                     uint64_t frame_stride, uint32_t v_size, uint32_t u_size);
+
+/* ScalarSdrWriter (src/encode/write/scalar_sdr_writer.rs:96-235): waypoint
+ * SDRs every `way_span` across [lo, hi], each v*u/48 seeded axon indices
+ * (held on the device); encode blends the two waypoints around each value. */
+typedef struct bm_sdr_writer_s* bm_sdr_writer;
+int bm_sdr_writer_create(bm_ctx ctx, float lo, float hi, float way_span, uint32_t v_size, uint32_t u_size,
+                         uint64_t seed, bm_sdr_writer* out);
+int bm_sdr_writer_destroy(bm_sdr_writer w);
+int bm_sdr_writer_info(bm_sdr_writer w, uint32_t* way_count, uint32_t* active, uint32_t* len);
+/* The waypoint table (way_count x active indices) into host memory. */
+int bm_sdr_writer_waypoints(bm_sdr_writer w, uint32_t* dst, uint64_t n);
+/* n values (host, n <= 2048) -> n frames (device). */
+int bm_sdr_writer_encode(bm_sdr_writer w, const float* vals, uint32_t n, uint8_t* frames, uint64_t frame_stride);
+
 #ifdef __cplusplus
 }
 #endif

@@ -45,6 +45,17 @@ def load_port():
         vp, u32, u64 = C.c_void_p, C.c_uint32, C.c_uint64
         L.bmo_run.restype = C.c_int
         L.bmo_run.argtypes = [vp, vp, vp, u64, u32, u64, C.c_int]
+        f32 = C.c_float
+        L.bmo_encode_image.restype = None
+        L.bmo_encode_image.argtypes = [vp, u32, u32, f32, vp, u32, u32]
+        L.bmo_hex_mold.restype = C.c_int
+        L.bmo_hex_mold.argtypes = [C.c_int, u32, u32, vp, u32, u32]
+        L.bmo_encode_scalar.restype = C.c_int
+        L.bmo_encode_scalar.argtypes = [f32, f32, f32, u64, u32, vp, u32, u32]
+        L.bmo_sdr_waypoints.restype = C.c_int
+        L.bmo_sdr_waypoints.argtypes = [f32, f32, f32, u32, u32, u64, vp]
+        L.bmo_sdr_encode.restype = C.c_int
+        L.bmo_sdr_encode.argtypes = [f32, f32, f32, f32, u32, vp, vp, u32]
         L.bmo_intake.restype = C.c_int
         L.bmo_intake.argtypes = [vp, vp, u32, u32, vp, u32]
         L.bmo_grow.restype = C.c_int
@@ -142,3 +153,50 @@ def ref_axn_idxs(plan, depth, v_size, u_size, v_offs, u_offs):
     if rc != 0:
         raise RuntimeError("test_axn_idxs failed (%d)" % rc)
     return o1, o2
+
+
+# ----------------------------------------------------------------- encoders --
+
+def encode_image(image, scale_factor, v_size, u_size, target=None):
+    """encode_2d_image of one (x_size, y_size)-shaped image (rows of x_size
+    bytes, y_size rows) onto a v_size x u_size frame; cells outside the image
+    keep `target`'s bytes (zeros when not given)."""
+    img = np.ascontiguousarray(image, dtype=np.uint8)
+    y_size, x_size = img.shape
+    out = np.zeros(v_size * u_size, np.uint8) if target is None else np.array(target, np.uint8, copy=True)
+    load_port().bmo_encode_image(_np_ptr(img), x_size, y_size, scale_factor, _np_ptr(out), v_size, u_size)
+    return out
+
+
+def hex_mold(radius, src_dims, v_size, u_size):
+    out = np.zeros(v_size * u_size, np.uint8)
+    n = load_port().bmo_hex_mold(radius, src_dims[0], src_dims[1], _np_ptr(out), v_size, u_size)
+    if n < 0:
+        raise ValueError("hex mold refused")
+    return out, n
+
+
+def encode_scalar(vals, lo, hi, seed, v_size, u_size):
+    out = np.zeros((len(vals), v_size * u_size), np.uint8)
+    for k, v in enumerate(vals):
+        if load_port().bmo_encode_scalar(v, lo, hi, seed, k, _np_ptr(out[k]), v_size, u_size) != 0:
+            raise ValueError("value %r refused" % v)
+    return out
+
+
+def sdr_waypoints(lo, hi, way_span, v_size, u_size, seed):
+    n = load_port().bmo_sdr_waypoints(lo, hi, way_span, v_size, u_size, seed, None)
+    if n < 0:
+        raise ValueError("writer refused")
+    ways = np.zeros((n, (v_size * u_size) // 48), np.uint32)
+    load_port().bmo_sdr_waypoints(lo, hi, way_span, v_size, u_size, seed, _np_ptr(ways))
+    return ways
+
+
+def sdr_encode(vals, lo, hi, way_span, ways, length):
+    out = np.zeros((len(vals), length), np.uint8)
+    w = np.ascontiguousarray(ways, dtype=np.uint32)
+    for k, v in enumerate(vals):
+        if load_port().bmo_sdr_encode(v, lo, hi, way_span, w.shape[0], _np_ptr(w), _np_ptr(out[k]), length) != 0:
+            raise ValueError("value %r refused" % v)
+    return out

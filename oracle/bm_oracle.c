@@ -11,6 +11,7 @@
  */
 #include "bm_oracle.h"
 
+#include <math.h>
 #include <stdlib.h>
 #include <string.h>
 #ifdef _OPENMP
@@ -999,4 +1000,157 @@ static void regrow_layer(const bm_area_plan* P, lview* V, uint64_t cyc) {
         }
         free_pools(&Q);
     }
+}
+
+/* ------------------------------------------------------------ encoders --- */
+
+static uint64_t enc_splitmix(uint64_t x) {
+    x += 0x9E3779B97F4A7C15ull;
+    x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+    x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+    return x ^ (x >> 31);
+}
+
+/* coord_hex_to_pixel, src/encode/mod.rs:52-72 (f32, as written). */
+static int enc_hex_to_pixel(float v_id, float u_id, float x_size, float y_size, float hex_side, float x_ofs,
+                            float y_ofs, float* xo, float* yo) {
+    const float u = u_id;
+    const float u_inv = 0.0f - u;
+    const float v = v_id;
+    const float w_inv = v + u;
+    float x = w_inv * 1.5f * hex_side;
+    float y = (u_inv + (w_inv / 2.0f)) * 1.73205080756f * hex_side;
+    x -= x_ofs;
+    y += y_ofs;
+    *xo = x;
+    *yo = y;
+    return (y >= 0.0f && y < y_size) && (x >= 0.0f && x < x_size);
+}
+
+/* encode_2d_image (src/encode/mod.rs:66-93) with calc_offs (:36-48), whose
+ * caller hands it (x_size, y_size) in the slots it names (y_size, x_size). */
+void bmo_encode_image(const uint8_t* source, uint32_t x_size, uint32_t y_size, float scale_factor,
+                      uint8_t* target, uint32_t v_size, uint32_t u_size) {
+    const float hex_side = (float)(x_size + y_size) / (scale_factor * (float)(v_size + u_size));
+    /* calc_offs(v_size, u_size, y_size := x_size, x_size := y_size, hex_side) */
+    const uint32_t co_y = x_size, co_x = y_size;
+    float x_ofs_inv, y_ofs_inv;
+    enc_hex_to_pixel((float)(v_size >> 1), (float)(u_size >> 1), (float)co_x, (float)co_y, hex_side, 0.0f, 0.0f,
+                     &x_ofs_inv, &y_ofs_inv);
+    const float x_ofs = x_ofs_inv - (float)(co_x >> 1);
+    const float y_ofs = (float)(co_y >> 1) - y_ofs_inv;
+    for (uint32_t v = 0; v < v_size; v++)
+        for (uint32_t u = 0; u < u_size; u++) {
+            float x, y;
+            if (enc_hex_to_pixel((float)v, (float)u, (float)x_size, (float)y_size, hex_side, x_ofs, y_ofs, &x, &y))
+                target[v * u_size + u] = source[(uint32_t)y * x_size + (uint32_t)x];
+        }
+}
+
+/* calc_scale, src/cmn/slice_dims.rs:201-224; -1 where the reference errs. */
+static int64_t enc_calc_scale(uint32_t src_dim, uint32_t tar_dim) {
+    const uint64_t src = (uint64_t)src_dim * 1024, tar = (uint64_t)tar_dim * 1024;
+    if (tar == 0) return -1;
+    const uint64_t incr = tar < 16 ? 1 : tar / 16;
+    const uint64_t s = src / incr;
+    return (s == 0 || s > 255) ? -1 : (int64_t)s;
+}
+
+/* encode_hex_mold_scaled (src/encode/write/mod.rs:190-217): -1 where the
+ * scales or offsets fail, or a tile would leave the frame. */
+int bmo_hex_mold(int radius, uint32_t src_v, uint32_t src_u, uint8_t* frame, uint32_t v_size, uint32_t u_size) {
+    const int64_t vs = enc_calc_scale(v_size, src_v), us = enc_calc_scale(u_size, src_u);
+    if (vs < 0 || us < 0) return -1;
+    int8_t ov[3 * 127 * 128 + 1], ou[3 * 127 * 128 + 1];
+    const int n = bmo_gen_syn_offs(radius, (uint32_t)vs, (uint32_t)us, ov, ou, 3 * 127 * 128 + 1);
+    if (n < 0) return -1;
+    for (int k = 0; k < n; k++) {
+        const int row = ov[k] + (int)(v_size / 2), col = ou[k] + (int)(u_size / 2);
+        if (row < 0 || row >= (int)v_size || col < 0 || col >= (int)u_size) return -1;
+    }
+    for (int k = 0; k < n; k++)
+        frame[(uint32_t)((ov[k] + (int)(v_size / 2)) * (int)u_size + ou[k] + (int)(u_size / 2))] = 1;
+    return n;
+}
+
+/* encode_scalar (src/encode/write/mod.rs:28-172) for frame `frame_idx` of a
+ * call: clears the frame and draws the hexagon. Its random bytes (64..127)
+ * come from the seeded stream (the reference's are entropy-seeded). */
+int bmo_encode_scalar(float val, float lo, float hi, uint64_t seed, uint32_t frame_idx, uint8_t* frame,
+                      uint32_t v_size, uint32_t u_size) {
+    if (!(val >= lo && val <= hi) || v_size < 8 || u_size < 8 || !(hi > 0.0f)) return -1;
+    const int vs = (int)v_size, us = (int)u_size;
+    const int radius = (vs + us) / 32;
+    const int extra_margin = radius + 1;
+    const int margin = radius + extra_margin + 1;
+    const int track_len_v = vs - (margin * 2) - 1;
+    const int track_len_u = us - (margin * 2) - 1;
+    const float quad_size_val = hi / 4.0f;
+    const float quadrant = floorf(val / quad_size_val);
+    const float quad_pos_val = val - (quad_size_val * quadrant);
+#define VAL_TO_TRACT(len) ((int)((quad_pos_val / quad_size_val) * (float)(len)))
+    int cv, cu;
+    if (quadrant < 1.0f || quadrant >= 4.0f) {
+        cv = margin;
+        cu = VAL_TO_TRACT(track_len_u) + margin;
+    } else if (quadrant < 2.0f) {
+        cv = VAL_TO_TRACT(track_len_v) + margin;
+        cu = us - margin - 1;
+    } else if (quadrant < 3.0f) {
+        cv = vs - margin - 1;
+        cu = us - (VAL_TO_TRACT(track_len_u) + margin) - 1;
+    } else {
+        cv = vs - (VAL_TO_TRACT(track_len_v) + margin) - 1;
+        cu = margin;
+    }
+#undef VAL_TO_TRACT
+    const uint32_t len = v_size * u_size;
+    memset(frame, 0, len);
+    const uint64_t key = enc_splitmix(seed ^ 0x656E636F64657273ull);
+    for (int v = -radius; v <= radius; v++) {
+        const int u_z = imax(-radius, -v - radius), u_m = imin(radius, -v + radius);
+        for (int u = u_z; u <= u_m; u++) {
+            const int row = v + cv, col = u + cu;
+            if (row < 0 || row >= vs || col < 0 || col >= us) continue;
+            const uint32_t idx = (uint32_t)(row * us + col);
+            frame[idx] = (uint8_t)(64 + (enc_splitmix(key + (uint64_t)frame_idx * len + idx) >> 58));
+        }
+    }
+    return 0;
+}
+
+/* ScalarSdrWriter::new (src/encode/write/scalar_sdr_writer.rs:96-152): the
+ * waypoint count, and (when `ways` is given) the seeded waypoint table of
+ * way_count x (len / 48) indices in [0, len). */
+int bmo_sdr_waypoints(float lo, float hi, float way_span, uint32_t v_size, uint32_t u_size, uint64_t seed,
+                      uint32_t* ways) {
+    if (v_size < 8 || u_size < 8 || !(way_span > 0.0f) || !(lo <= hi)) return -1;
+    const float val_span = hi - lo;
+    const float val_span_norm = val_span / way_span;
+    const int way_count = (int)ceilf(val_span_norm) + 1;
+    const uint64_t len = (uint64_t)v_size * u_size, active = len / 48;
+    if (ways) {
+        const uint64_t key = enc_splitmix(seed ^ 0x7364727761797370ull);
+        for (uint64_t k = 0; k < (uint64_t)way_count * active; k++)
+            ways[k] = (uint32_t)(((unsigned __int128)enc_splitmix(key + k) * len) >> 64);
+    }
+    return way_count;
+}
+
+/* ScalarSdrWriter::encode (scalar_sdr_writer.rs:156-210). */
+int bmo_sdr_encode(float val, float lo, float hi, float way_span, uint32_t way_count, const uint32_t* ways,
+                   uint8_t* frame, uint32_t len) {
+    if (!(val >= lo && val <= hi)) return -1;
+    const uint32_t active = len / 48;
+    memset(frame, 0, len);
+    const float val_norm = (val - lo) / way_span;
+    const float way_0 = floorf(val_norm);
+    const float way_1_contrib_ratio = val_norm - way_0;
+    const uint32_t way_1_contrib_count = (uint32_t)((float)active * way_1_contrib_ratio);
+    const uint32_t way_0_contrib_count = active - way_1_contrib_count;
+    const uint32_t way_0_idx = (uint32_t)way_0, way_1_idx = way_0_idx + 1;
+    if (way_1_idx >= way_count) return -1;
+    for (uint32_t k = 0; k < way_0_contrib_count; k++) frame[ways[(uint64_t)way_0_idx * active + k]] = 128;
+    for (uint32_t k = way_1_contrib_count; k-- > 0;) frame[ways[(uint64_t)way_1_idx * active + k]] = 128;
+    return 0;
 }

@@ -54,6 +54,17 @@ uint32_t bmo_axn_idx_scl(const bm_area_plan* plan, uint8_t slc, uint32_t v, int8
 uint32_t bmo_axn_idx_vec4(const bm_area_plan* plan, uint8_t slc, int32_t v, int8_t v_ofs,
                           int32_t u, int8_t u_ofs, int* safe);
 
+/* Input encoders (src/encode/), restated for checking the device encoders. */
+void bmo_encode_image(const uint8_t* source, uint32_t x_size, uint32_t y_size, float scale_factor,
+                      uint8_t* target, uint32_t v_size, uint32_t u_size);
+int bmo_hex_mold(int radius, uint32_t src_v, uint32_t src_u, uint8_t* frame, uint32_t v_size, uint32_t u_size);
+int bmo_encode_scalar(float val, float lo, float hi, uint64_t seed, uint32_t frame_idx, uint8_t* frame,
+                      uint32_t v_size, uint32_t u_size);
+int bmo_sdr_waypoints(float lo, float hi, float way_span, uint32_t v_size, uint32_t u_size, uint64_t seed,
+                      uint32_t* ways);
+int bmo_sdr_encode(float val, float lo, float hi, float way_span, uint32_t way_count, const uint32_t* ways,
+                   uint8_t* frame, uint32_t len);
+
 #ifdef __cplusplus
 }
 #endif
