@@ -426,7 +426,7 @@ int build_step(bm_batch_s::StepPlan& p) {
             total += (uint64_t)L.cells * L.tufts[t].syns_per_tft;
             sms = A->fused.sms;
         }
-        const uint32_t target = (uint32_t)std::min<uint64_t>(32768, std::max<uint64_t>(4096, total / ((uint64_t)sms * 16)));
+        const uint32_t target = (uint32_t)std::min<uint64_t>(65536, std::max<uint64_t>(4096, total / ((uint64_t)sms * 16)));
         for (auto& [A, t] : p.tufts) {
             FusedTuft& FT = A->fused.t[st.layer][t];
             // An autotuned choice stays; an area another batch also holds

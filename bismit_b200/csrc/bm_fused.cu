@@ -1094,6 +1094,9 @@ uint32_t ring_stages(uint64_t stride, uint64_t halo, uint32_t max_n) {
     return 2;
 }
 
+// Largest default tile, in synapses (an explicit target may ask for more).
+constexpr uint64_t kMaxTileSyns = 65536;
+
 int device_sms() {
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
@@ -1147,23 +1150,39 @@ void plan_tuft(FusedTuft& FT, const bm_area_plan& P, uint32_t i, uint32_t t, int
     const uint32_t cpu = S > 512 ? S / 512 : 1;
     const uint32_t SB = kWarps * cpu * 512;
     const uint64_t n_syn = (uint64_t)L.cells * S;
-    uint64_t target = std::min<uint64_t>(32768, std::max<uint64_t>(4096, n_syn / ((uint64_t)sms * 16)));
+    uint64_t target = std::min<uint64_t>(kMaxTileSyns, std::max<uint64_t>(4096, n_syn / ((uint64_t)sms * 16)));
     if (target_syns) target = target_syns;
-    uint64_t cells = std::max<uint64_t>(1, target / S);
-    uint32_t W, H;
+    const uint64_t cells = std::max<uint64_t>(1, target / S);
+    const uint32_t vs = P.slc_v_scale[lo], us = P.slc_u_scale[lo];
+    // Tiles are whole rows (H of them) when `cells` covers a row, else a row
+    // cut into k equal parts, k the nearest whole number of `cells`-wide
+    // parts (no sliver at the row's end). The tile narrows until its
+    // footprint fits the 16-bit gather offsets.
+    uint32_t W, H, k = 1;
     if (cells >= L.u_size) {
         W = L.u_size;
         H = (uint32_t)std::min<uint64_t>(L.v_size, cells / L.u_size);
     } else {
-        W = (uint32_t)cells;
+        k = (uint32_t)std::max<uint64_t>(1, (L.u_size + cells / 2) / cells);
+        W = (L.u_size + k - 1) / k;
         H = 1;
     }
-    const uint32_t vs = P.slc_v_scale[lo], us = P.slc_u_scale[lo];
-    const uint64_t frows = ((uint64_t)(H - 1) * vs + 15) / 16 + 1 + 2 * (uint64_t)rv;
-    const uint64_t fw = ((uint64_t)(W - 1) * us + 15) / 16 + 1 + 2 * (uint64_t)ru;
-    const uint64_t fsz = frows * fw;
-    const uint64_t halo = (uint64_t)nrec * fsz;
-    if (halo >= 32768) return;   // gather offsets are 16-bit
+    uint64_t frows, fw, fsz, halo;
+    for (;;) {
+        frows = ((uint64_t)(H - 1) * vs + 15) / 16 + 1 + 2 * (uint64_t)rv;
+        fw = ((uint64_t)(W - 1) * us + 15) / 16 + 1 + 2 * (uint64_t)ru;
+        fsz = frows * fw;
+        halo = (uint64_t)nrec * fsz;
+        if (halo < 32768) break;
+        if (H > 1) {
+            H--;
+        } else if (W > 1) {
+            k++;
+            W = (L.u_size + k - 1) / k;
+        } else {
+            return;   // even one cell's footprint is too large for 16-bit offsets
+        }
+    }
     // Windows: up to SB / 16 dendrites (or cells) per stage, widened by 16
     // at both ends.
     const uint32_t win_bytes = SB / 16 + 32;
