@@ -1084,7 +1084,8 @@ namespace {
 
 // Stages of the shared-memory ring: the deepest ring of at most max_n stages
 // with which three CTAs share an SM, else with which two do. Measured on
-// B200: one tuft alone (area_256) runs fastest with two stages, batched steps
+// B200: one tuft alone (area_256, 64K-synapse tiles) runs fastest with three
+// stages (four no longer leave room for three CTAs per SM), batched steps
 // (many tufts of several areas per launch) with up to four.
 uint32_t ring_stages(uint64_t stride, uint64_t halo, uint32_t max_n) {
     for (uint32_t n = max_n; n >= 2; n--)
@@ -1190,7 +1191,7 @@ void plan_tuft(FusedTuft& FT, const bm_area_plan& P, uint32_t i, uint32_t t, int
     // The footprint sits at the start of dynamic shared memory (gathers then
     // address it with a constant base), the ring after it.
     const uint64_t ring_off = ((halo + 127) / 128) * 128;
-    const uint32_t nst = ring_stages(buf_bytes, ring_off, 2);
+    const uint32_t nst = ring_stages(buf_bytes, ring_off, 3);
     // Gathers mask offsets to 15 bits: at least 32 KB of shared memory keeps
     // every masked offset inside the CTA's allocation.
     const uint64_t smem = std::max<uint64_t>(32768, ring_off + 128 + (uint64_t)nst * buf_bytes);
