@@ -325,6 +325,9 @@ def run_hierarchy(args, ctx, stream, K, W, ws):
     def max_ms(ms):
         return max_over_ranks(ms, "cuda")
 
+    t_tune = time.perf_counter()
+    tuned = cx.batch.autotune(None)
+    t_tune = time.perf_counter() - t_tune
     cx.batch.cycle_frames_device(fr.data_ptr(), W)
     torch.cuda.synchronize()
     e0.record(stream)
@@ -354,7 +357,8 @@ def run_hierarchy(args, ctx, stream, K, W, ws):
         "tracts": len(cx.tracts),
         "batched": {"value": n_syn * K * ws / (ms_b / 1e3), "unit": UNIT, "ms_per_step": ms_b / K,
                     "launches_per_cycle": cx.batch.launches_per_cycle(),
-                    "hbm_frac": round(alg / (ms_b / K / 1e3) / 1e9 / peak, 4)},
+                    "hbm_frac": round(alg / (ms_b / K / 1e3) / 1e9 / peak, 4),
+                    "autotuned_steps": tuned, "autotune_s": round(t_tune, 2)},
         "plain": {"value": n_syn * K * ws / (ms_p / 1e3), "unit": UNIT, "ms_per_step": ms_p / K,
                   "launches_per_cycle": sum(a.launches_per_cycle() for a in plain),
                   "hbm_frac": round(alg / (ms_p / K / 1e3) / 1e9 / peak, 4)},

@@ -1025,7 +1025,7 @@ int bm_batch_autotune(bm_batch batch, const char* cache_path, uint32_t* n_tuned)
     cudaStream_t s = B->stream();
     std::map<std::string, uint32_t> cache = read_cache(cache_path);
     uint32_t tuned = 0;
-    static const uint32_t kTargets[] = {4096, 8192, 16384, 32768, 65536};
+    static const uint32_t kTargets[] = {4096, 8192, 16384, 32768, 65536, 131072};
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
