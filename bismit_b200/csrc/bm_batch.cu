@@ -426,13 +426,19 @@ int build_step(bm_batch_s::StepPlan& p) {
             total += (uint64_t)L.cells * L.tufts[t].syns_per_tft;
             sms = A->fused.sms;
         }
-        const uint32_t target = (uint32_t)std::min<uint64_t>(65536, std::max<uint64_t>(4096, total / ((uint64_t)sms * 16)));
+        // A power of two, so that batches rebuilt as areas come and go keep
+        // their tiles (and compiled offsets) until the work doubles or halves.
+        uint64_t want = std::min<uint64_t>(65536, std::max<uint64_t>(4096, total / ((uint64_t)sms * 16)));
+        uint32_t target = 4096;
+        while ((uint64_t)target * 2 <= want) target *= 2;
         for (auto& [A, t] : p.tufts) {
             FusedTuft& FT = A->fused.t[st.layer][t];
             // An autotuned choice stays; an area another batch also holds
             // keeps its tiles (that batch's launches are planned on them).
             if (!FT.tiled || FT.tile_tuned || FT.tile_target == target || A->n_batches > 1) continue;
-            if (retile_fused_tuft(A->fused, A->plan, st.layer, t, target)) A->verify_pending[st.layer] = true;
+            bool changed = false;
+            if (retile_fused_tuft(A->fused, A->plan, st.layer, t, target, &changed) && changed)
+                A->verify_pending[st.layer] = true;
         }
         return build_fused(p);
     }
@@ -835,13 +841,12 @@ bool apply_target(bm_batch_s* B, bm_batch_s::StepPlan& p, uint32_t target) {
     for (auto& [A, t] : p.tufts)
         if (A->n_batches > 1) return false;   // another batch's launches are planned on these tiles
     for (auto& [A, t] : p.tufts) {
-        if (!retile_fused_tuft(A->fused, A->plan, p.st.layer, t, target)) return false;
+        bool changed = false;
+        if (!retile_fused_tuft(A->fused, A->plan, p.st.layer, t, target, &changed)) return false;
         A->fused.t[p.st.layer][t].tile_tuned = true;
+        if (changed) A->verify_pending[p.st.layer] = true;
     }
-    for (bm_area A : p.areas) {
-        A->verify_pending[p.st.layer] = true;
-        run_pending_verifies(A, B->stream());
-    }
+    for (bm_area A : p.areas) run_pending_verifies(A, B->stream());
     return build_fused(p) == BM_OK && p.form == bm_batch_s::F_FUSED;
 }
 

@@ -1246,13 +1246,20 @@ int plan_fused_tuft(FusedArea& F, const bm_area_plan& P, uint32_t layer, uint32_
     return BM_OK;
 }
 
-bool retile_fused_tuft(FusedArea& F, const bm_area_plan& P, uint32_t layer, uint32_t t, uint32_t target_syns) {
+bool retile_fused_tuft(FusedArea& F, const bm_area_plan& P, uint32_t layer, uint32_t t, uint32_t target_syns,
+                       bool* changed) {
+    *changed = false;
     FusedTuft& FT = F.t[layer][t];
     if (!FT.tiled || !FT.gidx) return false;
     FusedTuft next;
     plan_tuft(next, P, layer, t, F.sms, target_syns);
     cudaGetLastError();
     if (!next.tiled) return false;
+    if (next.tile_w == FT.tile_w && next.tile_h == FT.tile_h && next.nst == FT.nst && next.smem == FT.smem) {
+        FT.tile_target = target_syns;   // same tiles: the compiled offsets stay valid
+        return true;
+    }
+    *changed = true;
     next.gidx = FT.gidx;
     next.tile_target = target_syns;
     FT = next;

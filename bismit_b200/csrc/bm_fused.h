@@ -47,9 +47,11 @@ int prepare_fused(FusedArea& F, const bm_area_plan& P, std::string* err);
 int plan_fused(FusedArea& F, const bm_area_plan& P);
 int plan_fused_tuft(FusedArea& F, const bm_area_plan& P, uint32_t layer, uint32_t t);
 // Replans a tiled tuft for about `target_syns` synapses per tile, keeping its
-// gather-offset buffer (the caller recompiles the offsets before the next
-// launch). False, and nothing changed, when the tuft would not stay tiled.
-bool retile_fused_tuft(FusedArea& F, const bm_area_plan& P, uint32_t layer, uint32_t t, uint32_t target_syns);
+// gather-offset buffer. False, and nothing changed, when the tuft would not
+// stay tiled. *changed tells whether the tiles changed, in which case the
+// caller recompiles the offsets before the next launch.
+bool retile_fused_tuft(FusedArea& F, const bm_area_plan& P, uint32_t layer, uint32_t t, uint32_t target_syns,
+                       bool* changed);
 void free_fused(FusedArea& F);
 // Gather geometry of tiled tuft t of data layer `layer` as planned in F.
 GatherGeo gather_geo(const FusedArea& F, const bm_area_plan& P, uint32_t layer, uint32_t t);
