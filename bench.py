@@ -511,23 +511,57 @@ def run_ours(args):
                     "algorithmic_bytes_per_launch": int(alg), "avg_launch_ms": round(avg_ms, 4),
                     "share": round(dom_ms / sum(v[1] for v in prof.values()), 3)}
 
-    # End to end through the public API with host buffers.
+    # End to end through the public API with host buffers: each cycle's frame
+    # goes in with bm_area_write_input from pinned host memory, and each
+    # cycle's output axons come back through a sampler with backpressure
+    # (CorticalArea::sampler, the reference's per-cycle readback), taken by a
+    # receiver thread as a sampler's TractReceiver is. Backpressure makes every
+    # cycle's frame arrive (none skipped); the cycling thread enqueues the next
+    # cycle while the receiver waits for the previous frame.
     import ctypes
+    import threading
     pin_in = torch.from_numpy(host_frames).pin_memory()
     pin_out = torch.empty(out_len, dtype=torch.uint8).pin_memory()
     lib = area.lib
+    # The output's layer_idx indexes the layer map; the sampler takes the
+    # data (cellular) layer that owns those slices.
+    out_layer = area.data_layer(area.layer_names[int(plan.outputs[0].layer_idx)])
+    smp = area.sampler("axons", out_layer, backpressure=True)
+    if smp.len != out_len:
+        raise RuntimeError("output sampler covers %d bytes, the output slice %d" % (smp.len, out_len))
+    smp.set_timeout(60000)
+    got_cycles = []
+    recv_err = []
+
+    def receive():
+        cyc, got = ctypes.c_uint64(), ctypes.c_int()
+        for _ in range(K):
+            rc = lib.bm_sampler_recv(smp.h, 1, ctypes.c_void_p(pin_out.data_ptr()), ctypes.c_uint64(out_len),
+                                     ctypes.byref(cyc), ctypes.byref(got))
+            if rc != 0 or not got.value:
+                recv_err.append(rc)
+                return
+            got_cycles.append(cyc.value)
+
     torch.cuda.synchronize()
     barrier()
+    rx = threading.Thread(target=receive)
     t0 = time.perf_counter()
+    rx.start()
     e0.record(stream)
     for k in range(K):
-        lib.bm_area_write_input(area.h, 0, ctypes.c_void_p(pin_in[W + k].data_ptr()), flen)
-        lib.bm_area_cycle(area.h, 1)
-        lib.bm_area_read_output(area.h, 0, ctypes.c_void_p(pin_out.data_ptr()), out_len)
+        if lib.bm_area_write_input(area.h, 0, ctypes.c_void_p(pin_in[W + k].data_ptr()), ctypes.c_size_t(flen)):
+            raise RuntimeError("bm_area_write_input failed")
+        if lib.bm_area_cycle(area.h, 1):
+            raise RuntimeError("bm_area_cycle failed")
     e1.record(stream)
+    rx.join()
     torch.cuda.synchronize()
     e2e_ms = e0.elapsed_time(e1)
     e2e_wall = time.perf_counter() - t0
+    smp.close()
+    if recv_err or len(got_cycles) != K or got_cycles != list(range(got_cycles[0], got_cycles[0] + K)):
+        raise RuntimeError("output sampler: %d of %d cycles received in order" % (len(got_cycles), K))
     barrier()
     e2e_ms = max_over_ranks(e2e_ms, "cuda")
     e2e_val = n_syn * K * ws / (e2e_ms / 1e3)
