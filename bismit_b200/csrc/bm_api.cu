@@ -610,6 +610,21 @@ int prepare_regrow(bm_area_s* A, const std::vector<TuftGrowSpec>& grow, const st
     return BM_OK;
 }
 
+// The host-frame upload ring (bm_area_s::up*).
+void free_upload(bm_area_s* A) {
+    for (int k = 0; k < 2; k++) {
+        if (A->up_host[k]) cudaFreeHost(A->up_host[k]);
+        if (A->up_dev[k]) cudaFree(A->up_dev[k]);
+        if (A->up_loaded[k]) cudaEventDestroy(A->up_loaded[k]);
+        if (A->up_taken[k]) cudaEventDestroy(A->up_taken[k]);
+        A->up_host[k] = A->up_dev[k] = nullptr;
+        A->up_loaded[k] = A->up_taken[k] = nullptr;
+    }
+    if (A->up) cudaStreamDestroy(A->up);
+    A->up = nullptr;
+    A->up_cap = 0;
+}
+
 void free_area(bm_area_s* A) {
     if (!A) return;
     if (A->ctx) {
@@ -619,6 +634,8 @@ void free_area(bm_area_s* A) {
         if (A->slices) cudaFree(A->slices);
         detach_from_batches(A);
         free_samplers(A);
+        free_upload(A);
+        if (A->down) cudaStreamDestroy(A->down);
         free_fused(A->fused);
         if (A->d_regrow) cudaFree(A->d_regrow);
         if (A->grow_offs) cudaFree(A->grow_offs);
@@ -673,6 +690,48 @@ int write_frame(bm_area_s* A, uint32_t input, const void* src, cudaMemcpyKind ki
     for (const FramePiece& p : pieces)
         CU(cudaMemcpyAsync(p.dst, (const uint8_t*)src + p.off, p.len, kind, s));
     return BM_OK;
+}
+
+// A host frame: the caller's bytes are read during the call only, into a
+// pinned slot; the slot is uploaded on A->up (beside the cycles still
+// running on the area's stream) and then moved into place on the area's
+// stream, ordered before the next cycle as a direct copy would be.
+int write_host_frame(bm_area_s* A, uint32_t input, const uint8_t* frame, size_t len) {
+    cudaError_t e = cudaSuccess;
+    if (!A->up) {
+        size_t cap = 0;
+        for (uint32_t i = 0; i < A->plan.n_inputs; i++) cap = std::max<size_t>(cap, A->plan.inputs[i].len);
+        for (int k = 0; k < 2 && e == cudaSuccess; k++) {
+            e = cudaHostAlloc((void**)&A->up_host[k], cap, cudaHostAllocDefault);
+            if (e == cudaSuccess) e = cudaMalloc(&A->up_dev[k], cap);
+            if (e == cudaSuccess) e = cudaEventCreateWithFlags(&A->up_loaded[k], cudaEventDisableTiming);
+            if (e == cudaSuccess) e = cudaEventCreateWithFlags(&A->up_taken[k], cudaEventDisableTiming);
+        }
+        if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&A->up, cudaStreamNonBlocking);
+        if (e != cudaSuccess) {
+            free_upload(A);
+            return cuda_err(e, "input upload set-up");
+        }
+        A->up_cap = cap;
+        A->up_next = 0;
+    }
+    if (len > A->up_cap) return set_err(BM_ERR_INVALID, "frame of %zu bytes exceeds the upload slot", len);
+    const uint32_t k = A->up_next;
+    A->up_next ^= 1;
+    // The slot's previous upload has finished reading its pinned bytes.
+    e = cudaEventSynchronize(A->up_loaded[k]);
+    if (e != cudaSuccess) return cuda_err(e, "input upload");
+    std::memcpy(A->up_host[k], frame, len);
+    // The area's stream has moved the slot's previous frame into place.
+    e = cudaStreamWaitEvent(A->up, A->up_taken[k], 0);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(A->up_dev[k], A->up_host[k], len, cudaMemcpyHostToDevice, A->up);
+    if (e == cudaSuccess) e = cudaEventRecord(A->up_loaded[k], A->up);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(A->stream(), A->up_loaded[k], 0);
+    if (e != cudaSuccess) return cuda_err(e, "input upload");
+    const int rc = write_frame(A, input, A->up_dev[k], cudaMemcpyDeviceToDevice, A->stream());
+    if (rc != BM_OK) return rc;
+    e = cudaEventRecord(A->up_taken[k], A->stream());
+    return e == cudaSuccess ? BM_OK : cuda_err(e, "input upload");
 }
 
 }  // namespace
@@ -870,7 +929,7 @@ int bm_area_write_input(bm_area area, uint32_t input_idx, const uint8_t* frame, 
     if (len != P.inputs[input_idx].len)
         return set_err(BM_ERR_INVALID, "frame length %zu != input layer axon count %u", len, P.inputs[input_idx].len);
     DevGuard g(area->ctx->device);
-    return write_frame(area, input_idx, frame, cudaMemcpyHostToDevice, area->stream());
+    return write_host_frame(area, input_idx, frame, len);
 }
 
 int bm_area_write_input_device(bm_area area, uint32_t input_idx, const void* dev_frame, size_t len) {

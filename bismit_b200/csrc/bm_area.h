@@ -130,6 +130,19 @@ struct bm_area_s {
     cudaEvent_t ev_fork = nullptr;
     std::vector<cudaEvent_t> side_ev;
     std::vector<bm_sampler_s*> samplers;   // per-cycle readback channels (bm_sampler.cu)
+    // Host frames (bm_area_write_input) are copied into a pinned slot during
+    // the call, uploaded on `up` into a device slot while earlier cycles
+    // run, and moved into place on the area's stream. Two slots, each reused
+    // once the area's stream has taken the frame it held (up_taken).
+    cudaStream_t up = nullptr;
+    uint8_t* up_host[2] = {};
+    uint8_t* up_dev[2] = {};
+    cudaEvent_t up_loaded[2] = {}, up_taken[2] = {};
+    uint32_t up_next = 0;
+    size_t up_cap = 0;
+    // Samplers' device-to-host copies run on `down`, from a device copy of
+    // the sampled range taken on the cycling stream.
+    cudaStream_t down = nullptr;
     // Activity smoothers: group centers per (host layer, control), six
     // lattices in center_off ranges.
     int32_t* d_centers[BM_MAX_LAYERS][BM_MAX_CTRL] = {};

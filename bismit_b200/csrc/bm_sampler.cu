@@ -15,9 +15,11 @@
 // recv(wait_for_frame) takes the unread frame, or waits for the next send, or
 // returns none.
 //
-// Here a send is an asynchronous device-to-host copy into the sampler's
-// pinned frame buffer, enqueued on the cycling stream after the cycle's
-// kernels, with an event the receiver waits on. The channel state is a mutex
+// Here a send is a device copy of the range, enqueued on the cycling stream
+// after the cycle's kernels, then a device-to-host copy of it into the
+// sampler's pinned frame buffer on a stream of its own (so the next cycle
+// does not wait for it), with an event the receiver waits on. The channel
+// state is a mutex
 // and a condition variable shared by the cycling and the receiving thread.
 // A wait may be bounded (bm_sampler_set_timeout); the reference waits forever,
 // which is also the default.
@@ -35,6 +37,8 @@ struct bm_sampler_s {
     bm_area area = nullptr;
     uint64_t off = 0, len = 0;   // sampled range of the area's state slab
     uint8_t* host = nullptr;     // pinned frame buffer
+    uint8_t* dev = nullptr;      // device copy of the range (ranges up to kStageMax)
+    cudaEvent_t staged = nullptr;  // the device copy is taken
     cudaEvent_t done = nullptr;  // the frame's copy has landed
     std::mutex mu;
     std::condition_variable cv;
@@ -46,6 +50,11 @@ struct bm_sampler_s {
 };
 
 namespace {
+
+// Ranges up to this size are first copied on the device, on the cycling
+// stream, and downloaded on the area's `down` stream beside the next cycle;
+// larger ones are downloaded on the cycling stream directly.
+constexpr uint64_t kStageMax = 64ull << 20;
 
 template <class Pred>
 bool wait_for(bm_sampler_s* S, std::unique_lock<std::mutex>& lk, Pred pred) {
@@ -61,6 +70,8 @@ void destroy_sampler(bm_sampler_s* S) {
         cudaEventSynchronize(S->done);
         cudaEventDestroy(S->done);
     }
+    if (S->staged) cudaEventDestroy(S->staged);
+    if (S->dev) cudaFree(S->dev);
     if (S->host) cudaFreeHost(S->host);
     delete S;
 }
@@ -83,8 +94,20 @@ int bm::sample_after_cycle(bm_area_s* A, cudaStream_t s) {
                 continue;
             }
         }
-        cudaError_t e = cudaMemcpyAsync(S->host, A->slab + S->off, S->len, cudaMemcpyDeviceToHost, s);
-        if (e == cudaSuccess) e = cudaEventRecord(S->done, s);
+        cudaError_t e;
+        if (S->dev) {
+            // The previous download has left S->dev (long since: its frame
+            // was taken or this one would be skipped).
+            e = cudaStreamWaitEvent(s, S->done, 0);
+            if (e == cudaSuccess) e = cudaMemcpyAsync(S->dev, A->slab + S->off, S->len, cudaMemcpyDeviceToDevice, s);
+            if (e == cudaSuccess) e = cudaEventRecord(S->staged, s);
+            if (e == cudaSuccess) e = cudaStreamWaitEvent(A->down, S->staged, 0);
+            if (e == cudaSuccess) e = cudaMemcpyAsync(S->host, S->dev, S->len, cudaMemcpyDeviceToHost, A->down);
+            if (e == cudaSuccess) e = cudaEventRecord(S->done, A->down);
+        } else {
+            e = cudaMemcpyAsync(S->host, A->slab + S->off, S->len, cudaMemcpyDeviceToHost, s);
+            if (e == cudaSuccess) e = cudaEventRecord(S->done, s);
+        }
         if (e != cudaSuccess) return cuda_err(e, "sampler copy");
         S->ready = true;
         S->frame_cycle = A->host_cycle - 1;
@@ -147,6 +170,11 @@ int bm_sampler_create(bm_area area, uint32_t kind, uint32_t layer, int backpress
     S->backpressure = backpressure != 0;
     cudaError_t e = cudaHostAlloc((void**)&S->host, len, cudaHostAllocDefault);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&S->done, cudaEventDisableTiming);
+    if (e == cudaSuccess && len <= kStageMax) {
+        e = cudaMalloc(&S->dev, len);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&S->staged, cudaEventDisableTiming);
+        if (e == cudaSuccess && !area->down) e = cudaStreamCreateWithFlags(&area->down, cudaStreamNonBlocking);
+    }
     if (e != cudaSuccess) {
         destroy_sampler(S);
         return cuda_err(e, "sampler set-up");
@@ -203,12 +231,19 @@ int bm_sampler_recv(bm_sampler sampler, int wait_for_frame, void* dst, uint64_t 
         if (!wait_for(S, lk, [&] { return S->ready; }))
             return set_err(BM_ERR_TIMEOUT, "sampler: no frame within %u ms", S->timeout_ms);
     }
+    // The frame stays unread (ready) while the receiver waits for its copy
+    // and takes it, so a sender meanwhile skips or waits as for any unread
+    // frame; the lock is not held across the device wait, so a sender without
+    // backpressure never blocks on it.
+    const uint64_t frame_cycle = S->frame_cycle;
+    lk.unlock();
     DevGuard g(S->area->ctx->device);
     cudaError_t e = cudaEventSynchronize(S->done);
     if (e != cudaSuccess) return cuda_err(e, "sampler frame");
     std::memcpy(dst, S->host, S->len);
-    if (cycle) *cycle = S->frame_cycle;
+    if (cycle) *cycle = frame_cycle;
     *got = 1;
+    lk.lock();
     S->ready = false;
     S->cv.notify_all();
     return BM_OK;

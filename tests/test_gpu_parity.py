@@ -96,6 +96,37 @@ def test_filtered_frames_from_device_match_oracle(ctx):
     area.close()
 
 
+@pytest.mark.parametrize("scheme", ["mixed", "retina"])
+def test_host_frames_read_during_the_call_only(ctx, scheme):
+    """bm_area_write_input reads the caller's bytes during the call only, even
+    from pinned memory, whose copies are otherwise asynchronous: one pinned
+    buffer, written twice before each cycle (the second frame wins) and
+    spoiled right after each call, gives the oracle's state."""
+    import ctypes as C
+    import torch
+    area = _area(ctx, scheme, settings_for())
+    plan = area.plan
+    slab = initial_slab(plan, 7, scramble_seed=11)
+    area.write_slab(slab)
+    area.set_cycle(0)
+    n = 5
+    fr = frames_for(plan, n + 1, 5, 0.05)
+    flen = fr.shape[1]
+    buf = torch.empty(flen, dtype=torch.uint8).pin_memory()
+    lib = area.lib
+    for k in range(n):
+        for f in (fr[n - k], fr[k]):
+            buf.copy_(torch.from_numpy(np.ascontiguousarray(f)))
+            F.check(lib.bm_area_write_input(area.h, 0, C.c_void_p(buf.data_ptr()), C.c_size_t(flen)))
+            buf.fill_(0xA5)
+        area.cycle(1)
+    ora = slab.copy()
+    oracle.run(plan, ora, fr[:n], n, start_cycle=0)
+    got = area.read_slab()
+    assert np.array_equal(got, ora), diff_report(plan, got, ora)
+    area.close()
+
+
 @pytest.mark.parametrize("plain", [True, False], ids=["plain", "fused"])
 @pytest.mark.parametrize("kind", ["bypass_inhib", "no_learning", "no_pyrs", "no_sscs"])
 def test_settings_match_oracle(ctx, kind, plain):
