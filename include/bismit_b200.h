@@ -348,7 +348,10 @@ int bm_plan_resolve(const bm_area_desc* desc, uint64_t seed, bm_area_plan* out);
 
 /* Writes one thalamic frame into the axon range of input layer `input_idx`
  * (index into plan.inputs); len must equal that range (AxonSpace::intake,
- * src/cortex/axon_space.rs:509-588). The copy is ordered before the next cycle. */
+ * src/cortex/axon_space.rs:509-588). The copy is ordered before the next cycle.
+ * The frame's bytes are read during the call only, pinned or pageable: the
+ * caller may reuse its buffer as soon as the call returns. The upload runs
+ * beside the cycles already enqueued. */
 int bm_area_write_input(bm_area area, uint32_t input_idx, const uint8_t* frame, size_t len);
 
 /* Same, from device memory (a frame already resident in HBM). */
