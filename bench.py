@@ -32,7 +32,7 @@ UNIT = "synapse-cycles/s"
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="area_256")
@@ -91,6 +91,68 @@ def algorithmic_bytes(plan, kernel):
     if kernel == "tft_set_syn_flags":
         return 3 * syn / plan.n_layers
     return None
+
+
+class _DevBytes:
+    """A u8 view of n bytes of device memory at ptr, for torch.as_tensor."""
+
+    def __init__(self, ptr, n):
+        self.__cuda_array_interface__ = {"shape": (int(n),), "typestr": "|u1", "data": (int(ptr), False),
+                                         "version": 3, "strides": None, "stream": None}
+
+
+def learn_syns_per_cycle(area, plan, dev_frames, flen, first, n):
+    """Synapses that learning touches per cycle, counted on the device over n
+    cycles (frames first .. first + n - 1 of dev_frames):
+      * spiny stellate cells whose axon is non-zero after inhibition rewrite
+        their tuft's synapses (ssc_mtp_simple, cl/bismit.cl:888-915);
+      * pyramidal cells that became active this cycle (CEL_PREV_ACTIVE clear
+        before it) and whose previous best dendrite of the first distal tuft
+        had a non-zero raw state rewrite that dendrite's synapses
+        (tft_dst_mtp, cl/bismit.cl:1195-1268); CEL_PREV_ACTIVE is set by the
+        first distal tuft, so later ones never learn.
+    Returns the mean count per cycle."""
+    import torch
+    from bismit_b200 import _ffi as F
+    base = area.slab_ptr()
+    jobs = []
+    for i in range(plan.n_layers):
+        L = plan.layers[i]
+        ax = torch.as_tensor(_DevBytes(base + int(plan.axon_off) + int(L.axn_idz), L.cells), device="cuda")
+        if L.kind == F.BM_LYR_SPINY_STELLATE and L.n_tufts:
+            jobs.append(("ssc", ax, int(L.tufts[0].syns_per_tft), None, None))
+        elif L.kind == F.BM_LYR_PYRAMIDAL:
+            dist = [L.tufts[t] for t in range(L.n_tufts) if L.tufts[t].den_kind == F.BM_DEN_DISTAL]
+            if not dist:
+                continue
+            T = dist[0]
+            fl = torch.as_tensor(_DevBytes(base + int(L.buf_off[F.BUF["cel_flag_sets"]]), L.cells), device="cuda")
+            raw = torch.as_tensor(_DevBytes(base + int(L.buf_off[F.BUF["tft_prev_best_den_states_raw"]])
+                                            + int(T.cel_idz), L.cells), device="cuda")
+            jobs.append(("pyr", ax, int(T.syns_per_den), fl, raw))
+    total = torch.zeros((), dtype=torch.int64, device="cuda")
+    for k in range(n):
+        before = [j[3].clone() if j[0] == "pyr" else None for j in jobs]
+        area.cycle_frames_device(dev_frames.data_ptr() + (first + k) * flen, flen, 1)
+        for j, fb in zip(jobs, before):
+            kind, ax, per, _, raw = j
+            if kind == "ssc":
+                total += (ax != 0).sum() * per
+            else:
+                total += ((fb & 0x08) == 0).logical_and(ax != 0).logical_and(raw != 0).sum() * per
+    torch.cuda.synchronize()
+    return int(total.item()) / n
+
+
+def cycle_bytes(plan, flen, n_learn):
+    """Algorithmic bytes of one cycle: 7 per synapse, 4 per dendrite, 12 per
+    pyramidal cell-tuft, 4 per cell, the input frame and 3 per synapse that
+    learning touches."""
+    syn = sum(int(plan.layers[i].n_syns) for i in range(plan.n_layers))
+    den = sum(int(plan.layers[i].n_dens) for i in range(plan.n_layers))
+    ct = sum(int(plan.layers[i].n_celtfts) for i in range(plan.n_layers) if plan.layers[i].kind == 2)
+    cells = sum(int(plan.layers[i].cells) for i in range(plan.n_layers))
+    return 7 * syn + 4 * den + 12 * ct + 4 * cells + int(flen) + 3 * n_learn
 
 
 class Clocks:
@@ -511,6 +573,17 @@ def run_ours(args):
                     "algorithmic_bytes_per_launch": int(alg), "avg_launch_ms": round(avg_ms, 4),
                     "share": round(dom_ms / sum(v[1] for v in prof.values()), 3)}
 
+    # The whole cycle against the same peak: algorithmic bytes per cycle with
+    # the synapses that learning touches counted on the device (untimed
+    # cycles of the same frames), over the timed cycle time.
+    n_count = min(K, 20)
+    n_learn = learn_syns_per_cycle(area, plan, dev_frames, flen, W, n_count)
+    b_cycle = cycle_bytes(plan, flen, n_learn)
+    cyc_gbs = b_cycle / (ms / K / 1e3) / 1e9
+    cycle_roofline = {"bytes_per_cycle": int(b_cycle), "learn_syns_per_cycle": round(n_learn, 1),
+                      "learn_counted_over_cycles": n_count, "achieved": round(cyc_gbs, 1), "peak": peak,
+                      "unit": "GB/s", "frac": round(cyc_gbs / peak, 4), "peak_source": peak_kind}
+
     # End to end through the public API with host buffers: each cycle's frame
     # goes in with bm_area_write_input from pinned host memory, and each
     # cycle's output axons come back through a sampler with backpressure
@@ -596,6 +669,7 @@ def run_ours(args):
                     "wall_s": round(e2e_wall, 4)},
             "gpu_launches": launches,
             "roofline": roofline,
+            "cycle_roofline": cycle_roofline,
             "cpu_baseline": cpu,
             "kernels": {k: {"launches": v[0], "ms": round(v[1], 4)} for k, v in prof.items()},
             "batched_instances": batched,
