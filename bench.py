@@ -101,6 +101,13 @@ class _DevBytes:
                                          "version": 3, "strides": None, "stream": None}
 
 
+def pyr_learners(flags_before, axons, prev_best_raw):
+    """Pyramidal cells whose first distal tuft learns this cycle (numpy or
+    torch arrays, one entry per cell): active now, CEL_PREV_ACTIVE (0x08)
+    clear before the cycle, and a non-zero previous best raw state."""
+    return ((flags_before & 0x08) == 0) & (axons != 0) & (prev_best_raw != 0)
+
+
 def learn_syns_per_cycle(area, plan, dev_frames, flen, first, n):
     """Synapses that learning touches per cycle, counted on the device over n
     cycles (frames first .. first + n - 1 of dev_frames):
@@ -139,7 +146,7 @@ def learn_syns_per_cycle(area, plan, dev_frames, flen, first, n):
             if kind == "ssc":
                 total += (ax != 0).sum() * per
             else:
-                total += ((fb & 0x08) == 0).logical_and(ax != 0).logical_and(raw != 0).sum() * per
+                total += pyr_learners(fb, ax, raw).sum() * per
     torch.cuda.synchronize()
     return int(total.item()) / n
 
@@ -210,6 +217,27 @@ def peaks():
         d = json.load(open(p))
         return float(d["hbm_gbs"]), "measured"
     return 6650.0, "fallback"
+
+
+def live_copy_gbs(n_bytes=2 << 30, reps=5):
+    """A STREAM-style device copy on this GPU (torch's copy of n_bytes, read
+    plus write counted), for context beside the roofline's peak."""
+    import torch
+    src = torch.empty(n_bytes, dtype=torch.uint8, device="cuda")
+    dst = torch.empty_like(src)
+    dst.copy_(src)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    best = 0.0
+    for _ in range(reps):
+        e0.record()
+        dst.copy_(src)
+        e1.record()
+        e1.synchronize()
+        best = max(best, 2 * n_bytes / (e0.elapsed_time(e1) / 1e3) / 1e9)
+    del src, dst
+    torch.cuda.empty_cache()
+    return best
 
 
 def traffic_for(kernel, workload):
@@ -564,6 +592,7 @@ def run_ours(args):
     avg_ms = dom_ms / dom_launches
     alg = algorithmic_bytes(plan, dom_name)
     peak, peak_kind = peaks()
+    copy_live = live_copy_gbs()
     roofline = None
     if alg is not None:
         ach = alg / (avg_ms / 1e3) / 1e9
@@ -571,7 +600,8 @@ def run_ours(args):
         roofline = {"bound": "hbm", "kernel": dom_name, "achieved": round(ach, 1), "peak": peak, "unit": "GB/s",
                     "frac": round(ach / peak, 4), "peak_source": peak_kind, "traffic": tr,
                     "algorithmic_bytes_per_launch": int(alg), "avg_launch_ms": round(avg_ms, 4),
-                    "share": round(dom_ms / sum(v[1] for v in prof.values()), 3)}
+                    "share": round(dom_ms / sum(v[1] for v in prof.values()), 3),
+                    "live_copy_gbs": round(copy_live, 1), "frac_of_live_copy": round(ach / copy_live, 4)}
 
     # The whole cycle against the same peak: algorithmic bytes per cycle with
     # the synapses that learning touches counted on the device (untimed
@@ -582,7 +612,8 @@ def run_ours(args):
     cyc_gbs = b_cycle / (ms / K / 1e3) / 1e9
     cycle_roofline = {"bytes_per_cycle": int(b_cycle), "learn_syns_per_cycle": round(n_learn, 1),
                       "learn_counted_over_cycles": n_count, "achieved": round(cyc_gbs, 1), "peak": peak,
-                      "unit": "GB/s", "frac": round(cyc_gbs / peak, 4), "peak_source": peak_kind}
+                      "unit": "GB/s", "frac": round(cyc_gbs / peak, 4), "peak_source": peak_kind,
+                      "frac_of_live_copy": round(cyc_gbs / copy_live, 4)}
 
     # End to end through the public API with host buffers: each cycle's frame
     # goes in with bm_area_write_input from pinned host memory, and each
