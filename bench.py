@@ -44,6 +44,7 @@ def parse():
     ap.add_argument("--batch-instances", type=int, default=64)
     ap.add_argument("--no-serving", action="store_true", help="skip the serving measurement")
     ap.add_argument("--no-hierarchy", action="store_true", help="skip the three-area hierarchy measurement")
+    ap.add_argument("--no-small", action="store_true", help="skip the 64 x 64 area measurement")
     ap.add_argument("--serve-sessions", type=int, default=64)
     ap.add_argument("--serve-rate", type=float, default=200.0, help="mean session arrivals per second (Poisson)")
     ap.add_argument("--serve-budget-gb", type=float, default=8.0)
@@ -454,9 +455,77 @@ def run_hierarchy(args, ctx, stream, K, W, ws):
                   "hbm_frac": round(alg / (ms_p / K / 1e3) / 1e9 / peak, 4)},
         "batched_over_plain": round(ms_p / ms_b, 3),
     }
+    if ws == 1 and not args.no_cpu_baseline:
+        plans = [cx.area(n).plan for n in names]
+        slabs = [cx.area(n).read_slab() for n in names]
+        tracts, _ext = M.area_tracts(lmaps, areas, names, plans)
+        out["cpu_baseline"] = hierarchy_cpu_baseline(plans, slabs, tracts, args.cpu_sample_seconds / 2, args.seed)
     for a in plain:
         a.close()
     cx.close()
+    return out
+
+
+def hierarchy_cpu_baseline(plans, slabs, tracts, budget_s, seed):
+    """bismit's kernels compiled for the CPU (oracle/_ref, all host threads;
+    the C restatement without it) on cycles of the hierarchy, each area after
+    its tract intakes (previous-cycle outputs) as on the device."""
+    import oracle
+    impl = "ref" if oracle.load_ref() is not None else "port"
+    threads = os.cpu_count() or 1
+    from bismit_b200 import configs
+    ext = configs.frames(8, int(plans[0].inputs[0].len), 0.02, seed + 5)
+    n_syn = sum(int(p.n_syns_total) for p in plans)
+    t0 = time.perf_counter()
+    n = 0
+    while True:
+        outs = [sl[int(p.axon_off):].copy() for p, sl in zip(plans, slabs)]
+        for (si, o, d, i, off, ln) in tracts:
+            src = int(plans[si].outputs[o].axn_idz)
+            oracle.intake(plans[d], slabs[d], i, off, outs[si][src:src + ln])
+        oracle.intake(plans[0], slabs[0], 0, 0, ext[n % len(ext)])
+        for p, sl in zip(plans, slabs):
+            oracle.run(p, sl, None, 1, start_cycle=n, threads=threads, impl=impl)
+        n += 1
+        if time.perf_counter() - t0 >= budget_s or n >= 1000:
+            break
+    dt = time.perf_counter() - t0
+    return {"value": n_syn * n / dt, "unit": UNIT, "cores": threads,
+            "kind": "reference" if impl == "ref" else "port",
+            "sample": "%d cycle(s) of the three areas with their tract intakes (%.1f s)" % (n, dt)}
+
+
+def run_small_area(args, ctx, stream, n_cycles=1000):
+    """area_64 (64 x 64 columns, 2.23 M synapses; its 16 MB per cycle stay in
+    L2, so it is judged on cycles/s): n_cycles cycles over device frames timed
+    with CUDA events, beside bismit's kernels compiled for the CPU on the same
+    area and frames (bounded sample)."""
+    import torch
+    from bismit_b200 import configs, cortex, map as M
+    lmaps, areas, act = configs.workload("area_64")
+    area = cortex.CorticalArea(ctx, M.area_desc("v1", lmaps, areas, configs.bench_settings()), args.seed + 64)
+    plan = area.plan
+    flen = area.input_len()
+    warm = 10
+    fr = configs.frames(n_cycles + warm, flen, act, args.seed + 64)
+    init = area.read_slab()
+    dev = torch.from_numpy(fr).to("cuda")
+    area.cycle_frames_device(dev.data_ptr(), flen, warm)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    area.cycle_frames_device(dev.data_ptr() + warm * flen, flen, n_cycles)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    n_syn = int(plan.n_syns_total)
+    out = {"workload": "area_64", "columns": "64x64", "synapses": n_syn, "cycles": n_cycles,
+           "value": n_syn * n_cycles / (ms / 1e3), "unit": UNIT, "cycles_per_s": round(n_cycles / (ms / 1e3), 1),
+           "ms_per_step": ms / n_cycles, "launches_per_cycle": area.launches_per_cycle()}
+    area.close()
+    if not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_baseline(plan, init, fr[warm:], args.cpu_sample_seconds / 2)
     return out
 
 
@@ -680,6 +749,7 @@ def run_ours(args):
     batched = None if args.no_batched else run_batched(args, ctx, stream, K, W, ws)
     hierarchy = None if args.no_hierarchy else run_hierarchy(args, ctx, stream, K, W, ws)
     serving = None if (args.no_serving or ws > 1) else run_serving(args, ctx)
+    small = None if (args.no_small or ws > 1) else run_small_area(args, ctx, stream)
 
     cpu = None
     if init_slab is not None:
@@ -706,6 +776,7 @@ def run_ours(args):
             "batched_instances": batched,
             "hierarchy": hierarchy,
             "serving": serving,
+            "small_area": small,
         }
         print(json.dumps(line), flush=True)
     ctx.close()
