@@ -523,6 +523,23 @@ def run_small_area(args, ctx, stream, n_cycles=1000):
     out = {"workload": "area_64", "columns": "64x64", "synapses": n_syn, "cycles": n_cycles,
            "value": n_syn * n_cycles / (ms / 1e3), "unit": UNIT, "cycles_per_s": round(n_cycles / (ms / 1e3), 1),
            "ms_per_step": ms / n_cycles, "launches_per_cycle": area.launches_per_cycle()}
+    # The same area as a batch of one, its cycle replayed from a CUDA graph
+    # (same seed and frames, so the two end states must be equal).
+    twin = cortex.CorticalArea(ctx, M.area_desc("v1", lmaps, areas, configs.bench_settings()), args.seed + 64)
+    b = cortex.Batch(ctx, [twin])
+    b.cycle_frames_device(dev.data_ptr(), warm)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    b.cycle_frames_device(dev.data_ptr() + warm * flen, n_cycles)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms_g = e0.elapsed_time(e1)
+    out["graph"] = {"value": n_syn * n_cycles / (ms_g / 1e3), "unit": UNIT,
+                    "cycles_per_s": round(n_cycles / (ms_g / 1e3), 1), "ms_per_step": ms_g / n_cycles,
+                    "launches_per_cycle": b.launches_per_cycle(),
+                    "states_identical": bool(np.array_equal(area.read_slab(), twin.read_slab()))}
+    b.close()
+    twin.close()
     area.close()
     if not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(plan, init, fr[warm:], args.cpu_sample_seconds / 2)
