@@ -39,6 +39,8 @@ def parse():
     ap.add_argument("--path", default="fused", choices=["fused", "plain"])
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--parity-cycles", type=int, default=3,
+                    help="cycles of the headline area compared with bismit's kernels on the host (0: skip)")
     ap.add_argument("--cpu-sample-seconds", type=float, default=12.0)
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-instances measurement")
     ap.add_argument("--batch-instances", type=int, default=64)
@@ -56,7 +58,9 @@ def dist_env():
     return env()
 
 
-def workload_config(name):
+def workload_config(name, n_syn):
+    """The workload of one area, as both arms print it (the same keys and
+    values; with N GPUs each rank runs one such area)."""
     from bismit_b200 import configs
     side, s, d, pd, ps, pr, act = configs.WORKLOADS[name]
     return {
@@ -67,11 +71,16 @@ def workload_config(name):
         "input_active": act,
         "learning": True,
         "regrowth": False,
+        "synapses_per_area": int(n_syn),
     }
 
 
 def algorithmic_bytes(plan, kernel):
-    """Algorithmic bytes of one launch of `kernel` (per-unit figures in DESIGN.md)."""
+    """Algorithmic bytes of one launch of `kernel`, averaged over the area's
+    launches of it. fused_tuft_cycle: 7 bytes per synapse (source slice, v and
+    u offsets, strength and old state read; new state and flags written), 4
+    per dendrite (activity read and written, raw state, state) and 12 per
+    pyramidal cell-tuft (four tuft fields read, eight written)."""
     syn = sum(int(plan.layers[i].n_syns) for i in range(plan.n_layers))
     per_tuft = []
     for i in range(plan.n_layers):
@@ -273,6 +282,33 @@ def cpu_baseline(plan, slab, frames, budget_s, prefer_ref=True):
             "sample": "%d cycle(s) of %s on the host cores (%.1f s)" % (n, "the same area", dt)}
 
 
+def measure_parity(area, plan, frames, n):
+    """Cycles the area n times through the public API with host frames and
+    compares its whole state slab (every axon, synapse, dendrite, tuft and
+    cell byte) with bismit's own kernels compiled for the CPU (oracle/_ref;
+    the C restatement when that was not built) run from the same state on the
+    same frames."""
+    import oracle
+    impl = "ref" if oracle.load_ref() is not None else "port"
+    ref = area.read_slab()
+    c0 = area.cycle_count()
+    for k in range(n):
+        area.write_input(frames[k])
+        area.cycle(1)
+    dev = area.read_slab()
+    t0 = time.perf_counter()
+    oracle.run(plan, ref, frames[:n], n, start_cycle=c0, threads=os.cpu_count() or 1, impl=impl)
+    t_ora = time.perf_counter() - t0
+    diff = int(np.count_nonzero(dev != ref))
+    return {"identical": diff == 0, "differing_bytes": diff, "bytes_compared": int(ref.size), "cycles": n,
+            "from_cycle": int(c0), "learning": True,
+            "against": ("bismit's cl/*.cl compiled for the CPU (oracle/_ref)" if impl == "ref"
+                        else "the C restatement of bismit's kernels (oracle)"),
+            "what": "whole state slab after each run: axons, synapse states, strengths, sources and flags, "
+                    "dendrite, tuft and cell buffers",
+            "oracle_s": round(t_ora, 2)}
+
+
 SOAK_S = 0.6   # seconds of the same cycles on each side of a timed region, for the clock samples
 
 
@@ -310,23 +346,38 @@ def batch_profile(batch, frames, fb, W, K):
     return {"%s L%d.%d" % (n, l, i): [a, round(ms / K, 4)] for (n, l, i, a, _c, ms) in prof}
 
 
+def slabs_equal(arms):
+    """Whether every arm's areas hold the same whole state slabs (arms: lists
+    of areas in the same order), read one area at a time."""
+    for group in zip(*arms):
+        first = group[0].read_slab()
+        if not all(np.array_equal(first, a.read_slab()) for a in group[1:]):
+            return False
+    return True
+
+
 def run_batched(args, ctx, stream, K, W, ws):
     """The batched-instances workload: `--batch-instances` independent areas of
-    uneven size (configs.batch_instances), cycled (a) as one batch with graph
-    replay and (b) in the plain form, one area after another with one kernel
-    per reference stage, on the same seeded frames. Returns the JSON object."""
+    uneven size (configs.batch_instances), cycled on the same seeded frames
+    (a) as one batch with graph replay, (b) one area after another with the
+    same fused kernels (one launch sequence per area, no graph), and (c) in
+    the plain form, one area after another with one kernel per reference
+    stage. (a) against (b) isolates batching and graph replay; (b) against
+    (c) is the fusion. The three arms' whole state slabs are compared after
+    the same cycles. Returns the JSON object."""
     import torch
     from bismit_b200 import configs, cortex, map as M
     n = args.batch_instances
     ins = configs.batch_instances(n, args.seed)
-    areas_b, areas_p, frames_h = [], [], []
+    areas_b, areas_f, areas_p, frames_h = [], [], [], []
     for i, (side, depth, dens, syns, act) in enumerate(ins):
         lmaps, areas = configs.instance_area(side, depth, dens, syns)
-        st = configs.bench_settings()
-        areas_b.append(cortex.CorticalArea(ctx, M.area_desc("v1", lmaps, areas, st), args.seed * 1000 + i))
-        areas_p.append(cortex.CorticalArea(ctx, M.area_desc("v1", lmaps, areas, st.plain_kernels()),
-                                           args.seed * 1000 + i))
-        frames_h.append(configs.frames(K + W, areas_b[-1].input_len(), act, args.seed * 1000 + i))
+        seed = args.seed * 1000 + i
+        areas_b.append(cortex.CorticalArea(ctx, M.area_desc("v1", lmaps, areas, configs.bench_settings()), seed))
+        areas_f.append(cortex.CorticalArea(ctx, M.area_desc("v1", lmaps, areas, configs.bench_settings()), seed))
+        areas_p.append(cortex.CorticalArea(ctx, M.area_desc("v1", lmaps, areas,
+                                                            configs.bench_settings().plain_kernels()), seed))
+        frames_h.append(configs.frames(K + W, areas_b[-1].input_len(), act, seed))
     n_syn = sum(int(a.plan.n_syns_total) for a in areas_b)
     alg = sum(alg_bytes_cycle(a.plan) for a in areas_b)
     batch = cortex.Batch(ctx, areas_b)
@@ -345,68 +396,81 @@ def run_batched(args, ctx, stream, K, W, ws):
     def max_ms(ms):
         return max_over_ranks(ms, "cuda")
 
-    # (a) batched, graph replay
-    batch.cycle_frames_device(packed.data_ptr(), W)
-    torch.cuda.synchronize()
-    e0.record(stream)
-    batch.cycle_frames_device(packed.data_ptr() + W * fb, K)
-    e1.record(stream)
-    torch.cuda.synchronize()
-    ms_b = max_ms(e0.elapsed_time(e1))
-    # (b) plain, one area per launch sequence
-    def plain_cycles(c0, nc):
-        for c in range(c0, c0 + nc):
-            for a, f in zip(areas_p, per_area):
-                a.cycle_frames_device(f.data_ptr() + c * f.shape[1], f.shape[1], 1)
-    plain_cycles(0, W)
-    torch.cuda.synchronize()
-    e0.record(stream)
-    plain_cycles(W, K)
-    e1.record(stream)
-    torch.cuda.synchronize()
-    ms_p = max_ms(e0.elapsed_time(e1))
-    same = all(np.array_equal(a.read_output(), b.read_output()) for a, b in zip(areas_b, areas_p))
+    def timed(fn):
+        fn(0, W)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        fn(W, K)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return max_ms(e0.elapsed_time(e1))
+
+    def batched_cycles(c0, nc):
+        batch.cycle_frames_device(packed.data_ptr() + c0 * fb, nc)
+
+    def one_by_one(arm):
+        def run(c0, nc):
+            for c in range(c0, c0 + nc):
+                for a, f in zip(arm, per_area):
+                    a.cycle_frames_device(f.data_ptr() + c * f.shape[1], f.shape[1], 1)
+        return run
+
+    ms_b = timed(batched_cycles)
+    ms_f = timed(one_by_one(areas_f))
+    ms_p = timed(one_by_one(areas_p))
+    same = slabs_equal([areas_b, areas_f, areas_p])
     steps_b = batch_profile(batch, packed, fb, W, K)
     peak, peak_kind = peaks()
-    val_b = n_syn * K * ws / (ms_b / 1e3)
-    val_p = n_syn * K * ws / (ms_p / 1e3)
+
+    def arm(ms, launches, **kw):
+        d = {"value": n_syn * K * ws / (ms / 1e3), "unit": UNIT, "ms_per_step": ms / K, "launches_per_cycle": launches,
+             "hbm_frac": round(alg / (ms / K / 1e3) / 1e9 / peak, 4)}
+        d.update(kw)
+        return d
+
     out = {
         "workload": "batch_%d" % n, "instances": n, "synapses": n_syn,
         "sizes": "side 32..192 step 16, depth 1..4, distal dens {8,16} x syns {16,32,64}, proximal 1x1, "
                  "spiny stellate 1x32; active 1-4%",
-        "batched": {"value": val_b, "unit": UNIT, "ms_per_step": ms_b / K, "launches_per_cycle": batch.launches_per_cycle(),
-                    "graph": True, "hbm_frac": round(alg / (ms_b / K / 1e3) / 1e9 / peak, 4),
-                    "algorithmic_bytes_per_cycle": alg, "autotuned_steps": tuned, "autotune_s": round(t_tune, 2)},
-        "plain": {"value": val_p, "unit": UNIT, "ms_per_step": ms_p / K,
-                  "launches_per_cycle": sum(a.launches_per_cycle() for a in areas_p),
-                  "hbm_frac": round(alg / (ms_p / K / 1e3) / 1e9 / peak, 4)},
+        "batched": arm(ms_b, batch.launches_per_cycle(), graph=True, algorithmic_bytes_per_cycle=alg,
+                       autotuned_steps=tuned, autotune_s=round(t_tune, 2)),
+        "fused_single": arm(ms_f, sum(a.launches_per_cycle() for a in areas_f), graph=False),
+        "plain": arm(ms_p, sum(a.launches_per_cycle() for a in areas_p), graph=False),
+        "batched_over_fused_single": round(ms_f / ms_b, 3),
         "batched_over_plain": round(ms_p / ms_b, 3),
-        "outputs_identical": bool(same),
+        "slabs_identical": bool(same),
+        "compared": "whole state slab of every instance, three arms, after %d cycles" % (W + K),
         "steps": steps_b,
         "peak_source": peak_kind,
     }
     batch.close()
-    for a in areas_b + areas_p:
+    for a in areas_b + areas_f + areas_p:
         a.close()
     return out
 
 
 def run_hierarchy(args, ctx, stream, K, W, ws):
     """The three-area hierarchy (128 -> 192 -> 96, depth 2, feed-forward and
-    feedback tracts, input 2 % active): (a) one batch with tracts and graph
-    replay, (b) the plain form, one area after another with one kernel per
-    reference stage (the tract copies, about 0.1 MB a cycle, left out)."""
+    feedback tracts, input 2 % active), on the same seeded frames: (a) one
+    batch with its tracts, replayed from a CUDA graph; (b) the same fused
+    kernels one area after another (one launch sequence per area, no graph)
+    and (c) the plain form, one kernel per reference stage, one area after
+    another. (b) and (c) deliver the tracts as the batch does: at the head of
+    each cycle every tract copies its source's output of the previous cycle,
+    then the areas cycle. The three arms' whole state slabs are compared."""
     import torch
     from bismit_b200 import Cortex, configs, cortex, map as M
     lmaps, areas, names = configs.hierarchy()
-    st = configs.bench_settings()
-    cx = Cortex(lmaps, areas, st, seed=args.seed, ctx=ctx)
+    cx = Cortex(lmaps, areas, configs.bench_settings(), seed=args.seed, ctx=ctx)
+    batched = [cx.area(n) for n in names]
+    single = [cortex.CorticalArea(ctx, M.area_desc(n, lmaps, areas, configs.bench_settings()), args.seed)
+              for n in names]
     plain = [cortex.CorticalArea(ctx, M.area_desc(n, lmaps, areas, configs.bench_settings().plain_kernels()),
                                  args.seed) for n in names]
     fb = cx.batch.frame_bytes()
     fr = torch.from_numpy(configs.frames(K + W, fb, 0.02, args.seed + 3)).to("cuda")
-    n_syn = sum(int(cx.area(n).plan.n_syns_total) for n in names)
-    alg = sum(alg_bytes_cycle(cx.area(n).plan) for n in names)
+    n_syn = sum(int(a.plan.n_syns_total) for a in batched)
+    alg = sum(alg_bytes_cycle(a.plan) for a in batched)
     torch.cuda.synchronize()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
@@ -416,51 +480,72 @@ def run_hierarchy(args, ctx, stream, K, W, ws):
     def max_ms(ms):
         return max_over_ranks(ms, "cuda")
 
+    def timed(fn):
+        fn(0, W)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        fn(W, K)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return max_ms(e0.elapsed_time(e1))
+
     t_tune = time.perf_counter()
     tuned = cx.batch.autotune(None)
     t_tune = time.perf_counter() - t_tune
-    cx.batch.cycle_frames_device(fr.data_ptr(), W)
-    torch.cuda.synchronize()
-    e0.record(stream)
-    cx.batch.cycle_frames_device(fr.data_ptr() + W * fb, K)
-    e1.record(stream)
-    torch.cuda.synchronize()
-    ms_b = max_ms(e0.elapsed_time(e1))
-    v1 = plain[0]
 
-    def plain_cycles(c0, nc):
-        for c in range(c0, c0 + nc):
-            v1.cycle_frames_device(fr.data_ptr() + c * fb, fb, 1)
-            for a in plain[1:]:
-                a.cycle(1)
-    plain_cycles(0, W)
-    torch.cuda.synchronize()
-    e0.record(stream)
-    plain_cycles(W, K)
-    e1.record(stream)
-    torch.cuda.synchronize()
-    ms_p = max_ms(e0.elapsed_time(e1))
+    def batched_cycles(c0, nc):
+        cx.batch.cycle_frames_device(fr.data_ptr() + c0 * fb, nc)
+
+    def one_by_one(arm):
+        pairs = []
+        for (sk, so, dk, di, off, n) in cx.tracts:
+            ps, pd = arm[sk].plan, arm[dk].plan
+            src = arm[sk].slab_ptr() + int(ps.axon_off) + int(ps.outputs[so].axn_idz)
+            dst = arm[dk].slab_ptr() + int(pd.axon_off) + int(pd.inputs[di].axn_idz) + int(off)
+            pairs.append((torch.as_tensor(_DevBytes(src, n), device="cuda"),
+                          torch.as_tensor(_DevBytes(dst, n), device="cuda")))
+
+        def run(c0, nc):
+            for c in range(c0, c0 + nc):
+                for src, dst in pairs:
+                    dst.copy_(src)
+                arm[0].cycle_frames_device(fr.data_ptr() + c * fb, fb, 1)
+                for a in arm[1:]:
+                    a.cycle(1)
+        return run
+
+    ms_b = timed(batched_cycles)
+    ms_f = timed(one_by_one(single))
+    ms_p = timed(one_by_one(plain))
+    same = slabs_equal([batched, single, plain])
     peak, _ = peaks()
     steps_h = batch_profile(cx.batch, fr, fb, W, K)
+
+    def arm(ms, launches, **kw):
+        d = {"value": n_syn * K * ws / (ms / 1e3), "unit": UNIT, "ms_per_step": ms / K, "launches_per_cycle": launches,
+             "hbm_frac": round(alg / (ms / K / 1e3) / 1e9 / peak, 4)}
+        d.update(kw)
+        return d
+
     out = {
         "steps": steps_h,
         "workload": "hierarchy_3", "areas": "128x128 -> 192x192 -> 96x96, depth 2", "synapses": n_syn,
         "tracts": len(cx.tracts),
-        "batched": {"value": n_syn * K * ws / (ms_b / 1e3), "unit": UNIT, "ms_per_step": ms_b / K,
-                    "launches_per_cycle": cx.batch.launches_per_cycle(),
-                    "hbm_frac": round(alg / (ms_b / K / 1e3) / 1e9 / peak, 4),
-                    "autotuned_steps": tuned, "autotune_s": round(t_tune, 2)},
-        "plain": {"value": n_syn * K * ws / (ms_p / 1e3), "unit": UNIT, "ms_per_step": ms_p / K,
-                  "launches_per_cycle": sum(a.launches_per_cycle() for a in plain),
-                  "hbm_frac": round(alg / (ms_p / K / 1e3) / 1e9 / peak, 4)},
+        "batched": arm(ms_b, cx.batch.launches_per_cycle(), graph=True, autotuned_steps=tuned,
+                       autotune_s=round(t_tune, 2)),
+        "fused_single": arm(ms_f, sum(a.launches_per_cycle() for a in single) + len(cx.tracts), graph=False),
+        "plain": arm(ms_p, sum(a.launches_per_cycle() for a in plain) + len(cx.tracts), graph=False),
+        "batched_over_fused_single": round(ms_f / ms_b, 3),
         "batched_over_plain": round(ms_p / ms_b, 3),
+        "slabs_identical": bool(same),
+        "compared": "whole state slab of every area, three arms, after %d cycles" % (W + K),
     }
     if ws == 1 and not args.no_cpu_baseline:
-        plans = [cx.area(n).plan for n in names]
-        slabs = [cx.area(n).read_slab() for n in names]
+        plans = [a.plan for a in batched]
+        slabs = [a.read_slab() for a in batched]
         tracts, _ext = M.area_tracts(lmaps, areas, names, plans)
         out["cpu_baseline"] = hierarchy_cpu_baseline(plans, slabs, tracts, args.cpu_sample_seconds / 2, args.seed)
-    for a in plain:
+    for a in single + plain:
         a.close()
     cx.close()
     return out
@@ -642,6 +727,10 @@ def run_ours(args):
 
     init_slab = area.read_slab() if (rank == 0 and ws == 1 and not args.no_cpu_baseline) else None
     out_len = area.output_len()
+    # Bit-exactness at this size, measured: a few cycles through the public
+    # API against bismit's kernels on the host (untimed; the timed cycles
+    # continue from the state they leave).
+    parity = measure_parity(area, plan, host_frames, args.parity_cycles) if (rank == 0 and args.parity_cycles) else None
 
     # warm-up
     area.cycle_frames_device(dev_frames.data_ptr(), flen, W)
@@ -773,22 +862,23 @@ def run_ours(args):
         cpu = cpu_baseline(plan, init_slab, host_frames, args.cpu_sample_seconds)
 
     if rank == 0:
-        cfg = workload_config(args.workload)
-        cfg.update({"path": args.path, "synapses_per_area": n_syn, "areas": ws, "parallelism": "replicas x%d" % ws,
-                    "l2": "state slab %.2f GB per area > 126 MB L2, no flush needed" % (plan.slab_bytes / 1e9),
-                    "clocks_window": "nvidia-smi every 200 ms over the timed region plus %.1f s of the same "
-                                     "cycles on each side" % SOAK_S})
+        cfg = workload_config(args.workload, n_syn)
+        setup = {"path": args.path, "areas": ws, "parallelism": "replicas x%d" % ws,
+                 "l2": "state slab %.2f GB per area > 126 MB L2, no flush needed" % (plan.slab_bytes / 1e9),
+                 "clocks_window": "nvidia-smi every 200 ms over the timed region plus %.1f s of the same "
+                                  "cycles on each side" % SOAK_S}
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": K, "warmup": W,
             "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "u8/i8", "data": "synthetic (seeded frames, seeded synapse growth)", "config": cfg,
-            "clocks": clk,
+            "setup": setup, "clocks": clk,
             "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": flen, "d2h_bytes_per_step": out_len,
                     "wall_s": round(e2e_wall, 4)},
             "gpu_launches": launches,
             "roofline": roofline,
             "cycle_roofline": cycle_roofline,
             "cpu_baseline": cpu,
+            "parity": parity,
             "kernels": {k: {"launches": v[0], "ms": round(v[1], 4)} for k, v in prof.items()},
             "batched_instances": batched,
             "hierarchy": hierarchy,
@@ -808,14 +898,17 @@ def run_reference(args):
     if rank != 0:
         return
     import oracle
-    from bismit_b200 import configs, map as M, plan_of
+    from oracle import plan as OP
+    from bismit_b200 import configs, map as M
     if oracle.load_ref() is None:
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref (bismit's cl/*.cl compiled for the CPU) "
                                                              "was not built: no bismit checkout at build time"}))
         return
     lmaps, areas, act = configs.workload(args.workload)
     desc = M.area_desc("v1", lmaps, areas, configs.bench_settings())
-    plan = plan_of(desc, args.seed + 1)
+    # The oracle's own restatement of bismit's map code: this arm loads none
+    # of the library's native code.
+    plan = OP.resolve(desc, args.seed + 1)
     slab = np.zeros(int(plan.slab_bytes), np.uint8)
     oracle.grow(plan, slab, args.seed + 1, desc.init_flags)
     flen = int(plan.inputs[0].len)
@@ -828,12 +921,11 @@ def run_reference(args):
         oracle.run(plan, slab, fr[args.warmup + k][None, :], 1, start_cycle=args.warmup + k, threads=threads, impl="ref")
     dt = time.perf_counter() - t0
     value = int(plan.n_syns_total) * args.steps / dt
-    cfg = workload_config(args.workload)
-    cfg.update({"synapses_per_area": int(plan.n_syns_total), "areas": 1})
+    cfg = workload_config(args.workload, plan.n_syns_total)
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": dt * 1e3 / args.steps, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "u8/i8", "data": "synthetic", "config": cfg,
+        "vs_baseline": None, "dtype": "u8/i8", "data": "synthetic (seeded frames, seeded synapse growth)", "config": cfg,
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
                          "sample": "%d full cycles of the area" % args.steps},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},

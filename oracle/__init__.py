@@ -17,17 +17,19 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 PORT_PATH = os.path.join(HERE, "libbm_oracle.so")
 REF_PATH = os.path.join(HERE, "_ref", "libbm_ref.so")
-REFERENCE_CHECKOUT = os.environ.get("BISMIT_REFERENCE", "/root/reference")
+REFERENCE_CHECKOUT = os.environ.get("BISMIT_REFERENCE", "")
 
 _port = None
 _ref = None
 
 
-def build(ref=True):
-    """Builds the port (and the reference kernels when a bismit checkout exists)."""
+def build(ref=True, checkout=None):
+    """Builds the port, and the reference kernels when a bismit checkout is
+    given (`checkout`, else $BISMIT_REFERENCE) and holds cl/."""
     subprocess.run(["make", "-s", "-C", HERE], check=True)
-    if ref and os.path.isdir(os.path.join(REFERENCE_CHECKOUT, "cl")):
-        subprocess.run(["make", "-s", "-C", HERE, "ref", "BISMIT=%s" % REFERENCE_CHECKOUT], check=True)
+    checkout = checkout or REFERENCE_CHECKOUT
+    if ref and checkout and os.path.isdir(os.path.join(checkout, "cl")):
+        subprocess.run(["make", "-s", "-C", HERE, "ref", "BISMIT=%s" % checkout], check=True)
 
 
 def _plan_ptr(plan):

@@ -199,3 +199,58 @@ def test_filter_chain_plans_and_refusals():
     areas.by_name("v1").filter_chain(M.InputTrack.Efferent, [M.THAL_SP], ["retina"])
     with pytest.raises(ValueError, match="Unable to find a layer"):
         M.area_desc("v1", lmaps, areas, configs.bench_settings())
+
+
+def _plan_cases():
+    """Every area scheme the tests and benchmarks use, as (label, desc)."""
+    from helpers import SCHEMES
+    out = []
+    for name in sorted(SCHEMES):
+        lm, ar = SCHEMES[name]()
+        for kind in ("default", "regrowth"):
+            out.append(("%s/%s" % (name, kind), M.area_desc("v1", lm, ar, settings_for(kind))))
+    for w in ("area_64", "area_256"):
+        lm, ar, _ = configs.workload(w)
+        out.append((w, M.area_desc("v1", lm, ar, configs.bench_settings())))
+    for i, (side, depth, dens, syns, _a) in enumerate(configs.batch_instances(64, 0)[:12]):
+        lm, ar = configs.instance_area(side, depth, dens, syns)
+        out.append(("instance%d" % i, M.area_desc("v1", lm, ar, configs.bench_settings())))
+    lm, ar, names = configs.hierarchy()
+    for n in names:
+        out.append(("hierarchy/" + n, M.area_desc(n, lm, ar, configs.bench_settings())))
+    return out
+
+
+def test_oracle_plan_resolver_agrees_with_the_library():
+    """The oracle's own restatement of bismit's slice map and index spaces
+    (oracle/plan.py) and the library's bm_plan_resolve give the same plan,
+    byte for byte, for every scheme in use; so the oracle and the CPU
+    reference arm stand on a plan the library did not make."""
+    from bismit_b200 import plan_of
+    from oracle import plan as OP
+    for label, d in _plan_cases():
+        mine = OP.resolve(d, 7)
+        lib = plan_of(d, 7)
+        a, b = bytes(mine), bytes(lib)
+        assert a == b, "%s: plans differ at byte %d" % (label, next(i for i in range(len(a)) if a[i] != b[i]))
+
+
+def test_oracle_plan_resolver_refuses_what_the_library_refuses():
+    from bismit_b200 import plan_of
+    from oracle import plan as OP
+    lm, ar, _ = configs.workload("area_64")
+    bad = []
+    d = M.area_desc("v1", lm, ar, configs.bench_settings())
+    d.layers[3].tufts[0].dens_per_tft = 0
+    bad.append(d)
+    d = M.area_desc("v1", lm, ar, configs.bench_settings())
+    d.layers[3].tufts[1].syns_per_den = 4096   # more than the pool's offsets
+    bad.append(d)
+    d = M.area_desc("v1", lm, ar, configs.bench_settings())
+    d.layers[3].tufts[1].src[0].prevalence = 0
+    bad.append(d)
+    for d in bad:
+        with pytest.raises(OP.PlanError):
+            OP.resolve(d, 0)
+        with pytest.raises(F.BismitError):
+            plan_of(d, 0)
