@@ -813,6 +813,8 @@ def run_ours(args):
     smp.set_timeout(60000)
     got_cycles = []
     recv_err = []
+    t_recv = []     # host time each frame was taken
+    t_call = []     # host time of each cycle's write_input + cycle calls
 
     def receive():
         cyc, got = ctypes.c_uint64(), ctypes.c_int()
@@ -822,14 +824,17 @@ def run_ours(args):
             if rc != 0 or not got.value:
                 recv_err.append(rc)
                 return
+            t_recv.append(time.perf_counter())
             got_cycles.append(cyc.value)
 
     def host_cycles(k0, n):
         for k in range(k0, k0 + n):
+            ta = time.perf_counter()
             if lib.bm_area_write_input(area.h, 0, ctypes.c_void_p(pin_in[k].data_ptr()), ctypes.c_size_t(flen)):
                 raise RuntimeError("bm_area_write_input failed")
             if lib.bm_area_cycle(area.h, 1):
                 raise RuntimeError("bm_area_cycle failed")
+            t_call.append(time.perf_counter() - ta)
 
     rx = threading.Thread(target=receive)
     rx.start()
@@ -850,6 +855,13 @@ def run_ours(args):
     barrier()
     e2e_ms = max_over_ranks(e2e_ms, "cuda")
     e2e_val = n_syn * K * ws / (e2e_ms / 1e3)
+    # Host-side view of the timed cycles: each cycle's calls, the gaps between
+    # frames reaching the receiver, and the wall time to the last frame.
+    calls = np.array(t_call[W:]) * 1e3
+    gaps = np.diff(np.array(t_recv[W - 1:])) * 1e3 if W > 0 else np.diff(np.array(t_recv)) * 1e3
+    e2e_host = {"call_ms_median": round(float(np.median(calls)), 4), "call_ms_max": round(float(calls.max()), 4),
+                "frame_gap_ms_median": round(float(np.median(gaps)), 4), "frame_gap_ms_max": round(float(gaps.max()), 4),
+                "wall_ms_to_last_frame": round((t_recv[-1] - t0) * 1e3, 3), "device_ms": round(e2e_ms, 3)}
 
     area.close()
     batched = None if args.no_batched else run_batched(args, ctx, stream, K, W, ws)
@@ -873,7 +885,7 @@ def run_ours(args):
             "dtype": "u8/i8", "data": "synthetic (seeded frames, seeded synapse growth)", "config": cfg,
             "setup": setup, "clocks": clk,
             "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": flen, "d2h_bytes_per_step": out_len,
-                    "wall_s": round(e2e_wall, 4)},
+                    "wall_s": round(e2e_wall, 4), "host": e2e_host},
             "gpu_launches": launches,
             "roofline": roofline,
             "cycle_roofline": cycle_roofline,

@@ -178,7 +178,14 @@ class bm_server_stats(C.Structure):
                 ("admit_s", C.c_double), ("gpu_s", C.c_double), ("span_s", C.c_double),
                 ("p50_ms", C.c_double), ("p99_ms", C.c_double), ("mean_ms", C.c_double),
                 ("used_bytes", C.c_uint64), ("budget_bytes", C.c_uint64),
-                ("resident", C.c_uint32), ("waiting", C.c_uint32)]
+                ("resident", C.c_uint32), ("waiting", C.c_uint32), ("failed", C.c_uint32)]
+
+
+class bm_tuft_form(C.Structure):
+    _fields_ = [("fused", C.c_uint32), ("tiled", C.c_uint32), ("consumer", C.c_uint32),
+                ("sources_outside", C.c_uint32), ("flags_foreign", C.c_uint32), ("tile_w", C.c_uint32),
+                ("tile_h", C.c_uint32), ("stages", C.c_uint32), ("grid", C.c_uint32), ("smem", C.c_uint32),
+                ("footprint_tma", C.c_uint32)]
 
 
 def lib():
@@ -233,6 +240,11 @@ def lib():
         "bm_area_slab_ptr": (C.c_int, [vp, P(vp)]),
         "bm_area_sources_changed": (C.c_int, [vp, u32]),
         "bm_area_device_errors": (C.c_int, [vp, P(u32)]),
+        "bm_area_tuft_form": (C.c_int, [vp, u32, u32, P(bm_tuft_form)]),
+        "bm_area_clear_errors": (C.c_int, [vp]),
+        "bm_area_deliver_tract": (C.c_int, [vp, u32, vp, u32, u64]),
+        "bm_area_set_wait_limit": (C.c_int, [vp, u32]),
+        "bm_area_inject_stall": (C.c_int, [vp, u32]),
         "bm_area_set_profiling": (C.c_int, [vp, C.c_int]),
         "bm_area_get_profile": (C.c_int, [vp, u32, P(C.c_char_p), P(u64), P(C.c_double), P(u32)]),
         "bm_area_reset_profile": (C.c_int, [vp]),
@@ -256,6 +268,7 @@ def lib():
         "bm_server_open": (C.c_int, [vp, P(bm_area_desc), u64, P(u32)]),
         "bm_server_submit": (C.c_int, [vp, u32, vp, sz, u32]),
         "bm_server_close": (C.c_int, [vp, u32]),
+        "bm_server_cancel": (C.c_int, [vp, u32]),
         "bm_server_tick": (C.c_int, [vp, P(u32)]),
         "bm_server_drain": (C.c_int, [vp]),
         "bm_server_read_output": (C.c_int, [vp, u32, vp, sz, P(u64)]),

@@ -178,6 +178,7 @@ WORKLOADS = {
     "area_128": (128, 32, 2, 1, 1, 0, 0.02),
     "area_32": (32, 32, 1, 1, 1, 0, 0.02),
     "area_48_deep": (48, 32, 2, 4, 16, 3, 0.03),
+    "area_256_shape": (48, 64, 4, 16, 32, 6, 0.03),
 }
 
 

@@ -157,6 +157,34 @@ class CorticalArea:
     def set_cycle(self, c):
         F.check(self.lib.bm_area_set_cycle(self.h, C.c_uint64(c)))
 
+    def device_errors(self):
+        """The area's sticky device error bits (bit 0: a bounded wait gave up)."""
+        v = C.c_uint32()
+        rc = self.lib.bm_area_device_errors(self.h, C.byref(v))
+        if rc not in (F.BM_OK, F.BM_ERR_TIMEOUT):
+            F.check(rc)
+        return v.value
+
+    def clear_errors(self):
+        F.check(self.lib.bm_area_clear_errors(self.h))
+
+    def set_wait_limit(self, us):
+        """Limit of each bounded wait in the tuft kernels, microseconds (0: default)."""
+        F.check(self.lib.bm_area_set_wait_limit(self.h, int(us)))
+
+    def inject_stall(self, stage):
+        """Fault injection: in each tiled tuft launch, the block that takes
+        the tuft's first tile withholds the `stage`-th stage it issues from
+        that tile on (from 1; 0: off)."""
+        F.check(self.lib.bm_area_inject_stall(self.h, int(stage)))
+
+    def tuft_form(self, layer, tuft):
+        """How the fused path runs a tuft (bm_area_tuft_form): a dict of the
+        bm_tuft_form fields."""
+        f = F.bm_tuft_form()
+        F.check(self.lib.bm_area_tuft_form(self.h, self.data_layer(layer), int(tuft), C.byref(f)))
+        return {n: int(getattr(f, n)) for n, _ in F.bm_tuft_form._fields_}
+
     def slab_ptr(self):
         p = C.c_void_p()
         F.check(self.lib.bm_area_slab_ptr(self.h, C.byref(p)))
@@ -413,6 +441,10 @@ class Server:
             a = a[None, :]
         F.check(self.lib.bm_server_submit(self.h, sid, a.ctypes.data_as(C.c_void_p), a.shape[1], a.shape[0]))
 
+    def cancel_session(self, sid):
+        """Closes a session and discards its queued frames."""
+        F.check(self.lib.bm_server_cancel(self.h, sid))
+
     def close_session(self, sid):
         F.check(self.lib.bm_server_close(self.h, sid))
 
@@ -462,17 +494,35 @@ class Server:
             pass
 
 
+PREVIOUS_CYCLE = "previous_cycle"
+SAME_CYCLE = "same_cycle"
+
+
 class Cortex:
-    """A set of cortical areas (Cortex, src/cortex/cortex.rs:37-120). The areas
-    are cycled together as one batch; outputs of one area that feed inputs of
-    another (the thalamic routing of the area schemes) travel as tracts,
-    copied at the head of every cycle from the previous cycle's outputs.
+    """A set of cortical areas (Cortex, src/cortex/cortex.rs:37-120). Outputs
+    of one area that feed inputs of another (the thalamic routing of the area
+    schemes) travel as tracts. Two timings:
+
+    * PREVIOUS_CYCLE (the default): the areas are cycled together as one
+      batch, one launch per stage step for all of them, and every tract
+      carries its source's output of the previous cycle, copied at the head
+      of each cycle.
+    * SAME_CYCLE: bismit's own order. Cortex::cycle cycles the areas one after
+      another in scheme order (src/cortex/cortex.rs:99-119), each starting
+      with its intake (src/cortex/cortical_area.rs:716-719), so a tract from
+      an earlier area carries that area's output of the same cycle and one
+      from a later area its output of the previous cycle. Each area then runs
+      its own launch sequence (slower than the batch).
+
     Inputs fed from outside (subcortical areas) are written per area with
     `area(name).write_input(..)`; `external_inputs()` lists them."""
 
-    def __init__(self, lmaps, areas, settings=None, seed=0, device=0, ctx=None):
+    def __init__(self, lmaps, areas, settings=None, seed=0, device=0, ctx=None, tract_timing=PREVIOUS_CYCLE):
+        if tract_timing not in (PREVIOUS_CYCLE, SAME_CYCLE):
+            raise ValueError("tract_timing must be %r or %r" % (PREVIOUS_CYCLE, SAME_CYCLE))
         self._own_ctx = ctx is None
         self.ctx = _Ctx(device) if ctx is None else ctx
+        self.tract_timing = tract_timing
         self.areas = {}
         self._order = []
         for a in areas.areas:
@@ -483,9 +533,11 @@ class Cortex:
             self._order.append(a.name)
         plans = [self.areas[n].plan for n in self._order]
         self.tracts, self.external = area_tracts(lmaps, areas, self._order, plans)
-        self.batch = Batch(self.ctx, [self.areas[n] for n in self._order]) if self._order else None
-        for (sk, so, dk, di, off, _n) in self.tracts:
-            F.check(self.batch.lib.bm_batch_connect(self.batch.h, sk, so, dk, di, C.c_uint64(off)))
+        self.batch = None
+        if self._order and tract_timing == PREVIOUS_CYCLE:
+            self.batch = Batch(self.ctx, [self.areas[n] for n in self._order])
+            for (sk, so, dk, di, off, _n) in self.tracts:
+                F.check(self.batch.lib.bm_batch_connect(self.batch.h, sk, so, dk, di, C.c_uint64(off)))
 
     @staticmethod
     def builder(lmaps, areas):
@@ -495,6 +547,14 @@ class Cortex:
         """Cortex::cycle: every area once (src/cortex/cortex.rs:99-119)."""
         if self.batch is not None:
             self.batch.cycle(n)
+            return
+        areas = [self.areas[name] for name in self._order]
+        for _ in range(n):
+            for k, a in enumerate(areas):
+                for (sk, so, dk, di, off, _n) in self.tracts:
+                    if dk == k:
+                        F.check(a.lib.bm_area_deliver_tract(areas[sk].h, so, a.h, di, C.c_uint64(off)))
+                a.cycle(1)
 
     def area(self, name):
         return self.areas[name]
@@ -529,6 +589,12 @@ class CortexBuilder:
         self._settings = None
         self._seed = 0
         self._device = 0
+        self._timing = PREVIOUS_CYCLE
+
+    def tract_timing(self, timing):
+        """PREVIOUS_CYCLE (batched) or SAME_CYCLE (bismit's area order)."""
+        self._timing = timing
+        return self
 
     def ca_settings(self, s):
         self._settings = s
@@ -543,4 +609,4 @@ class CortexBuilder:
         return self
 
     def build(self):
-        return Cortex(self.lmaps, self.areas_, self._settings, self._seed, self._device)
+        return Cortex(self.lmaps, self.areas_, self._settings, self._seed, self._device, tract_timing=self._timing)

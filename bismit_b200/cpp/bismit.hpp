@@ -577,15 +577,23 @@ class CorticalArea {
 
 class CortexBuilder;
 
-// Cortex (src/cortex/cortex.rs:37-120): its cortical areas cycled together as
-// one batch, with the thalamic routes between them as tracts (each carrying
-// its source's output of the previous cycle).
+// When a tract delivers its source's output.
+enum class TractTiming {
+    PreviousCycle,   // every tract at the head of each cycle, from the previous cycle: the areas
+                     // cycle together as one batch
+    SameCycle,       // bismit's order (src/cortex/cortex.rs:99-119): area after area, each taking
+                     // its tracts first, so a tract from an earlier area carries this cycle's output
+};
+
+// Cortex (src/cortex/cortex.rs:37-120): its cortical areas, with the thalamic
+// routes between them as tracts, cycled as `timing` says.
 class Cortex {
    public:
     static CortexBuilder builder(const LayerMapSchemeList& lmaps, const AreaSchemeList& areas);
 
     Cortex(const LayerMapSchemeList& lmaps, const AreaSchemeList& areas, const CorticalAreaSettings& settings,
-           uint64_t seed, int device) {
+           uint64_t seed, int device, TractTiming timing = TractTiming::PreviousCycle)
+        : timing_(timing) {
         check(bm_ctx_create(device, 0, &ctx_));
         try {
             for (const auto& a : areas.areas) {
@@ -593,7 +601,7 @@ class Cortex {
                 areas_.emplace_back(new CorticalArea(ctx_, area_desc(a.name, lmaps, areas, settings), seed, a.name));
             }
             route(lmaps, areas);
-            if (!areas_.empty()) {
+            if (!areas_.empty() && timing_ == TractTiming::PreviousCycle) {
                 std::vector<bm_area> hs;
                 for (auto& p : areas_) hs.push_back(p->handle());
                 check(bm_batch_create(ctx_, hs.data(), (uint32_t)hs.size(), &batch_));
@@ -611,8 +619,20 @@ class Cortex {
 
     // Cortex::cycle (src/cortex/cortex.rs:99-119).
     void cycle(uint32_t n = 1) {
-        if (batch_) check(bm_batch_cycle(batch_, n));
+        if (batch_) {
+            check(bm_batch_cycle(batch_, n));
+            return;
+        }
+        for (uint32_t c = 0; c < n; c++)
+            for (uint32_t k = 0; k < areas_.size(); k++) {
+                for (const auto& t : tracts_)
+                    if (t.dst_area == k)
+                        check(bm_area_deliver_tract(areas_[t.src_area]->handle(), t.src_output, areas_[k]->handle(),
+                                                    t.dst_input, t.dst_offset));
+                areas_[k]->cycle(1);
+            }
     }
+    TractTiming tract_timing() const { return timing_; }
     CorticalArea& area(const std::string& name) {
         for (auto& p : areas_)
             if (p->name() == name) return *p;
@@ -662,6 +682,7 @@ class Cortex {
         ctx_ = nullptr;
     }
 
+    TractTiming timing_;
     bm_ctx ctx_ = nullptr;
     bm_batch batch_ = nullptr;
     std::vector<std::unique_ptr<CorticalArea>> areas_;
@@ -685,8 +706,12 @@ class CortexBuilder {
         device_ = d;
         return *this;
     }
+    CortexBuilder& tract_timing(TractTiming t) {
+        timing_ = t;
+        return *this;
+    }
     std::unique_ptr<Cortex> build() const {
-        return std::make_unique<Cortex>(lmaps_, areas_, settings_, seed_, device_);
+        return std::make_unique<Cortex>(lmaps_, areas_, settings_, seed_, device_, timing_);
     }
 
    private:
@@ -695,6 +720,7 @@ class CortexBuilder {
     CorticalAreaSettings settings_ = CorticalAreaSettings().disable_regrowth();
     uint64_t seed_ = 0;
     int device_ = 0;
+    TractTiming timing_ = TractTiming::PreviousCycle;
 };
 
 inline CortexBuilder Cortex::builder(const LayerMapSchemeList& lmaps, const AreaSchemeList& areas) {

@@ -631,6 +631,7 @@ void free_area(bm_area_s* A) {
         DevGuard g(A->ctx->device);
         if (A->slab) cudaFree(A->slab);
         if (A->ctl) cudaFree(A->ctl);
+        if (A->host_err) cudaFreeHost(A->host_err);
         if (A->slices) cudaFree(A->slices);
         detach_from_batches(A);
         free_samplers(A);
@@ -818,10 +819,16 @@ int bm_area_create(bm_ctx ctx, const bm_area_desc* desc, uint64_t seed, bm_area*
     }
     e = cudaMalloc(&A->ctl, sizeof(AreaCtl));
     if (e == cudaSuccess) e = cudaMalloc(&A->slices, sizeof(SliceRec) * BM_MAX_SLICES);
+    if (e == cudaSuccess) e = cudaHostAlloc(&A->host_err, sizeof(unsigned int), cudaHostAllocMapped);
     if (e != cudaSuccess) { free_area(A); return cuda_err(e, "cudaMalloc"); }
+    *A->host_err = 0;
     std::vector<SliceRec> tab(BM_MAX_SLICES);
     fill_slice_table(A->plan, tab.data());
     AreaCtl ctl0{};
+    unsigned int* dev_err = nullptr;
+    e = cudaHostGetDevicePointer((void**)&dev_err, A->host_err, 0);
+    if (e != cudaSuccess) { free_area(A); return cuda_err(e, "cudaHostGetDevicePointer"); }
+    ctl0.host_err = dev_err;
     e = cudaMemsetAsync(A->slab, 0, A->plan.slab_bytes, s);
     if (e == cudaSuccess) e = cudaMemcpyAsync(A->slices, tab.data(), sizeof(SliceRec) * BM_MAX_SLICES, cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess) e = cudaMemcpyAsync(A->ctl, &ctl0, sizeof ctl0, cudaMemcpyHostToDevice, s);
@@ -872,6 +879,7 @@ int bm_area_create(bm_ctx ctx, const bm_area_desc* desc, uint64_t seed, bm_area*
     else if (d_off) cudaFree(d_off);
     if (e != cudaSuccess) { free_area(A); return cuda_err(e, "synapse growth"); }
     rc = prepare_fused(A->fused, A->plan, &err);
+    if (rc == BM_OK) rc = bind_fused(A->fused, A->plan, A->axns());
     if (rc != BM_OK) { free_area(A); return set_err(rc, "%s", err.c_str()); }
     if (regrow) {
         rc = prepare_regrow(A, grow, gts);
@@ -941,8 +949,22 @@ int bm_area_write_input_device(bm_area area, uint32_t input_idx, const void* dev
     return write_frame(area, input_idx, dev_frame, cudaMemcpyDeviceToDevice, area->stream());
 }
 
+namespace {
+// A cycle that completed with device error bits stops further cycles of the
+// area until bm_area_clear_errors (its state is no longer a cycle's result).
+int refuse_after_errors(const bm_area_s* A) {
+    const unsigned int e = A->seen_errors();
+    if (!e) return BM_OK;
+    return set_err(BM_ERR_TIMEOUT,
+                   "an earlier cycle of this area ended with device error bits 0x%x (bit 0: a bounded wait gave "
+                   "up); bm_area_clear_errors re-enables cycling",
+                   e);
+}
+}  // namespace
+
 int bm_area_cycle(bm_area area, uint32_t n_cycles) {
     if (!area) return set_err(BM_ERR_INVALID, "null area");
+    if (int rc = refuse_after_errors(area)) return rc;
     DevGuard g(area->ctx->device);
     for (uint32_t k = 0; k < n_cycles; k++) {
         const int rc = enqueue_cycle(area);
@@ -957,6 +979,7 @@ int bm_area_cycle_frames_device(bm_area area, const void* dev_frames, size_t fra
     const bm_area_plan& P = area->plan;
     if (P.n_inputs == 0) return set_err(BM_ERR_INVALID, "area has no input layer");
     if (frame_len != P.inputs[0].len) return set_err(BM_ERR_INVALID, "frame length %zu != %u", frame_len, P.inputs[0].len);
+    if (int rc = refuse_after_errors(area)) return rc;
     DevGuard g(area->ctx->device);
     for (uint32_t k = 0; k < n_cycles; k++) {
         int rc = BM_OK;
@@ -1049,6 +1072,90 @@ int bm_area_device_errors(bm_area area, uint32_t* bits) {
     CU(cudaStreamSynchronize(area->stream()));
     *bits = e;
     if (e) return set_err(BM_ERR_TIMEOUT, "device-side wait timed out (error bits 0x%x)", e);
+    return BM_OK;
+}
+
+int bm_area_deliver_tract(bm_area src, uint32_t src_output, bm_area dst, uint32_t dst_input, uint64_t dst_offset) {
+    if (!src || !dst) return set_err(BM_ERR_INVALID, "null area");
+    if (src->ctx->device != dst->ctx->device) return set_err(BM_ERR_INVALID, "tract between areas on different devices");
+    if (src_output >= src->plan.n_outputs) return set_err(BM_ERR_INVALID, "output %u out of range", src_output);
+    if (dst_input >= dst->plan.n_inputs) return set_err(BM_ERR_INVALID, "input %u out of range", dst_input);
+    const uint32_t len = src->plan.outputs[src_output].len;
+    if (dst_offset + len > dst->plan.inputs[dst_input].len)
+        return set_err(BM_ERR_INVALID, "tract of %u axons at offset %llu overruns input %u (%u axons)", len,
+                       (unsigned long long)dst_offset, dst_input, dst->plan.inputs[dst_input].len);
+    DevGuard g(dst->ctx->device);
+    cudaStream_t s = dst->stream();
+    if (src->stream() != s) {
+        // After the work already queued for the source area.
+        cudaEvent_t e = src->ev();
+        CU(cudaEventRecord(e, src->stream()));
+        CU(cudaStreamWaitEvent(s, e, 0));
+        src->pool.push_back(e);
+    }
+    const uint8_t* from = src->axns() + src->plan.outputs[src_output].axn_idz;
+    std::vector<FramePiece> pieces;
+    frame_pieces(dst, dst_input, (uint32_t)dst_offset, len, pieces);
+    for (const FramePiece& p : pieces) CU(cudaMemcpyAsync(p.dst, from + p.off, p.len, cudaMemcpyDeviceToDevice, s));
+    return BM_OK;
+}
+
+int bm_area_clear_errors(bm_area area) {
+    if (!area) return set_err(BM_ERR_INVALID, "null area");
+    DevGuard g(area->ctx->device);
+    const unsigned int zero = 0;
+    CU(cudaStreamSynchronize(area->stream()));
+    CU(cudaMemcpyAsync(&area->ctl->error, &zero, sizeof zero, cudaMemcpyHostToDevice, area->stream()));
+    CU(cudaStreamSynchronize(area->stream()));
+    *(volatile unsigned int*)area->host_err = 0;
+    return BM_OK;
+}
+
+int bm_area_set_wait_limit(bm_area area, uint32_t us) {
+    if (!area) return set_err(BM_ERR_INVALID, "null area");
+    DevGuard g(area->ctx->device);
+    CU(cudaMemcpyAsync(&area->ctl->wait_us, &us, sizeof us, cudaMemcpyHostToDevice, area->stream()));
+    CU(cudaStreamSynchronize(area->stream()));
+    return BM_OK;
+}
+
+int bm_area_inject_stall(bm_area area, uint32_t stage) {
+    if (!area) return set_err(BM_ERR_INVALID, "null area");
+    DevGuard g(area->ctx->device);
+    CU(cudaMemcpyAsync(&area->ctl->stall_stage, &stage, sizeof stage, cudaMemcpyHostToDevice, area->stream()));
+    CU(cudaStreamSynchronize(area->stream()));
+    return BM_OK;
+}
+
+int bm_area_tuft_form(bm_area area, uint32_t layer, uint32_t tuft, bm_tuft_form* out) {
+    if (!area || !out) return set_err(BM_ERR_INVALID, "null argument");
+    if (layer >= area->plan.n_layers || tuft >= area->plan.layers[layer].n_tufts)
+        return set_err(BM_ERR_INVALID, "layer %u tuft %u out of range", layer, tuft);
+    DevGuard g(area->ctx->device);
+    *out = bm_tuft_form{};
+    const FusedTuft& FT = area->fused.t[layer][tuft];
+    const bm_layer_plan& L = area->plan.layers[layer];
+    if (area->exec_path != BM_PATH_FUSED || !FT.ok) return BM_OK;
+    // The status words reflect the sources and flags as of the last write.
+    run_pending_verifies(area, area->stream());
+    unsigned int status = 0;
+    CU(cudaMemcpyAsync(&status, &area->ctl->tuft_status[layer * BM_MAX_TUFTS + tuft], sizeof status,
+                       cudaMemcpyDeviceToHost, area->stream()));
+    CU(cudaStreamSynchronize(area->stream()));
+    out->fused = 1;
+    out->tiled = FT.tiled ? 1 : 0;
+    out->consumer = consumer_shape(FT, L.tufts[tuft].syns_per_tft, L.tufts[tuft].syns_per_den,
+                                   L.kind == BM_LYR_PYRAMIDAL);
+    out->sources_outside = (status & kTuftSrcOutsideTile) ? 1 : 0;
+    out->flags_foreign = (status & kTuftFlagsForeign) ? 1 : 0;
+    if (FT.tiled) {
+        out->tile_w = FT.tile_w;
+        out->tile_h = FT.tile_h;
+        out->stages = FT.nst;
+        out->grid = FT.grid;
+        out->smem = FT.smem;
+        out->footprint_tma = FT.fp_tma ? 1 : 0;
+    }
     return BM_OK;
 }
 

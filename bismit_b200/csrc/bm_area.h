@@ -6,6 +6,8 @@
 #include <cstdint>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "bm_fused.h"
 #include "bm_kernels.h"
 
@@ -106,6 +108,7 @@ struct bm_area_s {
     bm_area_plan plan;
     uint8_t* slab = nullptr;
     bm::AreaCtl* ctl = nullptr;
+    unsigned int* host_err = nullptr;   // host-mapped mirror of ctl->error (written when non-zero)
     bm::SliceRec* slices = nullptr;
     bm::DevLayer dl[BM_MAX_LAYERS];
     uint64_t inhib_key[BM_MAX_LAYERS][BM_MAX_CTRL];
@@ -163,6 +166,8 @@ struct bm_area_s {
     bm::TuftGeo geo[BM_MAX_LAYERS][BM_MAX_TUFTS] = {};
 
     cudaStream_t stream() const { return ctx->stream(); }
+    // Device error bits a completed cycle mirrored to the host (0: none seen).
+    unsigned int seen_errors() const { return host_err ? *(volatile const unsigned int*)host_err : 0u; }
     uint8_t* axns() const { return slab + plan.axon_off; }
 
     cudaEvent_t ev() {
@@ -171,8 +176,15 @@ struct bm_area_s {
         cudaEventCreate(&e);
         return e;
     }
+    // Every stage launch sits in an NVTX range named after its kernel kind
+    // (a no-op unless a profiler is attached), and is timed with CUDA events
+    // when profiling is on.
     template <class F> void run(int kind, F&& f) {
         if (kind != bm::K_INTAKE) launches++;
+        struct Range {
+            explicit Range(const char* n) { nvtxRangePushA(n); }
+            ~Range() { nvtxRangePop(); }
+        } range(bm::kKindNames[kind]);
         if (!profiling) { f(); return; }
         Rec r{kind, ev(), ev()};
         cudaEventRecord(r.a, stream());
@@ -231,6 +243,10 @@ int sample_after_cycle(bm_area_s* A, cudaStream_t s);
 void free_samplers(bm_area_s* A);
 // Detaches A from the batches holding it before it is destroyed (bm_batch.cu).
 void detach_from_batches(bm_area_s* A);
+// One batched cycle over device frames that does not refuse areas with
+// device error bits: the caller (the server) checked them itself before
+// taking frames from its queues (bm_batch.cu).
+int batch_cycle_frames_unchecked(bm_batch_s* B, const void* dev_frames);
 int cuda_err(cudaError_t e, const char* what);
 
 }  // namespace bm

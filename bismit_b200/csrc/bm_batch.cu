@@ -140,7 +140,7 @@ __global__ void __launch_bounds__(kIntakeBlock)
 __global__ void k_batch_cycle_end(AreaCtl* const* __restrict__ ctls, uint32_t n, BatchCtl* bc) {
     pdl_begin();
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) ctls[i]->cycle += 1;
+    if (i < n) end_cycle(ctls[i]);
     if (i == 0) bc->cursor += 1;
 }
 
@@ -746,8 +746,14 @@ int after_cycle(bm_batch_s* B, cudaStream_t s) {
     return BM_OK;
 }
 
-int run_cycles(bm_batch_s* B, const void* frames, uint32_t n_cycles) {
+int run_cycles(bm_batch_s* B, const void* frames, uint32_t n_cycles, bool refuse_after_errors = true) {
     if (B->detached) return set_err(BM_ERR_INVALID, "an area of this batch was destroyed");
+    // An area whose earlier cycle ended with device error bits stops the batch
+    // (bm_area_clear_errors on that area re-enables it).
+    for (size_t a = 0; a < B->areas.size() && refuse_after_errors; a++)
+        if (const unsigned int e = B->areas[a]->seen_errors())
+            return set_err(BM_ERR_TIMEOUT, "area %zu of the batch ended an earlier cycle with device error bits 0x%x",
+                           a, e);
     cudaStream_t s = B->stream();
     for (bm_area A : B->areas) run_pending_verifies(A, s);
     // Caller writes may have changed what an area's tuft steps read.
@@ -851,6 +857,11 @@ bool apply_target(bm_batch_s* B, bm_batch_s::StepPlan& p, uint32_t target) {
 }
 
 }  // namespace
+
+int bm::batch_cycle_frames_unchecked(bm_batch_s* B, const void* dev_frames) {
+    DevGuard g(B->ctx->device);
+    return run_cycles(B, dev_frames, 1, false);
+}
 
 extern "C" {
 

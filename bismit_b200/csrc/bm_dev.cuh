@@ -84,9 +84,23 @@ constexpr unsigned int kTuftFlagsForeign = 2u;     // some flag byte has bits ot
 struct AreaCtl {
     unsigned long long cycle;       // cycle number of the cycle in flight
     unsigned int error;             // sticky device-side error bits (kErr*)
+    unsigned int wait_us;           // limit of each bounded wait in the tuft kernels, us (0: kDefaultWaitUs)
+    unsigned int stall_stage;       // fault injection: CTA 0's producer withholds its stall_stage-th
+                                    // stage (counted from 1) of every tiled tuft launch (0: none)
     unsigned int pad;
+    unsigned int* host_err;         // host-mapped word the cycle end copies non-zero error bits to
+                                    // (null: none), so the host sees them without a synchronisation
     unsigned int tuft_status[BM_MAX_LAYERS * BM_MAX_TUFTS];
 };
+constexpr unsigned int kDefaultWaitUs = 2000000u;   // 2 s
+
+// The cycle's last kernel: advance the counter, and mirror any error bits to
+// the host-mapped word.
+__device__ __forceinline__ void end_cycle(AreaCtl* c) {
+    c->cycle += 1;
+    const unsigned int e = c->error;
+    if (e && c->host_err) *(volatile unsigned int*)c->host_err = e;
+}
 
 __host__ __device__ inline uint64_t splitmix64(uint64_t x) {
     x += 0x9E3779B97F4A7C15ull;

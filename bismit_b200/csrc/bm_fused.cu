@@ -39,6 +39,8 @@
 // kErrWaitTimeout, lets its own copies in flight land and returns.
 #include "bm_fused.h"
 
+#include <cuda.h>
+
 #include <algorithm>
 #include <cstddef>
 #include <cstring>
@@ -58,6 +60,7 @@ constexpr uint32_t kSmem3 = 73 * 1024;       // ... with which three CTAs fit on
 constexpr uint32_t kWaitLimit = 1u << 22;
 
 struct FusedTuftArgs {
+    CUtensorMap tmap;       // footprint box of the recorded slices (fp_tma); first, for its 64-byte alignment
     const uint8_t* axns;
     const SliceRec* slices;
     AreaCtl* ctl;
@@ -109,7 +112,11 @@ struct FusedTuftArgs {
     uint32_t win;                       // dendrite / cell-tuft windows ride in the stages
     uint32_t win_bytes;                 // bytes per window
     uint32_t geom;                      // specialised consumer for this shape (0: the general one)
+    uint32_t fp_tma;                    // the footprint comes from a tensor box load (else consumers stage it)
+    uint32_t fp_bytes;                  // bytes of that box (nrec * frows * fw)
 };
+static_assert(offsetof(FusedTuftArgs, tmap) == 0 && alignof(FusedTuftArgs) >= 64,
+              "the tensor map must sit 64-byte aligned in the parameter block");
 
 // Lanes of a cell write its eight cell-tuft fields through one pointer table.
 static_assert(offsetof(FusedTuftArgs, t_st) == offsetof(FusedTuftArgs, t_pid) + 7 * sizeof(uint8_t*),
@@ -165,17 +172,21 @@ __device__ __forceinline__ uint64_t global_ns() {
     asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
     return t;
 }
-// Bounded wait: false once kWaitNs of wall time have passed without the
-// phase completing.
-constexpr uint64_t kWaitNs = 2000000000ull;
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+// Bounded wait: false once `limit_ns` of wall time have passed without the
+// phase completing (and in any case after kWaitLimit suspended tries).
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, uint64_t limit_ns) {
     if (mbar_try_wait(bar, parity)) return true;
     const uint64_t t0 = global_ns();
     for (uint32_t i = 0; i < kWaitLimit; i++) {
         if (mbar_try_wait_sleep(bar, parity, 200000u)) return true;
-        if (global_ns() - t0 > kWaitNs) return false;
+        if (global_ns() - t0 > limit_ns) return false;
     }
     return false;
+}
+// The wait limit of an area's tuft launches (AreaCtl::wait_us; 0: the default).
+__device__ __forceinline__ uint64_t wait_limit_ns(const AreaCtl* ctl) {
+    const unsigned int us = ctl ? ctl->wait_us : 0u;
+    return 1000ull * (us ? us : kDefaultWaitUs);
 }
 // 1-D bulk copy global -> shared completing on `bar` (16-byte aligned, size % 16 == 0).
 __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
@@ -184,8 +195,36 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
         "l"(src), "r"(bytes), "r"(smem_addr(bar))
         : "memory");
 }
+// 3-D tensor box load global -> shared completing on `bar` (no multicast;
+// the box's x coordinate is a multiple of 16 bytes, elements outside the
+// tensor read as 0).
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, int32_t x, int32_t y, int32_t z,
+                                            uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+        "[%5];" ::"r"(smem_addr(dst)),
+        "l"(map), "r"(x), "r"(y), "r"(z), "r"(smem_addr(bar))
+        : "memory");
+}
+// Orders this thread's generic shared-memory writes before later writes of
+// the async proxy (a tensor load into the same bytes).
+__device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 // Barrier among the consumer warps only (the producer warp runs free).
 __device__ __forceinline__ void consumers_sync() { asm volatile("bar.sync 1, %0;" ::"n"(kWarps * 32) : "memory"); }
+// The same barrier, returning the OR of `p` over the consumer warps: every
+// consumer thread gets the same answer, so decisions taken on it stay uniform.
+__device__ __forceinline__ bool consumers_sync_or(bool p) {
+    uint32_t r;
+    asm volatile(
+        "{\n\t.reg .pred q, o;\n\t"
+        "setp.ne.u32 q, %1, 0;\n\t"
+        "barrier.cta.red.or.pred o, 1, %2, q;\n\t"
+        "selp.u32 %0, 1, 0, o;\n\t}"
+        : "=r"(r)
+        : "r"((uint32_t)p), "n"(kWarps * 32)
+        : "memory");
+    return r != 0;
+}
 
 // ------------------------------------------------------------ helpers ----
 // 0xFF in every byte of x whose sign bit is set (prmt's sign-replicate mode).
@@ -420,6 +459,7 @@ __device__ __forceinline__ uint32_t fast_div(uint32_t x, uint32_t d, uint64_t m)
 struct TileGeo {
     uint32_t v0, u0, h, w;
     int32_t vlo, ulo;
+    uint32_t xoff;                   // fp_tma: columns sit (ulo & 15) bytes into each footprint row
     uint32_t cell0, syn0, syn_end;   // tuft-relative (a tuft has fewer than 2^32 synapses)
 };
 
@@ -435,6 +475,7 @@ __device__ __forceinline__ TileGeo tile_geo(const FusedTuftArgs& A, uint32_t t) 
     g.w = min(A.tile_w, A.u_size - g.u0);
     g.vlo = (int32_t)((g.v0 * A.src_vs) >> kSlcSclCoeffL2) - A.rv;
     g.ulo = (int32_t)((g.u0 * A.src_us) >> kSlcSclCoeffL2) - A.ru;
+    g.xoff = A.fp_tma ? ((uint32_t)g.ulo & 15u) : 0u;
     g.cell0 = s_lyr * A.cols + g.v0 * A.u_size + g.u0;
     g.syn0 = g.cell0 << A.S_l2;
     g.syn_end = (g.cell0 + g.h * g.w) << A.S_l2;
@@ -455,7 +496,24 @@ __device__ __forceinline__ int32_t footprint_base(const FusedTuftArgs& A, const 
         u = local - q * A.u_size;
     }
     return ((int32_t)((v * A.src_vs) >> kSlcSclCoeffL2) - G.vlo) * (int32_t)A.fw +
-           ((int32_t)((u * A.src_us) >> kSlcSclCoeffL2) - G.ulo);
+           ((int32_t)((u * A.src_us) >> kSlcSclCoeffL2) - G.ulo) + (int32_t)G.xoff;
+}
+
+// syn_fire of four packed axon bytes (cl/syns.cl:2-4).
+__device__ __forceinline__ uint32_t fire4(uint32_t x) { return nz_bits(x) | ((x >> 1) & 0x7F7F7F7Fu); }
+
+// A footprint the tensor load brought in holds raw axon bytes: fire them in
+// place (consumer threads, 16 bytes each per step; the box is a multiple of
+// 16 bytes).
+__device__ __forceinline__ void fire_footprint(uint8_t* halo, uint32_t bytes) {
+    for (uint32_t i = threadIdx.x * 16u; i < bytes; i += kWarps * 32 * 16) {
+        uint4 v = *(const uint4*)(halo + i);
+        v.x = fire4(v.x);
+        v.y = fire4(v.y);
+        v.z = fire4(v.z);
+        v.w = fire4(v.w);
+        *(uint4*)(halo + i) = v;
+    }
 }
 
 // Stages the tile's footprint: element (k, row, column), row-major, holds
@@ -617,6 +675,22 @@ __host__ __device__ constexpr int geom_lpc_l2(int g) {
     return g == 1 ? 1 : g == 2 ? 2 : g == 3 ? 3 : g == 4 ? 4 : g == 5 ? 4 : 5;
 }
 
+}  // namespace
+
+// The specialised consumer a tiled tuft's launches dispatch to: shapes 3..7
+// on pyramidal layers, 1..2 on spiny stellate layers, 0 (the general
+// consumer) otherwise. It applies while the tuft's flags are clean and its
+// sources lie in the footprint.
+uint32_t consumer_shape(const FusedTuft& FT, uint32_t spt, uint32_t spd, bool pyramidal) {
+    if (!FT.tiled || !FT.win || spt > 512 || FT.stage_bytes != (uint32_t)kWarps * 512) return 0;
+    for (int g = 1; g < kGeoms; g++)
+        if ((1u << geom_spd_l2(g)) == spd && (1u << (geom_lpc_l2(g) + 4)) == spt)
+            return (pyramidal ? g >= 3 : g <= 2) ? (uint32_t)g : 0u;
+    return 0;
+}
+
+namespace {
+
 template <bool TUFT, int SPD_L2, int LPC_L2>
 __device__ __forceinline__ void stage_fast(const FusedTuftArgs& A, const TileGeo& G, const uint8_t* halo,
                                            const uint8_t* sb, uint32_t pos, int lane, int wib, int32_t rnd) {
@@ -734,21 +808,46 @@ __device__ __forceinline__ void stage_fast(const FusedTuftArgs& A, const TileGeo
     }
 }
 
-// Producer lane: issues every stage of tile G into the ring (buffer pb of
-// round pround). False when a bounded wait gave up.
+// Raises the CTA's abort flag. The thread that raises it first records the
+// give-up in the error bits of the area it was serving (its bounded wait ran
+// out); the others' waits then end at once.
+__device__ __forceinline__ void raise_abort(volatile int& s_abort, AreaCtl* ctl) {
+    if (atomicExch((int*)&s_abort, 1) == 0 && ctl) atomicOr(&ctl->error, kErrWaitTimeout);
+}
+
+// The producer lane's ring position and fault-injection state.
+struct ProducerState {
+    uint32_t pb = 0, pround = 0;   // next buffer, and its round
+    uint64_t issued = 0;           // stages issued (withheld ones included)
+    uint64_t stall = 0;            // withhold the stage issued as number `stall` (counted from 1; 0: none)
+    int withheld = -1;             // buffer of the withheld stage (-1: none)
+    uint64_t limit_ns = 0;         // bounded-wait limit
+};
+
+// Producer lane: issues every stage of tile G into the ring. False when a
+// bounded wait gave up. A stage withheld for fault injection is neither
+// copied nor armed, so its full barrier never completes and the consumers'
+// bounded wait runs out; the producer cannot use that buffer again (its
+// release never comes), so it is the buffer's last use.
 template <bool TUFT, int MODE, bool FCLEAN>
 __device__ __forceinline__ bool produce_tile(const FusedTuftArgs& A, const TileGeo& G, uint8_t* stages,
-                                             uint64_t* full, uint64_t* empty, uint32_t& pb, uint32_t& pround,
-                                             uint64_t& issued, volatile int& s_abort) {
+                                             uint64_t* full, uint64_t* empty, ProducerState& ps,
+                                             volatile int& s_abort) {
     const uint32_t SB = stage_syns<MODE, FCLEAN>(A.stage_bytes);
     const uint32_t buf_bytes = A.stage_stride;
     const uint32_t nst = A.nst;
     for (uint32_t pos = G.syn0; pos < G.syn_end; pos += SB) {
         if (s_abort) return false;
+        uint32_t& pb = ps.pb;
         // Buffer pb's previous use (round pround - 1) must be released.
-        if (pround > 0 && !mbar_wait(&empty[pb], (pround - 1) & 1)) {
-            s_abort = 1;
+        if (ps.pround > 0 && !mbar_wait(&empty[pb], (ps.pround - 1) & 1, ps.limit_ns)) {
+            raise_abort(s_abort, A.ctl);
             return false;
+        }
+        if (++ps.issued == ps.stall) {
+            ps.withheld = (int)pb;
+            if (++pb == nst) { pb = 0; ps.pround++; }
+            continue;
         }
         const uint32_t left = G.syn_end - pos;
         const uint32_t nb = left < SB ? left : SB;
@@ -780,40 +879,55 @@ __device__ __forceinline__ bool produce_tile(const FusedTuftArgs& A, const TileG
         bulk_g2s(dst + arr_off<MODE>(0, SB), A.str + pos, nb, &full[pb]);
         bulk_g2s(dst + arr_off<MODE>(1, SB), A.st + pos, nb, &full[pb]);
         if (!FCLEAN) bulk_g2s(dst + arr_off<MODE>(2, SB), A.fl + pos, nb, &full[pb]);
-        issued++;
-        if (++pb == nst) { pb = 0; pround++; }
+        if (++pb == nst) { pb = 0; ps.pround++; }
     }
     return true;
 }
 
-// After a give-up: record it and let this CTA's copies land before its
-// shared memory is released (the latest use of every buffer must complete).
-__device__ __forceinline__ void producer_drain(AreaCtl* ctl, uint64_t* full, uint32_t nst, uint64_t issued) {
-    if (ctl) atomicOr(&ctl->error, kErrWaitTimeout);
+// After a give-up (or a withheld stage): let this CTA's copies land before
+// its shared memory is released -- the latest armed use of every buffer must
+// complete. A withheld stage was its buffer's last use and was never armed,
+// so that buffer's latest armed use is the one before it.
+__device__ __forceinline__ void producer_drain(uint64_t* full, uint32_t nst, const ProducerState& ps) {
     for (uint32_t b = 0; b < nst; b++) {
-        const uint64_t uses = issued / nst + (b < issued % nst ? 1 : 0);
-        if (uses) mbar_wait(&full[b], (uint32_t)((uses - 1) & 1));
+        uint64_t uses = ps.issued / nst + (b < ps.issued % nst ? 1 : 0);
+        if ((int)b == ps.withheld) uses--;
+        if (uses) mbar_wait(&full[b], (uint32_t)((uses - 1) & 1), ps.limit_ns);
     }
 }
 
-// Consumer warps: stage tile G's footprint, then process its stages from the
-// ring (buffer cb, phase cphase). A give-up sets s_abort; every consumer then
-// leaves at the next tile's barrier.
+// Consumer warps: take tile G's footprint -- wait for its tensor load and
+// fire it in place, or stage it themselves -- then process the tile's stages
+// from the ring (buffer cb, phase cphase) and release the footprint. False
+// when this warp gave up (a bounded wait ran out, or a give-up elsewhere was
+// seen); the consumer warps then leave together at the next tile's barrier,
+// whose OR-reduction keeps that decision uniform.
 template <bool TUFT, int MODE, bool FCLEAN, int GEOM>
-__device__ __forceinline__ void consume_tile(const FusedTuftArgs& A, const TileGeo& G, uint8_t* halo, uint8_t* stages,
-                                             uint64_t* full, uint64_t* empty, uint32_t& cb, uint32_t& cphase,
-                                             int lane, int wib, int32_t rnd, volatile int& s_abort) {
-    build_footprint(A, G, halo, lane, wib);
+__device__ __forceinline__ bool consume_tile(const FusedTuftArgs& A, const TileGeo& G, uint8_t* halo, uint8_t* stages,
+                                             uint64_t* full, uint64_t* empty, uint64_t* fp_full, uint64_t* fp_empty,
+                                             uint32_t& cb, uint32_t& cphase, uint32_t& fp_n, int lane, int wib,
+                                             int32_t rnd, uint64_t limit_ns, volatile int& s_abort) {
+    if (A.fp_tma) {
+        bool got = !s_abort && mbar_wait(fp_full, fp_n & 1, limit_ns);
+        got = __all_sync(0xFFFFFFFFu, got);
+        fp_n++;
+        if (!got && lane == 0) raise_abort(s_abort, A.ctl);
+        if (consumers_sync_or(!got)) return false;
+        fire_footprint(halo, A.fp_bytes);
+        fence_proxy_async_smem();   // the next tile's load overwrites these bytes
+    } else {
+        build_footprint(A, G, halo, lane, wib);
+    }
     consumers_sync();
     const uint32_t SB = stage_syns<MODE, FCLEAN>(A.stage_bytes);
     const uint32_t cpu = A.chunks_per_unit;
     const uint32_t n_units_tile = cpu > 1 ? G.h * G.w : (G.syn_end - G.syn0 + 511) >> 9;
     for (uint32_t pos = G.syn0; pos < G.syn_end; pos += SB) {
-        bool got = !s_abort && mbar_wait(&full[cb], cphase);
+        bool got = !s_abort && mbar_wait(&full[cb], cphase, limit_ns);
         got = __all_sync(0xFFFFFFFFu, got);
         if (!got) {
-            if (lane == 0) s_abort = 1;
-            return;
+            if (lane == 0) raise_abort(s_abort, A.ctl);
+            return false;
         }
         if constexpr (GEOM == 0)
             tma_stage<TUFT, MODE, FCLEAN>(A, G, halo, stages + (size_t)cb * A.stage_stride, pos, n_units_tile, lane,
@@ -825,36 +939,83 @@ __device__ __forceinline__ void consume_tile(const FusedTuftArgs& A, const TileG
         if (lane == 0) mbar_arrive(&empty[cb]);
         if (++cb == A.nst) { cb = 0; cphase ^= 1; }
     }
+    __syncwarp();
+    if (lane == 0) mbar_arrive(fp_empty);   // done with this tile's footprint
+    return true;
 }
+
+// Footprint lane of the producer warp: for the i-th tile of this CTA that
+// loads its footprint with a tensor box, waits until the consumers released
+// the footprint of tile i - 1 (they release one per tile), then arms fp_full
+// and issues the box. False when that wait gave up.
+__device__ __forceinline__ bool produce_footprint(const FusedTuftArgs& A, const TileGeo& G, uint8_t* halo,
+                                                  uint64_t* fp_full, uint64_t* fp_empty, uint32_t i,
+                                                  uint32_t& fp_issued, uint64_t limit_ns) {
+    if (i > 0 && !mbar_wait(fp_empty, (i - 1) & 1, limit_ns)) return false;   // the caller raises the abort
+    mbar_arrive_expect_tx(fp_full, A.fp_bytes);
+    tma_load_3d(halo, &A.tmap, G.ulo - (int32_t)G.xoff, G.vlo, 0, fp_full);
+    fp_issued++;
+    return true;
+}
+
+// After the footprint lane's last box (or a give-up): let the latest box land
+// before the CTA's shared memory is released.
+__device__ __forceinline__ void footprint_drain(uint64_t* fp_full, uint32_t fp_issued, uint64_t limit_ns) {
+    if (fp_issued) mbar_wait(fp_full, (fp_issued - 1) & 1, limit_ns);
+}
+
+// Shared-memory barriers of a CTA: the ring's full[nst] and empty[nst], then
+// the footprint's full and empty at fixed slots (nst <= 4).
+constexpr uint32_t kFpFullSlot = 8, kFpEmptySlot = 9;
 
 template <bool TUFT, int MODE, bool FCLEAN, int GEOM>
 __device__ __forceinline__ void tma_body(const FusedTuftArgs& A, uint8_t* smem, volatile int& s_abort) {
     uint64_t* full = (uint64_t*)(smem + A.ring_off);   // [nst]
     uint64_t* empty = full + A.nst;                    // [nst]
+    uint64_t* fp_full = full + kFpFullSlot;
+    uint64_t* fp_empty = full + kFpEmptySlot;
     uint8_t* stages = smem + A.ring_off + 128;
     uint8_t* halo = smem;
     const int tid = threadIdx.x;
     const int lane = tid & 31;
     const int wib = tid >> 5;
+    const uint64_t limit_ns = wait_limit_ns(A.ctl);
     if (wib == kWarps) {
-        // ---- producer warp: lane 0 streams every stage of this CTA's tiles ----
+        if (lane == 1) {
+            // ---- footprint lane: one tensor box per tile ----
+            uint32_t fp_issued = 0;
+            if (A.fp_tma) {
+                uint32_t i = 0;
+                for (uint32_t t = blockIdx.x; t < A.n_tiles && !s_abort; t += gridDim.x, i++)
+                    if (!produce_footprint(A, tile_geo(A, t), halo, fp_full, fp_empty, i, fp_issued, limit_ns)) {
+                        raise_abort(s_abort, A.ctl);
+                        break;
+                    }
+            }
+            footprint_drain(fp_full, fp_issued, limit_ns);
+            return;
+        }
+        // ---- stage lane: lane 0 streams every stage of this CTA's tiles ----
         if (lane != 0) return;
-        uint32_t pb = 0, pround = 0;
-        uint64_t issued = 0;
+        ProducerState ps;
+        ps.limit_ns = limit_ns;
+        ps.stall = blockIdx.x == 0 ? A.ctl->stall_stage : 0u;
         for (uint32_t t = blockIdx.x; t < A.n_tiles && !s_abort; t += gridDim.x)
-            if (!produce_tile<TUFT, MODE, FCLEAN>(A, tile_geo(A, t), stages, full, empty, pb, pround, issued, s_abort))
-                break;
-        if (s_abort) producer_drain(A.ctl, full, A.nst, issued);
+            if (!produce_tile<TUFT, MODE, FCLEAN>(A, tile_geo(A, t), stages, full, empty, ps, s_abort)) break;
+        if (s_abort || ps.withheld >= 0) producer_drain(full, A.nst, ps);
         return;
     }
     // ---- consumer warps ----
     const int32_t rnd = rnd_at(A.rnd_key, A.ctl->cycle);
-    uint32_t cb = 0, cphase = 0;
+    uint32_t cb = 0, cphase = 0, fp_n = 0;
+    bool ok = true;
     for (uint32_t t = blockIdx.x; t < A.n_tiles; t += gridDim.x) {
         const TileGeo G = tile_geo(A, t);
-        consumers_sync();   // every consumer is done with the previous footprint
-        if (s_abort) break;
-        consume_tile<TUFT, MODE, FCLEAN, GEOM>(A, G, halo, stages, full, empty, cb, cphase, lane, wib, rnd, s_abort);
+        // Every consumer is done with the previous tile; all leave together
+        // if any gave up.
+        if (consumers_sync_or(!ok || s_abort)) break;
+        ok = consume_tile<TUFT, MODE, FCLEAN, GEOM>(A, G, halo, stages, full, empty, fp_full, fp_empty, cb, cphase,
+                                                    fp_n, lane, wib, rnd, limit_ns, s_abort);
     }
 }
 
@@ -866,6 +1027,8 @@ __device__ __forceinline__ void init_ring(uint8_t* ring, uint32_t nst, volatile 
             mbar_init(&full[i], 1);
             mbar_init(&empty[i], kWarps);
         }
+        mbar_init(full + kFpFullSlot, 1);
+        mbar_init(full + kFpEmptySlot, kWarps);
         fence_mbar_init();
         s_abort = 0;
     }
@@ -880,7 +1043,7 @@ __device__ __forceinline__ uint32_t mode_of(const FusedTuftArgs& A) {
 }
 
 template <bool TUFT>
-__global__ void __launch_bounds__(kThreads, 3) k_fused_tuft_tma(FusedTuftArgs A) {
+__global__ void __launch_bounds__(kThreads, 3) k_fused_tuft_tma(const __grid_constant__ FusedTuftArgs A) {
     pdl_begin();
     extern __shared__ __align__(128) uint8_t smem[];
     __shared__ volatile int s_abort;   // a bounded wait gave up
@@ -952,6 +1115,8 @@ __global__ void __launch_bounds__(kThreads, 3) k_fused_tuft_batch(const __grid_c
     init_ring(smem + P.ring_off, nst, s_abort);
     uint64_t* full = (uint64_t*)(smem + P.ring_off);
     uint64_t* empty = full + nst;
+    uint64_t* fp_full = full + kFpFullSlot;
+    uint64_t* fp_empty = full + kFpEmptySlot;
     uint8_t* stages = smem + P.ring_off + 128;
     uint8_t* halo = smem;
     const uint32_t n_tiles = P.tile0[P.n_jobs];
@@ -959,9 +1124,29 @@ __global__ void __launch_bounds__(kThreads, 3) k_fused_tuft_batch(const __grid_c
     const int lane = tid & 31;
     const int wib = tid >> 5;
     if (wib == kWarps) {
+        if (lane == 1) {
+            // ---- footprint lane: one tensor box per tile of a job that uses them ----
+            uint32_t cur = 0xFFFFFFFFu, i = 0, fp_issued = 0;
+            uint64_t lim = 0;
+            for (uint32_t t = blockIdx.x; t < n_tiles && !s_abort; t += gridDim.x, i++) {
+                const uint32_t j = job_of(P, t);
+                const FusedTuftArgs& A = P.jobs[j];
+                if (j != cur) {
+                    cur = j;
+                    lim = wait_limit_ns(A.ctl);
+                }
+                if (!A.fp_tma) continue;
+                if (!produce_footprint(A, tile_geo(A, t - P.tile0[j]), halo, fp_full, fp_empty, i, fp_issued, lim)) {
+                    raise_abort(s_abort, A.ctl);
+                    break;
+                }
+            }
+            footprint_drain(fp_full, fp_issued, lim);
+            return;
+        }
         if (lane != 0) return;
-        uint32_t cur = 0xFFFFFFFFu, mode = 0, pb = 0, pround = 0;
-        uint64_t issued = 0;
+        uint32_t cur = 0xFFFFFFFFu, mode = 0;
+        ProducerState ps;
         AreaCtl* ctl = nullptr;
         for (uint32_t t = blockIdx.x; t < n_tiles && !s_abort; t += gridDim.x) {
             const uint32_t j = job_of(P, t);
@@ -970,35 +1155,45 @@ __global__ void __launch_bounds__(kThreads, 3) k_fused_tuft_batch(const __grid_c
                 cur = j;
                 mode = mode_of(A);
                 ctl = A.ctl;
+                // Waits follow the job's area. The fault hook: the CTA that
+                // takes a job's first tile withholds the job area's
+                // stall_stage-th stage from that tile on.
+                ps.limit_ns = wait_limit_ns(ctl);
+                if (t == P.tile0[j] && ctl->stall_stage) ps.stall = ps.issued + ctl->stall_stage;
             }
             const TileGeo G = tile_geo(A, t - P.tile0[j]);
             bool ok;
             switch (mode) {
-            case 0: ok = produce_tile<TUFT, 0, true>(A, G, stages, full, empty, pb, pround, issued, s_abort); break;
-            case 1: ok = produce_tile<TUFT, 0, false>(A, G, stages, full, empty, pb, pround, issued, s_abort); break;
-            case 2: ok = produce_tile<TUFT, 1, true>(A, G, stages, full, empty, pb, pround, issued, s_abort); break;
-            default: ok = produce_tile<TUFT, 1, false>(A, G, stages, full, empty, pb, pround, issued, s_abort); break;
+            case 0: ok = produce_tile<TUFT, 0, true>(A, G, stages, full, empty, ps, s_abort); break;
+            case 1: ok = produce_tile<TUFT, 0, false>(A, G, stages, full, empty, ps, s_abort); break;
+            case 2: ok = produce_tile<TUFT, 1, true>(A, G, stages, full, empty, ps, s_abort); break;
+            default: ok = produce_tile<TUFT, 1, false>(A, G, stages, full, empty, ps, s_abort); break;
             }
             if (!ok) break;
         }
-        if (s_abort) producer_drain(ctl, full, nst, issued);
+        if (s_abort || ps.withheld >= 0) producer_drain(full, nst, ps);
         return;
     }
-    uint32_t cur = 0xFFFFFFFFu, mode = 0, cb = 0, cphase = 0;
+    uint32_t cur = 0xFFFFFFFFu, mode = 0, cb = 0, cphase = 0, fp_n = 0;
     int32_t rnd = 0;
+    uint64_t limit_ns = 0;
+    bool ok = true;
     for (uint32_t t = blockIdx.x; t < n_tiles; t += gridDim.x) {
         const uint32_t j = job_of(P, t);
         const FusedTuftArgs& A = P.jobs[j];
-        consumers_sync();   // every consumer is done with the previous footprint
-        if (s_abort) break;
+        // Every consumer is done with the previous tile; all leave together
+        // if any gave up.
+        if (consumers_sync_or(!ok || s_abort)) break;
         if (j != cur) {
             cur = j;
             mode = mode_of(A);
             rnd = rnd_at(A.rnd_key, A.ctl->cycle);
+            limit_ns = wait_limit_ns(A.ctl);
         }
         const TileGeo G = tile_geo(A, t - P.tile0[j]);
-#define BM_CONSUME(M, FC, GM) \
-    consume_tile<TUFT, M, FC, GM>(A, G, halo, stages, full, empty, cb, cphase, lane, wib, rnd, s_abort)
+#define BM_CONSUME(M, FC, GM)                                                                                   \
+    ok = consume_tile<TUFT, M, FC, GM>(A, G, halo, stages, full, empty, fp_full, fp_empty, cb, cphase, fp_n, lane, \
+                                       wib, rnd, limit_ns, s_abort)
         switch (mode) {
         case 0:
             if (TUFT) {
@@ -1106,8 +1301,10 @@ int device_sms() {
 }
 
 // Launch parameters of tuft t of data layer i (gidx left null). `target` is
-// the synapses per tile to aim for (0: chosen from the tuft's size).
-void plan_tuft(FusedTuft& FT, const bm_area_plan& P, uint32_t i, uint32_t t, int sms, uint32_t target_syns = 0) {
+// the synapses per tile to aim for (0: chosen from the tuft's size);
+// `allow_tma` lets the footprint come from a tensor box load.
+void plan_tuft(FusedTuft& FT, const bm_area_plan& P, uint32_t i, uint32_t t, int sms, uint32_t target_syns = 0,
+               bool allow_tma = true) {
     const bm_layer_plan& L = P.layers[i];
     bool aligned = true;
     for (int k = 0; k < BM_BUF_COUNT; k++)
@@ -1184,6 +1381,20 @@ void plan_tuft(FusedTuft& FT, const bm_area_plan& P, uint32_t i, uint32_t t, int
             return;   // even one cell's footprint is too large for 16-bit offsets
         }
     }
+    // The footprint by tensor box: a 3-D view (column, row, slice) of the
+    // recorded slices, which must lie back to back with rows of a multiple of
+    // 16 bytes. A box starts on a 16-byte column boundary, so its rows are
+    // up to 15 bytes wider than the footprint's.
+    bool tma = allow_tma && P.slc_u_size[lo] % 16 == 0 && P.slc_axn_idz[lo] % 16 == 0;
+    for (uint32_t k = 1; k < nrec && tma; k++)
+        tma = P.slc_axn_idz[lo + k] == P.slc_axn_idz[lo] + k * P.slc_v_size[lo] * P.slc_u_size[lo];
+    const uint64_t fwb = (fw + 15 + 15) / 16 * 16;
+    tma = tma && fwb <= 256 && frows <= 256 && (uint64_t)nrec * frows * fwb < 32768;
+    if (tma) {
+        fw = fwb;
+        fsz = frows * fw;
+        halo = (uint64_t)nrec * fsz;
+    }
     // Windows: up to SB / 16 dendrites (or cells) per stage, widened by 16
     // at both ends.
     const uint32_t win_bytes = SB / 16 + 32;
@@ -1197,6 +1408,7 @@ void plan_tuft(FusedTuft& FT, const bm_area_plan& P, uint32_t i, uint32_t t, int
     const uint64_t smem = std::max<uint64_t>(32768, ring_off + 128 + (uint64_t)nst * buf_bytes);
     if (smem > kMaxSmem) return;
     FT.tiled = true;
+    FT.fp_tma = tma;
     FT.tile_w = W;
     FT.tile_h = H;
     FT.rv = rv;
@@ -1255,14 +1467,17 @@ bool retile_fused_tuft(FusedArea& F, const bm_area_plan& P, uint32_t layer, uint
     plan_tuft(next, P, layer, t, F.sms, target_syns);
     cudaGetLastError();
     if (!next.tiled) return false;
-    if (next.tile_w == FT.tile_w && next.tile_h == FT.tile_h && next.nst == FT.nst && next.smem == FT.smem) {
+    if (next.tile_w == FT.tile_w && next.tile_h == FT.tile_h && next.nst == FT.nst && next.smem == FT.smem &&
+        next.fp_tma == FT.fp_tma) {
         FT.tile_target = target_syns;   // same tiles: the compiled offsets stay valid
         return true;
     }
     *changed = true;
     next.gidx = FT.gidx;
     next.tile_target = target_syns;
+    next.bound_axns = FT.bound_axns;
     FT = next;
+    if (FT.bound_axns) bind_fused_tuft(F, P, layer, t, FT.bound_axns);
     return true;
 }
 
@@ -1283,6 +1498,75 @@ int prepare_fused(FusedArea& F, const bm_area_plan& P, std::string* err) {
                 return BM_ERR_OOM;
             }
         }
+    return BM_OK;
+}
+
+namespace {
+
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+// cuTensorMapEncodeTiled, resolved once through the runtime (the library does
+// not link the driver library).
+EncodeTiledFn encode_tiled() {
+    static EncodeTiledFn fn = [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) !=
+                cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            p = nullptr;
+        cudaGetLastError();
+        return (EncodeTiledFn)p;
+    }();
+    return fn;
+}
+
+// The footprint box of tiled tuft FT over the axon space at `axns`: u8
+// elements, dims (u_size, v_size, nrec) of the recorded slices, box (fw,
+// frows, nrec); coordinates outside the slices read as 0.
+bool encode_footprint_map(FusedTuft& FT, const bm_area_plan& P, const uint8_t* axns) {
+    EncodeTiledFn enc = encode_tiled();
+    if (!enc) return false;
+    const uint32_t lo = FT.slc0;
+    const cuuint64_t dims[3] = {P.slc_u_size[lo], P.slc_v_size[lo], FT.nrec};
+    const cuuint64_t strides[2] = {P.slc_u_size[lo], (cuuint64_t)P.slc_u_size[lo] * P.slc_v_size[lo]};
+    const cuuint32_t box[3] = {FT.fw, FT.frows, FT.nrec};
+    const cuuint32_t elem[3] = {1, 1, 1};
+    CUtensorMap m;
+    const CUresult r = enc(&m, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, (void*)(axns + P.slc_axn_idz[lo]), dims, strides, box,
+                           elem, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                           CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return false;
+    static_assert(sizeof m == sizeof FT.tmap, "tensor map size");
+    std::memcpy(FT.tmap, &m, sizeof m);
+    return true;
+}
+
+}  // namespace
+
+int bind_fused_tuft(FusedArea& F, const bm_area_plan& P, uint32_t layer, uint32_t t, const uint8_t* axns) {
+    FusedTuft& FT = F.t[layer][t];
+    FT.bound_axns = axns;
+    if (!FT.tiled || !FT.fp_tma) return BM_OK;
+    if (((uintptr_t)(axns + P.slc_axn_idz[FT.slc0]) & 15) == 0 && encode_footprint_map(FT, P, axns)) return BM_OK;
+    // The driver refused the box: the consumers stage the footprint instead
+    // (same tiles, rows without the column alignment).
+    FusedTuft next;
+    plan_tuft(next, P, layer, t, F.sms, FT.tile_target, false);
+    cudaGetLastError();
+    next.gidx = FT.gidx;
+    next.tile_target = FT.tile_target;
+    next.tile_tuned = FT.tile_tuned;
+    next.bound_axns = axns;
+    FT = next;
+    return BM_OK;
+}
+
+int bind_fused(FusedArea& F, const bm_area_plan& P, const uint8_t* axns) {
+    for (uint32_t i = 0; i < P.n_layers; i++)
+        for (uint32_t t = 0; t < P.layers[i].n_tufts; t++) bind_fused_tuft(F, P, i, t, axns);
     return BM_OK;
 }
 
@@ -1312,6 +1596,7 @@ GatherGeo geo_of(const FusedTuft& FT, const DevLayer& L, const DevTuft& T) {
     g.fsz = FT.fsz;
     g.slc0 = FT.slc0;
     g.nrec = FT.nrec;
+    g.xalign = FT.tiled && FT.fp_tma ? 1u : 0u;
     return g;
 }
 
@@ -1420,11 +1705,10 @@ void make_args(FusedTuftArgs& A, const FusedArea& F, const uint8_t* axns, const 
         A.stage_stride = FT.stage_stride;
         A.win = FT.win;
         A.win_bytes = FT.win_bytes;
-        // The specialised consumer of this shape, if there is one.
-        A.geom = 0;
-        if (FT.win && A.chunks_per_unit == 1 && FT.stage_bytes == (uint32_t)kWarps * 512)
-            for (int g = 1; g < kGeoms; g++)
-                if ((uint32_t)geom_spd_l2(g) == A.spd_l2 && (uint32_t)geom_lpc_l2(g) + 4 == A.S_l2) A.geom = (uint32_t)g;
+        A.fp_tma = FT.fp_tma ? 1u : 0u;
+        A.fp_bytes = FT.nrec * FT.fsz;
+        if (FT.fp_tma) std::memcpy(&A.tmap, FT.tmap, sizeof A.tmap);
+        A.geom = consumer_shape(FT, (uint32_t)S, T.spd, tuft);
     } else {
         A.n_units = S > 512 ? (uint64_t)L.cells : (A.n_syn + 511) / 512;
     }

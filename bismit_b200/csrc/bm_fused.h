@@ -31,6 +31,12 @@ struct FusedTuft {
     uint32_t src_idz[8] = {};
     uint32_t tile_target = 0;    // synapses per tile asked for (0: chosen from the tuft's size)
     bool tile_tuned = false;     // tile_target came from the autotuner
+    // Footprint loaded by the tensor memory accelerator (a 3-D box of the
+    // source slices) instead of staged by the consumer warps; rows of fw
+    // bytes then start on a 16-byte column boundary (GatherGeo::xalign).
+    bool fp_tma = false;
+    alignas(64) unsigned char tmap[128] = {};   // its tensor map (bind_fused_tuft), a CUtensorMap
+    const uint8_t* bound_axns = nullptr;        // the axon space the tensor map points into
 };
 
 struct FusedArea {
@@ -53,6 +59,14 @@ int plan_fused_tuft(FusedArea& F, const bm_area_plan& P, uint32_t layer, uint32_
 bool retile_fused_tuft(FusedArea& F, const bm_area_plan& P, uint32_t layer, uint32_t t, uint32_t target_syns,
                        bool* changed);
 void free_fused(FusedArea& F);
+// Encodes the footprint tensor maps of the tufts that load their footprint
+// with the tensor memory accelerator, for the axon space at `axns` (device
+// memory, 16-byte aligned). BM_ERR_CUDA when the driver refuses one.
+int bind_fused(FusedArea& F, const bm_area_plan& P, const uint8_t* axns);
+int bind_fused_tuft(FusedArea& F, const bm_area_plan& P, uint32_t layer, uint32_t t, const uint8_t* axns);
+// The specialised consumer shape tiled tuft FT's launches use while its flags
+// are clean and its sources lie in the footprint (0: the general consumer).
+uint32_t consumer_shape(const FusedTuft& FT, uint32_t spt, uint32_t spd, bool pyramidal);
 // Gather geometry of tiled tuft t of data layer `layer` as planned in F.
 GatherGeo gather_geo(const FusedArea& F, const bm_area_plan& P, uint32_t layer, uint32_t t);
 // Synapse flags + synapse cycle + dendrite cycle (+ tuft cycle for pyramidal

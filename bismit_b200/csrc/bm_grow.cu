@@ -82,7 +82,7 @@ __global__ void k_grow(DevLayer L, GrowTuft G) {
     }
 }
 
-__global__ void k_cycle_end(AreaCtl* ctl) { pdl_begin(); ctl->cycle += 1; }
+__global__ void k_cycle_end(AreaCtl* ctl) { pdl_begin(); end_cycle(ctl); }
 
 // Synapses::regrow (src/cortex/synapses.rs:411-501) with SynSrcIdxCache
 // (src/map/syn_src.rs:159-211), one dendrite per thread, on the cycles c with

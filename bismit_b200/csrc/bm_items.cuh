@@ -253,19 +253,55 @@ __device__ __forceinline__ void tuft_cell_item(const uint8_t* __restrict__ axns,
     if (L.kind == BM_LYR_PYRAMIDAL) tft_cycle_item(L, t, c);
 }
 
-// Lanes of the warp apply ssc_mtp_simple's update to cell cc's synapses
-// (prx_syns__active__mtp_ltd, cl/bismit.cl:604-639; seed syn_idz + i).
-__device__ __forceinline__ void ssc_mtp_lanes(const DevLayer& L, int32_t rnd, uint32_t cc, int lane) {
-    const uint32_t spt = L.tft[0].spt;
-    const uint8_t* st = L.buf[BM_BUF_SYN_STATES];
+// The strength updates of learning, for every learning cell of the warp
+// (lanes in `mask`, each with its run of synapses [z, z + n)), the warp sharing
+// each run; four runs at a time, all four loaded before any is stored, so
+// their latencies overlap (runs of different cells are disjoint). SSC:
+// prx_syns__active__mtp_ltd (cl/bismit.cl:604-639: a synapse is active when
+// its state is non-zero, depression mask 0x1FF); else
+// dst_syns__active__mtpot_mtdep (cl/bismit.cl:554-600: active when
+// SYN_PREV_ACTIVE is set, depression mask 0xFFF). Both seed with the run's
+// first index plus the synapse index (the doubled index, :589,592,629,630).
+template <bool SSC>
+__device__ __forceinline__ void learn_runs_warp(const DevLayer& L, int32_t rnd, unsigned mask, uint32_t z,
+                                                uint32_t n, int lane) {
+    const uint8_t* act = SSC ? L.buf[BM_BUF_SYN_STATES] : L.buf[BM_BUF_SYN_FLAG_SETS];
     int8_t* str = (int8_t*)L.buf[BM_BUF_SYN_STRENGTHS];
-    const uint32_t syn_idz = cc * spt;
-    for (uint32_t i = syn_idz + (uint32_t)lane; i < syn_idz + spt; i += 32) {
-        int8_t s = str[i];
-        const int32_t seed = (int32_t)(syn_idz + i);
-        if (st[i] != 0) s = (int8_t)(s + rnd_inc(rnd, seed, s, 0x7F));
-        else s = (int8_t)(s - rnd_dec(rnd, seed, s, 0x1FF));
-        str[i] = s;
+    constexpr int32_t kDecMask = SSC ? 0x1FF : 0xFFF;
+    while (mask) {
+        uint32_t zk[4], nk[4], nmax = 0;
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            const int b = mask ? __ffs(mask) - 1 : 0;
+            const uint32_t zb = __shfl_sync(0xFFFFFFFFu, z, b), nb = __shfl_sync(0xFFFFFFFFu, n, b);
+            zk[k] = zb;
+            nk[k] = mask ? nb : 0u;
+            nmax = max(nmax, nk[k]);
+            mask &= mask - 1;
+        }
+        for (uint32_t o = (uint32_t)lane; o < nmax; o += 32) {
+            int8_t sv[4];
+            uint8_t av[4];
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                if (o < nk[k]) {
+                    sv[k] = str[zk[k] + o];
+                    av[k] = act[zk[k] + o];
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                if (o < nk[k]) {
+                    const uint32_t i = zk[k] + o;
+                    const int32_t seed = (int32_t)(zk[k] + i);
+                    const bool on = SSC ? av[k] != 0 : (av[k] & kSynPrevActiveFlag) != 0;
+                    int8_t s = sv[k];
+                    if (on) s = (int8_t)(s + rnd_inc(rnd, seed, s, 0x7F));
+                    else s = (int8_t)(s - rnd_dec(rnd, seed, s, kDecMask));
+                    str[i] = s;
+                }
+            }
+        }
     }
 }
 
@@ -278,13 +314,8 @@ __device__ __forceinline__ void inhib_mtp_warp(uint8_t* __restrict__ axns, const
                                                bool learn, uint32_t c, bool valid) {
     const uint8_t ax = valid ? inhib_simple_item(axns, slices, L, radius, rnd_inhib, c) : (uint8_t)0;
     if (!learn) return;
-    const int lane = threadIdx.x & 31;
-    unsigned mask = __ballot_sync(0xFFFFFFFFu, ax != 0);
-    while (mask) {
-        const int b = __ffs(mask) - 1;
-        mask &= mask - 1;
-        ssc_mtp_lanes(L, rnd_mtp, __shfl_sync(0xFFFFFFFFu, c, b), lane);
-    }
+    const uint32_t spt = L.tft[0].spt;
+    learn_runs_warp<true>(L, rnd_mtp, __ballot_sync(0xFFFFFFFFu, ax != 0), c * spt, spt, threadIdx.x & 31);
 }
 
 // pyr_cycle for the cells of column col, then its control (1: inhib_intra_column,
@@ -297,19 +328,6 @@ __device__ __forceinline__ void inhib_mtp_warp(uint8_t* __restrict__ axns, const
 // input is loaded before any result is stored, so the loads overlap.
 constexpr uint32_t kTailDepth = 8;
 
-__device__ __forceinline__ void dst_mtp_lanes(const DevLayer& L, const DevTuft& T, int32_t rnd, uint32_t z,
-                                              uint32_t nn, int lane) {
-    const uint8_t* sfl = L.buf[BM_BUF_SYN_FLAG_SETS];
-    int8_t* str = (int8_t*)L.buf[BM_BUF_SYN_STRENGTHS];
-    for (uint32_t i = z + (uint32_t)lane; i < z + nn; i += 32) {
-        int8_t s = str[i];
-        const int32_t seed = (int32_t)(z + i);
-        if (sfl[i] & kSynPrevActiveFlag) s = (int8_t)(s + rnd_inc(rnd, seed, s, 0x7F));
-        else s = (int8_t)(s - rnd_dec(rnd, seed, s, 0xFFF));
-        str[i] = s;
-    }
-}
-
 // Cell c of distal tuft T learns (tft_dst_mtp's condition): its synapse run
 // [z, z + n), n = 0 when it does not.
 __device__ __forceinline__ void dst_mtp_range(const DevLayer& L, const DevTuft& T, uint32_t c, uint8_t f, bool active,
@@ -321,6 +339,19 @@ __device__ __forceinline__ void dst_mtp_range(const DevLayer& L, const DevTuft& 
         z = (uint32_t)L.buf[BM_BUF_TFT_PREV_BEST_DEN_IDS][tci] * T.spd + c * T.spt + (uint32_t)T.syn_idz;
         // A best-dendrite id written by the caller past the tuft can address
         // beyond the layer's synapses; such a range is skipped.
+        n = ((uint64_t)z + T.spd <= L.n_syns) ? T.spd : 0;
+    }
+}
+
+// The same decision from the cell's previous best raw state and id, already
+// loaded (so their loads can be issued with the cell's other inputs).
+__device__ __forceinline__ void dst_mtp_range_of(const DevLayer& L, const DevTuft& T, uint32_t c, uint8_t f,
+                                                 bool active, bool valid, uint8_t praw, uint8_t pid, uint32_t& z,
+                                                 uint32_t& n) {
+    z = 0;
+    n = 0;
+    if (valid && !(f & kCelPrevActiveFlag) && active && praw != 0) {
+        z = (uint32_t)pid * T.spd + c * T.spt + (uint32_t)T.syn_idz;
         n = ((uint64_t)z + T.spd <= L.n_syns) ? T.spd : 0;
     }
 }
@@ -352,10 +383,21 @@ __device__ __forceinline__ void pyr_tail_warp(uint8_t* __restrict__ axns, const 
         const bool prx_on = (L.enabled_flags & kDenBasalProximalFlag) != 0;
         const bool dst_on = (L.enabled_flags & kDenBasalDistalFlag) != 0;
         uint8_t prx = 0, dst = 0, f = 0, ax = 0;
+        uint8_t praw[BM_MAX_TUFTS] = {}, pid[BM_MAX_TUFTS] = {};   // distal tufts' previous best
         if (valid) {
             prx = prx_on ? L.buf[BM_BUF_TFT_STATES][(uint64_t)L.prx_id * L.cells + c] : (uint8_t)0;
             dst = dst_on ? L.buf[BM_BUF_TFT_BEST_DEN_STATES_RAW][(uint64_t)L.dst_id * L.cells + c] : (uint8_t)0;
-            if (learn) f = cfl[c];
+            if (learn) {
+                f = cfl[c];
+#pragma unroll
+                for (uint32_t t = 0; t < BM_MAX_TUFTS; t++) {
+                    if (t < L.n_tufts && L.tft[t].den_kind == BM_DEN_DISTAL) {
+                        const uint32_t tci = c + (uint32_t)L.tft[t].cel_idz;
+                        praw[t] = L.buf[BM_BUF_TFT_PREV_BEST_DEN_STATES_RAW][tci];
+                        pid[t] = L.buf[BM_BUF_TFT_PREV_BEST_DEN_IDS][tci];
+                    }
+                }
+            }
             if (ctrl == 0) ax = axns[L.axn_idz + c];
         }
         // pyr_cycle, cl/bismit.cl:961-1022 (as pyr_cycle_item).
@@ -378,18 +420,15 @@ __device__ __forceinline__ void pyr_tail_warp(uint8_t* __restrict__ axns, const 
         }
         if (valid && ctrl != 0) axns[L.axn_idz + c] = ax;
         if (!learn) return;
-        for (uint32_t t = 0; t < L.n_tufts; t++) {
+#pragma unroll
+        for (uint32_t t = 0; t < BM_MAX_TUFTS; t++) {
+            if (t >= L.n_tufts) break;
             const DevTuft& T = L.tft[t];
             if (T.den_kind != BM_DEN_DISTAL) continue;
             const int32_t rnd = rnd_at(T.rnd_key_mtp, ctl->cycle);
             uint32_t z, n;
-            dst_mtp_range(L, T, c, f, ax != 0, valid, z, n);
-            unsigned mask = __ballot_sync(0xFFFFFFFFu, n != 0);
-            while (mask) {
-                const int b = __ffs(mask) - 1;
-                mask &= mask - 1;
-                dst_mtp_lanes(L, T, rnd, __shfl_sync(0xFFFFFFFFu, z, b), __shfl_sync(0xFFFFFFFFu, n, b), lane);
-            }
+            dst_mtp_range_of(L, T, c, f, ax != 0, valid, praw[t], pid[t], z, n);
+            learn_runs_warp<false>(L, rnd, __ballot_sync(0xFFFFFFFFu, n != 0), z, n, lane);
             f = (uint8_t)((f & ~kCelPrevActiveFlag) | (ax ? kCelPrevActiveFlag : 0));
         }
         if (valid) cfl[c] = f;
@@ -415,12 +454,7 @@ __device__ __forceinline__ void pyr_tail_warp(uint8_t* __restrict__ axns, const 
             const int32_t rnd = rnd_at(T.rnd_key_mtp, ctl->cycle);
             uint32_t z, n;
             dst_mtp_range(L, T, c, f, active, valid, z, n);
-            unsigned mask = __ballot_sync(0xFFFFFFFFu, n != 0);
-            while (mask) {
-                const int b = __ffs(mask) - 1;
-                mask &= mask - 1;
-                dst_mtp_lanes(L, T, rnd, __shfl_sync(0xFFFFFFFFu, z, b), __shfl_sync(0xFFFFFFFFu, n, b), lane);
-            }
+            learn_runs_warp<false>(L, rnd, __ballot_sync(0xFFFFFFFFu, n != 0), z, n, lane);
             f = (uint8_t)((f & ~kCelPrevActiveFlag) | (active ? kCelPrevActiveFlag : 0));
         }
         if (valid) cfl[c] = f;

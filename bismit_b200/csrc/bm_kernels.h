@@ -40,8 +40,11 @@ constexpr uint32_t kRegrowBlock = 128;
 // Gather geometry of a tiled tuft. Its cells are cut into tiles of tile_h
 // rows x tile_w columns of one layer slice; a tile's footprint holds, for each
 // of the nrec source slices from slc0 on, the rows and columns its cells'
-// scaled positions reach with offsets up to rv, ru (fw columns, fsz bytes per
-// slice).
+// scaled positions reach with offsets up to rv, ru (rows of fw bytes, fsz
+// bytes per slice). With xalign the footprint is loaded by the tensor memory
+// accelerator, whose boxes start on a 16-byte column boundary: each row then
+// begins at the tile's first column rounded down to a multiple of 16, and
+// every column sits (first column & 15) bytes further in.
 struct GatherGeo {
     uint32_t S_l2;           // log2 synapses per cell-tuft
     uint32_t cols, u_size;   // layer columns, row width
@@ -50,6 +53,7 @@ struct GatherGeo {
     int32_t rv, ru;
     uint32_t fw, fsz;
     uint32_t slc0, nrec;
+    uint32_t xalign;
 };
 
 // The byte that the synapse at tuft offset i with source (slc, v_ofs, u_ofs)
@@ -63,8 +67,9 @@ __host__ __device__ __forceinline__ uint32_t gather_offset(const GatherGeo& g, u
     const uint32_t rem = c % g.cols;
     const uint32_t v = rem / g.u_size, u = rem - (rem / g.u_size) * g.u_size;
     const uint32_t v0 = v - v % g.tile_h, u0 = u - u % g.tile_w;
+    const int32_t ulo = (int32_t)((u0 * g.us) >> 4) - g.ru;   // the footprint's first column
     const int32_t row = (int32_t)((v * g.vs) >> 4) - (int32_t)((v0 * g.vs) >> 4) + g.rv + vo;
-    const int32_t col = (int32_t)((u * g.us) >> 4) - (int32_t)((u0 * g.us) >> 4) + g.ru + uo;
+    const int32_t col = (int32_t)((u * g.us) >> 4) - ulo + uo + (g.xalign ? (ulo & 15) : 0);
     const uint32_t k = slc - g.slc0;
     ok = k < g.nrec && vo >= -g.rv && vo <= g.rv && uo >= -g.ru && uo <= g.ru;
     return ok ? k * g.fsz + (uint32_t)row * g.fw + (uint32_t)col : 0u;

@@ -19,14 +19,24 @@
 // sessions: their areas are built and grown on a second stream, so set-up
 // overlaps the running cycles too.
 //
+// Admission runs off the tick path: a builder thread owned by the server
+// builds and grows each admitted session's area on its own stream (and
+// destroys retired ones), and a tick adopts the areas that are ready, so a
+// tick never waits for a set-up or a teardown.
+//
 // Latency of a frame = completion of the tick that cycled it minus the moment
 // it became ready (its submission, or the completion of the session's
 // previous frame if that came later): admission waits show up in it.
 #include <algorithm>
+#include <atomic>
 #include <chrono>
+#include <condition_variable>
 #include <cstring>
 #include <deque>
+#include <mutex>
 #include <new>
+#include <string>
+#include <thread>
 #include <vector>
 
 #include "bm_area.h"
@@ -105,7 +115,14 @@ struct bm_server_s {
         double last_done = 0;        // completion time of the latest cycled frame
         double opened = 0, admitted = 0;
         bool closing = false, resident = false, retired = false;
+        bool failed = false;         // dropped after its area ended a cycle with device error bits
+        // Set-up by the builder thread: kWaiting until the budget admits the
+        // session, kQueued while the builder has it, then kBuilt or kFailed.
+        std::atomic<int> build{0};
+        int build_rc = BM_OK;
+        std::string build_msg;       // the builder's error message (error text is per thread)
     };
+    static constexpr int kWaiting = 0, kQueued = 1, kBuilt = 2, kFailed = 3;
     // A queued tick: its sessions (with their frames' submission times), its
     // pinned blocks and completion event.
     struct Tick {
@@ -120,6 +137,7 @@ struct bm_server_s {
     uint64_t budget = 0, used = 0;
     uint32_t next_id = 1;
     std::vector<Session*> sessions;  // every open session, in open order
+    std::vector<uint32_t> failed_ids;    // sessions dropped after a device error
     bm_batch batch = nullptr;
     std::vector<Session*> members;   // the batch's sessions, in batch order
     uint8_t* h_frames[2] = {};       // pinned frame blocks (double-buffered)
@@ -139,8 +157,20 @@ struct bm_server_s {
     std::vector<float> lat_ms;
     uint64_t ticks = 0, frames_cycled = 0, rebuilds = 0;
     double syn_cycles = 0, busy_s = 0, first_tick = 0, last_tick = 0;
-    double rebuild_s = 0, admit_s = 0;   // host time in batch rebuilds and in admissions
+    double rebuild_s = 0;                // host time in batch rebuilds
+    std::atomic<double> admit_s{0};      // builder-thread time in admissions
     double gpu_s = 0;                    // device time of the ticks (frames in to outputs out)
+    // The builder thread and its queues (guarded by mu).
+    std::thread builder;
+    std::mutex mu;
+    std::condition_variable cv;
+    bool stop = false;
+    std::deque<Session*> build_q;        // admitted sessions whose areas the builder builds
+    struct Teardown {
+        bm_area area;
+        uint8_t* out;
+    };
+    std::deque<Teardown> free_q;         // retired sessions' areas and output buffers
 
     Session* find(uint32_t id) {
         for (Session* s : sessions)
@@ -157,18 +187,11 @@ void free_session(bm_server_s::Session* S) {
     delete S;
 }
 
-// Device bytes a session holds while resident (slab, gather offsets of every
-// tuft, control block and slice table), from its resolved plan.
-uint64_t footprint(const bm_area_plan& P) {
-    uint64_t b = P.slab_bytes + 2 * P.n_syns_total + sizeof(AreaCtl) + BM_MAX_SLICES * sizeof(SliceRec);
-    return (b + 0xFFFFF) & ~0xFFFFFull;   // the allocator's 1 MiB-ish granularity, rounded up
-}
-
-// Builds the area of S on the set-up context and moves it to the serving one.
-int admit(bm_server_s* V, bm_server_s::Session* S) {
+// Builds S's area on the set-up context and its pinned output buffer (builder
+// thread). The area is complete (grown, synchronised) when this returns.
+int build_session(bm_server_s* V, bm_server_s::Session* S) {
     int rc = bm_area_create(V->setup, &S->desc, S->seed, &S->area);
     if (rc != BM_OK) return rc;
-    S->area->ctx = V->ctx;   // same device; later work goes to the serving stream
     if (cudaHostAlloc(&S->out, S->out_len ? S->out_len : 1, cudaHostAllocDefault) != cudaSuccess) {
         cudaGetLastError();
         bm_area_destroy(S->area);
@@ -176,18 +199,83 @@ int admit(bm_server_s* V, bm_server_s::Session* S) {
         return set_err(BM_ERR_OOM, "pinned output buffer");
     }
     std::memset(S->out, 0, S->out_len ? S->out_len : 1);
-    S->resident = true;
-    S->admitted = now_s();
-    V->used += S->bytes;
     return BM_OK;
 }
 
+// The builder thread: tears down retired sessions' areas and builds admitted
+// sessions' areas, in queue order, until the server stops.
+void builder_loop(bm_server_s* V, int device) {
+    cudaSetDevice(device);
+    std::unique_lock<std::mutex> lk(V->mu);
+    for (;;) {
+        V->cv.wait(lk, [&] { return V->stop || !V->build_q.empty() || !V->free_q.empty(); });
+        if (!V->free_q.empty()) {
+            const bm_server_s::Teardown T = V->free_q.front();
+            V->free_q.pop_front();
+            lk.unlock();
+            if (T.area) bm_area_destroy(T.area);
+            if (T.out) cudaFreeHost(T.out);
+            lk.lock();
+            continue;
+        }
+        if (!V->build_q.empty()) {
+            bm_server_s::Session* S = V->build_q.front();
+            V->build_q.pop_front();
+            lk.unlock();
+            const double t0 = now_s();
+            S->build_rc = build_session(V, S);
+            if (S->build_rc != BM_OK) S->build_msg = bm_last_error();
+            V->admit_s.store(V->admit_s.load() + (now_s() - t0));
+            S->build.store(S->build_rc == BM_OK ? bm_server_s::kBuilt : bm_server_s::kFailed,
+                           std::memory_order_release);
+            lk.lock();
+            continue;
+        }
+        if (V->stop) return;
+    }
+}
+
+// Device bytes a session holds while resident (slab, gather offsets of every
+// tuft, control block and slice table), from its resolved plan.
+uint64_t footprint(const bm_area_plan& P) {
+    uint64_t b = P.slab_bytes + 2 * P.n_syns_total + sizeof(AreaCtl) + BM_MAX_SLICES * sizeof(SliceRec);
+    return (b + 0xFFFFF) & ~0xFFFFFull;   // the allocator's 1 MiB-ish granularity, rounded up
+}
+
+// Reserves S's bytes and hands it to the builder thread.
+void admit(bm_server_s* V, bm_server_s::Session* S) {
+    V->used += S->bytes;
+    S->build.store(bm_server_s::kQueued);
+    {
+        std::lock_guard<std::mutex> g(V->mu);
+        V->build_q.push_back(S);
+    }
+    V->cv.notify_one();
+}
+
+// A built session joins the ticks: its area's later work goes to the serving
+// stream (same device).
+void adopt(bm_server_s* V, bm_server_s::Session* S) {
+    S->area->ctx = V->ctx;
+    S->resident = true;
+    S->admitted = now_s();
+}
+
+// Releases S's budget and hands its area and output buffer to the builder
+// thread for teardown.
 void retire(bm_server_s* V, bm_server_s::Session* S) {
-    if (S->resident) V->used -= S->bytes;
+    if (S->build.load() != bm_server_s::kWaiting) V->used -= S->bytes;
     S->resident = false;
     S->retired = true;
-    if (S->area) bm_area_destroy(S->area);
+    if (S->area || S->out) {
+        {
+            std::lock_guard<std::mutex> g(V->mu);
+            V->free_q.push_back({S->area, S->out});
+        }
+        V->cv.notify_one();
+    }
     S->area = nullptr;
+    S->out = nullptr;
 }
 
 // Grows a pair of pinned blocks and their device block (the stream must be
@@ -303,6 +391,7 @@ int bm_server_create(bm_ctx ctx, uint64_t mem_budget, bm_server* out) {
         delete V;
         return set_err(BM_ERR_CUDA, "cudaEventCreate");
     }
+    V->builder = std::thread(builder_loop, V, ctx->device);
     *out = V;
     return BM_OK;
 }
@@ -310,6 +399,12 @@ int bm_server_create(bm_ctx ctx, uint64_t mem_budget, bm_server* out) {
 int bm_server_destroy(bm_server V) {
     if (!V) return BM_OK;
     DevGuard g(V->ctx->device);
+    {
+        std::lock_guard<std::mutex> lk(V->mu);
+        V->stop = true;
+    }
+    V->cv.notify_one();
+    if (V->builder.joinable()) V->builder.join();   // it finishes its queues first
     cudaStreamSynchronize(V->ctx->stream());
     if (V->batch) bm_batch_destroy(V->batch);
     for (auto* S : V->sessions) free_session(S);
@@ -379,6 +474,15 @@ int bm_server_close(bm_server V, uint32_t session) {
     return BM_OK;
 }
 
+int bm_server_cancel(bm_server V, uint32_t session) {
+    if (!V) return set_err(BM_ERR_INVALID, "null server");
+    auto* S = V->find(session);
+    if (!S) return set_err(BM_ERR_INVALID, "bm_server_cancel: no open session %u", session);
+    S->closing = true;
+    S->frames.chunks.clear();   // frames already in a queued tick still complete
+    return BM_OK;
+}
+
 int bm_server_tick(bm_server V, uint32_t* n_cycled) {
     if (!V) return set_err(BM_ERR_INVALID, "null server");
     DevGuard g(V->ctx->device);
@@ -386,10 +490,37 @@ int bm_server_tick(bm_server V, uint32_t* n_cycled) {
     const double t0 = now_s();
     if (!V->first_tick) V->first_tick = t0;
 
-    // 1. Retire drained, closed sessions (no frame left, none in flight). A
-    //    batch that holds one is dropped first.
+    // 0. A session whose area ended a cycle with device error bits (a bounded
+    //    wait in a kernel gave up) is dropped with its queued frames; the
+    //    tick reports it once, after the queued ticks complete, and the next
+    //    tick runs the other sessions without it.
+    {
+        uint32_t n_failed = 0, first = 0;
+        unsigned int bits = 0;
+        for (auto* S : V->sessions) {
+            if (!S->resident || S->failed || !S->area) continue;
+            const unsigned int e = S->area->seen_errors();
+            if (!e) continue;
+            S->failed = true;
+            S->closing = true;
+            S->frames.chunks.clear();
+            V->failed_ids.push_back(S->id);
+            if (!n_failed++) { first = S->id; bits = e; }
+        }
+        if (n_failed) {
+            const int rc = complete_all(V);
+            if (rc != BM_OK) return rc;
+            return set_err(BM_ERR_TIMEOUT,
+                           "bm_server_tick: session %u ended a cycle with device error bits 0x%x and was dropped "
+                           "(%u session(s) this tick)", first, bits, n_failed);
+        }
+    }
+
+    // 1. Retire drained, closed sessions (no frame left, none in flight, not
+    //    with the builder). A batch that holds one is dropped first.
     for (auto* S : V->sessions) {
         if (!S->closing || !S->frames.empty() || S->inflight) continue;
+        if (S->build.load(std::memory_order_acquire) == bm_server_s::kQueued) continue;
         if (std::find(V->members.begin(), V->members.end(), S) != V->members.end()) {
             if (V->batch) bm_batch_destroy(V->batch);
             V->batch = nullptr;
@@ -403,10 +534,26 @@ int bm_server_tick(bm_server V, uint32_t* n_cycled) {
         else free_session(S);
     V->sessions.swap(live);
 
-    // 2. Queue tick N: resident sessions with a pending frame.
+    // 2. Adopt the sessions the builder finished, then queue tick N: resident
+    //    sessions with a pending frame.
+    for (auto* S : V->sessions) {
+        if (S->resident || S->retired) continue;
+        const int b = S->build.load(std::memory_order_acquire);
+        if (b == bm_server_s::kBuilt) adopt(V, S);
+        else if (b == bm_server_s::kFailed) {
+            // Reported once; the session waits for admission again.
+            V->used -= S->bytes;
+            S->build.store(bm_server_s::kWaiting);
+            return set_err(S->build_rc, "bm_server_tick: building session %u failed: %s", S->id,
+                           S->build_msg.c_str());
+        }
+    }
+    // A session whose area shows device error bits is left out (the next
+    // tick drops it); the batch then runs without checking them again, so a
+    // bit that appears after this check cannot strand the tick's frames.
     std::vector<bm_server_s::Session*> m;
     for (auto* S : V->sessions)
-        if (S->resident && !S->frames.empty()) m.push_back(S);
+        if (S->resident && !S->frames.empty() && !S->area->seen_errors()) m.push_back(S);
     if (n_cycled) *n_cycled = (uint32_t)m.size();
     const uint32_t slot = (uint32_t)(V->tick_no & 1);
     if (!m.empty()) {
@@ -452,7 +599,7 @@ int bm_server_tick(bm_server V, uint32_t* n_cycled) {
         cudaError_t e = cudaEventRecord(V->start_ev[slot], s);
         if (e == cudaSuccess) e = cudaMemcpyAsync(V->d_frames, V->h_frames[slot], o, cudaMemcpyHostToDevice, s);
         if (e != cudaSuccess) return cuda_err(e, "frame block copy");
-        int rc = bm_batch_cycle_frames_device(V->batch, V->d_frames, 1);
+        int rc = batch_cycle_frames_unchecked(V->batch, V->d_frames);
         if (rc != BM_OK) return rc;
         if (V->out_blocks) k_gather_outputs<<<V->out_blocks, kGatherBlock, 0, s>>>(V->d_outjobs, (uint32_t)m.size(), V->d_out);
         e = cudaMemcpyAsync(V->h_out[slot], V->d_out, V->out_bytes, cudaMemcpyDeviceToHost, s);
@@ -461,17 +608,14 @@ int bm_server_tick(bm_server V, uint32_t* n_cycled) {
         V->tick_no++;
     }
 
-    // 3. While it runs: admit waiting sessions in FIFO order as the budget
-    //    allows (none overtakes an earlier one that does not fit). Their areas
-    //    are built and grown on the set-up stream; they join a later tick.
-    const double a0 = now_s();
+    // 3. Admit waiting sessions in FIFO order as the budget allows (none
+    //    overtakes an earlier one that does not fit). The builder thread
+    //    builds their areas; they join the first tick after it is done.
     for (auto* S : V->sessions) {
-        if (S->resident) continue;
+        if (S->resident || S->build.load() != bm_server_s::kWaiting || S->retired) continue;
         if (V->used + S->bytes > V->budget) break;
-        int rc = admit(V, S);
-        if (rc != BM_OK) return rc;
+        admit(V, S);
     }
-    V->admit_s += now_s() - a0;
 
     // 4. Complete the previous tick (with nothing queued now: every tick).
     if (!m.empty()) return complete(V, slot ^ 1);
@@ -487,6 +631,10 @@ int bm_server_drain(bm_server V) {
 int bm_server_read_output(bm_server V, uint32_t session, uint8_t* dst, size_t len, uint64_t* frames_done) {
     if (!V || !dst) return set_err(BM_ERR_INVALID, "null argument");
     auto* S = V->find(session);
+    const bool failed = S ? S->failed
+                          : std::find(V->failed_ids.begin(), V->failed_ids.end(), session) != V->failed_ids.end();
+    if (failed)
+        return set_err(BM_ERR_TIMEOUT, "bm_server_read_output: session %u was dropped after a device error", session);
     if (!S) return set_err(BM_ERR_INVALID, "bm_server_read_output: no open session %u", session);
     if (len != S->out_len) return set_err(BM_ERR_INVALID, "length %zu != %u", len, S->out_len);
     if (S->out) std::memcpy(dst, S->out, len);
@@ -514,13 +662,14 @@ int bm_server_get_stats(bm_server V, bm_server_stats* st) {
     st->span_s = V->last_tick > V->first_tick ? V->last_tick - V->first_tick : 0;
     st->rebuild_s = V->rebuild_s;
     st->gpu_s = V->gpu_s;
-    st->admit_s = V->admit_s;
+    st->admit_s = V->admit_s.load();
     st->used_bytes = V->used;
     st->budget_bytes = V->budget;
     for (auto* S : V->sessions) {
         if (S->resident) st->resident++;
         else st->waiting++;
     }
+    st->failed = (uint32_t)V->failed_ids.size();
     if (!V->lat_ms.empty()) {
         std::vector<float> v = V->lat_ms;
         auto q = [&](double f) {
@@ -541,7 +690,8 @@ int bm_server_reset_stats(bm_server V) {
     if (!V) return set_err(BM_ERR_INVALID, "null server");
     V->lat_ms.clear();
     V->ticks = V->frames_cycled = V->rebuilds = 0;
-    V->syn_cycles = V->busy_s = V->first_tick = V->last_tick = V->rebuild_s = V->admit_s = V->gpu_s = 0;
+    V->syn_cycles = V->busy_s = V->first_tick = V->last_tick = V->rebuild_s = V->gpu_s = 0;
+    V->admit_s.store(0);
     return BM_OK;
 }
 

@@ -20,6 +20,8 @@
 // recompiles the gather offsets, so nothing from an earlier call is read.
 // Calls share the array: two calls whose work overlaps on the GPU (on
 // different streams, or from different threads, on one device) race on it.
+#include <cuda.h>
+
 #include <cstring>
 #include <mutex>
 
@@ -44,23 +46,63 @@ static __device__ __align__(256) unsigned char g_scratch[kScratchBytes];
 
 constexpr int kMaxDevices = 64;
 std::mutex g_mu;
-unsigned char* g_scratch_dev[kMaxDevices];   // device address of g_scratch, per device
+struct ScratchAddr {
+    unsigned char* ptr = nullptr;   // device address of g_scratch
+    unsigned long long ctx = 0;     // id of the context it was looked up in
+};
+ScratchAddr g_scratch_dev[kMaxDevices];   // per device
 
-// Device address of the array on `dev` (the current device). Looked up once
-// per device, on the first call made with that device current.
+// Id of the calling thread's current context (cuCtxGetId: unique for the
+// life of the process, so a context created after a device reset has a new
+// one), or 0 when there is none or the driver lacks the call. The driver
+// entry points are resolved through the runtime, so the library needs no
+// link against the driver library.
+unsigned long long current_ctx_id() {
+    using GetCurrent = CUresult (*)(CUcontext*);
+    using GetId = CUresult (*)(CUcontext, unsigned long long*);
+    static GetCurrent get_current = nullptr;
+    static GetId get_id = nullptr;
+    static bool resolved = false;
+    if (!resolved) {
+        void* a = nullptr;
+        void* b = nullptr;
+        cudaDriverEntryPointQueryResult qa{}, qb{};
+        if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &a, 12000, cudaEnableDefault, &qa) == cudaSuccess &&
+            cudaGetDriverEntryPointByVersion("cuCtxGetId", &b, 12000, cudaEnableDefault, &qb) == cudaSuccess &&
+            qa == cudaDriverEntryPointSuccess && qb == cudaDriverEntryPointSuccess) {
+            get_current = (GetCurrent)a;
+            get_id = (GetId)b;
+        }
+        cudaGetLastError();
+        resolved = true;
+    }
+    if (!get_current || !get_id) return 0;
+    CUcontext c = nullptr;
+    unsigned long long id = 0;
+    if (get_current(&c) != CUDA_SUCCESS || !c || get_id(c, &id) != CUDA_SUCCESS) return 0;
+    return id;
+}
+
+// Device address of the array on `dev` (the current device). Looked up on the
+// first call made with that device current, and again whenever the current
+// context is not the one the address was looked up in (a device reset
+// replaces the primary context and may move the array).
 int scratch_on(int dev, unsigned char** out) {
     if (dev < 0 || dev >= kMaxDevices)
         return set_err(BM_ERR_NO_DEVICE, "bm_tuft_cycle_static: device %d beyond the %d served", dev, kMaxDevices);
     std::lock_guard<std::mutex> g(g_mu);
-    if (!g_scratch_dev[dev]) {
+    ScratchAddr& S = g_scratch_dev[dev];
+    const unsigned long long ctx = current_ctx_id();
+    if (!S.ptr || !ctx || ctx != S.ctx) {
         void* p = nullptr;
         cudaError_t e = cudaGetSymbolAddress(&p, g_scratch);
         if (e != cudaSuccess || !p)
             return set_err(BM_ERR_CUDA, "bm_tuft_cycle_static: cudaGetSymbolAddress of the scratch array on device %d: %s",
                            dev, cudaGetErrorString(e));
-        g_scratch_dev[dev] = (unsigned char*)p;
+        S.ptr = (unsigned char*)p;
+        S.ctx = current_ctx_id();   // the lookup made the device's context current if none was
     }
-    *out = g_scratch_dev[dev];
+    *out = S.ptr;
     return BM_OK;
 }
 
@@ -77,7 +119,10 @@ __global__ void k_static_begin(unsigned char* scratch, const SliceTable tab, uns
     if (threadIdx.x == 0) {
         ctl->cycle = cycle;
         ctl->error = 0;
+        ctl->wait_us = 0;
+        ctl->stall_stage = 0;
         ctl->pad = 0;
+        ctl->host_err = nullptr;
     }
 }
 
@@ -107,15 +152,24 @@ extern "C" int bm_tuft_cycle_static(const bm_area_plan* plan, uint32_t layer, ui
                        "bm_tuft_cycle_static: tuft %u of layer %u has %llu synapses; the library-held scratch "
                        "serves at most %llu per call",
                        tuft, layer, (unsigned long long)n_syn, (unsigned long long)kMaxSyns);
+    // An error the caller's own earlier work left pending is reported, not
+    // cleared: the launches below are checked on their own.
+    cudaError_t e = cudaPeekAtLastError();
+    if (e != cudaSuccess)
+        return set_err(BM_ERR_CUDA, "bm_tuft_cycle_static: a CUDA error was pending before the call: %s",
+                       cudaGetErrorString(e));
     int dev = -1;
-    cudaError_t e = cudaGetDevice(&dev);
+    e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return set_err(BM_ERR_NO_DEVICE, "bm_tuft_cycle_static: no CUDA device (%s)", cudaGetErrorString(e));
     unsigned char* scratch = nullptr;
     int rc = scratch_on(dev, &scratch);
     if (rc != BM_OK) return rc;
 
+    if ((uintptr_t)slab & 255)
+        return set_err(BM_ERR_INVALID, "bm_tuft_cycle_static: the slab must be 256-byte aligned (as cudaMalloc returns)");
     FusedArea F;
     plan_fused_tuft(F, P, layer, tuft);
+    bind_fused_tuft(F, P, layer, tuft, (const uint8_t*)slab + P.axon_off);
     FusedTuft& FT = F.t[layer][tuft];
     if (!FT.ok)
         return set_err(BM_ERR_UNSUPPORTED,
@@ -131,7 +185,6 @@ extern "C" int bm_tuft_cycle_static(const bm_area_plan* plan, uint32_t layer, ui
     cudaStream_t s = (cudaStream_t)stream;
     AreaCtl* ctl = (AreaCtl*)(scratch + kCtlOff);
     const SliceRec* slices = (const SliceRec*)(scratch + kSlicesOff);
-    cudaGetLastError();
     k_static_begin<<<1, 256, 0, s>>>(scratch, tab, (unsigned long long)cycle);
     launch_compile_tuft(F, D, layer, tuft, ctl, s);
     launch_fused_tuft(F, (const uint8_t*)slab + P.axon_off, slices, D, layer, tuft, ctl, s);

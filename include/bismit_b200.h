@@ -434,9 +434,61 @@ int bm_area_slab_ptr(bm_area area, void** out);
 int bm_area_side_steps(bm_area area, uint32_t* n);
 int bm_area_sources_changed(bm_area area, uint32_t layer);
 
+/* One tract's delivery between two areas of a cortex cycled one area after
+ * another, as bismit's Cortex::cycle does (src/cortex/cortex.rs:99-119): the
+ * current axons of output `src_output` of `src` -- what its latest cycle
+ * wrote, read by CorticalArea::output into the thalamic tract,
+ * src/cortex/axon_space.rs:594-629 -- into input `dst_input` of `dst` at axon
+ * `dst_offset`, landing where AxonSpace::intake puts a tract frame
+ * (src/cortex/axon_space.rs:509-588; a filtered source's bytes into its
+ * chain's first buffer). Enqueued on dst's stream after the work already
+ * queued for src. A batch with tracts (bm_batch_connect) instead delivers
+ * every tract at the head of each cycle, from the previous cycle. */
+int bm_area_deliver_tract(bm_area src, uint32_t src_output, bm_area dst, uint32_t dst_input, uint64_t dst_offset);
+
 /* Sticky device-side error bits of the area (bit 0: a bounded wait inside a
- * kernel gave up). Synchronous; returns BM_ERR_TIMEOUT when any bit is set. */
+ * kernel gave up). Synchronous; returns BM_ERR_TIMEOUT when any bit is set.
+ * No reference counterpart (bismit panics on errors, src/cortex/cortex.rs:111).
+ * A cycle that ends with error bits set also copies them to host memory the
+ * library reads without synchronising: the area's (or a batch holding it)
+ * next cycling call then returns BM_ERR_TIMEOUT without enqueueing anything,
+ * until bm_area_clear_errors. */
 int bm_area_device_errors(bm_area area, uint32_t* bits);
+/* Clears the area's device error bits (after the caller restored a state it
+ * trusts, e.g. with bm_area_write_slab). Synchronous. */
+int bm_area_clear_errors(bm_area area);
+/* Limit, in microseconds, of every bounded wait inside the area's tuft
+ * kernels (0: the default, 2 s). A wait that runs out sets error bit 0, the
+ * kernel lets its own copies land and returns. Synchronous. */
+int bm_area_set_wait_limit(bm_area area, uint32_t us);
+/* Fault injection for tests of the give-up path: in every tiled tuft launch
+ * of the area (alone or batched), the copy lane of the block that takes the
+ * tuft's first tile withholds the `stage`-th shared-memory stage it issues
+ * from that tile on (counted from 1; 0 switches it off), so the consumers'
+ * bounded wait for it runs out. Nothing faults: every wait stays bounded.
+ * Synchronous. */
+int bm_area_inject_stall(bm_area area, uint32_t stage);
+
+/* How the fused path runs tuft `tuft` of data layer `layer` (no reference
+ * counterpart: bismit runs one kernel per stage). For tests and profiling,
+ * which form a workload exercises. All zero when the tuft takes the plain
+ * per-stage or per-cell kernels. Synchronous. */
+typedef struct bm_tuft_form {
+    uint32_t fused;            /* the fused tuft kernel runs it                        */
+    uint32_t tiled;            /* it gathers from a shared-memory axon footprint       */
+    uint32_t consumer;         /* compile-time specialised consumer shape (1..7), 0 =
+                                  the general one                                      */
+    uint32_t sources_outside;  /* a source lies outside the footprint: checked gathers */
+    uint32_t flags_foreign;    /* a flag byte has bits besides SYN_PREV_ACTIVE: flags
+                                  stream through and keep those bits                   */
+    uint32_t tile_w, tile_h;   /* cells per tile (tiled form)                          */
+    uint32_t stages;           /* shared-memory ring stages                            */
+    uint32_t grid;             /* persistent CTAs                                      */
+    uint32_t smem;             /* dynamic shared memory per CTA, bytes                 */
+    uint32_t footprint_tma;    /* 1: each tile's axon footprint arrives as one tensor
+                                  box load (else the consumer warps stage it)          */
+} bm_tuft_form;
+int bm_area_tuft_form(bm_area area, uint32_t layer, uint32_t tuft, bm_tuft_form* out);
 
 /* Per-kernel CUDA-event timing of subsequent cycles (0 = off). */
 int bm_area_set_profiling(bm_area area, int on);
@@ -544,8 +596,11 @@ int bm_batch_autotune(bm_batch batch, const char* cache_path, uint32_t* n_tuned)
  * tufts of at most 4,194,304 synapses (cells * syns_per_tft); larger tufts
  * get BM_ERR_INVALID, and tufts outside the fused kernel's shapes
  * BM_ERR_UNSUPPORTED. The first call on a device looks up the array's device
- * address (cudaGetSymbolAddress, which may load the module); make that first
- * call before any stream capture. Every call shares the array and leaves its
+ * address (cudaGetSymbolAddress, which may load the module), and so does the
+ * first call after the device's context was replaced (cudaDeviceReset); make
+ * those calls before any stream capture. An error already pending in the
+ * calling thread (cudaPeekAtLastError) is returned as BM_ERR_CUDA and left
+ * pending. Every call shares the array and leaves its
  * contents behind; the call re-initialises what it reads, but calls whose work
  * overlaps on the GPU (different streams or threads, same device) race on
  * it and must be serialised by the caller. Calls no cudaMalloc or cudaFree. */
@@ -559,10 +614,15 @@ int bm_tuft_cycle_static(const bm_area_plan* plan, uint32_t layer, uint32_t tuft
  * its resolved plan before anything is allocated), in FIFO order, and stays
  * resident until closed and drained. Each bm_server_tick cycles every
  * resident session that has a pending frame exactly once, all in one batch
- * (rebuilt only when that set changes), and meanwhile builds the areas of
- * newly admitted sessions on a second stream so their set-up overlaps the
- * running cycles. No counterpart in the reference, which cycles a fixed set
- * of areas (Cortex::cycle, src/cortex/cortex.rs:99-119). */
+ * (rebuilt only when that set changes). Admitted sessions' areas are built
+ * and grown by a thread the server owns, on a stream of their own, and join
+ * the first tick after they are ready, so no tick waits for a set-up (or a
+ * teardown, which that thread does too). A session whose area ends a cycle
+ * with device error bits (a bounded wait gave up) is dropped with its queued
+ * frames: the tick that finds it returns BM_ERR_TIMEOUT once, later ticks
+ * run the other sessions, and reading its output returns BM_ERR_TIMEOUT.
+ * No counterpart in the reference, which cycles a fixed set of areas
+ * (Cortex::cycle, src/cortex/cortex.rs:99-119). */
 typedef struct bm_server_s* bm_server;
 
 typedef struct bm_server_stats {
@@ -577,6 +637,7 @@ typedef struct bm_server_stats {
                                      session's previous frame done)              */
     uint64_t used_bytes, budget_bytes;
     uint32_t resident, waiting;
+    uint32_t failed;              /* sessions dropped after a device error       */
 } bm_server_stats;
 
 /* mem_budget 0: 90 % of the device memory free at creation. */
@@ -589,9 +650,14 @@ int bm_server_submit(bm_server server, uint32_t session, const uint8_t* frames, 
                      uint32_t n_frames);
 /* The session leaves once its submitted frames are cycled. */
 int bm_server_close(bm_server server, uint32_t session);
+/* Closes a session and discards its queued frames (frames already in a
+ * queued tick still complete). */
+int bm_server_cancel(bm_server server, uint32_t session);
 /* Queues one tick (*n_cycled, optional: sessions in it) and completes the
  * previous one: ticks are pipelined two deep, so a session's output and
- * frame count reflect the tick before the latest. */
+ * frame count reflect the tick before the latest. Returns at once with
+ * *n_cycled 0 when no resident session has a frame (sessions may still be
+ * being built). */
 int bm_server_tick(bm_server server, uint32_t* n_cycled);
 /* Completes every queued tick. */
 int bm_server_drain(bm_server server);

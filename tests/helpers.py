@@ -16,6 +16,10 @@ SCHEMES = {
     "testbed_retina": lambda: configs.testbed_area(retina=True),
     "retina": lambda: configs.retina_area(48, n_filters=2, src_depth=2),
     "retina_scaled": lambda: configs.retina_area(64, n_filters=3, src_side=32),
+    # The 256 x 256 workload's layer shapes on a 48 x 48 grid: spiny stellate
+    # 1 x 64, pyramidal depth 4 with proximal and distal 16 x 32 tufts at
+    # reach 6 (the specialised consumers of both layer kinds, in seconds).
+    "area_256_shape": lambda: configs.workload("area_256_shape")[:2],
 }
 
 
@@ -87,11 +91,16 @@ def digests(plan, slab):
     return {name: hashlib.sha256(slab[off:off + n].tobytes()).hexdigest()[:32] for name, off, n in buffers(plan)}
 
 
-def scramble(plan, slab, seed):
+def scramble(plan, slab, seed, clean_flags=False):
     """Overwrites the cycle state (not the synapse sources) with seeded values so
     every branch of the kernels is reached: energies at and above the restless
     and dark cutoffs, flags with unrelated bits set, strengths over the whole i8
-    range (including -128 and 127), prior synapse and tuft states."""
+    range (including -128 and 127), prior synapse and tuft states.
+
+    With clean_flags the synapse flags keep only SYN_PREV_ACTIVE (0x10), the
+    only bit bismit's kernels ever write (cl/syns.cl:23-33): the state real
+    runs are in, which the fused kernel serves with its specialised consumers
+    (foreign bits send it to the form that streams flags through)."""
     rng = np.random.default_rng([seed, 0x5C7A])
     for l in range(plan.n_layers):
         L = plan.layers[l]
@@ -127,14 +136,19 @@ def scramble(plan, slab, seed):
     ax = rng.integers(0, 256, int(plan.n_axons), dtype=np.uint8)
     ax[rng.random(int(plan.n_axons)) < 0.8] = 0
     slab[int(plan.axon_off):int(plan.axon_off) + int(plan.n_axons)] = ax
+    if clean_flags:
+        for l in range(plan.n_layers):
+            L = plan.layers[l]
+            off = int(L.buf_off[F.BUF["syn_flag_sets"]])
+            slab[off:off + int(L.n_syns)] &= 0x10
 
 
-def initial_slab(plan, grow_seed, scramble_seed=None, init_flags=0):
+def initial_slab(plan, grow_seed, scramble_seed=None, init_flags=0, clean_flags=False):
     import oracle
     slab = np.zeros(int(plan.slab_bytes), np.uint8)
     oracle.grow(plan, slab, grow_seed, init_flags)
     if scramble_seed is not None:
-        scramble(plan, slab, scramble_seed)
+        scramble(plan, slab, scramble_seed, clean_flags=clean_flags)
     return slab
 
 
@@ -142,3 +156,36 @@ def frames_for(plan, n, seed, active=0.05):
     if plan.n_inputs == 0:
         return None
     return configs.frames(n, int(plan.inputs[0].len), active, seed)
+
+
+def oracle_cortex_cycle(plans, slabs, tracts, ext_frame, cycle):
+    """One cycle of a multi-area cortex on the oracle with the batched path's
+    tract timing: every tract first delivers its source's output of the
+    previous cycle, the external frame goes into area 0's first input, then
+    each area cycles."""
+    import oracle
+    outs = [s[int(p.axon_off):].copy() for p, s in zip(plans, slabs)]
+    for (s, o, d, i, off, n) in tracts:
+        src = int(plans[s].outputs[o].axn_idz)
+        oracle.intake(plans[d], slabs[d], i, off, outs[s][src:src + n])
+    oracle.intake(plans[0], slabs[0], 0, 0, ext_frame)
+    for p, s in zip(plans, slabs):
+        oracle.run(p, s, None, 1, start_cycle=cycle)
+
+
+def oracle_cortex_cycle_in_order(plans, slabs, tracts, ext_frame, cycle):
+    """One cycle of a multi-area cortex on the oracle in bismit's own order
+    (Cortex::cycle, src/cortex/cortex.rs:99-119): area after area, each
+    taking its tracts' current outputs -- an earlier area's of this cycle, a
+    later area's of the previous one -- and area 0 its external frame, then
+    cycling."""
+    import oracle
+    for k, (p, s) in enumerate(zip(plans, slabs)):
+        for (sk, o, d, i, off, n) in tracts:
+            if d != k:
+                continue
+            src = int(plans[sk].axon_off) + int(plans[sk].outputs[o].axn_idz)
+            oracle.intake(p, s, i, off, slabs[sk][src:src + n].copy())
+        if k == 0:
+            oracle.intake(p, s, 0, 0, ext_frame)
+        oracle.run(p, s, None, 1, start_cycle=cycle)

@@ -92,7 +92,8 @@ def test_rnd_stream_is_host_computable():
 
 
 STRUCTS = ["bm_src_layer_desc", "bm_tuft_desc", "bm_input_src_desc", "bm_layer_desc", "bm_area_desc",
-           "bm_tuft_plan", "bm_ctrl_plan", "bm_layer_plan", "bm_io_plan", "bm_filter_chain_plan", "bm_area_plan"]
+           "bm_tuft_plan", "bm_ctrl_plan", "bm_layer_plan", "bm_io_plan", "bm_filter_chain_plan", "bm_area_plan",
+           "bm_tuft_form", "bm_server_stats"]
 
 
 def test_ctypes_structures_match_the_header(tmp_path):

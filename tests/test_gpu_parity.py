@@ -39,13 +39,20 @@ def test_growth_matches_oracle(ctx, scheme, flags):
     area.close()
 
 
-def _run_parity(ctx, scheme, kind, plain, cycles, scramble=True, active=0.05, start=0):
+def _run_parity(ctx, scheme, kind, plain, cycles, scramble=True, active=0.05, start=0, clean_flags=False,
+                consumers=None, footprint_tma=None):
     s = settings_for(kind, plain=plain)
     area = _area(ctx, scheme, s)
     plan = area.plan
-    slab = initial_slab(plan, 7, scramble_seed=11 if scramble else None)
+    slab = initial_slab(plan, 7, scramble_seed=11 if scramble else None, clean_flags=clean_flags)
     area.write_slab(slab)
     area.set_cycle(start)
+    if consumers is not None:
+        forms = [area.tuft_form(i, t) for i in range(plan.n_layers) for t in range(plan.layers[i].n_tufts)]
+        got = {f["consumer"] for f in forms}
+        assert set(consumers) <= got, got
+        if footprint_tma is not None:
+            assert any(f["footprint_tma"] for f in forms) == footprint_tma, forms
     fr = frames_for(plan, cycles, 5, active)
     ora = slab.copy()
     for k in range(cycles):
@@ -61,9 +68,31 @@ def _run_parity(ctx, scheme, kind, plain, cycles, scramble=True, active=0.05, st
 
 @pytest.mark.parametrize("plain", [True, False], ids=["plain", "fused"])
 @pytest.mark.parametrize("scheme", ["testbed", "mixed", "area_64", "area_48_deep", "smoother", "testbed_retina",
-                                    "retina", "retina_scaled"])
+                                    "retina", "retina_scaled", "area_256_shape"])
 def test_cycles_match_oracle(ctx, scheme, plain):
     _run_parity(ctx, scheme, "default", plain, cycles=6)
+
+
+# Specialised consumers each scheme's fused tufts reach once the flags are
+# clean: 1 x 32 and 1 x 64 spiny stellate cells (1, 2), pyramidal cells of
+# 8 x 32 and 16 x 32 synapses (5, 6); the mixed area's odd shapes mostly take
+# the general consumer.
+CLEAN_CONSUMERS = {"area_64": [1, 6], "area_48_deep": [1, 6], "area_256_shape": [2, 6], "testbed": [1],
+                   "smoother": [1, 5], "mixed": []}
+# Whether some tuft's footprint arrives as a tensor box: rows of a multiple of
+# 16 bytes (64, 48 columns) do; the 24- and 40-column areas take the
+# consumer-staged footprint.
+CLEAN_TMA = {"area_64": True, "area_48_deep": True, "area_256_shape": True, "testbed": False, "smoother": False,
+             "mixed": None}
+
+
+@pytest.mark.parametrize("scheme", sorted(CLEAN_CONSUMERS))
+def test_clean_flag_cycles_match_oracle(ctx, scheme):
+    """From scrambled states whose synapse flags carry only SYN_PREV_ACTIVE
+    (the only bit bismit writes, cl/syns.cl:23-33), as in real runs: the fused
+    path then serves its tufts with the compile-time specialised consumers."""
+    _run_parity(ctx, scheme, "default", False, cycles=6, clean_flags=True, consumers=CLEAN_CONSUMERS[scheme],
+                footprint_tma=CLEAN_TMA[scheme])
 
 
 @pytest.mark.parametrize("plain", [True, False], ids=["plain", "fused"])

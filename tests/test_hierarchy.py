@@ -5,9 +5,8 @@ tract timing (every tract carries its source's output of the previous cycle).
 import numpy as np
 import pytest
 
-import oracle
 from bismit_b200 import Cortex, configs, map as M, plan_of
-from helpers import diff_report, scramble
+from helpers import diff_report, oracle_cortex_cycle, oracle_cortex_cycle_in_order, scramble
 
 SIDES = (32, 48, 24)
 
@@ -21,16 +20,6 @@ def test_tract_routing_of_the_hierarchy():
     for (s, o, d, i, off, n) in tracts:
         assert n == int(plans[s].outputs[o].len) and off + n <= int(plans[d].inputs[i].len)
     assert external == [(0, 0, 0, SIDES[0] ** 2, "v0", "ganglion")]
-
-
-def _oracle_cycle(plans, slabs, tracts, ext_frame, cycle):
-    outs = [s[int(p.axon_off):].copy() for p, s in zip(plans, slabs)]
-    for (s, o, d, i, off, n) in tracts:
-        src = int(plans[s].outputs[o].axn_idz)
-        oracle.intake(plans[d], slabs[d], i, off, outs[s][src:src + n])
-    oracle.intake(plans[0], slabs[0], 0, 0, ext_frame)
-    for p, s in zip(plans, slabs):
-        oracle.run(p, s, None, 1, start_cycle=cycle)
 
 
 def _with_filters(lm, ar):
@@ -63,8 +52,65 @@ def test_hierarchy_matches_oracle(filters):
     for c in range(6):
         v1.write_input(fr[c])
         cx.cycle()
-        _oracle_cycle(plans, slabs, cx.tracts, fr[c], c)
+        oracle_cortex_cycle(plans, slabs, cx.tracts, fr[c], c)
         for k, n in enumerate(names):
             dev = cx.area(n).read_slab()
             assert np.array_equal(dev, slabs[k]), "cycle %d, %s:\n%s" % (c, n, diff_report(plans[k], dev, slabs[k]))
     cx.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("filters", [False, True], ids=["plain_inputs", "filtered_inputs"])
+def test_same_cycle_tracts_match_oracle(filters):
+    """bismit's own tract timing (Cortex::cycle cycles the areas in order,
+    src/cortex/cortex.rs:99-119): a feed-forward tract carries its source's
+    output of the same cycle, a feedback tract the previous cycle's; against
+    the oracle cycling the areas in the same order."""
+    from bismit_b200.cortex import SAME_CYCLE
+    lm, ar, names = configs.hierarchy(SIDES)
+    if filters:
+        _with_filters(lm, ar)
+    cx = Cortex.builder(lm, ar).ca_settings(configs.bench_settings()).seed(3).tract_timing(SAME_CYCLE).build()
+    assert cx.batch is None
+    plans = [cx.area(n).plan for n in names]
+    slabs = []
+    for k, n in enumerate(names):
+        s = cx.area(n).read_slab()
+        scramble(plans[k], s, 60 + k, clean_flags=True)
+        cx.area(n).write_slab(s)
+        cx.area(n).set_cycle(0)
+        slabs.append(s.copy())
+    fr = configs.frames(5, SIDES[0] ** 2, 0.02, 7)
+    v1 = cx.area("v1")
+    for c in range(5):
+        v1.write_input(fr[c])
+        cx.cycle()
+        oracle_cortex_cycle_in_order(plans, slabs, cx.tracts, fr[c], c)
+        for k, n in enumerate(names):
+            dev = cx.area(n).read_slab()
+            assert np.array_equal(dev, slabs[k]), "cycle %d, %s:\n%s" % (c, n, diff_report(plans[k], dev, slabs[k]))
+    cx.close()
+
+
+def test_same_cycle_timing_differs_from_previous_cycle():
+    """The two timings are different methods: on the oracle, the hierarchy's
+    second area ends a few cycles in a different state under each (so the
+    same-cycle test above could not pass by accident)."""
+    import oracle
+    from bismit_b200 import plan_of
+    lm, ar, names = configs.hierarchy(SIDES)
+    plans = [plan_of(M.area_desc(n, lm, ar, configs.bench_settings()), 1) for n in names]
+    tracts, _ext = M.area_tracts(lm, ar, names, plans)
+    base = []
+    for k, p in enumerate(plans):
+        s = np.zeros(int(p.slab_bytes), np.uint8)
+        oracle.grow(p, s, 1, 0)
+        scramble(p, s, 70 + k, clean_flags=True)
+        base.append(s)
+    a = [s.copy() for s in base]
+    b = [s.copy() for s in base]
+    fr = configs.frames(4, SIDES[0] ** 2, 0.05, 8)
+    for c in range(4):
+        oracle_cortex_cycle(plans, a, tracts, fr[c], c)
+        oracle_cortex_cycle_in_order(plans, b, tracts, fr[c], c)
+    assert not np.array_equal(a[1], b[1])

@@ -4,6 +4,8 @@ session's state after its last frame must be byte-identical to the same
 session run alone (tolerance: exact), and its outputs must be the alone
 run's outputs.
 """
+import time
+
 import numpy as np
 import pytest
 
@@ -35,6 +37,7 @@ def test_sessions_in_the_mix_match_sessions_alone():
     sid = {}
     final, outs = {}, {k: [] for k in range(len(SESSIONS))}
     tick = 0
+    deadline = time.monotonic() + 120
     while len(final) < len(SESSIONS):
         for k, s in enumerate(SESSIONS):
             if s[5] == tick:
@@ -53,7 +56,9 @@ def test_sessions_in_the_mix_match_sessions_alone():
         st = srv.stats()
         assert st["used_bytes"] <= budget
         tick += 1
-        assert tick < 200, "sessions never drained"
+        assert time.monotonic() < deadline, "sessions never drained"
+        if n == 0:
+            time.sleep(0.001)   # areas are being built off the tick path
     st = srv.stats()
     assert st["frames"] == sum(s[4] for s in SESSIONS)
     assert st["p99_ms"] >= st["p50_ms"] > 0
@@ -83,12 +88,74 @@ def test_admission_waits_for_memory():
     srv.submit(b, fr)
     srv.close_session(a)
     srv.close_session(b)
-    ticks = 0
+    deadline = time.monotonic() + 60
     while srv.stats()["frames"] < 4:
-        srv.tick()
+        if srv.tick() == 0:
+            time.sleep(0.001)   # areas are being built off the tick path
         st = srv.stats()
-        assert st["resident"] <= 1
-        ticks += 1
-        assert ticks < 20
+        assert st["resident"] <= 1 and st["used_bytes"] <= _footprint(p) + 1024
+        assert time.monotonic() < deadline
     srv.close()
+    ctx.close()
+
+
+@pytest.mark.gpu
+def test_a_failing_session_is_dropped_and_the_others_match_alone():
+    """A session whose area ends a cycle with device error bits (here a
+    bounded wait made to run out through the fault hook, with a 1 ms limit)
+    is dropped: one tick reports BM_ERR_TIMEOUT, reading its output reports
+    it too, and the other sessions finish with the bytes they have alone. A
+    cancelled session leaves with its queued frames discarded."""
+    import ctypes
+    from bismit_b200 import _ffi as F
+    ctx = cortex._Ctx(0)
+    shapes = [(48, 2, 16, 32), (64, 1, 8, 64), (40, 2, 8, 16), (32, 1, 16, 16)]
+    n_frames = 8
+    descs = [_desc(*s) for s in shapes]
+    plans = [plan_of(d, 300 + k) for k, d in enumerate(descs)]
+    frames = [configs.frames(n_frames, int(p.inputs[0].len), 0.03, 400 + k) for k, p in enumerate(plans)]
+    srv = cortex.Server(ctx, 0)
+    sid = [srv.open(d, 300 + k) for k, d in enumerate(descs)]
+    for k in range(len(sid)):
+        srv.submit(sid[k], frames[k])
+    FAIL, CANCEL = 1, 3
+    deadline = time.monotonic() + 120
+    while srv.stats()["frames"] < len(sid):   # every session resident and cycling
+        if srv.tick() == 0:
+            time.sleep(0.001)
+        assert time.monotonic() < deadline
+    h = ctypes.c_void_p()
+    F.check(srv.lib.bm_server_session_area(srv.h, sid[FAIL], ctypes.byref(h)))
+    F.check(srv.lib.bm_area_set_wait_limit(h, 1000))
+    F.check(srv.lib.bm_area_inject_stall(h, 1))
+    srv.cancel_session(sid[CANCEL])
+    reported = 0
+    final = {}
+    while len(final) < len(sid) - 2:
+        try:
+            srv.tick()
+        except F.BismitError as e:
+            assert e.code == F.BM_ERR_TIMEOUT and "dropped" in str(e)
+            reported += 1
+        for k in (0, 2):
+            if k in final:
+                continue
+            _out, done = srv.read_output(sid[k], int(plans[k].outputs[0].len))
+            if done == n_frames:
+                final[k] = srv.session_slab(sid[k], plans[k].slab_bytes)
+                srv.close_session(sid[k])
+        assert time.monotonic() < deadline
+    assert reported == 1
+    with pytest.raises(F.BismitError) as e:
+        srv.read_output(sid[FAIL], int(plans[FAIL].outputs[0].len))
+    assert e.value.code == F.BM_ERR_TIMEOUT
+    assert srv.stats()["failed"] == 1
+    srv.close()
+    for k in final:
+        a = cortex.CorticalArea(ctx, descs[k], 300 + k)
+        for c in range(n_frames):
+            a.write_input(frames[k][c])
+            a.cycle(1)
+        assert np.array_equal(a.read_slab(), final[k]), "session %d differs from its run alone" % k
+        a.close()
     ctx.close()

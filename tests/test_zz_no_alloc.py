@@ -53,7 +53,13 @@ def _static(lib, plan, li, t, slab_ptr, cycle, err_ptr, stream):
 
 
 @pytest.mark.gpu
-def test_static_tuft_cycle_matches_area_cycle():
+@pytest.mark.parametrize("flags", ["clean", "foreign"])
+def test_static_tuft_cycle_matches_area_cycle(flags):
+    """With clean flags (only SYN_PREV_ACTIVE, as in real runs) the calls run
+    the tiled kernel with its specialised consumers and the gather offsets in
+    the shared scratch; with foreign flag bits, the form that streams flags
+    through. Device free memory is unchanged across the calls after the
+    first."""
     import torch
 
     ctx = cortex._Ctx(0)
@@ -75,9 +81,15 @@ def test_static_tuft_cycle_matches_area_cycle():
     stream = torch.cuda.Stream(device=0)
 
     slab = a.read_slab()
-    scramble(plan, slab, 11)
+    scramble(plan, slab, 11, clean_flags=flags == "clean")
     a.write_slab(slab)
     a.set_cycle(0)
+    forms = [a.tuft_form(li, t) for t in tufts]
+    assert any(f["tiled"] for f in forms), forms
+    if flags == "clean":
+        assert all(not f["flags_foreign"] for f in forms) and any(f["consumer"] for f in forms), forms
+    else:
+        assert all(f["flags_foreign"] for f in forms if f["fused"]), forms
     fr = frames_for(plan, 2, 5, 0.05)
     for k, order in enumerate((tufts[::-1], tufts)):
         b.write_slab(a.read_slab())
@@ -87,10 +99,15 @@ def test_static_tuft_cycle_matches_area_cycle():
         before = b.read_slab()
         a.cycle(1)
         want = a.read_slab()
+        torch.cuda.synchronize()
+        stream.wait_stream(torch.cuda.current_stream())   # err's fill comes first
+        free0 = torch.cuda.mem_get_info(0)[0]
         for j, t in enumerate(order):
             rc = _static(lib, plan, li, t, ptr.value, k, err.data_ptr() + 4 * j, stream.cuda_stream)
             assert rc == F.BM_OK, lib.bm_last_error().decode()
         stream.synchronize()
+        if k > 0:   # the first call on the device may load the library's module
+            assert torch.cuda.mem_get_info(0)[0] == free0
         got = b.read_slab()
         assert err.tolist() == [0] * len(tufts)
         written = np.zeros(got.size, bool)
