@@ -124,6 +124,16 @@ void fuse_steps(const bm_area_s* A, std::vector<Step>& v) {
     std::vector<Step> out;
     for (size_t k = 0; k < v.size(); k++) {
         const Step& s = v[k];
+        // A spiny stellate tuft whose cells have one dendrite, taken by the
+        // fused kernel, also runs the ssc_cycle that follows it (arg 1): the
+        // soma is that dendrite's state, known in the same launch.
+        if (s.kind == ST_TUFT && k + 1 < v.size() && v[k + 1].kind == ST_SSC_CYCLE && v[k + 1].layer == s.layer &&
+            P.layers[s.layer].kind == BM_LYR_SPINY_STELLATE && P.layers[s.layer].n_tufts == 1 &&
+            P.layers[s.layer].tufts[0].dens_per_tft == 1 && A->fused.t[s.layer][s.idx].ok) {
+            out.push_back({ST_TUFT, s.layer, s.idx, 1});
+            k++;
+            continue;
+        }
         if (s.kind == ST_INHIB_SIMPLE && layer_plain(P, s.layer) &&
             P.layers[s.layer].kind == BM_LYR_SPINY_STELLATE) {
             const bool learn = k + 1 < v.size() && v[k + 1].kind == ST_SSC_MTP && v[k + 1].layer == s.layer;
@@ -209,7 +219,8 @@ void bm::exec_step(bm_area_s* A, const Step& st, cudaStream_t s) {
     switch (st.kind) {
     case ST_TUFT:
         if (A->fused.t[i][x].ok) {
-            run(K_FUSED_TUFT, [&] { launch_fused_tuft(A->fused, A->axns(), A->slices, D, i, x, A->ctl, s); });
+            run(K_FUSED_TUFT,
+                [&] { launch_fused_tuft(A->fused, A->axns(), A->slices, D, i, x, A->ctl, s, (st.arg & 1) != 0); });
         } else {
             run(K_TUFT_CELLS, [&] { launch_tuft_cells(A->axns(), A->slices, D, x, A->ctl, s); });
         }
@@ -312,6 +323,7 @@ bm::StepAccess bm::step_access(const bm_area_s* A, const Step& st, int t) {
         if ((A->foreign_src[i] >> tt) & 1) a.ax_r.set();   // sources anywhere: any slice
         else tuft_sources(P, i, tt, a.ax_r);
         a.tf_r = a.tf_w = tuft_bit(i, tt);
+        if (st.arg & 1) a.ce_r = a.ce_w = 1u << i;          // with the folded ssc_cycle
         break;
     }
     case ST_TUFTS_PLAIN:

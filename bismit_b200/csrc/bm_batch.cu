@@ -366,7 +366,8 @@ int build_fused(bm_batch_s::StepPlan& p) {
     std::vector<FusedJob> jobs;
     for (auto& [A, t] : p.tufts) {
         if (!A->fused.t[p.st.layer][t].ok) return BM_OK;
-        jobs.push_back({&A->fused, &A->dl[p.st.layer], A->axns(), A->slices, A->ctl, p.st.layer, t});
+        jobs.push_back({&A->fused, &A->dl[p.st.layer], A->axns(), A->slices, A->ctl, p.st.layer, t,
+                        (p.st.arg & 1) != 0});
     }
     int rc = prepare_fused_batch(p.fb, jobs);
     if (rc != BM_OK) return rc;
@@ -454,7 +455,8 @@ int merge_tuft_steps(bm_batch_s* B) {
     std::vector<bm_batch_s::StepPlan> out;
     for (auto& p : B->plan) {
         if (!out.empty() && p.form == bm_batch_s::F_FUSED && out.back().form == bm_batch_s::F_FUSED &&
-            p.st.kind == ST_TUFT && out.back().st.kind == ST_TUFT && p.st.layer == out.back().st.layer) {
+            p.st.kind == ST_TUFT && out.back().st.kind == ST_TUFT && p.st.layer == out.back().st.layer &&
+            p.st.arg == out.back().st.arg) {
             auto& q = out.back();
             q.tufts.insert(q.tufts.end(), p.tufts.begin(), p.tufts.end());
             for (bm_area A : p.areas)

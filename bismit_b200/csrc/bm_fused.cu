@@ -74,6 +74,7 @@ struct FusedTuftArgs {
     uint8_t* den_act;       // tuft-relative dendrite arrays
     uint8_t* den_raw;
     uint8_t* den_st;
+    uint8_t* cel_en;        // spiny stellate cell energies (ssc_soma)
     uint8_t* t_pid;         // tuft-relative cell-tuft arrays (pyramidal)
     uint8_t* t_praw;
     uint8_t* t_pst;
@@ -113,6 +114,7 @@ struct FusedTuftArgs {
     uint32_t win_bytes;                 // bytes per window
     uint32_t geom;                      // specialised consumer for this shape (0: the general one)
     uint32_t fp_tma;                    // the footprint comes from a tensor box load (else consumers stage it)
+    uint32_t ssc_soma;                  // also run ssc_cycle (spiny stellate cells of one dendrite)
     uint32_t fp_bytes;                  // bytes of that box (nrec * frows * fw)
 };
 static_assert(offsetof(FusedTuftArgs, tmap) == 0 && alignof(FusedTuftArgs) >= 64,
@@ -242,6 +244,18 @@ __device__ __forceinline__ uint32_t nz_bits(uint32_t x) {
     return (((x & 0x7F7F7F7Fu) + 0x7F7F7F7Fu) | x) & 0x80808080u;
 }
 
+// ssc_cycle (cl/bismit.cl:849-884) folded into the spiny stellate tuft stage
+// for cells of one dendrite, whose soma state is that dendrite's state: from
+// cell c's energy and the dendrite state just computed, writes the energy and
+// returns the soma state.
+__device__ __forceinline__ uint32_t ssc_soma(uint8_t* en, uint32_t c, uint32_t energy, uint32_t state) {
+    const int active = state != 0;
+    const int restless = (energy > 191) & active;
+    const int dark = energy == 255;
+    en[c] = (uint8_t)((dark | restless) ? energy - 64 : energy);
+    return min(state + (uint32_t)restless * 255u + (uint32_t)dark * 255u, 255u);
+}
+
 __device__ __forceinline__ uint8_t gather_general(const FusedTuftArgs& A, uint32_t slc, uint32_t v, uint32_t u,
                                                   int vo, int uo) {
     bool safe;
@@ -314,6 +328,7 @@ __device__ __forceinline__ void finish_chunk(const FusedTuftArgs& A, const uint4
         d_raw = min(raw >> 4, 255u);
         d_st = min(s2 >> 4, 255u);
         A.den_raw[den] = (uint8_t)d_raw;
+        if (!TUFT && A.ssc_soma) d_st = ssc_soma(A.cel_en, den, A.cel_en[den], d_st);
         A.den_st[den] = (uint8_t)d_st;
     }
     if (TUFT) {
@@ -707,9 +722,12 @@ __device__ __forceinline__ void stage_fast(const FusedTuftArgs& A, const TileGeo
     const bool on = off < G.syn_end;
     const uint8_t* wd = sb + 4 * SB;
     const uint32_t f = (uint32_t)lane & (LPC - 1);
-    uint32_t act0 = 0, cur = 0;
+    uint32_t act0 = 0, cur = 0, en0 = 0;
     if (on) {
         if ((lane & (LPD - 1)) == 0) act0 = wd[(off >> SPD_L2) - ((pos >> SPD_L2) & ~15u)];
+        // The cell's energy for the folded ssc_cycle, loaded before the
+        // gathers so its latency overlaps them.
+        if (!TUFT && A.ssc_soma && (lane & (LPD - 1)) == 0) en0 = A.cel_en[off >> SPD_L2];
         if (TUFT) {
             const uint32_t ci = (off >> S_L2) - ((pos >> S_L2) & ~15u);
             if (LPC >= 8) {
@@ -761,6 +779,7 @@ __device__ __forceinline__ void stage_fast(const FusedTuftArgs& A, const TileGeo
         d_raw = min(raw >> 4, 255u);
         d_st = min(s2 >> 4, 255u);
         A.den_raw[den] = (uint8_t)d_raw;
+        if (!TUFT && A.ssc_soma) d_st = ssc_soma(A.cel_en, den, en0, d_st);
         A.den_st[den] = (uint8_t)d_st;
     }
     if (TUFT) {
@@ -1631,9 +1650,10 @@ void launch_verify_tufts(const FusedArea& F, const DevLayer& L, uint32_t layer, 
 
 namespace {
 
-// The kernel arguments of tuft t of data layer `layer`.
+// The kernel arguments of tuft t of data layer `layer` (with ssc_cycle folded
+// in when `ssc_soma`).
 void make_args(FusedTuftArgs& A, const FusedArea& F, const uint8_t* axns, const SliceRec* slices, const DevLayer& L,
-               uint32_t layer, uint32_t t, AreaCtl* ctl) {
+               uint32_t layer, uint32_t t, AreaCtl* ctl, bool ssc_soma) {
     const DevTuft& T = L.tft[t];
     const FusedTuft& FT = F.t[layer][t];
     std::memset(&A, 0, sizeof A);
@@ -1650,6 +1670,8 @@ void make_args(FusedTuftArgs& A, const FusedArea& F, const uint8_t* axns, const 
     A.den_act = L.buf[BM_BUF_DEN_ACTIVITIES] + T.den_idz;
     A.den_raw = L.buf[BM_BUF_DEN_STATES_RAW] + T.den_idz;
     A.den_st = L.buf[BM_BUF_DEN_STATES] + T.den_idz;
+    A.cel_en = L.buf[BM_BUF_CEL_ENERGIES];
+    A.ssc_soma = ssc_soma && L.kind == BM_LYR_SPINY_STELLATE && T.dpt == 1 && T.den_idz == 0;
     const bool tuft = L.kind == BM_LYR_PYRAMIDAL;
     if (tuft) {
         A.t_pid = L.buf[BM_BUF_TFT_PREV_BEST_DEN_IDS] + T.cel_idz;
@@ -1717,10 +1739,10 @@ void make_args(FusedTuftArgs& A, const FusedArea& F, const uint8_t* axns, const 
 }  // namespace
 
 void launch_fused_tuft(const FusedArea& F, const uint8_t* axns, const SliceRec* slices, const DevLayer& L,
-                       uint32_t layer, uint32_t t, AreaCtl* ctl, cudaStream_t s) {
+                       uint32_t layer, uint32_t t, AreaCtl* ctl, cudaStream_t s, bool ssc_soma) {
     const FusedTuft& FT = F.t[layer][t];
     FusedTuftArgs A;
-    make_args(A, F, axns, slices, L, layer, t, ctl);
+    make_args(A, F, axns, slices, L, layer, t, ctl, ssc_soma);
     const bool tuft = L.kind == BM_LYR_PYRAMIDAL;
     if (FT.tiled) {
         auto kern = tuft ? k_fused_tuft_tma<true> : k_fused_tuft_tma<false>;
@@ -1790,7 +1812,7 @@ int prepare_fused_batch(FusedBatch& B, const std::vector<FusedJob>& jobs) {
             uint32_t total = 0;
             for (size_t j = 0; j < n; j++) {
                 const FusedJob& J = *cls[j0 + j];
-                make_args(P->jobs[j], *J.F, J.axns, J.slices, *J.L, J.layer, J.t, J.ctl);
+                make_args(P->jobs[j], *J.F, J.axns, J.slices, *J.L, J.layer, J.t, J.ctl, J.ssc_soma);
                 P->jobs[j].nst = nst;
                 P->jobs[j].stage_stride = stride;
                 P->jobs[j].ring_off = (uint32_t)ring_off;

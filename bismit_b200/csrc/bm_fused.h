@@ -71,8 +71,10 @@ uint32_t consumer_shape(const FusedTuft& FT, uint32_t spt, uint32_t spd, bool py
 GatherGeo gather_geo(const FusedArea& F, const bm_area_plan& P, uint32_t layer, uint32_t t);
 // Synapse flags + synapse cycle + dendrite cycle (+ tuft cycle for pyramidal
 // layers) of one tuft in one launch.
+// With ssc_soma (a spiny stellate layer whose cells have one dendrite),
+// ssc_cycle runs in the same launch (the step that follows the tuft's).
 void launch_fused_tuft(const FusedArea& F, const uint8_t* axns, const SliceRec* slices, const DevLayer& L,
-                       uint32_t layer, uint32_t t, AreaCtl* ctl, cudaStream_t s);
+                       uint32_t layer, uint32_t t, AreaCtl* ctl, cudaStream_t s, bool ssc_soma = false);
 // Recomputes AreaCtl::tuft_status for the fused tufts of a layer (after its
 // synapse sources or flags were written by the caller).
 void launch_verify_tufts(const FusedArea& F, const DevLayer& L, uint32_t layer, AreaCtl* ctl, cudaStream_t s);
@@ -87,6 +89,7 @@ struct FusedJob {
     const SliceRec* slices;
     AreaCtl* ctl;
     uint32_t layer, t;   // the tuft: data layer index and tuft index
+    bool ssc_soma;       // ssc_cycle folded in (see launch_fused_tuft)
 };
 struct FusedBatch {
     bool ok = false;             // every job is tiled and the ring fits: batched launches serve them all
