@@ -229,6 +229,7 @@ def lib():
         "bm_encode_images": (C.c_int, [vp, vp, u32, u32, u32, C.c_float, vp, u64, u32, u32]),
         "bm_encode_hex_mold": (C.c_int, [vp, C.c_int32, u32, u32, vp, u32, u32]),
         "bm_encode_scalar": (C.c_int, [vp, vp, u32, C.c_float, C.c_float, u64, vp, u64, u32, u32]),
+        "bm_encode_scalar_glyph": (C.c_int, [vp, vp, u32, C.c_float, C.c_float, vp, u64, u32, u32]),
         "bm_sdr_writer_create": (C.c_int, [vp, C.c_float, C.c_float, C.c_float, u32, u32, u64, P(vp)]),
         "bm_sdr_writer_destroy": (C.c_int, [vp]),
         "bm_sdr_writer_info": (C.c_int, [vp, P(u32), P(u32), P(u32)]),

@@ -183,6 +183,32 @@ __global__ void k_encode_scalar(const __grid_constant__ ScalarArgs A, uint8_t* _
     }
 }
 
+// ---------------------------------------------------------- scalar glyph --
+
+struct GlyphArgs {
+    uint32_t n;
+    int32_t radius;
+    uint16_t cv[kMaxEncodeValues], cu[kMaxEncodeValues];   // each frame's hexagon center
+};
+
+// One block per frame (ScalarGlyphWriter::encode, src/encode/write/
+// scalar_glyph_writer.rs:69-151): the frame is cleared, then the hexagon of
+// radius `radius` around the frame's center is set to 127.
+__global__ void k_encode_glyph(const __grid_constant__ GlyphArgs A, uint8_t* __restrict__ frames, uint64_t stride,
+                               uint32_t v_size, uint32_t u_size) {
+    const uint32_t f = blockIdx.x;
+    uint8_t* frame = frames + f * stride;
+    const uint32_t len = v_size * u_size;
+    for (uint32_t i = threadIdx.x; i < len; i += blockDim.x) frame[i] = 0;
+    __syncthreads();
+    const int r = A.radius, side = 2 * r + 1, cv = A.cv[f], cu = A.cu[f];
+    for (int k = threadIdx.x; k < side * side; k += blockDim.x) {
+        const int v = -r + k / side, u = -r + k % side;
+        if (u < max(-r, -v - r) || u > min(r, -v + r)) continue;
+        frame[(uint32_t)((v + cv) * (int)u_size + u + cu)] = 127;
+    }
+}
+
 // ------------------------------------------------------------ SDR writer --
 
 struct SdrArgs {
@@ -295,6 +321,65 @@ int bm_encode_scalar(bm_ctx ctx, const float* vals, uint32_t n, float lo, float 
         k_encode_scalar<<<n, 256, 0, ctx->stream()>>>(*A, frames, frame_stride, v_size, u_size);
         const cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) rc = cuda_err(e, "encode_scalar");
+    }
+    delete A;
+    return rc;
+}
+
+int bm_encode_scalar_glyph(bm_ctx ctx, const float* vals, uint32_t n, float lo, float hi, uint8_t* frames,
+                           uint64_t frame_stride, uint32_t v_size, uint32_t u_size) {
+    if (!ctx || (n && (!vals || !frames))) return set_err(BM_ERR_INVALID, "null argument");
+    if (n > kMaxEncodeValues) return set_err(BM_ERR_INVALID, "scalar glyph: at most %u values per call", kMaxEncodeValues);
+    if (v_size < 8 || u_size < 8 || v_size > 0xFFFF || u_size > 0xFFFF)
+        return set_err(BM_ERR_INVALID,
+                       "ScalarGlyphWriter::new(): Tract frame too small. Side lengths must each be greater than 8.");
+    if (frame_stride < (uint64_t)v_size * u_size) return set_err(BM_ERR_INVALID, "scalar glyph: frame stride too small");
+    if (!(lo <= hi)) return set_err(BM_ERR_INVALID, "ScalarGlyphWriter::new(): empty value range");
+    // ScalarGlyphWriter::new (scalar_glyph_writer.rs:25-67).
+    const uint32_t radius = (v_size + u_size) / 32;
+    const uint32_t margin = radius + (radius + 1) + 1;
+    const uint32_t ttv = v_size - margin * 2 - 1, ttu = u_size - margin * 2 - 1;
+    const uint32_t total = ttv * 2 + ttu * 2;
+    const uint32_t side0 = ttu, side1 = ttu + ttv, side2 = 2 * ttu + ttv, side3 = total;
+    volatile float span = hi - lo;
+    GlyphArgs* A = new (std::nothrow) GlyphArgs;
+    if (!A) return set_err(BM_ERR_OOM, "host allocation failed");
+    std::memset(A, 0, sizeof *A);
+    A->n = n;
+    A->radius = (int32_t)radius;
+    for (uint32_t k = 0; k < n; k++) {
+        const float val = vals[k];
+        if (!(val >= lo && val <= hi)) {
+            delete A;
+            return set_err(BM_ERR_INVALID,
+                           "Unable to encode scalar value: '%g'. The value is outside of the allowed range: '(%g, %g)'.",
+                           (double)val, (double)lo, (double)hi);
+        }
+        // f32 arithmetic as the reference's; `as u32` saturates (NaN -> 0).
+        volatile float d = val - lo;
+        volatile float pct = d / span;
+        volatile float t = pct * (float)total;
+        const float fl = std::floor((float)t);
+        const uint32_t tile = !(fl > 0.0f) ? 0u : fl >= 4294967295.0f ? 0xFFFFFFFFu : (uint32_t)fl;
+        uint32_t cv, cu;
+        if (tile < side0) { cv = margin; cu = margin + tile; }
+        else if (tile < side1) { cv = margin + (tile - side0); cu = margin + ttu; }
+        else if (tile < side2) { cv = margin + ttv; cu = (margin + ttu) - (tile - side1); }
+        else if (tile < side3) { cv = (margin + ttv) - (tile - side2); cu = margin; }
+        else if (tile == total) { cv = margin; cu = margin; }
+        else {
+            delete A;
+            return set_err(BM_ERR_INVALID, "ScalarGlyphWriter::encode: value %g maps past the track", (double)val);
+        }
+        A->cv[k] = (uint16_t)cv;
+        A->cu[k] = (uint16_t)cu;
+    }
+    int rc = BM_OK;
+    if (n) {
+        DevGuard g(ctx->device);
+        k_encode_glyph<<<n, 256, 0, ctx->stream()>>>(*A, frames, frame_stride, v_size, u_size);
+        const cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) rc = cuda_err(e, "scalar glyph");
     }
     delete A;
     return rc;

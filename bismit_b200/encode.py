@@ -12,7 +12,12 @@ bm_area_cycle_frames_device / bm_batch_cycle_frames_device.
     encode_2d_image   src/encode/mod.rs:66-93
     encode_hex_mold_scaled, HexMoldTest   src/encode/write/mod.rs:190-217, src/encode/hex_mold_test.rs
     encode_scalar     src/encode/write/mod.rs:28-172
+    ReversoScalarSequence                src/encode/reverso_scalar_sequence.rs
+    ScalarGlyphWriter, ScalarSequence, VectorEncoder
+                      src/encode/write/scalar_glyph_writer.rs, src/encode/scalar_sequence.rs,
+                      src/encode/vector_encoder.rs
     ScalarSdrWriter, ScalarSdrGradiant    src/encode/write/scalar_sdr_writer.rs, src/encode/scalar_sdr_gradiant.rs
+    GlyphBuckets, GlyphSequences          src/encode/glyph_buckets.rs, src/encode/glyph_sequences.rs
 
 Random bytes and waypoint indices, entropy-seeded in the reference, come
 from a seeded stream (`seed`).
@@ -251,3 +256,226 @@ class ScalarSdrGradiant:
 
     def write_into(self, frame):
         self.writer.encode([self.next], frame)
+
+
+class ReversoScalarSequence:
+    """ReversoScalarSequence (src/encode/reverso_scalar_sequence.rs): a value
+    stepping by `incr` through [lo, hi), wrapping to lo; layer 0 gets
+    encode_scalar(next), layer 1 encode_scalar(hi - next). Values are f32,
+    as for T = f32."""
+
+    def __init__(self, ctx, val_range, incr, tract_dims, seed=0):
+        self.ctx = ctx
+        self.range = (np.float32(val_range[0]), np.float32(val_range[1]))
+        self.next = self.range[0]
+        self.incr = np.float32(incr)
+        self.tract_dims = tuple(tract_dims)
+        self.seed = seed
+
+    def increment_frame(self):
+        self.next = np.float32(self.next + self.incr)
+        if self.next >= self.range[1]:
+            self.next = self.range[0]
+
+    cycle_next = increment_frame
+
+    def write_into(self, frame, layer):
+        """Encodes into `frame` (device) for layer 0 or 1 (the reference
+        panics on a third)."""
+        if layer == 0:
+            v = self.next
+        elif layer == 1:
+            v = np.float32(self.range[1] - self.next)
+        else:
+            raise ValueError("ReversoScalarSequence::write_into(): Too many layers!")
+        encode_scalar(self.ctx, [v], (float(self.range[0]), float(self.range[1])), self.tract_dims, frame, self.seed)
+
+
+def encode_scalar_glyph(ctx, vals, val_range, tract_dims, frames, frame_stride=None):
+    """ScalarGlyphWriter::encode for each value (host floats) into frames
+    (device), one frame per value."""
+    v_size, u_size = tract_dims
+    a = np.ascontiguousarray(vals, dtype=np.float32)
+    stride = v_size * u_size if frame_stride is None else frame_stride
+    F.check(F.lib().bm_encode_scalar_glyph(ctx.h, a.ctypes.data_as(C.c_void_p), a.size, C.c_float(val_range[0]),
+                                           C.c_float(val_range[1]), _ptr(frames), stride, v_size, u_size))
+
+
+class ScalarGlyphWriter:
+    """ScalarGlyphWriter::new(val_range, tract_dims) and ::encode
+    (src/encode/write/scalar_glyph_writer.rs:25-151)."""
+
+    def __init__(self, ctx, val_range, tract_dims):
+        if tract_dims[0] < 8 or tract_dims[1] < 8:
+            raise ValueError("ScalarGlyphWriter::new(): Tract frame too small. Side lengths must each be "
+                             "greater than 8.")
+        if not val_range[0] <= val_range[1]:
+            raise ValueError("ScalarGlyphWriter::new(): empty value range")
+        self.ctx = ctx
+        self.val_range = (float(val_range[0]), float(val_range[1]))
+        self.tract_dims = tuple(tract_dims)
+
+    def encode(self, vals, frames, frame_stride=None):
+        encode_scalar_glyph(self.ctx, np.atleast_1d(vals), self.val_range, self.tract_dims, frames, frame_stride)
+
+
+class ScalarSequence:
+    """ScalarSequence (src/encode/scalar_sequence.rs): a value stepping by
+    `incr` through [lo, hi), wrapping to lo, written by a ScalarGlyphWriter."""
+
+    def __init__(self, ctx, val_range, incr, tract_dims):
+        self.range = (np.float32(val_range[0]), np.float32(val_range[1]))
+        self.next = self.range[0]
+        self.incr = np.float32(incr)
+        self.writer = ScalarGlyphWriter(ctx, val_range, tract_dims)
+
+    def increment_frame(self):
+        self.next = np.float32(self.next + self.incr)
+        if self.next >= self.range[1]:
+            self.next = self.range[0]
+
+    cycle_next = increment_frame
+
+    def write_into(self, frame):
+        self.writer.encode([self.next], frame)
+
+
+class VectorEncoder:
+    """VectorEncoder (src/encode/vector_encoder.rs): one value per layer, each
+    in its own range, each written by its layer's ScalarGlyphWriter.
+    `values` is the external frame the caller fills (ext_frame_mut)."""
+
+    def __init__(self, ctx, ranges, tract_dims):
+        if len(ranges) != len(tract_dims):
+            raise ValueError("VectorEncoder::new(): Range list length ('%d') and tract count ('%d') are not equal."
+                             % (len(ranges), len(tract_dims)))
+        self.ctx = ctx
+        self.tract_dims = [tuple(t) for t in tract_dims]
+        self.set_ranges(ranges)
+
+    def set_ranges(self, ranges):
+        """Resets the ranges and the number of scalars encoded (values to 0)."""
+        if len(ranges) > len(self.tract_dims):
+            raise ValueError("VectorEncoder::set_ranges(): Too many ranges provided ('%d'/'%d')."
+                             % (len(ranges), len(self.tract_dims)))
+        self.ranges = [tuple(r) for r in ranges]
+        self.writers = [ScalarGlyphWriter(self.ctx, r, t) for r, t in zip(self.ranges, self.tract_dims)]
+        self.values = np.zeros(len(self.ranges), np.float32)
+
+    def write_into(self, frame, layer):
+        """Layer `layer`'s value into `frame` (device); a layer past the
+        ranges set writes nothing, as in the reference."""
+        if layer >= len(self.tract_dims):
+            raise ValueError("VectorEncoder::write_into(): No layer %d" % layer)
+        if layer < len(self.writers):
+            self.writers[layer].encode([self.values[layer]], frame)
+
+    def cycle_next(self):
+        pass
+
+
+class GlyphBuckets:
+    """GlyphBuckets (src/encode/glyph_buckets.rs): the images of an idx image
+    file sorted into one bucket per label (10), and a cursor per bucket that
+    cycles through its images."""
+
+    BUCKET_COUNT = 10
+
+    def __init__(self, label_file, image_file):
+        labels = label_file if isinstance(label_file, IdxData) else IdxData(label_file)
+        images = image_file if isinstance(image_file, IdxData) else IdxData(image_file)
+        if len(images.dims) != 3:
+            raise ValueError("GlyphBuckets::new(): Source idx file must have three dimensions.")
+        if images.dims[0] != labels.dims[0]:
+            raise ValueError("GlyphBuckets::new(): The images file must contain the same number of elements as "
+                             "the labels file.")
+        self.glyph_dims = (images.dims[1], images.dims[2])
+        n = self.glyph_len()
+        imgs = images.data.reshape(images.dims[0], n)
+        lab = labels.data[:images.dims[0]]
+        if lab.size and int(lab.max()) > self.BUCKET_COUNT:
+            raise ValueError("GlyphBuckets::new(): label exceeds bucket count (%d)." % self.BUCKET_COUNT)
+        # A label equal to the bucket count passes the reference's assert and
+        # then indexes past its buckets.
+        if lab.size and int(lab.max()) == self.BUCKET_COUNT:
+            raise ValueError("GlyphBuckets::new(): label %d has no bucket" % self.BUCKET_COUNT)
+        self.buckets = [imgs[lab == b].reshape(-1) for b in range(self.BUCKET_COUNT)]
+        self.cursors = [0] * self.BUCKET_COUNT
+
+    def glyph_len(self):
+        return self.glyph_dims[0] * self.glyph_dims[1]
+
+    def count(self):
+        return len(self.buckets)
+
+    def next_glyph(self, bucket_id):
+        """The image under bucket_id's cursor; the cursor moves on (wrapping).
+        An empty bucket is refused (the reference panics slicing it)."""
+        if not 0 <= bucket_id < len(self.buckets):
+            raise ValueError("GlyphBuckets::next_glyph(): bucket_id (%d) exceeds bucket count (%d)."
+                             % (bucket_id, len(self.buckets)))
+        b = self.buckets[bucket_id]
+        if b.size == 0:
+            raise ValueError("GlyphBuckets::next_glyph(): bucket %d holds no glyph" % bucket_id)
+        z = self.cursors[bucket_id]
+        g = b[z:z + self.glyph_len()]
+        z += self.glyph_len()
+        self.cursors[bucket_id] = 0 if z == b.size else z
+        return g
+
+
+class GlyphSequences:
+    """GlyphSequences (src/encode/glyph_sequences.rs): `seq_count` sequences
+    of bucket ids, lengths uniform in seq_lens (inclusive), drawn from a
+    seeded stream (the reference's is entropy-seeded); a cursor walks them.
+    The image layer gets the next glyph of the cursor's bucket through
+    encode_2d_image; the value layer (dims 1 x hrz_dims) gets idx & 0xFF.
+    Every write draws a glyph from the bucket, as the reference's write_into
+    does for either layer."""
+
+    def __init__(self, ctx, seq_lens, seq_count, scale, hrz_dims, img_layer_dims, label_file, image_file, seed=0):
+        if seq_lens[1] < seq_lens[0]:
+            raise ValueError("GlyphSequences::new(): Sequence length range ('seq_lens') invalid. High end must at "
+                             "least be equal to low end: '%r'." % (tuple(seq_lens),))
+        self.ctx = ctx
+        self.buckets = GlyphBuckets(label_file, image_file)
+        self.scale = float(scale)
+        self.img_layer_dims = tuple(img_layer_dims)
+        self.val_layer_dims = (int(hrz_dims[0]), int(hrz_dims[1]))
+        rng = np.random.default_rng([int(seed) & 0xFFFFFFFF, 0x676C7970])
+        self.sequences = []
+        for _ in range(seq_count):
+            n = int(rng.integers(seq_lens[0], seq_lens[1] + 1))
+            self.sequences.append([int(x) for x in rng.integers(0, self.buckets.count(), n)])
+        self.seq_idx = 0
+        self.gly_idx = 0
+        torch = _torch()
+        self._device = torch.device("cuda:%d" % ctx.device)
+
+    def get(self):
+        return self.seq_idx, self.sequences[self.seq_idx][self.gly_idx]
+
+    def advance(self):
+        """SeqReader::advance (glyph_sequences.rs:28-36)."""
+        self.gly_idx += 1
+        if self.gly_idx >= len(self.sequences[self.seq_idx]):
+            self.gly_idx = 0
+            self.seq_idx += 1
+            if self.seq_idx >= len(self.sequences):
+                self.seq_idx = 0
+
+    cycle_next = advance
+
+    def write_into(self, frame, layer):
+        """layer "img" or "val"; `frame` (device) of that layer's dims."""
+        torch = _torch()
+        _, glyph_id = self.get()
+        glyph = self.buckets.next_glyph(glyph_id)
+        if layer == "img":
+            img = torch.from_numpy(np.ascontiguousarray(glyph)).to(self._device)
+            encode_2d_image(self.ctx, img, self.buckets.glyph_dims, self.img_layer_dims, self.scale, frame)
+        elif layer == "val":
+            n = self.val_layer_dims[0] * self.val_layer_dims[1]
+            frame[:n].copy_(torch.arange(n, device=self._device, dtype=torch.int64).bitwise_and(0xFF).to(torch.uint8))
+        else:
+            raise ValueError("GlyphSequences::write_into(): Layer address not found: %r." % (layer,))

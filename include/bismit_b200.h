@@ -704,6 +704,14 @@ int bm_encode_hex_mold(bm_ctx ctx, int32_t radius, uint32_t src_v_size, uint32_t
 int bm_encode_scalar(bm_ctx ctx, const float* vals, uint32_t n, float lo, float hi, uint64_t seed, uint8_t* frames,
                      uint64_t frame_stride, uint32_t v_size, uint32_t u_size);
 
+/* ScalarGlyphWriter (src/encode/write/scalar_glyph_writer.rs:25-151), which
+ * VectorEncoder and ScalarSequence write with: each of n values (host,
+ * n <= 4096, within [lo, hi]) clears its frame and sets to 127 the hexagon of
+ * radius (v + u) / 32 around the value's tile on a track along the frame's
+ * margin (clockwise from the upper left). */
+int bm_encode_scalar_glyph(bm_ctx ctx, const float* vals, uint32_t n, float lo, float hi, uint8_t* frames,
+                           uint64_t frame_stride, uint32_t v_size, uint32_t u_size);
+
 /* ScalarSdrWriter (src/encode/write/scalar_sdr_writer.rs:96-235): waypoint
  * SDRs every `way_span` across [lo, hi], each v*u/48 seeded axon indices
  * (held on the device); encode blends the two waypoints around each value. */

@@ -54,6 +54,8 @@ def load_port():
         L.bmo_hex_mold.argtypes = [C.c_int, u32, u32, vp, u32, u32]
         L.bmo_encode_scalar.restype = C.c_int
         L.bmo_encode_scalar.argtypes = [f32, f32, f32, u64, u32, vp, u32, u32]
+        L.bmo_encode_scalar_glyph.restype = C.c_int
+        L.bmo_encode_scalar_glyph.argtypes = [f32, f32, f32, vp, u32, u32]
         L.bmo_sdr_waypoints.restype = C.c_int
         L.bmo_sdr_waypoints.argtypes = [f32, f32, f32, u32, u32, u64, vp]
         L.bmo_sdr_encode.restype = C.c_int
@@ -182,6 +184,14 @@ def encode_scalar(vals, lo, hi, seed, v_size, u_size):
     out = np.zeros((len(vals), v_size * u_size), np.uint8)
     for k, v in enumerate(vals):
         if load_port().bmo_encode_scalar(v, lo, hi, seed, k, _np_ptr(out[k]), v_size, u_size) != 0:
+            raise ValueError("value %r refused" % v)
+    return out
+
+
+def encode_scalar_glyph(vals, lo, hi, v_size, u_size):
+    out = np.zeros((len(vals), v_size * u_size), np.uint8)
+    for k, v in enumerate(vals):
+        if load_port().bmo_encode_scalar_glyph(v, lo, hi, _np_ptr(out[k]), v_size, u_size) != 0:
             raise ValueError("value %r refused" % v)
     return out
 

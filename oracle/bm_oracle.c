@@ -1119,6 +1119,54 @@ int bmo_encode_scalar(float val, float lo, float hi, uint64_t seed, uint32_t fra
     return 0;
 }
 
+/* ScalarGlyphWriter (src/encode/write/scalar_glyph_writer.rs:25-151): the
+ * value's tile along the track that runs around the frame's margin (clockwise
+ * from the upper left), the frame cleared and the hexagon of radius
+ * (v + u) / 32 around that tile set to 127. f32 arithmetic as the
+ * reference's; `as u32` of the floored tile saturates (NaN to 0). */
+int bmo_encode_scalar_glyph(float val, float lo, float hi, uint8_t* frame, uint32_t v_size, uint32_t u_size) {
+    if (v_size < 8 || u_size < 8 || !(lo <= hi) || !(val >= lo && val <= hi)) return -1;
+    const uint32_t radius = (v_size + u_size) / 32;
+    const uint32_t extra_margin = radius + 1;
+    const uint32_t margin = radius + extra_margin + 1;
+    const uint32_t track_tiles_v = v_size - (margin * 2) - 1;
+    const uint32_t track_tiles_u = u_size - (margin * 2) - 1;
+    const uint32_t track_tiles_total = (track_tiles_v * 2) + (track_tiles_u * 2);
+    const float track_tiles_total_f32 = (float)track_tiles_total;
+    const float val_span = hi - lo;
+    const uint32_t sides0 = track_tiles_u, sides1 = track_tiles_u + track_tiles_v;
+    const uint32_t sides2 = (2 * track_tiles_u) + track_tiles_v, sides3 = track_tiles_total;
+    const float val_pct = (val - lo) / val_span;
+    const float tile_f = floorf(val_pct * track_tiles_total_f32);
+    const uint32_t val_tile = !(tile_f > 0.0f) ? 0u : tile_f >= 4294967295.0f ? 0xFFFFFFFFu : (uint32_t)tile_f;
+    uint32_t cv, cu;
+    if (val_tile < sides0) {
+        cv = margin;
+        cu = margin + val_tile;
+    } else if (val_tile < sides1) {
+        cv = margin + (val_tile - sides0);
+        cu = margin + track_tiles_u;
+    } else if (val_tile < sides2) {
+        cv = margin + track_tiles_v;
+        cu = (margin + track_tiles_u) - (val_tile - sides1);
+    } else if (val_tile < sides3) {
+        cv = (margin + track_tiles_v) - (val_tile - sides2);
+        cu = margin;
+    } else {
+        if (val_tile != track_tiles_total) return -1;
+        cv = margin;
+        cu = margin;
+    }
+    memset(frame, 0, (size_t)v_size * u_size);
+    const int r = (int)radius;
+    for (int v = -r; v < r + 1; v++) {
+        const int u_z = imax(-r, -v - r), u_m = imin(r, -v + r);
+        for (int u = u_z; u < u_m + 1; u++)
+            frame[(size_t)((v + (int)cv) * (int)u_size + u + (int)cu)] = 127;
+    }
+    return 0;
+}
+
 /* ScalarSdrWriter::new (src/encode/write/scalar_sdr_writer.rs:96-152): the
  * waypoint count, and (when `ways` is given) the seeded waypoint table of
  * way_count x (len / 48) indices in [0, len). */

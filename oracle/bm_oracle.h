@@ -60,6 +60,7 @@ void bmo_encode_image(const uint8_t* source, uint32_t x_size, uint32_t y_size, f
 int bmo_hex_mold(int radius, uint32_t src_v, uint32_t src_u, uint8_t* frame, uint32_t v_size, uint32_t u_size);
 int bmo_encode_scalar(float val, float lo, float hi, uint64_t seed, uint32_t frame_idx, uint8_t* frame,
                       uint32_t v_size, uint32_t u_size);
+int bmo_encode_scalar_glyph(float val, float lo, float hi, uint8_t* frame, uint32_t v_size, uint32_t u_size);
 int bmo_sdr_waypoints(float lo, float hi, float way_span, uint32_t v_size, uint32_t u_size, uint64_t seed,
                       uint32_t* ways);
 int bmo_sdr_encode(float val, float lo, float hi, float way_span, uint32_t way_count, const uint32_t* ways,

@@ -202,3 +202,128 @@ def test_idx_streamer_feeds_an_area(ctx, tmp_path):
     got = area.read_slab()
     assert np.array_equal(got, slab)
     area.close()
+
+
+def _glyph_py(val, lo, hi, v_size, u_size):
+    """ScalarGlyphWriter::new + ::encode (src/encode/write/scalar_glyph_
+    writer.rs:25-151) in numpy float32 scalars, loop by loop."""
+    radius = (v_size + u_size) // 32
+    margin = radius + (radius + 1) + 1
+    ttv, ttu = v_size - margin * 2 - 1, u_size - margin * 2 - 1
+    total = ttv * 2 + ttu * 2
+    sides = (ttu, ttu + ttv, 2 * ttu + ttv, total)
+    pct = (f32(val) - f32(lo)) / (f32(hi) - f32(lo))
+    t = np.floor(pct * f32(total))
+    tile = 0 if not t > 0 else int(t)
+    if tile < sides[0]:
+        c = (margin, margin + tile)
+    elif tile < sides[1]:
+        c = (margin + (tile - sides[0]), margin + ttu)
+    elif tile < sides[2]:
+        c = (margin + ttv, (margin + ttu) - (tile - sides[1]))
+    elif tile < sides[3]:
+        c = ((margin + ttv) - (tile - sides[2]), margin)
+    else:
+        assert tile == total
+        c = (margin, margin)
+    out = np.zeros(v_size * u_size, np.uint8)
+    for v in range(-radius, radius + 1):
+        for u in range(max(-radius, -v - radius), min(radius, -v + radius) + 1):
+            out[(v + c[0]) * u_size + u + c[1]] = 127
+    return out
+
+
+@pytest.mark.parametrize("dims", [(32, 32), (48, 64), (8, 8), (96, 40)])
+def test_scalar_glyph_writer_matches_loop_restatement(dims):
+    """The oracle's C restatement of the glyph writer against a loop-by-loop
+    float32 one, across the range's ends and every side of the track; values
+    outside the range are refused."""
+    lo, hi = -3.0, 7.5
+    vals = np.concatenate([np.linspace(lo, hi, 57, dtype=np.float32), np.float32([hi, lo, 0.1])])
+    got = oracle.encode_scalar_glyph(vals, lo, hi, *dims)
+    for k, v in enumerate(vals):
+        assert np.array_equal(got[k], _glyph_py(v, lo, hi, *dims)), (dims, float(v))
+    r = (dims[0] + dims[1]) // 32
+    assert all(np.count_nonzero(g) == 3 * r * r + 3 * r + 1 for g in got)
+    with pytest.raises(ValueError):
+        oracle.encode_scalar_glyph([np.float32(hi + 1)], lo, hi, *dims)
+
+
+def test_glyph_buckets_and_sequences_cycle(tmp_path):
+    """GlyphBuckets sorts images by label and cycles each bucket; GlyphSequences'
+    sequences have lengths in range and ids below the bucket count, and its
+    cursor walks them in order (src/encode/glyph_buckets.rs,
+    src/encode/glyph_sequences.rs:13-36)."""
+    rng = np.random.default_rng(1)
+    n = 40
+    labels = rng.integers(0, 10, n, dtype=np.uint8)
+    images = rng.integers(0, 256, (n, 6, 5), dtype=np.uint8)
+    E.IdxData.write(tmp_path / "labels.idx", labels)
+    E.IdxData.write(tmp_path / "images.idx", images)
+    b = E.GlyphBuckets(tmp_path / "labels.idx", tmp_path / "images.idx")
+    assert b.glyph_dims == (6, 5) and b.count() == 10
+    lab = int(labels[0])
+    members = [images[i].reshape(-1) for i in range(n) if labels[i] == lab]
+    for k in range(2 * len(members) + 1):
+        assert np.array_equal(b.next_glyph(lab), members[k % len(members)])
+    with pytest.raises(ValueError):
+        b.next_glyph(10)
+
+
+@pytest.mark.gpu
+def test_device_glyph_and_sequence_encoders_match_oracle(ctx, tmp_path):
+    """The device glyph writer and the sequence / vector encoders built on it
+    against the oracle, frame for frame; GlyphSequences' image frames against
+    the oracle's encode_2d_image of the glyph its cursor picks."""
+    import torch
+    dims = (48, 64)
+    lo, hi = 0.0, 10.0
+    vals = np.linspace(lo, hi, 41, dtype=np.float32)
+    fr = torch.zeros((len(vals), dims[0] * dims[1]), dtype=torch.uint8, device="cuda:0")
+    E.encode_scalar_glyph(ctx, vals, (lo, hi), dims, fr)
+    assert np.array_equal(fr.cpu().numpy(), oracle.encode_scalar_glyph(vals, lo, hi, *dims))
+    # ScalarSequence: f32 steps wrapping at hi.
+    seq = E.ScalarSequence(ctx, (lo, hi), 0.7, dims)
+    expect = []
+    one = torch.zeros(dims[0] * dims[1], dtype=torch.uint8, device="cuda:0")
+    for _ in range(20):
+        seq.write_into(one)
+        expect.append(seq.next)
+        assert np.array_equal(one.cpu().numpy(), oracle.encode_scalar_glyph([seq.next], lo, hi, *dims)[0])
+        seq.cycle_next()
+    assert min(expect) == np.float32(lo) and max(expect) < np.float32(hi)
+    # VectorEncoder: one value per layer, each in its range.
+    ve = E.VectorEncoder(ctx, [(0.0, 1.0), (-5.0, 5.0)], [dims, (32, 32)])
+    ve.values[:] = [0.25, -4.0]
+    out0 = torch.zeros(dims[0] * dims[1], dtype=torch.uint8, device="cuda:0")
+    out1 = torch.zeros(32 * 32, dtype=torch.uint8, device="cuda:0")
+    ve.write_into(out0, 0)
+    ve.write_into(out1, 1)
+    assert np.array_equal(out0.cpu().numpy(), oracle.encode_scalar_glyph([0.25], 0.0, 1.0, *dims)[0])
+    assert np.array_equal(out1.cpu().numpy(), oracle.encode_scalar_glyph([-4.0], -5.0, 5.0, 32, 32)[0])
+    # ReversoScalarSequence: encode_scalar(next) and encode_scalar(hi - next).
+    rs = E.ReversoScalarSequence(ctx, (0.0, 8.0), 1.5, dims, seed=4)
+    rs.cycle_next()
+    rs.write_into(out0, 0)
+    assert np.array_equal(out0.cpu().numpy(), oracle.encode_scalar([rs.next], 0.0, 8.0, 4, *dims)[0])
+    rs.write_into(out0, 1)
+    assert np.array_equal(out0.cpu().numpy(),
+                          oracle.encode_scalar([np.float32(8.0) - rs.next], 0.0, 8.0, 4, *dims)[0])
+    # GlyphSequences.
+    rng = np.random.default_rng(2)
+    labels = rng.integers(0, 10, 60, dtype=np.uint8)
+    images = rng.integers(0, 256, (60, 12, 12), dtype=np.uint8)
+    E.IdxData.write(tmp_path / "l.idx", labels)
+    E.IdxData.write(tmp_path / "i.idx", images)
+    gs = E.GlyphSequences(ctx, (2, 4), 5, 1.0, (8, 8), (32, 32), tmp_path / "l.idx", tmp_path / "i.idx", seed=3)
+    assert all(2 <= len(q) <= 4 for q in gs.sequences)
+    shadow = E.GlyphBuckets(tmp_path / "l.idx", tmp_path / "i.idx")
+    img = torch.zeros(32 * 32, dtype=torch.uint8, device="cuda:0")
+    for _ in range(12):
+        _, gid = gs.get()
+        glyph = shadow.next_glyph(gid)
+        img.zero_()
+        gs.write_into(img, "img")
+        want = oracle.encode_image(glyph.reshape(12, 12), 1.0, 32, 32)
+        assert np.array_equal(img.cpu().numpy(), want)
+        gs.cycle_next()
