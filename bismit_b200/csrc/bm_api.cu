@@ -161,7 +161,27 @@ void fuse_steps(const bm_area_s* A, std::vector<Step>& v) {
             }
             const bool learn = n_dst > 0 && all;
             if (learn || m == j) {
-                out.push_back({ST_PYR_TAIL, s.layer, ctrl, (uint8_t)learn});
+                // The layer's tuft steps that run per cell (tufts the fused
+                // kernel does not take) come right before its soma step with
+                // only other tuft steps of the layer in between, which write
+                // no axon: they fold into the tail, each cell's four stages
+                // ahead of its soma.
+                uint8_t tufts = 0;
+                for (size_t q = out.size(); q > 0; q--) {
+                    const Step& o = out[q - 1];
+                    if (o.kind != ST_TUFT || o.layer != s.layer) break;
+                    if (!A->fused.t[s.layer][o.idx].ok && o.idx < 8) tufts |= (uint8_t)(1u << o.idx);
+                }
+                if (tufts)
+                    out.erase(std::remove_if(out.begin(), out.end(),
+                                             [&](const Step& o) {
+                                                 return o.kind == ST_TUFT && o.layer == s.layer &&
+                                                        ((tufts >> o.idx) & 1);
+                                             }),
+                              out.end());
+                Step tail{ST_PYR_TAIL, s.layer, ctrl, (uint8_t)learn};
+                tail.tufts = tufts;
+                out.push_back(tail);
                 k = (learn ? m : j) - 1;
                 continue;
             }
@@ -204,7 +224,7 @@ void bm::area_steps(const bm_area_s* A, std::vector<Step>& out) {
 // each stage per tuft); the fused form takes each tuft on its own, one fused
 // launch where the tuft qualifies, else that tuft's four stages. The stages of
 // different tufts touch disjoint buffers, so both orders give the same bytes.
-void bm::exec_step(bm_area_s* A, const Step& st, cudaStream_t s) {
+void bm::exec_step(bm_area_s* A, const Step& st, cudaStream_t s, bool end_cycle) {
     const uint32_t i = st.layer, x = st.idx;
     const bm_layer_plan& L = A->plan.layers[i];
     const DevLayer& D = A->dl[i];
@@ -233,7 +253,8 @@ void bm::exec_step(bm_area_s* A, const Step& st, cudaStream_t s) {
         break;
     case ST_PYR_TAIL: {
         const int ctrl = x == 0xFF ? 0 : (L.ctrl[x].kind == BM_LYR_CTRL_INTRA_COLUMN ? 1 : 2);
-        run(K_PYR_TAIL, [&] { launch_pyr_tail(A->axns(), A->slices, D, ctrl, st.arg != 0, A->ctl, s); });
+        run(K_PYR_TAIL,
+            [&] { launch_pyr_tail(A->axns(), A->slices, D, ctrl, st.arg != 0, A->ctl, s, st.tufts, end_cycle); });
         break;
     }
     case ST_TUFTS_PLAIN:
@@ -436,6 +457,18 @@ int bm::schedule_area(bm_area_s* A) {
         for (size_t j = 0; j < k; j++)
             if (A->step_side[j] && conflict(acc[j], acc[k])) A->step_waits[k].push_back(j);
     }
+    // The cycle-end launch folds into a final pyramidal tail on the main
+    // stream that every side step has joined (so no step of the cycle reads
+    // the cycle number after it advances).
+    A->end_in_tail = false;
+    if (n >= 2 && A->steps[n - 1].kind == ST_CYCLE_END && A->steps[n - 2].kind == ST_PYR_TAIL && !A->step_side[n - 2]) {
+        bool joined = true;
+        for (size_t j = 0; j + 2 < n && joined; j++)
+            if (A->step_side[j])
+                joined = std::find(A->step_waits[n - 2].begin(), A->step_waits[n - 2].end(), j) !=
+                         A->step_waits[n - 2].end();
+        A->end_in_tail = joined;
+    }
     for (cudaEvent_t ev : A->side_ev)
         if (ev) cudaEventDestroy(ev);
     A->side_ev.clear();
@@ -490,11 +523,14 @@ int enqueue_cycle(bm_area_s* A) {
         cudaEventRecord(A->ev_fork, main);
         cudaStreamWaitEvent(A->side, A->ev_fork, 0);
     }
-    for (size_t k = 0; k < A->steps.size(); k++) {
+    // With end_in_tail the last pyramidal tail ends the cycle itself and the
+    // cycle-end step (the last) launches nothing.
+    const size_t n = A->steps.size() - (A->end_in_tail ? 1 : 0);
+    for (size_t k = 0; k < n; k++) {
         const bool on_side = fork && A->step_side[k];
         if (fork && !on_side)
             for (size_t j : A->step_waits[k]) cudaStreamWaitEvent(main, A->side_ev[j], 0);
-        exec_step(A, A->steps[k], on_side ? A->side : main);
+        exec_step(A, A->steps[k], on_side ? A->side : main, A->end_in_tail && k + 1 == n);
         if (on_side) cudaEventRecord(A->side_ev[k], A->side);
     }
     if (fork) cudaStreamWaitEvent(main, A->side_ev[A->last_side], 0);

@@ -62,8 +62,9 @@ enum StepKind : uint8_t {
 };
 struct Step {
     uint8_t kind, layer, idx, arg;
+    uint8_t tufts = 0;   // ST_PYR_TAIL: per-cell tufts (bit t) it runs first, folded in
     bool operator==(const Step& o) const {
-        return kind == o.kind && layer == o.layer && idx == o.idx && arg == o.arg;
+        return kind == o.kind && layer == o.layer && idx == o.idx && arg == o.arg && tufts == o.tufts;
     }
 };
 
@@ -124,6 +125,7 @@ struct bm_area_s {
     double prof_ms[bm::K_COUNT] = {};
     uint32_t launches = 0;   // kernel launches of the last enqueued cycle
     std::vector<Step> steps; // the cycle's stage program
+    bool end_in_tail = false;  // the last pyramidal tail also ends the cycle (no cycle-end launch)
     // Two-stream form of the program (schedule_area): steps on the side
     // stream, the side steps each main step waits for, events and the stream.
     std::vector<uint8_t> step_side;
@@ -211,8 +213,9 @@ namespace bm {
 
 // The steps of one cycle of A (CorticalArea::cycle order).
 void area_steps(const bm_area_s* A, std::vector<Step>& out);
-// Enqueues one step of A on stream s.
-void exec_step(bm_area_s* A, const Step& st, cudaStream_t s);
+// Enqueues one step of A on stream s (a pyramidal tail with end_cycle also
+// ends the cycle).
+void exec_step(bm_area_s* A, const Step& st, cudaStream_t s, bool end_cycle = false);
 // Recompiles the gather offsets of layers whose sources or flags were written.
 void run_pending_verifies(bm_area_s* A, cudaStream_t s);
 // Rebuilds A->geo (the tiled tufts' footprint geometry that regrowth uses).

@@ -47,6 +47,7 @@ struct CellJob {
     int32_t ctrl;       // pyramidal tail: 0 none, 1 intra-column, 2 output
     uint32_t learn;     // fused steps: learning included
     uint32_t x;         // tuft or control index
+    uint32_t tufts;     // pyramidal tail: per-cell tufts folded in (bit t)
     uint32_t n;         // work items (cells or columns)
     uint32_t block0;    // first block of this job
 };
@@ -102,7 +103,7 @@ __global__ void __launch_bounds__(kCellBlock) k_batch_cells(const CellJob* __res
         return;
     }
     if (ST == ST_PYR_TAIL) {
-        pyr_tail_warp(J.axns, J.slices, J.L, J.ctrl, J.learn != 0, J.ctl, i, i < J.n);
+        pyr_tail_warp(J.axns, J.slices, J.L, J.ctrl, J.learn != 0, J.ctl, i, i < J.n, J.tufts);
         return;
     }
     if (i >= J.n) return;
@@ -339,8 +340,10 @@ int add_cells(bm_batch_s::StepPlan& p, int k) {
             J.key = A->inhib_key[st.layer][st.idx];
             J.radius = (int32_t)A->plan.layers[st.layer].ctrl[st.idx].field_radius;
         }
-        if (k == ST_PYR_TAIL)
+        if (k == ST_PYR_TAIL) {
             J.ctrl = st.idx == 0xFF ? 0 : (A->plan.layers[st.layer].ctrl[st.idx].kind == BM_LYR_CTRL_INTRA_COLUMN ? 1 : 2);
+            J.tufts = st.tufts;
+        }
         J.learn = st.arg;
         const uint64_t n = items_of(A, k, st);
         if (n > 0xFFFFFFFFull) return set_err(BM_ERR_UNSUPPORTED, "batched step of more than 2^32 items");

@@ -85,9 +85,9 @@ struct AreaCtl {
     unsigned long long cycle;       // cycle number of the cycle in flight
     unsigned int error;             // sticky device-side error bits (kErr*)
     unsigned int wait_us;           // limit of each bounded wait in the tuft kernels, us (0: kDefaultWaitUs)
-    unsigned int stall_stage;       // fault injection: CTA 0's producer withholds its stall_stage-th
-                                    // stage (counted from 1) of every tiled tuft launch (0: none)
-    unsigned int pad;
+    unsigned int stall_stage;       // fault injection: the stage producer that takes a tuft's first tile
+                                    // withholds its stall_stage-th stage from it on (0: none)
+    unsigned int blocks_done;       // blocks of a cycle-ending kernel done so far (0 between cycles)
     unsigned int* host_err;         // host-mapped word the cycle end copies non-zero error bits to
                                     // (null: none), so the host sees them without a synchronisation
     unsigned int tuft_status[BM_MAX_LAYERS * BM_MAX_TUFTS];

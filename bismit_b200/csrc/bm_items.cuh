@@ -371,7 +371,7 @@ __host__ __device__ __forceinline__ uint64_t tail_items(uint32_t depth, uint32_t
 // whole column t when the column is deeper than kTailDepth.
 __device__ __forceinline__ void pyr_tail_warp(uint8_t* __restrict__ axns, const SliceRec* __restrict__ slices,
                                               const DevLayer& L, int ctrl, bool learn, const AreaCtl* ctl,
-                                              uint32_t item, bool valid_item) {
+                                              uint32_t item, bool valid_item, uint32_t tufts = 0) {
     const uint32_t cols = L.v_size * L.u_size;
     const int lane = threadIdx.x & 31;
     uint8_t* cfl = L.buf[BM_BUF_CEL_FLAG_SETS];
@@ -380,6 +380,10 @@ __device__ __forceinline__ void pyr_tail_warp(uint8_t* __restrict__ axns, const 
         const uint32_t col = item / G, d = item & (G - 1);
         const bool valid = valid_item && col < cols && d < L.depth;
         const uint32_t c = d * cols + col;
+        // Tufts the fused tuft kernel does not take, folded in: their four
+        // stages for this cell, which the soma reads next.
+        for (uint32_t t = 0; tufts && t < L.n_tufts; t++)
+            if (((tufts >> t) & 1) && valid) tuft_cell_item(axns, slices, L, t, rnd_at(L.tft[t].rnd_key_den, ctl->cycle), c);
         const bool prx_on = (L.enabled_flags & kDenBasalProximalFlag) != 0;
         const bool dst_on = (L.enabled_flags & kDenBasalDistalFlag) != 0;
         uint8_t prx = 0, dst = 0, f = 0, ax = 0;
@@ -438,6 +442,10 @@ __device__ __forceinline__ void pyr_tail_warp(uint8_t* __restrict__ axns, const 
     const bool valid = valid_item && col < cols;
     // Deeper columns: the same steps one cell at a time.
     if (valid) {
+        for (uint32_t t = 0; tufts && t < L.n_tufts; t++)
+            if ((tufts >> t) & 1)
+                for (uint32_t d = 0; d < L.depth; d++)
+                    tuft_cell_item(axns, slices, L, t, rnd_at(L.tft[t].rnd_key_den, ctl->cycle), d * cols + col);
         for (uint32_t d = 0; d < L.depth; d++) pyr_cycle_item(L, d * cols + col);
         if (ctrl == 1) intra_column_item(axns, slices, L, col);
         else if (ctrl == 2)

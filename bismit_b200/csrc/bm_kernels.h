@@ -127,8 +127,10 @@ void launch_tuft_cells(const uint8_t* axns, const SliceRec* slices, const DevLay
                        const AreaCtl* ctl, cudaStream_t s);
 void launch_inhib_mtp(uint8_t* axns, const SliceRec* slices, const DevLayer& L, int radius, uint64_t key,
                       bool learn, const AreaCtl* ctl, cudaStream_t s);
-void launch_pyr_tail(uint8_t* axns, const SliceRec* slices, const DevLayer& L, int ctrl, bool learn,
-                     const AreaCtl* ctl, cudaStream_t s);
+// `tufts` (bit t): tufts the fused tuft kernel does not take, run per cell
+// first; `end`: the last block to finish also ends the cycle.
+void launch_pyr_tail(uint8_t* axns, const SliceRec* slices, const DevLayer& L, int ctrl, bool learn, AreaCtl* ctl,
+                     cudaStream_t s, uint32_t tufts = 0, bool end = false);
 void launch_tft_dst_mtp_plain(const uint8_t* axns, const DevLayer& L, uint32_t t, const AreaCtl* ctl,
                               cudaStream_t s);
 

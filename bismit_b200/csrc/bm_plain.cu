@@ -122,11 +122,24 @@ __global__ void __launch_bounds__(128) k_inhib_mtp(uint8_t* __restrict__ axns, c
                    learn != 0, c, c < L.cells);
 }
 
+// With end_cycle, the last block to finish also ends the cycle (the cycle-end
+// launch folded in): every block has read the cycle number by then.
 __global__ void __launch_bounds__(128) k_pyr_tail(uint8_t* __restrict__ axns, const SliceRec* __restrict__ slices,
-                                                  DevLayer L, int ctrl, int learn, const AreaCtl* ctl) {
+                                                  DevLayer L, int ctrl, int learn, AreaCtl* ctl, uint32_t tufts,
+                                                  int end) {
     pdl_begin();
     const uint64_t i = gtid();
-    pyr_tail_warp(axns, slices, L, ctrl, learn != 0, ctl, (uint32_t)i, i < tail_items(L.depth, L.v_size * L.u_size));
+    pyr_tail_warp(axns, slices, L, ctrl, learn != 0, ctl, (uint32_t)i, i < tail_items(L.depth, L.v_size * L.u_size),
+                  tufts);
+    if (!end) return;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        if (atomicAdd(&ctl->blocks_done, 1u) == gridDim.x - 1) {
+            ctl->blocks_done = 0;
+            end_cycle(ctl);
+        }
+    }
 }
 
 inline unsigned nblk(uint64_t n, unsigned b) { return (unsigned)((n + b - 1) / b); }
@@ -285,10 +298,10 @@ void launch_inhib_mtp(uint8_t* axns, const SliceRec* slices, const DevLayer& L, 
                       bool learn, const AreaCtl* ctl, cudaStream_t s) {
     launch_pdl(k_inhib_mtp, nblk(L.cells, 128), 128, 0, s, axns, slices, L, radius, key, learn ? 1 : 0, ctl);
 }
-void launch_pyr_tail(uint8_t* axns, const SliceRec* slices, const DevLayer& L, int ctrl, bool learn,
-                     const AreaCtl* ctl, cudaStream_t s) {
+void launch_pyr_tail(uint8_t* axns, const SliceRec* slices, const DevLayer& L, int ctrl, bool learn, AreaCtl* ctl,
+                     cudaStream_t s, uint32_t tufts, bool end) {
     launch_pdl(k_pyr_tail, nblk(tail_items(L.depth, L.v_size * L.u_size), 128), 128, 0, s, axns, slices, L, ctrl,
-                                                                                   learn ? 1 : 0, ctl);
+               learn ? 1 : 0, ctl, tufts, end ? 1 : 0);
 }
 void launch_tft_dst_mtp_plain(const uint8_t* axns, const DevLayer& L, uint32_t t, const AreaCtl* ctl,
                               cudaStream_t s) {

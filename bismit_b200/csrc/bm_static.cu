@@ -121,7 +121,7 @@ __global__ void k_static_begin(unsigned char* scratch, const SliceTable tab, uns
         ctl->error = 0;
         ctl->wait_us = 0;
         ctl->stall_stage = 0;
-        ctl->pad = 0;
+        ctl->blocks_done = 0;
         ctl->host_err = nullptr;
     }
 }

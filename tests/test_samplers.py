@@ -176,3 +176,80 @@ def test_samplers_follow_batched_cycles(ctx):
     batch.close()
     for a in areas:
         a.close()
+
+
+class ChannelModel:
+    """The tract channel of src/subcortex/tract_channel.rs:400-488 restated
+    for one sender and one receiver polling from the same thread (recv with
+    wait_for_frame false): `send` sets the ready flag; if it was already set
+    the frame is skipped (without backpressure) or the sender waits (with it,
+    which a single-threaded script never reaches); `recv` takes the waiting
+    frame and clears the flag, or returns none. The library's channel also
+    serves a receiver that waits for a frame, which the reference leaves
+    untested (its direct hand-off keeps the ready flag set, :420-427)."""
+
+    def __init__(self, backpressure):
+        self.backpressure = backpressure
+        self.ready = False
+        self.frame = None
+        self.sent = self.skipped = 0
+
+    def send(self, cycle):
+        if self.ready:
+            assert not self.backpressure, "a single-threaded script would block here"
+            self.skipped += 1
+            return
+        self.ready = True
+        self.frame = cycle
+        self.sent += 1
+
+    def recv(self):
+        if not self.ready:
+            return None
+        self.ready = False
+        return self.frame
+
+
+@pytest.mark.parametrize("seed", [1, 2, 3])
+def test_channel_matches_a_restatement_of_the_reference_channel(ctx, seed):
+    """A seeded script of cycles, polls and backpressure switches drives the
+    area's sampler and the restated channel side by side: the same frames
+    (by cycle and content) come out, with the same sent and skipped counts.
+    Backpressure is only on while the receiver has taken the last frame, so
+    no send of the script blocks."""
+    rng = np.random.default_rng(seed)
+    a = _area(ctx)
+    li = _pyr_layer(a)
+    smp = a.sampler("soma_states", li)
+    model = ChannelModel(False)
+    fr = frames_for(a.plan, 40, 9, 0.05)
+    states = {}
+    c = 0
+    for _ in range(120):
+        op = rng.integers(0, 3)
+        if op == 0 and c < len(fr):
+            if not model.ready and rng.random() < 0.3:
+                want = not model.backpressure
+                assert smp.set_backpressure(want) == model.backpressure
+                model.backpressure = want
+            elif model.ready and model.backpressure:
+                assert smp.set_backpressure(False) is True
+                model.backpressure = False
+            a.write_input(fr[c])
+            a.cycle(1)
+            states[c] = a.read("cel_states", layer=li)
+            model.send(c)
+            c += 1
+        else:
+            got = smp.recv(False)
+            want = model.recv()
+            if want is None:
+                assert got is None
+            else:
+                assert got is not None and got[0] == want
+                assert np.array_equal(got[1], states[want])
+    st = smp.stats()
+    assert (st["sent"], st["skipped"]) == (model.sent, model.skipped)
+    assert model.skipped > 0 and model.sent > 0
+    smp.close()
+    a.close()
