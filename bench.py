@@ -50,6 +50,10 @@ def parse():
     ap.add_argument("--serve-sessions", type=int, default=64)
     ap.add_argument("--serve-rate", type=float, default=200.0, help="mean session arrivals per second (Poisson)")
     ap.add_argument("--serve-budget-gb", type=float, default=8.0)
+    ap.add_argument("--profile-run", default=None, choices=["area", "batched"],
+                    help="only W warm-up and K timed cycles of the workload (area: --workload through the plain "
+                         "cycling call; batched: the --batch-instances batch, autotuned, graph replay), no soak, "
+                         "arms or baselines: a short launch sequence for a profiler's launch list")
     return ap.parse_args()
 
 
@@ -903,6 +907,70 @@ def run_ours(args):
         torch.distributed.destroy_process_group()
 
 
+def run_profile(args):
+    """A short, fixed launch sequence for a profiler: W warm-up cycles, then K
+    cycles between CUDA events, of one workload on cuda:0; prints one JSON
+    line with the device time (informational: a run under a profiler is no
+    bench value). Area cycles are plain launches; the batch replays its CUDA
+    graph (under `--profile-run batched` its launch list is the graph's
+    kernels)."""
+    import torch
+    from bismit_b200 import configs, cortex, map as M
+    torch.cuda.set_device(0)
+    ctx = cortex._Ctx(0)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    ctx.set_stream(stream.cuda_stream)
+    K, W = args.steps, args.warmup
+    areas = []
+    if args.profile_run == "area":
+        lmaps, ar, act = configs.workload(args.workload)
+        st = configs.bench_settings()
+        if args.path == "plain":
+            st.plain_kernels()
+        areas.append(cortex.CorticalArea(ctx, M.area_desc("v1", lmaps, ar, st), seed=args.seed + 1))
+        flen = areas[0].input_len()
+        dev = torch.from_numpy(configs.frames(K + W, flen, act, args.seed)).to("cuda")
+
+        def cycles(c0, n):
+            areas[0].cycle_frames_device(dev.data_ptr() + c0 * flen, flen, n)
+        launches = areas[0].launches_per_cycle()
+        name = args.workload
+    else:
+        frames_h = []
+        for i, (side, depth, dens, syns, act) in enumerate(configs.batch_instances(args.batch_instances, args.seed)):
+            lmaps, ar = configs.instance_area(side, depth, dens, syns)
+            seed = args.seed * 1000 + i
+            areas.append(cortex.CorticalArea(ctx, M.area_desc("v1", lmaps, ar, configs.bench_settings()), seed))
+            frames_h.append(configs.frames(K + W, areas[-1].input_len(), act, seed))
+        batch = cortex.Batch(ctx, areas)
+        batch.autotune(None)
+        fb = batch.frame_bytes()
+        dev = torch.from_numpy(batch.pack_frames(frames_h)).to("cuda")
+
+        def cycles(c0, n):
+            batch.cycle_frames_device(dev.data_ptr() + c0 * fb, n)
+        launches = batch.launches_per_cycle()
+        name = "batch_%d" % args.batch_instances
+    torch.cuda.synchronize()
+    cycles(0, W)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    cycles(W, K)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    n_syn = sum(int(a.plan.n_syns_total) for a in areas)
+    print(json.dumps({"profile_run": name, "steps": K, "warmup": W, "launches_per_cycle": launches,
+                      "synapses": n_syn, "ms_per_cycle": e0.elapsed_time(e1) / K}), flush=True)
+    if args.profile_run == "batched":
+        batch.close()
+    for a in areas:
+        a.close()
+    ctx.close()
+
+
 def run_reference(args):
     """The reference's own kernels (cl/*.cl compiled for the CPU, all host
     threads) on the same workload; rank 0 only."""
@@ -948,6 +1016,8 @@ def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+    elif args.profile_run:
+        run_profile(args)
     else:
         run_ours(args)
 

@@ -153,6 +153,11 @@ struct bm_server_s {
     cudaEvent_t start_ev[2] = {};    // timing: device time of each tick
     Tick inflight[2];
     uint64_t tick_no = 0;
+    // Ticks since the latest rebuild. A new batch cycles by plain launches;
+    // it is captured into a CUDA graph once its membership has held for
+    // kGraphAfter ticks, so sessions that come and go pay no capture.
+    uint32_t same_ticks = 0;
+    static constexpr uint32_t kGraphAfter = 8;
     // Statistics.
     std::vector<float> lat_ms;
     uint64_t ticks = 0, frames_cycled = 0, rebuilds = 0;
@@ -569,7 +574,9 @@ int bm_server_tick(bm_server V, uint32_t* n_cycled) {
             std::vector<bm_area> areas;
             for (auto* S : m) areas.push_back(S->area);
             rc = bm_batch_create(V->ctx, areas.data(), (uint32_t)areas.size(), &V->batch);
+            if (rc == BM_OK) rc = bm_batch_set_graph(V->batch, 0);
             if (rc != BM_OK) return rc;
+            V->same_ticks = 0;
             V->members = m;
             V->rebuilds++;
             uint64_t fb = 0;
@@ -599,6 +606,10 @@ int bm_server_tick(bm_server V, uint32_t* n_cycled) {
         cudaError_t e = cudaEventRecord(V->start_ev[slot], s);
         if (e == cudaSuccess) e = cudaMemcpyAsync(V->d_frames, V->h_frames[slot], o, cudaMemcpyHostToDevice, s);
         if (e != cudaSuccess) return cuda_err(e, "frame block copy");
+        if (++V->same_ticks == bm_server_s::kGraphAfter) {
+            int rc = bm_batch_set_graph(V->batch, 1);
+            if (rc != BM_OK) return rc;
+        }
         int rc = batch_cycle_frames_unchecked(V->batch, V->d_frames);
         if (rc != BM_OK) return rc;
         if (V->out_blocks) k_gather_outputs<<<V->out_blocks, kGatherBlock, 0, s>>>(V->d_outjobs, (uint32_t)m.size(), V->d_out);
