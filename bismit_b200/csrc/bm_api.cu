@@ -673,6 +673,17 @@ void free_upload(bm_area_s* A) {
     A->up_cap = 0;
 }
 
+}  // namespace
+
+void bm::ctx_release(bm_ctx c) {
+    if (!c || c->refs.fetch_sub(1, std::memory_order_acq_rel) != 1) return;
+    DevGuard g(c->device);
+    if (c->own) { cudaStreamSynchronize(c->own); cudaStreamDestroy(c->own); }
+    delete c;
+}
+
+namespace {
+
 void free_area(bm_area_s* A) {
     if (!A) return;
     if (A->ctx) {
@@ -699,6 +710,7 @@ void free_area(bm_area_s* A) {
         for (auto& r : A->pending) { cudaEventDestroy(r.a); cudaEventDestroy(r.b); }
         for (auto e : A->pool) cudaEventDestroy(e);
     }
+    ctx_release(A->ctx);
     delete A;
 }
 
@@ -815,9 +827,7 @@ int bm_ctx_create(int device, uint32_t flags, bm_ctx* out) {
 
 int bm_ctx_destroy(bm_ctx ctx) {
     if (!ctx) return BM_OK;
-    DevGuard g(ctx->device);
-    if (ctx->own) { cudaStreamSynchronize(ctx->own); cudaStreamDestroy(ctx->own); }
-    delete ctx;
+    ctx_release(ctx);
     return BM_OK;
 }
 
@@ -848,7 +858,6 @@ int bm_area_create(bm_ctx ctx, const bm_area_desc* desc, uint64_t seed, bm_area*
     DevGuard g(ctx->device);
     bm_area_s* A = new (std::nothrow) bm_area_s;
     if (!A) return set_err(BM_ERR_OOM, "host allocation failed");
-    A->ctx = ctx;
     std::vector<TuftGrowSpec> grow;
     std::string err;
     int rc = resolve_area(desc, seed, &A->plan, &grow, &err);
@@ -858,6 +867,8 @@ int bm_area_create(bm_ctx ctx, const bm_area_desc* desc, uint64_t seed, bm_area*
         delete A;
         return set_err(BM_ERR_INVALID, "unknown exec_path %u", desc->exec_path);
     }
+    A->ctx = ctx;
+    ctx_retain(ctx);
     cudaStream_t s = ctx->stream();
     cudaError_t e = cudaMalloc(&A->slab, A->plan.slab_bytes);
     if (e != cudaSuccess) {

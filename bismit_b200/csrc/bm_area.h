@@ -2,6 +2,7 @@
 // per-area stage program (the ordered steps of one cycle) that the one-area
 // path and the batched path (bm_batch.cu) both execute.
 #pragma once
+#include <atomic>
 #include <bitset>
 #include <cstdint>
 #include <vector>
@@ -100,8 +101,18 @@ struct bm_ctx_s {
     cudaStream_t own = nullptr;
     cudaStream_t user = nullptr;
     bool user_set = false;
+    // References: the caller's handle (until bm_ctx_destroy) plus one per
+    // live area, batch, server and writer made on it; the last release frees
+    // the context, so destroying it before its children is safe.
+    std::atomic<int> refs{1};
     cudaStream_t stream() const { return user_set ? user : own; }
 };
+namespace bm {
+inline void ctx_retain(bm_ctx c) {
+    if (c) c->refs.fetch_add(1, std::memory_order_relaxed);
+}
+void ctx_release(bm_ctx c);   // frees the context with its last reference
+}  // namespace bm
 
 struct bm_area_s {
     using Step = bm::Step;

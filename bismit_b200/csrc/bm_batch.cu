@@ -18,9 +18,10 @@
 // One copy launch at the head of each cycle does the tracts and the frame
 // intake, so every tract carries its source's output of the previous cycle.
 //
-// A project-written autotuner (bm_batch_autotune) picks the tile size of each
-// batched tuft step by timing candidates on the live batch (with the touched
-// buffers saved and restored) and can keep its choices in a cache file.
+// A project-written autotuner (bm_batch_autotune) picks, for each batched
+// tuft step, the tile size, the ring's depth and the resident CTAs per SM by
+// timing candidates on the live batch (with the touched buffers saved and
+// restored), and can keep its choices in a cache file.
 #include <algorithm>
 #include <cstdio>
 #include <cstring>
@@ -196,6 +197,7 @@ struct bm_batch_s {
         Form form = F_EACH;
         std::vector<CellLaunch> cells;   // F_CELLS: launches in order
         FusedBatch fb;
+        BatchShape shape;                // F_FUSED: ring stages and CTAs per SM (autotuned)
         bool side = false;               // runs on the side stream (no conflict with any earlier main step)
         std::vector<size_t> waits;       // side steps this main step must wait for
         RegrowJob* d_regrow = nullptr;   // F_REGROW: every area's regrowth jobs, one launch
@@ -310,6 +312,7 @@ void free_batch(bm_batch_s* B) {
         if (e) cudaEventDestroy(e);
     for (auto& r : B->pending) { cudaEventDestroy(r.a); cudaEventDestroy(r.b); }
     for (auto e : B->pool) cudaEventDestroy(e);
+    ctx_release(B->ctx);
     delete B;
 }
 
@@ -372,7 +375,7 @@ int build_fused(bm_batch_s::StepPlan& p) {
         jobs.push_back({&A->fused, &A->dl[p.st.layer], A->axns(), A->slices, A->ctl, p.st.layer, t,
                         (p.st.arg & 1) != 0});
     }
-    int rc = prepare_fused_batch(p.fb, jobs);
+    int rc = prepare_fused_batch(p.fb, jobs, p.shape);
     if (rc != BM_OK) return rc;
     p.form = p.fb.ok ? bm_batch_s::F_FUSED : bm_batch_s::F_EACH;
     return BM_OK;
@@ -441,7 +444,7 @@ int build_step(bm_batch_s::StepPlan& p) {
             // keeps its tiles (that batch's launches are planned on them).
             if (!FT.tiled || FT.tile_tuned || FT.tile_target == target || A->n_batches > 1) continue;
             bool changed = false;
-            if (retile_fused_tuft(A->fused, A->plan, st.layer, t, target, &changed) && changed)
+            if (retile_fused_tuft(A->fused, A->plan, st.layer, t, target, &changed, FT.fp_staged) && changed)
                 A->verify_pending[st.layer] = true;
         }
         return build_fused(p);
@@ -793,13 +796,14 @@ int run_cycles(bm_batch_s* B, const void* frames, uint32_t n_cycles, bool refuse
 
 // --------------------------------------------------------- autotuner -----
 // The buffers one tuft step writes, per area: synapse states and flags,
-// dendrite raw states, states and activities, and (pyramidal) the eight
-// cell-tuft buffers.
+// dendrite raw states, states and activities, (pyramidal) the eight
+// cell-tuft buffers, and (spiny stellate, ssc_cycle folded in) the cell
+// energies.
 struct Range {
     uint8_t* p;
     uint64_t n;
 };
-void step_ranges(bm_area_s* A, uint32_t i, uint32_t t, std::vector<Range>& out) {
+void step_ranges(bm_area_s* A, uint32_t i, uint32_t t, bool ssc_soma, std::vector<Range>& out) {
     const bm_layer_plan& L = A->plan.layers[i];
     const bm_tuft_plan& T = L.tufts[t];
     auto add = [&](int k, uint64_t off, uint64_t n) { out.push_back({A->slab + L.buf_off[k] + off, n}); };
@@ -811,6 +815,8 @@ void step_ranges(bm_area_s* A, uint32_t i, uint32_t t, std::vector<Range>& out) 
     add(BM_BUF_DEN_ACTIVITIES, T.den_idz, nd);
     if (L.kind == BM_LYR_PYRAMIDAL)
         for (int k = BM_BUF_TFT_PREV_BEST_DEN_IDS; k <= BM_BUF_TFT_STATES; k++) add(k, T.cel_idz, L.cells);
+    if (ssc_soma && L.kind == BM_LYR_SPINY_STELLATE && L.buf_off[BM_BUF_CEL_ENERGIES] != UINT64_MAX)
+        add(BM_BUF_CEL_ENERGIES, 0, L.cells);
 }
 
 std::string step_key(const bm_batch_s::StepPlan& p) {
@@ -826,34 +832,48 @@ std::string step_key(const bm_batch_s::StepPlan& p) {
     return k;
 }
 
-std::map<std::string, uint32_t> read_cache(const char* path) {
-    std::map<std::string, uint32_t> m;
+// A step's tuned launch: synapses per tile, its BatchShape, and whether the
+// consumers stage the footprints (1) rather than load them as tensor boxes.
+struct Tuned {
+    uint32_t target = 0, stages = 0, ctas = 0, staged = 0;
+};
+
+// One line per step: its key, the tile target, the ring's most stages, the
+// CTAs per SM and the footprint form (fields left out read as 0).
+std::map<std::string, Tuned> read_cache(const char* path) {
+    std::map<std::string, Tuned> m;
     if (!path) return m;
     FILE* f = fopen(path, "r");
     if (!f) return m;
-    char key[4096];
-    unsigned v;
-    while (fscanf(f, "%4095s %u", key, &v) == 2) m[key] = v;
+    char line[4300], key[4096];
+    while (fgets(line, sizeof line, f)) {
+        Tuned v;
+        if (sscanf(line, "%4095s %u %u %u %u", key, &v.target, &v.stages, &v.ctas, &v.staged) >= 2 && v.target)
+            m[key] = v;
+    }
     fclose(f);
     return m;
 }
 
-void write_cache(const char* path, const std::map<std::string, uint32_t>& m) {
+void write_cache(const char* path, const std::map<std::string, Tuned>& m) {
     if (!path) return;
     FILE* f = fopen(path, "w");
     if (!f) return;
-    for (auto& kv : m) fprintf(f, "%s %u\n", kv.first.c_str(), kv.second);
+    for (auto& kv : m)
+        fprintf(f, "%s %u %u %u %u\n", kv.first.c_str(), kv.second.target, kv.second.stages, kv.second.ctas,
+                kv.second.staged);
     fclose(f);
 }
 
-// Retiles tuft (i, t) of every area for `target` synapses per tile and
-// rebuilds the step's batched launch. False when some area cannot take it.
-bool apply_target(bm_batch_s* B, bm_batch_s::StepPlan& p, uint32_t target) {
+// Retiles tuft (i, t) of every area for `target` synapses per tile (with
+// footprints staged by the consumers when `staged`) and rebuilds the step's
+// batched launch. False when some area cannot take it.
+bool apply_target(bm_batch_s* B, bm_batch_s::StepPlan& p, uint32_t target, bool staged = false) {
     for (auto& [A, t] : p.tufts)
         if (A->n_batches > 1) return false;   // another batch's launches are planned on these tiles
     for (auto& [A, t] : p.tufts) {
         bool changed = false;
-        if (!retile_fused_tuft(A->fused, A->plan, p.st.layer, t, target, &changed)) return false;
+        if (!retile_fused_tuft(A->fused, A->plan, p.st.layer, t, target, &changed, staged)) return false;
         A->fused.t[p.st.layer][t].tile_tuned = true;
         if (changed) A->verify_pending[p.st.layer] = true;
     }
@@ -883,6 +903,7 @@ int bm_batch_create(bm_ctx ctx, const bm_area* areas, uint32_t n_areas, bm_batch
     bm_batch_s* B = new (std::nothrow) bm_batch_s;
     if (!B) return set_err(BM_ERR_OOM, "host allocation failed");
     B->ctx = ctx;
+    ctx_retain(ctx);
     B->areas.assign(areas, areas + n_areas);
     for (bm_area A : B->areas) {
         A->n_batches++;
@@ -1044,24 +1065,40 @@ int bm_batch_autotune(bm_batch batch, const char* cache_path, uint32_t* n_tuned)
     bm_batch_s* B = batch;
     DevGuard g(B->ctx->device);
     cudaStream_t s = B->stream();
-    std::map<std::string, uint32_t> cache = read_cache(cache_path);
+    std::map<std::string, Tuned> cache = read_cache(cache_path);
     uint32_t tuned = 0;
     static const uint32_t kTargets[] = {4096, 8192, 16384, 32768, 65536, 131072};
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
+    // Device milliseconds of 5 launches of the step as planned (one warm-up
+    // launch first).
+    auto time_step = [&](const bm_batch_s::StepPlan& p) {
+        launch_fused_batch(p.fb, s);
+        cudaEventRecord(e0, s);
+        for (int r = 0; r < 5; r++) launch_fused_batch(p.fb, s);
+        cudaEventRecord(e1, s);
+        cudaEventSynchronize(e1);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        return ms;
+    };
     for (auto& p : B->plan) {
         if (p.form != bm_batch_s::F_FUSED) continue;
         const std::string key = step_key(p);
         auto hit = cache.find(key);
         if (hit != cache.end()) {
-            if (!apply_target(B, p, hit->second)) build_fused(p);
+            p.shape = {hit->second.stages, hit->second.ctas};
+            if (!apply_target(B, p, hit->second.target, hit->second.staged != 0)) {
+                p.shape = {};
+                build_fused(p);
+            }
             tuned++;
             continue;
         }
         // Save what the trials overwrite.
         std::vector<Range> ranges;
-        for (auto& [A, t] : p.tufts) step_ranges(A, p.st.layer, t, ranges);
+        for (auto& [A, t] : p.tufts) step_ranges(A, p.st.layer, t, (p.st.arg & 1) != 0, ranges);
         uint64_t total = 0;
         for (auto& r : ranges) total += r.n;
         uint8_t* save = nullptr;
@@ -1071,25 +1108,54 @@ int bm_batch_autotune(bm_batch batch, const char* cache_path, uint32_t* n_tuned)
         }
         uint64_t o = 0;
         for (auto& r : ranges) { cudaMemcpyAsync(save + o, r.p, r.n, cudaMemcpyDeviceToDevice, s); o += r.n; }
-        uint32_t best_t = 0;
+        // The tile size and footprint form first, with the default shape; then
+        // the ring depth and CTAs per SM for the chosen tiles (shapes that
+        // plan the same launches as one already timed are not timed again).
+        Tuned best;
         float best_ms = 1e30f;
-        for (uint32_t target : kTargets) {
-            if (!apply_target(B, p, target)) continue;
-            launch_fused_batch(p.fb, s);   // warm-up
-            cudaEventRecord(e0, s);
-            for (int r = 0; r < 5; r++) launch_fused_batch(p.fb, s);
-            cudaEventRecord(e1, s);
-            cudaEventSynchronize(e1);
-            float ms = 0.f;
-            cudaEventElapsedTime(&ms, e0, e1);
-            if (ms < best_ms) { best_ms = ms; best_t = target; }
+        p.shape = {};
+        for (uint32_t staged : {0u, 1u}) {
+            for (uint32_t target : kTargets) {
+                if (!apply_target(B, p, target, staged != 0)) continue;
+                const float ms = time_step(p);
+                if (ms < best_ms) {
+                    best_ms = ms;
+                    best.target = target;
+                    best.staged = staged;
+                }
+            }
         }
-        if (best_t == 0 || !apply_target(B, p, best_t)) build_fused(p);
+        if (best.target) {
+            std::vector<std::pair<std::vector<uint32_t>, std::vector<uint32_t>>> seen;
+            for (uint32_t stages : {0u, 2u, 3u}) {
+                for (uint32_t ctas : {0u, 1u, 2u}) {
+                    p.shape = {stages, ctas};
+                    if (!apply_target(B, p, best.target, best.staged != 0)) continue;
+                    std::vector<uint32_t> nst;
+                    for (void* q : p.fb.params) nst.push_back(fused_batch_stages(q));
+                    auto sig = std::make_pair(p.fb.grids, p.fb.smems);
+                    sig.second.insert(sig.second.end(), nst.begin(), nst.end());
+                    if (std::find(seen.begin(), seen.end(), sig) != seen.end()) continue;
+                    seen.push_back(sig);
+                    const float ms = (stages == 0 && ctas == 0) ? best_ms : time_step(p);
+                    if (ms < best_ms * 0.98f) {
+                        best_ms = ms;
+                        best.stages = stages;
+                        best.ctas = ctas;
+                    }
+                }
+            }
+        }
+        p.shape = {best.stages, best.ctas};
+        if (best.target == 0 || !apply_target(B, p, best.target, best.staged != 0)) {
+            p.shape = {};
+            build_fused(p);
+        }
         o = 0;
         for (auto& r : ranges) { cudaMemcpyAsync(r.p, save + o, r.n, cudaMemcpyDeviceToDevice, s); o += r.n; }
         cudaStreamSynchronize(s);
         cudaFree(save);
-        if (best_t) { cache[key] = best_t; tuned++; }
+        if (best.target) { cache[key] = best; tuned++; }
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);

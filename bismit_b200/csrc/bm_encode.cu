@@ -404,6 +404,7 @@ int bm_sdr_writer_create(bm_ctx ctx, float lo, float hi, float way_span, uint32_
     bm_sdr_writer_s* W = new (std::nothrow) bm_sdr_writer_s;
     if (!W) return set_err(BM_ERR_OOM, "host allocation failed");
     W->ctx = ctx;
+    ctx_retain(ctx);
     W->lo = lo;
     W->hi = hi;
     W->way_span = way_span;
@@ -424,6 +425,7 @@ int bm_sdr_writer_create(bm_ctx ctx, float lo, float hi, float way_span, uint32_
     }
     if (e != cudaSuccess) {
         if (W->ways) cudaFree(W->ways);
+        ctx_release(W->ctx);
         delete W;
         return cuda_err(e, "sdr writer waypoints");
     }
@@ -438,6 +440,7 @@ int bm_sdr_writer_destroy(bm_sdr_writer w) {
         cudaStreamSynchronize(w->ctx->stream());
         cudaFree(w->ways);
     }
+    ctx_release(w->ctx);
     delete w;
     return BM_OK;
 }

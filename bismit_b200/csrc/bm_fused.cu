@@ -915,27 +915,41 @@ __device__ __forceinline__ void producer_drain(uint64_t* full, uint32_t nst, con
     }
 }
 
-// Consumer warps: take tile G's footprint -- wait for its tensor load and
+// Consumer warps: take tile G's footprint -- load it as a tensor box and
 // fire it in place, or stage it themselves -- then process the tile's stages
-// from the ring (buffer cb, phase cphase) and release the footprint. False
-// when this warp gave up (a bounded wait ran out, or a give-up elsewhere was
+// from the ring (buffer cb, phase cphase). The caller's barrier before each
+// tile (every consumer warp done with the previous footprint, its shared
+// memory writes fenced for the async proxy) is what lets the box overwrite
+// the footprint, so consumer thread 0 issues it right there: the footprint
+// has one owner at a time whatever mix of tile forms a CTA takes. False when
+// this warp gave up (a bounded wait ran out, or a give-up elsewhere was
 // seen); the consumer warps then leave together at the next tile's barrier,
 // whose OR-reduction keeps that decision uniform.
 template <bool TUFT, int MODE, bool FCLEAN, int GEOM>
 __device__ __forceinline__ bool consume_tile(const FusedTuftArgs& A, const TileGeo& G, uint8_t* halo, uint8_t* stages,
-                                             uint64_t* full, uint64_t* empty, uint64_t* fp_full, uint64_t* fp_empty,
-                                             uint32_t& cb, uint32_t& cphase, uint32_t& fp_n, int lane, int wib,
-                                             int32_t rnd, uint64_t limit_ns, volatile int& s_abort) {
+                                             uint64_t* full, uint64_t* empty, uint64_t* fp_full, uint32_t& cb,
+                                             uint32_t& cphase, uint32_t& fp_n, int lane, int wib, int32_t rnd,
+                                             uint64_t limit_ns, volatile int& s_abort) {
     if (A.fp_tma) {
+        if (wib == 0 && lane == 0) {
+            mbar_arrive_expect_tx(fp_full, A.fp_bytes);
+            tma_load_3d(halo, &A.tmap, G.ulo - (int32_t)G.xoff, G.vlo, 0, fp_full);
+        }
         bool got = !s_abort && mbar_wait(fp_full, fp_n & 1, limit_ns);
         got = __all_sync(0xFFFFFFFFu, got);
-        fp_n++;
         if (!got && lane == 0) raise_abort(s_abort, A.ctl);
-        if (consumers_sync_or(!got)) return false;
+        if (consumers_sync_or(!got)) {
+            // Let the box land before the CTA's shared memory is released.
+            if (wib == 0 && lane == 0) mbar_wait(fp_full, fp_n & 1, limit_ns);
+            fp_n++;
+            return false;
+        }
+        fp_n++;
         fire_footprint(halo, A.fp_bytes);
         fence_proxy_async_smem();   // the next tile's load overwrites these bytes
     } else {
         build_footprint(A, G, halo, lane, wib);
+        fence_proxy_async_smem();   // a later tile's box may overwrite these bytes
     }
     consumers_sync();
     const uint32_t SB = stage_syns<MODE, FCLEAN>(A.stage_bytes);
@@ -958,41 +972,18 @@ __device__ __forceinline__ bool consume_tile(const FusedTuftArgs& A, const TileG
         if (lane == 0) mbar_arrive(&empty[cb]);
         if (++cb == A.nst) { cb = 0; cphase ^= 1; }
     }
-    __syncwarp();
-    if (lane == 0) mbar_arrive(fp_empty);   // done with this tile's footprint
     return true;
-}
-
-// Footprint lane of the producer warp: for the i-th tile of this CTA that
-// loads its footprint with a tensor box, waits until the consumers released
-// the footprint of tile i - 1 (they release one per tile), then arms fp_full
-// and issues the box. False when that wait gave up.
-__device__ __forceinline__ bool produce_footprint(const FusedTuftArgs& A, const TileGeo& G, uint8_t* halo,
-                                                  uint64_t* fp_full, uint64_t* fp_empty, uint32_t i,
-                                                  uint32_t& fp_issued, uint64_t limit_ns) {
-    if (i > 0 && !mbar_wait(fp_empty, (i - 1) & 1, limit_ns)) return false;   // the caller raises the abort
-    mbar_arrive_expect_tx(fp_full, A.fp_bytes);
-    tma_load_3d(halo, &A.tmap, G.ulo - (int32_t)G.xoff, G.vlo, 0, fp_full);
-    fp_issued++;
-    return true;
-}
-
-// After the footprint lane's last box (or a give-up): let the latest box land
-// before the CTA's shared memory is released.
-__device__ __forceinline__ void footprint_drain(uint64_t* fp_full, uint32_t fp_issued, uint64_t limit_ns) {
-    if (fp_issued) mbar_wait(fp_full, (fp_issued - 1) & 1, limit_ns);
 }
 
 // Shared-memory barriers of a CTA: the ring's full[nst] and empty[nst], then
-// the footprint's full and empty at fixed slots (nst <= 4).
-constexpr uint32_t kFpFullSlot = 8, kFpEmptySlot = 9;
+// the footprint's at a fixed slot (nst <= 4).
+constexpr uint32_t kFpFullSlot = 8;
 
 template <bool TUFT, int MODE, bool FCLEAN, int GEOM>
 __device__ __forceinline__ void tma_body(const FusedTuftArgs& A, uint8_t* smem, volatile int& s_abort) {
     uint64_t* full = (uint64_t*)(smem + A.ring_off);   // [nst]
     uint64_t* empty = full + A.nst;                    // [nst]
     uint64_t* fp_full = full + kFpFullSlot;
-    uint64_t* fp_empty = full + kFpEmptySlot;
     uint8_t* stages = smem + A.ring_off + 128;
     uint8_t* halo = smem;
     const int tid = threadIdx.x;
@@ -1000,21 +991,7 @@ __device__ __forceinline__ void tma_body(const FusedTuftArgs& A, uint8_t* smem, 
     const int wib = tid >> 5;
     const uint64_t limit_ns = wait_limit_ns(A.ctl);
     if (wib == kWarps) {
-        if (lane == 1) {
-            // ---- footprint lane: one tensor box per tile ----
-            uint32_t fp_issued = 0;
-            if (A.fp_tma) {
-                uint32_t i = 0;
-                for (uint32_t t = blockIdx.x; t < A.n_tiles && !s_abort; t += gridDim.x, i++)
-                    if (!produce_footprint(A, tile_geo(A, t), halo, fp_full, fp_empty, i, fp_issued, limit_ns)) {
-                        raise_abort(s_abort, A.ctl);
-                        break;
-                    }
-            }
-            footprint_drain(fp_full, fp_issued, limit_ns);
-            return;
-        }
-        // ---- stage lane: lane 0 streams every stage of this CTA's tiles ----
+        // ---- producer: lane 0 streams every stage of this CTA's tiles ----
         if (lane != 0) return;
         ProducerState ps;
         ps.limit_ns = limit_ns;
@@ -1033,8 +1010,8 @@ __device__ __forceinline__ void tma_body(const FusedTuftArgs& A, uint8_t* smem, 
         // Every consumer is done with the previous tile; all leave together
         // if any gave up.
         if (consumers_sync_or(!ok || s_abort)) break;
-        ok = consume_tile<TUFT, MODE, FCLEAN, GEOM>(A, G, halo, stages, full, empty, fp_full, fp_empty, cb, cphase,
-                                                    fp_n, lane, wib, rnd, limit_ns, s_abort);
+        ok = consume_tile<TUFT, MODE, FCLEAN, GEOM>(A, G, halo, stages, full, empty, fp_full, cb, cphase, fp_n, lane,
+                                                    wib, rnd, limit_ns, s_abort);
     }
 }
 
@@ -1047,7 +1024,6 @@ __device__ __forceinline__ void init_ring(uint8_t* ring, uint32_t nst, volatile 
             mbar_init(&empty[i], kWarps);
         }
         mbar_init(full + kFpFullSlot, 1);
-        mbar_init(full + kFpEmptySlot, kWarps);
         fence_mbar_init();
         s_abort = 0;
     }
@@ -1135,7 +1111,6 @@ __global__ void __launch_bounds__(kThreads, 3) k_fused_tuft_batch(const __grid_c
     uint64_t* full = (uint64_t*)(smem + P.ring_off);
     uint64_t* empty = full + nst;
     uint64_t* fp_full = full + kFpFullSlot;
-    uint64_t* fp_empty = full + kFpEmptySlot;
     uint8_t* stages = smem + P.ring_off + 128;
     uint8_t* halo = smem;
     const uint32_t n_tiles = P.tile0[P.n_jobs];
@@ -1143,26 +1118,6 @@ __global__ void __launch_bounds__(kThreads, 3) k_fused_tuft_batch(const __grid_c
     const int lane = tid & 31;
     const int wib = tid >> 5;
     if (wib == kWarps) {
-        if (lane == 1) {
-            // ---- footprint lane: one tensor box per tile of a job that uses them ----
-            uint32_t cur = 0xFFFFFFFFu, i = 0, fp_issued = 0;
-            uint64_t lim = 0;
-            for (uint32_t t = blockIdx.x; t < n_tiles && !s_abort; t += gridDim.x, i++) {
-                const uint32_t j = job_of(P, t);
-                const FusedTuftArgs& A = P.jobs[j];
-                if (j != cur) {
-                    cur = j;
-                    lim = wait_limit_ns(A.ctl);
-                }
-                if (!A.fp_tma) continue;
-                if (!produce_footprint(A, tile_geo(A, t - P.tile0[j]), halo, fp_full, fp_empty, i, fp_issued, lim)) {
-                    raise_abort(s_abort, A.ctl);
-                    break;
-                }
-            }
-            footprint_drain(fp_full, fp_issued, lim);
-            return;
-        }
         if (lane != 0) return;
         uint32_t cur = 0xFFFFFFFFu, mode = 0;
         ProducerState ps;
@@ -1211,8 +1166,8 @@ __global__ void __launch_bounds__(kThreads, 3) k_fused_tuft_batch(const __grid_c
         }
         const TileGeo G = tile_geo(A, t - P.tile0[j]);
 #define BM_CONSUME(M, FC, GM)                                                                                   \
-    ok = consume_tile<TUFT, M, FC, GM>(A, G, halo, stages, full, empty, fp_full, fp_empty, cb, cphase, fp_n, lane, \
-                                       wib, rnd, limit_ns, s_abort)
+    ok = consume_tile<TUFT, M, FC, GM>(A, G, halo, stages, full, empty, fp_full, cb, cphase, fp_n, lane, wib, rnd, \
+                                       limit_ns, s_abort)
         switch (mode) {
         case 0:
             if (TUFT) {
@@ -1478,22 +1433,24 @@ int plan_fused_tuft(FusedArea& F, const bm_area_plan& P, uint32_t layer, uint32_
 }
 
 bool retile_fused_tuft(FusedArea& F, const bm_area_plan& P, uint32_t layer, uint32_t t, uint32_t target_syns,
-                       bool* changed) {
+                       bool* changed, bool staged) {
     *changed = false;
     FusedTuft& FT = F.t[layer][t];
     if (!FT.tiled || !FT.gidx) return false;
     FusedTuft next;
-    plan_tuft(next, P, layer, t, F.sms, target_syns);
+    plan_tuft(next, P, layer, t, F.sms, target_syns, !staged);
     cudaGetLastError();
     if (!next.tiled) return false;
     if (next.tile_w == FT.tile_w && next.tile_h == FT.tile_h && next.nst == FT.nst && next.smem == FT.smem &&
         next.fp_tma == FT.fp_tma) {
         FT.tile_target = target_syns;   // same tiles: the compiled offsets stay valid
+        FT.fp_staged = staged;
         return true;
     }
     *changed = true;
     next.gidx = FT.gidx;
     next.tile_target = target_syns;
+    next.fp_staged = staged;
     next.bound_axns = FT.bound_axns;
     FT = next;
     if (FT.bound_axns) bind_fused_tuft(F, P, layer, t, FT.bound_axns);
@@ -1578,6 +1535,7 @@ int bind_fused_tuft(FusedArea& F, const bm_area_plan& P, uint32_t layer, uint32_
     next.gidx = FT.gidx;
     next.tile_target = FT.tile_target;
     next.tile_tuned = FT.tile_tuned;
+    next.fp_staged = FT.fp_staged;
     next.bound_axns = axns;
     FT = next;
     return BM_OK;
@@ -1759,7 +1717,7 @@ void launch_fused_tuft(const FusedArea& F, const uint8_t* axns, const SliceRec* 
 }
 
 // ---------------------------------------------------------- batched form --
-int prepare_fused_batch(FusedBatch& B, const std::vector<FusedJob>& jobs) {
+int prepare_fused_batch(FusedBatch& B, const std::vector<FusedJob>& jobs, const BatchShape& shape) {
     free_fused_batch(B);
     B = FusedBatch{};
     if (jobs.empty()) return BM_OK;
@@ -1789,7 +1747,7 @@ int prepare_fused_batch(FusedBatch& B, const std::vector<FusedJob>& jobs) {
             cls.push_back(&J);
             halo = std::max(halo, ((FT.nrec * FT.fsz + 127) / 128) * 128);
         }
-        uint32_t nst = ring_stages(stride, halo, 4);
+        uint32_t nst = ring_stages(stride, halo, shape.max_stages ? std::max<uint32_t>(2, std::min<uint32_t>(4, shape.max_stages)) : 4);
         while (nst > 2 && 128 + (uint64_t)nst * stride + halo > kMaxSmem) nst--;
         const uint64_t ring_off = halo;
         const uint64_t smem = std::max<uint64_t>(32768, ring_off + 128 + (uint64_t)nst * stride);
@@ -1801,6 +1759,7 @@ int prepare_fused_batch(FusedBatch& B, const std::vector<FusedJob>& jobs) {
         if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads, (size_t)smem) != cudaSuccess)
             per_sm = 1;
         cudaGetLastError();
+        if (shape.ctas_per_sm && (int)shape.ctas_per_sm < per_sm) per_sm = (int)shape.ctas_per_sm;
         for (size_t j0 = 0; j0 < cls.size(); j0 += kMaxBatchJobs) {
             auto* P = new (std::nothrow) BatchParams;
             if (!P) {
@@ -1834,6 +1793,8 @@ int prepare_fused_batch(FusedBatch& B, const std::vector<FusedJob>& jobs) {
     B.n_jobs = (uint32_t)jobs.size();
     return BM_OK;
 }
+
+uint32_t fused_batch_stages(const void* params) { return ((const BatchParams*)params)->nst; }
 
 void launch_fused_batch(const FusedBatch& B, cudaStream_t s) {
     if (!B.ok || !B.n_tiles) return;

@@ -31,6 +31,8 @@ struct FusedTuft {
     uint32_t src_idz[8] = {};
     uint32_t tile_target = 0;    // synapses per tile asked for (0: chosen from the tuft's size)
     bool tile_tuned = false;     // tile_target came from the autotuner
+    bool fp_staged = false;      // the consumers stage the footprint even where a tensor box could load it
+                                 // (the autotuner's choice)
     // Footprint loaded by the tensor memory accelerator (a 3-D box of the
     // source slices) instead of staged by the consumer warps; rows of fw
     // bytes then start on a 16-byte column boundary (GatherGeo::xalign).
@@ -53,11 +55,12 @@ int prepare_fused(FusedArea& F, const bm_area_plan& P, std::string* err);
 int plan_fused(FusedArea& F, const bm_area_plan& P);
 int plan_fused_tuft(FusedArea& F, const bm_area_plan& P, uint32_t layer, uint32_t t);
 // Replans a tiled tuft for about `target_syns` synapses per tile, keeping its
-// gather-offset buffer. False, and nothing changed, when the tuft would not
-// stay tiled. *changed tells whether the tiles changed, in which case the
-// caller recompiles the offsets before the next launch.
+// gather-offset buffer; `staged`: the consumers stage the footprint (no
+// tensor box). False, and nothing changed, when the tuft would not stay
+// tiled. *changed tells whether the tiles or the footprint form changed, in
+// which case the caller recompiles the offsets before the next launch.
 bool retile_fused_tuft(FusedArea& F, const bm_area_plan& P, uint32_t layer, uint32_t t, uint32_t target_syns,
-                       bool* changed);
+                       bool* changed, bool staged = false);
 void free_fused(FusedArea& F);
 // Encodes the footprint tensor maps of the tufts that load their footprint
 // with the tensor memory accelerator, for the axon space at `axns` (device
@@ -99,10 +102,19 @@ struct FusedBatch {
     std::vector<uint32_t> smems;
     uint32_t n_jobs = 0, n_tiles = 0;
 };
+// Launch shape of a batched tuft step, as the autotuner sets it: the ring's
+// most stages (0: up to 4, fewest CTAs per SM lost) and the resident CTAs per
+// SM of the persistent grid (0: as many as fit).
+struct BatchShape {
+    uint32_t max_stages = 0;
+    uint32_t ctas_per_sm = 0;
+};
 // Plans the launches (B.ok false when some job cannot share them; the caller
 // then launches each job's own form).
-int prepare_fused_batch(FusedBatch& B, const std::vector<FusedJob>& jobs);
+int prepare_fused_batch(FusedBatch& B, const std::vector<FusedJob>& jobs, const BatchShape& shape = {});
 void launch_fused_batch(const FusedBatch& B, cudaStream_t s);
+// Ring stages of one planned launch (an entry of FusedBatch::params).
+uint32_t fused_batch_stages(const void* params);
 void free_fused_batch(FusedBatch& B);
 
 }  // namespace bm

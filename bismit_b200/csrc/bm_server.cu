@@ -261,6 +261,8 @@ void admit(bm_server_s* V, bm_server_s::Session* S) {
 // A built session joins the ticks: its area's later work goes to the serving
 // stream (same device).
 void adopt(bm_server_s* V, bm_server_s::Session* S) {
+    ctx_retain(V->ctx);
+    ctx_release(S->area->ctx);
     S->area->ctx = V->ctx;
     S->resident = true;
     S->admitted = now_s();
@@ -380,9 +382,10 @@ int bm_server_create(bm_ctx ctx, uint64_t mem_budget, bm_server* out) {
     DevGuard g(ctx->device);
     bm_server_s* V = new (std::nothrow) bm_server_s;
     if (!V) return set_err(BM_ERR_OOM, "host allocation failed");
-    V->ctx = ctx;
     int rc = bm_ctx_create(ctx->device, 0, &V->setup);
     if (rc != BM_OK) { delete V; return rc; }
+    V->ctx = ctx;
+    ctx_retain(ctx);
     if (!mem_budget) {
         size_t fr = 0, tot = 0;
         cudaMemGetInfo(&fr, &tot);
@@ -392,7 +395,12 @@ int bm_server_create(bm_ctx ctx, uint64_t mem_budget, bm_server* out) {
     if (cudaEventCreate(&V->done_ev[0]) != cudaSuccess || cudaEventCreate(&V->done_ev[1]) != cudaSuccess ||
         cudaEventCreate(&V->start_ev[0]) != cudaSuccess || cudaEventCreate(&V->start_ev[1]) != cudaSuccess) {
         cudaGetLastError();
+        for (int b = 0; b < 2; b++) {
+            if (V->done_ev[b]) cudaEventDestroy(V->done_ev[b]);
+            if (V->start_ev[b]) cudaEventDestroy(V->start_ev[b]);
+        }
         bm_ctx_destroy(V->setup);
+        ctx_release(V->ctx);
         delete V;
         return set_err(BM_ERR_CUDA, "cudaEventCreate");
     }
@@ -423,6 +431,7 @@ int bm_server_destroy(bm_server V) {
     if (V->d_out) cudaFree(V->d_out);
     if (V->d_outjobs) cudaFree(V->d_outjobs);
     bm_ctx_destroy(V->setup);
+    ctx_release(V->ctx);
     delete V;
     return BM_OK;
 }

@@ -325,6 +325,10 @@ const char* bm_version(void);
 
 /* Creates a context on CUDA device `device` (Cortex::new, src/cortex/cortex.rs:51-61). */
 int bm_ctx_create(int device, uint32_t flags, bm_ctx* out);
+/* Releases the caller's handle. Areas, batches, servers and writers made on
+ * the context hold it too, so it may be destroyed before them (as a garbage
+ * collector may order it): it is freed with the last of them. The handle
+ * must not be used after this call. */
 int bm_ctx_destroy(bm_ctx ctx);
 /* Issues all subsequent work of areas created from ctx on `stream` (a
  * cudaStream_t passed as void*; NULL is the CUDA legacy default stream).
@@ -562,11 +566,16 @@ int bm_batch_reset_profile(bm_batch batch);
 /* OR of the areas' sticky device error bits; BM_ERR_TIMEOUT when any is set. */
 int bm_batch_device_errors(bm_batch batch, uint32_t* bits);
 
-/* Chooses the tile size of each batched tuft step by timing candidates on the
- * batch itself (the buffers the trials write are saved and restored, so the
- * areas' state is unchanged). With a non-NULL cache_path, choices already in
- * that file are applied without timing and new ones are added to it.
- * *n_tuned (optional) = steps tuned. Synchronous. */
+/* Chooses, for each batched tuft step, the tile size (4K..128K synapses per
+ * tile) and the footprint form (a tensor box load, or staged by the
+ * consumers), then for those tiles the ring's depth (2..4 shared-memory
+ * stages) and the resident CTAs per SM of the persistent grid, by timing
+ * candidates on the batch itself (the buffers the trials write are saved and
+ * restored, so the areas' state is unchanged). With a non-NULL cache_path,
+ * choices already in that file are applied without timing and new ones are
+ * added to it (one line per step: key, tile target, stages, CTAs per SM,
+ * staged footprints; 0 = the default). *n_tuned (optional) = steps tuned.
+ * Synchronous. */
 int bm_batch_autotune(bm_batch batch, const char* cache_path, uint32_t* n_tuned);
 
 /* One tuft's stage of a cycle -- synapse flags, synapse cycle, dendrite cycle,

@@ -158,8 +158,10 @@ def test_batch_autotune_keeps_state_and_parity(tmp_path):
     assert n >= 1
     for a, s in zip(batched, before):
         assert np.array_equal(a.read_slab(), s), "autotune changed an area's state"
-    lines = open(cache).read().split("\n")
-    assert any(l.strip() for l in lines)
+    rows = [l.split() for l in open(cache).read().split("\n") if l.strip()]
+    assert rows and all(len(r) == 5 for r in rows), rows   # key, tile target, stages, CTAs per SM, staged
+    assert all(int(r[1]) >= 4096 and int(r[2]) in (0, 2, 3) and int(r[3]) in (0, 1, 2) and int(r[4]) in (0, 1)
+               for r in rows), rows
     assert batch.autotune(cache) == n   # applied from the cache
     fr = [_frames(a, 4, 90 + k) for k, a in enumerate(batched)]
     for c in range(4):
@@ -169,6 +171,48 @@ def test_batch_autotune_keeps_state_and_parity(tmp_path):
             alone[k].cycle(1)
         batch.cycle(1)
     _check_equal(batched, alone, "after autotune")
+    batch.close()
+    for a in batched + alone:
+        a.close()
+    ctx.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("stages,ctas,staged", [(2, 1, 0), (3, 2, 1), (2, 0, 1), (0, 1, 0)])
+def test_batch_launch_shapes_from_cache(tmp_path, stages, ctas, staged):
+    """Every launch shape the autotuner may choose (ring stages, CTAs per SM,
+    footprint form) leaves the batched areas equal to cycling alone: the
+    shapes are forced through a cache file written with the tuned keys."""
+    ctx = cortex._Ctx(0)
+    descs = [_desc(*s) for s in SMALL] + [_deep_desc(64)]
+    batched, alone = _pairs(ctx, descs, seed=31)
+    batch = cortex.Batch(ctx, batched)
+    cache = str(tmp_path / "tiles.txt")
+    batch.autotune(cache)
+    rows = [l.split() for l in open(cache).read().split("\n") if l.strip()]
+    assert rows
+    with open(cache, "w") as f:
+        for r in rows:
+            f.write("%s %s %d %d %d\n" % (r[0], r[1], stages, ctas, staged))
+    batch.close()
+    for a in batched:   # autotuning restored the state it touched
+        a.set_cycle(0)
+    batch = cortex.Batch(ctx, batched)
+    assert batch.autotune(cache) == len(rows)
+    tma = {area.tuft_form(i, t)["footprint_tma"] for area in batched for i in range(area.plan.n_layers)
+           for t in range(area.plan.layers[i].n_tufts) if area.tuft_form(i, t)["tiled"]}
+    # Side 40 rows are not a multiple of 16 bytes: with tensor boxes allowed,
+    # one launch mixes boxed and staged footprints.
+    assert tma == ({False} if staged else {False, True}), tma
+    fr = [_frames(a, 3, 70 + k) for k, a in enumerate(batched)]
+    for c in range(3):
+        for k in range(len(batched)):
+            batched[k].write_input(fr[k][c])
+            alone[k].write_input(fr[k][c])
+            alone[k].cycle(1)
+        batch.cycle(1)
+        _check_equal(batched, alone, "stages %d, CTAs per SM %d, staged %d, cycle %d" % (stages, ctas, staged, c))
+    assert batch.device_errors() == 0
     batch.close()
     for a in batched + alone:
         a.close()

@@ -55,7 +55,7 @@ def test_cpp_builders_resolve_the_python_descriptors(exe, tmp_path):
 
 @pytest.mark.gpu
 def test_cpp_cortex_matches_oracle(exe, tmp_path):
-    from test_hierarchy import _oracle_cycle
+    from helpers import oracle_cortex_cycle
     lmaps, areas, names = configs.hierarchy(SIDES)
     n = 5
     frames = configs.frames(n, SIDES[0] ** 2, 0.02, 8)
@@ -75,7 +75,7 @@ def test_cpp_cortex_matches_oracle(exe, tmp_path):
         assert np.array_equal(ref, s), "growth of %s" % names[k]
     tracts, _ext = M.area_tracts(lmaps, areas, names, plans)
     for c in range(n):
-        _oracle_cycle(plans, slabs, tracts, frames[c], c)
+        oracle_cortex_cycle(plans, slabs, tracts, frames[c], c)
     for k, nm in enumerate(names):
         dev = np.fromfile(str(tmp_path / ("final_%s.bin" % nm)), np.uint8)
         assert np.array_equal(dev, slabs[k]), nm
