@@ -691,7 +691,8 @@ def run_serving(args, ctx):
         "value": st["syn_cycles"] / st["span_s"] if st["span_s"] else None, "unit": UNIT,
         "p50_ms": round(st["p50_ms"], 3), "p99_ms": round(st["p99_ms"], 3), "mean_ms": round(st["mean_ms"], 3),
         "ticks": int(st["ticks"]), "batch_rebuilds": int(st["batch_rebuilds"]),
-        "rebuild_s": round(st["rebuild_s"], 3), "admit_s": round(st["admit_s"], 3), "gpu_s": round(st["gpu_s"], 3),
+        "rebuild_s": round(st["rebuild_s"], 3), "rebuild_drains": st["rebuild_drains"],
+        "capture_s": round(st["capture_s"], 3), "admit_s": round(st["admit_s"], 3), "gpu_s": round(st["gpu_s"], 3),
         "tick_call_s": round(t_tick, 3), "submit_s": round(t_submit, 3), "wall_s": round(wall, 3),
         "latency": "per frame: tick completion minus the moment the frame was ready (its session's previous "
                    "frame done, or its arrival); admission waits included",

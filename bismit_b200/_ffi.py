@@ -178,7 +178,8 @@ class bm_server_stats(C.Structure):
                 ("admit_s", C.c_double), ("gpu_s", C.c_double), ("span_s", C.c_double),
                 ("p50_ms", C.c_double), ("p99_ms", C.c_double), ("mean_ms", C.c_double),
                 ("used_bytes", C.c_uint64), ("budget_bytes", C.c_uint64),
-                ("resident", C.c_uint32), ("waiting", C.c_uint32), ("failed", C.c_uint32)]
+                ("resident", C.c_uint32), ("waiting", C.c_uint32), ("failed", C.c_uint32),
+                ("rebuild_drains", C.c_uint64), ("capture_s", C.c_double)]
 
 
 class bm_tuft_form(C.Structure):

@@ -167,7 +167,7 @@ struct bm_area_s {
     // pool (written by the caller), so its steps may read any axon slice.
     uint8_t foreign_src[BM_MAX_LAYERS] = {};
     uint32_t access_version = 0;   // bumped whenever foreign_src changes
-    uint32_t n_batches = 0;  // batches holding this area (its tiles are retiled only when one does)
+    std::atomic<uint32_t> n_batches{0};   // batches holding this area (its tiles are retiled only when one does)
     std::vector<bm_batch_s*> batches;   // the batches holding it (detached when it is destroyed)
     // Regrowth (absent when disabled): one job per (data layer, tuft), layers
     // in cycle order, block0 counted within the area's own launch.

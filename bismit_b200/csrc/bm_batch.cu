@@ -26,6 +26,7 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <new>
 #include <string>
 #include <vector>
@@ -265,9 +266,15 @@ struct bm_batch_s {
     }
 };
 
+// The links between areas and the batches holding them (bm_area_s::batches
+// and n_batches). A batch may be destroyed on another thread than the one
+// creating the next batch over the same areas (a server's builder thread).
+static std::mutex g_links;
+
 // An area being destroyed leaves every batch holding it: the batch keeps
 // nothing that points into the area and will not cycle again.
 void bm::detach_from_batches(bm_area_s* A) {
+    std::lock_guard<std::mutex> lk(g_links);
     for (bm_batch_s* B : A->batches) {
         DevGuard g(B->ctx->device);
         cudaStreamSynchronize(B->stream());
@@ -295,10 +302,13 @@ void free_batch(bm_batch_s* B) {
     if (!B) return;
     DevGuard g(B->ctx->device);
     // Areas destroyed before the batch were detached (their entries are null).
-    for (bm_area A : B->areas) {
-        if (!A) continue;
-        if (A->n_batches) A->n_batches--;
-        A->batches.erase(std::remove(A->batches.begin(), A->batches.end(), B), A->batches.end());
+    {
+        std::lock_guard<std::mutex> lk(g_links);
+        for (bm_area A : B->areas) {
+            if (!A) continue;
+            if (A->n_batches) A->n_batches--;
+            A->batches.erase(std::remove(A->batches.begin(), A->batches.end(), B), A->batches.end());
+        }
     }
     B->drop_graph();
     free_plan(B);
@@ -905,9 +915,12 @@ int bm_batch_create(bm_ctx ctx, const bm_area* areas, uint32_t n_areas, bm_batch
     B->ctx = ctx;
     ctx_retain(ctx);
     B->areas.assign(areas, areas + n_areas);
-    for (bm_area A : B->areas) {
-        A->n_batches++;
-        A->batches.push_back(B);
+    {
+        std::lock_guard<std::mutex> lk(g_links);
+        for (bm_area A : B->areas) {
+            A->n_batches++;
+            A->batches.push_back(B);
+        }
     }
     cudaError_t e = cudaStreamCreateWithFlags(&B->cap, cudaStreamNonBlocking);
     if (e != cudaSuccess) { free_batch(B); return cuda_err(e, "cudaStreamCreate"); }

@@ -161,8 +161,10 @@ struct bm_server_s {
     // Statistics.
     std::vector<float> lat_ms;
     uint64_t ticks = 0, frames_cycled = 0, rebuilds = 0;
+    uint64_t rebuild_drains = 0;         // rebuilds that waited for the queued ticks (staging blocks grew)
     double syn_cycles = 0, busy_s = 0, first_tick = 0, last_tick = 0;
     double rebuild_s = 0;                // host time in batch rebuilds
+    double capture_s = 0;                // host time of the ticks that captured a batch's CUDA graph
     std::atomic<double> admit_s{0};      // builder-thread time in admissions
     double gpu_s = 0;                    // device time of the ticks (frames in to outputs out)
     // The builder thread and its queues (guarded by mu).
@@ -171,11 +173,16 @@ struct bm_server_s {
     std::condition_variable cv;
     bool stop = false;
     std::deque<Session*> build_q;        // admitted sessions whose areas the builder builds
+    // What the builder releases, in queue order: a retired batch (after the
+    // ticks queued with it), a device buffer (likewise), a retired session's
+    // area and output buffer. A session's batches are queued before its area.
     struct Teardown {
-        bm_area area;
-        uint8_t* out;
+        bm_area area = nullptr;
+        uint8_t* out = nullptr;
+        bm_batch batch = nullptr;
+        void* dev = nullptr;
     };
-    std::deque<Teardown> free_q;         // retired sessions' areas and output buffers
+    std::deque<Teardown> free_q;
 
     Session* find(uint32_t id) {
         for (Session* s : sessions)
@@ -218,6 +225,11 @@ void builder_loop(bm_server_s* V, int device) {
             const bm_server_s::Teardown T = V->free_q.front();
             V->free_q.pop_front();
             lk.unlock();
+            if (T.batch) bm_batch_destroy(T.batch);   // waits for the serving stream first
+            if (T.dev) {
+                cudaStreamSynchronize(V->ctx->stream());
+                cudaFree(T.dev);
+            }
             if (T.area) bm_area_destroy(T.area);
             if (T.out) cudaFreeHost(T.out);
             lk.lock();
@@ -268,6 +280,14 @@ void adopt(bm_server_s* V, bm_server_s::Session* S) {
     S->admitted = now_s();
 }
 
+void hand_to_builder(bm_server_s* V, const bm_server_s::Teardown& T) {
+    {
+        std::lock_guard<std::mutex> g(V->mu);
+        V->free_q.push_back(T);
+    }
+    V->cv.notify_one();
+}
+
 // Releases S's budget and hands its area and output buffer to the builder
 // thread for teardown.
 void retire(bm_server_s* V, bm_server_s::Session* S) {
@@ -275,18 +295,30 @@ void retire(bm_server_s* V, bm_server_s::Session* S) {
     S->resident = false;
     S->retired = true;
     if (S->area || S->out) {
-        {
-            std::lock_guard<std::mutex> g(V->mu);
-            V->free_q.push_back({S->area, S->out});
-        }
-        V->cv.notify_one();
+        bm_server_s::Teardown T;
+        T.area = S->area;
+        T.out = S->out;
+        hand_to_builder(V, T);
     }
     S->area = nullptr;
     S->out = nullptr;
 }
 
-// Grows a pair of pinned blocks and their device block (the stream must be
-// idle: callers only grow right after a batch rebuild, which synchronises).
+// The current batch leaves the ticks: the builder destroys it once the ticks
+// queued with it are done, so the tick thread does not wait for them.
+void retire_batch(bm_server_s* V) {
+    if (V->batch) {
+        bm_server_s::Teardown T;
+        T.batch = V->batch;
+        hand_to_builder(V, T);
+    }
+    V->batch = nullptr;
+    V->members.clear();
+}
+
+// Grows a pair of pinned blocks and their device block, by half again what
+// is asked for (the stream must be idle: callers complete the queued ticks
+// before a growth).
 int ensure_blocks(uint8_t* (&h)[2], uint8_t*& d, uint64_t& cap, uint64_t bytes, const char* what) {
     if (bytes <= cap) return BM_OK;
     for (auto& p : h)
@@ -295,7 +327,7 @@ int ensure_blocks(uint8_t* (&h)[2], uint8_t*& d, uint64_t& cap, uint64_t bytes, 
     h[0] = h[1] = nullptr;
     d = nullptr;
     cap = 0;
-    uint64_t c = std::max<uint64_t>(bytes, 1 << 20);
+    uint64_t c = std::max<uint64_t>(bytes + bytes / 2, 1 << 20);
     if (cudaHostAlloc(&h[0], c, cudaHostAllocDefault) != cudaSuccess ||
         cudaHostAlloc(&h[1], c, cudaHostAllocDefault) != cudaSuccess || cudaMalloc(&d, c) != cudaSuccess) {
         cudaGetLastError();
@@ -346,9 +378,15 @@ int complete_all(bm_server_s* V) {
     return rc;
 }
 
-// Output gather of the current batch's members, packed in batch order.
+// Output gather of the current batch's members, packed in batch order. The
+// previous gather table may still be read by a queued tick: the builder frees
+// it after that.
 int build_outjobs(bm_server_s* V) {
-    if (V->d_outjobs) cudaFree(V->d_outjobs);
+    if (V->d_outjobs) {
+        bm_server_s::Teardown T;
+        T.dev = V->d_outjobs;
+        hand_to_builder(V, T);
+    }
     V->d_outjobs = nullptr;
     std::vector<OutJob> jobs;
     uint64_t blocks = 0, o = 0;
@@ -364,6 +402,11 @@ int build_outjobs(bm_server_s* V) {
     }
     V->out_blocks = (uint32_t)blocks;
     V->out_bytes = o;
+    if (o > V->out_cap) {
+        int rc = complete_all(V);
+        if (rc != BM_OK) return rc;
+        V->rebuild_drains++;
+    }
     int rc = ensure_blocks(V->h_out, V->d_out, V->out_cap, o, "output");
     if (rc != BM_OK) return rc;
     cudaError_t e = cudaMalloc(&V->d_outjobs, jobs.size() * sizeof(OutJob));
@@ -535,11 +578,7 @@ int bm_server_tick(bm_server V, uint32_t* n_cycled) {
     for (auto* S : V->sessions) {
         if (!S->closing || !S->frames.empty() || S->inflight) continue;
         if (S->build.load(std::memory_order_acquire) == bm_server_s::kQueued) continue;
-        if (std::find(V->members.begin(), V->members.end(), S) != V->members.end()) {
-            if (V->batch) bm_batch_destroy(V->batch);
-            V->batch = nullptr;
-            V->members.clear();
-        }
+        if (std::find(V->members.begin(), V->members.end(), S) != V->members.end()) retire_batch(V);
         retire(V, S);
     }
     std::vector<bm_server_s::Session*> live;
@@ -572,17 +611,14 @@ int bm_server_tick(bm_server V, uint32_t* n_cycled) {
     const uint32_t slot = (uint32_t)(V->tick_no & 1);
     if (!m.empty()) {
         if (m != V->members || !V->batch) {
-            // The previous tick completes first: its outputs sit in the pinned
-            // blocks that a rebuild may reallocate.
+            // A new batch for the new membership; the previous tick stays
+            // queued (its batch and gather table are released behind it),
+            // unless a staging block must grow.
             const double r0 = now_s();
-            int rc = complete_all(V);
-            if (rc != BM_OK) return rc;
-            if (V->batch) bm_batch_destroy(V->batch);
-            V->batch = nullptr;
-            V->members.clear();
+            retire_batch(V);
             std::vector<bm_area> areas;
             for (auto* S : m) areas.push_back(S->area);
-            rc = bm_batch_create(V->ctx, areas.data(), (uint32_t)areas.size(), &V->batch);
+            int rc = bm_batch_create(V->ctx, areas.data(), (uint32_t)areas.size(), &V->batch);
             if (rc == BM_OK) rc = bm_batch_set_graph(V->batch, 0);
             if (rc != BM_OK) return rc;
             V->same_ticks = 0;
@@ -590,6 +626,11 @@ int bm_server_tick(bm_server V, uint32_t* n_cycled) {
             V->rebuilds++;
             uint64_t fb = 0;
             bm_batch_frame_bytes(V->batch, &fb);
+            if (fb > V->frames_cap) {
+                rc = complete_all(V);
+                if (rc != BM_OK) return rc;
+                V->rebuild_drains++;
+            }
             rc = ensure_blocks(V->h_frames, V->d_frames, V->frames_cap, fb, "frame");
             if (rc == BM_OK) rc = build_outjobs(V);
             if (rc != BM_OK) return rc;
@@ -615,12 +656,15 @@ int bm_server_tick(bm_server V, uint32_t* n_cycled) {
         cudaError_t e = cudaEventRecord(V->start_ev[slot], s);
         if (e == cudaSuccess) e = cudaMemcpyAsync(V->d_frames, V->h_frames[slot], o, cudaMemcpyHostToDevice, s);
         if (e != cudaSuccess) return cuda_err(e, "frame block copy");
-        if (++V->same_ticks == bm_server_s::kGraphAfter) {
+        const bool capture = ++V->same_ticks == bm_server_s::kGraphAfter;
+        const double c0 = capture ? now_s() : 0.0;
+        if (capture) {
             int rc = bm_batch_set_graph(V->batch, 1);
             if (rc != BM_OK) return rc;
         }
         int rc = batch_cycle_frames_unchecked(V->batch, V->d_frames);
         if (rc != BM_OK) return rc;
+        if (capture) V->capture_s += now_s() - c0;
         if (V->out_blocks) k_gather_outputs<<<V->out_blocks, kGatherBlock, 0, s>>>(V->d_outjobs, (uint32_t)m.size(), V->d_out);
         e = cudaMemcpyAsync(V->h_out[slot], V->d_out, V->out_bytes, cudaMemcpyDeviceToHost, s);
         if (e == cudaSuccess) e = cudaEventRecord(V->done_ev[slot], s);
@@ -681,6 +725,8 @@ int bm_server_get_stats(bm_server V, bm_server_stats* st) {
     st->busy_s = V->busy_s;
     st->span_s = V->last_tick > V->first_tick ? V->last_tick - V->first_tick : 0;
     st->rebuild_s = V->rebuild_s;
+    st->rebuild_drains = V->rebuild_drains;
+    st->capture_s = V->capture_s;
     st->gpu_s = V->gpu_s;
     st->admit_s = V->admit_s.load();
     st->used_bytes = V->used;
@@ -709,8 +755,8 @@ int bm_server_get_stats(bm_server V, bm_server_stats* st) {
 int bm_server_reset_stats(bm_server V) {
     if (!V) return set_err(BM_ERR_INVALID, "null server");
     V->lat_ms.clear();
-    V->ticks = V->frames_cycled = V->rebuilds = 0;
-    V->syn_cycles = V->busy_s = V->first_tick = V->last_tick = V->rebuild_s = V->gpu_s = 0;
+    V->ticks = V->frames_cycled = V->rebuilds = V->rebuild_drains = 0;
+    V->syn_cycles = V->busy_s = V->first_tick = V->last_tick = V->rebuild_s = V->gpu_s = V->capture_s = 0;
     V->admit_s.store(0);
     return BM_OK;
 }

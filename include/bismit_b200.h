@@ -647,6 +647,12 @@ typedef struct bm_server_stats {
     uint64_t used_bytes, budget_bytes;
     uint32_t resident, waiting;
     uint32_t failed;              /* sessions dropped after a device error       */
+    uint64_t rebuild_drains;      /* rebuilds that waited for the queued ticks
+                                     (a staging block grew)                      */
+    double   capture_s;           /* host time of the ticks that captured a
+                                     batch's CUDA graph (a batch cycles by plain
+                                     launches until its membership has held for
+                                     8 ticks)                                    */
 } bm_server_stats;
 
 /* mem_budget 0: 90 % of the device memory free at creation. */
