@@ -935,7 +935,7 @@ def run_profile(args):
 
         def cycles(c0, n):
             areas[0].cycle_frames_device(dev.data_ptr() + c0 * flen, flen, n)
-        launches = areas[0].launches_per_cycle()
+        launches = areas[0].launches_per_cycle
         name = args.workload
     else:
         frames_h = []
@@ -951,7 +951,7 @@ def run_profile(args):
 
         def cycles(c0, n):
             batch.cycle_frames_device(dev.data_ptr() + c0 * fb, n)
-        launches = batch.launches_per_cycle()
+        launches = batch.launches_per_cycle
         name = "batch_%d" % args.batch_instances
     torch.cuda.synchronize()
     cycles(0, W)
@@ -963,7 +963,7 @@ def run_profile(args):
     e1.record(stream)
     torch.cuda.synchronize()
     n_syn = sum(int(a.plan.n_syns_total) for a in areas)
-    print(json.dumps({"profile_run": name, "steps": K, "warmup": W, "launches_per_cycle": launches,
+    print(json.dumps({"profile_run": name, "steps": K, "warmup": W, "launches_per_cycle": launches(),
                       "synapses": n_syn, "ms_per_cycle": e0.elapsed_time(e1) / K}), flush=True)
     if args.profile_run == "batched":
         batch.close()
