@@ -54,6 +54,9 @@ def parse():
                     help="only W warm-up and K timed cycles of the workload (area: --workload through the plain "
                          "cycling call; batched: the --batch-instances batch, autotuned, graph replay), no soak, "
                          "arms or baselines: a short launch sequence for a profiler's launch list")
+    ap.add_argument("--autotune-cache", default=None,
+                    help="--profile-run batched: the autotuner's cache file (choices found there are applied "
+                         "without trial launches; new ones are added)")
     return ap.parse_args()
 
 
@@ -945,7 +948,7 @@ def run_profile(args):
             areas.append(cortex.CorticalArea(ctx, M.area_desc("v1", lmaps, ar, configs.bench_settings()), seed))
             frames_h.append(configs.frames(K + W, areas[-1].input_len(), act, seed))
         batch = cortex.Batch(ctx, areas)
-        batch.autotune(None)
+        batch.autotune(args.autotune_cache)
         fb = batch.frame_bytes()
         dev = torch.from_numpy(batch.pack_frames(frames_h)).to("cuda")
 

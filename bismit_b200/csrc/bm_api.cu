@@ -119,7 +119,7 @@ bool layer_plain(const bm_area_plan& P, uint32_t i) {
 
 // Fused forms of adjacent steps whose later stages only read what the earlier
 // ones wrote for the same cell (bm_items.cuh).
-void fuse_steps(const bm_area_s* A, std::vector<Step>& v) {
+void fuse_steps(const bm_area_s* A, std::vector<Step>& v, bool fold_cell_tufts) {
     const bm_area_plan& P = A->plan;
     std::vector<Step> out;
     for (size_t k = 0; k < v.size(); k++) {
@@ -167,7 +167,7 @@ void fuse_steps(const bm_area_s* A, std::vector<Step>& v) {
                 // no axon: they fold into the tail, each cell's four stages
                 // ahead of its soma.
                 uint8_t tufts = 0;
-                for (size_t q = out.size(); q > 0; q--) {
+                for (size_t q = out.size(); q > 0 && fold_cell_tufts; q--) {
                     const Step& o = out[q - 1];
                     if (o.kind != ST_TUFT || o.layer != s.layer) break;
                     if (!A->fused.t[s.layer][o.idx].ok && o.idx < 8) tufts |= (uint8_t)(1u << o.idx);
@@ -197,7 +197,19 @@ void fuse_steps(const bm_area_s* A, std::vector<Step>& v) {
 // before the cycle; output is read on demand), with CorticalArea::regrow
 // (src/cortex/cortical_area.rs:792-806) as a step of every cycle that acts on
 // the cycles its counter fires.
-void bm::area_steps(const bm_area_s* A, std::vector<Step>& out) {
+uint64_t bm::cell_tuft_cells(const bm_area_s* A) {
+    const bm_area_plan& P = A->plan;
+    uint64_t n = 0;
+    for (uint32_t i = 0; i < P.n_layers; i++) {
+        if (P.layers[i].kind != BM_LYR_PYRAMIDAL) continue;
+        bool cell_tuft = false;
+        for (uint32_t t = 0; t < P.layers[i].n_tufts; t++) cell_tuft |= !A->fused.t[i][t].ok;
+        if (cell_tuft) n += P.layers[i].cells;
+    }
+    return n;
+}
+
+void bm::area_steps(const bm_area_s* A, std::vector<Step>& out, bool fold_cell_tufts) {
     const bm_area_plan& P = A->plan;
     out.clear();
     // AxonSpace::intake (src/cortex/axon_space.rs:510-525): each filtered
@@ -216,7 +228,7 @@ void bm::area_steps(const bm_area_s* A, std::vector<Step>& out) {
     }
     if (A->regrow_blocks) out.push_back({ST_REGROW, 0, 0, 0});
     out.push_back({ST_CYCLE_END, 0, 0, 0});
-    if (A->exec_path == BM_PATH_FUSED) fuse_steps(A, out);
+    if (A->exec_path == BM_PATH_FUSED) fuse_steps(A, out, fold_cell_tufts);
 }
 
 // Synapse flags, synapse cycle, dendrite cycle and (pyramidal) tuft cycle: the
@@ -458,16 +470,17 @@ int bm::schedule_area(bm_area_s* A) {
             if (A->step_side[j] && conflict(acc[j], acc[k])) A->step_waits[k].push_back(j);
     }
     // The cycle-end launch folds into a final pyramidal tail on the main
-    // stream that every side step has joined (so no step of the cycle reads
-    // the cycle number after it advances).
+    // stream once every side step has joined the main stream by then (so no
+    // step of the cycle reads the cycle number after it advances). The side
+    // stream runs its steps in order, so a main step's wait for side step j
+    // joins every side step up to j.
     A->end_in_tail = false;
     if (n >= 2 && A->steps[n - 1].kind == ST_CYCLE_END && A->steps[n - 2].kind == ST_PYR_TAIL && !A->step_side[n - 2]) {
-        bool joined = true;
-        for (size_t j = 0; j + 2 < n && joined; j++)
-            if (A->step_side[j])
-                joined = std::find(A->step_waits[n - 2].begin(), A->step_waits[n - 2].end(), j) !=
-                         A->step_waits[n - 2].end();
-        A->end_in_tail = joined;
+        size_t joined = 0;   // side steps below this index have joined
+        for (size_t k = 0; k + 1 < n; k++)
+            if (!A->step_side[k])
+                for (size_t j : A->step_waits[k]) joined = std::max(joined, j + 1);
+        A->end_in_tail = A->last_side == SIZE_MAX || A->last_side < joined;
     }
     for (cudaEvent_t ev : A->side_ev)
         if (ev) cudaEventDestroy(ev);
@@ -958,7 +971,7 @@ int bm_area_create(bm_ctx ctx, const bm_area_desc* desc, uint64_t seed, bm_area*
         }
     }
     for (uint32_t i = 0; i < A->plan.n_layers; i++) A->verify_pending[i] = true;
-    area_steps(A, A->steps);
+    area_steps(A, A->steps, cell_tuft_cells(A) <= kFoldCellTufts);
     rc = schedule_area(A);
     if (rc != BM_OK) { free_area(A); return rc; }
     *out = A;

@@ -223,7 +223,16 @@ struct bm_area_s {
 namespace bm {
 
 // The steps of one cycle of A (CorticalArea::cycle order).
-void area_steps(const bm_area_s* A, std::vector<Step>& out);
+// `fold_cell_tufts`: per-cell tuft steps of a pyramidal layer fold into its
+// tail (one launch fewer; worth it while that work is small, see
+// kFoldCellTufts), else they stay steps of their own.
+void area_steps(const bm_area_s* A, std::vector<Step>& out, bool fold_cell_tufts);
+// Cells of the pyramidal layers with per-cell (unfused) tufts: up to this many
+// (over an area, or over a batch's areas) those tufts fold into the tail.
+// Beyond it they stay a step of their own, which overlaps a side-stream tuft
+// step where the tail, after the streams join, would not.
+constexpr uint64_t kFoldCellTufts = 16384;
+uint64_t cell_tuft_cells(const bm_area_s* A);
 // Enqueues one step of A on stream s (a pyramidal tail with end_cycle also
 // ends the cycle).
 void exec_step(bm_area_s* A, const Step& st, cudaStream_t s, bool end_cycle = false);

@@ -581,14 +581,20 @@ int schedule_side(bm_batch_s* B) {
 // cycle-end step is done once for the whole batch.
 int build_plan(bm_batch_s* B) {
     free_plan(B);
+    // Each area's program, with per-cell tufts folded into the tails only
+    // while the batch's cells with such tufts stay within kFoldCellTufts.
+    uint64_t cells = 0;
+    for (bm_area A : B->areas) cells += cell_tuft_cells(A);
+    std::vector<std::vector<Step>> progs(B->areas.size());
+    for (size_t a = 0; a < B->areas.size(); a++) area_steps(B->areas[a], progs[a], cells <= kFoldCellTufts);
     std::vector<Step> U;
     std::vector<std::vector<uint32_t>> who;   // who[k]: areas (batch indices) having U[k]
     for (uint32_t a = 0; a < B->areas.size(); a++) {
-        const std::vector<Step>& P = B->areas[a]->steps;
+        const std::vector<Step>& P = progs[a];
         // Same program as an earlier area: its positions in U are known.
         bool placed = false;
         for (uint32_t b = 0; b < a && !placed; b++) {
-            if (!(B->areas[b]->steps == P)) continue;
+            if (!(progs[b] == P)) continue;
             for (auto& w : who)
                 if (std::find(w.begin(), w.end(), b) != w.end()) w.push_back(a);
             placed = true;

@@ -174,22 +174,30 @@ __device__ __forceinline__ uint64_t global_ns() {
     asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
     return t;
 }
-// Bounded wait: false once `limit_ns` of wall time have passed without the
-// phase completing (and in any case after kWaitLimit suspended tries).
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, uint64_t limit_ns) {
+// Bounded wait: false once `limit_us` microseconds of wall time have passed
+// without the phase completing (and in any case after kWaitLimit suspended
+// tries).
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, uint32_t limit_us) {
     if (mbar_try_wait(bar, parity)) return true;
     const uint64_t t0 = global_ns();
     for (uint32_t i = 0; i < kWaitLimit; i++) {
         if (mbar_try_wait_sleep(bar, parity, 200000u)) return true;
-        if (global_ns() - t0 > limit_ns) return false;
+        if (global_ns() - t0 > 1000ull * limit_us) return false;
     }
     return false;
 }
-// The wait limit of an area's tuft launches (AreaCtl::wait_us; 0: the default).
-__device__ __forceinline__ uint64_t wait_limit_ns(const AreaCtl* ctl) {
+// The wait limit of an area's tuft launches, us (AreaCtl::wait_us; 0: the
+// default).
+__device__ __forceinline__ uint32_t wait_limit_us(const AreaCtl* ctl) {
     const unsigned int us = ctl ? ctl->wait_us : 0u;
-    return 1000ull * (us ? us : kDefaultWaitUs);
+    return us ? us : kDefaultWaitUs;
 }
+
+// A consumer warp's ring position and hand-over parities, in one word (it is
+// carried across every tile and stage): bits 0-2 the ring buffer, bit 3 the
+// ring's phase, bit 4 the footprint box's phase, bit 5 the pair hand-over's
+// phase, bit 6 set once a pair hand-over happened.
+constexpr uint32_t kRingBuf = 7u, kRingPhase = 8u, kFpPhase = 16u, kPairPhase = 32u, kPairSeen = 64u;
 // 1-D bulk copy global -> shared completing on `bar` (16-byte aligned, size % 16 == 0).
 __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
     asm volatile(
@@ -681,13 +689,13 @@ __device__ __forceinline__ void tma_stage(const FusedTuftArgs& A, const TileGeo&
 // tma_stage + finish_chunk compute for that case, with every loop bound,
 // shift and branch on the shape resolved by the compiler.
 // Shapes: 1 (spd 32, S 32), 2 (64, 64), 3 (16, 128), 4 (16, 256), 5 (32, 256),
-// 6 (32, 512), 7 (64, 512).
-constexpr int kGeoms = 8;
+// 6 (32, 512), 7 (64, 512), 8 (64, 1024: a cell spans a pair of warps).
+constexpr int kGeoms = 9;
 __host__ __device__ constexpr int geom_spd_l2(int g) {
     return g == 1 ? 5 : g == 2 ? 6 : g == 3 ? 4 : g == 4 ? 4 : g == 5 ? 5 : g == 6 ? 5 : 6;
 }
 __host__ __device__ constexpr int geom_lpc_l2(int g) {
-    return g == 1 ? 1 : g == 2 ? 2 : g == 3 ? 3 : g == 4 ? 4 : g == 5 ? 4 : 5;
+    return g == 1 ? 1 : g == 2 ? 2 : g == 3 ? 3 : g == 4 ? 4 : g == 5 ? 4 : g == 8 ? 6 : 5;
 }
 
 }  // namespace
@@ -697,7 +705,7 @@ __host__ __device__ constexpr int geom_lpc_l2(int g) {
 // consumer) otherwise. It applies while the tuft's flags are clean and its
 // sources lie in the footprint.
 uint32_t consumer_shape(const FusedTuft& FT, uint32_t spt, uint32_t spd, bool pyramidal) {
-    if (!FT.tiled || !FT.win || spt > 512 || FT.stage_bytes != (uint32_t)kWarps * 512) return 0;
+    if (!FT.tiled || !FT.win || spt > 1024 || FT.stage_bytes != (uint32_t)kWarps * 512) return 0;
     for (int g = 1; g < kGeoms; g++)
         if ((1u << geom_spd_l2(g)) == spd && (1u << (geom_lpc_l2(g) + 4)) == spt)
             return (pyramidal ? g >= 3 : g <= 2) ? (uint32_t)g : 0u;
@@ -706,22 +714,46 @@ uint32_t consumer_shape(const FusedTuft& FT, uint32_t spt, uint32_t spd, bool py
 
 namespace {
 
+__device__ __forceinline__ void raise_abort(volatile int& s_abort, AreaCtl* ctl);
+
+// Hand-over between the two warps of a pair that share a cell of 1024
+// synapses: per pair, an mbarrier the odd warp arrives on once its half's
+// key, best and total are written, one the even warp arrives on once it took
+// them, and the three words.
+__device__ __forceinline__ uint64_t* pair_bars() {
+    __shared__ uint64_t bars[kWarps];
+    return bars;
+}
+__device__ __forceinline__ uint32_t* pair_words() {
+    __shared__ uint32_t words[kWarps / 2][4];
+    return &words[0][0];
+}
+
 template <bool TUFT, int SPD_L2, int LPC_L2>
 __device__ __forceinline__ void stage_fast(const FusedTuftArgs& A, const TileGeo& G, const uint8_t* halo,
-                                           const uint8_t* sb, uint32_t pos, int lane, int wib, int32_t rnd) {
+                                           const uint8_t* sb, uint32_t pos, int lane, int wib, int32_t rnd,
+                                           uint32_t& ring, uint32_t limit_us, volatile int& s_abort) {
     constexpr uint32_t SB = kWarps * 512;
     constexpr uint32_t WIN = SB / 16 + 32;
     constexpr uint32_t LPD = 1u << (SPD_L2 - 4);
     constexpr uint32_t LPC = 1u << LPC_L2;
     constexpr uint32_t S_L2 = LPC_L2 + 4;
+    // A cell of 1024 synapses spans a pair of warps (2k, 2k + 1): each reduces
+    // its half, the odd warp hands its key, best and total to the even one
+    // through shared memory, and the even warp writes the cell-tuft fields.
+    // Stages and tiles hold whole cells, so both warps of a pair take part in
+    // a stage or neither does.
+    constexpr bool PAIR = LPC_L2 == 6;
+    constexpr uint32_t LPCW = PAIR ? 32u : LPC;   // lanes of a cell within one warp
     static_assert(LPC >= LPD, "a cell holds whole dendrites");
+    const bool cell_warp = !PAIR || (wib & 1) == 0;   // the warp that writes the cell-tuft fields
     const uint32_t unit0 = pos + (uint32_t)wib * 512;
     if (unit0 >= G.syn_end) return;   // the warp's unit lies past the tile (uniform per warp)
     const uint32_t so = (uint32_t)wib * 512 + (uint32_t)lane * 16;
     const uint32_t off = pos + so;
     const bool on = off < G.syn_end;
     const uint8_t* wd = sb + 4 * SB;
-    const uint32_t f = (uint32_t)lane & (LPC - 1);
+    const uint32_t f = (uint32_t)lane & (LPCW - 1);
     uint32_t act0 = 0, cur = 0, en0 = 0;
     if (on) {
         if ((lane & (LPD - 1)) == 0) act0 = wd[(off >> SPD_L2) - ((pos >> SPD_L2) & ~15u)];
@@ -731,7 +763,7 @@ __device__ __forceinline__ void stage_fast(const FusedTuftArgs& A, const TileGeo
         if (TUFT) {
             const uint32_t ci = (off >> S_L2) - ((pos >> S_L2) & ~15u);
             if (LPC >= 8) {
-                if (f < 4) cur = wd[(1 + f) * WIN + ci];
+                if (f < 4 && cell_warp) cur = wd[(1 + f) * WIN + ci];
             } else if (f == 0) {
                 cur = (uint32_t)wd[WIN + ci] | ((uint32_t)wd[2 * WIN + ci] << 8) | ((uint32_t)wd[3 * WIN + ci] << 16) |
                       ((uint32_t)wd[4 * WIN + ci] << 24);
@@ -786,10 +818,39 @@ __device__ __forceinline__ void stage_fast(const FusedTuftArgs& A, const TileGeo
         constexpr uint32_t kDenMask = (1u << (S_L2 - SPD_L2)) - 1;   // dendrite index within its cell
         uint32_t key = lead ? ((d_raw << 16) | (0xFFFFu - (den & kDenMask))) : 0u;
         uint32_t best = d_st, tot = d_st;
-        if (LPC == 32) {
+        if (LPC >= 32) {
             key = __reduce_max_sync(0xFFFFFFFFu, key);
             best = __reduce_max_sync(0xFFFFFFFFu, best);
             tot = __reduce_add_sync(0xFFFFFFFFu, tot);
+            if (PAIR) {
+                // The pair's next hand-over (both warps take the same
+                // stages): the odd warp writes once the even one took the
+                // previous values; every wait is bounded.
+                uint64_t* bar = pair_bars() + 2 * (wib >> 1);
+                uint32_t* x = pair_words() + 4 * (wib >> 1);
+                const uint32_t ph = (ring & kPairPhase) ? 1u : 0u;
+                bool ok;
+                if (wib & 1) {
+                    ok = !(ring & kPairSeen) || mbar_wait(&bar[1], ph ^ 1u, limit_us);
+                    if (ok && lane == 0) {
+                        x[0] = key;
+                        x[1] = best;
+                        x[2] = tot;
+                        mbar_arrive(&bar[0]);
+                    }
+                } else {
+                    ok = mbar_wait(&bar[0], ph, limit_us);
+                    if (ok) {
+                        key = max(key, x[0]);
+                        best = max(best, x[1]);
+                        tot += x[2];
+                    }
+                    __syncwarp();
+                    if (ok && lane == 0) mbar_arrive(&bar[1]);
+                }
+                if (!__all_sync(0xFFFFFFFFu, ok) && lane == 0) raise_abort(s_abort, A.ctl);
+                ring = (ring ^ kPairPhase) | kPairSeen;
+            }
         } else {
 #pragma unroll
             for (uint32_t m = LPD; m < LPC; m <<= 1) {
@@ -804,7 +865,7 @@ __device__ __forceinline__ void stage_fast(const FusedTuftArgs& A, const TileGeo
                 tot = __shfl_sync(0xFFFFFFFFu, tot, src);
             }
         }
-        if (on && (LPC >= 8 ? f < 8 : f == 0)) {
+        if (on && cell_warp && (LPC >= 8 ? f < 8 : f == 0)) {
             const uint32_t c = off >> S_L2;
             const uint32_t best_raw = key >> 16;
             const uint32_t best_id = best_raw ? (0xFFFFu - (key & 0xFFFFu)) : 0u;
@@ -840,7 +901,7 @@ struct ProducerState {
     uint64_t issued = 0;           // stages issued (withheld ones included)
     uint64_t stall = 0;            // withhold the stage issued as number `stall` (counted from 1; 0: none)
     int withheld = -1;             // buffer of the withheld stage (-1: none)
-    uint64_t limit_ns = 0;         // bounded-wait limit
+    uint32_t limit_us = 0;         // bounded-wait limit
 };
 
 // Producer lane: issues every stage of tile G into the ring. False when a
@@ -859,7 +920,7 @@ __device__ __forceinline__ bool produce_tile(const FusedTuftArgs& A, const TileG
         if (s_abort) return false;
         uint32_t& pb = ps.pb;
         // Buffer pb's previous use (round pround - 1) must be released.
-        if (ps.pround > 0 && !mbar_wait(&empty[pb], (ps.pround - 1) & 1, ps.limit_ns)) {
+        if (ps.pround > 0 && !mbar_wait(&empty[pb], (ps.pround - 1) & 1, ps.limit_us)) {
             raise_abort(s_abort, A.ctl);
             return false;
         }
@@ -911,13 +972,13 @@ __device__ __forceinline__ void producer_drain(uint64_t* full, uint32_t nst, con
     for (uint32_t b = 0; b < nst; b++) {
         uint64_t uses = ps.issued / nst + (b < ps.issued % nst ? 1 : 0);
         if ((int)b == ps.withheld) uses--;
-        if (uses) mbar_wait(&full[b], (uint32_t)((uses - 1) & 1), ps.limit_ns);
+        if (uses) mbar_wait(&full[b], (uint32_t)((uses - 1) & 1), ps.limit_us);
     }
 }
 
 // Consumer warps: take tile G's footprint -- load it as a tensor box and
 // fire it in place, or stage it themselves -- then process the tile's stages
-// from the ring (buffer cb, phase cphase). The caller's barrier before each
+// from the ring (position `ring`). The caller's barrier before each
 // tile (every consumer warp done with the previous footprint, its shared
 // memory writes fenced for the async proxy) is what lets the box overwrite
 // the footprint, so consumer thread 0 issues it right there: the footprint
@@ -927,24 +988,25 @@ __device__ __forceinline__ void producer_drain(uint64_t* full, uint32_t nst, con
 // whose OR-reduction keeps that decision uniform.
 template <bool TUFT, int MODE, bool FCLEAN, int GEOM>
 __device__ __forceinline__ bool consume_tile(const FusedTuftArgs& A, const TileGeo& G, uint8_t* halo, uint8_t* stages,
-                                             uint64_t* full, uint64_t* empty, uint64_t* fp_full, uint32_t& cb,
-                                             uint32_t& cphase, uint32_t& fp_n, int lane, int wib, int32_t rnd,
-                                             uint64_t limit_ns, volatile int& s_abort) {
+                                             uint64_t* full, uint64_t* empty, uint64_t* fp_full, uint32_t& ring,
+                                             int lane, int wib, int32_t rnd, uint32_t limit_us,
+                                             volatile int& s_abort) {
     if (A.fp_tma) {
         if (wib == 0 && lane == 0) {
             mbar_arrive_expect_tx(fp_full, A.fp_bytes);
             tma_load_3d(halo, &A.tmap, G.ulo - (int32_t)G.xoff, G.vlo, 0, fp_full);
         }
-        bool got = !s_abort && mbar_wait(fp_full, fp_n & 1, limit_ns);
+        const uint32_t fph = (ring & kFpPhase) ? 1u : 0u;
+        bool got = !s_abort && mbar_wait(fp_full, fph, limit_us);
         got = __all_sync(0xFFFFFFFFu, got);
         if (!got && lane == 0) raise_abort(s_abort, A.ctl);
         if (consumers_sync_or(!got)) {
             // Let the box land before the CTA's shared memory is released.
-            if (wib == 0 && lane == 0) mbar_wait(fp_full, fp_n & 1, limit_ns);
-            fp_n++;
+            if (wib == 0 && lane == 0) mbar_wait(fp_full, fph, limit_us);
+            ring ^= kFpPhase;
             return false;
         }
-        fp_n++;
+        ring ^= kFpPhase;
         fire_footprint(halo, A.fp_bytes);
         fence_proxy_async_smem();   // the next tile's load overwrites these bytes
     } else {
@@ -956,7 +1018,8 @@ __device__ __forceinline__ bool consume_tile(const FusedTuftArgs& A, const TileG
     const uint32_t cpu = A.chunks_per_unit;
     const uint32_t n_units_tile = cpu > 1 ? G.h * G.w : (G.syn_end - G.syn0 + 511) >> 9;
     for (uint32_t pos = G.syn0; pos < G.syn_end; pos += SB) {
-        bool got = !s_abort && mbar_wait(&full[cb], cphase, limit_ns);
+        const uint32_t cb = ring & kRingBuf;
+        bool got = !s_abort && mbar_wait(&full[cb], (ring & kRingPhase) ? 1u : 0u, limit_us);
         got = __all_sync(0xFFFFFFFFu, got);
         if (!got) {
             if (lane == 0) raise_abort(s_abort, A.ctl);
@@ -967,10 +1030,10 @@ __device__ __forceinline__ bool consume_tile(const FusedTuftArgs& A, const TileG
                                           wib, rnd);
         else
             stage_fast<TUFT, geom_spd_l2(GEOM), geom_lpc_l2(GEOM)>(A, G, halo, stages + (size_t)cb * A.stage_stride,
-                                                                   pos, lane, wib, rnd);
+                                                                   pos, lane, wib, rnd, ring, limit_us, s_abort);
         __syncwarp();
         if (lane == 0) mbar_arrive(&empty[cb]);
-        if (++cb == A.nst) { cb = 0; cphase ^= 1; }
+        ring = cb + 1 == A.nst ? (ring & ~kRingBuf) ^ kRingPhase : ring + 1;
     }
     return true;
 }
@@ -989,12 +1052,12 @@ __device__ __forceinline__ void tma_body(const FusedTuftArgs& A, uint8_t* smem, 
     const int tid = threadIdx.x;
     const int lane = tid & 31;
     const int wib = tid >> 5;
-    const uint64_t limit_ns = wait_limit_ns(A.ctl);
+    const uint32_t limit_us = wait_limit_us(A.ctl);
     if (wib == kWarps) {
         // ---- producer: lane 0 streams every stage of this CTA's tiles ----
         if (lane != 0) return;
         ProducerState ps;
-        ps.limit_ns = limit_ns;
+        ps.limit_us = limit_us;
         ps.stall = blockIdx.x == 0 ? A.ctl->stall_stage : 0u;
         for (uint32_t t = blockIdx.x; t < A.n_tiles && !s_abort; t += gridDim.x)
             if (!produce_tile<TUFT, MODE, FCLEAN>(A, tile_geo(A, t), stages, full, empty, ps, s_abort)) break;
@@ -1003,15 +1066,15 @@ __device__ __forceinline__ void tma_body(const FusedTuftArgs& A, uint8_t* smem, 
     }
     // ---- consumer warps ----
     const int32_t rnd = rnd_at(A.rnd_key, A.ctl->cycle);
-    uint32_t cb = 0, cphase = 0, fp_n = 0;
+    uint32_t ring = 0;
     bool ok = true;
     for (uint32_t t = blockIdx.x; t < A.n_tiles; t += gridDim.x) {
         const TileGeo G = tile_geo(A, t);
         // Every consumer is done with the previous tile; all leave together
         // if any gave up.
         if (consumers_sync_or(!ok || s_abort)) break;
-        ok = consume_tile<TUFT, MODE, FCLEAN, GEOM>(A, G, halo, stages, full, empty, fp_full, cb, cphase, fp_n, lane,
-                                                    wib, rnd, limit_ns, s_abort);
+        ok = consume_tile<TUFT, MODE, FCLEAN, GEOM>(A, G, halo, stages, full, empty, fp_full, ring, lane, wib, rnd,
+                                                    limit_us, s_abort);
     }
 }
 
@@ -1024,6 +1087,7 @@ __device__ __forceinline__ void init_ring(uint8_t* ring, uint32_t nst, volatile 
             mbar_init(&empty[i], kWarps);
         }
         mbar_init(full + kFpFullSlot, 1);
+        for (int i = 0; i < kWarps; i++) mbar_init(&pair_bars()[i], 1);
         fence_mbar_init();
         s_abort = 0;
     }
@@ -1055,6 +1119,7 @@ __global__ void __launch_bounds__(kThreads, 3) k_fused_tuft_tma(const __grid_con
             case 5: tma_body<TUFT, 0, true, 5>(A, smem, s_abort); return;
             case 6: tma_body<TUFT, 0, true, 6>(A, smem, s_abort); return;
             case 7: tma_body<TUFT, 0, true, 7>(A, smem, s_abort); return;
+            case 8: tma_body<TUFT, 0, true, 8>(A, smem, s_abort); return;
             default: break;
             }
         } else {
@@ -1132,7 +1197,7 @@ __global__ void __launch_bounds__(kThreads, 3) k_fused_tuft_batch(const __grid_c
                 // Waits follow the job's area. The fault hook: the CTA that
                 // takes a job's first tile withholds the job area's
                 // stall_stage-th stage from that tile on.
-                ps.limit_ns = wait_limit_ns(ctl);
+                ps.limit_us = wait_limit_us(ctl);
                 if (t == P.tile0[j] && ctl->stall_stage) ps.stall = ps.issued + ctl->stall_stage;
             }
             const TileGeo G = tile_geo(A, t - P.tile0[j]);
@@ -1148,9 +1213,9 @@ __global__ void __launch_bounds__(kThreads, 3) k_fused_tuft_batch(const __grid_c
         if (s_abort || ps.withheld >= 0) producer_drain(full, nst, ps);
         return;
     }
-    uint32_t cur = 0xFFFFFFFFu, mode = 0, cb = 0, cphase = 0, fp_n = 0;
+    uint32_t cur = 0xFFFFFFFFu, mode = 0, ring = 0;
     int32_t rnd = 0;
-    uint64_t limit_ns = 0;
+    uint32_t limit_us = 0;
     bool ok = true;
     for (uint32_t t = blockIdx.x; t < n_tiles; t += gridDim.x) {
         const uint32_t j = job_of(P, t);
@@ -1162,12 +1227,12 @@ __global__ void __launch_bounds__(kThreads, 3) k_fused_tuft_batch(const __grid_c
             cur = j;
             mode = mode_of(A);
             rnd = rnd_at(A.rnd_key, A.ctl->cycle);
-            limit_ns = wait_limit_ns(A.ctl);
+            limit_us = wait_limit_us(A.ctl);
         }
         const TileGeo G = tile_geo(A, t - P.tile0[j]);
 #define BM_CONSUME(M, FC, GM)                                                                                   \
-    ok = consume_tile<TUFT, M, FC, GM>(A, G, halo, stages, full, empty, fp_full, cb, cphase, fp_n, lane, wib, rnd, \
-                                       limit_ns, s_abort)
+    ok = consume_tile<TUFT, M, FC, GM>(A, G, halo, stages, full, empty, fp_full, ring, lane, wib, rnd, limit_us, \
+                                       s_abort)
         switch (mode) {
         case 0:
             if (TUFT) {
@@ -1177,6 +1242,7 @@ __global__ void __launch_bounds__(kThreads, 3) k_fused_tuft_batch(const __grid_c
                 case 5: BM_CONSUME(0, true, 5); break;
                 case 6: BM_CONSUME(0, true, 6); break;
                 case 7: BM_CONSUME(0, true, 7); break;
+                case 8: BM_CONSUME(0, true, 8); break;
                 default: BM_CONSUME(0, true, 0); break;
                 }
             } else {

@@ -20,6 +20,9 @@ SCHEMES = {
     # 1 x 64, pyramidal depth 4 with proximal and distal 16 x 32 tufts at
     # reach 6 (the specialised consumers of both layer kinds, in seconds).
     "area_256_shape": lambda: configs.workload("area_256_shape")[:2],
+    # A batched instance's largest cells: pyramidal depth 2 with a distal
+    # 16 x 64 tuft (1024 synapses a cell, shared by a pair of warps).
+    "distal_1024": lambda: configs.instance_area(48, 2, 16, 64),
 }
 
 

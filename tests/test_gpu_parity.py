@@ -75,15 +75,15 @@ def test_cycles_match_oracle(ctx, scheme, plain):
 
 # Specialised consumers each scheme's fused tufts reach once the flags are
 # clean: 1 x 32 and 1 x 64 spiny stellate cells (1, 2), pyramidal cells of
-# 8 x 32 and 16 x 32 synapses (5, 6); the mixed area's odd shapes mostly take
-# the general consumer.
+# 8 x 32, 16 x 32 and 16 x 64 synapses (5, 6, 8); the mixed area's odd shapes
+# mostly take the general consumer.
 CLEAN_CONSUMERS = {"area_64": [1, 6], "area_48_deep": [1, 6], "area_256_shape": [2, 6], "testbed": [1],
-                   "smoother": [1, 5], "mixed": []}
+                   "smoother": [1, 5], "mixed": [], "distal_1024": [1, 8]}
 # Whether some tuft's footprint arrives as a tensor box: rows of a multiple of
 # 16 bytes (64, 48 columns) do; the 24- and 40-column areas take the
 # consumer-staged footprint.
 CLEAN_TMA = {"area_64": True, "area_48_deep": True, "area_256_shape": True, "testbed": False, "smoother": False,
-             "mixed": None}
+             "mixed": None, "distal_1024": True}
 
 
 @pytest.mark.parametrize("scheme", sorted(CLEAN_CONSUMERS))
