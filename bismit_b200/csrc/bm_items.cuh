@@ -91,8 +91,12 @@ __device__ __forceinline__ uint8_t* soma_of(const DevLayer& L) {
 }
 
 // inhib_simple, cl/control.cl:28-191; cell c. Returns the axon it wrote.
-__device__ __forceinline__ uint8_t inhib_simple_item(uint8_t* __restrict__ axns, const SliceRec* __restrict__ slices,
-                                                     const DevLayer& L, int radius, int32_t rnd, uint32_t c) {
+// R > 0: the radius fixed at compile time (the neighbourhood loop unrolls, its
+// 3R(R+1)+1 loads independent of one another); R == 0: `radius` at run time.
+template <int R>
+__device__ __forceinline__ uint8_t inhib_simple_cell(uint8_t* __restrict__ axns, const SliceRec* __restrict__ slices,
+                                                     const DevLayer& L, int radius_rt, int32_t rnd, uint32_t c) {
+    const int radius = R > 0 ? R : radius_rt;
     const uint8_t* cs = soma_of(L);
     int vsz = (int)L.v_size, usz = (int)L.u_size;
     int s = (int)(c / (uint32_t)(vsz * usz)), rem = (int)(c % (uint32_t)(vsz * usz));
@@ -103,8 +107,10 @@ __device__ __forceinline__ uint8_t inhib_simple_item(uint8_t* __restrict__ axns,
     int uninhibited = 1;
     int horizon = radius + kInhibHorizOffset;
     int infl_max = horizon * horizon;
+#pragma unroll
     for (int vo = -radius; vo <= radius; vo++) {
         int uz = max(-radius, -vo - radius), um = min(radius, -vo + radius);
+#pragma unroll
         for (int uo = uz; uo <= um; uo++) {
             int vt = v + (int)(int8_t)vo, ut = u + (int)(int8_t)uo;
             bool ns = (vt >= 0) & (vt < vsz) & (ut >= 0) & (ut < usz);
@@ -120,6 +126,12 @@ __device__ __forceinline__ uint8_t inhib_simple_item(uint8_t* __restrict__ axns,
     uint8_t* act = L.buf[BM_BUF_CEL_ACTIVITIES];
     act[c] = update_activity(act[c], axon_active, rnd, (int32_t)((uint32_t)cel_state | c), kCellActivityDecay);
     return out;
+}
+__device__ __forceinline__ uint8_t inhib_simple_item(uint8_t* __restrict__ axns, const SliceRec* __restrict__ slices,
+                                                     const DevLayer& L, int radius, int32_t rnd, uint32_t c) {
+    // Radius 4 (the configurations' inhibition radius) has its own copy.
+    return radius == 4 ? inhib_simple_cell<4>(axns, slices, L, radius, rnd, c)
+                       : inhib_simple_cell<0>(axns, slices, L, radius, rnd, c);
 }
 
 // inhib_passthrough, cl/control.cl:194-217 (rnd is left at 0 by bismit's host,
@@ -255,23 +267,25 @@ __device__ __forceinline__ void tuft_cell_item(const uint8_t* __restrict__ axns,
 
 // The strength updates of learning, for every learning cell of the warp
 // (lanes in `mask`, each with its run of synapses [z, z + n)), the warp sharing
-// each run; four runs at a time, all four loaded before any is stored, so
-// their latencies overlap (runs of different cells are disjoint). SSC:
+// each run; kLearnRuns runs at a time, all of them loaded before any is
+// stored, so their latencies overlap (runs of different cells are disjoint). SSC:
 // prx_syns__active__mtp_ltd (cl/bismit.cl:604-639: a synapse is active when
 // its state is non-zero, depression mask 0x1FF); else
 // dst_syns__active__mtpot_mtdep (cl/bismit.cl:554-600: active when
 // SYN_PREV_ACTIVE is set, depression mask 0xFFF). Both seed with the run's
 // first index plus the synapse index (the doubled index, :589,592,629,630).
-template <bool SSC>
+// Learning runs a warp keeps in flight at once: 8 for spiny stellate cells;
+// 4 in the pyramidal tail, where more leaves arrays in local memory.
+template <bool SSC, int kLearnRuns = SSC ? 8 : 4>
 __device__ __forceinline__ void learn_runs_warp(const DevLayer& L, int32_t rnd, unsigned mask, uint32_t z,
                                                 uint32_t n, int lane) {
     const uint8_t* act = SSC ? L.buf[BM_BUF_SYN_STATES] : L.buf[BM_BUF_SYN_FLAG_SETS];
     int8_t* str = (int8_t*)L.buf[BM_BUF_SYN_STRENGTHS];
     constexpr int32_t kDecMask = SSC ? 0x1FF : 0xFFF;
     while (mask) {
-        uint32_t zk[4], nk[4], nmax = 0;
+        uint32_t zk[kLearnRuns], nk[kLearnRuns], nmax = 0;
 #pragma unroll
-        for (int k = 0; k < 4; k++) {
+        for (int k = 0; k < kLearnRuns; k++) {
             const int b = mask ? __ffs(mask) - 1 : 0;
             const uint32_t zb = __shfl_sync(0xFFFFFFFFu, z, b), nb = __shfl_sync(0xFFFFFFFFu, n, b);
             zk[k] = zb;
@@ -280,17 +294,17 @@ __device__ __forceinline__ void learn_runs_warp(const DevLayer& L, int32_t rnd, 
             mask &= mask - 1;
         }
         for (uint32_t o = (uint32_t)lane; o < nmax; o += 32) {
-            int8_t sv[4];
-            uint8_t av[4];
+            int8_t sv[kLearnRuns];
+            uint8_t av[kLearnRuns];
 #pragma unroll
-            for (int k = 0; k < 4; k++) {
+            for (int k = 0; k < kLearnRuns; k++) {
                 if (o < nk[k]) {
                     sv[k] = str[zk[k] + o];
                     av[k] = act[zk[k] + o];
                 }
             }
 #pragma unroll
-            for (int k = 0; k < 4; k++) {
+            for (int k = 0; k < kLearnRuns; k++) {
                 if (o < nk[k]) {
                     const uint32_t i = zk[k] + o;
                     const int32_t seed = (int32_t)(zk[k] + i);
