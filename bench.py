@@ -50,10 +50,13 @@ def parse():
     ap.add_argument("--serve-sessions", type=int, default=64)
     ap.add_argument("--serve-rate", type=float, default=200.0, help="mean session arrivals per second (Poisson)")
     ap.add_argument("--serve-budget-gb", type=float, default=8.0)
-    ap.add_argument("--profile-run", default=None, choices=["area", "batched"],
+    ap.add_argument("--profile-run", default=None, choices=["area", "batched", "encoders"],
                     help="only W warm-up and K timed cycles of the workload (area: --workload through the plain "
-                         "cycling call; batched: the --batch-instances batch, autotuned, graph replay), no soak, "
-                         "arms or baselines: a short launch sequence for a profiler's launch list")
+                         "cycling call, --workload also smoother or retina; batched: the --batch-instances batch, "
+                         "autotuned, graph replay; encoders: rounds of every device encoder into 64 frames of "
+                         "256 x 256), no soak, arms or baselines: a short launch sequence for a profiler's launch "
+                         "list")
+    ap.add_argument("--regrowth", action="store_true", help="--profile-run area: with synapse regrowth on")
     ap.add_argument("--autotune-cache", default=None,
                     help="--profile-run batched: the autotuner's cache file (choices found there are applied "
                          "without trial launches; new ones are added)")
@@ -928,8 +931,13 @@ def run_profile(args):
     K, W = args.steps, args.warmup
     areas = []
     if args.profile_run == "area":
-        lmaps, ar, act = configs.workload(args.workload)
-        st = configs.bench_settings()
+        if args.workload == "smoother":
+            (lmaps, ar), act = configs.smoother_area(), 0.03
+        elif args.workload == "retina":
+            (lmaps, ar), act = configs.retina_area(48, n_filters=2, src_depth=2), 0.05
+        else:
+            lmaps, ar, act = configs.workload(args.workload)
+        st = M.CorticalAreaSettings().strengths_start_at_zero() if args.regrowth else configs.bench_settings()
         if args.path == "plain":
             st.plain_kernels()
         areas.append(cortex.CorticalArea(ctx, M.area_desc("v1", lmaps, ar, st), seed=args.seed + 1))
@@ -939,7 +947,24 @@ def run_profile(args):
         def cycles(c0, n):
             areas[0].cycle_frames_device(dev.data_ptr() + c0 * flen, flen, n)
         launches = areas[0].launches_per_cycle
-        name = args.workload
+        name = args.workload + (" with regrowth" if args.regrowth else "")
+    elif args.profile_run == "encoders":
+        from bismit_b200 import encode as E
+        n, side = 64, 256
+        frames = torch.zeros(n, side * side, dtype=torch.uint8, device="cuda")
+        images = torch.randint(0, 256, (n, 28, 28), dtype=torch.uint8, device="cuda")
+        vals = np.linspace(0.0, 1.0, n, dtype=np.float32)
+        sdr = E.ScalarSdrWriter(ctx, (0.0, 1.0), 0.05, (side, side), seed=args.seed)
+
+        def cycles(c0, k):
+            for _ in range(k):
+                E.encode_2d_image(ctx, images, (28, 28), (side, side), 1.0, frames)
+                E.encode_scalar(ctx, vals, (0.0, 1.0), (side, side), frames, seed=args.seed)
+                E.encode_scalar_glyph(ctx, vals, (0.0, 1.0), (side, side), frames)
+                sdr.encode(vals, frames)
+                E.encode_hex_mold_scaled(ctx, 6, (side, side), (side, side), frames[0])
+        launches = lambda: 5
+        name = "encoders: 64 frames of 256 x 256 per encoder"
     else:
         frames_h = []
         for i, (side, depth, dens, syns, act) in enumerate(configs.batch_instances(args.batch_instances, args.seed)):
@@ -966,6 +991,8 @@ def run_profile(args):
     e1.record(stream)
     torch.cuda.synchronize()
     n_syn = sum(int(a.plan.n_syns_total) for a in areas)
+    if args.profile_run == "encoders":
+        sdr.close()
     print(json.dumps({"profile_run": name, "steps": K, "warmup": W, "launches_per_cycle": launches(),
                       "synapses": n_syn, "ms_per_cycle": e0.elapsed_time(e1) / K}), flush=True)
     if args.profile_run == "batched":
