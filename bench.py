@@ -762,7 +762,8 @@ def run_ours(args):
     soak(lambda: area.cycle_frames_device(dev_frames.data_ptr(), flen, W), stream, SOAK_S)
     clk = clocks.stop()
     ms = max_over_ranks(e0.elapsed_time(e1), "cuda")
-    launches = area.launches_per_cycle() * K
+    # The cycle's kernels plus each cycle's frame intake (one copy kernel).
+    launches = (area.launches_per_cycle() + 1) * K
     n_syn = int(plan.n_syns_total)
     value = n_syn * K * ws / (ms / 1e3)
 

@@ -758,12 +758,29 @@ void bm::frame_pieces(bm_area_s* A, uint32_t input, uint32_t off, uint32_t len, 
 namespace {
 
 // Copies one input frame to where its pieces land (see frame_pieces).
+// Copies of frame pieces on stream s: device-to-device ones as one copy
+// kernel launched like the cycle's kernels (see CopyPieces).
+int copy_pieces(const std::vector<FramePiece>& pieces, const uint8_t* src, cudaMemcpyKind kind, cudaStream_t s) {
+    if (kind == cudaMemcpyDeviceToDevice && !pieces.empty() && pieces.size() <= kMaxCopyPieces) {
+        CopyPieces P = {};
+        for (const FramePiece& p : pieces) {
+            P.dst[P.n] = p.dst;
+            P.src[P.n] = src + p.off;
+            P.len[P.n] = p.len;
+            P.n++;
+        }
+        launch_copy_pieces(P, s);
+        CU(cudaGetLastError());
+        return BM_OK;
+    }
+    for (const FramePiece& p : pieces) CU(cudaMemcpyAsync(p.dst, src + p.off, p.len, kind, s));
+    return BM_OK;
+}
+
 int write_frame(bm_area_s* A, uint32_t input, const void* src, cudaMemcpyKind kind, cudaStream_t s) {
     std::vector<FramePiece> pieces;
     frame_pieces(A, input, 0, A->plan.inputs[input].len, pieces);
-    for (const FramePiece& p : pieces)
-        CU(cudaMemcpyAsync(p.dst, (const uint8_t*)src + p.off, p.len, kind, s));
-    return BM_OK;
+    return copy_pieces(pieces, (const uint8_t*)src, kind, s);
 }
 
 // A host frame: the caller's bytes are read during the call only, into a
@@ -1168,8 +1185,7 @@ int bm_area_deliver_tract(bm_area src, uint32_t src_output, bm_area dst, uint32_
     const uint8_t* from = src->axns() + src->plan.outputs[src_output].axn_idz;
     std::vector<FramePiece> pieces;
     frame_pieces(dst, dst_input, (uint32_t)dst_offset, len, pieces);
-    for (const FramePiece& p : pieces) CU(cudaMemcpyAsync(p.dst, from + p.off, p.len, cudaMemcpyDeviceToDevice, s));
-    return BM_OK;
+    return copy_pieces(pieces, from, cudaMemcpyDeviceToDevice, s);
 }
 
 int bm_area_clear_errors(bm_area area) {

@@ -7,6 +7,8 @@
 // so one thread grows one dendrite and the result does not depend on launch
 // order. The same rule is restated in the oracle (bmo_grow). Regrowth
 // (k_regrow) draws from the same pools with a per-round stream.
+#include <algorithm>
+
 #include "bm_kernels.h"
 
 namespace bm {
@@ -83,6 +85,24 @@ __global__ void k_grow(DevLayer L, GrowTuft G) {
 }
 
 __global__ void k_cycle_end(AreaCtl* ctl) { pdl_begin(); end_cycle(ctl); }
+
+// Piece blockIdx.y of P, 16 bytes a thread where both ends allow it.
+__global__ void __launch_bounds__(256) k_copy_pieces(const __grid_constant__ CopyPieces P) {
+    pdl_begin();
+    const uint32_t k = blockIdx.y;
+    uint8_t* dst = P.dst[k];
+    const uint8_t* src = P.src[k];
+    const uint32_t n = P.len[k];
+    const uint32_t stride = gridDim.x * blockDim.x;
+    const uint32_t t0 = blockIdx.x * blockDim.x + threadIdx.x;
+    if ((((uintptr_t)dst | (uintptr_t)src) & 15) == 0) {
+        const uint32_t n16 = n / 16;
+        for (uint32_t i = t0; i < n16; i += stride) ((uint4*)dst)[i] = ((const uint4*)src)[i];
+        for (uint32_t i = n16 * 16 + t0; i < n; i += stride) dst[i] = src[i];
+    } else {
+        for (uint32_t i = t0; i < n; i += stride) dst[i] = src[i];
+    }
+}
 
 // Synapses::regrow (src/cortex/synapses.rs:411-501) with SynSrcIdxCache
 // (src/map/syn_src.rs:159-211), one dendrite per thread, on the cycles c with
@@ -175,6 +195,14 @@ void launch_grow(const DevLayer& L, const GrowTuft& G, cudaStream_t s) {
 }
 
 void launch_cycle_end(AreaCtl* ctl, cudaStream_t s) { launch_pdl(k_cycle_end, 1, 1, 0, s, ctl); }
+
+void launch_copy_pieces(const CopyPieces& P, cudaStream_t s) {
+    uint32_t most = 0;
+    for (uint32_t k = 0; k < P.n; k++) most = std::max(most, P.len[k]);
+    if (!most) return;
+    const uint32_t blocks = std::min<uint32_t>(148, (most + 4095) / 4096);
+    launch_pdl(k_copy_pieces, dim3(blocks, P.n), 256, 0, s, P);
+}
 
 uint64_t regrow_key(uint64_t gkey) { return splitmix64(gkey ^ 0x7265677277ull); }
 

@@ -98,6 +98,18 @@ struct RegrowJob {
 uint64_t regrow_key(uint64_t grow_key);
 void launch_regrow(const RegrowJob* jobs, uint32_t n_jobs, uint32_t n_blocks, cudaStream_t s);
 void launch_cycle_end(AreaCtl* ctl, cudaStream_t s);
+// Device-to-device copies of a frame's pieces as one programmatic-dependent
+// launch: on the cycling stream it chains with the cycle's kernels, where a
+// memcpy would end the chain (the next kernel could only start once the copy
+// had completed).
+constexpr uint32_t kMaxCopyPieces = 8;
+struct CopyPieces {
+    uint8_t* dst[kMaxCopyPieces];
+    const uint8_t* src[kMaxCopyPieces];
+    uint32_t len[kMaxCopyPieces];
+    uint32_t n;
+};
+void launch_copy_pieces(const CopyPieces& P, cudaStream_t s);
 
 // Plain form: one kernel per reference stage (bm_plain.cu).
 void launch_set_syn_flags(const DevLayer& L, cudaStream_t s);
