@@ -193,11 +193,10 @@ __device__ __forceinline__ uint32_t wait_limit_us(const AreaCtl* ctl) {
     return us ? us : kDefaultWaitUs;
 }
 
-// A consumer warp's ring position and hand-over parities, in one word (it is
-// carried across every tile and stage): bits 0-2 the ring buffer, bit 3 the
-// ring's phase, bit 4 the footprint box's phase, bit 5 the pair hand-over's
-// phase, bit 6 set once a pair hand-over happened.
-constexpr uint32_t kRingBuf = 7u, kRingPhase = 8u, kFpPhase = 16u, kPairPhase = 32u, kPairSeen = 64u;
+// A consumer warp's ring position and phases, in one word (it is carried
+// across every tile and stage): bits 0-2 the ring buffer, bit 3 the ring's
+// phase, bit 4 the footprint box's phase.
+constexpr uint32_t kRingBuf = 7u, kRingPhase = 8u, kFpPhase = 16u;
 // 1-D bulk copy global -> shared completing on `bar` (16-byte aligned, size % 16 == 0).
 __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
     asm volatile(
@@ -689,7 +688,7 @@ __device__ __forceinline__ void tma_stage(const FusedTuftArgs& A, const TileGeo&
 // tma_stage + finish_chunk compute for that case, with every loop bound,
 // shift and branch on the shape resolved by the compiler.
 // Shapes: 1 (spd 32, S 32), 2 (64, 64), 3 (16, 128), 4 (16, 256), 5 (32, 256),
-// 6 (32, 512), 7 (64, 512), 8 (64, 1024: a cell spans a pair of warps).
+// 6 (32, 512), 7 (64, 512), 8 (64, 1024: a warp takes a cell in two halves).
 constexpr int kGeoms = 9;
 __host__ __device__ constexpr int geom_spd_l2(int g) {
     return g == 1 ? 5 : g == 2 ? 6 : g == 3 ? 4 : g == 4 ? 4 : g == 5 ? 5 : g == 6 ? 5 : 6;
@@ -705,7 +704,8 @@ __host__ __device__ constexpr int geom_lpc_l2(int g) {
 // consumer) otherwise. It applies while the tuft's flags are clean and its
 // sources lie in the footprint.
 uint32_t consumer_shape(const FusedTuft& FT, uint32_t spt, uint32_t spd, bool pyramidal) {
-    if (!FT.tiled || !FT.win || spt > 1024 || FT.stage_bytes != (uint32_t)kWarps * 512) return 0;
+    if (!FT.tiled || !FT.win || spt > 1024 || FT.stage_bytes != (uint32_t)kWarps * 512 * (spt > 512 ? spt / 512 : 1))
+        return 0;
     for (int g = 1; g < kGeoms; g++)
         if ((1u << geom_spd_l2(g)) == spd && (1u << (geom_lpc_l2(g) + 4)) == spt)
             return (pyramidal ? g >= 3 : g <= 2) ? (uint32_t)g : 0u;
@@ -714,143 +714,107 @@ uint32_t consumer_shape(const FusedTuft& FT, uint32_t spt, uint32_t spd, bool py
 
 namespace {
 
-__device__ __forceinline__ void raise_abort(volatile int& s_abort, AreaCtl* ctl);
-
-// Hand-over between the two warps of a pair that share a cell of 1024
-// synapses: per pair, an mbarrier the odd warp arrives on once its half's
-// key, best and total are written, one the even warp arrives on once it took
-// them, and the three words.
-__device__ __forceinline__ uint64_t* pair_bars() {
-    __shared__ uint64_t bars[kWarps];
-    return bars;
-}
-__device__ __forceinline__ uint32_t* pair_words() {
-    __shared__ uint32_t words[kWarps / 2][4];
-    return &words[0][0];
-}
-
 template <bool TUFT, int SPD_L2, int LPC_L2>
 __device__ __forceinline__ void stage_fast(const FusedTuftArgs& A, const TileGeo& G, const uint8_t* halo,
-                                           const uint8_t* sb, uint32_t pos, int lane, int wib, int32_t rnd,
-                                           uint32_t& ring, uint32_t limit_us, volatile int& s_abort) {
-    constexpr uint32_t SB = kWarps * 512;
+                                           const uint8_t* sb, uint32_t pos, int lane, int wib, int32_t rnd) {
+    // A cell of 1024 synapses (LPC_L2 == 6) is one warp's unit, taken as two
+    // halves of 512 synapses whose per-lane tuft reductions combine before
+    // the warp's; its stages hold kWarps such cells (the general consumer's
+    // layout for cells above 512 synapses).
+    constexpr uint32_t HALVES = LPC_L2 == 6 ? 2u : 1u;
+    constexpr uint32_t UNIT = 512u * HALVES;             // synapses of a warp per stage
+    constexpr uint32_t SB = kWarps * UNIT;
     constexpr uint32_t WIN = SB / 16 + 32;
     constexpr uint32_t LPD = 1u << (SPD_L2 - 4);
-    constexpr uint32_t LPC = 1u << LPC_L2;
+    constexpr uint32_t LPC = 1u << LPC_L2;               // lanes a cell spans over its halves
+    constexpr uint32_t LPCW = LPC > 32 ? 32u : LPC;      // lanes of a cell within one half
     constexpr uint32_t S_L2 = LPC_L2 + 4;
-    // A cell of 1024 synapses spans a pair of warps (2k, 2k + 1): each reduces
-    // its half, the odd warp hands its key, best and total to the even one
-    // through shared memory, and the even warp writes the cell-tuft fields.
-    // Stages and tiles hold whole cells, so both warps of a pair take part in
-    // a stage or neither does.
-    constexpr bool PAIR = LPC_L2 == 6;
-    constexpr uint32_t LPCW = PAIR ? 32u : LPC;   // lanes of a cell within one warp
     static_assert(LPC >= LPD, "a cell holds whole dendrites");
-    const bool cell_warp = !PAIR || (wib & 1) == 0;   // the warp that writes the cell-tuft fields
-    const uint32_t unit0 = pos + (uint32_t)wib * 512;
+    const uint32_t unit0 = pos + (uint32_t)wib * UNIT;
     if (unit0 >= G.syn_end) return;   // the warp's unit lies past the tile (uniform per warp)
-    const uint32_t so = (uint32_t)wib * 512 + (uint32_t)lane * 16;
-    const uint32_t off = pos + so;
-    const bool on = off < G.syn_end;
     const uint8_t* wd = sb + 4 * SB;
     const uint32_t f = (uint32_t)lane & (LPCW - 1);
-    uint32_t act0 = 0, cur = 0, en0 = 0;
-    if (on) {
-        if ((lane & (LPD - 1)) == 0) act0 = wd[(off >> SPD_L2) - ((pos >> SPD_L2) & ~15u)];
-        // The cell's energy for the folded ssc_cycle, loaded before the
-        // gathers so its latency overlaps them.
-        if (!TUFT && A.ssc_soma && (lane & (LPD - 1)) == 0) en0 = A.cel_en[off >> SPD_L2];
-        if (TUFT) {
-            const uint32_t ci = (off >> S_L2) - ((pos >> S_L2) & ~15u);
-            if (LPC >= 8) {
-                if (f < 4 && cell_warp) cur = wd[(1 + f) * WIN + ci];
-            } else if (f == 0) {
-                cur = (uint32_t)wd[WIN + ci] | ((uint32_t)wd[2 * WIN + ci] << 8) | ((uint32_t)wd[3 * WIN + ci] << 16) |
-                      ((uint32_t)wd[4 * WIN + ci] << 24);
+    uint32_t cur = 0;
+    uint32_t c_key = 0, c_best = 0, c_tot = 0;   // the cell's reduction over its halves (HALVES == 2)
+#pragma unroll 1
+    for (uint32_t h = 0; h < HALVES; h++) {
+        const uint32_t so = (uint32_t)wib * UNIT + h * 512u + (uint32_t)lane * 16;
+        const uint32_t off = pos + so;
+        const bool on = off < G.syn_end;
+        uint32_t act0 = 0, en0 = 0;
+        if (on) {
+            if ((lane & (LPD - 1)) == 0) act0 = wd[(off >> SPD_L2) - ((pos >> SPD_L2) & ~15u)];
+            // The cell's energy for the folded ssc_cycle, loaded before the
+            // gathers so its latency overlaps them.
+            if (!TUFT && A.ssc_soma && (lane & (LPD - 1)) == 0) en0 = A.cel_en[off >> SPD_L2];
+            if (TUFT && h == 0) {
+                const uint32_t ci = (off >> S_L2) - ((pos >> S_L2) & ~15u);
+                if (LPC >= 8) {
+                    if (f < 4) cur = wd[(1 + f) * WIN + ci];
+                } else if (f == 0) {
+                    cur = (uint32_t)wd[WIN + ci] | ((uint32_t)wd[2 * WIN + ci] << 8) |
+                          ((uint32_t)wd[3 * WIN + ci] << 16) | ((uint32_t)wd[4 * WIN + ci] << 24);
+                }
             }
         }
-    }
-    uint32_t sum = 0, raw = 0;
-    if (on) {
-        const uint4 str4 = *(const uint4*)(sb + 2 * SB + so);
-        const uint4 st4 = *(const uint4*)(sb + 3 * SB + so);
-        const uint4 g0 = *(const uint4*)(sb + 2 * so);
-        const uint4 g1 = *(const uint4*)(sb + 2 * so + 16);
-        const uint32_t gw[8] = {g0.x, g0.y, g0.z, g0.w, g1.x, g1.y, g1.z, g1.w};
-        const uint32_t strw[4] = {str4.x, str4.y, str4.z, str4.w};
-        const uint32_t stw[4] = {st4.x, st4.y, st4.z, st4.w};
-        uint32_t nst[4], nfl[4];
+        uint32_t sum = 0, raw = 0;
+        if (on) {
+            const uint4 str4 = *(const uint4*)(sb + 2 * SB + so);
+            const uint4 st4 = *(const uint4*)(sb + 3 * SB + so);
+            const uint4 g0 = *(const uint4*)(sb + 2 * so);
+            const uint4 g1 = *(const uint4*)(sb + 2 * so + 16);
+            const uint32_t gw[8] = {g0.x, g0.y, g0.z, g0.w, g1.x, g1.y, g1.z, g1.w};
+            const uint32_t strw[4] = {str4.x, str4.y, str4.z, str4.w};
+            const uint32_t stw[4] = {st4.x, st4.y, st4.z, st4.w};
+            uint32_t nst[4], nfl[4];
 #pragma unroll
-        for (int w = 0; w < 4; w++) {
-            const uint32_t lo = gw[2 * w], hi = gw[2 * w + 1];
-            nst[w] = pack4(halo[lo & 0x7FFFu], halo[(lo >> 16) & 0x7FFFu], halo[hi & 0x7FFFu],
-                           halo[(hi >> 16) & 0x7FFFu]);
+            for (int w = 0; w < 4; w++) {
+                const uint32_t lo = gw[2 * w], hi = gw[2 * w + 1];
+                nst[w] = pack4(halo[lo & 0x7FFFu], halo[(lo >> 16) & 0x7FFFu], halo[hi & 0x7FFFu],
+                               halo[(hi >> 16) & 0x7FFFu]);
+            }
+#pragma unroll
+            for (int w = 0; w < 4; w++) {
+                nfl[w] = nz_bits(stw[w]) >> 3;
+                raw = __dp4a(nst[w], 0x01010101u, raw);
+                sum = __dp4a(nst[w] & ~sign_bytes(strw[w]), 0x01010101u, sum);
+            }
+            *(uint4*)(A.st + off) = make_uint4(nst[0], nst[1], nst[2], nst[3]);
+            *(uint4*)(A.fl + off) = make_uint4(nfl[0], nfl[1], nfl[2], nfl[3]);
         }
 #pragma unroll
-        for (int w = 0; w < 4; w++) {
-            nfl[w] = nz_bits(stw[w]) >> 3;
-            raw = __dp4a(nst[w], 0x01010101u, raw);
-            sum = __dp4a(nst[w] & ~sign_bytes(strw[w]), 0x01010101u, sum);
+        for (uint32_t m = 1; m < LPD; m <<= 1) {
+            sum += __shfl_xor_sync(0xFFFFFFFFu, sum, m);
+            raw += __shfl_xor_sync(0xFFFFFFFFu, raw, m);
         }
-        *(uint4*)(A.st + off) = make_uint4(nst[0], nst[1], nst[2], nst[3]);
-        *(uint4*)(A.fl + off) = make_uint4(nfl[0], nfl[1], nfl[2], nfl[3]);
-    }
-#pragma unroll
-    for (uint32_t m = 1; m < LPD; m <<= 1) {
-        sum += __shfl_xor_sync(0xFFFFFFFFu, sum, m);
-        raw += __shfl_xor_sync(0xFFFFFFFFu, raw, m);
-    }
-    const bool lead = on && (lane & (LPD - 1)) == 0;
-    const uint32_t den = off >> SPD_L2;
-    uint32_t d_raw = 0, d_st = 0;
-    if (lead) {
-        const int active = sum > A.thresh;
-        const uint32_t s2 = active ? sum : 0u;
-        const uint32_t seed = (raw + A.thresh) | (den + A.den_idz);
-        A.den_act[den] = update_activity((uint8_t)act0, active, rnd, (int32_t)seed, kDendriteActivityDecay);
-        d_raw = min(raw >> 4, 255u);
-        d_st = min(s2 >> 4, 255u);
-        A.den_raw[den] = (uint8_t)d_raw;
-        if (!TUFT && A.ssc_soma) d_st = ssc_soma(A.cel_en, den, en0, d_st);
-        A.den_st[den] = (uint8_t)d_st;
-    }
-    if (TUFT) {
+        const bool lead = on && (lane & (LPD - 1)) == 0;
+        const uint32_t den = off >> SPD_L2;
+        uint32_t d_raw = 0, d_st = 0;
+        if (lead) {
+            const int active = sum > A.thresh;
+            const uint32_t s2 = active ? sum : 0u;
+            const uint32_t seed = (raw + A.thresh) | (den + A.den_idz);
+            A.den_act[den] = update_activity((uint8_t)act0, active, rnd, (int32_t)seed, kDendriteActivityDecay);
+            d_raw = min(raw >> 4, 255u);
+            d_st = min(s2 >> 4, 255u);
+            A.den_raw[den] = (uint8_t)d_raw;
+            if (!TUFT && A.ssc_soma) d_st = ssc_soma(A.cel_en, den, en0, d_st);
+            A.den_st[den] = (uint8_t)d_st;
+        }
+        if (!TUFT) continue;
         constexpr uint32_t kDenMask = (1u << (S_L2 - SPD_L2)) - 1;   // dendrite index within its cell
         uint32_t key = lead ? ((d_raw << 16) | (0xFFFFu - (den & kDenMask))) : 0u;
         uint32_t best = d_st, tot = d_st;
-        if (LPC >= 32) {
+        if (HALVES == 2) {
+            c_key = max(c_key, key);
+            c_best = max(c_best, best);
+            c_tot += tot;
+            continue;
+        }
+        if (LPC == 32) {
             key = __reduce_max_sync(0xFFFFFFFFu, key);
             best = __reduce_max_sync(0xFFFFFFFFu, best);
             tot = __reduce_add_sync(0xFFFFFFFFu, tot);
-            if (PAIR) {
-                // The pair's next hand-over (both warps take the same
-                // stages): the odd warp writes once the even one took the
-                // previous values; every wait is bounded.
-                uint64_t* bar = pair_bars() + 2 * (wib >> 1);
-                uint32_t* x = pair_words() + 4 * (wib >> 1);
-                const uint32_t ph = (ring & kPairPhase) ? 1u : 0u;
-                bool ok;
-                if (wib & 1) {
-                    ok = !(ring & kPairSeen) || mbar_wait(&bar[1], ph ^ 1u, limit_us);
-                    if (ok && lane == 0) {
-                        x[0] = key;
-                        x[1] = best;
-                        x[2] = tot;
-                        mbar_arrive(&bar[0]);
-                    }
-                } else {
-                    ok = mbar_wait(&bar[0], ph, limit_us);
-                    if (ok) {
-                        key = max(key, x[0]);
-                        best = max(best, x[1]);
-                        tot += x[2];
-                    }
-                    __syncwarp();
-                    if (ok && lane == 0) mbar_arrive(&bar[1]);
-                }
-                if (!__all_sync(0xFFFFFFFFu, ok) && lane == 0) raise_abort(s_abort, A.ctl);
-                ring = (ring ^ kPairPhase) | kPairSeen;
-            }
         } else {
 #pragma unroll
             for (uint32_t m = LPD; m < LPC; m <<= 1) {
@@ -865,25 +829,35 @@ __device__ __forceinline__ void stage_fast(const FusedTuftArgs& A, const TileGeo
                 tot = __shfl_sync(0xFFFFFFFFu, tot, src);
             }
         }
-        if (on && cell_warp && (LPC >= 8 ? f < 8 : f == 0)) {
-            const uint32_t c = off >> S_L2;
-            const uint32_t best_raw = key >> 16;
-            const uint32_t best_id = best_raw ? (0xFFFFu - (key & 0xFFFFu)) : 0u;
-            const bool is_max = tot >= (1u << (A.mad_l2 + 8));
-            const uint32_t tst = is_max ? 255u : ((tot >> A.mad_l2) & 0xFFu);
-            if (LPC >= 8) {
-                const uint32_t nv = f == 4 ? best_id : f == 5 ? best_raw : f == 6 ? best : tst;
-                (&A.t_pid)[f][c] = (uint8_t)(f < 4 ? cur : nv);
-            } else {
-                A.t_pid[c] = (uint8_t)cur;
-                A.t_praw[c] = (uint8_t)(cur >> 8);
-                A.t_pst[c] = (uint8_t)(cur >> 16);
-                A.t_ptft[c] = (uint8_t)(cur >> 24);
-                A.t_bid[c] = (uint8_t)best_id;
-                A.t_braw[c] = (uint8_t)best_raw;
-                A.t_bst[c] = (uint8_t)best;
-                A.t_st[c] = (uint8_t)tst;
-            }
+        c_key = key;
+        c_best = best;
+        c_tot = tot;
+    }
+    if (!TUFT) return;
+    if (HALVES == 2) {
+        c_key = __reduce_max_sync(0xFFFFFFFFu, c_key);
+        c_best = __reduce_max_sync(0xFFFFFFFFu, c_best);
+        c_tot = __reduce_add_sync(0xFFFFFFFFu, c_tot);
+    }
+    const uint32_t off = pos + (uint32_t)wib * UNIT + (uint32_t)lane * 16;   // in the cell's first half
+    if (off < G.syn_end && (LPC >= 8 ? f < 8 : f == 0)) {
+        const uint32_t c = off >> S_L2;
+        const uint32_t best_raw = c_key >> 16;
+        const uint32_t best_id = best_raw ? (0xFFFFu - (c_key & 0xFFFFu)) : 0u;
+        const bool is_max = c_tot >= (1u << (A.mad_l2 + 8));
+        const uint32_t tst = is_max ? 255u : ((c_tot >> A.mad_l2) & 0xFFu);
+        if (LPC >= 8) {
+            const uint32_t nv = f == 4 ? best_id : f == 5 ? best_raw : f == 6 ? c_best : tst;
+            (&A.t_pid)[f][c] = (uint8_t)(f < 4 ? cur : nv);
+        } else {
+            A.t_pid[c] = (uint8_t)cur;
+            A.t_praw[c] = (uint8_t)(cur >> 8);
+            A.t_pst[c] = (uint8_t)(cur >> 16);
+            A.t_ptft[c] = (uint8_t)(cur >> 24);
+            A.t_bid[c] = (uint8_t)best_id;
+            A.t_braw[c] = (uint8_t)best_raw;
+            A.t_bst[c] = (uint8_t)c_best;
+            A.t_st[c] = (uint8_t)tst;
         }
     }
 }
@@ -1030,7 +1004,7 @@ __device__ __forceinline__ bool consume_tile(const FusedTuftArgs& A, const TileG
                                           wib, rnd);
         else
             stage_fast<TUFT, geom_spd_l2(GEOM), geom_lpc_l2(GEOM)>(A, G, halo, stages + (size_t)cb * A.stage_stride,
-                                                                   pos, lane, wib, rnd, ring, limit_us, s_abort);
+                                                                   pos, lane, wib, rnd);
         __syncwarp();
         if (lane == 0) mbar_arrive(&empty[cb]);
         ring = cb + 1 == A.nst ? (ring & ~kRingBuf) ^ kRingPhase : ring + 1;
@@ -1087,7 +1061,6 @@ __device__ __forceinline__ void init_ring(uint8_t* ring, uint32_t nst, volatile 
             mbar_init(&empty[i], kWarps);
         }
         mbar_init(full + kFpFullSlot, 1);
-        for (int i = 0; i < kWarps; i++) mbar_init(&pair_bars()[i], 1);
         fence_mbar_init();
         s_abort = 0;
     }

@@ -21,7 +21,7 @@ SCHEMES = {
     # reach 6 (the specialised consumers of both layer kinds, in seconds).
     "area_256_shape": lambda: configs.workload("area_256_shape")[:2],
     # A batched instance's largest cells: pyramidal depth 2 with a distal
-    # 16 x 64 tuft (1024 synapses a cell, shared by a pair of warps).
+    # 16 x 64 tuft (1024 synapses a cell, one warp's unit in two halves).
     "distal_1024": lambda: configs.instance_area(48, 2, 16, 64),
 }
 
