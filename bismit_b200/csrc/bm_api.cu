@@ -290,6 +290,11 @@ void bm::exec_step(bm_area_s* A, const Step& st, cudaStream_t s, bool end_cycle)
     case ST_DST_MTP: run(K_TFT_DST_MTP, [&] { launch_tft_dst_mtp_plain(A->axns(), D, x, A->ctl, s); }); break;
     case ST_SSC_MTP: run(K_SSC_MTP, [&] { launch_ssc_mtp_plain(A->axns(), D, A->ctl, s); }); break;
     case ST_REGROW:
+        // Only the area's own cycles come here, enqueued as they run, with
+        // host_cycle the number of the cycle being enqueued: the launch is
+        // left out on the cycles it would return at once (graph-replayed
+        // batches launch it every cycle and let the device decide).
+        if (A->host_cycle % kRegrowPeriod != kRegrowPeriod - 1) break;
         run(K_REGROW, [&] { launch_regrow(A->d_regrow, (uint32_t)A->regrow.size(), A->regrow_blocks, s); });
         break;
     case ST_SMOOTH: {

@@ -123,8 +123,10 @@ __global__ void __launch_bounds__(128) k_inhib_mtp(uint8_t* __restrict__ axns, c
 }
 
 // With end_cycle, the last block to finish also ends the cycle (the cycle-end
-// launch folded in): every block has read the cycle number by then.
-__global__ void __launch_bounds__(128) k_pyr_tail(uint8_t* __restrict__ axns, const SliceRec* __restrict__ slices,
+// launch folded in): every block has read the cycle number by then. Twelve
+// blocks of 128 per SM (40 registers): area_256's 262,144 cells then need 1.15
+// waves of warps instead of the 1.54 that 54 registers allowed.
+__global__ void __launch_bounds__(128, 12) k_pyr_tail(uint8_t* __restrict__ axns, const SliceRec* __restrict__ slices,
                                                   DevLayer L, int ctrl, int learn, AreaCtl* ctl, uint32_t tufts,
                                                   int end) {
     pdl_begin();
