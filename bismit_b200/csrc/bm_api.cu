@@ -492,7 +492,7 @@ int bm::schedule_area(bm_area_s* A) {
     A->side_ev.clear();
     if (A->last_side == SIZE_MAX) return BM_OK;
     cudaError_t e = cudaSuccess;
-    if (!A->side) e = cudaStreamCreateWithFlags(&A->side, cudaStreamNonBlocking);
+    if (!A->side) e = stream_like(A->stream(), &A->side);
     if (e == cudaSuccess && !A->ev_fork) e = cudaEventCreateWithFlags(&A->ev_fork, cudaEventDisableTiming);
     A->side_ev.assign(n, nullptr);
     for (size_t k = 0; k < n && e == cudaSuccess; k++)

@@ -108,6 +108,16 @@ struct bm_ctx_s {
     cudaStream_t stream() const { return user_set ? user : own; }
 };
 namespace bm {
+// A non-blocking stream at `base`'s priority: a side or capture stream runs
+// its share of a cycle at the priority of the stream it forks from.
+inline cudaError_t stream_like(cudaStream_t base, cudaStream_t* out) {
+    int prio = 0;
+    if (cudaStreamGetPriority(base, &prio) != cudaSuccess) {
+        cudaGetLastError();
+        prio = 0;
+    }
+    return cudaStreamCreateWithPriority(out, cudaStreamNonBlocking, prio);
+}
 inline void ctx_retain(bm_ctx c) {
     if (c) c->refs.fetch_add(1, std::memory_order_relaxed);
 }

@@ -563,7 +563,7 @@ int schedule_side(bm_batch_s* B) {
     }
     if (B->last_side == SIZE_MAX) return BM_OK;
     cudaError_t e = cudaSuccess;
-    if (!B->side) e = cudaStreamCreateWithFlags(&B->side, cudaStreamNonBlocking);
+    if (!B->side) e = stream_like(B->stream(), &B->side);
     if (e == cudaSuccess && !B->ev_fork) e = cudaEventCreateWithFlags(&B->ev_fork, cudaEventDisableTiming);
     for (cudaEvent_t ev : B->side_ev)
         if (ev) cudaEventDestroy(ev);
@@ -928,7 +928,7 @@ int bm_batch_create(bm_ctx ctx, const bm_area* areas, uint32_t n_areas, bm_batch
             A->batches.push_back(B);
         }
     }
-    cudaError_t e = cudaStreamCreateWithFlags(&B->cap, cudaStreamNonBlocking);
+    cudaError_t e = stream_like(ctx->stream(), &B->cap);
     if (e != cudaSuccess) { free_batch(B); return cuda_err(e, "cudaStreamCreate"); }
 
     std::vector<AreaCtl*> ctls;
