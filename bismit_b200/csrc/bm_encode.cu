@@ -160,6 +160,18 @@ __device__ inline void scalar_center(float val, float hi, int v_size, int u_size
     }
 }
 
+// Zeroes a frame of len bytes with the block's threads, 16 bytes a store
+// where the frame starts on a 16-byte boundary.
+__device__ __forceinline__ void clear_frame(uint8_t* frame, uint32_t len) {
+    uint32_t head = 0;
+    if (((uintptr_t)frame & 15) == 0) {
+        const uint32_t n16 = len / 16;
+        for (uint32_t i = threadIdx.x; i < n16; i += blockDim.x) ((uint4*)frame)[i] = make_uint4(0, 0, 0, 0);
+        head = n16 * 16;
+    }
+    for (uint32_t i = head + threadIdx.x; i < len; i += blockDim.x) frame[i] = 0;
+}
+
 // One block per frame: the frame is cleared, then the hexagon of radius
 // (v + u) / 32 around the value's center gets bytes in 64..127.
 __global__ void k_encode_scalar(const __grid_constant__ ScalarArgs A, uint8_t* __restrict__ frames, uint64_t stride,
@@ -167,7 +179,7 @@ __global__ void k_encode_scalar(const __grid_constant__ ScalarArgs A, uint8_t* _
     const uint32_t f = blockIdx.x;
     uint8_t* frame = frames + f * stride;
     const uint32_t len = v_size * u_size;
-    for (uint32_t i = threadIdx.x; i < len; i += blockDim.x) frame[i] = 0;
+    clear_frame(frame, len);
     __syncthreads();
     int cv, cu;
     scalar_center(A.vals[f], A.hi, (int)v_size, (int)u_size, cv, cu);
@@ -199,7 +211,7 @@ __global__ void k_encode_glyph(const __grid_constant__ GlyphArgs A, uint8_t* __r
     const uint32_t f = blockIdx.x;
     uint8_t* frame = frames + f * stride;
     const uint32_t len = v_size * u_size;
-    for (uint32_t i = threadIdx.x; i < len; i += blockDim.x) frame[i] = 0;
+    clear_frame(frame, len);
     __syncthreads();
     const int r = A.radius, side = 2 * r + 1, cv = A.cv[f], cu = A.cu[f];
     for (int k = threadIdx.x; k < side * side; k += blockDim.x) {
@@ -224,7 +236,7 @@ __global__ void k_encode_sdr(const __grid_constant__ SdrArgs A, const uint32_t* 
                              uint8_t* __restrict__ frames, uint64_t stride, uint32_t len) {
     const uint32_t f = blockIdx.x;
     uint8_t* frame = frames + f * stride;
-    for (uint32_t i = threadIdx.x; i < len; i += blockDim.x) frame[i] = 0;
+    clear_frame(frame, len);
     __syncthreads();
     const uint32_t* w0 = ways + (uint64_t)A.way0[f] * active;
     const uint32_t* w1 = w0 + active;
