@@ -220,6 +220,7 @@ def lib():
         "bm_area_write": (C.c_int, [vp, u32, u32, u64, vp, u64]),
         "bm_area_read_slab": (C.c_int, [vp, vp, u64]),
         "bm_area_side_steps": (C.c_int, [vp, P(u32)]),
+        "bm_area_front_steps": (C.c_int, [vp, P(u32)]),
         "bm_sampler_create": (C.c_int, [vp, u32, u32, C.c_int, P(vp)]),
         "bm_sampler_destroy": (C.c_int, [vp]),
         "bm_sampler_len": (C.c_int, [vp, P(u64)]),

@@ -196,6 +196,13 @@ class CorticalArea:
         F.check(self.lib.bm_area_side_steps(self.h, C.byref(v)))
         return v.value
 
+    def front_steps(self):
+        """Leading steps of the cycle that run on the front stream, beside the
+        previous cycle's later steps (0: none this cycle)."""
+        v = C.c_uint32()
+        F.check(self.lib.bm_area_front_steps(self.h, C.byref(v)))
+        return v.value
+
     def sampler(self, kind, layer=None, backpressure=False):
         """CorticalArea::sampler: a Sampler over `kind` (a SAMPLER_KINDS name)
         of data layer `layer` (name or index; for "axons", None = every axon)."""

@@ -243,7 +243,11 @@ void bm::exec_step(bm_area_s* A, const Step& st, cudaStream_t s, bool end_cycle)
     const bool pyr = L.kind == BM_LYR_PYRAMIDAL;
     // Launches on the area's own stream are counted (and timed when profiling);
     // a batch passes its own stream and does its own counting.
-    const bool own = s == A->stream() || (A->side && s == A->side);
+    const bool front = A->front && s == A->front;
+    const bool own = s == A->stream() || (A->side && s == A->side) || front;
+    // Launches on the front stream may run ahead of the area's counter: they
+    // take the number of the cycle being enqueued from the host.
+    const int64_t host_cycle = front ? (int64_t)A->host_cycle : -1;
     auto run = [&](int kind, auto&& f) {
         if (own) A->run(kind, f);
         else f();
@@ -252,7 +256,7 @@ void bm::exec_step(bm_area_s* A, const Step& st, cudaStream_t s, bool end_cycle)
     case ST_TUFT:
         if (A->fused.t[i][x].ok) {
             run(K_FUSED_TUFT,
-                [&] { launch_fused_tuft(A->fused, A->axns(), A->slices, D, i, x, A->ctl, s, (st.arg & 1) != 0); });
+                [&] { launch_fused_tuft(A->fused, A->axns(), A->slices, D, i, x, A->ctl, s, (st.arg & 1) != 0, host_cycle); });
         } else {
             run(K_TUFT_CELLS, [&] { launch_tuft_cells(A->axns(), A->slices, D, x, A->ctl, s); });
         }
@@ -260,7 +264,7 @@ void bm::exec_step(bm_area_s* A, const Step& st, cudaStream_t s, bool end_cycle)
     case ST_INHIB_MTP:
         run(K_INHIB_MTP, [&] {
             launch_inhib_mtp(A->axns(), A->slices, D, (int)L.ctrl[x].field_radius, A->inhib_key[i][x], st.arg != 0,
-                             A->ctl, s);
+                             A->ctl, s, host_cycle);
         });
         break;
     case ST_PYR_TAIL: {
@@ -403,7 +407,14 @@ bm::StepAccess bm::step_access(const bm_area_s* A, const Step& st, int t) {
     }
     case ST_DST_MTP:
     case ST_PYR_TAIL:
-        a.ax_r.set();
+        // The layer's own axons (soma output, learning's activity test), and
+        // the sources of the per-cell tufts folded into the tail.
+        layer_axons(P, i, a.ax_r);
+        for (uint32_t t = 0; t < P.layers[i].n_tufts && st.kind == ST_PYR_TAIL; t++)
+            if ((st.tufts >> t) & 1) {
+                if ((A->foreign_src[i] >> t) & 1) a.ax_r.set();
+                else tuft_sources(P, i, t, a.ax_r);
+            }
         layer_axons(P, i, a.ax_w);
         a.tf_r = a.tf_w = layer_tufts(P, i);
         a.ce_r = a.ce_w = 1u << i;
@@ -451,6 +462,123 @@ void bm::note_sources(bm_area_s* A, uint32_t i, uint64_t b, uint64_t e, const ui
     schedule_area(A);
 }
 
+namespace {
+
+// A step the front stream can take: a spatial layer's fused tuft (with its
+// folded soma step) or its inhibition with learning; their kernels take the
+// cycle number from the host.
+bool front_step_ok(const bm_area_s* A, const Step& st) {
+    const bm_area_plan& P = A->plan;
+    if (!(P.layers[st.layer].tags & BM_TAG_SPATIAL)) return false;
+    if (st.kind == ST_TUFT) return A->fused.t[st.layer][st.idx].ok;
+    return st.kind == ST_INHIB_MTP;
+}
+
+// What a frame intake writes: the axon slices of every input.
+StepAccess intake_access(const bm_area_plan& P) {
+    StepAccess a;
+    for (uint32_t i = 0; i < P.n_inputs; i++) {
+        const uint64_t b = P.inputs[i].axn_idz, e = b + P.inputs[i].len;
+        for (uint32_t s = 0; s < P.n_slices && s < BM_MAX_SLICES; s++) {
+            const uint64_t sb = P.slc_axn_idz[s], se = sb + (uint64_t)P.slc_v_size[s] * P.slc_u_size[s];
+            if (sb < e && b < se) a.ax_w.set(s);
+        }
+    }
+    return a;
+}
+
+void free_front_events(bm_area_s* A) {
+    for (cudaEvent_t ev : A->front_ev)
+        if (ev) cudaEventDestroy(ev);
+    for (cudaEvent_t ev : A->main_ev)
+        if (ev) cudaEventDestroy(ev);
+    A->front_ev.clear();
+    A->main_ev.clear();
+}
+
+// The front stream's part of the schedule (see bm_area_s::front_n): the
+// leading steps front_step_ok takes (at least one step must stay behind), the
+// previous cycle's steps each waits for (the cycle end excepted: front kernels
+// do not read the counter), the front steps each later step waits for, and
+// the intake's waits both ways. Filtered inputs keep the program's first step
+// a filter, so such areas have no front stream.
+int schedule_front(bm_area_s* A, const std::vector<StepAccess>& acc) {
+    const size_t n = A->steps.size();
+    free_front_events(A);
+    A->front_n = 0;
+    A->front_prev.clear();
+    A->front_waits.clear();
+    A->intake_prev.clear();
+    A->intake_readers.clear();
+    A->main_ev_needed.clear();
+    A->front_ax_w.reset();
+    size_t f = 0;
+    if (A->exec_path == BM_PATH_FUSED)
+        while (f < n && front_step_ok(A, A->steps[f])) f++;
+    // Work already queued on the main stream comes before the front stream's
+    // next steps (the new events have no records yet).
+    A->mark_main();
+    if (f == 0 || f >= n) return BM_OK;
+    A->front_prev.assign(f, {});
+    A->front_waits.assign(n, {});
+    A->main_ev_needed.assign(n, 0);
+    A->intake_readers.assign(n, 0);
+    for (size_t k = 0; k < f; k++) A->front_ax_w |= acc[k].ax_w;
+    const StepAccess in = intake_access(A->plan);
+    for (size_t t = f; t < n; t++) {
+        const bool counter_only = A->steps[t].kind == ST_CYCLE_END;
+        for (size_t k = 0; k < f; k++) {
+            if (!counter_only && conflict(acc[t], acc[k])) {
+                A->front_prev[k].push_back(t);
+                if (!A->step_side[t]) A->main_ev_needed[t] = 1;
+            }
+            if (conflict(acc[k], acc[t])) A->front_waits[t].push_back(k);
+        }
+        if (!counter_only && conflict(in, acc[t])) {
+            A->intake_prev.push_back(t);
+            if (!A->step_side[t]) A->main_ev_needed[t] = 1;
+            A->intake_readers[t] = 1;
+        }
+    }
+    cudaError_t e = cudaSuccess;
+    if (!A->front) e = stream_like(A->stream(), &A->front);
+    if (e == cudaSuccess && !A->intake_ev) e = cudaEventCreateWithFlags(&A->intake_ev, cudaEventDisableTiming);
+    if (e == cudaSuccess && !A->main_mark) e = cudaEventCreateWithFlags(&A->main_mark, cudaEventDisableTiming);
+    A->front_ev.assign(f, nullptr);
+    A->main_ev.assign(n, nullptr);
+    for (size_t k = 0; k < f && e == cudaSuccess; k++) e = cudaEventCreateWithFlags(&A->front_ev[k], cudaEventDisableTiming);
+    for (size_t t = 0; t < n && e == cudaSuccess; t++)
+        if (A->main_ev_needed[t]) e = cudaEventCreateWithFlags(&A->main_ev[t], cudaEventDisableTiming);
+    if (e != cudaSuccess) {
+        free_front_events(A);
+        return cuda_err(e, "front stream");
+    }
+    A->front_n = f;
+    return BM_OK;
+}
+
+}  // namespace
+
+// Front stream in use: scheduled, not profiling, and no sampler reading an
+// axon slice the front steps write (or anything but axons): a sampler's copy
+// follows its cycle on the main stream, and the next cycle's front steps
+// could otherwise overwrite the range before it is taken.
+bool bm_area_s::front_active() const {
+    if (!front_n || profiling || !front) return false;
+    for (const bm_sampler_s* S : samplers) {
+        uint64_t off, len;
+        sampler_range(S, &off, &len);
+        if (off < plan.axon_off || off + len > plan.axon_off + plan.n_axons) return false;
+        for (uint32_t s = 0; s < plan.n_slices && s < BM_MAX_SLICES; s++) {
+            if (!front_ax_w.test(s)) continue;
+            const uint64_t b = plan.axon_off + plan.slc_axn_idz[s];
+            const uint64_t e = b + (uint64_t)plan.slc_v_size[s] * plan.slc_u_size[s];
+            if (b < off + len && off < e) return false;
+        }
+    }
+    return true;
+}
+
 int bm::schedule_area(bm_area_s* A) {
     const size_t n = A->steps.size();
     std::vector<StepAccess> acc(n);
@@ -490,15 +618,16 @@ int bm::schedule_area(bm_area_s* A) {
     for (cudaEvent_t ev : A->side_ev)
         if (ev) cudaEventDestroy(ev);
     A->side_ev.clear();
-    if (A->last_side == SIZE_MAX) return BM_OK;
     cudaError_t e = cudaSuccess;
-    if (!A->side) e = stream_like(A->stream(), &A->side);
-    if (e == cudaSuccess && !A->ev_fork) e = cudaEventCreateWithFlags(&A->ev_fork, cudaEventDisableTiming);
-    A->side_ev.assign(n, nullptr);
-    for (size_t k = 0; k < n && e == cudaSuccess; k++)
-        if (A->step_side[k]) e = cudaEventCreateWithFlags(&A->side_ev[k], cudaEventDisableTiming);
-    if (e != cudaSuccess) return cuda_err(e, "side stream");
-    return BM_OK;
+    if (A->last_side != SIZE_MAX) {
+        if (!A->side) e = stream_like(A->stream(), &A->side);
+        if (e == cudaSuccess && !A->ev_fork) e = cudaEventCreateWithFlags(&A->ev_fork, cudaEventDisableTiming);
+        A->side_ev.assign(n, nullptr);
+        for (size_t k = 0; k < n && e == cudaSuccess; k++)
+            if (A->step_side[k]) e = cudaEventCreateWithFlags(&A->side_ev[k], cudaEventDisableTiming);
+        if (e != cudaSuccess) return cuda_err(e, "side stream");
+    }
+    return schedule_front(A, acc);
 }
 
 void bm::run_pending_verifies(bm_area_s* A, cudaStream_t s) {
@@ -531,12 +660,61 @@ void bm::refresh_geo(bm_area_s* A) {
 
 namespace {
 
+// Makes stream s wait for step t's event of the latest cycle that recorded it
+// (a side step's, or a main step's the front stream depends on).
+void wait_step(bm_area_s* A, size_t t, cudaStream_t s) {
+    if (A->last_side != SIZE_MAX && A->step_side[t]) cudaStreamWaitEvent(s, A->side_ev[t], 0);
+    else if (t < A->main_ev.size() && A->main_ev[t]) cudaStreamWaitEvent(s, A->main_ev[t], 0);
+}
+
+// Before front-stream work (an intake, or a cycle's front steps): after the
+// main stream's marked position, and after everything queued on the main
+// stream when the latest cycle did not use the front stream (nothing recorded
+// the events the front stream's waits refer to).
+void front_begin(bm_area_s* A) {
+    if (!A->front_last) A->mark_main();
+    cudaStreamWaitEvent(A->front, A->main_mark, 0);
+}
+
+// The stream a frame intake goes to, with its waits on the previous cycle
+// when that is the front stream.
+cudaStream_t intake_begin(bm_area_s* A) {
+    if (!A->front_active()) return A->stream();
+    front_begin(A);
+    for (size_t t : A->intake_prev) wait_step(A, t, A->front);
+    return A->front;
+}
+
+// After an intake's copies: later steps reading the inputs follow it, and with
+// `join` the main stream does too (an intake outside a cycling call).
+void intake_end(bm_area_s* A, cudaStream_t s, bool join) {
+    if (s != A->front) return;
+    cudaEventRecord(A->intake_ev, s);
+    if (join) cudaStreamWaitEvent(A->stream(), A->intake_ev, 0);
+}
+
 int enqueue_cycle(bm_area_s* A) {
     A->launches = 0;
     cudaStream_t main = A->stream();
+    bool verify = false;
+    for (uint32_t i = 0; i < A->plan.n_layers; i++) verify = verify || A->verify_pending[i];
     run_pending_verifies(A, main);
+    const bool front = A->front_active();
+    if (front && verify) A->mark_main();   // the compiled offsets the front steps read
+    const size_t nf = front ? A->front_n : 0;
     // Profiling times each launch on its own: everything on the main stream.
-    const bool fork = !A->profiling && A->last_side != SIZE_MAX;
+    size_t last_side = SIZE_MAX;
+    for (size_t k = nf; k < A->steps.size() && !A->profiling; k++)
+        if (A->step_side[k]) last_side = k;
+    const bool fork = last_side != SIZE_MAX;
+    if (front) {
+        front_begin(A);
+        for (size_t k = 0; k < nf; k++) {
+            for (size_t t : A->front_prev[k]) wait_step(A, t, A->front);
+            exec_step(A, A->steps[k], A->front, false);
+            cudaEventRecord(A->front_ev[k], A->front);
+        }
+    }
     if (fork) {
         cudaEventRecord(A->ev_fork, main);
         cudaStreamWaitEvent(A->side, A->ev_fork, 0);
@@ -544,14 +722,25 @@ int enqueue_cycle(bm_area_s* A) {
     // With end_in_tail the last pyramidal tail ends the cycle itself and the
     // cycle-end step (the last) launches nothing.
     const size_t n = A->steps.size() - (A->end_in_tail ? 1 : 0);
-    for (size_t k = 0; k < n; k++) {
+    const bool regrow_fires = A->host_cycle % kRegrowPeriod == kRegrowPeriod - 1;
+    for (size_t k = nf; k < n; k++) {
         const bool on_side = fork && A->step_side[k];
+        cudaStream_t s = on_side ? A->side : main;
         if (fork && !on_side)
-            for (size_t j : A->step_waits[k]) cudaStreamWaitEvent(main, A->side_ev[j], 0);
-        exec_step(A, A->steps[k], on_side ? A->side : main, A->end_in_tail && k + 1 == n);
+            for (size_t j : A->step_waits[k])
+                if (j >= nf) cudaStreamWaitEvent(main, A->side_ev[j], 0);
+        if (front) {
+            for (size_t j : A->front_waits[k]) cudaStreamWaitEvent(s, A->front_ev[j], 0);
+            if (A->intake_readers[k]) cudaStreamWaitEvent(s, A->intake_ev, 0);
+        }
+        exec_step(A, A->steps[k], s, A->end_in_tail && k + 1 == n);
         if (on_side) cudaEventRecord(A->side_ev[k], A->side);
+        else if (front && A->main_ev_needed[k] && (A->steps[k].kind != ST_REGROW || regrow_fires))
+            cudaEventRecord(A->main_ev[k], main);
     }
-    if (fork) cudaStreamWaitEvent(main, A->side_ev[A->last_side], 0);
+    if (fork) cudaStreamWaitEvent(main, A->side_ev[last_side], 0);
+    if (front) cudaStreamWaitEvent(main, A->front_ev[nf - 1], 0);
+    A->front_last = front;
     A->host_cycle++;
     return A->samplers.empty() ? BM_OK : sample_after_cycle(A, main);
 }
@@ -723,6 +912,10 @@ void free_area(bm_area_s* A) {
                 if (c) cudaFree(c);
         if (A->side) cudaStreamDestroy(A->side);
         if (A->ev_fork) cudaEventDestroy(A->ev_fork);
+        free_front_events(A);
+        if (A->front) cudaStreamDestroy(A->front);
+        if (A->intake_ev) cudaEventDestroy(A->intake_ev);
+        if (A->main_mark) cudaEventDestroy(A->main_mark);
         for (cudaEvent_t e : A->side_ev)
             if (e) cudaEventDestroy(e);
         for (auto& r : A->pending) { cudaEventDestroy(r.a); cudaEventDestroy(r.b); }
@@ -822,11 +1015,13 @@ int write_host_frame(bm_area_s* A, uint32_t input, const uint8_t* frame, size_t 
     e = cudaStreamWaitEvent(A->up, A->up_taken[k], 0);
     if (e == cudaSuccess) e = cudaMemcpyAsync(A->up_dev[k], A->up_host[k], len, cudaMemcpyHostToDevice, A->up);
     if (e == cudaSuccess) e = cudaEventRecord(A->up_loaded[k], A->up);
-    if (e == cudaSuccess) e = cudaStreamWaitEvent(A->stream(), A->up_loaded[k], 0);
+    const cudaStream_t s = intake_begin(A);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(s, A->up_loaded[k], 0);
     if (e != cudaSuccess) return cuda_err(e, "input upload");
-    const int rc = write_frame(A, input, A->up_dev[k], cudaMemcpyDeviceToDevice, A->stream());
+    const int rc = write_frame(A, input, A->up_dev[k], cudaMemcpyDeviceToDevice, s);
     if (rc != BM_OK) return rc;
-    e = cudaEventRecord(A->up_taken[k], A->stream());
+    e = cudaEventRecord(A->up_taken[k], s);
+    intake_end(A, s, true);
     return e == cudaSuccess ? BM_OK : cuda_err(e, "input upload");
 }
 
@@ -1040,7 +1235,10 @@ int bm_area_write_input_device(bm_area area, uint32_t input_idx, const void* dev
     if (input_idx >= P.n_inputs) return set_err(BM_ERR_INVALID, "input %u out of range", input_idx);
     if (len != P.inputs[input_idx].len) return set_err(BM_ERR_INVALID, "frame length %zu != %u", len, P.inputs[input_idx].len);
     DevGuard g(area->ctx->device);
-    return write_frame(area, input_idx, dev_frame, cudaMemcpyDeviceToDevice, area->stream());
+    const cudaStream_t s = intake_begin(area);
+    const int rc = write_frame(area, input_idx, dev_frame, cudaMemcpyDeviceToDevice, s);
+    intake_end(area, s, true);
+    return rc;
 }
 
 namespace {
@@ -1078,8 +1276,10 @@ int bm_area_cycle_frames_device(bm_area area, const void* dev_frames, size_t fra
     for (uint32_t k = 0; k < n_cycles; k++) {
         int rc = BM_OK;
         area->run(K_INTAKE, [&] {
+            const cudaStream_t s = intake_begin(area);
             rc = write_frame(area, 0, (const uint8_t*)dev_frames + (uint64_t)k * frame_len, cudaMemcpyDeviceToDevice,
-                             area->stream());
+                             s);
+            intake_end(area, s, false);
         });
         if (rc == BM_OK) rc = enqueue_cycle(area);
         if (rc != BM_OK) return rc;
@@ -1190,7 +1390,9 @@ int bm_area_deliver_tract(bm_area src, uint32_t src_output, bm_area dst, uint32_
     const uint8_t* from = src->axns() + src->plan.outputs[src_output].axn_idz;
     std::vector<FramePiece> pieces;
     frame_pieces(dst, dst_input, (uint32_t)dst_offset, len, pieces);
-    return copy_pieces(pieces, from, cudaMemcpyDeviceToDevice, s);
+    const int rc = copy_pieces(pieces, from, cudaMemcpyDeviceToDevice, s);
+    dst->mark_main();   // the destination's front steps read its inputs
+    return rc;
 }
 
 int bm_area_clear_errors(bm_area area) {
@@ -1266,6 +1468,12 @@ int bm_area_set_cycle(bm_area area, uint64_t cycle) {
     CU(cudaMemcpyAsync(&area->ctl->cycle, &c, sizeof c, cudaMemcpyHostToDevice, area->stream()));
     CU(cudaStreamSynchronize(area->stream()));
     area->host_cycle = cycle;
+    return BM_OK;
+}
+
+int bm_area_front_steps(bm_area area, uint32_t* n) {
+    if (!area || !n) return set_err(BM_ERR_INVALID, "null argument");
+    *n = area->front_active() ? (uint32_t)area->front_n : 0u;
     return BM_OK;
 }
 

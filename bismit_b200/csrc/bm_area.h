@@ -155,6 +155,27 @@ struct bm_area_s {
     cudaStream_t side = nullptr;
     cudaEvent_t ev_fork = nullptr;
     std::vector<cudaEvent_t> side_ev;
+    // Front stream (schedule_area): the program's leading spatial-layer steps
+    // (fused tuft, inhibition with learning) and the frame intake run there,
+    // each ordered against the previous cycle only by what it touches, so a
+    // cycle's spatial chain runs beside the previous cycle's pyramidal steps.
+    // Their kernels take the cycle number from the host (the area's counter
+    // advances at the end of the previous cycle on the main stream).
+    size_t front_n = 0;                                  // leading steps on the front stream (0: none)
+    std::vector<std::vector<size_t>> front_prev;         // per front step: steps of the previous cycle to wait for
+    std::vector<std::vector<size_t>> front_waits;        // per later step: front steps of its cycle to wait for
+    std::vector<size_t> intake_prev;                     // steps of the previous cycle the intake waits for
+    std::vector<uint8_t> intake_readers;                 // later steps reading what the intake writes
+    std::vector<uint8_t> main_ev_needed;                 // main steps a front step or the intake waits for
+    std::bitset<BM_MAX_SLICES> front_ax_w;               // axon slices the front steps write
+    std::vector<cudaEvent_t> front_ev, main_ev;
+    cudaEvent_t intake_ev = nullptr;
+    // Recorded on the main stream after work there that the front stream's
+    // next steps must follow (verifications, batched cycles, tract copies,
+    // control writes); the front stream waits for it at each cycle's start.
+    cudaEvent_t main_mark = nullptr;
+    cudaStream_t front = nullptr;
+    bool front_last = false;      // the latest enqueued cycle used the front stream
     std::vector<bm_sampler_s*> samplers;   // per-cycle readback channels (bm_sampler.cu)
     // Host frames (bm_area_write_input) are copied into a pinned slot during
     // the call, uploaded on `up` into a device slot while earlier cycles
@@ -189,6 +210,14 @@ struct bm_area_s {
     bm::TuftGeo geo[BM_MAX_LAYERS][BM_MAX_TUFTS] = {};
 
     cudaStream_t stream() const { return ctx->stream(); }
+    // Front stream in use this cycle (see front_n).
+    bool front_active() const;
+    // The stream frame intakes go to: the front stream when it is in use.
+    cudaStream_t intake_stream() const { return front_active() ? front : stream(); }
+    // Marks the main stream's current position for the front stream.
+    void mark_main() {
+        if (main_mark) cudaEventRecord(main_mark, stream());
+    }
     // Device error bits a completed cycle mirrored to the host (0: none seen).
     unsigned int seen_errors() const { return host_err ? *(volatile const unsigned int*)host_err : 0u; }
     uint8_t* axns() const { return slab + plan.axon_off; }
@@ -273,6 +302,8 @@ void note_sources(bm_area_s* A, uint32_t i, uint64_t b, uint64_t e, const uint8_
 // After a cycle of A enqueued on stream s: sends each sampler's frame, or
 // skips it, or waits for the receiver (bm_sampler.cu).
 int sample_after_cycle(bm_area_s* A, cudaStream_t s);
+// The slab range a sampler reads.
+void sampler_range(const bm_sampler_s* S, uint64_t* off, uint64_t* len);
 void free_samplers(bm_area_s* A);
 // Detaches A from the batches holding it before it is destroyed (bm_batch.cu).
 void detach_from_batches(bm_area_s* A);

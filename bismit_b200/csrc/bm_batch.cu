@@ -805,6 +805,8 @@ int run_cycles(bm_batch_s* B, const void* frames, uint32_t n_cycles, bool refuse
             if (rc != BM_OK) return rc;
         }
     }
+    // An area cycling on its own later starts its front stream after these.
+    for (bm_area A : B->areas) A->mark_main();
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_err(e, "batched cycle");
     return BM_OK;

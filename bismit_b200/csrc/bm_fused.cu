@@ -116,7 +116,14 @@ struct FusedTuftArgs {
     uint32_t fp_tma;                    // the footprint comes from a tensor box load (else consumers stage it)
     uint32_t ssc_soma;                  // also run ssc_cycle (spiny stellate cells of one dendrite)
     uint32_t fp_bytes;                  // bytes of that box (nrec * frows * fw)
+    uint32_t cycle_from_host;           // take the cycle number from `cycle` rather than the area's counter
+    unsigned long long cycle;           // (a launch on the area's front stream, which may run ahead of the
+                                        // counter: the host knows the number of the cycle it enqueues)
 };
+// The cycle number a launch draws its random value for.
+__device__ __forceinline__ unsigned long long cycle_of(const FusedTuftArgs& A) {
+    return A.cycle_from_host ? A.cycle : A.ctl->cycle;
+}
 static_assert(offsetof(FusedTuftArgs, tmap) == 0 && alignof(FusedTuftArgs) >= 64,
               "the tensor map must sit 64-byte aligned in the parameter block");
 
@@ -404,7 +411,7 @@ __global__ void __launch_bounds__(kWarps * 32) k_fused_tuft(FusedTuftArgs A) {
     const int wib = threadIdx.x >> 5;
     const uint64_t gwarp = (uint64_t)blockIdx.x * kWarps + wib;
     const uint64_t nwarps = (uint64_t)gridDim.x * kWarps;
-    const int32_t rnd = rnd_at(A.rnd_key, A.ctl->cycle);
+    const int32_t rnd = rnd_at(A.rnd_key, cycle_of(A));
     const bool flags_clean = (A.ctl->tuft_status[A.status_idx] & kTuftFlagsForeign) == 0;
     for (uint64_t unit = gwarp; unit < A.n_units; unit += nwarps) {
         uint32_t t_key = 0, t_best = 0, t_sum = 0, tuft_cur = 0;
@@ -1039,7 +1046,7 @@ __device__ __forceinline__ void tma_body(const FusedTuftArgs& A, uint8_t* smem, 
         return;
     }
     // ---- consumer warps ----
-    const int32_t rnd = rnd_at(A.rnd_key, A.ctl->cycle);
+    const int32_t rnd = rnd_at(A.rnd_key, cycle_of(A));
     uint32_t ring = 0;
     bool ok = true;
     for (uint32_t t = blockIdx.x; t < A.n_tiles; t += gridDim.x) {
@@ -1199,7 +1206,7 @@ __global__ void __launch_bounds__(kThreads, 3) k_fused_tuft_batch(const __grid_c
         if (j != cur) {
             cur = j;
             mode = mode_of(A);
-            rnd = rnd_at(A.rnd_key, A.ctl->cycle);
+            rnd = rnd_at(A.rnd_key, cycle_of(A));
             limit_us = wait_limit_us(A.ctl);
         }
         const TileGeo G = tile_geo(A, t - P.tile0[j]);
@@ -1736,10 +1743,14 @@ void make_args(FusedTuftArgs& A, const FusedArea& F, const uint8_t* axns, const 
 }  // namespace
 
 void launch_fused_tuft(const FusedArea& F, const uint8_t* axns, const SliceRec* slices, const DevLayer& L,
-                       uint32_t layer, uint32_t t, AreaCtl* ctl, cudaStream_t s, bool ssc_soma) {
+                       uint32_t layer, uint32_t t, AreaCtl* ctl, cudaStream_t s, bool ssc_soma, int64_t host_cycle) {
     const FusedTuft& FT = F.t[layer][t];
     FusedTuftArgs A;
     make_args(A, F, axns, slices, L, layer, t, ctl, ssc_soma);
+    if (host_cycle >= 0) {
+        A.cycle_from_host = 1;
+        A.cycle = (unsigned long long)host_cycle;
+    }
     const bool tuft = L.kind == BM_LYR_PYRAMIDAL;
     if (FT.tiled) {
         auto kern = tuft ? k_fused_tuft_tma<true> : k_fused_tuft_tma<false>;

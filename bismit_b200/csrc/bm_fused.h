@@ -77,7 +77,9 @@ GatherGeo gather_geo(const FusedArea& F, const bm_area_plan& P, uint32_t layer, 
 // With ssc_soma (a spiny stellate layer whose cells have one dendrite),
 // ssc_cycle runs in the same launch (the step that follows the tuft's).
 void launch_fused_tuft(const FusedArea& F, const uint8_t* axns, const SliceRec* slices, const DevLayer& L,
-                       uint32_t layer, uint32_t t, AreaCtl* ctl, cudaStream_t s, bool ssc_soma = false);
+                       uint32_t layer, uint32_t t, AreaCtl* ctl, cudaStream_t s, bool ssc_soma = false,
+                       int64_t host_cycle = -1);   // >= 0: the cycle number, for a launch that may run ahead of
+                                                   // the area's counter
 // Recomputes AreaCtl::tuft_status for the fused tufts of a layer (after its
 // synapse sources or flags were written by the caller).
 void launch_verify_tufts(const FusedArea& F, const DevLayer& L, uint32_t layer, AreaCtl* ctl, cudaStream_t s);

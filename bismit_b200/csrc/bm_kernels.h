@@ -138,7 +138,7 @@ void launch_retina(const uint8_t* in, uint8_t* out, const SliceRec* slices, uint
 void launch_tuft_cells(const uint8_t* axns, const SliceRec* slices, const DevLayer& L, uint32_t t,
                        const AreaCtl* ctl, cudaStream_t s);
 void launch_inhib_mtp(uint8_t* axns, const SliceRec* slices, const DevLayer& L, int radius, uint64_t key,
-                      bool learn, const AreaCtl* ctl, cudaStream_t s);
+                      bool learn, const AreaCtl* ctl, cudaStream_t s, int64_t host_cycle = -1);
 // `tufts` (bit t): tufts the fused tuft kernel does not take, run per cell
 // first; `end`: the last block to finish also ends the cycle.
 void launch_pyr_tail(uint8_t* axns, const SliceRec* slices, const DevLayer& L, int ctrl, bool learn, AreaCtl* ctl,

@@ -112,14 +112,17 @@ __global__ void k_tuft_cells(const uint8_t* __restrict__ axns, const SliceRec* _
     if (c < L.cells) tuft_cell_item(axns, slices, L, t, rnd_at(L.tft[t].rnd_key_den, ctl->cycle), c);
 }
 
-// Warp-cooperative: no thread leaves before the warp's shared part.
+// Warp-cooperative: no thread leaves before the warp's shared part. With
+// host_cycle >= 0 the cycle number comes from the host (a launch on the
+// area's front stream, which may run ahead of the area's counter).
 __global__ void __launch_bounds__(128) k_inhib_mtp(uint8_t* __restrict__ axns, const SliceRec* __restrict__ slices,
                                                    DevLayer L, int radius, uint64_t key, int learn,
-                                                   const AreaCtl* ctl) {
+                                                   const AreaCtl* ctl, long long host_cycle) {
     pdl_begin();
     uint32_t c = (uint32_t)gtid();
-    inhib_mtp_warp(axns, slices, L, radius, rnd_at(key, ctl->cycle), rnd_at(L.rnd_key_ssc_mtp, ctl->cycle),
-                   learn != 0, c, c < L.cells);
+    const unsigned long long cyc = host_cycle >= 0 ? (unsigned long long)host_cycle : ctl->cycle;
+    inhib_mtp_warp(axns, slices, L, radius, rnd_at(key, cyc), rnd_at(L.rnd_key_ssc_mtp, cyc), learn != 0, c,
+                   c < L.cells);
 }
 
 // With end_cycle, the last block to finish also ends the cycle (the cycle-end
@@ -297,8 +300,9 @@ void launch_tuft_cells(const uint8_t* axns, const SliceRec* slices, const DevLay
     launch_pdl(k_tuft_cells, nblk(L.cells, 128), 128, 0, s, axns, slices, L, t, ctl);
 }
 void launch_inhib_mtp(uint8_t* axns, const SliceRec* slices, const DevLayer& L, int radius, uint64_t key,
-                      bool learn, const AreaCtl* ctl, cudaStream_t s) {
-    launch_pdl(k_inhib_mtp, nblk(L.cells, 128), 128, 0, s, axns, slices, L, radius, key, learn ? 1 : 0, ctl);
+                      bool learn, const AreaCtl* ctl, cudaStream_t s, int64_t host_cycle) {
+    launch_pdl(k_inhib_mtp, nblk(L.cells, 128), 128, 0, s, axns, slices, L, radius, key, learn ? 1 : 0, ctl,
+               (long long)host_cycle);
 }
 void launch_pyr_tail(uint8_t* axns, const SliceRec* slices, const DevLayer& L, int ctrl, bool learn, AreaCtl* ctl,
                      cudaStream_t s, uint32_t tufts, bool end) {

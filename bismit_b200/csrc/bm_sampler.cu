@@ -78,6 +78,11 @@ void destroy_sampler(bm_sampler_s* S) {
 
 }  // namespace
 
+void bm::sampler_range(const bm_sampler_s* S, uint64_t* off, uint64_t* len) {
+    *off = S->off;
+    *len = S->len;
+}
+
 int bm::sample_after_cycle(bm_area_s* A, cudaStream_t s) {
     for (bm_sampler_s* S : A->samplers) {
         std::unique_lock<std::mutex> lk(S->mu);

@@ -436,6 +436,13 @@ int bm_area_slab_ptr(bm_area area, void** out);
  * cycle, e.g. pyramidal distal tufts). Caller-written source slice ids
  * outside a tuft's pool keep that tuft's steps in the chain. */
 int bm_area_side_steps(bm_area area, uint32_t* n);
+/* Leading steps of the area's cycle that run on its front stream (0: none
+ * this cycle): the spatial layers' fused tuft and inhibition launches, with
+ * the frame intake. Each waits only for the steps of the previous cycle it
+ * touches the buffers of, so one cycle's spatial chain runs beside the
+ * previous cycle's pyramidal steps; they take the cycle number from the host.
+ * Not used while profiling, or while a sampler reads a buffer they write. */
+int bm_area_front_steps(bm_area area, uint32_t* n);
 int bm_area_sources_changed(bm_area area, uint32_t layer);
 
 /* One tract's delivery between two areas of a cortex cycled one area after

@@ -87,6 +87,9 @@ def test_area_256_matches_oracle(ctx, state, plain):
             assert not f["flags_foreign"] and not f["sources_outside"], (i, t, f)
             assert f["consumer"] == (2 if i == ssc else 6), (i, t, f)
         assert forms[(pyr, 0)]["tile_w"] < plan.layers[pyr].u_size   # rows cut into parts
+    # The spiny stellate tuft and inhibition run on the front stream, beside
+    # the previous cycle's pyramidal steps (none on the plain path).
+    assert area.front_steps() == (0 if plain else 2)
     n = 2 if plain else 3
     fr = configs.frames(n, area.input_len(), act, 5)
     ora = slab.copy()
@@ -127,6 +130,9 @@ def test_area_64_thousand_cycles(ctx, form):
         ssc = _layer_of_kind(plan, F.BM_LYR_SPINY_STELLATE)
         assert forms[(ssc, 0)]["consumer"] == 1
         assert any(f["consumer"] == 6 for f in forms.values())   # the distal 16 x 32 tuft
+    # Eager cycles from device frames overlap one cycle's spiny stellate chain
+    # with the previous cycle's pyramidal steps (the front stream).
+    assert area.front_steps() == (2 if form == "fused" else 0)
     ora = area.read_slab()
     start = ora.copy()
     done = 0

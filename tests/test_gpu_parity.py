@@ -246,6 +246,45 @@ def test_side_stream_follows_caller_sources(ctx):
     area.close()
 
 
+@pytest.mark.parametrize("sampled", ["none", "pyramidal_axons", "ssc_axons"])
+def test_front_stream_cycles_match_oracle(ctx, sampled):
+    """The spiny stellate tuft and inhibition run on the front stream, each
+    cycle's beside the previous cycle's pyramidal steps, with host frames
+    (one call per cycle) and with a block of device frames (one call for
+    several cycles). A sampler of the pyramidal axons leaves the front stream
+    in use and gets every cycle's frame; one of the spiny stellate axons, which
+    the front steps write, turns it off. Whole slabs equal the oracle's."""
+    import torch
+    area = _area(ctx, "area_256_shape", settings_for())
+    plan = area.plan
+    slab = initial_slab(plan, 7, scramble_seed=23, clean_flags=True)
+    area.write_slab(slab)
+    area.set_cycle(0)
+    ssc = next(i for i in range(plan.n_layers) if plan.layers[i].kind == F.BM_LYR_SPINY_STELLATE)
+    pyr = next(i for i in range(plan.n_layers) if plan.layers[i].kind == F.BM_LYR_PYRAMIDAL)
+    smp = None if sampled == "none" else area.sampler("axons", pyr if sampled == "pyramidal_axons" else ssc)
+    assert area.front_steps() == (0 if sampled == "ssc_axons" else 2)
+    fr = frames_for(plan, 8, 5, 0.05)
+    ora = slab.copy()
+    for c in range(3):
+        area.write_input(fr[c])
+        area.cycle(1)
+        oracle.run(plan, ora, fr[c:c + 1], 1, start_cycle=c)
+        if smp is not None:
+            cyc, frame = smp.recv(wait_for_frame=True)
+            assert cyc == c
+    dev = torch.from_numpy(np.ascontiguousarray(fr[3:])).to("cuda:0")
+    torch.cuda.synchronize()
+    area.cycle_frames_device(dev.data_ptr(), fr.shape[1], 5)
+    oracle.run(plan, ora, fr[3:], 5, start_cycle=3)
+    got = area.read_slab()
+    assert np.array_equal(got, ora), diff_report(plan, got, ora)
+    assert area.cycle_count() == 8
+    if smp is not None:
+        smp.close()
+    area.close()
+
+
 def test_device_error_bits_clear(ctx):
     import ctypes
     area = _area(ctx, "area_64", settings_for())
