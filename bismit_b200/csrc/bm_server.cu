@@ -132,9 +132,8 @@ struct bm_server_s {
         double syn = 0, started = 0;
         uint32_t buf = 0;
     };
-    bm_ctx ctx = nullptr;            // the serving stream (the server's own, highest priority)
-    bm_ctx setup = nullptr;          // area construction, overlapping the ticks (lowest priority)
-    bm_ctx caller = nullptr;         // the context the server was created on (held, for its device)
+    bm_ctx ctx = nullptr;            // the serving stream
+    bm_ctx setup = nullptr;          // area construction, overlapping the ticks
     uint64_t budget = 0, used = 0;
     uint32_t next_id = 1;
     std::vector<Session*> sessions;  // every open session, in open order
@@ -212,19 +211,6 @@ int build_session(bm_server_s* V, bm_server_s::Session* S) {
         return set_err(BM_ERR_OOM, "pinned output buffer");
     }
     std::memset(S->out, 0, S->out_len ? S->out_len : 1);
-    return BM_OK;
-}
-
-// Replaces c's own stream with a non-blocking one at the device's highest
-// (or lowest) stream priority.
-int prioritise(bm_ctx c, bool highest) {
-    int least = 0, greatest = 0;
-    cudaError_t e = cudaDeviceGetStreamPriorityRange(&least, &greatest);
-    cudaStream_t st = nullptr;
-    if (e == cudaSuccess) e = cudaStreamCreateWithPriority(&st, cudaStreamNonBlocking, highest ? greatest : least);
-    if (e != cudaSuccess) return cuda_err(e, "server stream");
-    cudaStreamDestroy(c->own);
-    c->own = st;
     return BM_OK;
 }
 
@@ -441,19 +427,7 @@ int bm_server_create(bm_ctx ctx, uint64_t mem_budget, bm_server* out) {
     if (!V) return set_err(BM_ERR_OOM, "host allocation failed");
     int rc = bm_ctx_create(ctx->device, 0, &V->setup);
     if (rc != BM_OK) { delete V; return rc; }
-    // Ticks run on the server's own stream at the device's highest priority,
-    // the builder's set-up (growth kernels of up to tens of ms) at the lowest:
-    // blocks of a tick are scheduled ahead of a growth kernel's as SMs free up.
-    rc = bm_ctx_create(ctx->device, 0, &V->ctx);
-    if (rc == BM_OK) rc = prioritise(V->ctx, true);
-    if (rc == BM_OK) rc = prioritise(V->setup, false);
-    if (rc != BM_OK) {
-        if (V->ctx) bm_ctx_destroy(V->ctx);
-        bm_ctx_destroy(V->setup);
-        delete V;
-        return rc;
-    }
-    V->caller = ctx;
+    V->ctx = ctx;
     ctx_retain(ctx);
     if (!mem_budget) {
         size_t fr = 0, tot = 0;
@@ -469,8 +443,7 @@ int bm_server_create(bm_ctx ctx, uint64_t mem_budget, bm_server* out) {
             if (V->start_ev[b]) cudaEventDestroy(V->start_ev[b]);
         }
         bm_ctx_destroy(V->setup);
-        bm_ctx_destroy(V->ctx);
-        ctx_release(V->caller);
+        ctx_release(V->ctx);
         delete V;
         return set_err(BM_ERR_CUDA, "cudaEventCreate");
     }
@@ -501,8 +474,7 @@ int bm_server_destroy(bm_server V) {
     if (V->d_out) cudaFree(V->d_out);
     if (V->d_outjobs) cudaFree(V->d_outjobs);
     bm_ctx_destroy(V->setup);
-    bm_ctx_destroy(V->ctx);
-    ctx_release(V->caller);
+    ctx_release(V->ctx);
     delete V;
     return BM_OK;
 }

@@ -662,9 +662,7 @@ typedef struct bm_server_stats {
                                      8 ticks)                                    */
 } bm_server_stats;
 
-/* mem_budget 0: 90 % of the device memory free at creation. The server runs
- * its ticks on a stream of its own at the device's highest stream priority
- * and builds sessions' areas on one at the lowest (ctx gives the device). */
+/* mem_budget 0: 90 % of the device memory free at creation. */
 int bm_server_create(bm_ctx ctx, uint64_t mem_budget, bm_server* out);
 int bm_server_destroy(bm_server server);
 /* Queues a session; BM_ERR_OOM if it could never fit the budget. */
