@@ -132,7 +132,7 @@ def test_area_64_thousand_cycles(ctx, form):
         assert any(f["consumer"] == 6 for f in forms.values())   # the distal 16 x 32 tuft
     # Eager cycles from device frames overlap one cycle's spiny stellate chain
     # with the previous cycle's pyramidal steps (the front stream).
-    assert area.front_steps() == (2 if form == "fused" else 0)
+    assert area.front_steps() == (0 if form == "plain" else 2)
     ora = area.read_slab()
     start = ora.copy()
     done = 0
