@@ -48,7 +48,15 @@ __device__ __forceinline__ void draw_src(const GrowTuft& G, uint64_t w, uint64_t
     }
 }
 
-__global__ void k_grow(DevLayer L, GrowTuft G) {
+// Dendrites of up to this many synapses keep their drawn sources' keys in
+// shared memory for the uniqueness test (one row per thread, padded against
+// bank conflicts; 32-bit while the keys fit, below 2^31); longer ones, or
+// grids too large for those keys, read the sources back from the slab.
+constexpr uint32_t kGrowKeys = 64;
+constexpr uint32_t kGrowBlock = 128;
+
+__global__ void __launch_bounds__(kGrowBlock) k_grow(DevLayer L, GrowTuft G) {
+    __shared__ int32_t keys[kGrowBlock][kGrowKeys + 1];
     uint64_t d = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const DevTuft& T = L.tft[G.tft];
     uint64_t n_dens = (uint64_t)L.cells * T.dpt;
@@ -60,23 +68,28 @@ __global__ void k_grow(DevLayer L, GrowTuft G) {
     int64_t cols = (int64_t)L.v_size * L.u_size;
     uint64_t s0 = T.syn_idz + d * T.spd;
     uint64_t wk = 0;
+    const bool cached = T.spd <= kGrowKeys && cols < (1ll << 22);   // |key| < 382 * 2^22 < 2^31
+    int32_t* my = keys[threadIdx.x];
     for (uint32_t j = 0; j < T.spd; j++) {
         uint8_t ns = 0;
         int nv = 0, nu = 0, nstr = 0;
+        int64_t nk = 0;
         for (int att = 0; att < kGrowMaxAttempts; att++) {
             const uint64_t w = grow_word(G.key, d, wk++);
             const uint64_t w2 = grow_word(G.key, d, wk++);
             draw_src(G, w, w2, ns, nv, nu, nstr);
+            nk = (int64_t)ns * cols + (int64_t)nv * L.u_size + nu;
             if (!G.unique) break;
-            int64_t nk = (int64_t)ns * cols + (int64_t)nv * L.u_size + nu;
             if (nk == 0) break;  // key 0 is never retained (old-source removal at init)
             bool dup = false;
             for (uint32_t jj = 0; jj < j; jj++) {
-                int64_t ok = (int64_t)slc[s0 + jj] * cols + (int64_t)vo[s0 + jj] * L.u_size + uo[s0 + jj];
+                const int64_t ok = cached ? (int64_t)my[jj]
+                                          : (int64_t)slc[s0 + jj] * cols + (int64_t)vo[s0 + jj] * L.u_size + uo[s0 + jj];
                 if (ok == nk) { dup = true; break; }
             }
             if (!dup) break;
         }
+        if (cached) my[j] = (int32_t)nk;
         slc[s0 + j] = ns;
         vo[s0 + j] = (int8_t)nv;
         uo[s0 + j] = (int8_t)nu;
@@ -191,7 +204,7 @@ __global__ void __launch_bounds__(kRegrowBlock) k_regrow(const RegrowJob* __rest
 
 void launch_grow(const DevLayer& L, const GrowTuft& G, cudaStream_t s) {
     uint64_t n = (uint64_t)L.cells * L.tft[G.tft].dpt;
-    k_grow<<<(unsigned)((n + 127) / 128), 128, 0, s>>>(L, G);
+    k_grow<<<(unsigned)((n + kGrowBlock - 1) / kGrowBlock), kGrowBlock, 0, s>>>(L, G);
 }
 
 void launch_cycle_end(AreaCtl* ctl, cudaStream_t s) { launch_pdl(k_cycle_end, 1, 1, 0, s, ctl); }
