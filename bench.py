@@ -662,6 +662,7 @@ def run_serving(args, ctx):
     srv = cortex.Server(ctx, int(args.serve_budget_gb * 1e9))
     opened, total, queued = 0, 0, 0
     t_tick = t_submit = 0.0
+    tick_calls = []
     t0 = time.perf_counter()
     while True:
         now = time.perf_counter() - t0
@@ -679,7 +680,9 @@ def run_serving(args, ctx):
             opened += 1
         ts = time.perf_counter()
         cycled = srv.tick()
-        t_tick += time.perf_counter() - ts
+        dt = time.perf_counter() - ts
+        t_tick += dt
+        tick_calls.append(dt)
         queued += cycled
         if opened == n and queued >= total:
             srv.drain()
@@ -699,6 +702,9 @@ def run_serving(args, ctx):
         "ticks": int(st["ticks"]), "batch_rebuilds": int(st["batch_rebuilds"]),
         "rebuild_s": round(st["rebuild_s"], 3), "rebuild_drains": st["rebuild_drains"],
         "capture_s": round(st["capture_s"], 3), "admit_s": round(st["admit_s"], 3), "gpu_s": round(st["gpu_s"], 3),
+        "tick_device_p99_ms": round(st["tick_p99_ms"], 3), "tick_device_max_ms": round(st["tick_max_ms"], 3),
+        "tick_call_p99_ms": round(float(np.percentile(tick_calls, 99)) * 1e3, 3) if tick_calls else None,
+        "tick_call_max_ms": round(max(tick_calls) * 1e3, 3) if tick_calls else None,
         "tick_call_s": round(t_tick, 3), "submit_s": round(t_submit, 3), "wall_s": round(wall, 3),
         "latency": "per frame: tick completion minus the moment the frame was ready (its session's previous "
                    "frame done, or its arrival); admission waits included",

@@ -179,7 +179,8 @@ class bm_server_stats(C.Structure):
                 ("p50_ms", C.c_double), ("p99_ms", C.c_double), ("mean_ms", C.c_double),
                 ("used_bytes", C.c_uint64), ("budget_bytes", C.c_uint64),
                 ("resident", C.c_uint32), ("waiting", C.c_uint32), ("failed", C.c_uint32),
-                ("rebuild_drains", C.c_uint64), ("capture_s", C.c_double)]
+                ("rebuild_drains", C.c_uint64), ("capture_s", C.c_double),
+                ("tick_p99_ms", C.c_double), ("tick_max_ms", C.c_double)]
 
 
 class bm_tuft_form(C.Structure):

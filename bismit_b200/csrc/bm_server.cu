@@ -160,6 +160,7 @@ struct bm_server_s {
     static constexpr uint32_t kGraphAfter = 8;
     // Statistics.
     std::vector<float> lat_ms;
+    std::vector<float> tick_ms;          // device time of each tick (frames in to outputs out)
     uint64_t ticks = 0, frames_cycled = 0, rebuilds = 0;
     uint64_t rebuild_drains = 0;         // rebuilds that waited for the queued ticks (staging blocks grew)
     double syn_cycles = 0, busy_s = 0, first_tick = 0, last_tick = 0;
@@ -204,6 +205,15 @@ void free_session(bm_server_s::Session* S) {
 int build_session(bm_server_s* V, bm_server_s::Session* S) {
     int rc = bm_area_create(V->setup, &S->desc, S->seed, &S->area);
     if (rc != BM_OK) return rc;
+    // The gather-offset compile a new area's first cycle would run happens
+    // here, on the set-up stream, not inside a tick.
+    run_pending_verifies(S->area, V->setup->stream());
+    const cudaError_t e = cudaStreamSynchronize(V->setup->stream());
+    if (e != cudaSuccess) {
+        bm_area_destroy(S->area);
+        S->area = nullptr;
+        return cuda_err(e, "session set-up");
+    }
     if (cudaHostAlloc(&S->out, S->out_len ? S->out_len : 1, cudaHostAllocDefault) != cudaSuccess) {
         cudaGetLastError();
         bm_area_destroy(S->area);
@@ -345,7 +355,10 @@ int complete(bm_server_s* V, uint32_t b) {
     if (e != cudaSuccess) return cuda_err(e, "tick");
     const double t1 = now_s();
     float ms = 0.f;
-    if (cudaEventElapsedTime(&ms, V->start_ev[b], V->done_ev[b]) == cudaSuccess) V->gpu_s += ms * 1e-3;
+    if (cudaEventElapsedTime(&ms, V->start_ev[b], V->done_ev[b]) == cudaSuccess) {
+        V->gpu_s += ms * 1e-3;
+        V->tick_ms.push_back(ms);
+    }
     cudaGetLastError();
     uint64_t o = 0;
     for (size_t k = 0; k < T.members.size(); k++) {
@@ -745,6 +758,13 @@ int bm_server_get_stats(bm_server V, bm_server_stats* st) {
         };
         st->p50_ms = q(0.50);
         st->p99_ms = q(0.99);
+        if (!V->tick_ms.empty()) {
+            std::vector<float> t = V->tick_ms;
+            const size_t k = (size_t)(0.99 * (t.size() - 1) + 0.5);
+            std::nth_element(t.begin(), t.begin() + k, t.end());
+            st->tick_p99_ms = t[k];
+            st->tick_max_ms = *std::max_element(t.begin(), t.end());
+        }
         double sum = 0;
         for (float x : V->lat_ms) sum += x;
         st->mean_ms = sum / V->lat_ms.size();
@@ -755,6 +775,7 @@ int bm_server_get_stats(bm_server V, bm_server_stats* st) {
 int bm_server_reset_stats(bm_server V) {
     if (!V) return set_err(BM_ERR_INVALID, "null server");
     V->lat_ms.clear();
+    V->tick_ms.clear();
     V->ticks = V->frames_cycled = V->rebuilds = V->rebuild_drains = 0;
     V->syn_cycles = V->busy_s = V->first_tick = V->last_tick = V->rebuild_s = V->gpu_s = V->capture_s = 0;
     V->admit_s.store(0);

@@ -660,6 +660,8 @@ typedef struct bm_server_stats {
                                      batch's CUDA graph (a batch cycles by plain
                                      launches until its membership has held for
                                      8 ticks)                                    */
+    double   tick_p99_ms, tick_max_ms; /* device time of a tick: 99th percentile
+                                     and largest                                 */
 } bm_server_stats;
 
 /* mem_budget 0: 90 % of the device memory free at creation. */
