@@ -167,6 +167,7 @@ def learn_syns_per_cycle(area, plan, dev_frames, flen, first, n):
                 total += (ax != 0).sum() * per
             else:
                 total += pyr_learners(fb, ax, raw).sum() * per
+        area.axons_touched()
     torch.cuda.synchronize()
     return int(total.item()) / n
 
@@ -466,8 +467,8 @@ def run_hierarchy(args, ctx, stream, K, W, ws):
     kernels one area after another (one launch sequence per area, no graph)
     and (c) the plain form, one kernel per reference stage, one area after
     another. (b) and (c) deliver the tracts as the batch does: at the head of
-    each cycle every tract copies its source's output of the previous cycle,
-    then the areas cycle. The three arms' whole state slabs are compared."""
+    each cycle every tract copies its source's output of the previous cycle
+    (bm_area_deliver_tract), then the areas cycle. The three arms' whole state slabs are compared."""
     import torch
     from bismit_b200 import Cortex, configs, cortex, map as M
     lmaps, areas, names = configs.hierarchy()
@@ -507,18 +508,10 @@ def run_hierarchy(args, ctx, stream, K, W, ws):
         cx.batch.cycle_frames_device(fr.data_ptr() + c0 * fb, nc)
 
     def one_by_one(arm):
-        pairs = []
-        for (sk, so, dk, di, off, n) in cx.tracts:
-            ps, pd = arm[sk].plan, arm[dk].plan
-            src = arm[sk].slab_ptr() + int(ps.axon_off) + int(ps.outputs[so].axn_idz)
-            dst = arm[dk].slab_ptr() + int(pd.axon_off) + int(pd.inputs[di].axn_idz) + int(off)
-            pairs.append((torch.as_tensor(_DevBytes(src, n), device="cuda"),
-                          torch.as_tensor(_DevBytes(dst, n), device="cuda")))
-
         def run(c0, nc):
             for c in range(c0, c0 + nc):
-                for src, dst in pairs:
-                    dst.copy_(src)
+                for (sk, so, dk, di, off, _n) in cx.tracts:
+                    arm[dk].deliver_tract(arm[sk], so, di, off)
                 arm[0].cycle_frames_device(fr.data_ptr() + c * fb, fb, 1)
                 for a in arm[1:]:
                     a.cycle(1)
@@ -703,6 +696,11 @@ def run_serving(args, ctx):
         "rebuild_s": round(st["rebuild_s"], 3), "rebuild_drains": st["rebuild_drains"],
         "capture_s": round(st["capture_s"], 3), "admit_s": round(st["admit_s"], 3), "gpu_s": round(st["gpu_s"], 3),
         "tick_device_p99_ms": round(st["tick_p99_ms"], 3), "tick_device_max_ms": round(st["tick_max_ms"], 3),
+        "tick_device_max_at": {"tick": int(st["tick_max_no"]), "sessions": int(st["tick_max_members"]),
+                               "with": [w for w, b in (("first", 1), ("rebuild", 2), ("drain", 4), ("capture", 8))
+                                        if int(st["tick_max_what"]) & b]},
+        "tick_call_slowest": [[int(i), round(tick_calls[i] * 1e3, 3)] for i in np.argsort(tick_calls)[-3:][::-1]]
+        if tick_calls else None,
         "tick_call_p99_ms": round(float(np.percentile(tick_calls, 99)) * 1e3, 3) if tick_calls else None,
         "tick_call_max_ms": round(max(tick_calls) * 1e3, 3) if tick_calls else None,
         "tick_call_s": round(t_tick, 3), "submit_s": round(t_submit, 3), "wall_s": round(wall, 3),

@@ -180,7 +180,12 @@ class bm_server_stats(C.Structure):
                 ("used_bytes", C.c_uint64), ("budget_bytes", C.c_uint64),
                 ("resident", C.c_uint32), ("waiting", C.c_uint32), ("failed", C.c_uint32),
                 ("rebuild_drains", C.c_uint64), ("capture_s", C.c_double),
-                ("tick_p99_ms", C.c_double), ("tick_max_ms", C.c_double)]
+                ("tick_p99_ms", C.c_double), ("tick_max_ms", C.c_double), ("tick_max_no", C.c_uint64),
+                ("tick_max_members", C.c_uint32), ("tick_max_what", C.c_uint32)]
+
+
+# bm_server_stats.tick_max_what bits
+BM_TICK_FIRST, BM_TICK_REBUILD, BM_TICK_DRAIN, BM_TICK_CAPTURE = 1, 2, 4, 8
 
 
 class bm_tuft_form(C.Structure):
@@ -247,6 +252,7 @@ def lib():
         "bm_area_tuft_form": (C.c_int, [vp, u32, u32, P(bm_tuft_form)]),
         "bm_area_clear_errors": (C.c_int, [vp]),
         "bm_area_deliver_tract": (C.c_int, [vp, u32, vp, u32, u64]),
+        "bm_area_axons_touched": (C.c_int, [vp]),
         "bm_area_set_wait_limit": (C.c_int, [vp, u32]),
         "bm_area_inject_stall": (C.c_int, [vp, u32]),
         "bm_area_set_profiling": (C.c_int, [vp, C.c_int]),

@@ -190,6 +190,18 @@ class CorticalArea:
         F.check(self.lib.bm_area_slab_ptr(self.h, C.byref(p)))
         return p.value
 
+    def deliver_tract(self, src, src_output, dst_input, dst_offset):
+        """bm_area_deliver_tract: src's current output `src_output` into this
+        area's input `dst_input` at axon `dst_offset`, on this area's stream."""
+        F.check(self.lib.bm_area_deliver_tract(src.h, int(src_output), self.h, int(dst_input),
+                                               C.c_uint64(int(dst_offset))))
+
+    def axons_touched(self):
+        """Orders the next cycle's front steps after axon reads or writes the
+        caller queued on the area's stream through slab_ptr
+        (bm_area_axons_touched)."""
+        F.check(self.lib.bm_area_axons_touched(self.h))
+
     def side_steps(self):
         """Steps of the cycle that run beside the chain of dependent steps."""
         v = C.c_uint32()
@@ -560,7 +572,7 @@ class Cortex:
             for k, a in enumerate(areas):
                 for (sk, so, dk, di, off, _n) in self.tracts:
                     if dk == k:
-                        F.check(a.lib.bm_area_deliver_tract(areas[sk].h, so, a.h, di, C.c_uint64(off)))
+                        a.deliver_tract(areas[sk], so, di, off)
                 a.cycle(1)
 
     def area(self, name):

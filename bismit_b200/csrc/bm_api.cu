@@ -1392,7 +1392,22 @@ int bm_area_deliver_tract(bm_area src, uint32_t src_output, bm_area dst, uint32_
     frame_pieces(dst, dst_input, (uint32_t)dst_offset, len, pieces);
     const int rc = copy_pieces(pieces, from, cudaMemcpyDeviceToDevice, s);
     dst->mark_main();   // the destination's front steps read its inputs
+    if (src->stream() != s) {
+        // The source's next cycle overwrites the axons the copy reads.
+        cudaEvent_t e = dst->ev();
+        CU(cudaEventRecord(e, s));
+        CU(cudaStreamWaitEvent(src->stream(), e, 0));
+        dst->pool.push_back(e);
+    }
+    src->mark_main();
     return rc;
+}
+
+int bm_area_axons_touched(bm_area area) {
+    if (!area) return set_err(BM_ERR_INVALID, "null area");
+    DevGuard g(area->ctx->device);
+    area->mark_main();
+    return BM_OK;
 }
 
 int bm_area_clear_errors(bm_area area) {

@@ -131,6 +131,8 @@ struct bm_server_s {
         std::vector<double> submitted;
         double syn = 0, started = 0;
         uint32_t buf = 0;
+        uint32_t what = 0;    // BM_TICK_* bits of what the queueing call also did
+        uint64_t no = 0;      // tick number
     };
     bm_ctx ctx = nullptr;            // the serving stream
     bm_ctx setup = nullptr;          // area construction, overlapping the ticks
@@ -161,6 +163,9 @@ struct bm_server_s {
     // Statistics.
     std::vector<float> lat_ms;
     std::vector<float> tick_ms;          // device time of each tick (frames in to outputs out)
+    float tick_max = 0;                  // the slowest tick: device ms, number, members, BM_TICK_* bits
+    uint64_t tick_max_no = 0;
+    uint32_t tick_max_members = 0, tick_max_what = 0;
     uint64_t ticks = 0, frames_cycled = 0, rebuilds = 0;
     uint64_t rebuild_drains = 0;         // rebuilds that waited for the queued ticks (staging blocks grew)
     double syn_cycles = 0, busy_s = 0, first_tick = 0, last_tick = 0;
@@ -358,6 +363,12 @@ int complete(bm_server_s* V, uint32_t b) {
     if (cudaEventElapsedTime(&ms, V->start_ev[b], V->done_ev[b]) == cudaSuccess) {
         V->gpu_s += ms * 1e-3;
         V->tick_ms.push_back(ms);
+        if (ms > V->tick_max) {
+            V->tick_max = ms;
+            V->tick_max_no = T.no;
+            V->tick_max_members = (uint32_t)T.members.size();
+            V->tick_max_what = T.what;
+        }
     }
     cudaGetLastError();
     uint64_t o = 0;
@@ -622,8 +633,10 @@ int bm_server_tick(bm_server V, uint32_t* n_cycled) {
         if (S->resident && !S->frames.empty() && !S->area->seen_errors()) m.push_back(S);
     if (n_cycled) *n_cycled = (uint32_t)m.size();
     const uint32_t slot = (uint32_t)(V->tick_no & 1);
+    uint32_t what = V->tick_no == 0 ? BM_TICK_FIRST : 0u;
     if (!m.empty()) {
         if (m != V->members || !V->batch) {
+            what |= BM_TICK_REBUILD;
             // A new batch for the new membership; the previous tick stays
             // queued (its batch and gather table are released behind it),
             // unless a staging block must grow.
@@ -643,6 +656,7 @@ int bm_server_tick(bm_server V, uint32_t* n_cycled) {
                 rc = complete_all(V);
                 if (rc != BM_OK) return rc;
                 V->rebuild_drains++;
+                what |= BM_TICK_DRAIN;
             }
             rc = ensure_blocks(V->h_frames, V->d_frames, V->frames_cap, fb, "frame");
             if (rc == BM_OK) rc = build_outjobs(V);
@@ -657,6 +671,7 @@ int bm_server_tick(bm_server V, uint32_t* n_cycled) {
         T.started = t0;
         T.syn = 0;
         T.members = m;
+        T.no = V->tick_no;
         uint64_t o = 0;
         for (auto* S : m) {
             std::memcpy(V->h_frames[slot] + o, S->frames.front(), S->in_len);
@@ -677,7 +692,11 @@ int bm_server_tick(bm_server V, uint32_t* n_cycled) {
         }
         int rc = batch_cycle_frames_unchecked(V->batch, V->d_frames);
         if (rc != BM_OK) return rc;
-        if (capture) V->capture_s += now_s() - c0;
+        if (capture) {
+            V->capture_s += now_s() - c0;
+            what |= BM_TICK_CAPTURE;
+        }
+        T.what = what;
         if (V->out_blocks) k_gather_outputs<<<V->out_blocks, kGatherBlock, 0, s>>>(V->d_outjobs, (uint32_t)m.size(), V->d_out);
         e = cudaMemcpyAsync(V->h_out[slot], V->d_out, V->out_bytes, cudaMemcpyDeviceToHost, s);
         if (e == cudaSuccess) e = cudaEventRecord(V->done_ev[slot], s);
@@ -763,7 +782,10 @@ int bm_server_get_stats(bm_server V, bm_server_stats* st) {
             const size_t k = (size_t)(0.99 * (t.size() - 1) + 0.5);
             std::nth_element(t.begin(), t.begin() + k, t.end());
             st->tick_p99_ms = t[k];
-            st->tick_max_ms = *std::max_element(t.begin(), t.end());
+            st->tick_max_ms = V->tick_max;
+            st->tick_max_no = V->tick_max_no;
+            st->tick_max_members = V->tick_max_members;
+            st->tick_max_what = V->tick_max_what;
         }
         double sum = 0;
         for (float x : V->lat_ms) sum += x;
@@ -776,6 +798,9 @@ int bm_server_reset_stats(bm_server V) {
     if (!V) return set_err(BM_ERR_INVALID, "null server");
     V->lat_ms.clear();
     V->tick_ms.clear();
+    V->tick_max = 0;
+    V->tick_max_no = 0;
+    V->tick_max_members = V->tick_max_what = 0;
     V->ticks = V->frames_cycled = V->rebuilds = V->rebuild_drains = 0;
     V->syn_cycles = V->busy_s = V->first_tick = V->last_tick = V->rebuild_s = V->gpu_s = V->capture_s = 0;
     V->admit_s.store(0);

@@ -429,8 +429,17 @@ int bm_sampler_stats(bm_sampler sampler, uint64_t* sent, uint64_t* skipped);
 /* Device pointer of the state slab (for callers that move data with their own
  * copies on the same device). A caller that writes synapse sources or flags
  * through it must call bm_area_sources_changed for that layer before the next
- * cycle. */
+ * cycle; one that reads or writes axons (its own tract copies, say) with work
+ * queued on the area's stream must call bm_area_axons_touched after queueing
+ * it. */
 int bm_area_slab_ptr(bm_area area, void** out);
+/* The caller queued reads or writes of the area's axons on its stream
+ * (through bm_area_slab_ptr): the next cycle's front steps, which otherwise
+ * wait only for the previous cycle's steps they touch the buffers of, wait for
+ * the stream's current position. The area's own intakes and reads
+ * (bm_area_write_*, bm_area_read*, bm_area_deliver_tract, samplers) need no
+ * call. */
+int bm_area_axons_touched(bm_area area);
 /* Steps of the area's cycle that run on its side stream, beside the chain of
  * steps they do not touch (tuft steps that depend on nothing earlier in the
  * cycle, e.g. pyramidal distal tufts). Caller-written source slice ids
@@ -453,8 +462,9 @@ int bm_area_sources_changed(bm_area area, uint32_t layer);
  * `dst_offset`, landing where AxonSpace::intake puts a tract frame
  * (src/cortex/axon_space.rs:509-588; a filtered source's bytes into its
  * chain's first buffer). Enqueued on dst's stream after the work already
- * queued for src. A batch with tracts (bm_batch_connect) instead delivers
- * every tract at the head of each cycle, from the previous cycle. */
+ * queued for src; src's next cycle follows the copy. A batch with tracts
+ * (bm_batch_connect) instead delivers every tract at the head of each cycle,
+ * from the previous cycle. */
 int bm_area_deliver_tract(bm_area src, uint32_t src_output, bm_area dst, uint32_t dst_input, uint64_t dst_offset);
 
 /* Sticky device-side error bits of the area (bit 0: a bounded wait inside a
@@ -662,7 +672,16 @@ typedef struct bm_server_stats {
                                      8 ticks)                                    */
     double   tick_p99_ms, tick_max_ms; /* device time of a tick: 99th percentile
                                      and largest                                 */
+    uint64_t tick_max_no;         /* the slowest tick: its number (0: the first),  */
+    uint32_t tick_max_members;    /* its sessions, and BM_TICK_* bits of what the  */
+    uint32_t tick_max_what;       /* call that queued it also did                  */
 } bm_server_stats;
+
+/* bm_server_stats.tick_max_what */
+#define BM_TICK_FIRST   1u   /* the server's first tick                  */
+#define BM_TICK_REBUILD 2u   /* a new batch for a new membership         */
+#define BM_TICK_DRAIN   4u   /* the rebuild waited for the queued ticks  */
+#define BM_TICK_CAPTURE 8u   /* the batch's CUDA graph was captured      */
 
 /* mem_budget 0: 90 % of the device memory free at creation. */
 int bm_server_create(bm_ctx ctx, uint64_t mem_budget, bm_server* out);

@@ -114,3 +114,65 @@ def test_same_cycle_timing_differs_from_previous_cycle():
         oracle_cortex_cycle(plans, a, tracts, fr[c], c)
         oracle_cortex_cycle_in_order(plans, b, tracts, fr[c], c)
     assert not np.array_equal(a[1], b[1])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("delivery", ["api", "raw"])
+def test_unbatched_tracts_without_reads_match_oracle(delivery):
+    """Areas cycled one after another with every tract delivered at the head
+    of each cycle (the batched path's timing), six cycles queued with no read
+    in between, so that each area's front steps could run ahead of a tract's
+    copy: through bm_area_deliver_tract ("api"), or by the caller's own copies
+    on the area's stream followed by bm_area_axons_touched ("raw")."""
+    import torch
+    from bismit_b200.cortex import SAME_CYCLE
+    lm, ar, names = configs.hierarchy(SIDES)
+    cx = Cortex.builder(lm, ar).ca_settings(configs.bench_settings()).seed(5).tract_timing(SAME_CYCLE).build()
+    stream = torch.cuda.Stream()
+    cx.ctx.set_stream(stream.cuda_stream)
+    areas = [cx.area(n) for n in names]
+    plans = [a.plan for a in areas]
+    assert any(a.front_steps() for a in areas)
+    slabs = []
+    for k, a in enumerate(areas):
+        s = a.read_slab()
+        scramble(plans[k], s, 80 + k, clean_flags=True)
+        a.write_slab(s)
+        a.set_cycle(0)
+        slabs.append(s.copy())
+    copies = []
+    for (sk, so, dk, di, off, n) in cx.tracts:
+        ps, pd = plans[sk], plans[dk]
+        src = areas[sk].slab_ptr() + int(ps.axon_off) + int(ps.outputs[so].axn_idz)
+        dst = areas[dk].slab_ptr() + int(pd.axon_off) + int(pd.inputs[di].axn_idz) + int(off)
+        copies.append((_dev_bytes(src, n), _dev_bytes(dst, n)))
+    fr = configs.frames(6, SIDES[0] ** 2, 0.03, 9)
+    with torch.cuda.stream(stream):
+        for c in range(6):
+            if delivery == "api":
+                for (sk, so, dk, di, off, _n) in cx.tracts:
+                    areas[dk].deliver_tract(areas[sk], so, di, off)
+            else:
+                for src, dst in copies:
+                    dst.copy_(src)
+                for a in areas:   # every area's axons were read or written
+                    a.axons_touched()
+            areas[0].write_input(fr[c])
+            for a in areas:
+                a.cycle(1)
+    for c in range(6):
+        oracle_cortex_cycle(plans, slabs, cx.tracts, fr[c], c)
+    for k, n in enumerate(names):
+        dev = areas[k].read_slab()
+        assert np.array_equal(dev, slabs[k]), "%s:\n%s" % (n, diff_report(plans[k], dev, slabs[k]))
+    cx.close()
+
+
+def _dev_bytes(ptr, n):
+    """A torch u8 tensor over n bytes of device memory at ptr."""
+    import torch
+
+    class _View:
+        __cuda_array_interface__ = {"shape": (int(n),), "typestr": "|u1", "data": (int(ptr), False),
+                                    "version": 3, "strides": None, "stream": None}
+    return torch.as_tensor(_View(), device="cuda")
