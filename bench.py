@@ -698,7 +698,12 @@ def run_serving(args, ctx):
         "tick_device_p99_ms": round(st["tick_p99_ms"], 3), "tick_device_max_ms": round(st["tick_max_ms"], 3),
         "tick_device_max_at": {"tick": int(st["tick_max_no"]), "sessions": int(st["tick_max_members"]),
                                "with": [w for w, b in (("first", 1), ("rebuild", 2), ("drain", 4), ("capture", 8))
-                                        if int(st["tick_max_what"]) & b]},
+                                        if int(st["tick_max_what"]) & b],
+                               "queue_ms": round(st["tick_max_queue_ms"], 3),
+                               "builder": [w for w, b in (("build", 1), ("batch_free", 2), ("buffer_free", 4),
+                                                          ("area_free", 8), ("output_free", 16))
+                                           if int(st["tick_max_builder"]) & b],
+                               "builder_longest_ms": round(st["tick_max_builder_ms"], 3)},
         "tick_call_slowest": [[int(i), round(tick_calls[i] * 1e3, 3)] for i in np.argsort(tick_calls)[-3:][::-1]]
         if tick_calls else None,
         "tick_call_p99_ms": round(float(np.percentile(tick_calls, 99)) * 1e3, 3) if tick_calls else None,

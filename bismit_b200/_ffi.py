@@ -181,11 +181,16 @@ class bm_server_stats(C.Structure):
                 ("resident", C.c_uint32), ("waiting", C.c_uint32), ("failed", C.c_uint32),
                 ("rebuild_drains", C.c_uint64), ("capture_s", C.c_double),
                 ("tick_p99_ms", C.c_double), ("tick_max_ms", C.c_double), ("tick_max_no", C.c_uint64),
-                ("tick_max_members", C.c_uint32), ("tick_max_what", C.c_uint32)]
+                ("tick_max_members", C.c_uint32), ("tick_max_what", C.c_uint32),
+                ("tick_max_queue_ms", C.c_double), ("tick_max_builder", C.c_uint32), ("pad0", C.c_uint32),
+                ("tick_max_builder_ms", C.c_double)]
 
 
 # bm_server_stats.tick_max_what bits
 BM_TICK_FIRST, BM_TICK_REBUILD, BM_TICK_DRAIN, BM_TICK_CAPTURE = 1, 2, 4, 8
+# bm_server_stats.tick_max_builder bits
+BM_BUILDER_BUILD, BM_BUILDER_BATCH, BM_BUILDER_DEVICE_BUFFER, BM_BUILDER_AREA_FREE, BM_BUILDER_OUTPUT_FREE = \
+    1, 2, 4, 8, 16
 
 
 class bm_tuft_form(C.Structure):

@@ -1408,13 +1408,23 @@ void plan_tuft(FusedTuft& FT, const bm_area_plan& P, uint32_t i, uint32_t t, int
     bool tma = allow_tma && P.slc_u_size[lo] % 16 == 0 && P.slc_axn_idz[lo] % 16 == 0;
     for (uint32_t k = 1; k < nrec && tma; k++)
         tma = P.slc_axn_idz[lo + k] == P.slc_axn_idz[lo] + k * P.slc_v_size[lo] * P.slc_u_size[lo];
-    const uint64_t fwb = (fw + 15 + 15) / 16 * 16;
+    // Row pitch and shared-memory banks: a warp's byte gathers reach up to
+    // 2 * rv + 1 rows of one cell's neighbourhood, and rows whose pitch puts
+    // the same column in the same bank cost a wavefront each. A pitch of an
+    // odd number of words spreads 32 consecutive rows over every bank; a box
+    // row (a multiple of 16 bytes) does best at 16 bytes past a multiple of
+    // 32 (8 rows before a bank repeats, against 4 or fewer otherwise).
+    uint64_t fwb = (fw + 15 + 15) / 16 * 16;
+    if (fwb % 32 == 0 && fwb + 16 <= 256 && (uint64_t)nrec * frows * (fwb + 16) < 32768) fwb += 16;
     tma = tma && fwb <= 256 && frows <= 256 && (uint64_t)nrec * frows * fwb < 32768;
     if (tma) {
         fw = fwb;
-        fsz = frows * fw;
-        halo = (uint64_t)nrec * fsz;
+    } else {
+        const uint64_t fwo = fw + (12 - fw % 8) % 8;   // fw % 8 == 4: rows an odd number of words apart
+        if ((uint64_t)nrec * frows * fwo < 32768) fw = fwo;
     }
+    fsz = frows * fw;
+    halo = (uint64_t)nrec * fsz;
     // Windows: up to SB / 16 dendrites (or cells) per stage, widened by 16
     // at both ends.
     const uint32_t win_bytes = SB / 16 + 32;

@@ -31,6 +31,7 @@
 #include <atomic>
 #include <chrono>
 #include <condition_variable>
+#include <cstdlib>
 #include <cstring>
 #include <deque>
 #include <mutex>
@@ -108,7 +109,7 @@ struct bm_server_s {
         uint64_t bytes = 0;          // device bytes while resident
         bm_area area = nullptr;
         FrameQueue frames;
-        uint8_t* out = nullptr;      // pinned: output 0 after the latest cycled frame
+        uint8_t* out = nullptr;      // output 0 after the latest cycled frame (host memory)
         uint32_t out_len = 0, in_len = 0;
         uint64_t done = 0;           // frames cycled
         uint32_t inflight = 0;       // queued ticks holding one of its frames
@@ -133,6 +134,7 @@ struct bm_server_s {
         uint32_t buf = 0;
         uint32_t what = 0;    // BM_TICK_* bits of what the queueing call also did
         uint64_t no = 0;      // tick number
+        double enq0 = 0, enq1 = 0;   // host time around queueing its work
     };
     bm_ctx ctx = nullptr;            // the serving stream
     bm_ctx setup = nullptr;          // area construction, overlapping the ticks
@@ -166,6 +168,7 @@ struct bm_server_s {
     float tick_max = 0;                  // the slowest tick: device ms, number, members, BM_TICK_* bits
     uint64_t tick_max_no = 0;
     uint32_t tick_max_members = 0, tick_max_what = 0;
+    double tick_max_enq0 = 0, tick_max_enq1 = 0, tick_max_done = 0;   // its host-time window
     uint64_t ticks = 0, frames_cycled = 0, rebuilds = 0;
     uint64_t rebuild_drains = 0;         // rebuilds that waited for the queued ticks (staging blocks grew)
     double syn_cycles = 0, busy_s = 0, first_tick = 0, last_tick = 0;
@@ -189,6 +192,17 @@ struct bm_server_s {
         void* dev = nullptr;
     };
     std::deque<Teardown> free_q;
+    // The builder's recent operations (guarded by mu): host-time span and
+    // BM_BUILDER_* kind, to tell which ones overlapped a slow tick.
+    struct BuilderOp {
+        double t0, t1;
+        uint32_t kind;
+    };
+    std::vector<BuilderOp> builder_ops;
+    void log_op(double t0, uint32_t kind) {   // with mu held
+        if (builder_ops.size() >= 8192) builder_ops.erase(builder_ops.begin(), builder_ops.begin() + 4096);
+        builder_ops.push_back({t0, now_s(), kind});
+    }
 
     Session* find(uint32_t id) {
         for (Session* s : sessions)
@@ -201,7 +215,7 @@ namespace {
 
 void free_session(bm_server_s::Session* S) {
     if (S->area) bm_area_destroy(S->area);
-    if (S->out) cudaFreeHost(S->out);
+    std::free(S->out);
     delete S;
 }
 
@@ -219,8 +233,11 @@ int build_session(bm_server_s* V, bm_server_s::Session* S) {
         S->area = nullptr;
         return cuda_err(e, "session set-up");
     }
-    if (cudaHostAlloc(&S->out, S->out_len ? S->out_len : 1, cudaHostAllocDefault) != cudaSuccess) {
-        cudaGetLastError();
+    // The latest output, copied out of the pinned gather block on the host:
+    // plain memory (no page-locking, whose release would synchronize the
+    // device beside the ticks).
+    S->out = (uint8_t*)std::malloc(S->out_len ? S->out_len : 1);
+    if (!S->out) {
         bm_area_destroy(S->area);
         S->area = nullptr;
         return set_err(BM_ERR_OOM, "pinned output buffer");
@@ -240,14 +257,27 @@ void builder_loop(bm_server_s* V, int device) {
             const bm_server_s::Teardown T = V->free_q.front();
             V->free_q.pop_front();
             lk.unlock();
-            if (T.batch) bm_batch_destroy(T.batch);   // waits for the serving stream first
+            const double t0 = now_s();
+            uint32_t kind = 0;
+            if (T.batch) {
+                bm_batch_destroy(T.batch);   // waits for the serving stream first
+                kind |= BM_BUILDER_BATCH;
+            }
             if (T.dev) {
                 cudaStreamSynchronize(V->ctx->stream());
                 cudaFree(T.dev);
+                kind |= BM_BUILDER_DEVICE_BUFFER;
             }
-            if (T.area) bm_area_destroy(T.area);
-            if (T.out) cudaFreeHost(T.out);
+            if (T.area) {
+                bm_area_destroy(T.area);
+                kind |= BM_BUILDER_AREA_FREE;
+            }
+            if (T.out) {
+                std::free(T.out);
+                kind |= BM_BUILDER_OUTPUT_FREE;
+            }
             lk.lock();
+            V->log_op(t0, kind);
             continue;
         }
         if (!V->build_q.empty()) {
@@ -261,6 +291,7 @@ void builder_loop(bm_server_s* V, int device) {
             S->build.store(S->build_rc == BM_OK ? bm_server_s::kBuilt : bm_server_s::kFailed,
                            std::memory_order_release);
             lk.lock();
+            V->log_op(t0, BM_BUILDER_BUILD);
             continue;
         }
         if (V->stop) return;
@@ -368,6 +399,9 @@ int complete(bm_server_s* V, uint32_t b) {
             V->tick_max_no = T.no;
             V->tick_max_members = (uint32_t)T.members.size();
             V->tick_max_what = T.what;
+            V->tick_max_enq0 = T.enq0;
+            V->tick_max_enq1 = T.enq1;
+            V->tick_max_done = t1;
         }
     }
     cudaGetLastError();
@@ -681,6 +715,7 @@ int bm_server_tick(bm_server V, uint32_t* n_cycled) {
             S->frames.pop();
             S->inflight++;
         }
+        T.enq0 = now_s();
         cudaError_t e = cudaEventRecord(V->start_ev[slot], s);
         if (e == cudaSuccess) e = cudaMemcpyAsync(V->d_frames, V->h_frames[slot], o, cudaMemcpyHostToDevice, s);
         if (e != cudaSuccess) return cuda_err(e, "frame block copy");
@@ -701,6 +736,7 @@ int bm_server_tick(bm_server V, uint32_t* n_cycled) {
         e = cudaMemcpyAsync(V->h_out[slot], V->d_out, V->out_bytes, cudaMemcpyDeviceToHost, s);
         if (e == cudaSuccess) e = cudaEventRecord(V->done_ev[slot], s);
         if (e != cudaSuccess) return cuda_err(e, "tick");
+        T.enq1 = now_s();
         V->tick_no++;
     }
 
@@ -786,6 +822,13 @@ int bm_server_get_stats(bm_server V, bm_server_stats* st) {
             st->tick_max_no = V->tick_max_no;
             st->tick_max_members = V->tick_max_members;
             st->tick_max_what = V->tick_max_what;
+            st->tick_max_queue_ms = (V->tick_max_enq1 - V->tick_max_enq0) * 1e3;
+            std::lock_guard<std::mutex> g(V->mu);
+            for (const auto& op : V->builder_ops) {
+                if (op.t1 < V->tick_max_enq0 || op.t0 > V->tick_max_done) continue;
+                st->tick_max_builder |= op.kind;
+                st->tick_max_builder_ms = std::max(st->tick_max_builder_ms, (op.t1 - op.t0) * 1e3);
+            }
         }
         double sum = 0;
         for (float x : V->lat_ms) sum += x;
@@ -801,6 +844,7 @@ int bm_server_reset_stats(bm_server V) {
     V->tick_max = 0;
     V->tick_max_no = 0;
     V->tick_max_members = V->tick_max_what = 0;
+    V->tick_max_enq0 = V->tick_max_enq1 = V->tick_max_done = 0;
     V->ticks = V->frames_cycled = V->rebuilds = V->rebuild_drains = 0;
     V->syn_cycles = V->busy_s = V->first_tick = V->last_tick = V->rebuild_s = V->gpu_s = V->capture_s = 0;
     V->admit_s.store(0);

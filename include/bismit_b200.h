@@ -675,7 +675,20 @@ typedef struct bm_server_stats {
     uint64_t tick_max_no;         /* the slowest tick: its number (0: the first),  */
     uint32_t tick_max_members;    /* its sessions, and BM_TICK_* bits of what the  */
     uint32_t tick_max_what;       /* call that queued it also did                  */
+    double   tick_max_queue_ms;   /* host time queueing its work took              */
+    uint32_t tick_max_builder;    /* BM_BUILDER_* kinds of the builder thread's
+                                     operations between its queueing and its
+                                     completion, and the longest one's host ms   */
+    uint32_t pad0;
+    double   tick_max_builder_ms;
 } bm_server_stats;
+
+/* bm_server_stats.tick_max_builder */
+#define BM_BUILDER_BUILD          1u   /* a session's area built and grown      */
+#define BM_BUILDER_BATCH          2u   /* a retired batch released               */
+#define BM_BUILDER_DEVICE_BUFFER  4u   /* a retired gather table released        */
+#define BM_BUILDER_AREA_FREE      8u   /* a retired session's area released      */
+#define BM_BUILDER_OUTPUT_FREE   16u   /* a retired session's output buffer freed */
 
 /* bm_server_stats.tick_max_what */
 #define BM_TICK_FIRST   1u   /* the server's first tick                  */
