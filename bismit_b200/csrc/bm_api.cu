@@ -7,6 +7,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <new>
 #include <string>
 #include <vector>
@@ -827,10 +828,10 @@ void build_dev_layers(bm_area_s* A) {
 // stream keyed by its growth key.
 int prepare_regrow(bm_area_s* A, const std::vector<TuftGrowSpec>& grow, const std::vector<GrowTuft>& gts) {
     const bm_area_plan& P = A->plan;
-    cudaError_t e = cudaMalloc(&A->d_geo, sizeof A->geo);
+    cudaError_t e = dev_alloc(A->ctx, &A->d_geo, sizeof A->geo);
     if (e != cudaSuccess) return cuda_err(e, "regrowth geometry");
     refresh_geo(A);
-    e = cudaMemcpy(A->d_geo, A->geo, sizeof A->geo, cudaMemcpyHostToDevice);
+    e = cudaMemcpyAsync(A->d_geo, A->geo, sizeof A->geo, cudaMemcpyHostToDevice, A->stream());
     if (e != cudaSuccess) return cuda_err(e, "regrowth geometry");
     uint64_t blocks = 0;
     for (uint32_t k = 0; k < P.n_cycle_order; k++) {
@@ -857,9 +858,10 @@ int prepare_regrow(bm_area_s* A, const std::vector<TuftGrowSpec>& grow, const st
     }
     if (blocks > 0x7FFFFFFFull) return set_err(BM_ERR_UNSUPPORTED, "regrowth launch of too many blocks");
     if (A->regrow.empty()) return BM_OK;
-    e = cudaMalloc(&A->d_regrow, A->regrow.size() * sizeof(RegrowJob));
+    e = dev_alloc(A->ctx, &A->d_regrow, A->regrow.size() * sizeof(RegrowJob));
     if (e == cudaSuccess)
-        e = cudaMemcpy(A->d_regrow, A->regrow.data(), A->regrow.size() * sizeof(RegrowJob), cudaMemcpyHostToDevice);
+        e = cudaMemcpyAsync(A->d_regrow, A->regrow.data(), A->regrow.size() * sizeof(RegrowJob),
+                            cudaMemcpyHostToDevice, A->stream());
     if (e != cudaSuccess) return cuda_err(e, "regrowth jobs");
     A->regrow_blocks = (uint32_t)blocks;
     return BM_OK;
@@ -882,6 +884,44 @@ void free_upload(bm_area_s* A) {
 
 }  // namespace
 
+namespace {
+// Page-locked, device-mapped words handed out one at a time (bm::host_word_get).
+struct HostWords {
+    std::mutex mu;
+    std::vector<unsigned int*> free;
+};
+HostWords& host_words() {
+    static HostWords* w = new HostWords;   // kept for the process
+    return *w;
+}
+constexpr size_t kHostWordBlock = 1024;
+}  // namespace
+
+cudaError_t bm::host_word_get(unsigned int** host, unsigned int** dev) {
+    HostWords& W = host_words();
+    std::lock_guard<std::mutex> lk(W.mu);
+    if (W.free.empty()) {
+        unsigned int* blk = nullptr;
+        const cudaError_t e = cudaHostAlloc((void**)&blk, kHostWordBlock * sizeof(unsigned int),
+                                            cudaHostAllocMapped | cudaHostAllocPortable);
+        if (e != cudaSuccess) return e;
+        for (size_t k = kHostWordBlock; k-- > 0;) W.free.push_back(blk + k);
+    }
+    unsigned int* h = W.free.back();
+    const cudaError_t e = cudaHostGetDevicePointer((void**)dev, h, 0);
+    if (e != cudaSuccess) return e;
+    W.free.pop_back();
+    *(volatile unsigned int*)h = 0;
+    *host = h;
+    return cudaSuccess;
+}
+
+void bm::host_word_put(unsigned int* host) {
+    HostWords& W = host_words();
+    std::lock_guard<std::mutex> lk(W.mu);
+    W.free.push_back(host);
+}
+
 void bm::ctx_release(bm_ctx c) {
     if (!c || c->refs.fetch_sub(1, std::memory_order_acq_rel) != 1) return;
     DevGuard g(c->device);
@@ -895,21 +935,25 @@ void free_area(bm_area_s* A) {
     if (!A) return;
     if (A->ctx) {
         DevGuard g(A->ctx->device);
-        if (A->slab) cudaFree(A->slab);
-        if (A->ctl) cudaFree(A->ctl);
-        if (A->host_err) cudaFreeHost(A->host_err);
-        if (A->slices) cudaFree(A->slices);
+        // Batches and samplers first: they may still use the memory on their
+        // own streams. Pooled memory is then freed in order on the area's
+        // stream, which every cycle of the area ends on.
         detach_from_batches(A);
         free_samplers(A);
         free_upload(A);
+        const bool pl = A->pooled;
+        cudaStream_t s = A->stream();
+        dev_free(A->slab, pl, s);
+        dev_free(A->ctl, pl, s);
+        if (A->host_err) host_word_put(A->host_err);
+        dev_free(A->slices, pl, s);
         if (A->down) cudaStreamDestroy(A->down);
-        free_fused(A->fused);
-        if (A->d_regrow) cudaFree(A->d_regrow);
-        if (A->grow_offs) cudaFree(A->grow_offs);
-        if (A->d_geo) cudaFree(A->d_geo);
+        free_fused(A->fused, s);
+        dev_free(A->d_regrow, pl, s);
+        dev_free(A->grow_offs, pl, s);
+        dev_free(A->d_geo, pl, s);
         for (auto& row : A->d_centers)
-            for (int32_t* c : row)
-                if (c) cudaFree(c);
+            for (int32_t* c : row) dev_free(c, pl, s);
         if (A->side) cudaStreamDestroy(A->side);
         if (A->ev_fork) cudaEventDestroy(A->ev_fork);
         free_front_events(A);
@@ -1099,24 +1143,25 @@ int bm_area_create(bm_ctx ctx, const bm_area_desc* desc, uint64_t seed, bm_area*
     }
     A->ctx = ctx;
     ctx_retain(ctx);
+    A->pooled = ctx->pool != nullptr;
+    A->fused.pool = ctx->pool;
+    A->fused.pool_stream = ctx->stream();
     cudaStream_t s = ctx->stream();
-    cudaError_t e = cudaMalloc(&A->slab, A->plan.slab_bytes);
+    cudaError_t e = dev_alloc(ctx, &A->slab, A->plan.slab_bytes);
     if (e != cudaSuccess) {
         free_area(A);
         return set_err(BM_ERR_OOM, "cudaMalloc of %llu state bytes failed: %s",
                        (unsigned long long)A->plan.slab_bytes, cudaGetErrorString(e));
     }
-    e = cudaMalloc(&A->ctl, sizeof(AreaCtl));
-    if (e == cudaSuccess) e = cudaMalloc(&A->slices, sizeof(SliceRec) * BM_MAX_SLICES);
-    if (e == cudaSuccess) e = cudaHostAlloc(&A->host_err, sizeof(unsigned int), cudaHostAllocMapped);
+    e = dev_alloc(ctx, &A->ctl, sizeof(AreaCtl));
+    if (e == cudaSuccess) e = dev_alloc(ctx, &A->slices, sizeof(SliceRec) * BM_MAX_SLICES);
     if (e != cudaSuccess) { free_area(A); return cuda_err(e, "cudaMalloc"); }
-    *A->host_err = 0;
     std::vector<SliceRec> tab(BM_MAX_SLICES);
     fill_slice_table(A->plan, tab.data());
     AreaCtl ctl0{};
     unsigned int* dev_err = nullptr;
-    e = cudaHostGetDevicePointer((void**)&dev_err, A->host_err, 0);
-    if (e != cudaSuccess) { free_area(A); return cuda_err(e, "cudaHostGetDevicePointer"); }
+    e = host_word_get(&A->host_err, &dev_err);
+    if (e != cudaSuccess) { free_area(A); return cuda_err(e, "host-mapped error word"); }
     ctl0.host_err = dev_err;
     e = cudaMemsetAsync(A->slab, 0, A->plan.slab_bytes, s);
     if (e == cudaSuccess) e = cudaMemcpyAsync(A->slices, tab.data(), sizeof(SliceRec) * BM_MAX_SLICES, cudaMemcpyHostToDevice, s);
@@ -1131,10 +1176,10 @@ int bm_area_create(bm_ctx ctx, const bm_area_desc* desc, uint64_t seed, bm_area*
     int8_t* d_off = nullptr;
     size_t n_off = ov.size();
     if (n_off) {
-        e = cudaMalloc(&d_off, 2 * n_off);
+        e = dev_alloc(ctx, &d_off, 2 * n_off);
         if (e == cudaSuccess) e = cudaMemcpyAsync(d_off, ov.data(), n_off, cudaMemcpyHostToDevice, s);
         if (e == cudaSuccess) e = cudaMemcpyAsync(d_off + n_off, ou.data(), n_off, cudaMemcpyHostToDevice, s);
-        if (e != cudaSuccess) { if (d_off) cudaFree(d_off); free_area(A); return cuda_err(e, "growth pools"); }
+        if (e != cudaSuccess) { dev_free(d_off, A->pooled, s); free_area(A); return cuda_err(e, "growth pools"); }
     }
     uint32_t base = 0;
     std::vector<GrowTuft> gts;
@@ -1165,7 +1210,7 @@ int bm_area_create(bm_ctx ctx, const bm_area_desc* desc, uint64_t seed, bm_area*
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     const bool regrow = !(A->plan.settings & BM_SET_DISABLE_REGROWTH);
     if (regrow) A->grow_offs = d_off;   // kept: regrowth draws from the same pools
-    else if (d_off) cudaFree(d_off);
+    else dev_free(d_off, A->pooled, s);
     if (e != cudaSuccess) { free_area(A); return cuda_err(e, "synapse growth"); }
     rc = prepare_fused(A->fused, A->plan, &err);
     if (rc == BM_OK) rc = bind_fused(A->fused, A->plan, A->axns());
@@ -1181,9 +1226,10 @@ int bm_area_create(bm_ctx ctx, const bm_area_desc* desc, uint64_t seed, bm_area*
             if (L.ctrl[k].kind != BM_LYR_CTRL_SMOOTHER) continue;
             std::vector<int32_t> c;
             smoother_centers((int)L.ctrl[k].field_radius, (int)L.v_size, (int)L.u_size, c, A->center_off[i][k]);
-            e = cudaMalloc(&A->d_centers[i][k], std::max<size_t>(1, c.size()) * sizeof(int32_t));
+            e = dev_alloc(ctx, &A->d_centers[i][k], std::max<size_t>(1, c.size()) * sizeof(int32_t));
             if (e == cudaSuccess && !c.empty())
-                e = cudaMemcpy(A->d_centers[i][k], c.data(), c.size() * sizeof(int32_t), cudaMemcpyHostToDevice);
+                e = cudaMemcpyAsync(A->d_centers[i][k], c.data(), c.size() * sizeof(int32_t), cudaMemcpyHostToDevice,
+                                    s);
             if (e != cudaSuccess) { free_area(A); return cuda_err(e, "smoother centers"); }
         }
     }
@@ -1191,6 +1237,10 @@ int bm_area_create(bm_ctx ctx, const bm_area_desc* desc, uint64_t seed, bm_area*
     area_steps(A, A->steps, cell_tuft_cells(A) <= kFoldCellTufts);
     rc = schedule_area(A);
     if (rc != BM_OK) { free_area(A); return rc; }
+    // Tables copied up in order on the creating stream are in place before
+    // the area is cycled on whatever stream the context has then.
+    e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) { free_area(A); return cuda_err(e, "area set-up"); }
     *out = A;
     return BM_OK;
 }

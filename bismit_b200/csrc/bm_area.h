@@ -105,6 +105,10 @@ struct bm_ctx_s {
     // live area, batch, server and writer made on it; the last release frees
     // the context, so destroying it before its children is safe.
     std::atomic<int> refs{1};
+    // Device memory of the areas and batches made on this context comes from
+    // this pool in stream order when set (a server's contexts: areas come and
+    // go beside the ticks, and a plain free would wait for the whole device).
+    cudaMemPool_t pool = nullptr;
     cudaStream_t stream() const { return user_set ? user : own; }
 };
 namespace bm {
@@ -118,6 +122,27 @@ inline cudaError_t stream_like(cudaStream_t base, cudaStream_t* out) {
     }
     return cudaStreamCreateWithPriority(out, cudaStreamNonBlocking, prio);
 }
+// A device allocation of an object made on context c: from c's pool in
+// stream order on c's stream when it has one, else cudaMalloc.
+inline cudaError_t dev_alloc(bm_ctx c, void** p, size_t n) {
+    if (c && c->pool) return cudaMallocFromPoolAsync(p, n, c->pool, c->stream());
+    return cudaMalloc(p, n);
+}
+template <class T> inline cudaError_t dev_alloc(bm_ctx c, T** p, size_t n) {
+    return dev_alloc(c, (void**)p, n);
+}
+// Frees what dev_alloc gave: in stream order on s when it came from a pool,
+// else cudaFree (which first waits for the device).
+inline void dev_free(void* p, bool pooled, cudaStream_t s) {
+    if (!p) return;
+    if (pooled) cudaFreeAsync(p, s);
+    else cudaFree(p);
+}
+// A host-mapped word the device writes and the host polls (an area's error
+// mirror): slots of page-locked blocks kept for the process, so areas that
+// come and go page-lock and release nothing.
+cudaError_t host_word_get(unsigned int** host, unsigned int** dev);
+void host_word_put(unsigned int* host);
 inline void ctx_retain(bm_ctx c) {
     if (c) c->refs.fetch_add(1, std::memory_order_relaxed);
 }
@@ -131,6 +156,7 @@ struct bm_area_s {
     uint8_t* slab = nullptr;
     bm::AreaCtl* ctl = nullptr;
     unsigned int* host_err = nullptr;   // host-mapped mirror of ctl->error (written when non-zero)
+    bool pooled = false;                // device memory from the creating context's pool
     bm::SliceRec* slices = nullptr;
     bm::DevLayer dl[BM_MAX_LAYERS];
     uint64_t inhib_key[BM_MAX_LAYERS][BM_MAX_CTRL];

@@ -290,9 +290,10 @@ void bm::detach_from_batches(bm_area_s* A) {
 namespace {
 
 void free_plan(bm_batch_s* B) {
+    const bool pl = B->ctx->pool != nullptr;
     for (auto& p : B->plan) {
-        for (auto& c : p.cells) cudaFree(c.d_jobs);
-        if (p.d_regrow) cudaFree(p.d_regrow);
+        for (auto& c : p.cells) dev_free(c.d_jobs, pl, B->stream());
+        dev_free(p.d_regrow, pl, B->stream());
         free_fused_batch(p.fb);
     }
     B->plan.clear();
@@ -312,9 +313,10 @@ void free_batch(bm_batch_s* B) {
     }
     B->drop_graph();
     free_plan(B);
-    if (B->d_intake) cudaFree(B->d_intake);
-    if (B->d_bctl) cudaFree(B->d_bctl);
-    if (B->d_ctls) cudaFree(B->d_ctls);
+    const bool pl = B->ctx->pool != nullptr;
+    dev_free(B->d_intake, pl, B->stream());
+    dev_free(B->d_bctl, pl, B->stream());
+    dev_free(B->d_ctls, pl, B->stream());
     if (B->cap) cudaStreamDestroy(B->cap);
     if (B->side) cudaStreamDestroy(B->side);
     if (B->ev_fork) cudaEventDestroy(B->ev_fork);
@@ -337,7 +339,7 @@ uint64_t items_of(const bm_area_s* A, int k, const Step& st) {
 }
 
 // One batched per-cell launch of kind k for step st over every area.
-int add_cells(bm_batch_s::StepPlan& p, int k) {
+int add_cells(bm_ctx ctx, bm_batch_s::StepPlan& p, int k) {
     const Step& st = p.st;
     std::vector<CellJob> jobs;
     uint64_t blocks = 0;
@@ -367,10 +369,11 @@ int add_cells(bm_batch_s::StepPlan& p, int k) {
     }
     if (blocks > 0x7FFFFFFFull) return set_err(BM_ERR_UNSUPPORTED, "batched step of too many blocks");
     bm_batch_s::CellLaunch c{k, nullptr, (uint32_t)jobs.size(), (uint32_t)blocks};
-    cudaError_t e = cudaMalloc(&c.d_jobs, jobs.size() * sizeof(CellJob));
-    if (e == cudaSuccess) e = cudaMemcpy(c.d_jobs, jobs.data(), jobs.size() * sizeof(CellJob), cudaMemcpyHostToDevice);
+    cudaError_t e = dev_alloc(ctx, &c.d_jobs, jobs.size() * sizeof(CellJob));
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(c.d_jobs, jobs.data(), jobs.size() * sizeof(CellJob), cudaMemcpyHostToDevice, ctx->stream());
     if (e != cudaSuccess) {
-        if (c.d_jobs) cudaFree(c.d_jobs);
+        dev_free(c.d_jobs, ctx->pool != nullptr, ctx->stream());
         return cuda_err(e, "batched step jobs");
     }
     p.cells.push_back(c);
@@ -392,7 +395,7 @@ int build_fused(bm_batch_s::StepPlan& p) {
 }
 
 // Every area's regrowth jobs in one table (block0 rebased), one launch.
-int build_regrow(bm_batch_s::StepPlan& p) {
+int build_regrow(bm_ctx ctx, bm_batch_s::StepPlan& p) {
     std::vector<RegrowJob> jobs;
     uint64_t blocks = 0;
     for (bm_area A : p.areas)
@@ -406,8 +409,10 @@ int build_regrow(bm_batch_s::StepPlan& p) {
         p.form = bm_batch_s::F_END;
         return BM_OK;
     }
-    cudaError_t e = cudaMalloc(&p.d_regrow, jobs.size() * sizeof(RegrowJob));
-    if (e == cudaSuccess) e = cudaMemcpy(p.d_regrow, jobs.data(), jobs.size() * sizeof(RegrowJob), cudaMemcpyHostToDevice);
+    cudaError_t e = dev_alloc(ctx, &p.d_regrow, jobs.size() * sizeof(RegrowJob));
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(p.d_regrow, jobs.data(), jobs.size() * sizeof(RegrowJob), cudaMemcpyHostToDevice,
+                            ctx->stream());
     if (e != cudaSuccess) return cuda_err(e, "batched regrowth jobs");
     p.n_regrow = (uint32_t)jobs.size();
     p.regrow_blocks = (uint32_t)blocks;
@@ -415,14 +420,14 @@ int build_regrow(bm_batch_s::StepPlan& p) {
     return BM_OK;
 }
 
-int build_step(bm_batch_s::StepPlan& p) {
+int build_step(bm_ctx ctx, bm_batch_s::StepPlan& p) {
     const Step& st = p.st;
     if (st.kind == ST_CYCLE_END) {
         p.form = bm_batch_s::F_END;
         return BM_OK;
     }
-    if (st.kind == ST_REGROW) return build_regrow(p);
-    if (is_cell_step(st.kind)) return add_cells(p, st.kind);
+    if (st.kind == ST_REGROW) return build_regrow(ctx, p);
+    if (is_cell_step(st.kind)) return add_cells(ctx, p, st.kind);
     if (st.kind != ST_TUFT) return BM_OK;   // the plain form's whole-layer tuft stages: each area's own
     p.tufts.clear();
     for (bm_area A : p.areas) p.tufts.push_back({A, st.idx});
@@ -462,7 +467,7 @@ int build_step(bm_batch_s::StepPlan& p) {
     if (!none_ok) return BM_OK;
     // No area can take the fused kernel here (e.g. one-synapse dendrites):
     // the tuft's four stages per cell, batched.
-    return add_cells(p, BK_TUFT_CELLS);
+    return add_cells(ctx, p, BK_TUFT_CELLS);
 }
 
 // Consecutive batched tuft steps of one layer touch disjoint buffers: one
@@ -631,7 +636,7 @@ int build_plan(bm_batch_s* B) {
         bm_batch_s::StepPlan p;
         p.st = U[k];
         for (uint32_t a : who[k]) p.areas.push_back(B->areas[a]);
-        int rc = p.st.kind == ST_CYCLE_END ? (p.form = bm_batch_s::F_END, BM_OK) : build_step(p);
+        int rc = p.st.kind == ST_CYCLE_END ? (p.form = bm_batch_s::F_END, BM_OK) : build_step(B->ctx, p);
         B->plan.push_back(p);
         if (rc != BM_OK) return rc;
     }
@@ -644,7 +649,7 @@ int build_plan(bm_batch_s* B) {
 // The head-of-cycle copies: every tract, then every input of every area that
 // no tract feeds, taken from the frame block in (area, input) order.
 int build_intake(bm_batch_s* B) {
-    if (B->d_intake) cudaFree(B->d_intake);
+    dev_free(B->d_intake, B->ctx->pool != nullptr, B->stream());
     B->d_intake = nullptr;
     B->n_intake = B->intake_blocks = 0;
     B->frame_bytes = 0;
@@ -688,8 +693,10 @@ int build_intake(bm_batch_s* B) {
     }
     if (jobs.empty()) return BM_OK;
     if (blocks > 0x7FFFFFFFull) return set_err(BM_ERR_UNSUPPORTED, "batched intake too large");
-    cudaError_t e = cudaMalloc(&B->d_intake, jobs.size() * sizeof(IntakeJob));
-    if (e == cudaSuccess) e = cudaMemcpy(B->d_intake, jobs.data(), jobs.size() * sizeof(IntakeJob), cudaMemcpyHostToDevice);
+    cudaError_t e = dev_alloc(B->ctx, &B->d_intake, jobs.size() * sizeof(IntakeJob));
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(B->d_intake, jobs.data(), jobs.size() * sizeof(IntakeJob), cudaMemcpyHostToDevice,
+                            B->stream());
     if (e != cudaSuccess) return cuda_err(e, "batched intake jobs");
     B->n_intake = (uint32_t)jobs.size();
     B->intake_blocks = (uint32_t)blocks;
@@ -935,13 +942,20 @@ int bm_batch_create(bm_ctx ctx, const bm_area* areas, uint32_t n_areas, bm_batch
 
     std::vector<AreaCtl*> ctls;
     for (bm_area A : B->areas) ctls.push_back(A->ctl);
-    e = cudaMalloc(&B->d_bctl, sizeof(BatchCtl));
-    if (e == cudaSuccess) e = cudaMemset(B->d_bctl, 0, sizeof(BatchCtl));
-    if (e == cudaSuccess) e = cudaMalloc(&B->d_ctls, ctls.size() * sizeof(AreaCtl*));
-    if (e == cudaSuccess) e = cudaMemcpy(B->d_ctls, ctls.data(), ctls.size() * sizeof(AreaCtl*), cudaMemcpyHostToDevice);
+    e = dev_alloc(ctx, &B->d_bctl, sizeof(BatchCtl));
+    if (e == cudaSuccess) e = cudaMemsetAsync(B->d_bctl, 0, sizeof(BatchCtl), ctx->stream());
+    if (e == cudaSuccess) e = dev_alloc(ctx, &B->d_ctls, ctls.size() * sizeof(AreaCtl*));
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(B->d_ctls, ctls.data(), ctls.size() * sizeof(AreaCtl*), cudaMemcpyHostToDevice,
+                            ctx->stream());
     if (e != cudaSuccess) { free_batch(B); return cuda_err(e, "batch set-up"); }
     int rc = build_intake(B);
     if (rc == BM_OK) rc = build_plan(B);
+    // The job tables went up in order on the context's stream; a batch on a
+    // pooled context (a server's) is cycled on that stream, any other may be
+    // cycled on another stream once the caller changes it.
+    if (rc == BM_OK && !ctx->pool) e = cudaStreamSynchronize(ctx->stream());
+    if (rc == BM_OK && e != cudaSuccess) rc = cuda_err(e, "batch set-up");
     if (rc != BM_OK) { free_batch(B); return rc; }
     *out = B;
     return BM_OK;
@@ -1006,6 +1020,10 @@ int bm_batch_connect(bm_batch batch, uint32_t src_area, uint32_t src_output, uin
         B->tracts.pop_back();
         build_intake(B);
         return rc;
+    }
+    if (!B->ctx->pool) {
+        const cudaError_t e = cudaStreamSynchronize(B->stream());
+        if (e != cudaSuccess) return cuda_err(e, "tract intake tables");
     }
     return BM_OK;
 }

@@ -1522,11 +1522,14 @@ int prepare_fused(FusedArea& F, const bm_area_plan& P, std::string* err) {
             FusedTuft& FT = F.t[i][t];
             if (!FT.tiled) continue;
             const uint64_t n_syn = (uint64_t)P.layers[i].cells * P.layers[i].tufts[t].syns_per_tft;
-            if (cudaMalloc(&FT.gidx, n_syn * sizeof(int16_t)) != cudaSuccess) {
+            const cudaError_t e = F.pool ? cudaMallocFromPoolAsync((void**)&FT.gidx, n_syn * sizeof(int16_t), F.pool,
+                                                                   F.pool_stream)
+                                         : cudaMalloc(&FT.gidx, n_syn * sizeof(int16_t));
+            if (e != cudaSuccess) {
                 cudaGetLastError();
                 FT.gidx = nullptr;
                 if (err) *err = "cudaMalloc of the gather offsets failed";
-                free_fused(F);
+                free_fused(F, F.pool_stream);
                 return BM_ERR_OOM;
             }
         }
@@ -1603,11 +1606,12 @@ int bind_fused(FusedArea& F, const bm_area_plan& P, const uint8_t* axns) {
     return BM_OK;
 }
 
-void free_fused(FusedArea& F) {
+void free_fused(FusedArea& F, cudaStream_t s) {
     for (auto& row : F.t)
         for (auto& FT : row)
             if (FT.gidx) {
-                cudaFree(FT.gidx);
+                if (F.pool) cudaFreeAsync(FT.gidx, s);
+                else cudaFree(FT.gidx);
                 FT.gidx = nullptr;
             }
 }

@@ -44,6 +44,10 @@ struct FusedTuft {
 struct FusedArea {
     int sms = 148;
     FusedTuft t[BM_MAX_LAYERS][BM_MAX_TUFTS];
+    // Where the gather offsets come from: this pool in stream order on
+    // pool_stream when set, else cudaMalloc.
+    cudaMemPool_t pool = nullptr;
+    cudaStream_t pool_stream = nullptr;
 };
 
 // Decides, per tuft, whether the fused kernel applies (syns_per_den a power of
@@ -61,7 +65,8 @@ int plan_fused_tuft(FusedArea& F, const bm_area_plan& P, uint32_t layer, uint32_
 // which case the caller recompiles the offsets before the next launch.
 bool retile_fused_tuft(FusedArea& F, const bm_area_plan& P, uint32_t layer, uint32_t t, uint32_t target_syns,
                        bool* changed, bool staged = false);
-void free_fused(FusedArea& F);
+// Frees the gather offsets (pooled ones in stream order on s).
+void free_fused(FusedArea& F, cudaStream_t s = nullptr);
 // Encodes the footprint tensor maps of the tufts that load their footprint
 // with the tensor memory accelerator, for the axon space at `axns` (device
 // memory, 16-byte aligned). BM_ERR_CUDA when the driver refuses one.

@@ -138,6 +138,13 @@ struct bm_server_s {
     };
     bm_ctx ctx = nullptr;            // the serving stream
     bm_ctx setup = nullptr;          // area construction, overlapping the ticks
+    // Sessions' areas and the batches over them draw device memory from one
+    // pool in stream order (set-up on `setup`, batches and adopted areas on
+    // `serve`, a context on the serving stream): memory retired sessions
+    // release is freed behind the ticks that used it and reused by new ones,
+    // with no allocation or free that waits for the device beside the ticks.
+    cudaMemPool_t pool = nullptr;
+    bm_ctx serve = nullptr;
     uint64_t budget = 0, used = 0;
     uint32_t next_id = 1;
     std::vector<Session*> sessions;  // every open session, in open order
@@ -264,8 +271,7 @@ void builder_loop(bm_server_s* V, int device) {
                 kind |= BM_BUILDER_BATCH;
             }
             if (T.dev) {
-                cudaStreamSynchronize(V->ctx->stream());
-                cudaFree(T.dev);
+                dev_free(T.dev, true, V->serve->stream());   // behind the ticks that read it
                 kind |= BM_BUILDER_DEVICE_BUFFER;
             }
             if (T.area) {
@@ -319,9 +325,9 @@ void admit(bm_server_s* V, bm_server_s::Session* S) {
 // A built session joins the ticks: its area's later work goes to the serving
 // stream (same device).
 void adopt(bm_server_s* V, bm_server_s::Session* S) {
-    ctx_retain(V->ctx);
+    ctx_retain(V->serve);
     ctx_release(S->area->ctx);
-    S->area->ctx = V->ctx;
+    S->area->ctx = V->serve;
     S->resident = true;
     S->admitted = now_s();
 }
@@ -365,17 +371,17 @@ void retire_batch(bm_server_s* V) {
 // Grows a pair of pinned blocks and their device block, by half again what
 // is asked for (the stream must be idle: callers complete the queued ticks
 // before a growth).
-int ensure_blocks(uint8_t* (&h)[2], uint8_t*& d, uint64_t& cap, uint64_t bytes, const char* what) {
+int ensure_blocks(bm_ctx serve, uint8_t* (&h)[2], uint8_t*& d, uint64_t& cap, uint64_t bytes, const char* what) {
     if (bytes <= cap) return BM_OK;
     for (auto& p : h)
         if (p) cudaFreeHost(p);
-    if (d) cudaFree(d);
+    dev_free(d, true, serve->stream());
     h[0] = h[1] = nullptr;
     d = nullptr;
     cap = 0;
     uint64_t c = std::max<uint64_t>(bytes + bytes / 2, 1 << 20);
     if (cudaHostAlloc(&h[0], c, cudaHostAllocDefault) != cudaSuccess ||
-        cudaHostAlloc(&h[1], c, cudaHostAllocDefault) != cudaSuccess || cudaMalloc(&d, c) != cudaSuccess) {
+        cudaHostAlloc(&h[1], c, cudaHostAllocDefault) != cudaSuccess || dev_alloc(serve, &d, c) != cudaSuccess) {
         cudaGetLastError();
         return set_err(BM_ERR_OOM, "%s staging of %llu bytes", what, (unsigned long long)c);
     }
@@ -465,10 +471,12 @@ int build_outjobs(bm_server_s* V) {
         if (rc != BM_OK) return rc;
         V->rebuild_drains++;
     }
-    int rc = ensure_blocks(V->h_out, V->d_out, V->out_cap, o, "output");
+    int rc = ensure_blocks(V->serve, V->h_out, V->d_out, V->out_cap, o, "output");
     if (rc != BM_OK) return rc;
-    cudaError_t e = cudaMalloc(&V->d_outjobs, jobs.size() * sizeof(OutJob));
-    if (e == cudaSuccess) e = cudaMemcpy(V->d_outjobs, jobs.data(), jobs.size() * sizeof(OutJob), cudaMemcpyHostToDevice);
+    cudaError_t e = dev_alloc(V->serve, &V->d_outjobs, jobs.size() * sizeof(OutJob));
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(V->d_outjobs, jobs.data(), jobs.size() * sizeof(OutJob), cudaMemcpyHostToDevice,
+                            V->serve->stream());
     if (e != cudaSuccess) return cuda_err(e, "output gather jobs");
     return BM_OK;
 }
@@ -487,6 +495,31 @@ int bm_server_create(bm_ctx ctx, uint64_t mem_budget, bm_server* out) {
     if (rc != BM_OK) { delete V; return rc; }
     V->ctx = ctx;
     ctx_retain(ctx);
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = ctx->device;
+    V->serve = new (std::nothrow) bm_ctx_s;
+    cudaError_t pe = V->serve ? cudaMemPoolCreate(&V->pool, &props) : cudaErrorMemoryAllocation;
+    if (pe == cudaSuccess) {
+        // Memory freed to the pool stays there for the next sessions.
+        uint64_t keep = ~0ull;
+        pe = cudaMemPoolSetAttribute(V->pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
+    if (pe != cudaSuccess) {
+        cudaGetLastError();
+        if (V->pool) cudaMemPoolDestroy(V->pool);
+        delete V->serve;
+        bm_ctx_destroy(V->setup);
+        ctx_release(V->ctx);
+        delete V;
+        return cuda_err(pe, "server memory pool");
+    }
+    V->serve->device = ctx->device;
+    V->serve->user = ctx->stream();
+    V->serve->user_set = true;
+    V->serve->pool = V->pool;
+    V->setup->pool = V->pool;
     if (!mem_budget) {
         size_t fr = 0, tot = 0;
         cudaMemGetInfo(&fr, &tot);
@@ -500,7 +533,9 @@ int bm_server_create(bm_ctx ctx, uint64_t mem_budget, bm_server* out) {
             if (V->done_ev[b]) cudaEventDestroy(V->done_ev[b]);
             if (V->start_ev[b]) cudaEventDestroy(V->start_ev[b]);
         }
+        ctx_release(V->serve);
         bm_ctx_destroy(V->setup);
+        cudaMemPoolDestroy(V->pool);
         ctx_release(V->ctx);
         delete V;
         return set_err(BM_ERR_CUDA, "cudaEventCreate");
@@ -528,10 +563,14 @@ int bm_server_destroy(bm_server V) {
         if (V->done_ev[b]) cudaEventDestroy(V->done_ev[b]);
         if (V->start_ev[b]) cudaEventDestroy(V->start_ev[b]);
     }
-    if (V->d_frames) cudaFree(V->d_frames);
-    if (V->d_out) cudaFree(V->d_out);
-    if (V->d_outjobs) cudaFree(V->d_outjobs);
+    dev_free(V->d_frames, true, V->serve->stream());
+    dev_free(V->d_out, true, V->serve->stream());
+    dev_free(V->d_outjobs, true, V->serve->stream());
+    cudaStreamSynchronize(V->serve->stream());
+    ctx_release(V->serve);
     bm_ctx_destroy(V->setup);
+    // The pool's memory is released once every allocation from it is freed.
+    cudaMemPoolDestroy(V->pool);
     ctx_release(V->ctx);
     delete V;
     return BM_OK;
@@ -602,6 +641,7 @@ int bm_server_tick(bm_server V, uint32_t* n_cycled) {
     if (!V) return set_err(BM_ERR_INVALID, "null server");
     DevGuard g(V->ctx->device);
     cudaStream_t s = V->ctx->stream();
+    V->serve->user = s;   // the serving stream, should the caller have changed it
     const double t0 = now_s();
     if (!V->first_tick) V->first_tick = t0;
 
@@ -678,7 +718,7 @@ int bm_server_tick(bm_server V, uint32_t* n_cycled) {
             retire_batch(V);
             std::vector<bm_area> areas;
             for (auto* S : m) areas.push_back(S->area);
-            int rc = bm_batch_create(V->ctx, areas.data(), (uint32_t)areas.size(), &V->batch);
+            int rc = bm_batch_create(V->serve, areas.data(), (uint32_t)areas.size(), &V->batch);
             if (rc == BM_OK) rc = bm_batch_set_graph(V->batch, 0);
             if (rc != BM_OK) return rc;
             V->same_ticks = 0;
@@ -692,7 +732,7 @@ int bm_server_tick(bm_server V, uint32_t* n_cycled) {
                 V->rebuild_drains++;
                 what |= BM_TICK_DRAIN;
             }
-            rc = ensure_blocks(V->h_frames, V->d_frames, V->frames_cap, fb, "frame");
+            rc = ensure_blocks(V->serve, V->h_frames, V->d_frames, V->frames_cap, fb, "frame");
             if (rc == BM_OK) rc = build_outjobs(V);
             if (rc != BM_OK) return rc;
             V->rebuild_s += now_s() - r0;
