@@ -62,6 +62,10 @@ def test_sessions_in_the_mix_match_sessions_alone():
     st = srv.stats()
     assert st["frames"] == sum(s[4] for s in SESSIONS)
     assert st["p99_ms"] >= st["p50_ms"] > 0
+    # The slowest tick is described: its device time, number and sessions.
+    assert st["tick_max_ms"] >= st["tick_p99_ms"] > 0
+    assert st["tick_max_no"] < st["ticks"] and 1 <= st["tick_max_members"] <= len(SESSIONS)
+    assert st["tick_max_queue_ms"] >= 0
     srv.close()
     # Each session alone.
     for k, d in enumerate(descs):
