@@ -50,15 +50,15 @@ def parse():
     ap.add_argument("--serve-sessions", type=int, default=64)
     ap.add_argument("--serve-rate", type=float, default=200.0, help="mean session arrivals per second (Poisson)")
     ap.add_argument("--serve-budget-gb", type=float, default=8.0)
-    ap.add_argument("--profile-run", default=None, choices=["area", "batched", "encoders"],
+    ap.add_argument("--profile-run", default=None, choices=["area", "batched", "hierarchy", "encoders"],
                     help="only W warm-up and K timed cycles of the workload (area: --workload through the plain "
                          "cycling call, --workload also smoother or retina; batched: the --batch-instances batch, "
-                         "autotuned, graph replay; encoders: rounds of every device encoder into 64 frames of "
-                         "256 x 256), no soak, arms or baselines: a short launch sequence for a profiler's launch "
-                         "list")
+                         "autotuned, graph replay; hierarchy: the three-area cortex with its tracts, autotuned, "
+                         "graph replay; encoders: rounds of every device encoder into 64 frames of 256 x 256), "
+                         "no soak, arms or baselines: a short launch sequence for a profiler's launch list")
     ap.add_argument("--regrowth", action="store_true", help="--profile-run area: with synapse regrowth on")
     ap.add_argument("--autotune-cache", default=None,
-                    help="--profile-run batched: the autotuner's cache file (choices found there are applied "
+                    help="--profile-run batched or hierarchy: the autotuner's cache file (choices found there are applied "
                          "without trial launches; new ones are added)")
     return ap.parse_args()
 
@@ -975,6 +975,20 @@ def run_profile(args):
                 E.encode_hex_mold_scaled(ctx, 6, (side, side), (side, side), frames[0])
         launches = lambda: 5
         name = "encoders: 64 frames of 256 x 256 per encoder"
+    elif args.profile_run == "hierarchy":
+        from bismit_b200 import Cortex
+        lmaps, ar, names = configs.hierarchy()
+        cx = Cortex(lmaps, ar, configs.bench_settings(), seed=args.seed, ctx=ctx)
+        batch = cx.batch
+        batch.autotune(args.autotune_cache)
+        fb = batch.frame_bytes()
+        dev = torch.from_numpy(configs.frames(K + W, fb, 0.02, args.seed + 3)).to("cuda")
+        hier_syn = sum(int(cx.area(n).plan.n_syns_total) for n in names)
+
+        def cycles(c0, n):
+            batch.cycle_frames_device(dev.data_ptr() + c0 * fb, n)
+        launches = batch.launches_per_cycle
+        name = "hierarchy_3"
     else:
         frames_h = []
         for i, (side, depth, dens, syns, act) in enumerate(configs.batch_instances(args.batch_instances, args.seed)):
@@ -1000,13 +1014,15 @@ def run_profile(args):
     cycles(W, K)
     e1.record(stream)
     torch.cuda.synchronize()
-    n_syn = sum(int(a.plan.n_syns_total) for a in areas)
+    n_syn = hier_syn if args.profile_run == "hierarchy" else sum(int(a.plan.n_syns_total) for a in areas)
     if args.profile_run == "encoders":
         sdr.close()
     print(json.dumps({"profile_run": name, "steps": K, "warmup": W, "launches_per_cycle": launches(),
                       "synapses": n_syn, "ms_per_cycle": e0.elapsed_time(e1) / K}), flush=True)
     if args.profile_run == "batched":
         batch.close()
+    if args.profile_run == "hierarchy":
+        cx.close()
     for a in areas:
         a.close()
     ctx.close()
